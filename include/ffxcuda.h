@@ -1,0 +1,199 @@
+/*
+ * ffxcuda.h -- C ABI of the B200 AMOEBA energy/gradient library (libffxcuda.so).
+ *
+ * This is the drop-in boundary for Force Field X's AMOEBA polarizable
+ * energy-and-gradient path.  A Java `CudaForceFieldEnergy extends
+ * ForceFieldEnergy` (selected through the `platform` key in
+ * ForceFieldEnergy.energyFactory, modules/potential/.../ForceFieldEnergy.java:1464-1510,
+ * the same plug point OpenMMEnergy uses, modules/potential/.../openmm/OpenMMEnergy.java:80)
+ * binds these symbols with the JDK Foreign Function & Memory API.
+ *
+ * Conventions
+ *  - Plain C types only; every array is a caller-owned host buffer.  The
+ *    library copies in and out and never retains a caller pointer.
+ *  - Units follow Force Field X: Angstrom, electron, kcal/mol.  Multipoles are
+ *    passed in e, e*A, e*A^2 (already converted from the Bohr units of the
+ *    parameter file, MultipoleType.java:1115-1119), in the order
+ *    t000,t100,t010,t001,t200,t020,t002,t110,t101,t011 (MultipoleType.java:109-137).
+ *  - Every call returns an ffxg_status; 0 is success.  Java maps a nonzero
+ *    status to EnergyException (ffx/potential/utils/EnergyException.java), as the
+ *    reference throws at PCGSolver.java:554-568 and RealSpaceEnergyRegion.java:384-391.
+ *  - One handle owns one CUDA stream.  Calls on one handle must be serialised
+ *    by the caller; distinct handles may be used concurrently.
+ *  - There is no CPU fallback: if no sm_100 device is present, ffxg_create
+ *    returns FFXG_ERR_CUDA.
+ */
+#ifndef FFXCUDA_H
+#define FFXCUDA_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct ffxg_handle ffxg_handle;
+
+typedef enum {
+  FFXG_OK = 0,
+  FFXG_ERR_BAD_ARG = 1,       /* invalid argument / unsupported configuration */
+  FFXG_ERR_CUDA = 2,          /* CUDA runtime error or no usable device */
+  FFXG_ERR_SCF_DIVERGED = 3,  /* PCG residual grew (PCGSolver.java:547-559) */
+  FFXG_ERR_SCF_MAXITER = 4,   /* PCG hit the iteration cap (PCGSolver.java:563-568) */
+  FFXG_ERR_NONFINITE = 5,     /* NaN/Inf energy, torque or gradient */
+  FFXG_ERR_CAPACITY = 6       /* neighbour capacity exceeded even after regrowth */
+} ffxg_status;
+
+/* Local multipole frame definitions (MultipoleType.MultipoleFrameDefinition). */
+typedef enum {
+  FFXG_FRAME_NONE = 0,
+  FFXG_FRAME_ZONLY = 1,
+  FFXG_FRAME_ZTHENX = 2,
+  FFXG_FRAME_BISECTOR = 3,
+  FFXG_FRAME_ZTHENBISECTOR = 4,
+  FFXG_FRAME_THREEFOLD = 5
+} ffxg_frame;
+
+typedef enum {
+  FFXG_PRECISION_FP64 = 0,    /* plain FP64 form: the reference's arithmetic */
+  FFXG_PRECISION_MIXED = 1    /* FP32 pair tensors/splines/FFT, FP64 PCG scalars and energies */
+} ffxg_precision;
+
+typedef enum {
+  FFXG_POLAR_NONE = 0,
+  FFXG_POLAR_DIRECT = 1,
+  FFXG_POLAR_MUTUAL = 2
+} ffxg_polarization;
+
+/* Energy terms returned by ffxg_energy (kcal/mol). */
+enum {
+  FFXG_TERM_VDW = 0,
+  FFXG_TERM_PERMANENT = 1,       /* real + self + reciprocal + charge correction */
+  FFXG_TERM_POLARIZATION = 2,    /* real + self + reciprocal */
+  FFXG_TERM_PERM_REAL = 3,
+  FFXG_TERM_PERM_SELF = 4,
+  FFXG_TERM_PERM_RECIP = 5,
+  FFXG_TERM_POL_REAL = 6,
+  FFXG_TERM_POL_SELF = 7,
+  FFXG_TERM_POL_RECIP = 8,
+  FFXG_TERM_TOTAL = 9,
+  FFXG_N_TERMS = 10
+};
+
+/* Interaction counts returned by ffxg_energy. */
+enum {
+  FFXG_COUNT_VDW = 0,          /* VanDerWaals.getInteractions (VanDerWaals.java:583) */
+  FFXG_COUNT_PERMANENT = 1,    /* ParticleMeshEwald.getInteractions (ParticleMeshEwald.java:1014) */
+  FFXG_COUNT_SCF_ITER = 2,     /* completed PCG cycles (PCGSolver.scfByPCG return value) */
+  FFXG_COUNT_LIST_BUILDS = 3,  /* neighbour-list rebuilds performed during this call */
+  FFXG_COUNT_LIST_PAIRS = 4,   /* unordered pairs in the buffered neighbour list */
+  FFXG_N_COUNTS = 5
+};
+
+/* Resolved per-atom topology and parameters.  This is exactly the data that
+ * ParticleMeshEwald and VanDerWaals hold after assignment: localMultipole,
+ * frame/axisAtom (ParticleMeshEwald.java:2535-2600), polarizability / thole /
+ * ipdamp (:1395-1410), mask12..mask15 and ip11 (:1414-1445, :2616-2650), and the
+ * vdW class tables (VanDerWaalsForm.java:355-470). */
+typedef struct {
+  int32_t n_atoms;
+  const double *xyz;             /* [n][3] coordinates */
+  const double *multipole;       /* [n][10] local-frame multipoles */
+  const int32_t *frame;          /* [n] ffxg_frame */
+  const int32_t *axis;           /* [n][3] frame-defining atoms (z, x, y), -1 = unused */
+  const double *polarizability;  /* [n] A^3 */
+  const double *thole;           /* [n] Thole damping parameter */
+  const double *pdamp;           /* [n] polarizability^(1/6); <= 0 disables damping */
+  const int32_t *vdw_type;       /* [n] row of the vdW pair tables */
+  const int32_t *red_parent;     /* [n] heavy atom for hydrogen reduction (self if none) */
+  const double *red_factor;      /* [n] reduction factor (0 if none) */
+  int32_t n_vdw_types;
+  const double *vdw_inv_rmin;    /* [t][t] 1 / combined Rmin (0 = no interaction) */
+  const double *vdw_eps;         /* [t][t] combined well depth */
+  /* Bonded relationship lists in CSR form: ptr[n+1], idx[ptr[n]]. */
+  const int32_t *mask12_ptr, *mask12_idx;
+  const int32_t *mask13_ptr, *mask13_idx;
+  const int32_t *mask14_ptr, *mask14_idx;
+  const int32_t *mask15_ptr, *mask15_idx;
+  const int32_t *ip11_ptr, *ip11_idx;   /* polarization group of each atom (includes itself) */
+} ffxg_system;
+
+typedef struct {
+  double box[3];                 /* orthorhombic cell edges a, b, c (A) */
+  double vdw_cutoff;             /* A (vdw-cutoff) */
+  double vdw_taper;              /* fraction of the cutoff where the taper starts (vdw-taper, 0.9) */
+  double ewald_cutoff;           /* A (ewald-cutoff) */
+  double ewald_alpha;            /* 1/A (ewald-alpha) */
+  double list_buffer;            /* A (list-buffer, 2.0) */
+  int32_t pme_grid[3];           /* PME mesh dimensions */
+  int32_t pme_order;             /* B-spline order (5) */
+  double polar_eps;              /* PCG convergence, Debye RMS (polar-eps) */
+  int32_t max_scf_iter;          /* PCG iteration cap (1000 in the reference) */
+  int32_t polarization;          /* ffxg_polarization */
+  double precond_cutoff;         /* cg-preconditioner-cutoff (4.5) */
+  double precond_scale;          /* cg-preconditioner-scale (2.0) */
+  double electric;               /* 332.0637133 */
+  double m12, m13, m14, m15;     /* mpole-1n-scale */
+  double p12, p13, p14, p15;     /* polar-1n-scale */
+  double intra14;                /* polar-14-intra */
+  double d11;                    /* direct-11-scale */
+  double v12, v13, v14;          /* vdw-1n-scale */
+  int32_t precision;             /* ffxg_precision */
+} ffxg_params;
+
+/* Build a handle: validate the system, upload topology and parameters, pick a
+ * device, allocate device buffers.  Replaces the ForceFieldEnergy /
+ * ParticleMeshEwald / VanDerWaals constructors (ForceFieldEnergy.java:1207-1245,
+ * ParticleMeshEwald.java:490-741, VanDerWaals.java:308-404). */
+int ffxg_create(const ffxg_system *sys, const ffxg_params *params, ffxg_handle **out);
+
+/* Release every device resource held by the handle. */
+void ffxg_destroy(ffxg_handle *h);
+
+/* Last error message recorded on the handle (or the last create failure when h is NULL). */
+const char *ffxg_last_error(const ffxg_handle *h);
+
+/* Copy new coordinates ([n][3], A) to the device.  ForceFieldEnergy.setCoordinates
+ * (ForceFieldEnergy.java:2629). */
+int ffxg_set_coordinates(ffxg_handle *h, const double *xyz);
+
+/* Energy (and optionally gradient) at the current coordinates.
+ * ForceFieldEnergy.energy(gradient, print) (ForceFieldEnergy.java:1638-1800) for the
+ * vdW + PME terms.  terms[FFXG_N_TERMS] (kcal/mol), grad[n][3] (kcal/mol/A, may be
+ * NULL when want_grad == 0), counts[FFXG_N_COUNTS] (may be NULL). */
+int ffxg_energy(ffxg_handle *h, int want_grad, double *terms, double *grad, int64_t *counts);
+
+/* Same as ffxg_energy with the coordinates passed in: energyAndGradient(x, g)
+ * (ForceFieldEnergy.java:1843-1890) without the optimizer scaling. */
+int ffxg_energy_and_gradient(ffxg_handle *h, const double *xyz, double *terms, double *grad,
+                             int64_t *counts);
+
+/* Device-resident variant used by the benchmark and by callers that keep
+ * coordinates on the GPU: d_xyz[n][3] and d_grad[n][3] are device pointers on
+ * the handle's device; the call is asynchronous on the handle's stream except
+ * for the PCG convergence check.  terms/counts are host buffers. */
+int ffxg_energy_device(ffxg_handle *h, const double *d_xyz, double *d_grad, double *terms,
+                       int64_t *counts);
+
+/* Induced dipoles from the last energy call: ParticleMeshEwald.inducedDipole[0]
+ * and inducedDipoleCR[0] (ParticleMeshEwald.java:276-277), each [n][3] e*A. */
+int ffxg_get_induced_dipoles(ffxg_handle *h, double *u, double *u_cr);
+
+/* Global-frame multipoles from the last energy call ([n][10]). */
+int ffxg_get_global_multipoles(ffxg_handle *h, double *mpole);
+
+/* Pair set of the buffered neighbour list (NeighborList.java:905-1115) as
+ * unordered (i, k) with i < k.  With pairs == NULL only *n_pairs is written. */
+int ffxg_get_neighbor_pairs(ffxg_handle *h, int32_t *pairs, int64_t *n_pairs);
+
+/* The CUDA stream (cudaStream_t) the handle launches on, for event timing. */
+void *ffxg_stream(ffxg_handle *h);
+
+/* Device count of kernel launches issued by the last energy call. */
+int64_t ffxg_last_launch_count(const ffxg_handle *h);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* FFXCUDA_H */

@@ -1,0 +1,102 @@
+"""ctypes binding of liboracle.so, the CPU FP64 restatement of the reference path.
+
+TEST INFRASTRUCTURE: imported only by tests/, __graft_entry__.smoke() and
+bench.py's CPU-baseline leg, always as the checker or the timed CPU baseline.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+import subprocess
+
+import numpy as np
+
+from forcefieldx_b200 import cabi
+from forcefieldx_b200.system import AmoebaParams, AmoebaSystem, params_struct
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB = os.path.join(HERE, "liboracle.so")
+_lib = None
+
+
+def build(force: bool = False) -> str:
+    if force or not os.path.exists(LIB) or \
+            os.path.getmtime(LIB) < os.path.getmtime(os.path.join(HERE, "ffx_oracle.cpp")):
+        subprocess.run(["make", "-s", "-C", HERE, "liboracle.so"], check=True)
+    return LIB
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        build()
+        L = ctypes.CDLL(LIB)
+        D = ctypes.POINTER(ctypes.c_double)
+        L.oracle_energy.restype = ctypes.c_int
+        L.oracle_energy.argtypes = [ctypes.POINTER(cabi.FfxgSystem), ctypes.POINTER(cabi.FfxgParams), D,
+                                    ctypes.c_int, ctypes.c_int, D, D, ctypes.POINTER(ctypes.c_int64), D, D, D]
+        L.oracle_neighbor_pairs.restype = ctypes.c_int64
+        L.oracle_neighbor_pairs.argtypes = [ctypes.POINTER(cabi.FfxgSystem), ctypes.POINTER(cabi.FfxgParams), D,
+                                            ctypes.POINTER(ctypes.c_int32)]
+        L.oracle_erfc.restype = ctypes.c_double
+        L.oracle_erfc.argtypes = [ctypes.c_double]
+        L.oracle_bspline.restype = None
+        L.oracle_bspline.argtypes = [ctypes.c_double, ctypes.c_int, D]
+        L.oracle_fft3d.restype = None
+        L.oracle_fft3d.argtypes = [D, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int]
+        _lib = L
+    return _lib
+
+
+def _dp(a):
+    return a.ctypes.data_as(ctypes.POINTER(ctypes.c_double))
+
+
+def energy(system: AmoebaSystem, params: AmoebaParams, xyz=None, gradient=True, nthreads=0):
+    """Returns dict(terms, grad, counts, induced, induced_cr, global_mpole, status)."""
+    L = lib()
+    s, keep = system.c_struct(cabi)
+    p = params_struct(params, cabi)
+    n = system.n_atoms
+    x = np.ascontiguousarray(system.xyz if xyz is None else xyz, dtype=np.float64)
+    terms = np.zeros(cabi.N_TERMS)
+    grad = np.zeros((n, 3))
+    counts = np.zeros(cabi.N_COUNTS, dtype=np.int64)
+    ind = np.zeros((n, 3))
+    indcr = np.zeros((n, 3))
+    gm = np.zeros((n, 10))
+    st = L.oracle_energy(ctypes.byref(s), ctypes.byref(p), _dp(x), 1 if gradient else 0, int(nthreads),
+                         _dp(terms), _dp(grad), counts.ctypes.data_as(ctypes.POINTER(ctypes.c_int64)),
+                         _dp(ind), _dp(indcr), _dp(gm))
+    return dict(terms=terms, grad=grad, counts=counts, induced=ind, induced_cr=indcr,
+                global_mpole=gm, status=int(st))
+
+
+def neighbor_pairs(system: AmoebaSystem, params: AmoebaParams, xyz=None) -> np.ndarray:
+    L = lib()
+    s, keep = system.c_struct(cabi)
+    p = params_struct(params, cabi)
+    x = np.ascontiguousarray(system.xyz if xyz is None else xyz, dtype=np.float64)
+    n = L.oracle_neighbor_pairs(ctypes.byref(s), ctypes.byref(p), _dp(x), None)
+    out = np.zeros((n, 2), dtype=np.int32)
+    L.oracle_neighbor_pairs(ctypes.byref(s), ctypes.byref(p), _dp(x),
+                            out.ctypes.data_as(ctypes.POINTER(ctypes.c_int32)))
+    return out
+
+
+def erfc(x: float) -> float:
+    return lib().oracle_erfc(float(x))
+
+
+def bspline(x: float, order: int = 5) -> np.ndarray:
+    out = np.zeros((order, 4))
+    lib().oracle_bspline(float(x), int(order), _dp(out))
+    return out
+
+
+def fft3d(data: np.ndarray, sign: int) -> np.ndarray:
+    """data: complex128 array of shape (nz, ny, nx)."""
+    nz, ny, nx = data.shape
+    buf = np.ascontiguousarray(np.stack([data.real, data.imag], axis=-1), dtype=np.float64)
+    lib().oracle_fft3d(_dp(buf), nx, ny, nz, int(sign))
+    return buf[..., 0] + 1j * buf[..., 1]

@@ -1,0 +1,26 @@
+"""Pin the CPU oracle to the reference's own golden energies and interaction counts.
+
+EnergyTest.java (modules/potential/src/test/java/ffx/potential/commands/EnergyTest.java)
+asserts per-term energies to 1e-2 kcal/mol and exact interaction counts for DHFR
+(:147-182) and ubiquitin (:363-398); tests/golden/make_fixtures.py resolved the
+same inputs into tests/golden/*_system.npz.
+"""
+import pytest
+
+from oracle import binding as ob
+from tests.common import golden_system
+
+
+@pytest.mark.parametrize("name", ["ubiquitin", "dhfr"])
+def test_oracle_matches_reference_golden(name, fixtures):
+    system, params = golden_system(name, fixtures)
+    g = fixtures[name]["golden"]
+    tol = g["tolerance"]
+    r = ob.energy(system, params, gradient=False)
+    assert r["status"] == 0
+    t, c = r["terms"], r["counts"]
+    assert abs(t[0] - g["vdw"]) < tol
+    assert abs(t[1] - g["permanent"]) < tol
+    assert abs(t[2] - g["polarization"]) < tol
+    assert c[0] == g["n_vdw"]
+    assert c[1] == g["n_permanent"]
