@@ -64,7 +64,12 @@ PROTOTYPES = {
     "ffxg_get_neighbor_pairs": (ctypes.c_int, [ctypes.c_void_p, _I, _L]),
     "ffxg_stream": (ctypes.c_void_p, [ctypes.c_void_p]),
     "ffxg_last_launch_count": (ctypes.c_int64, [ctypes.c_void_p]),
+    "ffxg_set_timing": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int]),
+    "ffxg_get_timings": (ctypes.c_int, [ctypes.c_void_p, _D, _L, ctypes.c_int]),
 }
+
+STAGE_NAMES = ["lists", "vdw", "multipoles", "perm_recip", "perm_field", "ind_recip", "ind_field",
+               "precond", "pcg_vector", "real_energy", "recip_energy", "gradient"]
 
 LIB_PATH = os.path.join(os.path.dirname(os.path.abspath(__file__)), "libffxcuda.so")
 

@@ -1,0 +1,246 @@
+// ffx_internal.cuh -- shared definitions of the B200 AMOEBA energy/gradient library.
+//
+// Data layout in HBM (all per-atom arrays are structure-of-arrays, index = atom):
+//   x,y,z            coordinates (double)
+//   rx,ry,rz         hydrogen-reduced vdW coordinates (double)
+//   gm[10][n]        global-frame multipoles
+//   fm[10][n]        fractional multipoles (PME)
+//   uD,uP[3][n]      induced dipoles (direct-field / chain-rule systems)
+//   nbr[n][cap]      buffered Verlet list (both directions), nbr_cnt[n]
+//   ewl[n][capE]     real-space (Ewald) list, ewl_cnt[n]
+//   prl[n][capP]     preconditioner list, prl_cnt[n]
+//   grid[nz][ny][nx] interleaved complex PME mesh (double2)
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include <string>
+#include <vector>
+
+#include "../../include/ffxcuda.h"
+
+namespace ffx {
+
+constexpr int kWarp = 32;
+constexpr int kOrder = 5;            // PME B-spline order supported by the kernels
+constexpr double kElecAngToDebye = 4.80321;
+
+// Status bits written by kernels into Handle::d_flags.
+enum : int {
+  FLAG_NBR_OVERFLOW = 1,
+  FLAG_EWALD_OVERFLOW = 2,
+  FLAG_PRECOND_OVERFLOW = 4,
+  FLAG_NONFINITE = 8,
+  FLAG_REBUILD = 16,
+};
+
+// Exclusion codes: bits 0-2 mpole class, 3-5 polar class, 6 same polarization group,
+// 7-8 vdW class.
+struct ScaleTables {
+  double m[5];   // 1, m12, m13, m14, m15
+  double p[5];   // 1, p12, p13, p14, intra14*p14
+  double d[2];   // 1, d11
+  double v[4];   // 1, v12, v13, v14
+};
+
+// Cell / Crystal description for the device (orthorhombic; the general
+// fractional round trip of Crystal.image is kept term by term).
+struct Box {
+  double a, b, c;
+  double A00, A11, A22;    // 1/a, 1/b, 1/c
+  double Ai00, Ai11, Ai22; // a, b, c
+  double volume;
+};
+
+// Minimum image exactly as Crystal.image (Crystal.java:1069-1083): no FMA
+// contraction, Java signum semantics, same operation order.
+__device__ __forceinline__ double jsignum(double v) { return v > 0.0 ? 1.0 : (v < 0.0 ? -1.0 : v); }
+
+__device__ __forceinline__ double image_exact(double &x, double &y, double &z, const Box &bx) {
+  double xf = __dmul_rn(x, bx.A00);
+  double yf = __dmul_rn(y, bx.A11);
+  double zf = __dmul_rn(z, bx.A22);
+  xf = __dadd_rn(__dmul_rn(floor(__dadd_rn(fabs(xf), 0.5)), jsignum(-xf)), xf);
+  yf = __dadd_rn(__dmul_rn(floor(__dadd_rn(fabs(yf), 0.5)), jsignum(-yf)), yf);
+  zf = __dadd_rn(__dmul_rn(floor(__dadd_rn(fabs(zf), 0.5)), jsignum(-zf)), zf);
+  x = __dmul_rn(xf, bx.Ai00);
+  y = __dmul_rn(yf, bx.Ai11);
+  z = __dmul_rn(zf, bx.Ai22);
+  return __dadd_rn(__dadd_rn(__dmul_rn(x, x), __dmul_rn(y, y)), __dmul_rn(z, z));
+}
+
+template <typename T>
+__device__ __forceinline__ T warp_sum(T v) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  return v;
+}
+
+// PME transforms of one handle (passed to kernels by value).
+struct PmeConst {
+  double tmm[10][10];   // ReciprocalSpace.transformMultipoleMatrix
+  double tfm[10][10];   // ReciprocalSpace.transformFieldMatrix
+  double afrac[3][3];   // Cartesian -> fractional dipole (ReciprocalSpace.a)
+  double recip[3][3];   // crystal.A
+};
+
+// One axis of the batched line FFT (see pme.cu).
+struct FftAxis {
+  int len;            // transform length
+  int stride;         // element stride within a line (complex units)
+  int L;              // lines per CTA
+  int line_step;      // memory step between adjacent lines of a CTA group
+  int groups_inner;   // CTA groups along the inner index
+  int group_step_inner, group_step_outer;
+  int nradix;
+  int radix[12];
+};
+
+struct Handle {
+  // ---- configuration
+  int n = 0;
+  ffxg_params prm{};
+  Box box{};
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  std::string err;
+  int64_t launches = 0;
+
+  // ---- static per-atom parameters (device)
+  double *d_lmp = nullptr;        // [10][n] local multipoles
+  int *d_frame = nullptr;         // [n]
+  int *d_axis = nullptr;          // [3][n]
+  double *d_polar = nullptr, *d_thole = nullptr, *d_ipdamp = nullptr;
+  int *d_vtype = nullptr, *d_redp = nullptr;
+  double *d_redf = nullptr;
+  int ntypes = 0;
+  double *d_vrad = nullptr, *d_veps = nullptr;   // [t][t]
+  int *d_excl_ptr = nullptr, *d_excl_k = nullptr;  // exclusions CSR (sorted by k)
+  unsigned *d_excl_code = nullptr;
+  int *d_excl_lo = nullptr, *d_excl_hi = nullptr;  // min/max partner per atom
+  int *d_tq_ptr = nullptr, *d_tq_ent = nullptr;    // torque gather CSR: entry = i*4 + slot
+  int *d_red_ptr = nullptr, *d_red_child = nullptr;  // reduction children CSR
+  ScaleTables scales{};
+
+  // ---- coordinates and list state
+  double *d_x = nullptr, *d_y = nullptr, *d_z = nullptr;
+  double *d_rx = nullptr, *d_ry = nullptr, *d_rz = nullptr;
+  double *d_refx = nullptr, *d_refy = nullptr, *d_refz = nullptr;  // list reference coords
+  bool list_valid = false;
+  int ncell[3] = {0, 0, 0};
+  int *d_cell_cnt = nullptr, *d_cell_start = nullptr, *d_cell_atoms = nullptr, *d_atom_cell = nullptr;
+  int cap_nbr = 0, cap_ewl = 0, cap_prl = 0;
+  int *d_nbr = nullptr, *d_nbr_cnt = nullptr;
+  int *d_ewl = nullptr, *d_ewl_cnt = nullptr;
+  int *d_prl = nullptr, *d_prl_cnt = nullptr;
+
+  // ---- electrostatics work arrays
+  double *d_gm = nullptr;                     // [10][n]
+  double *d_fm = nullptr;                     // [10][n]
+  double *d_spl = nullptr;                    // [n][3][order][4]
+  int *d_igrid = nullptr;                     // [3][n]
+  double *d_cphi = nullptr, *d_fphi = nullptr;    // [20][n] permanent
+  double *d_cphiI = nullptr, *d_fphiI = nullptr;  // [20][n] induced D
+  double *d_cphiP = nullptr, *d_fphiP = nullptr;  // [20][n] induced CR
+  double *d_fieldD = nullptr, *d_fieldP = nullptr;  // [3][n]
+  double *d_uD = nullptr, *d_uP = nullptr, *d_udirD = nullptr, *d_udirP = nullptr;
+  // PCG vectors [3][n]
+  double *d_r = nullptr, *d_rP = nullptr, *d_zpre = nullptr, *d_zpreP = nullptr, *d_p = nullptr, *d_pP = nullptr;
+  double *d_vec = nullptr, *d_vecP = nullptr;
+  double *d_partials = nullptr;               // block partial sums [nblk][8]
+  double *d_scalars = nullptr;                // PCG scalars on device
+  double *h_scalars = nullptr;                // pinned mirror
+  // PME
+  int nfft[3] = {0, 0, 0};
+  double2 *d_grid = nullptr;
+  double *d_influence = nullptr;
+  double2 *d_twiddle = nullptr;               // per-axis twiddle tables (3 x max n)
+  PmeConst pc{};
+  FftAxis axes[3]{};
+
+  // ---- outputs
+  double *d_grad = nullptr, *d_torque = nullptr;  // [3][n]
+  double *d_gred = nullptr;                        // [3][n] vdW reduced-site force
+  double *d_eatom = nullptr;                       // [8][n] per-atom energy terms
+  long long *d_catom = nullptr;                    // [2][n] per-atom counts
+  double *d_result = nullptr;                      // reduced terms
+  long long *d_cresult = nullptr;
+  int *d_flags = nullptr;
+  int *h_flags = nullptr;
+  double *d_xyz_in = nullptr, *d_grad_out = nullptr;  // interleaved staging [n][3]
+  double *h_xyz_pin = nullptr, *h_grad_pin = nullptr;
+
+  int scf_iter = 0;
+  double e_charge_correction = 0.0;
+  // Stage timers (PMETimings counterpart).
+  bool timing = false;
+  std::vector<cudaEvent_t> ev_pool;
+  std::vector<int> ev_stage;       // stage of each begin/end pair recorded this call
+  int ev_used = 0;
+  double stage_ms[16] = {0};
+  int64_t stage_calls[16] = {0};
+  int64_t list_builds = 0;
+};
+
+// ---- kernels / launchers (defined in the .cu files)
+void launch_set_coordinates(Handle &h, const double *d_xyz);
+void launch_neighbor_list(Handle &h, bool force);
+void launch_realspace_lists(Handle &h);
+void launch_vdw(Handle &h, bool grad);
+void launch_rotate(Handle &h);
+void launch_bsplines(Handle &h);
+void launch_spread_permanent(Handle &h);
+void launch_spread_induced(Handle &h, const double *ud, const double *up);
+void launch_fft_convolution(Handle &h);
+void launch_phi_permanent(Handle &h);
+void launch_phi_induced(Handle &h, bool full);
+void launch_permanent_field(Handle &h);
+void launch_direct(Handle &h);
+void launch_induced_recip(Handle &h, const double *ud, const double *up);
+void launch_induced_real(Handle &h, const double *ud, const double *up, double *outD, double *outP);
+void launch_precond_field(Handle &h, const double *rD, const double *rP, double *outD, double *outP);
+int run_pcg(Handle &h);
+void launch_recip_energy(Handle &h, bool grad);
+void launch_real_energy(Handle &h, bool grad);
+void launch_torque(Handle &h);
+void launch_assemble(Handle &h, double *d_grad_xyz);
+void launch_reduce_results(Handle &h);
+void setup_pme(Handle &h);
+
+inline int nblocks(int64_t n, int t) { return (int)((n + t - 1) / t); }
+
+// Bracket a stage with events when timing is on; returns a token for timer_end.
+inline int timer_begin(Handle &h, int stage) {
+  if (!h.timing) return -1;
+  if (h.ev_used + 2 > (int)h.ev_pool.size()) {
+    for (int k = 0; k < 64; k++) {
+      cudaEvent_t e;
+      cudaEventCreate(&e);
+      h.ev_pool.push_back(e);
+    }
+  }
+  const int tok = h.ev_used;
+  h.ev_used += 2;
+  h.ev_stage.push_back(stage);
+  cudaEventRecord(h.ev_pool[tok], h.stream);
+  return tok;
+}
+inline void timer_end(Handle &h, int tok) {
+  if (tok >= 0) cudaEventRecord(h.ev_pool[tok + 1], h.stream);
+}
+// Accumulate the recorded pairs (stream must be synchronised).
+inline void timer_collect(Handle &h) {
+  for (size_t q = 0; q < h.ev_stage.size(); q++) {
+    float ms = 0.f;
+    cudaEventElapsedTime(&ms, h.ev_pool[2 * q], h.ev_pool[2 * q + 1]);
+    h.stage_ms[h.ev_stage[q]] += ms;
+    h.stage_calls[h.ev_stage[q]] += 1;
+  }
+  h.ev_stage.clear();
+  h.ev_used = 0;
+}
+
+#define FFX_LAUNCHED(h) ((h).launches++)
+
+}  // namespace ffx

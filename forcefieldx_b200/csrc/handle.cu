@@ -1,0 +1,560 @@
+// handle.cu -- the C ABI (include/ffxcuda.h) and the per-evaluation pipeline.
+//
+// One evaluation follows ForceFieldEnergy.energy (ForceFieldEnergy.java:1638-1800) for the
+// vdW and PME terms and ParticleMeshEwald.computeEnergy (ParticleMeshEwald.java:1871-2183):
+//   coordinates -> reduced coordinates + motion check -> (re)build lists when needed
+//   -> vdW -> rotate multipoles -> B-splines -> permanent spread/FFT/phi -> permanent field
+//   -> direct dipoles -> PCG -> induced phi -> reciprocal and real-space energy/gradient
+//   -> torque to gradient -> deterministic sums.
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <map>
+#include <string>
+#include <vector>
+
+#include "ffx_internal.cuh"
+
+struct ffxg_handle {
+  ffx::Handle h;
+};
+
+using namespace ffx;
+
+static std::string g_create_error;
+
+#define CK(call)                                                                    \
+  do {                                                                              \
+    cudaError_t e_ = (call);                                                        \
+    if (e_ != cudaSuccess) {                                                        \
+      h.err = std::string(#call) + ": " + cudaGetErrorString(e_);                   \
+      return FFXG_ERR_CUDA;                                                         \
+    }                                                                               \
+  } while (0)
+
+template <typename T>
+static cudaError_t dalloc(T **p, size_t count) {
+  return cudaMalloc((void **)p, std::max<size_t>(count, 1) * sizeof(T));
+}
+
+static bool fft_supported(int n) {
+  if (n < kOrder) return false;
+  for (int f : {2, 3, 5, 7})
+    while (n % f == 0) n /= f;
+  return n == 1;
+}
+
+__global__ void k_set_flags(int *flags, int v) { *flags = v; }
+
+static int alloc_lists(Handle &h) {
+  if (h.d_nbr) cudaFree(h.d_nbr);
+  if (h.d_ewl) cudaFree(h.d_ewl);
+  if (h.d_prl) cudaFree(h.d_prl);
+  h.d_nbr = h.d_ewl = h.d_prl = nullptr;
+  CK(dalloc(&h.d_nbr, (size_t)h.n * h.cap_nbr));
+  CK(dalloc(&h.d_ewl, (size_t)h.n * h.cap_ewl));
+  CK(dalloc(&h.d_prl, (size_t)h.n * h.cap_prl));
+  h.list_valid = false;
+  return FFXG_OK;
+}
+
+static int round32(double v) { return ((int)std::ceil(v) + 31) / 32 * 32; }
+
+static int create_impl(const ffxg_system *s, const ffxg_params *p, Handle &h) {
+  const int n = s->n_atoms;
+  h.n = n;
+  h.prm = *p;
+  if (n <= 0) { h.err = "n_atoms must be positive"; return FFXG_ERR_BAD_ARG; }
+  if (p->pme_order != kOrder) { h.err = "only pme-order 5 is supported"; return FFXG_ERR_BAD_ARG; }
+  for (int d = 0; d < 3; d++) {
+    if (!(p->box[d] > 0.0)) { h.err = "box edges must be positive"; return FFXG_ERR_BAD_ARG; }
+    if (!fft_supported(p->pme_grid[d])) {
+      h.err = "PME grid dimensions must be >= 5 and factor into 2, 3, 5 and 7";
+      return FFXG_ERR_BAD_ARG;
+    }
+  }
+  const double rlist = std::max(p->vdw_cutoff, p->ewald_cutoff) + p->list_buffer;
+  for (int d = 0; d < 3; d++)
+    if (p->box[d] < 2.0 * rlist) {
+      h.err = "box edge shorter than twice the buffered cutoff: replicate cells (nSymm > 1) are not supported";
+      return FFXG_ERR_BAD_ARG;
+    }
+  if (p->ewald_alpha <= 0.0) { h.err = "ewald-alpha must be positive"; return FFXG_ERR_BAD_ARG; }
+  if (p->precision != FFXG_PRECISION_FP64 && p->precision != FFXG_PRECISION_MIXED) {
+    h.err = "unknown precision"; return FFXG_ERR_BAD_ARG;
+  }
+  if (p->polarization < FFXG_POLAR_NONE || p->polarization > FFXG_POLAR_MUTUAL) {
+    h.err = "unknown polarization"; return FFXG_ERR_BAD_ARG;
+  }
+  // Device.
+  int dev = 0;
+  CK(cudaGetDevice(&dev));
+  cudaDeviceProp prop;
+  CK(cudaGetDeviceProperties(&prop, dev));
+  if (prop.major < 10) { h.err = "requires an sm_100 (Blackwell) device"; return FFXG_ERR_CUDA; }
+  h.device = dev;
+  CK(cudaStreamCreateWithFlags(&h.stream, cudaStreamNonBlocking));
+
+  h.box.a = p->box[0]; h.box.b = p->box[1]; h.box.c = p->box[2];
+  h.box.A00 = 1.0 / h.box.a; h.box.A11 = 1.0 / h.box.b; h.box.A22 = 1.0 / h.box.c;
+  h.box.Ai00 = h.box.a; h.box.Ai11 = h.box.b; h.box.Ai22 = h.box.c;
+  h.box.volume = h.box.a * h.box.b * h.box.c;
+
+  // ---- validate topology indices
+  for (int i = 0; i < n; i++) {
+    const int fr = s->frame[i];
+    if (fr < FFXG_FRAME_NONE || fr > FFXG_FRAME_THREEFOLD) { h.err = "bad frame type"; return FFXG_ERR_BAD_ARG; }
+    const int need = (fr == FFXG_FRAME_NONE) ? 0 : (fr == FFXG_FRAME_ZONLY) ? 1
+                     : (fr == FFXG_FRAME_ZTHENBISECTOR || fr == FFXG_FRAME_THREEFOLD) ? 3 : 2;
+    for (int a = 0; a < need; a++) {
+      const int ax = s->axis[3 * i + a];
+      if (ax < 0 || ax >= n || ax == i) { h.err = "bad frame-defining atom index"; return FFXG_ERR_BAD_ARG; }
+    }
+    if (s->red_parent[i] < 0 || s->red_parent[i] >= n) { h.err = "bad reduction parent"; return FFXG_ERR_BAD_ARG; }
+    if (s->vdw_type[i] < 0 || s->vdw_type[i] >= s->n_vdw_types) { h.err = "bad vdW type"; return FFXG_ERR_BAD_ARG; }
+  }
+
+  // ---- exclusion codes: bits 0-2 mpole class, 3-5 polar class, 6 group, 7-8 vdW class
+  std::vector<std::map<int, unsigned>> ex(n);
+  auto each = [&](const int32_t *ptr, const int32_t *idx, auto fn) {
+    for (int i = 0; i < n; i++)
+      for (int e = ptr[i]; e < ptr[i + 1]; e++) fn(i, idx[e]);
+  };
+  auto setbits = [&](int i, int k, unsigned mask, unsigned val) {
+    if (k < 0 || k >= n || k == i) return;
+    unsigned &c = ex[i][k];
+    c = (c & ~mask) | val;
+  };
+  each(s->mask12_ptr, s->mask12_idx, [&](int i, int k) { setbits(i, k, 7u | (7u << 3) | (3u << 7), 1u | (1u << 3) | (1u << 7)); });
+  each(s->mask13_ptr, s->mask13_idx, [&](int i, int k) { setbits(i, k, 7u | (7u << 3) | (3u << 7), 2u | (2u << 3) | (2u << 7)); });
+  each(s->mask14_ptr, s->mask14_idx, [&](int i, int k) { setbits(i, k, 7u | (7u << 3) | (3u << 7), 3u | (3u << 3) | (3u << 7)); });
+  each(s->mask15_ptr, s->mask15_idx, [&](int i, int k) { setbits(i, k, 7u, 4u); });
+  each(s->ip11_ptr, s->ip11_idx, [&](int i, int k) { setbits(i, k, 1u << 6, 1u << 6); });
+  // A 1-4 partner inside the same polarization group takes polar-14-intra (PermanentFieldRegion.java:241-248).
+  for (int i = 0; i < n; i++)
+    for (auto &kv : ex[i])
+      if (((kv.second >> 3) & 7u) == 3u && (kv.second & (1u << 6))) kv.second = (kv.second & ~(7u << 3)) | (4u << 3);
+  std::vector<int> eptr(n + 1, 0), ek, elo(n, 0x7fffffff), ehi(n, -1);
+  std::vector<unsigned> ecode;
+  for (int i = 0; i < n; i++) {
+    for (auto &kv : ex[i]) {
+      ek.push_back(kv.first);
+      ecode.push_back(kv.second);
+      elo[i] = std::min(elo[i], kv.first);
+      ehi[i] = std::max(ehi[i], kv.first);
+    }
+    eptr[i + 1] = (int)ek.size();
+  }
+  h.scales.m[0] = 1.0; h.scales.m[1] = p->m12; h.scales.m[2] = p->m13; h.scales.m[3] = p->m14; h.scales.m[4] = p->m15;
+  h.scales.p[0] = 1.0; h.scales.p[1] = p->p12; h.scales.p[2] = p->p13; h.scales.p[3] = p->p14;
+  h.scales.p[4] = p->intra14 * p->p14;
+  h.scales.d[0] = 1.0; h.scales.d[1] = p->d11;
+  h.scales.v[0] = 1.0; h.scales.v[1] = p->v12; h.scales.v[2] = p->v13; h.scales.v[3] = p->v14;
+
+  // ---- torque gather CSR: atom j <- (i, slot) for each frame atom of i and i itself
+  std::vector<std::vector<int>> tq(n);
+  std::vector<std::vector<int>> kids(n);
+  for (int i = 0; i < n; i++) {
+    const int fr = s->frame[i];
+    if (fr != FFXG_FRAME_NONE) {
+      tq[s->axis[3 * i]].push_back(i * 4 + 0);
+      if (fr != FFXG_FRAME_ZONLY) tq[s->axis[3 * i + 1]].push_back(i * 4 + 1);
+      if (fr == FFXG_FRAME_ZTHENBISECTOR || fr == FFXG_FRAME_THREEFOLD) tq[s->axis[3 * i + 2]].push_back(i * 4 + 2);
+      tq[i].push_back(i * 4 + 3);
+    }
+    if (s->red_parent[i] != i) kids[s->red_parent[i]].push_back(i);
+  }
+  std::vector<int> tqp(n + 1, 0), tqe, rp(n + 1, 0), rc;
+  for (int j = 0; j < n; j++) {
+    std::sort(tq[j].begin(), tq[j].end());
+    tqe.insert(tqe.end(), tq[j].begin(), tq[j].end());
+    tqp[j + 1] = (int)tqe.size();
+    rc.insert(rc.end(), kids[j].begin(), kids[j].end());
+    rp[j + 1] = (int)rc.size();
+  }
+
+  // ---- capacities from the density
+  const double rho = n / h.box.volume;
+  const double PI = 3.14159265358979323846;
+  auto sphere = [&](double r) { return 4.0 / 3.0 * PI * r * r * r * rho; };
+  h.cap_nbr = round32(1.3 * sphere(rlist) + 64);
+  h.cap_ewl = round32(1.3 * sphere(p->ewald_cutoff) + 32);
+  h.cap_prl = round32(1.3 * sphere(p->precond_cutoff) + 32);
+  for (int d = 0; d < 3; d++) h.ncell[d] = std::max(1, (int)std::floor(p->box[d] / (rlist * 0.5)));
+  const int ncells = h.ncell[0] * h.ncell[1] * h.ncell[2];
+
+  // ---- allocations
+  const size_t N = n;
+  CK(dalloc(&h.d_lmp, 10 * N)); CK(dalloc(&h.d_frame, N)); CK(dalloc(&h.d_axis, 3 * N));
+  CK(dalloc(&h.d_polar, N)); CK(dalloc(&h.d_thole, N)); CK(dalloc(&h.d_ipdamp, N));
+  CK(dalloc(&h.d_vtype, N)); CK(dalloc(&h.d_redp, N)); CK(dalloc(&h.d_redf, N));
+  h.ntypes = s->n_vdw_types;
+  CK(dalloc(&h.d_vrad, (size_t)h.ntypes * h.ntypes)); CK(dalloc(&h.d_veps, (size_t)h.ntypes * h.ntypes));
+  CK(dalloc(&h.d_excl_ptr, N + 1)); CK(dalloc(&h.d_excl_k, ek.size())); CK(dalloc(&h.d_excl_code, ecode.size()));
+  CK(dalloc(&h.d_excl_lo, N)); CK(dalloc(&h.d_excl_hi, N));
+  CK(dalloc(&h.d_tq_ptr, N + 1)); CK(dalloc(&h.d_tq_ent, tqe.size()));
+  CK(dalloc(&h.d_red_ptr, N + 1)); CK(dalloc(&h.d_red_child, rc.size()));
+  CK(dalloc(&h.d_x, N)); CK(dalloc(&h.d_y, N)); CK(dalloc(&h.d_z, N));
+  CK(dalloc(&h.d_rx, N)); CK(dalloc(&h.d_ry, N)); CK(dalloc(&h.d_rz, N));
+  CK(dalloc(&h.d_refx, N)); CK(dalloc(&h.d_refy, N)); CK(dalloc(&h.d_refz, N));
+  CK(dalloc(&h.d_cell_cnt, 2 * (size_t)ncells)); CK(dalloc(&h.d_cell_start, (size_t)ncells + 1));
+  CK(dalloc(&h.d_cell_atoms, N)); CK(dalloc(&h.d_atom_cell, N));
+  CK(dalloc(&h.d_nbr_cnt, N)); CK(dalloc(&h.d_ewl_cnt, N)); CK(dalloc(&h.d_prl_cnt, N));
+  if (int st = alloc_lists(h)) return st;
+  CK(dalloc(&h.d_gm, 10 * N)); CK(dalloc(&h.d_fm, 10 * N));
+  CK(dalloc(&h.d_spl, N * 3 * kOrder * 4)); CK(dalloc(&h.d_igrid, 3 * N));
+  CK(dalloc(&h.d_cphi, 20 * N)); CK(dalloc(&h.d_fphi, 20 * N));
+  CK(dalloc(&h.d_cphiI, 20 * N)); CK(dalloc(&h.d_fphiI, 20 * N));
+  CK(dalloc(&h.d_cphiP, 20 * N)); CK(dalloc(&h.d_fphiP, 20 * N));
+  CK(dalloc(&h.d_fieldD, 3 * N)); CK(dalloc(&h.d_fieldP, 3 * N));
+  CK(dalloc(&h.d_uD, 3 * N)); CK(dalloc(&h.d_uP, 3 * N)); CK(dalloc(&h.d_udirD, 3 * N)); CK(dalloc(&h.d_udirP, 3 * N));
+  CK(dalloc(&h.d_r, 3 * N)); CK(dalloc(&h.d_rP, 3 * N)); CK(dalloc(&h.d_zpre, 3 * N)); CK(dalloc(&h.d_zpreP, 3 * N));
+  CK(dalloc(&h.d_p, 3 * N)); CK(dalloc(&h.d_pP, 3 * N)); CK(dalloc(&h.d_vec, 3 * N)); CK(dalloc(&h.d_vecP, 3 * N));
+  const size_t nparts = std::max<size_t>((size_t)nblocks(n, 256) * 8, 148 * 16) + 64;
+  CK(dalloc(&h.d_partials, nparts));
+  CK(dalloc(&h.d_scalars, 16));
+  CK(cudaMallocHost((void **)&h.h_scalars, 16 * sizeof(double)));
+  const int nfx = p->pme_grid[0], nfy = p->pme_grid[1], nfz = p->pme_grid[2];
+  const size_t ng = (size_t)nfx * nfy * nfz;
+  CK(dalloc(&h.d_grid, ng)); CK(dalloc(&h.d_influence, ng));
+  CK(dalloc(&h.d_twiddle, 3 * (size_t)std::max(nfx, std::max(nfy, nfz))));
+  CK(dalloc(&h.d_grad, 3 * N)); CK(dalloc(&h.d_torque, 3 * N)); CK(dalloc(&h.d_gred, 6 * N));
+  CK(dalloc(&h.d_eatom, 8 * N)); CK(dalloc(&h.d_catom, 2 * N));
+  CK(dalloc(&h.d_result, 16)); CK(dalloc(&h.d_cresult, 8));
+  CK(dalloc(&h.d_flags, 1));
+  CK(cudaMallocHost((void **)&h.h_flags, 64));
+  CK(dalloc(&h.d_xyz_in, 3 * N)); CK(dalloc(&h.d_grad_out, 3 * N));
+  CK(cudaMallocHost((void **)&h.h_xyz_pin, 3 * N * sizeof(double)));
+  CK(cudaMallocHost((void **)&h.h_grad_pin, 3 * N * sizeof(double)));
+
+  // ---- uploads (SoA)
+  std::vector<double> lmp(10 * N);
+  std::vector<int> axis(3 * N);
+  std::vector<double> ipd(N);
+  for (int i = 0; i < n; i++) {
+    for (int t = 0; t < 10; t++) lmp[t * N + i] = s->multipole[10 * (size_t)i + t];
+    for (int a = 0; a < 3; a++) axis[a * N + i] = s->axis[3 * (size_t)i + a];
+    ipd[i] = (s->pdamp[i] > 0.0) ? 1.0 / s->pdamp[i] : INFINITY;  // ParticleMeshEwald.java:1401-1406
+  }
+  CK(cudaMemcpy(h.d_lmp, lmp.data(), 10 * N * sizeof(double), cudaMemcpyHostToDevice));
+  CK(cudaMemcpy(h.d_frame, s->frame, N * sizeof(int), cudaMemcpyHostToDevice));
+  CK(cudaMemcpy(h.d_axis, axis.data(), 3 * N * sizeof(int), cudaMemcpyHostToDevice));
+  CK(cudaMemcpy(h.d_polar, s->polarizability, N * sizeof(double), cudaMemcpyHostToDevice));
+  CK(cudaMemcpy(h.d_thole, s->thole, N * sizeof(double), cudaMemcpyHostToDevice));
+  CK(cudaMemcpy(h.d_ipdamp, ipd.data(), N * sizeof(double), cudaMemcpyHostToDevice));
+  CK(cudaMemcpy(h.d_vtype, s->vdw_type, N * sizeof(int), cudaMemcpyHostToDevice));
+  CK(cudaMemcpy(h.d_redp, s->red_parent, N * sizeof(int), cudaMemcpyHostToDevice));
+  CK(cudaMemcpy(h.d_redf, s->red_factor, N * sizeof(double), cudaMemcpyHostToDevice));
+  CK(cudaMemcpy(h.d_vrad, s->vdw_inv_rmin, (size_t)h.ntypes * h.ntypes * sizeof(double), cudaMemcpyHostToDevice));
+  CK(cudaMemcpy(h.d_veps, s->vdw_eps, (size_t)h.ntypes * h.ntypes * sizeof(double), cudaMemcpyHostToDevice));
+  CK(cudaMemcpy(h.d_excl_ptr, eptr.data(), (N + 1) * sizeof(int), cudaMemcpyHostToDevice));
+  if (!ek.empty()) {
+    CK(cudaMemcpy(h.d_excl_k, ek.data(), ek.size() * sizeof(int), cudaMemcpyHostToDevice));
+    CK(cudaMemcpy(h.d_excl_code, ecode.data(), ecode.size() * sizeof(unsigned), cudaMemcpyHostToDevice));
+  }
+  CK(cudaMemcpy(h.d_excl_lo, elo.data(), N * sizeof(int), cudaMemcpyHostToDevice));
+  CK(cudaMemcpy(h.d_excl_hi, ehi.data(), N * sizeof(int), cudaMemcpyHostToDevice));
+  CK(cudaMemcpy(h.d_tq_ptr, tqp.data(), (N + 1) * sizeof(int), cudaMemcpyHostToDevice));
+  if (!tqe.empty()) CK(cudaMemcpy(h.d_tq_ent, tqe.data(), tqe.size() * sizeof(int), cudaMemcpyHostToDevice));
+  CK(cudaMemcpy(h.d_red_ptr, rp.data(), (N + 1) * sizeof(int), cudaMemcpyHostToDevice));
+  if (!rc.empty()) CK(cudaMemcpy(h.d_red_child, rc.data(), rc.size() * sizeof(int), cudaMemcpyHostToDevice));
+  CK(cudaMemset(h.d_refx, 0, N * sizeof(double)));
+  CK(cudaMemset(h.d_refy, 0, N * sizeof(double)));
+  CK(cudaMemset(h.d_refz, 0, N * sizeof(double)));
+  CK(cudaMemset(h.d_grad, 0, 3 * N * sizeof(double)));
+  CK(cudaMemset(h.d_torque, 0, 3 * N * sizeof(double)));
+  CK(cudaMemset(h.d_gred, 0, 6 * N * sizeof(double)));
+  CK(cudaMemset(h.d_eatom, 0, 8 * N * sizeof(double)));
+  CK(cudaMemset(h.d_catom, 0, 2 * N * sizeof(long long)));
+  CK(cudaMemset(h.d_uD, 0, 3 * N * sizeof(double)));
+  CK(cudaMemset(h.d_uP, 0, 3 * N * sizeof(double)));
+  // Charge correction for a charged cell (ReciprocalEnergyRegion.java:229-255).
+  {
+    double q = 0.0;
+    for (int i = 0; i < n; i++) q += s->multipole[10 * (size_t)i];
+    h.e_charge_correction = (q != 0.0) ? -0.5 * p->electric * PI * (q * q) / (h.box.volume * p->ewald_alpha * p->ewald_alpha) : 0.0;
+  }
+  setup_pme(h);
+  CK(cudaGetLastError());
+  // Coordinates.
+  std::memcpy(h.h_xyz_pin, s->xyz, 3 * N * sizeof(double));
+  CK(cudaMemcpy(h.d_xyz_in, h.h_xyz_pin, 3 * N * sizeof(double), cudaMemcpyHostToDevice));
+  CK(cudaDeviceSynchronize());
+  return FFXG_OK;
+}
+
+static void free_all(Handle &h) {
+  void *ptrs[] = {h.d_lmp, h.d_frame, h.d_axis, h.d_polar, h.d_thole, h.d_ipdamp, h.d_vtype, h.d_redp, h.d_redf,
+                  h.d_vrad, h.d_veps, h.d_excl_ptr, h.d_excl_k, h.d_excl_code, h.d_excl_lo, h.d_excl_hi, h.d_tq_ptr,
+                  h.d_tq_ent, h.d_red_ptr, h.d_red_child, h.d_x, h.d_y, h.d_z, h.d_rx, h.d_ry, h.d_rz, h.d_refx,
+                  h.d_refy, h.d_refz, h.d_cell_cnt, h.d_cell_start, h.d_cell_atoms, h.d_atom_cell, h.d_nbr,
+                  h.d_nbr_cnt, h.d_ewl, h.d_ewl_cnt, h.d_prl, h.d_prl_cnt, h.d_gm, h.d_fm, h.d_spl, h.d_igrid,
+                  h.d_cphi, h.d_fphi, h.d_cphiI, h.d_fphiI, h.d_cphiP, h.d_fphiP, h.d_fieldD, h.d_fieldP, h.d_uD,
+                  h.d_uP, h.d_udirD, h.d_udirP, h.d_r, h.d_rP, h.d_zpre, h.d_zpreP, h.d_p, h.d_pP, h.d_vec, h.d_vecP,
+                  h.d_partials, h.d_scalars, h.d_grid, h.d_influence, h.d_twiddle, h.d_grad, h.d_torque, h.d_gred,
+                  h.d_eatom, h.d_catom, h.d_result, h.d_cresult, h.d_flags, h.d_xyz_in, h.d_grad_out};
+  for (void *q : ptrs)
+    if (q) cudaFree(q);
+  if (h.h_scalars) cudaFreeHost(h.h_scalars);
+  if (h.h_flags) cudaFreeHost(h.h_flags);
+  if (h.h_xyz_pin) cudaFreeHost(h.h_xyz_pin);
+  if (h.h_grad_pin) cudaFreeHost(h.h_grad_pin);
+  for (cudaEvent_t e : h.ev_pool) cudaEventDestroy(e);
+  if (h.stream) cudaStreamDestroy(h.stream);
+}
+
+// One evaluation on device-resident coordinates; grows list capacities and repeats on overflow.
+static int evaluate(Handle &h, const double *d_xyz, double *d_grad_xyz, bool grad, double *terms, int64_t *counts) {
+  h.launches = 0;
+  for (int attempt = 0; attempt < 4; attempt++) {
+    h.ev_stage.clear();
+    h.ev_used = 0;
+    int tk = timer_begin(h, FFXG_STAGE_LISTS);
+    k_set_flags<<<1, 1, 0, h.stream>>>(h.d_flags, h.list_valid ? 0 : FLAG_REBUILD);
+    FFX_LAUNCHED(h);
+    launch_set_coordinates(h, d_xyz);
+    launch_neighbor_list(h, false);
+    launch_realspace_lists(h);
+    timer_end(h, tk);
+    // List overflow invalidates everything downstream and non-finite coordinates
+    // make the evaluation meaningless: check both before the expensive stages.
+    cudaMemcpyAsync(h.h_flags, h.d_flags, sizeof(int), cudaMemcpyDeviceToHost, h.stream);
+    if (cudaStreamSynchronize(h.stream) != cudaSuccess) {
+      h.err = std::string("CUDA error: ") + cudaGetErrorString(cudaGetLastError());
+      return FFXG_ERR_CUDA;
+    }
+    const int f = h.h_flags[0];
+    if (f & FLAG_NONFINITE) { h.err = "non-finite coordinates"; return FFXG_ERR_NONFINITE; }
+    if (f & (FLAG_NBR_OVERFLOW | FLAG_EWALD_OVERFLOW | FLAG_PRECOND_OVERFLOW)) {
+      if (f & FLAG_NBR_OVERFLOW) h.cap_nbr = round32(h.cap_nbr * 1.5);
+      if (f & FLAG_EWALD_OVERFLOW) h.cap_ewl = round32(h.cap_ewl * 1.5);
+      if (f & FLAG_PRECOND_OVERFLOW) h.cap_prl = round32(h.cap_prl * 1.5);
+      if (int a = alloc_lists(h)) return a;
+      continue;
+    }
+    const bool rebuilt = (f & FLAG_REBUILD) != 0;
+    if (rebuilt) h.list_builds++;
+    h.list_valid = true;
+    tk = timer_begin(h, FFXG_STAGE_VDW);
+    launch_vdw(h, grad);
+    timer_end(h, tk);
+    tk = timer_begin(h, FFXG_STAGE_MULTIPOLES);
+    launch_rotate(h);
+    launch_bsplines(h);
+    timer_end(h, tk);
+    tk = timer_begin(h, FFXG_STAGE_PERM_RECIP);
+    launch_spread_permanent(h);
+    launch_fft_convolution(h);
+    launch_phi_permanent(h);
+    timer_end(h, tk);
+    tk = timer_begin(h, FFXG_STAGE_PERM_FIELD);
+    launch_permanent_field(h);
+    int st = FFXG_OK;
+    h.scf_iter = 0;
+    if (h.prm.polarization != FFXG_POLAR_NONE) launch_direct(h);
+    timer_end(h, tk);
+    if (h.prm.polarization != FFXG_POLAR_NONE) {
+      if (h.prm.polarization == FFXG_POLAR_MUTUAL) st = run_pcg(h);
+      if (st == FFXG_OK) {
+        tk = timer_begin(h, FFXG_STAGE_IND_RECIP);
+        launch_spread_induced(h, h.d_uD, h.d_uP);
+        launch_fft_convolution(h);
+        launch_phi_induced(h, true);
+        timer_end(h, tk);
+      }
+    } else {
+      cudaMemsetAsync(h.d_uD, 0, 3 * (size_t)h.n * sizeof(double), h.stream);
+      cudaMemsetAsync(h.d_uP, 0, 3 * (size_t)h.n * sizeof(double), h.stream);
+    }
+    if (st != FFXG_OK) {
+      h.err = (st == FFXG_ERR_SCF_DIVERGED) ? "SCF convergence failure (residual grew)"
+              : (st == FFXG_ERR_SCF_MAXITER) ? "maximum SCF iterations reached"
+                                             : "non-finite SCF residual";
+      return st;
+    }
+    tk = timer_begin(h, FFXG_STAGE_REAL_ENERGY);
+    launch_real_energy(h, grad);
+    timer_end(h, tk);
+    tk = timer_begin(h, FFXG_STAGE_RECIP_ENERGY);
+    launch_recip_energy(h, grad);
+    timer_end(h, tk);
+    tk = timer_begin(h, FFXG_STAGE_GRADIENT);
+    if (grad) {
+      launch_torque(h);
+      launch_assemble(h, d_grad_xyz);
+    }
+    launch_reduce_results(h);
+    timer_end(h, tk);
+    double res[8];
+    long long cres[2];
+    cudaMemcpyAsync(h.h_scalars, h.d_result, 7 * sizeof(double), cudaMemcpyDeviceToHost, h.stream);
+    cudaMemcpyAsync(h.h_flags + 2, h.d_cresult, 2 * sizeof(long long), cudaMemcpyDeviceToHost, h.stream);
+    cudaMemcpyAsync(h.h_flags, h.d_flags, sizeof(int), cudaMemcpyDeviceToHost, h.stream);
+    if (cudaStreamSynchronize(h.stream) != cudaSuccess) {
+      h.err = std::string("CUDA error: ") + cudaGetErrorString(cudaGetLastError());
+      return FFXG_ERR_CUDA;
+    }
+    std::memcpy(res, h.h_scalars, 7 * sizeof(double));
+    if (h.timing) timer_collect(h);
+    std::memcpy(cres, h.h_flags + 2, 2 * sizeof(long long));
+    const double eCorr = h.e_charge_correction;
+    if (terms) {
+      terms[FFXG_TERM_VDW] = res[0];
+      terms[FFXG_TERM_PERM_REAL] = res[1];
+      terms[FFXG_TERM_POL_REAL] = res[2];
+      terms[FFXG_TERM_PERM_SELF] = res[3];
+      terms[FFXG_TERM_PERM_RECIP] = res[4] + eCorr;
+      terms[FFXG_TERM_POL_SELF] = res[5];
+      terms[FFXG_TERM_POL_RECIP] = res[6];
+      terms[FFXG_TERM_PERMANENT] = res[1] + res[3] + res[4] + eCorr;
+      terms[FFXG_TERM_POLARIZATION] = res[2] + res[5] + res[6];
+      terms[FFXG_TERM_TOTAL] = res[0] + terms[FFXG_TERM_PERMANENT] + terms[FFXG_TERM_POLARIZATION];
+    }
+    if (counts) {
+      counts[FFXG_COUNT_VDW] = cres[0];
+      counts[FFXG_COUNT_PERMANENT] = cres[1] + h.n;
+      counts[FFXG_COUNT_SCF_ITER] = h.scf_iter;
+      counts[FFXG_COUNT_LIST_BUILDS] = rebuilt ? 1 : 0;
+      counts[FFXG_COUNT_LIST_PAIRS] = -1;
+    }
+    if (h.h_flags[0] & FLAG_NONFINITE) { h.err = "non-finite energy, torque or gradient"; return FFXG_ERR_NONFINITE; }
+    for (int t = 0; t < 7; t++)
+      if (!std::isfinite(res[t])) { h.err = "non-finite energy"; return FFXG_ERR_NONFINITE; }
+    return FFXG_OK;
+  }
+  h.err = "neighbour capacity could not be satisfied";
+  return FFXG_ERR_CAPACITY;
+}
+
+extern "C" {
+
+int ffxg_create(const ffxg_system *sys, const ffxg_params *params, ffxg_handle **out) {
+  if (!sys || !params || !out) { g_create_error = "null argument"; return FFXG_ERR_BAD_ARG; }
+  *out = nullptr;
+  ffxg_handle *hh = new ffxg_handle();
+  const int st = create_impl(sys, params, hh->h);
+  if (st != FFXG_OK) {
+    g_create_error = hh->h.err;
+    free_all(hh->h);
+    delete hh;
+    return st;
+  }
+  *out = hh;
+  return FFXG_OK;
+}
+
+void ffxg_destroy(ffxg_handle *hh) {
+  if (!hh) return;
+  free_all(hh->h);
+  delete hh;
+}
+
+const char *ffxg_last_error(const ffxg_handle *hh) { return hh ? hh->h.err.c_str() : g_create_error.c_str(); }
+
+int ffxg_set_coordinates(ffxg_handle *hh, const double *xyz) {
+  if (!hh || !xyz) return FFXG_ERR_BAD_ARG;
+  Handle &h = hh->h;
+  for (size_t j = 0; j < 3 * (size_t)h.n; j++)
+    if (!std::isfinite(xyz[j])) { h.err = "non-finite coordinates"; return FFXG_ERR_NONFINITE; }
+  std::memcpy(h.h_xyz_pin, xyz, 3 * (size_t)h.n * sizeof(double));
+  CK(cudaMemcpyAsync(h.d_xyz_in, h.h_xyz_pin, 3 * (size_t)h.n * sizeof(double), cudaMemcpyHostToDevice, h.stream));
+  return FFXG_OK;
+}
+
+int ffxg_energy(ffxg_handle *hh, int want_grad, double *terms, double *grad, int64_t *counts) {
+  if (!hh) return FFXG_ERR_BAD_ARG;
+  Handle &h = hh->h;
+  const int st = evaluate(h, h.d_xyz_in, h.d_grad_out, want_grad != 0, terms, counts);
+  if (st != FFXG_OK) return st;
+  if (want_grad && grad) {
+    CK(cudaMemcpyAsync(h.h_grad_pin, h.d_grad_out, 3 * (size_t)h.n * sizeof(double), cudaMemcpyDeviceToHost, h.stream));
+    CK(cudaStreamSynchronize(h.stream));
+    std::memcpy(grad, h.h_grad_pin, 3 * (size_t)h.n * sizeof(double));
+  }
+  return FFXG_OK;
+}
+
+int ffxg_energy_and_gradient(ffxg_handle *hh, const double *xyz, double *terms, double *grad, int64_t *counts) {
+  if (const int st = ffxg_set_coordinates(hh, xyz)) return st;
+  return ffxg_energy(hh, grad != nullptr, terms, grad, counts);
+}
+
+int ffxg_energy_device(ffxg_handle *hh, const double *d_xyz, double *d_grad, double *terms, int64_t *counts) {
+  if (!hh || !d_xyz) return FFXG_ERR_BAD_ARG;
+  Handle &h = hh->h;
+  return evaluate(h, d_xyz, d_grad ? d_grad : h.d_grad_out, d_grad != nullptr, terms, counts);
+}
+
+int ffxg_get_induced_dipoles(ffxg_handle *hh, double *u, double *u_cr) {
+  if (!hh) return FFXG_ERR_BAD_ARG;
+  Handle &h = hh->h;
+  const size_t N = h.n;
+  std::vector<double> a(3 * N), b(3 * N);
+  CK(cudaMemcpy(a.data(), h.d_uD, 3 * N * sizeof(double), cudaMemcpyDeviceToHost));
+  CK(cudaMemcpy(b.data(), h.d_uP, 3 * N * sizeof(double), cudaMemcpyDeviceToHost));
+  for (size_t i = 0; i < N; i++)
+    for (int d = 0; d < 3; d++) {
+      if (u) u[3 * i + d] = a[d * N + i];
+      if (u_cr) u_cr[3 * i + d] = b[d * N + i];
+    }
+  return FFXG_OK;
+}
+
+int ffxg_get_global_multipoles(ffxg_handle *hh, double *mpole) {
+  if (!hh || !mpole) return FFXG_ERR_BAD_ARG;
+  Handle &h = hh->h;
+  const size_t N = h.n;
+  std::vector<double> a(10 * N);
+  CK(cudaMemcpy(a.data(), h.d_gm, 10 * N * sizeof(double), cudaMemcpyDeviceToHost));
+  for (size_t i = 0; i < N; i++)
+    for (int t = 0; t < 10; t++) mpole[10 * i + t] = a[t * N + i];
+  return FFXG_OK;
+}
+
+int ffxg_get_neighbor_pairs(ffxg_handle *hh, int32_t *pairs, int64_t *n_pairs) {
+  if (!hh || !n_pairs) return FFXG_ERR_BAD_ARG;
+  Handle &h = hh->h;
+  if (!h.list_valid) { h.err = "no neighbour list yet: call ffxg_energy first"; return FFXG_ERR_BAD_ARG; }
+  const size_t N = h.n;
+  std::vector<int> cnt(N), lst(N * h.cap_nbr);
+  CK(cudaMemcpy(cnt.data(), h.d_nbr_cnt, N * sizeof(int), cudaMemcpyDeviceToHost));
+  CK(cudaMemcpy(lst.data(), h.d_nbr, N * h.cap_nbr * sizeof(int), cudaMemcpyDeviceToHost));
+  int64_t c = 0;
+  for (size_t i = 0; i < N; i++)
+    for (int a = 0; a < std::min(cnt[i], h.cap_nbr); a++) {
+      const int k = lst[i * h.cap_nbr + a];
+      if (k > (int)i) {
+        if (pairs) { pairs[2 * c] = (int32_t)i; pairs[2 * c + 1] = k; }
+        c++;
+      }
+    }
+  *n_pairs = c;
+  return FFXG_OK;
+}
+
+void *ffxg_stream(ffxg_handle *hh) { return hh ? (void *)hh->h.stream : nullptr; }
+
+int64_t ffxg_last_launch_count(const ffxg_handle *hh) { return hh ? hh->h.launches : 0; }
+
+int ffxg_set_timing(ffxg_handle *hh, int on) {
+  if (!hh) return FFXG_ERR_BAD_ARG;
+  Handle &h = hh->h;
+  h.timing = on != 0;
+  for (int s = 0; s < 16; s++) { h.stage_ms[s] = 0.0; h.stage_calls[s] = 0; }
+  h.ev_stage.clear();
+  h.ev_used = 0;
+  return FFXG_OK;
+}
+
+int ffxg_get_timings(ffxg_handle *hh, double *ms, int64_t *launches, int n) {
+  if (!hh || n < 0) return FFXG_ERR_BAD_ARG;
+  Handle &h = hh->h;
+  for (int s = 0; s < n && s < FFXG_N_STAGES; s++) {
+    if (ms) ms[s] = h.stage_ms[s];
+    if (launches) launches[s] = h.stage_calls[s];
+  }
+  return FFXG_OK;
+}
+
+}  // extern "C"

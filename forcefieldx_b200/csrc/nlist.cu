@@ -1,0 +1,312 @@
+// nlist.cu -- coordinates, hydrogen reduction, cell list and Verlet lists.
+//
+// Replaces NeighborList.buildList/run (NeighborList.java:351-572): the buffered
+// list at max(vdw, ewald) cutoff + buffer on the hydrogen-reduced coordinates of
+// VanDerWaals.ExpandLoop (VanDerWaals.java:1505-1541), rebuilt only when an atom
+// moved more than half the buffer (MotionLoop, NeighborList.java:777-799).  The
+// pair test is Crystal.image's exact arithmetic (d2 <= (cutoff+buffer)^2), so the
+// pair set is the reference's.  The list is stored in both directions so every
+// pair kernel gathers into its own atom without atomics.
+#include "ffx_internal.cuh"
+
+namespace ffx {
+
+struct CellOffsets {
+  int n[3];
+  int off[3][5];
+};
+
+// Interleaved [n][3] -> SoA, plus reduced coordinates r = a*(x - x_p) + x_p evaluated
+// without contraction like Java (VanDerWaals.java:1521-1527).
+__global__ void k_set_coordinates(int n, const double *__restrict__ xyz, const int *__restrict__ redp,
+                                  const double *__restrict__ redf, double *x, double *y, double *z,
+                                  double *rx, double *ry, double *rz) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  x[i] = xyz[3 * i];
+  y[i] = xyz[3 * i + 1];
+  z[i] = xyz[3 * i + 2];
+}
+
+__global__ void k_reduce_coordinates(int n, const double *__restrict__ x, const double *__restrict__ y,
+                                     const double *__restrict__ z, const int *__restrict__ redp,
+                                     const double *__restrict__ redf, double *rx, double *ry, double *rz,
+                                     const double *__restrict__ refx, const double *__restrict__ refy,
+                                     const double *__restrict__ refz, double half_buffer2, int *flags) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const int p = redp[i];
+  const double a = redf[i];
+  const double xi = x[i], yi = y[i], zi = z[i];
+  double vx = xi, vy = yi, vz = zi;
+  if (p != i || a != 0.0) {
+    const double px = x[p], py = y[p], pz = z[p];
+    vx = __dadd_rn(__dmul_rn(a, __dsub_rn(xi, px)), px);
+    vy = __dadd_rn(__dmul_rn(a, __dsub_rn(yi, py)), py);
+    vz = __dadd_rn(__dmul_rn(a, __dsub_rn(zi, pz)), pz);
+  }
+  rx[i] = vx; ry[i] = vy; rz[i] = vz;
+  const double dx = vx - refx[i], dy = vy - refy[i], dz = vz - refz[i];
+  const double d2 = dx * dx + dy * dy + dz * dz;
+  if (!(d2 <= half_buffer2)) atomicOr(flags, FLAG_REBUILD);
+  if (!isfinite(vx) || !isfinite(vy) || !isfinite(vz)) atomicOr(flags, FLAG_NONFINITE);
+}
+
+__device__ __forceinline__ int cell_of(double v, double inv, int nc) {
+  double f = v * inv;
+  f = f - floor(f);
+  int c = (int)(f * nc);
+  return c < 0 ? 0 : (c >= nc ? nc - 1 : c);
+}
+
+__global__ void k_cell_count(int n, const double *__restrict__ rx, const double *__restrict__ ry,
+                             const double *__restrict__ rz, Box bx, int ncx, int ncy, int ncz,
+                             int *cell_cnt, int *atom_cell, const int *flags) {
+  if (!(*flags & FLAG_REBUILD)) return;
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const int cx = cell_of(rx[i], bx.A00, ncx), cy = cell_of(ry[i], bx.A11, ncy), cz = cell_of(rz[i], bx.A22, ncz);
+  const int c = (cz * ncy + cy) * ncx + cx;
+  atom_cell[i] = c;
+  atomicAdd(&cell_cnt[c], 1);
+}
+
+// Exclusive scan of the cell counts in one CTA (cells <= a few 1e5).
+__global__ void k_cell_scan(int ncells, const int *__restrict__ cnt, int *start, const int *flags) {
+  if (!(*flags & FLAG_REBUILD)) return;
+  __shared__ int warp_tot[32];
+  __shared__ int carry;
+  if (threadIdx.x == 0) carry = 0;
+  __syncthreads();
+  for (int base = 0; base < ncells; base += blockDim.x) {
+    const int idx = base + threadIdx.x;
+    const int v = idx < ncells ? cnt[idx] : 0;
+    int incl = v;
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const int t = __shfl_up_sync(0xffffffffu, incl, o);
+      if (lane >= o) incl += t;
+    }
+    if (lane == 31) warp_tot[wid] = incl;
+    __syncthreads();
+    if (wid == 0) {
+      int w = lane < (int)(blockDim.x >> 5) ? warp_tot[lane] : 0;
+#pragma unroll
+      for (int o = 1; o < 32; o <<= 1) {
+        const int t = __shfl_up_sync(0xffffffffu, w, o);
+        if (lane >= o) w += t;
+      }
+      warp_tot[lane] = w;
+    }
+    __syncthreads();
+    const int prev = (wid > 0) ? warp_tot[wid - 1] : 0;
+    if (idx < ncells) start[idx] = carry + prev + incl - v;
+    __syncthreads();
+    if (threadIdx.x == blockDim.x - 1) carry += prev + incl;
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) start[ncells] = carry;
+}
+
+// Deterministic placement: an atom's slot is the number of lower-indexed atoms in
+// its cell (cells hold tens of atoms; the scan over the cell is short).
+__global__ void k_cell_fill(int n, const int *__restrict__ atom_cell, const int *__restrict__ start,
+                            int *cell_atoms, int *cell_cursor, const int *flags) {
+  if (!(*flags & FLAG_REBUILD)) return;
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const int c = atom_cell[i];
+  const int slot = atomicAdd(&cell_cursor[c], 1);
+  cell_atoms[start[c] + slot] = i;
+}
+
+__global__ void k_cell_sort(int ncells, const int *__restrict__ start, int *cell_atoms, const int *flags) {
+  if (!(*flags & FLAG_REBUILD)) return;
+  const int c = blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= ncells) return;
+  const int s = start[c], e = start[c + 1];
+  for (int a = s + 1; a < e; a++) {
+    const int v = cell_atoms[a];
+    int b = a - 1;
+    while (b >= s && cell_atoms[b] > v) { cell_atoms[b + 1] = cell_atoms[b]; b--; }
+    cell_atoms[b + 1] = v;
+  }
+}
+
+// One warp per atom i: every atom k != i of the neighbouring cells with
+// image d2 <= rl2 on reduced coordinates (NeighborList.atomCellPairs, :1026-1115).
+__global__ void k_verlet(int n, const double *__restrict__ rx, const double *__restrict__ ry,
+                         const double *__restrict__ rz, Box bx, CellOffsets co,
+                         const int *__restrict__ atom_cell, const int *__restrict__ start,
+                         const int *__restrict__ cell_atoms, double rl2, int cap, int *nbr, int *nbr_cnt,
+                         int *flags) {
+  if (!(*flags & FLAG_REBUILD)) return;
+  const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const int lane = threadIdx.x & 31;
+  if (warp >= n) return;
+  const int i = warp;
+  const double xi = rx[i], yi = ry[i], zi = rz[i];
+  const int c = atom_cell[i];
+  const int ncx = co.n[0], ncy = co.n[1], ncz = co.n[2];
+  const int cx = c % ncx, cy = (c / ncx) % ncy, cz = c / (ncx * ncy);
+  int count = 0;
+  int *row = nbr + (size_t)i * cap;
+  for (int oz = 0; oz < 5; oz++) {
+    const int dz = co.off[2][oz];
+    if (dz == 0x7fff) break;
+    const int z2 = ((cz + dz) % ncz + ncz) % ncz;
+    for (int oy = 0; oy < 5; oy++) {
+      const int dy = co.off[1][oy];
+      if (dy == 0x7fff) break;
+      const int y2 = ((cy + dy) % ncy + ncy) % ncy;
+      for (int ox = 0; ox < 5; ox++) {
+        const int dx = co.off[0][ox];
+        if (dx == 0x7fff) break;
+        const int x2 = ((cx + dx) % ncx + ncx) % ncx;
+        const int cell = (z2 * ncy + y2) * ncx + x2;
+        const int s = start[cell], e = start[cell + 1];
+        for (int base = s; base < e; base += 32) {
+          const int a = base + lane;
+          bool pass = false;
+          int k = -1;
+          if (a < e) {
+            k = cell_atoms[a];
+            if (k != i) {
+              double ddx = __dsub_rn(xi, rx[k]), ddy = __dsub_rn(yi, ry[k]), ddz = __dsub_rn(zi, rz[k]);
+              const double d2 = image_exact(ddx, ddy, ddz, bx);
+              pass = d2 <= rl2;
+            }
+          }
+          const unsigned m = __ballot_sync(0xffffffffu, pass);
+          if (pass) {
+            const int pos = count + __popc(m & ((1u << lane) - 1u));
+            if (pos < cap) row[pos] = k;
+          }
+          count += __popc(m);
+        }
+      }
+    }
+  }
+  if (lane == 0) {
+    nbr_cnt[i] = count;
+    if (count > cap) atomicOr(flags, FLAG_NBR_OVERFLOW);
+  }
+}
+
+__global__ void k_list_done(int n, double *refx, double *refy, double *refz, const double *__restrict__ rx,
+                            const double *__restrict__ ry, const double *__restrict__ rz, const int *flags) {
+  if (!(*flags & FLAG_REBUILD)) return;
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  refx[i] = rx[i]; refy[i] = ry[i]; refz[i] = rz[i];
+}
+
+// Real-space (Ewald) and preconditioner sub-lists on the actual coordinates, as
+// PermanentRealSpaceFieldLoop derives them (pme/PermanentFieldRegion.java:669-717).
+__global__ void k_realspace_lists(int n, const double *__restrict__ x, const double *__restrict__ y,
+                                  const double *__restrict__ z, Box bx, const int *__restrict__ nbr,
+                                  const int *__restrict__ nbr_cnt, int cap, double off2, double pcut,
+                                  int *ewl, int *ewl_cnt, int capE, int *prl, int *prl_cnt, int capP, int *flags) {
+  const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const int lane = threadIdx.x & 31;
+  if (warp >= n) return;
+  const int i = warp;
+  const double xi = x[i], yi = y[i], zi = z[i];
+  const int cnt = min(nbr_cnt[i], cap);
+  const int *row = nbr + (size_t)i * cap;
+  int ce = 0, cp = 0;
+  for (int base = 0; base < cnt; base += 32) {
+    const int a = base + lane;
+    bool ew = false, pr = false;
+    int k = -1;
+    if (a < cnt) {
+      k = row[a];
+      double dx = __dsub_rn(x[k], xi), dy = __dsub_rn(y[k], yi), dz = __dsub_rn(z[k], zi);
+      const double r2 = image_exact(dx, dy, dz, bx);
+      ew = r2 <= off2;
+      pr = ew && (sqrt(r2) < pcut);
+    }
+    const unsigned me = __ballot_sync(0xffffffffu, ew);
+    const unsigned mp = __ballot_sync(0xffffffffu, pr);
+    const unsigned lt = (1u << lane) - 1u;
+    if (ew) {
+      const int pos = ce + __popc(me & lt);
+      if (pos < capE) ewl[(size_t)i * capE + pos] = k;
+    }
+    if (pr) {
+      const int pos = cp + __popc(mp & lt);
+      if (pos < capP) prl[(size_t)i * capP + pos] = k;
+    }
+    ce += __popc(me);
+    cp += __popc(mp);
+  }
+  if (lane == 0) {
+    ewl_cnt[i] = ce;
+    prl_cnt[i] = cp;
+    if (ce > capE) atomicOr(flags, FLAG_EWALD_OVERFLOW);
+    if (cp > capP) atomicOr(flags, FLAG_PRECOND_OVERFLOW);
+  }
+}
+
+// ---------------------------------------------------------------------------
+void launch_set_coordinates(Handle &h, const double *d_xyz) {
+  const int n = h.n;
+  k_set_coordinates<<<nblocks(n, 256), 256, 0, h.stream>>>(n, d_xyz, h.d_redp, h.d_redf, h.d_x, h.d_y, h.d_z,
+                                                            h.d_rx, h.d_ry, h.d_rz);
+  FFX_LAUNCHED(h);
+  const double hb = 0.5 * h.prm.list_buffer;
+  k_reduce_coordinates<<<nblocks(n, 256), 256, 0, h.stream>>>(n, h.d_x, h.d_y, h.d_z, h.d_redp, h.d_redf, h.d_rx,
+                                                               h.d_ry, h.d_rz, h.d_refx, h.d_refy, h.d_refz,
+                                                               hb * hb, h.d_flags);
+  FFX_LAUNCHED(h);
+}
+
+static CellOffsets cell_offsets(const int nc[3]) {
+  CellOffsets co;
+  for (int d = 0; d < 3; d++) {
+    co.n[d] = nc[d];
+    for (int j = 0; j < 5; j++) co.off[d][j] = 0x7fff;
+    if (nc[d] >= 5) {
+      for (int j = 0; j < 5; j++) co.off[d][j] = j - 2;
+    } else {
+      for (int j = 0; j < nc[d]; j++) co.off[d][j] = j;
+    }
+  }
+  return co;
+}
+
+void launch_neighbor_list(Handle &h, bool force) {
+  const int n = h.n;
+  if (force) {
+    int f = FLAG_REBUILD;
+    cudaMemcpyAsync(h.d_flags, &f, sizeof(int), cudaMemcpyHostToDevice, h.stream);
+    cudaStreamSynchronize(h.stream);
+  }
+  const int ncells = h.ncell[0] * h.ncell[1] * h.ncell[2];
+  cudaMemsetAsync(h.d_cell_cnt, 0, sizeof(int) * (size_t)ncells * 2, h.stream);  // counts and cursors
+  k_cell_count<<<nblocks(n, 256), 256, 0, h.stream>>>(n, h.d_rx, h.d_ry, h.d_rz, h.box, h.ncell[0], h.ncell[1],
+                                                       h.ncell[2], h.d_cell_cnt, h.d_atom_cell, h.d_flags);
+  k_cell_scan<<<1, 1024, 0, h.stream>>>(ncells, h.d_cell_cnt, h.d_cell_start, h.d_flags);
+  k_cell_fill<<<nblocks(n, 256), 256, 0, h.stream>>>(n, h.d_atom_cell, h.d_cell_start, h.d_cell_atoms,
+                                                      h.d_cell_cnt + ncells, h.d_flags);
+  k_cell_sort<<<nblocks(ncells, 128), 128, 0, h.stream>>>(ncells, h.d_cell_start, h.d_cell_atoms, h.d_flags);
+  const double rl = fmax(h.prm.vdw_cutoff, h.prm.ewald_cutoff) + h.prm.list_buffer;
+  k_verlet<<<nblocks((int64_t)n * 32, 256), 256, 0, h.stream>>>(
+      n, h.d_rx, h.d_ry, h.d_rz, h.box, cell_offsets(h.ncell), h.d_atom_cell, h.d_cell_start, h.d_cell_atoms,
+      rl * rl, h.cap_nbr, h.d_nbr, h.d_nbr_cnt, h.d_flags);
+  k_list_done<<<nblocks(n, 256), 256, 0, h.stream>>>(n, h.d_refx, h.d_refy, h.d_refz, h.d_rx, h.d_ry, h.d_rz,
+                                                      h.d_flags);
+  h.launches += 6;
+}
+
+void launch_realspace_lists(Handle &h) {
+  const int n = h.n;
+  const double off2 = h.prm.ewald_cutoff * h.prm.ewald_cutoff;
+  k_realspace_lists<<<nblocks((int64_t)n * 32, 256), 256, 0, h.stream>>>(
+      n, h.d_x, h.d_y, h.d_z, h.box, h.d_nbr, h.d_nbr_cnt, h.cap_nbr, off2, h.prm.precond_cutoff, h.d_ewl,
+      h.d_ewl_cnt, h.cap_ewl, h.d_prl, h.d_prl_cnt, h.cap_prl, h.d_flags);
+  FFX_LAUNCHED(h);
+}
+
+}  // namespace ffx

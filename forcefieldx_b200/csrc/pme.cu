@@ -1,0 +1,687 @@
+// pme.cu -- multipole rotation and the particle-mesh Ewald reciprocal space.
+//
+//  k_rotate           InitializationRegion.RotateMultipolesLoop (pme/InitializationRegion.java:375-480)
+//                     with MultipoleType.getRotationMatrix / rotateMultipole (MultipoleType.java:385-536, 1031-1062)
+//  k_bsplines         ReciprocalSpace.BSplineLoop (ReciprocalSpace.java:1338-1412), UniformBSpline (:98-183),
+//                     toFractionalMultipole (:1212-1236)
+//  k_spread_*         SpatialPermanentLoop / SpatialInducedLoop (ReciprocalSpace.java:1445-1505, 1573-1628)
+//  k_fft_axis         Complex3DParallel.convolution (N/fft/Complex3DParallel.java:445, 775-795, 972-1010):
+//                     X and Y passes, a fused Z pass (FFT, influence function, inverse FFT), inverse Y, X.
+//  k_phi              PermanentPhiLoop / InducedPhiLoop (ReciprocalSpace.java:2295-2454, 2506-2775)
+//
+// The mesh is one interleaved complex double grid [nz][ny][nx], 16 B per point, kept
+// L2-resident between passes.  Spreading uses FP64 atomics into the mesh.
+#include <cmath>
+#include <cstring>
+
+#include "ffx_internal.cuh"
+
+namespace ffx {
+
+enum { t000 = 0, t100, t010, t001, t200, t020, t002, t110, t101, t011,
+       t300, t030, t003, t210, t201, t120, t021, t102, t012, t111 };
+
+
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ void d_norm(double *v) {
+  const double l = sqrt(v[0] * v[0] + v[1] * v[1] + v[2] * v[2]);
+  v[0] /= l; v[1] /= l; v[2] /= l;
+}
+
+__global__ void k_rotate(int n, const double *__restrict__ x, const double *__restrict__ y,
+                         const double *__restrict__ z, const int *__restrict__ frame, const int *__restrict__ axis,
+                         const double *__restrict__ lmp, double *gm) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  double R[3][3] = {{1, 0, 0}, {0, 1, 0}, {0, 0, 1}};
+  const int fr = frame[i];
+  if (fr != FFXG_FRAME_NONE) {
+    const double o[3] = {x[i], y[i], z[i]};
+    double zA[3], xA[3], yA[3];
+    const int az = axis[i], ax = axis[n + i], ay = axis[2 * n + i];
+    zA[0] = x[az] - o[0]; zA[1] = y[az] - o[1]; zA[2] = z[az] - o[2];
+    if (ax >= 0) { xA[0] = x[ax] - o[0]; xA[1] = y[ax] - o[1]; xA[2] = z[ax] - o[2]; }
+    if (ay >= 0) { yA[0] = x[ay] - o[0]; yA[1] = y[ay] - o[1]; yA[2] = z[ay] - o[2]; }
+    if (fr == FFXG_FRAME_BISECTOR) {
+      d_norm(zA); d_norm(xA);
+      for (int d = 0; d < 3; d++) zA[d] = xA[d] + zA[d];
+      d_norm(zA);
+      R[0][2] = zA[0]; R[1][2] = zA[1]; R[2][2] = zA[2];
+      const double dt = xA[0] * zA[0] + xA[1] * zA[1] + xA[2] * zA[2];
+      for (int d = 0; d < 3; d++) xA[d] = xA[d] - zA[d] * dt;
+      d_norm(xA);
+    } else if (fr == FFXG_FRAME_ZTHENBISECTOR) {
+      d_norm(zA);
+      R[0][2] = zA[0]; R[1][2] = zA[1]; R[2][2] = zA[2];
+      d_norm(xA); d_norm(yA);
+      for (int d = 0; d < 3; d++) xA[d] = xA[d] + yA[d];
+      d_norm(xA);
+      const double dt = xA[0] * zA[0] + xA[1] * zA[1] + xA[2] * zA[2];
+      for (int d = 0; d < 3; d++) xA[d] = xA[d] - zA[d] * dt;
+      d_norm(xA);
+    } else if (fr == FFXG_FRAME_ZONLY) {
+      d_norm(zA);
+      R[0][2] = zA[0]; R[1][2] = zA[1]; R[2][2] = zA[2];
+      xA[0] = 1.0; xA[1] = 0.0; xA[2] = 0.0;
+      double dt = R[0][2];
+      if (fabs(dt) > 0.866) { xA[0] = 0.0; xA[1] = 1.0; dt = R[1][2]; }
+      for (int d = 0; d < 3; d++) xA[d] = xA[d] - zA[d] * dt;
+      d_norm(xA);
+    } else if (fr == FFXG_FRAME_THREEFOLD) {
+      d_norm(zA); d_norm(xA); d_norm(yA);
+      double s[3];
+      for (int d = 0; d < 3; d++) s[d] = (zA[d] + xA[d]) + yA[d];
+      d_norm(s);
+      R[0][2] = s[0]; R[1][2] = s[1]; R[2][2] = s[2];
+      const double dt = zA[0] * s[0] + zA[1] * s[1] + zA[2] * s[2];
+      for (int d = 0; d < 3; d++) xA[d] = zA[d] - s[d] * dt;
+      d_norm(xA);
+    } else {  // ZTHENX
+      d_norm(zA);
+      R[0][2] = zA[0]; R[1][2] = zA[1]; R[2][2] = zA[2];
+      const double dt = xA[0] * zA[0] + xA[1] * zA[1] + xA[2] * zA[2];
+      for (int d = 0; d < 3; d++) xA[d] = xA[d] - zA[d] * dt;
+      d_norm(xA);
+    }
+    R[0][0] = xA[0]; R[1][0] = xA[1]; R[2][0] = xA[2];
+    R[0][1] = R[2][0] * R[1][2] - R[1][0] * R[2][2];
+    R[1][1] = R[0][0] * R[2][2] - R[2][0] * R[0][2];
+    R[2][1] = R[1][0] * R[0][2] - R[0][0] * R[1][2];
+  }
+  const double d[3] = {lmp[t100 * n + i], lmp[t010 * n + i], lmp[t001 * n + i]};
+  double Q[3][3];
+  Q[0][0] = lmp[t200 * n + i]; Q[1][1] = lmp[t020 * n + i]; Q[2][2] = lmp[t002 * n + i];
+  Q[0][1] = Q[1][0] = lmp[t110 * n + i];
+  Q[0][2] = Q[2][0] = lmp[t101 * n + i];
+  Q[1][2] = Q[2][1] = lmp[t011 * n + i];
+  double rd[3], rq[3][3];
+#pragma unroll
+  for (int a = 0; a < 3; a++) {
+    rd[a] = R[a][0] * d[0] + R[a][1] * d[1] + R[a][2] * d[2];
+#pragma unroll
+    for (int b = a; b < 3; b++) {
+      double s = 0.0;
+#pragma unroll
+      for (int k = 0; k < 3; k++) s += R[a][k] * (R[b][0] * Q[k][0] + R[b][1] * Q[k][1] + R[b][2] * Q[k][2]);
+      rq[a][b] = s;
+    }
+  }
+  gm[t000 * n + i] = lmp[i];
+  gm[t100 * n + i] = rd[0]; gm[t010 * n + i] = rd[1]; gm[t001 * n + i] = rd[2];
+  gm[t200 * n + i] = rq[0][0]; gm[t020 * n + i] = rq[1][1]; gm[t002 * n + i] = rq[2][2];
+  gm[t110 * n + i] = rq[0][1]; gm[t101 * n + i] = rq[0][2]; gm[t011 * n + i] = rq[1][2];
+}
+
+// ---------------------------------------------------------------------------
+// Order-5 B-spline values and three derivatives (UniformBSpline.bSplineDerivatives).
+__device__ __forceinline__ void bspline5(double x, double *out /* [5][4] */) {
+  double w[5][6];
+#pragma unroll
+  for (int a = 0; a < 5; a++)
+#pragma unroll
+    for (int b = 0; b < 6; b++) w[a][b] = 0.0;
+  w[1][0] = 1.0 - x;
+  w[1][1] = x;
+  w[2][0] = 0.5 * (1.0 - x) * w[1][0];
+  w[2][1] = 0.5 * ((x + 1.0) * w[1][0] + (2.0 - x) * w[1][1]);
+  w[2][2] = 0.5 * x * w[1][1];
+#pragma unroll
+  for (int k = 3; k < 5; k++) {
+    const double div = 1.0 / (double)k;
+    const double k1mw = k + (1.0 - x);
+    w[k][k] = div * x * w[k - 1][k - 1];
+#pragma unroll
+    for (int i = 1; i < k; i++) w[k][k - i] = div * ((x + (double)i) * w[k - 1][k - 1 - i] + (k1mw - (double)i) * w[k - 1][k - i]);
+    w[k][0] = div * (1.0 - x) * w[k - 1][0];
+  }
+  // bSplineDiff(work[o2], o1); (work[o3], o2), (o3, o1); (o4, o3), (o4, o2), (o4, o1) with order 5.
+  auto diff = [](double *c, int order) {
+    const int o1 = order - 1;
+    c[order] = c[o1];
+    for (int i = o1; i > 0; i--) c[i] = c[i - 1] - c[i];
+    c[0] = -c[0];
+  };
+  diff(w[3], 4);
+  diff(w[2], 3); diff(w[2], 4);
+  diff(w[1], 2); diff(w[1], 3); diff(w[1], 4);
+#pragma unroll
+  for (int k = 0; k < 5; k++)
+#pragma unroll
+    for (int j = 0; j < 4; j++) out[k * 4 + j] = w[4 - j][k];
+}
+
+__global__ void k_bsplines(int n, const double *__restrict__ x, const double *__restrict__ y,
+                           const double *__restrict__ z, const double *__restrict__ gm, int nfx, int nfy, int nfz,
+                           double *spl, int *igrid, double *fm, PmeConst pc) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const double xi = x[i], yi = y[i], zi = z[i];
+  const int nf[3] = {nfx, nfy, nfz};
+  double w[3];
+  w[0] = xi * pc.recip[0][0] + yi * pc.recip[1][0] + zi * pc.recip[2][0];
+  w[1] = xi * pc.recip[0][1] + yi * pc.recip[1][1] + zi * pc.recip[2][1];
+  w[2] = xi * pc.recip[0][2] + yi * pc.recip[1][2] + zi * pc.recip[2][2];
+  for (int d = 0; d < 3; d++) {
+    const double u = w[d] - floor(w[d] + 0.5) + 0.5;
+    const double fr = nf[d] * u;
+    const int ifr = (int)fr;
+    igrid[d * n + i] = ifr - kOrder;
+    bspline5(fr - ifr, spl + ((size_t)i * 3 + d) * kOrder * 4);
+  }
+  double g[10];
+#pragma unroll
+  for (int j = 0; j < 10; j++) g[j] = gm[j * n + i];
+  fm[i] = g[0];
+#pragma unroll
+  for (int j = 1; j < 4; j++) {
+    double f = 0.0;
+#pragma unroll
+    for (int k = 1; k < 4; k++) f = fma(pc.tmm[j][k], g[k], f);
+    fm[j * n + i] = f;
+  }
+#pragma unroll
+  for (int j = 4; j < 10; j++) {
+    double f = 0.0;
+#pragma unroll
+    for (int k = 4; k < 7; k++) f = fma(pc.tmm[j][k], g[k], f);
+#pragma unroll
+    for (int k = 7; k < 10; k++) f = fma(pc.tmm[j][k] * 2.0, g[k], f);
+    fm[j * n + i] = f * (1.0 / 3.0);
+  }
+}
+
+__device__ __forceinline__ int jmod(int a, int m) {
+  int r = a % m;
+  return r < 0 ? r + m : r;
+}
+
+// One warp per atom; lanes walk the 125 mesh points of the atom's support.
+__global__ void k_spread_permanent(int n, const double *__restrict__ fm, const double *__restrict__ spl,
+                                   const int *__restrict__ igrid, int nfx, int nfy, int nfz, double2 *grid) {
+  const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const int lane = threadIdx.x & 31;
+  if (warp >= n) return;
+  const int i = warp;
+  const double *s = spl + (size_t)i * 3 * kOrder * 4;
+  const double *sx = s, *sy = s + kOrder * 4, *sz = s + 2 * kOrder * 4;
+  const int i0 = igrid[i], j0 = igrid[n + i], k0 = igrid[2 * n + i];
+  double f[10];
+#pragma unroll
+  for (int j = 0; j < 10; j++) f[j] = fm[j * n + i];
+  for (int p = lane; p < 125; p += 32) {
+    const int a1 = p % 5, a2 = (p / 5) % 5, a3 = p / 25;
+    const double v0 = sz[a3 * 4], v1 = sz[a3 * 4 + 1], v2 = sz[a3 * 4 + 2];
+    const double u0 = sy[a2 * 4], u1 = sy[a2 * 4 + 1], u2 = sy[a2 * 4 + 2];
+    const double c0dz1qzz2 = f[t000] * v0 + f[t001] * v1 + f[t002] * v2;
+    const double dy0qyz1 = f[t010] * v0 + f[t011] * v1;
+    const double dx0qxz1 = f[t100] * v0 + f[t101] * v1;
+    const double term0 = fma(c0dz1qzz2, u0, fma(dy0qyz1, u1, f[t020] * v0 * u2));
+    const double term1 = fma(dx0qxz1, u0, f[t110] * v0 * u1);
+    const double term2 = f[t200] * v0 * u0;
+    const double val = fma(sx[a1 * 4], term0, fma(sx[a1 * 4 + 1], term1, sx[a1 * 4 + 2] * term2));
+    const int ii = jmod(i0 + 1 + a1, nfx), jj = jmod(j0 + 1 + a2, nfy), kk = jmod(k0 + 1 + a3, nfz);
+    atomicAdd(&grid[((size_t)kk * nfy + jj) * nfx + ii].x, val);
+  }
+}
+
+__global__ void k_spread_induced(int n, const double *__restrict__ ud, const double *__restrict__ up,
+                                 const double *__restrict__ spl, const int *__restrict__ igrid, int nfx, int nfy,
+                                 int nfz, double2 *grid, PmeConst pc) {
+  const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const int lane = threadIdx.x & 31;
+  if (warp >= n) return;
+  const int i = warp;
+  const double *s = spl + (size_t)i * 3 * kOrder * 4;
+  const double *sx = s, *sy = s + kOrder * 4, *sz = s + 2 * kOrder * 4;
+  const int i0 = igrid[i], j0 = igrid[n + i], k0 = igrid[2 * n + i];
+  double u[3], q[3];
+  const double c[3] = {ud[i], ud[n + i], ud[2 * n + i]};
+  const double cp[3] = {up[i], up[n + i], up[2 * n + i]};
+#pragma unroll
+  for (int a = 0; a < 3; a++) {
+    u[a] = pc.afrac[a][0] * c[0] + pc.afrac[a][1] * c[1] + pc.afrac[a][2] * c[2];
+    q[a] = pc.afrac[a][0] * cp[0] + pc.afrac[a][1] * cp[1] + pc.afrac[a][2] * cp[2];
+  }
+  for (int p = lane; p < 125; p += 32) {
+    const int a1 = p % 5, a2 = (p / 5) % 5, a3 = p / 25;
+    const double v0 = sz[a3 * 4], v1 = sz[a3 * 4 + 1];
+    const double u0 = sy[a2 * 4], u1 = sy[a2 * 4 + 1];
+    const double t0 = fma(u[2] * v1, u0, u[1] * v0 * u1), t1 = u[0] * v0 * u0;
+    const double tp0 = fma(q[2] * v1, u0, q[1] * v0 * u1), tp1 = q[0] * v0 * u0;
+    const double re = fma(sx[a1 * 4], t0, sx[a1 * 4 + 1] * t1);
+    const double im = fma(sx[a1 * 4], tp0, sx[a1 * 4 + 1] * tp1);
+    const int ii = jmod(i0 + 1 + a1, nfx), jj = jmod(j0 + 1 + a2, nfy), kk = jmod(k0 + 1 + a3, nfz);
+    double2 *g = &grid[((size_t)kk * nfy + jj) * nfx + ii];
+    atomicAdd(&g->x, re);
+    atomicAdd(&g->y, im);
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Batched line FFT in shared memory: a CTA transforms `L` lines of length `len`.
+// Stockham self-sorting mixed-radix passes (radices 4, 2, 3, 5, 7), ping-pong
+// between two shared buffers.  `tw` holds exp(-2*pi*i*j/len), j < len.
+
+__device__ __forceinline__ double2 cmul(double2 a, double2 b) {
+  return make_double2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
+}
+
+template <bool FUSE_G>
+__global__ void __launch_bounds__(256) k_fft_axis(double2 *grid, FftAxis ax, int sign, const double2 *__restrict__ tw,
+                                                  const double *__restrict__ G, int gnx, int gny) {
+  // Shared layout is element-major, line-minor: buf[j * L + l].  Consecutive threads
+  // take consecutive lines, so butterflies are bank-conflict free and the Y and Z
+  // passes (adjacent lines adjacent in memory) load and store coalesced.
+  extern __shared__ double2 sm[];
+  const int len = ax.len, L = ax.L;
+  double2 *buf0 = sm, *buf1 = sm + (size_t)len * L;
+  const int gi = blockIdx.x % ax.groups_inner, go = blockIdx.x / ax.groups_inner;
+  const size_t base = (size_t)gi * ax.group_step_inner + (size_t)go * ax.group_step_outer;
+  const bool contiguous = (ax.stride == 1);
+  for (int t = threadIdx.x; t < len * L; t += blockDim.x) {
+    const int l = contiguous ? t / len : t % L, j = contiguous ? t % len : t / L;
+    buf0[j * L + l] = grid[base + (size_t)l * ax.line_step + (size_t)j * ax.stride];
+  }
+  __syncthreads();
+  double2 *in = buf0, *out = buf1;
+  const int npass = FUSE_G ? 2 : 1;
+  for (int pass = 0; pass < npass; pass++) {
+    const int sg = (pass == 0) ? sign : -sign;
+    int Ns = 1;
+    for (int st = 0; st < ax.nradix; st++) {
+      const int R = ax.radix[st];
+      const int nb = len / R;
+      const int tstep = len / (Ns * R);
+      const int wstep = len / R;
+      for (int t = threadIdx.x; t < nb * L; t += blockDim.x) {
+        const int l = t % L, j = t / L;
+        double2 v[7];
+        const int k = j % Ns;
+        for (int r = 0; r < R; r++) {
+          double2 a = in[(j + r * nb) * L + l];
+          if (r > 0 && k > 0) {
+            double2 w = tw[r * k * tstep];
+            if (sg > 0) w.y = -w.y;
+            a = cmul(a, w);
+          }
+          v[r] = a;
+        }
+        const int idxD = (j / Ns) * Ns * R + k;
+        for (int s = 0; s < R; s++) {
+          double2 acc = v[0];
+          for (int r = 1; r < R; r++) {
+            double2 w = tw[((r * s) % R) * wstep];
+            if (sg > 0) w.y = -w.y;
+            const double2 m = cmul(v[r], w);
+            acc.x += m.x; acc.y += m.y;
+          }
+          out[(idxD + s * Ns) * L + l] = acc;
+        }
+      }
+      __syncthreads();
+      double2 *tmp = in; in = out; out = tmp;
+      Ns *= R;
+    }
+    if (FUSE_G && pass == 0) {
+      // Influence function: lines run along z at fixed (x, y) = base + l (line_step 1).
+      for (int t = threadIdx.x; t < len * L; t += blockDim.x) {
+        const int l = t % L, j = t / L;
+        const double g = G[(size_t)j * gnx * gny + base + (size_t)l * ax.line_step];
+        in[j * L + l].x *= g;
+        in[j * L + l].y *= g;
+      }
+      __syncthreads();
+    }
+  }
+  for (int t = threadIdx.x; t < len * L; t += blockDim.x) {
+    const int l = contiguous ? t / len : t % L, j = contiguous ? t % len : t / L;
+    grid[base + (size_t)l * ax.line_step + (size_t)j * ax.stride] = in[j * L + l];
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Potential and derivatives at each atom (20 fractional terms -> Cartesian).
+template <int NT>
+__device__ __forceinline__ void interp(int i, int n, const double *__restrict__ spl, const int *__restrict__ igrid,
+                                       const double2 *__restrict__ grid, int nfx, int nfy, int nfz, bool imag,
+                                       double *tuv) {
+  const double *s = spl + (size_t)i * 3 * kOrder * 4;
+  const double *sx = s, *sy = s + kOrder * 4, *sz = s + 2 * kOrder * 4;
+  const int i0 = igrid[i], j0 = igrid[n + i], k0 = igrid[2 * n + i];
+#pragma unroll
+  for (int t = 0; t < NT; t++) tuv[t] = 0.0;
+  for (int a3 = 0; a3 < kOrder; a3++) {
+    const int kk = jmod(k0 + 1 + a3, nfz);
+    double tu00 = 0, tu10 = 0, tu01 = 0, tu20 = 0, tu11 = 0, tu02 = 0, tu30 = 0, tu21 = 0, tu12 = 0, tu03 = 0;
+    for (int a2 = 0; a2 < kOrder; a2++) {
+      const int jj = jmod(j0 + 1 + a2, nfy);
+      double t0 = 0, t1 = 0, t2 = 0, t3 = 0;
+#pragma unroll
+      for (int a1 = 0; a1 < kOrder; a1++) {
+        const int ii = jmod(i0 + 1 + a1, nfx);
+        const double2 gv = grid[((size_t)kk * nfy + jj) * nfx + ii];
+        const double tq = imag ? gv.y : gv.x;
+        t0 = fma(tq, sx[a1 * 4], t0);
+        t1 = fma(tq, sx[a1 * 4 + 1], t1);
+        if (NT > 4) {
+          t2 = fma(tq, sx[a1 * 4 + 2], t2);
+          t3 = fma(tq, sx[a1 * 4 + 3], t3);
+        }
+      }
+      const double u0 = sy[a2 * 4], u1 = sy[a2 * 4 + 1], u2 = sy[a2 * 4 + 2], u3 = sy[a2 * 4 + 3];
+      tu00 = fma(t0, u0, tu00); tu10 = fma(t1, u0, tu10); tu01 = fma(t0, u1, tu01);
+      if (NT > 4) {
+        tu20 = fma(t2, u0, tu20); tu11 = fma(t1, u1, tu11); tu02 = fma(t0, u2, tu02);
+        tu30 = fma(t3, u0, tu30); tu21 = fma(t2, u1, tu21); tu12 = fma(t1, u2, tu12); tu03 = fma(t0, u3, tu03);
+      }
+    }
+    const double v0 = sz[a3 * 4], v1 = sz[a3 * 4 + 1], v2 = sz[a3 * 4 + 2], v3 = sz[a3 * 4 + 3];
+    tuv[t000] = fma(tu00, v0, tuv[t000]); tuv[t100] = fma(tu10, v0, tuv[t100]);
+    tuv[t010] = fma(tu01, v0, tuv[t010]); tuv[t001] = fma(tu00, v1, tuv[t001]);
+    if (NT > 4) {
+      tuv[t200] = fma(tu20, v0, tuv[t200]); tuv[t020] = fma(tu02, v0, tuv[t020]);
+      tuv[t002] = fma(tu00, v2, tuv[t002]); tuv[t110] = fma(tu11, v0, tuv[t110]);
+      tuv[t101] = fma(tu10, v1, tuv[t101]); tuv[t011] = fma(tu01, v1, tuv[t011]);
+      tuv[t300] = fma(tu30, v0, tuv[t300]); tuv[t030] = fma(tu03, v0, tuv[t030]);
+      tuv[t003] = fma(tu00, v3, tuv[t003]); tuv[t210] = fma(tu21, v0, tuv[t210]);
+      tuv[t201] = fma(tu20, v1, tuv[t201]); tuv[t120] = fma(tu12, v0, tuv[t120]);
+      tuv[t021] = fma(tu02, v1, tuv[t021]); tuv[t102] = fma(tu10, v2, tuv[t102]);
+      tuv[t012] = fma(tu01, v2, tuv[t012]); tuv[t111] = fma(tu11, v1, tuv[t111]);
+    }
+  }
+}
+
+template <int NT>
+__device__ __forceinline__ void store_phi(int i, int n, const double *tuv, double *fphi, double *cphi,
+                                          const PmeConst &pc) {
+  if (fphi) {
+#pragma unroll
+    for (int t = 0; t < NT; t++) fphi[t * n + i] = tuv[t];
+  }
+  cphi[i] = pc.tfm[0][0] * tuv[0];
+#pragma unroll
+  for (int j = 1; j < 4; j++) {
+    double s = 0.0;
+#pragma unroll
+    for (int k = 1; k < 4; k++) s = fma(pc.tfm[j][k], tuv[k], s);
+    cphi[j * n + i] = s;
+  }
+  if (NT > 4) {
+#pragma unroll
+    for (int j = 4; j < 10; j++) {
+      double s = 0.0;
+#pragma unroll
+      for (int k = 4; k < 10; k++) s = fma(pc.tfm[j][k], tuv[k], s);
+      cphi[j * n + i] = s;
+    }
+  }
+}
+
+template <int NT>
+__global__ void k_phi(int n, const double *__restrict__ spl, const int *__restrict__ igrid,
+                      const double2 *__restrict__ grid, int nfx, int nfy, int nfz, double *fphiR, double *cphiR,
+                      double *fphiI, double *cphiI, PmeConst pc) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  double tuv[NT];
+  interp<NT>(i, n, spl, igrid, grid, nfx, nfy, nfz, false, tuv);
+  store_phi<NT>(i, n, tuv, fphiR, cphiR, pc);
+  if (cphiI) {
+    interp<NT>(i, n, spl, igrid, grid, nfx, nfy, nfz, true, tuv);
+    store_phi<NT>(i, n, tuv, fphiI, cphiI, pc);
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Host set-up: transform matrices (ReciprocalSpace.java:1123-1210), twiddles and the
+// generalized influence function with zeta-corrected B-spline moduli (:435-492, :1045-1121).
+static void bspline_coeffs_host(double x, int order, double *c) {
+  double w[16] = {0};
+  w[0] = 1.0 - x;
+  w[1] = x;
+  for (int k = 2; k < order; k++) {
+    double t[16] = {0};
+    const double div = 1.0 / (double)k;
+    const double k1mw = k + (1.0 - x);
+    t[k] = div * x * w[k - 1];
+    for (int i = 1; i < k; i++) t[k - i] = div * ((x + (double)i) * w[k - 1 - i] + (k1mw - (double)i) * w[k - i]);
+    t[0] = div * (1.0 - x) * w[0];
+    std::memcpy(w, t, sizeof(w));
+  }
+  for (int k = 0; k < order; k++) c[k] = w[k];
+}
+
+static std::vector<double> bsmod_host(int nfft, int order, const std::vector<double> &bsarray) {
+  const double PI = 3.14159265358979323846;
+  std::vector<double> bsmod(nfft);
+  double factor = 2.0 * PI / nfft;
+  for (int i = 0; i < nfft; i++) {
+    double s1 = 0.0, s2 = 0.0;
+    for (int j = 0; j < nfft; j++) {
+      const double arg = factor * (double)(i * j);
+      s1 = s1 + bsarray[j] * std::cos(arg);
+      s2 = s2 + bsarray[j] * std::sin(arg);
+    }
+    bsmod[i] = s1 * s1 + s2 * s2;
+  }
+  const double eps = 1.0e-7;
+  if (bsmod[0] < eps) bsmod[0] = 0.5 * bsmod[1];
+  for (int i = 1; i < nfft - 1; i++)
+    if (bsmod[i] < eps) bsmod[i] = 0.5 * (bsmod[i - 1] + bsmod[i + 1]);
+  if (bsmod[nfft - 1] < eps) bsmod[nfft - 1] = 0.5 * bsmod[nfft - 2];
+  for (int i = 0; i < nfft; i++) {
+    int k = i;
+    if (i > nfft / 2) k = k - nfft;
+    double zeta = 1.0;
+    if (k != 0) {
+      double sum1 = 1.0, sum2 = 1.0;
+      const double fct = PI * k / nfft;
+      for (int j = 0; j < 50; j++) {
+        const double arg = fct / (fct + PI * (j + 1));
+        sum1 = sum1 + std::pow(arg, order);
+        sum2 = sum2 + std::pow(arg, 2 * order);
+      }
+      for (int j = 0; j < 50; j++) {
+        const double arg = fct / (fct - PI * (j + 1));
+        sum1 = sum1 + std::pow(arg, order);
+        sum2 = sum2 + std::pow(arg, 2 * order);
+      }
+      zeta = sum2 / sum1;
+    }
+    bsmod[i] = bsmod[i] * zeta * zeta;
+  }
+  return bsmod;
+}
+
+static FftAxis make_axis(int axis, const int nf[3]) {
+  FftAxis a{};
+  const int nx = nf[0], ny = nf[1], nz = nf[2];
+  a.len = nf[axis];
+  int m = a.len;
+  a.nradix = 0;
+  for (int f : {4, 2, 3, 5, 7}) {
+    while (m % f == 0) { a.radix[a.nradix++] = f; m /= f; }
+  }
+  // Lines of a CTA: consecutive along the fastest index that is not the transform axis.
+  const int inner = (axis == 0) ? ny : nx;
+  int L = 1;
+  const int cap = std::max(1, std::min(16, 4096 / a.len));
+  for (int d = 1; d <= cap; d++)
+    if (inner % d == 0) L = d;
+  a.L = L;
+  if (axis == 0) {          // lines (y, z); elements contiguous
+    a.stride = 1; a.line_step = nx;
+    a.groups_inner = ny / L; a.group_step_inner = L * nx; a.group_step_outer = nx * ny;
+  } else if (axis == 1) {   // lines (x, z); elements stride nx
+    a.stride = nx; a.line_step = 1;
+    a.groups_inner = nx / L; a.group_step_inner = L; a.group_step_outer = nx * ny;
+  } else {                  // lines (x, y); elements stride nx*ny
+    a.stride = nx * ny; a.line_step = 1;
+    a.groups_inner = nx / L; a.group_step_inner = L; a.group_step_outer = nx;
+  }
+  return a;
+}
+
+
+void setup_pme(Handle &h) {
+  const int nfx = h.prm.pme_grid[0], nfy = h.prm.pme_grid[1], nfz = h.prm.pme_grid[2];
+  h.nfft[0] = nfx; h.nfft[1] = nfy; h.nfft[2] = nfz;
+  const int nf[3] = {nfx, nfy, nfz};
+  const double A[3][3] = {{h.box.A00, 0, 0}, {0, h.box.A11, 0}, {0, 0, h.box.A22}};
+  static const int qi1[6] = {0, 1, 2, 0, 0, 1};
+  static const int qi2[6] = {0, 1, 2, 1, 2, 2};
+  double a[3][3];
+  for (int i = 0; i < 3; i++)
+    for (int j = 0; j < 3; j++) a[j][i] = nf[j] * A[i][j];
+  std::memset(h.pc.tmm, 0, sizeof(h.pc.tmm));
+  h.pc.tmm[0][0] = 1.0;
+  for (int i = 1; i < 4; i++)
+    for (int j = 0; j < 3; j++) h.pc.tmm[i][1 + j] = a[i - 1][j];
+  for (int i1 = 0; i1 < 3; i1++)
+    for (int i2 = 0; i2 < 6; i2++) h.pc.tmm[i1 + 4][i2 + 4] = a[qi1[i1]][qi1[i2]] * a[qi1[i1]][qi2[i2]];
+  for (int i1 = 3; i1 < 6; i1++) {
+    const int k = qi1[i1], l = qi2[i1];
+    for (int i2 = 0; i2 < 6; i2++) {
+      const int ii = qi1[i2], jj = qi2[i2];
+      h.pc.tmm[i1 + 4][i2 + 4] = a[k][ii] * a[l][jj] + a[k][jj] * a[l][ii];
+    }
+  }
+  double af[3][3];
+  for (int i = 0; i < 3; i++)
+    for (int j = 0; j < 3; j++) af[i][j] = nf[j] * A[i][j];
+  std::memset(h.pc.tfm, 0, sizeof(h.pc.tfm));
+  h.pc.tfm[0][0] = 1.0;
+  for (int i = 1; i < 4; i++)
+    for (int j = 0; j < 3; j++) h.pc.tfm[i][1 + j] = af[i - 1][j];
+  for (int i1 = 0; i1 < 3; i1++) {
+    const int k = qi1[i1];
+    for (int i2 = 0; i2 < 3; i2++) h.pc.tfm[i1 + 4][i2 + 4] = af[k][qi1[i2]] * af[k][qi1[i2]];
+    for (int i2 = 3; i2 < 6; i2++) h.pc.tfm[i1 + 4][i2 + 4] = 2.0 * af[k][qi1[i2]] * af[k][qi2[i2]];
+  }
+  for (int i1 = 3; i1 < 6; i1++) {
+    const int k = qi1[i1], nn = qi2[i1];
+    for (int i2 = 0; i2 < 3; i2++) h.pc.tfm[i1 + 4][i2 + 4] = af[k][qi1[i2]] * af[nn][qi1[i2]];
+    for (int i2 = 3; i2 < 6; i2++) {
+      const int ii = qi1[i2], jj = qi2[i2];
+      h.pc.tfm[i1 + 4][i2 + 4] = af[k][ii] * af[nn][jj] + af[nn][ii] * af[k][jj];
+    }
+  }
+  for (int i = 0; i < 3; i++)
+    for (int j = 0; j < 3; j++) h.pc.afrac[i][j] = nf[i] * A[j][i];
+  std::memcpy(h.pc.recip, A, sizeof(A));
+
+  // Influence function.
+  const int order = h.prm.pme_order;
+  const int maxfft = std::max(std::max(std::max(nfx, nfy), nfz), order + 1);
+  std::vector<double> bsarray(maxfft, 0.0);
+  double c[16];
+  bspline_coeffs_host(0.0, order, c);
+  for (int i = 0; i < order; i++) bsarray[1 + i] = c[i];
+  const std::vector<double> bx = bsmod_host(nfx, order, bsarray), by = bsmod_host(nfy, order, bsarray),
+                            bz = bsmod_host(nfz, order, bsarray);
+  const double PI = 3.14159265358979323846;
+  const double aewald = h.prm.ewald_alpha;
+  const double piTerm = (PI / aewald) * (PI / aewald);
+  const double volTerm = PI * h.box.volume;
+  std::vector<double> G((size_t)nfx * nfy * nfz, 0.0);
+  const int nX2 = (nfx + 1) / 2, nY2 = (nfy + 1) / 2, nZ2 = (nfz + 1) / 2;
+  for (int kz = 0; kz < nfz; kz++)
+    for (int ky = 0; ky < nfy; ky++)
+      for (int kx = 0; kx < nfx; kx++) {
+        if (kx == 0 && ky == 0 && kz == 0) continue;
+        int hh = kx, k = ky, l = kz;
+        if (kx >= nX2) hh -= nfx;
+        if (ky >= nY2) k -= nfy;
+        if (kz >= nZ2) l -= nfz;
+        const double sX = A[0][0] * hh + A[0][1] * k + A[0][2] * l;
+        const double sY = A[1][0] * hh + A[1][1] * k + A[1][2] * l;
+        const double sZ = A[2][0] * hh + A[2][1] * k + A[2][2] * l;
+        const double s2 = sX * sX + sY * sY + sZ * sZ;
+        const double term = -piTerm * s2;
+        double e = 0.0;
+        if (term > -50.0) e = std::exp(term) / (s2 * volTerm * bx[kx] * by[ky] * bz[kz]);
+        G[((size_t)kz * nfy + ky) * nfx + kx] = e;
+      }
+  cudaMemcpy(h.d_influence, G.data(), G.size() * sizeof(double), cudaMemcpyHostToDevice);
+  const int maxn = std::max(nfx, std::max(nfy, nfz));
+  std::vector<double2> tw(3 * (size_t)maxn);
+  for (int d = 0; d < 3; d++)
+    for (int j = 0; j < nf[d]; j++) {
+      const double ang = 2.0 * PI * (double)j / (double)nf[d];
+      tw[(size_t)d * maxn + j] = make_double2(std::cos(ang), -std::sin(ang));
+    }
+  cudaMemcpy(h.d_twiddle, tw.data(), tw.size() * sizeof(double2), cudaMemcpyHostToDevice);
+  for (int d = 0; d < 3; d++) h.axes[d] = make_axis(d, nf);
+  for (int d = 0; d < 3; d++) {
+    const size_t smem = 2 * (size_t)h.axes[d].len * h.axes[d].L * sizeof(double2);
+    cudaFuncSetAttribute(k_fft_axis<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)std::max<size_t>(smem, 48 * 1024));
+    cudaFuncSetAttribute(k_fft_axis<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)std::max<size_t>(smem, 48 * 1024));
+  }
+}
+
+// ---------------------------------------------------------------------------
+void launch_rotate(Handle &h) {
+  k_rotate<<<nblocks(h.n, 128), 128, 0, h.stream>>>(h.n, h.d_x, h.d_y, h.d_z, h.d_frame, h.d_axis, h.d_lmp, h.d_gm);
+  FFX_LAUNCHED(h);
+}
+
+void launch_bsplines(Handle &h) {
+  k_bsplines<<<nblocks(h.n, 128), 128, 0, h.stream>>>(h.n, h.d_x, h.d_y, h.d_z, h.d_gm, h.nfft[0], h.nfft[1],
+                                                       h.nfft[2], h.d_spl, h.d_igrid, h.d_fm, h.pc);
+  FFX_LAUNCHED(h);
+}
+
+static size_t grid_points(const Handle &h) { return (size_t)h.nfft[0] * h.nfft[1] * h.nfft[2]; }
+
+void launch_spread_permanent(Handle &h) {
+  cudaMemsetAsync(h.d_grid, 0, grid_points(h) * sizeof(double2), h.stream);
+  k_spread_permanent<<<nblocks((int64_t)h.n * 32, 256), 256, 0, h.stream>>>(h.n, h.d_fm, h.d_spl, h.d_igrid,
+                                                                             h.nfft[0], h.nfft[1], h.nfft[2], h.d_grid);
+  FFX_LAUNCHED(h);
+}
+
+void launch_spread_induced(Handle &h, const double *ud, const double *up) {
+  cudaMemsetAsync(h.d_grid, 0, grid_points(h) * sizeof(double2), h.stream);
+  k_spread_induced<<<nblocks((int64_t)h.n * 32, 256), 256, 0, h.stream>>>(h.n, ud, up, h.d_spl, h.d_igrid, h.nfft[0],
+                                                                           h.nfft[1], h.nfft[2], h.d_grid, h.pc);
+  FFX_LAUNCHED(h);
+}
+
+void launch_fft_convolution(Handle &h) {
+  const int nfx = h.nfft[0], nfy = h.nfft[1], nfz = h.nfft[2];
+  const int maxn = std::max(nfx, std::max(nfy, nfz));
+  auto run = [&](int d, int sign, bool fuse) {
+    const FftAxis &a = h.axes[d];
+    const int outer = (d == 0) ? nfz : ((d == 1) ? nfz : nfy);
+    const int blocks = a.groups_inner * outer;
+    const size_t smem = 2 * (size_t)a.len * a.L * sizeof(double2);
+    if (fuse)
+      k_fft_axis<true><<<blocks, 256, smem, h.stream>>>(h.d_grid, a, sign, h.d_twiddle + (size_t)d * maxn, h.d_influence, nfx, nfy);
+    else
+      k_fft_axis<false><<<blocks, 256, smem, h.stream>>>(h.d_grid, a, sign, h.d_twiddle + (size_t)d * maxn, nullptr, nfx, nfy);
+    FFX_LAUNCHED(h);
+  };
+  run(0, -1, false);
+  run(1, -1, false);
+  run(2, -1, true);
+  run(1, +1, false);
+  run(0, +1, false);
+}
+
+void launch_phi_permanent(Handle &h) {
+  k_phi<20><<<nblocks(h.n, 128), 128, 0, h.stream>>>(h.n, h.d_spl, h.d_igrid, h.d_grid, h.nfft[0], h.nfft[1],
+                                                      h.nfft[2], h.d_fphi, h.d_cphi, nullptr, nullptr, h.pc);
+  FFX_LAUNCHED(h);
+}
+
+void launch_phi_induced(Handle &h, bool full) {
+  if (full)
+    k_phi<20><<<nblocks(h.n, 128), 128, 0, h.stream>>>(h.n, h.d_spl, h.d_igrid, h.d_grid, h.nfft[0], h.nfft[1],
+                                                        h.nfft[2], h.d_fphiI, h.d_cphiI, h.d_fphiP, h.d_cphiP, h.pc);
+  else
+    k_phi<4><<<nblocks(h.n, 128), 128, 0, h.stream>>>(h.n, h.d_spl, h.d_igrid, h.d_grid, h.nfft[0], h.nfft[1],
+                                                       h.nfft[2], nullptr, h.d_cphiI, nullptr, h.d_cphiP, h.pc);
+  FFX_LAUNCHED(h);
+}
+
+}  // namespace ffx

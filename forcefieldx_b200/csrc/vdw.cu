@@ -1,0 +1,150 @@
+// vdw.cu -- buffered 14-7 van der Waals on the hydrogen-reduced coordinates.
+//
+// VanDerWaalsLoop (VanDerWaals.java:1602-1850) with the Halgren constants
+// (VanDerWaalsForm.java:313-334; delta 0.07, gamma 0.12), the multiplicative taper
+// from vdw-taper * cutoff to the cutoff (MultiplicativeSwitch.java:84-124, 234-236) and
+// the 1-2/1-3/1-4 masks (VanDerWaals.applyMask, :412-428).  A warp owns atom i and
+// gathers over the buffered list in both directions: the force on i's reduced site
+// accumulates in registers; k_vdw_distribute then splits every reduced-site force
+// between the hydrogen and its heavy atom (VanDerWaals.java:1786-1797) as a gather.
+#include "ffx_internal.cuh"
+
+namespace ffx {
+
+
+struct VdwForm {
+  double off2, cut2, t1n, gamma1, delta, gamma;
+  double c0, c1, c2, c3, c4, c5;
+};
+
+__device__ __forceinline__ unsigned vexcl_code(int i, int k, const int *__restrict__ ptr, const int *__restrict__ ek,
+                                               const unsigned *__restrict__ code, const int *__restrict__ lo,
+                                               const int *__restrict__ hi) {
+  if (k < lo[i] || k > hi[i]) return 0u;
+  const int e1 = ptr[i + 1];
+  for (int e = ptr[i]; e < e1; e++)
+    if (ek[e] == k) return code[e];
+  return 0u;
+}
+
+__global__ void __launch_bounds__(256) k_vdw(int n, const double *__restrict__ rx, const double *__restrict__ ry,
+                                             const double *__restrict__ rz, Box bx, const int *__restrict__ vtype,
+                                             int ntypes, const double *__restrict__ vrad,
+                                             const double *__restrict__ veps, const int *__restrict__ nbr,
+                                             const int *__restrict__ nbr_cnt, int cap, const int *__restrict__ eptr,
+                                             const int *__restrict__ ek, const unsigned *__restrict__ ecode,
+                                             const int *__restrict__ elo, const int *__restrict__ ehi, VdwForm vf,
+                                             ScaleTables c_vscales, int gradient, double *eatom, long long *catom, double *gred) {
+  const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const int lane = threadIdx.x & 31;
+  if (warp >= n) return;
+  const int i = warp;
+  const double xi = rx[i], yi = ry[i], zi = rz[i];
+  const int ti = vtype[i];
+  double e = 0.0, gx = 0.0, gy = 0.0, gz = 0.0;
+  long long cnt = 0;
+  const int m = min(nbr_cnt[i], cap);
+  const int *row = nbr + (size_t)i * cap;
+  for (int a = lane; a < m; a += 32) {
+    const int k = row[a];
+    double dx = __dsub_rn(xi, rx[k]), dy = __dsub_rn(yi, ry[k]), dz = __dsub_rn(zi, rz[k]);
+    const double r2 = image_exact(dx, dy, dz, bx);
+    const int tk = vtype[k];
+    const double irv = vrad[ti * ntypes + tk];
+    if (!(r2 <= vf.off2) || !(irv > 0.0)) continue;
+    const unsigned code = vexcl_code(i, k, eptr, ek, ecode, elo, ehi);
+    const double mask = c_vscales.v[(code >> 7) & 3u];
+    if (!(mask > 0.0)) continue;
+    const double r = sqrt(r2);
+    const double ev = mask * veps[ti * ntypes + tk];
+    const double rho = r * irv;
+    const double rho2 = rho * rho;
+    const double rhoDisp1 = rho2 * rho2 * rho2;
+    const double rhoDisp = rhoDisp1 * rho;
+    const double rd = rho + vf.delta, rd2 = rd * rd;
+    const double rhoDelta1 = rd2 * rd2 * rd2;
+    const double rhoDelta = rhoDelta1 * rd;
+    const double t1d = 1.0 / rhoDelta;
+    const double t2d = 1.0 / (rhoDisp + vf.gamma);
+    const double t1 = vf.t1n * t1d;
+    const double t2a = vf.gamma1 * t2d;
+    const double t2 = t2a - 2.0;
+    const double eik = ev * t1 * t2;
+    double taper = 1.0, dtaper = 0.0;
+    if (r2 > vf.cut2) {
+      const double r3 = r2 * r, r4 = r2 * r2, r5 = r2 * r3;
+      taper = vf.c5 * r5 + vf.c4 * r4 + vf.c3 * r3 + vf.c2 * r2 + vf.c1 * r + vf.c0;
+      dtaper = 5.0 * vf.c5 * r4 + 4.0 * vf.c4 * r3 + 3.0 * vf.c3 * r2 + 2.0 * vf.c2 * r + vf.c1;
+    }
+    e += 0.5 * eik * taper;
+    if (k > i) cnt++;
+    if (gradient) {
+      const double dt1d_dr = 7.0 * rhoDelta1 * irv;
+      const double dt2d_dr = 7.0 * rhoDisp1 * irv;
+      const double dt1_dr = t1 * dt1d_dr * t1d;
+      const double dt2_dr = t2a * dt2d_dr * t2d;
+      const double dedr = -ev * (dt1_dr * t2 + t1 * dt2_dr);
+      const double ir = 1.0 / r;
+      const double dsw = eik * dtaper + dedr * taper;
+      gx += dsw * dx * ir; gy += dsw * dy * ir; gz += dsw * dz * ir;
+    }
+  }
+  e = warp_sum(e);
+  gx = warp_sum(gx); gy = warp_sum(gy); gz = warp_sum(gz);
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) cnt += __shfl_xor_sync(0xffffffffu, cnt, o);
+  if (lane == 0) {
+    eatom[i] = e;
+    catom[i] = cnt;
+    if (gradient) { gred[i] = gx; gred[n + i] = gy; gred[2 * n + i] = gz; }
+  }
+}
+
+// g[j] = red_j * G[j] (reduced hydrogen) or G[j] (heavy / unreduced) + sum over the
+// hydrogens c reduced toward j of (1 - red_c) * G[c].
+__global__ void k_vdw_distribute(int n, const double *__restrict__ gred, const int *__restrict__ redp,
+                                 const double *__restrict__ redf, const int *__restrict__ cptr,
+                                 const int *__restrict__ child, double *gvdw) {
+  const int j = blockIdx.x * blockDim.x + threadIdx.x;
+  if (j >= n) return;
+  const double w = (redp[j] != j) ? redf[j] : 1.0 - redf[j];
+  double s0 = w * gred[j], s1 = w * gred[n + j], s2 = w * gred[2 * n + j];
+  for (int e = cptr[j]; e < cptr[j + 1]; e++) {
+    const int c = child[e];
+    const double wc = 1.0 - redf[c];
+    s0 += wc * gred[c]; s1 += wc * gred[n + c]; s2 += wc * gred[2 * n + c];
+  }
+  gvdw[j] = s0; gvdw[n + j] = s1; gvdw[2 * n + j] = s2;
+}
+
+
+void launch_vdw(Handle &h, bool grad) {
+  VdwForm vf{};
+  const double off = h.prm.vdw_cutoff, cut = h.prm.vdw_taper * h.prm.vdw_cutoff;
+  vf.off2 = off * off;
+  vf.cut2 = cut * cut;
+  vf.delta = 0.07;
+  vf.gamma = 0.12;
+  vf.t1n = pow(1.0 + vf.delta, 7.0);
+  vf.gamma1 = 1.0 + vf.gamma;
+  const double a = cut, b = off, a2 = a * a, b2 = b * b, den = pow(b - a, 5.0);
+  vf.c0 = b * b2 * (b2 - 5.0 * a * b + 10.0 * a2) / den;
+  vf.c1 = -30.0 * a2 * b2 / den;
+  vf.c2 = 30.0 * b * a * (b + a) / den;
+  vf.c3 = -10.0 * (a2 + 4.0 * a * b + b2) / den;
+  vf.c4 = 15.0 * (a + b) / den;
+  vf.c5 = -6.0 / den;
+  k_vdw<<<nblocks((int64_t)h.n * 32, 256), 256, 0, h.stream>>>(
+      h.n, h.d_rx, h.d_ry, h.d_rz, h.box, h.d_vtype, h.ntypes, h.d_vrad, h.d_veps, h.d_nbr, h.d_nbr_cnt, h.cap_nbr,
+      h.d_excl_ptr, h.d_excl_k, h.d_excl_code, h.d_excl_lo, h.d_excl_hi, vf, h.scales, grad ? 1 : 0, h.d_eatom, h.d_catom,
+      h.d_gred);
+  FFX_LAUNCHED(h);
+  if (grad) {
+    // Rows 3-5 of d_gred hold the distributed per-atom vdW gradient.
+    k_vdw_distribute<<<nblocks(h.n, 256), 256, 0, h.stream>>>(h.n, h.d_gred, h.d_redp, h.d_redf, h.d_red_ptr,
+                                                               h.d_red_child, h.d_gred + 3 * (size_t)h.n);
+    FFX_LAUNCHED(h);
+  }
+}
+
+}  // namespace ffx

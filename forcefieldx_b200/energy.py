@@ -1,0 +1,172 @@
+"""Host-side mirror of Force Field X's ForceFieldEnergy for the AMOEBA vdW + PME path.
+
+Method names and meanings follow the reference
+(modules/potential/src/main/java/ffx/potential/ForceFieldEnergy.java):
+
+=============================  ===========================================================
+this class                     reference
+=============================  ===========================================================
+energy(x)                      ForceFieldEnergy.energy(double[])            :1806-1830
+energy_and_gradient(x, g)      ForceFieldEnergy.energyAndGradient(x, g)     :1843-1890
+set_coordinates(x)             ForceFieldEnergy.setCoordinates             :2629
+get_permanent_multipole_energy getPermanentMultipoleEnergy                  :2294
+get_polarization_energy        getPolarizationEnergy                        :2322
+get_vdw_energy                 getVanDerWaalsEnergy
+get_induced_dipoles            ParticleMeshEwald.inducedDipole[0] / inducedDipoleCR[0]
+=============================  ===========================================================
+
+Every call goes through libffxcuda.so (include/ffxcuda.h).  There is no CPU
+fallback: a missing library or device raises.  A nonzero status raises
+EnergyException, as the reference throws it from PCGSolver.java:554-568 and
+RealSpaceEnergyRegion.java:384-391.
+"""
+from __future__ import annotations
+
+import ctypes
+from typing import Optional
+
+import numpy as np
+
+from . import cabi
+from .system import COUNT_NAMES, TERM_NAMES, AmoebaParams, AmoebaSystem, params_struct
+
+
+class EnergyException(RuntimeError):
+    """ffx.potential.utils.EnergyException: the evaluation failed (status code attached)."""
+
+    def __init__(self, status: int, message: str):
+        super().__init__(f"{cabi.STATUS_NAMES.get(status, status)}: {message}")
+        self.status = status
+
+
+_LIB = None
+
+
+def library() -> ctypes.CDLL:
+    global _LIB
+    if _LIB is None:
+        _LIB = cabi.load_library()
+    return _LIB
+
+
+def _dp(a: np.ndarray):
+    return a.ctypes.data_as(ctypes.POINTER(ctypes.c_double))
+
+
+class ForceFieldEnergy:
+    """AMOEBA vdW + PME energy and gradient on one B200 (one handle, one CUDA stream)."""
+
+    def __init__(self, system: AmoebaSystem, params: AmoebaParams):
+        self.lib = library()
+        self.system = system
+        self.params = params
+        self.n = system.n_atoms
+        s, self._keep = system.c_struct(cabi)
+        p = params_struct(params, cabi)
+        h = ctypes.c_void_p()
+        st = self.lib.ffxg_create(ctypes.byref(s), ctypes.byref(p), ctypes.byref(h))
+        if st != 0:
+            raise EnergyException(st, self.lib.ffxg_last_error(None).decode())
+        self._h = h
+        self.terms = np.zeros(cabi.N_TERMS)
+        self.counts = np.zeros(cabi.N_COUNTS, dtype=np.int64)
+        self._x = np.ascontiguousarray(system.xyz, dtype=np.float64).copy()
+
+    # ------------------------------------------------------------------
+    def _check(self, st: int):
+        if st != 0:
+            raise EnergyException(st, self.lib.ffxg_last_error(self._h).decode())
+
+    def close(self):
+        if getattr(self, "_h", None):
+            self.lib.ffxg_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    # ------------------------------------------------------------------
+    def set_coordinates(self, x) -> None:
+        self._x = np.ascontiguousarray(np.asarray(x, dtype=np.float64).reshape(self.n, 3))
+        self._check(self.lib.ffxg_set_coordinates(self._h, _dp(self._x)))
+
+    def energy(self, x=None) -> float:
+        if x is not None:
+            self.set_coordinates(x)
+        else:
+            self._check(self.lib.ffxg_set_coordinates(self._h, _dp(self._x)))
+        self._check(self.lib.ffxg_energy(self._h, 0, _dp(self.terms), None,
+                                         self.counts.ctypes.data_as(ctypes.POINTER(ctypes.c_int64))))
+        return float(self.terms[9])
+
+    def energy_and_gradient(self, x=None, g: Optional[np.ndarray] = None):
+        """Returns (energy, gradient[n,3]); fills ``g`` in place when given."""
+        if x is not None:
+            self._x = np.ascontiguousarray(np.asarray(x, dtype=np.float64).reshape(self.n, 3))
+        out = np.zeros((self.n, 3)) if g is None else g
+        buf = out if (out.flags.c_contiguous and out.dtype == np.float64) else np.zeros((self.n, 3))
+        self._check(self.lib.ffxg_energy_and_gradient(
+            self._h, _dp(self._x), _dp(self.terms), _dp(buf),
+            self.counts.ctypes.data_as(ctypes.POINTER(ctypes.c_int64))))
+        if buf is not out:
+            out[...] = buf.reshape(out.shape)
+        return float(self.terms[9]), out
+
+    def energy_device(self, d_xyz: int, d_grad: int = 0) -> float:
+        """Device-resident evaluation: d_xyz / d_grad are device pointers ([n][3] float64)."""
+        self._check(self.lib.ffxg_energy_device(self._h, ctypes.c_void_p(d_xyz),
+                                                ctypes.c_void_p(d_grad) if d_grad else None,
+                                                _dp(self.terms),
+                                                self.counts.ctypes.data_as(ctypes.POINTER(ctypes.c_int64))))
+        return float(self.terms[9])
+
+    # ------------------------------------------------------------------
+    def term(self, name: str) -> float:
+        return float(self.terms[TERM_NAMES.index(name)])
+
+    def count(self, name: str) -> int:
+        return int(self.counts[COUNT_NAMES.index(name)])
+
+    def get_vdw_energy(self) -> float:
+        return self.term("vdw")
+
+    def get_permanent_multipole_energy(self) -> float:
+        return self.term("permanent")
+
+    def get_polarization_energy(self) -> float:
+        return self.term("polarization")
+
+    def get_induced_dipoles(self):
+        u = np.zeros((self.n, 3))
+        ucr = np.zeros((self.n, 3))
+        self._check(self.lib.ffxg_get_induced_dipoles(self._h, _dp(u), _dp(ucr)))
+        return u, ucr
+
+    def get_global_multipoles(self):
+        m = np.zeros((self.n, 10))
+        self._check(self.lib.ffxg_get_global_multipoles(self._h, _dp(m)))
+        return m
+
+    def neighbor_pairs(self) -> np.ndarray:
+        cnt = ctypes.c_int64(0)
+        self._check(self.lib.ffxg_get_neighbor_pairs(self._h, None, ctypes.byref(cnt)))
+        out = np.zeros((cnt.value, 2), dtype=np.int32)
+        self._check(self.lib.ffxg_get_neighbor_pairs(self._h, out.ctypes.data_as(ctypes.POINTER(ctypes.c_int32)),
+                                                     ctypes.byref(cnt)))
+        return out
+
+    @property
+    def stream(self) -> int:
+        return int(self.lib.ffxg_stream(self._h) or 0)
+
+    def launch_count(self) -> int:
+        return int(self.lib.ffxg_last_launch_count(self._h))

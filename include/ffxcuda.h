@@ -192,6 +192,29 @@ void *ffxg_stream(ffxg_handle *h);
 /* Device count of kernel launches issued by the last energy call. */
 int64_t ffxg_last_launch_count(const ffxg_handle *h);
 
+/* Per-stage device timings, the counterpart of PMETimings (pme/PMETimings.java:60-124)
+ * and the per-thread vdW / neighbour-list timers (VanDerWaals.java:1241-1288).  With
+ * timing on, every stage launch is bracketed by CUDA events on the handle's stream;
+ * ffxg_get_timings returns the accumulated milliseconds and launch counts per stage
+ * since timing was (re)enabled. */
+enum {
+  FFXG_STAGE_LISTS = 0,          /* coordinates, motion check, cell and Verlet lists */
+  FFXG_STAGE_VDW = 1,
+  FFXG_STAGE_MULTIPOLES = 2,     /* rotation, B-splines, fractional multipoles */
+  FFXG_STAGE_PERM_RECIP = 3,     /* permanent spread + FFT convolution + potential */
+  FFXG_STAGE_PERM_FIELD = 4,     /* real-space permanent field + direct dipoles */
+  FFXG_STAGE_IND_RECIP = 5,      /* induced spread + FFT convolution + potential */
+  FFXG_STAGE_IND_FIELD = 6,      /* real-space induced field (one launch per field) */
+  FFXG_STAGE_PRECOND = 7,        /* preconditioner field */
+  FFXG_STAGE_PCG_VECTOR = 8,     /* PCG vector updates and dot products */
+  FFXG_STAGE_REAL_ENERGY = 9,    /* real-space energy, force and torque */
+  FFXG_STAGE_RECIP_ENERGY = 10,  /* reciprocal-space energy, force and torque */
+  FFXG_STAGE_GRADIENT = 11,      /* torque to gradient, assembly, sums */
+  FFXG_N_STAGES = 12
+};
+int ffxg_set_timing(ffxg_handle *h, int on);
+int ffxg_get_timings(ffxg_handle *h, double *ms, int64_t *launches, int n);
+
 #ifdef __cplusplus
 }
 #endif

@@ -329,14 +329,22 @@ struct Oracle {
       cidx(i, ca[i], cb[i], cc[i]);
       cells[((size_t)cc[i] * ncb + cb[i]) * nca + ca[i]].push_back(i);
     }
-    const int ea = std::min(2, (nca - 1) / 2), eb = std::min(2, (ncb - 1) / 2), ec = std::min(2, (ncc - 1) / 2);
+    // Offsets -2..2 when a dimension has at least 5 cells, otherwise every cell of
+    // that dimension once (a +-2 search would revisit or miss cells).
+    auto offsets = [](int nc) {
+      std::vector<int> o;
+      if (nc >= 5) { for (int d = -2; d <= 2; d++) o.push_back(d); }
+      else { for (int d = 0; d < nc; d++) o.push_back(d); }
+      return o;
+    };
+    const std::vector<int> oa = offsets(nca), ob = offsets(ncb), oc = offsets(ncc);
     nlist.assign(n, {});
 #pragma omp parallel for schedule(dynamic, 64)
     for (int i = 0; i < n; i++) {
       std::vector<int> &li = nlist[i];
-      for (int dc = -ec; dc <= ec; dc++)
-        for (int db = -eb; db <= eb; db++)
-          for (int da = -ea; da <= ea; da++) {
+      for (int dc : oc)
+        for (int db : ob)
+          for (int da : oa) {
             const int a2 = ((ca[i] + da) % nca + nca) % nca;
             const int b2 = ((cb[i] + db) % ncb + ncb) % ncb;
             const int c2 = ((cc[i] + dc) % ncc + ncc) % ncc;
