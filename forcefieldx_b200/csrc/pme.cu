@@ -11,6 +11,7 @@
 //
 // The mesh is one interleaved complex double grid [nz][ny][nx], 16 B per point, kept
 // L2-resident between passes.  Spreading uses FP64 atomics into the mesh.
+#include <atomic>
 #include <cmath>
 #include <cstring>
 
@@ -682,6 +683,360 @@ void launch_phi_induced(Handle &h, bool full) {
     k_phi<4><<<nblocks(h.n, 128), 128, 0, h.stream>>>(h.n, h.d_spl, h.d_igrid, h.d_grid, h.nfft[0], h.nfft[1],
                                                        h.nfft[2], nullptr, h.d_cphiI, nullptr, h.d_cphiP, h.pc);
   FFX_LAUNCHED(h);
+}
+
+
+// ===========================================================================
+// Allocation-free permanent reciprocal-space potential (ffxg_pme_recip_permanent_noalloc).
+//
+// For callers that may not allocate device memory: a host process whose device
+// memory is owned by another allocator (a framework's caching pool that has
+// reserved the GPU, a JVM or plugin host that forbids new device allocations after
+// start-up), or latency-critical callers that must not pay cudaMalloc's implicit
+// synchronisation.  Inputs and outputs are the caller's device buffers; every
+// intermediate (mesh, influence function, twiddles, B-spline moduli, partial
+// sums) lives in the one file-scope array below, sized for at most
+// kNaMaxAtoms atoms and a kNaMaxDim^3 mesh.  The array exists once per device
+// that loads the library and is held until the process exits.
+namespace {
+constexpr int kNaMaxAtoms = 32768;
+constexpr int kNaMaxDim = 64;
+constexpr int kNaMaxPoints = kNaMaxDim * kNaMaxDim * kNaMaxDim;
+constexpr int kNaThreads = 128;
+constexpr int kNaPartials = kNaMaxAtoms / kNaThreads;   // one partial energy per phi block
+constexpr int kNaMaxDevices = 64;
+
+struct NoAllocScratch {
+  double2 grid[kNaMaxPoints];        // complex mesh
+  double influence[kNaMaxPoints];    // generalized influence function
+  double2 twiddle[3 * kNaMaxDim];    // exp(-2 pi i j / n) per axis
+  double bsmod[3 * kNaMaxDim];       // zeta-corrected B-spline moduli per axis
+  double partial[kNaPartials];       // per-block energy sums
+};
+}  // namespace
+
+static __device__ __align__(256) NoAllocScratch g_noalloc_scratch;
+
+// Device address of the array, looked up once per device.  In host code the name
+// g_noalloc_scratch is only a host-side stand-in, never a device address.
+static std::atomic<NoAllocScratch *> g_noalloc_ptr[kNaMaxDevices];
+
+__device__ void na_bspline_coeffs(double x, double *c) {  // UniformBSpline.bSpline, order 5
+  double w[6] = {1.0 - x, x, 0, 0, 0, 0};
+  for (int k = 2; k < kOrder; k++) {
+    double t[6] = {0, 0, 0, 0, 0, 0};
+    const double div = 1.0 / (double)k;
+    const double k1mw = k + (1.0 - x);
+    t[k] = div * x * w[k - 1];
+    for (int i = 1; i < k; i++) t[k - i] = div * ((x + (double)i) * w[k - 1 - i] + (k1mw - (double)i) * w[k - i]);
+    t[0] = div * (1.0 - x) * w[0];
+    for (int i = 0; i < 6; i++) w[i] = t[i];
+  }
+  for (int i = 0; i < kOrder; i++) c[i] = w[i];
+}
+
+// One block per axis: twiddles, raw moduli, the reference's sequential fix-ups of
+// tiny moduli, then the zeta correction (ReciprocalSpace.discreteFTMod, :435-492).
+__global__ void k_na_tables(int nx, int ny, int nz, NoAllocScratch *s) {
+  const int d = blockIdx.x;
+  const int nf = d == 0 ? nx : (d == 1 ? ny : nz);
+  const int t = threadIdx.x;
+  const double PI = 3.14159265358979323846;
+  double *bsmod = s->bsmod + d * kNaMaxDim;
+  if (t < nf) {
+    double sn, cs;
+    sincospi(2.0 * (double)t / (double)nf, &sn, &cs);
+    s->twiddle[d * kNaMaxDim + t] = make_double2(cs, -sn);
+    double c[kOrder];
+    na_bspline_coeffs(0.0, c);
+    const double factor = 2.0 * PI / nf;
+    double s1 = 0.0, s2 = 0.0;
+    for (int j = 0; j < nf; j++) {
+      const double bj = (j >= 1 && j <= kOrder) ? c[j - 1] : 0.0;
+      const double arg = factor * (double)(t * j);
+      s1 = s1 + bj * cos(arg);
+      s2 = s2 + bj * sin(arg);
+    }
+    bsmod[t] = s1 * s1 + s2 * s2;
+  }
+  __syncthreads();
+  if (t == 0) {
+    const double eps = 1.0e-7;
+    if (bsmod[0] < eps) bsmod[0] = 0.5 * bsmod[1];
+    for (int i = 1; i < nf - 1; i++)
+      if (bsmod[i] < eps) bsmod[i] = 0.5 * (bsmod[i - 1] + bsmod[i + 1]);
+    if (bsmod[nf - 1] < eps) bsmod[nf - 1] = 0.5 * bsmod[nf - 2];
+  }
+  __syncthreads();
+  if (t < nf) {
+    int k = t;
+    if (t > nf / 2) k = k - nf;
+    double zeta = 1.0;
+    if (k != 0) {
+      double sum1 = 1.0, sum2 = 1.0;
+      const double fct = PI * k / nf;
+      for (int j = 0; j < 50; j++) {
+        const double arg = fct / (fct + PI * (j + 1));
+        sum1 = sum1 + pow(arg, (double)kOrder);
+        sum2 = sum2 + pow(arg, (double)(2 * kOrder));
+      }
+      for (int j = 0; j < 50; j++) {
+        const double arg = fct / (fct - PI * (j + 1));
+        sum1 = sum1 + pow(arg, (double)kOrder);
+        sum2 = sum2 + pow(arg, (double)(2 * kOrder));
+      }
+      zeta = sum2 / sum1;
+    }
+    bsmod[t] = bsmod[t] * zeta * zeta;
+  }
+}
+
+// Influence function (ReciprocalSpace.generalizedInfluenceFunction, :1045-1121) and a
+// cleared mesh: every call starts from zero regardless of what the last call left.
+__global__ void k_na_influence(int nx, int ny, int nz, double ax, double ay, double az, double aewald,
+                               double volume, NoAllocScratch *s) {
+  const int m = blockIdx.x * blockDim.x + threadIdx.x;
+  if (m >= nx * ny * nz) return;
+  s->grid[m] = make_double2(0.0, 0.0);
+  const int kx = m % nx, ky = (m / nx) % ny, kz = m / (nx * ny);
+  if (m == 0) { s->influence[0] = 0.0; return; }
+  const double PI = 3.14159265358979323846;
+  int h = kx, k = ky, l = kz;
+  if (kx >= (nx + 1) / 2) h -= nx;
+  if (ky >= (ny + 1) / 2) k -= ny;
+  if (kz >= (nz + 1) / 2) l -= nz;
+  const double sX = ax * h, sY = ay * k, sZ = az * l;
+  const double s2 = sX * sX + sY * sY + sZ * sZ;
+  const double term = -(PI / aewald) * (PI / aewald) * s2;
+  double e = 0.0;
+  if (term > -50.0)
+    e = exp(term) / (s2 * (PI * volume) * s->bsmod[kx] * s->bsmod[kNaMaxDim + ky] * s->bsmod[2 * kNaMaxDim + kz]);
+  s->influence[m] = e;
+}
+
+// Grid origin and order-5 splines of one coordinate (BSplineLoop, :1338-1412).
+__device__ __forceinline__ int na_spline(double w, int nf, double *out) {
+  const double u = w - floor(w + 0.5) + 0.5;
+  const double fr = nf * u;
+  const int ifr = (int)fr;
+  bspline5(fr - ifr, out);
+  return ifr - kOrder;
+}
+
+// Warp per atom: lanes 0-2 build the three spline sets and lanes 0-9 the fractional
+// multipole in shared memory, then all lanes spread the 125 mesh points.
+__global__ void k_na_spread(int n, const double *__restrict__ xyz, const double *__restrict__ mpole, int nx, int ny,
+                            int nz, PmeConst pc, NoAllocScratch *s) {
+  __shared__ double sp[kNaThreads / 32][3][kOrder * 4];
+  __shared__ double sfm[kNaThreads / 32][10];
+  __shared__ int sg[kNaThreads / 32][3];
+  const int wib = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int i = blockIdx.x * (kNaThreads / 32) + wib;
+  if (i >= n) return;
+  const int nf[3] = {nx, ny, nz};
+  if (lane < 3) {
+    const double w = xyz[3 * i] * pc.recip[0][lane] + xyz[3 * i + 1] * pc.recip[1][lane] +
+                     xyz[3 * i + 2] * pc.recip[2][lane];
+    sg[wib][lane] = na_spline(w, nf[lane], sp[wib][lane]);
+  }
+  if (lane < 10) {
+    const double *g = mpole + 10 * (size_t)i;
+    double f = 0.0;
+    if (lane == 0) {
+      f = g[0];
+    } else if (lane < 4) {
+      for (int k = 1; k < 4; k++) f = fma(pc.tmm[lane][k], g[k], f);
+    } else {
+      for (int k = 4; k < 7; k++) f = fma(pc.tmm[lane][k], g[k], f);
+      for (int k = 7; k < 10; k++) f = fma(pc.tmm[lane][k] * 2.0, g[k], f);
+      f = f * (1.0 / 3.0);
+    }
+    sfm[wib][lane] = f;
+  }
+  __syncwarp();
+  const double *sx = sp[wib][0], *sy = sp[wib][1], *sz = sp[wib][2];
+  const double *f = sfm[wib];
+  for (int p = lane; p < 125; p += 32) {
+    const int a1 = p % 5, a2 = (p / 5) % 5, a3 = p / 25;
+    const double v0 = sz[a3 * 4], v1 = sz[a3 * 4 + 1], v2 = sz[a3 * 4 + 2];
+    const double u0 = sy[a2 * 4], u1 = sy[a2 * 4 + 1], u2 = sy[a2 * 4 + 2];
+    const double c0dz1qzz2 = f[t000] * v0 + f[t001] * v1 + f[t002] * v2;
+    const double dy0qyz1 = f[t010] * v0 + f[t011] * v1;
+    const double dx0qxz1 = f[t100] * v0 + f[t101] * v1;
+    const double term0 = fma(c0dz1qzz2, u0, fma(dy0qyz1, u1, f[t020] * v0 * u2));
+    const double term1 = fma(dx0qxz1, u0, f[t110] * v0 * u1);
+    const double term2 = f[t200] * v0 * u0;
+    const double val = fma(sx[a1 * 4], term0, fma(sx[a1 * 4 + 1], term1, sx[a1 * 4 + 2] * term2));
+    const int ii = jmod(sg[wib][0] + 1 + a1, nx), jj = jmod(sg[wib][1] + 1 + a2, ny), kk = jmod(sg[wib][2] + 1 + a3, nz);
+    atomicAdd(&s->grid[((size_t)kk * ny + jj) * nx + ii].x, val);
+  }
+}
+
+// Thread per atom: Cartesian potential and derivatives (10 terms, [n][10]) and the
+// per-block sum of M . Phi (PermanentReciprocalEnergyLoop, :430-446).
+__global__ void k_na_phi(int n, const double *__restrict__ xyz, const double *__restrict__ mpole, int nx, int ny,
+                         int nz, PmeConst pc, double *phi_out, NoAllocScratch *s) {
+  __shared__ double red[kNaThreads / 32];
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  double e = 0.0;
+  if (i < n) {
+    const int nf[3] = {nx, ny, nz};
+    double spl[3][kOrder * 4];
+    int g0[3];
+    for (int d = 0; d < 3; d++) {
+      const double w = xyz[3 * i] * pc.recip[0][d] + xyz[3 * i + 1] * pc.recip[1][d] + xyz[3 * i + 2] * pc.recip[2][d];
+      g0[d] = na_spline(w, nf[d], spl[d]);
+    }
+    double tuv[10] = {0, 0, 0, 0, 0, 0, 0, 0, 0, 0};
+    for (int a3 = 0; a3 < kOrder; a3++) {
+      const int kk = jmod(g0[2] + 1 + a3, nz);
+      double tu00 = 0, tu10 = 0, tu01 = 0, tu20 = 0, tu11 = 0, tu02 = 0;
+      for (int a2 = 0; a2 < kOrder; a2++) {
+        const int jj = jmod(g0[1] + 1 + a2, ny);
+        double t0 = 0, t1 = 0, t2 = 0;
+        for (int a1 = 0; a1 < kOrder; a1++) {
+          const int ii = jmod(g0[0] + 1 + a1, nx);
+          const double tq = s->grid[((size_t)kk * ny + jj) * nx + ii].x;
+          t0 = fma(tq, spl[0][a1 * 4], t0);
+          t1 = fma(tq, spl[0][a1 * 4 + 1], t1);
+          t2 = fma(tq, spl[0][a1 * 4 + 2], t2);
+        }
+        const double u0 = spl[1][a2 * 4], u1 = spl[1][a2 * 4 + 1], u2 = spl[1][a2 * 4 + 2];
+        tu00 = fma(t0, u0, tu00); tu10 = fma(t1, u0, tu10); tu01 = fma(t0, u1, tu01);
+        tu20 = fma(t2, u0, tu20); tu11 = fma(t1, u1, tu11); tu02 = fma(t0, u2, tu02);
+      }
+      const double v0 = spl[2][a3 * 4], v1 = spl[2][a3 * 4 + 1], v2 = spl[2][a3 * 4 + 2];
+      tuv[t000] = fma(tu00, v0, tuv[t000]); tuv[t100] = fma(tu10, v0, tuv[t100]);
+      tuv[t010] = fma(tu01, v0, tuv[t010]); tuv[t001] = fma(tu00, v1, tuv[t001]);
+      tuv[t200] = fma(tu20, v0, tuv[t200]); tuv[t020] = fma(tu02, v0, tuv[t020]);
+      tuv[t002] = fma(tu00, v2, tuv[t002]); tuv[t110] = fma(tu11, v0, tuv[t110]);
+      tuv[t101] = fma(tu10, v1, tuv[t101]); tuv[t011] = fma(tu01, v1, tuv[t011]);
+    }
+    double c[10];
+    c[0] = pc.tfm[0][0] * tuv[0];
+    for (int j = 1; j < 4; j++) {
+      double v = 0.0;
+      for (int k = 1; k < 4; k++) v = fma(pc.tfm[j][k], tuv[k], v);
+      c[j] = v;
+    }
+    for (int j = 4; j < 10; j++) {
+      double v = 0.0;
+      for (int k = 4; k < 10; k++) v = fma(pc.tfm[j][k], tuv[k], v);
+      c[j] = v;
+    }
+    const double *mp = mpole + 10 * (size_t)i;
+    if (phi_out)
+      for (int j = 0; j < 10; j++) phi_out[10 * (size_t)i + j] = c[j];
+    e = mp[t000] * c[t000] + mp[t100] * c[t100] + mp[t010] * c[t010] + mp[t001] * c[t001] +
+        (1.0 / 3.0) * (mp[t200] * c[t200] + mp[t020] * c[t020] + mp[t002] * c[t002] +
+                       2.0 * (mp[t110] * c[t110] + mp[t101] * c[t101] + mp[t011] * c[t011]));
+  }
+  e = warp_sum(e);
+  if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = e;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double b = 0.0;
+    for (int w = 0; w < kNaThreads / 32; w++) b += red[w];
+    s->partial[blockIdx.x] = b;
+  }
+}
+
+__global__ void k_na_energy(int nb, double electric, const NoAllocScratch *s, double *energy) {
+  if (threadIdx.x == 0) {
+    double sum = 0.0;
+    for (int b = 0; b < nb; b++) sum += s->partial[b];
+    *energy = 0.5 * electric * sum;
+  }
+}
+
+static bool na_dim_ok(int n) {
+  if (n < kOrder) return false;
+  for (int f : {2, 3, 5, 7})
+    while (n % f == 0) n /= f;
+  return n == 1;
+}
+
+extern "C" int ffxg_pme_recip_permanent_noalloc(const double *d_xyz, const double *d_mpole, int32_t n_atoms,
+                                                const double box[3], const int32_t pme_grid[3], double ewald_alpha,
+                                                double electric, double *d_phi, double *d_energy, void *stream) {
+  if (!d_xyz || !d_mpole || !d_energy || !box || !pme_grid || n_atoms <= 0 || !(ewald_alpha > 0.0))
+    return FFXG_ERR_BAD_ARG;
+  for (int d = 0; d < 3; d++) {
+    if (!(box[d] > 0.0)) return FFXG_ERR_BAD_ARG;
+    if (pme_grid[d] > kNaMaxDim) return FFXG_ERR_CAPACITY;
+    if (!na_dim_ok(pme_grid[d])) return FFXG_ERR_BAD_ARG;
+  }
+  if (n_atoms > kNaMaxAtoms) return FFXG_ERR_CAPACITY;
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kNaMaxDevices) return FFXG_ERR_CUDA;
+  NoAllocScratch *s = g_noalloc_ptr[dev].load();
+  if (!s) {
+    // First call on this device (device current): resolve the array's device address.
+    if (cudaGetSymbolAddress((void **)&s, g_noalloc_scratch) != cudaSuccess || !s) return FFXG_ERR_CUDA;
+    g_noalloc_ptr[dev].store(s);
+  }
+  cudaStream_t st = (cudaStream_t)stream;
+  // Transforms of this box and mesh, on the host stack.
+  const int nf[3] = {pme_grid[0], pme_grid[1], pme_grid[2]};
+  const double A[3][3] = {{1.0 / box[0], 0, 0}, {0, 1.0 / box[1], 0}, {0, 0, 1.0 / box[2]}};
+  static const int qi1[6] = {0, 1, 2, 0, 0, 1};
+  static const int qi2[6] = {0, 1, 2, 1, 2, 2};
+  PmeConst pc{};
+  double a[3][3], af[3][3];
+  for (int i = 0; i < 3; i++)
+    for (int j = 0; j < 3; j++) { a[j][i] = nf[j] * A[i][j]; af[i][j] = nf[j] * A[i][j]; }
+  pc.tmm[0][0] = 1.0;
+  for (int i = 1; i < 4; i++)
+    for (int j = 0; j < 3; j++) pc.tmm[i][1 + j] = a[i - 1][j];
+  for (int i1 = 0; i1 < 3; i1++)
+    for (int i2 = 0; i2 < 6; i2++) pc.tmm[i1 + 4][i2 + 4] = a[qi1[i1]][qi1[i2]] * a[qi1[i1]][qi2[i2]];
+  for (int i1 = 3; i1 < 6; i1++)
+    for (int i2 = 0; i2 < 6; i2++) {
+      const int k = qi1[i1], l = qi2[i1], ii = qi1[i2], jj = qi2[i2];
+      pc.tmm[i1 + 4][i2 + 4] = a[k][ii] * a[l][jj] + a[k][jj] * a[l][ii];
+    }
+  pc.tfm[0][0] = 1.0;
+  for (int i = 1; i < 4; i++)
+    for (int j = 0; j < 3; j++) pc.tfm[i][1 + j] = af[i - 1][j];
+  for (int i1 = 0; i1 < 3; i1++) {
+    const int k = qi1[i1];
+    for (int i2 = 0; i2 < 3; i2++) pc.tfm[i1 + 4][i2 + 4] = af[k][qi1[i2]] * af[k][qi1[i2]];
+    for (int i2 = 3; i2 < 6; i2++) pc.tfm[i1 + 4][i2 + 4] = 2.0 * af[k][qi1[i2]] * af[k][qi2[i2]];
+  }
+  for (int i1 = 3; i1 < 6; i1++) {
+    const int k = qi1[i1], nn = qi2[i1];
+    for (int i2 = 0; i2 < 3; i2++) pc.tfm[i1 + 4][i2 + 4] = af[k][qi1[i2]] * af[nn][qi1[i2]];
+    for (int i2 = 3; i2 < 6; i2++) {
+      const int ii = qi1[i2], jj = qi2[i2];
+      pc.tfm[i1 + 4][i2 + 4] = af[k][ii] * af[nn][jj] + af[nn][ii] * af[k][jj];
+    }
+  }
+  for (int i = 0; i < 3; i++)
+    for (int j = 0; j < 3; j++) pc.recip[i][j] = A[i][j];
+  const int npts = nf[0] * nf[1] * nf[2];
+  k_na_tables<<<3, kNaMaxDim, 0, st>>>(nf[0], nf[1], nf[2], s);
+  k_na_influence<<<nblocks(npts, 256), 256, 0, st>>>(nf[0], nf[1], nf[2], A[0][0], A[1][1], A[2][2], ewald_alpha,
+                                                       box[0] * box[1] * box[2], s);
+  k_na_spread<<<nblocks(n_atoms, kNaThreads / 32), kNaThreads, 0, st>>>(n_atoms, d_xyz, d_mpole, nf[0], nf[1], nf[2],
+                                                                        pc, s);
+  double2 *grid = s->grid;
+  for (int pass = 0; pass < 5; pass++) {
+    const int d = (pass < 2) ? pass : (pass == 2 ? 2 : 4 - pass);
+    const int sign = (pass < 3) ? -1 : +1;
+    const FftAxis ax = make_axis(d, nf);
+    const int outer = (d == 2) ? nf[1] : nf[2];
+    const size_t smem = 2 * (size_t)ax.len * ax.L * sizeof(double2);
+    if (pass == 2)
+      k_fft_axis<true><<<ax.groups_inner * outer, 256, smem, st>>>(grid, ax, sign, s->twiddle + d * kNaMaxDim,
+                                                                   s->influence, nf[0], nf[1]);
+    else
+      k_fft_axis<false><<<ax.groups_inner * outer, 256, smem, st>>>(grid, ax, sign, s->twiddle + d * kNaMaxDim,
+                                                                    nullptr, nf[0], nf[1]);
+  }
+  const int nb = nblocks(n_atoms, kNaThreads);
+  k_na_phi<<<nb, kNaThreads, 0, st>>>(n_atoms, d_xyz, d_mpole, nf[0], nf[1], nf[2], pc, d_phi, s);
+  k_na_energy<<<1, 32, 0, st>>>(nb, electric, s, d_energy);
+  return cudaGetLastError() == cudaSuccess ? FFXG_OK : FFXG_ERR_CUDA;
 }
 
 }  // namespace ffx

@@ -215,6 +215,34 @@ enum {
 int ffxg_set_timing(ffxg_handle *h, int on);
 int ffxg_get_timings(ffxg_handle *h, double *ms, int64_t *launches, int n);
 
+/* Permanent-multipole reciprocal-space potential and energy without any device
+ * allocation.  This entry point has no counterpart in the reference; it is for
+ * callers that may not allocate device memory themselves or through this library:
+ * a process whose GPU memory is owned by another allocator (a framework's caching
+ * pool, a JVM or plugin host that forbids new device allocations after start-up),
+ * or a latency-critical caller that must not pay cudaMalloc's implicit
+ * synchronisation.  It creates no handle and calls no allocator.
+ *
+ * Inputs and outputs are the caller's device buffers on the current device:
+ * d_xyz[n][3] coordinates (A), d_mpole[n][10] global-frame multipoles (the order of
+ * ffxg_get_global_multipoles), d_phi[n][10] Cartesian potential and derivatives
+ * (may be NULL) and d_energy[1], the permanent reciprocal energy 1/2 * electric *
+ * sum(M . Phi) (kcal/mol, the FFXG_TERM_PERM_RECIP of a neutral cell).  box[3] and
+ * pme_grid[3] are host arrays; `stream` is a cudaStream_t (NULL: the legacy default
+ * stream) and the call is asynchronous on it.
+ *
+ * All intermediates live in one fixed array of about 6.3 MB that each device
+ * holds from the first call until the process exits.  Limits: n_atoms <= 32768 and
+ * every mesh dimension <= 64 (factors 2, 3, 5, 7); beyond them the call returns
+ * FFXG_ERR_CAPACITY without launching anything.  The first call on a device looks
+ * up the array's device address (cudaGetSymbolAddress) with that device current;
+ * make that first call before any stream capture.  Every call on a device shares
+ * the one array: calls that overlap on the GPU (different streams or threads)
+ * race, so the caller must serialise them.  Each call clears the mesh itself. */
+int ffxg_pme_recip_permanent_noalloc(const double *d_xyz, const double *d_mpole, int32_t n_atoms,
+                                     const double box[3], const int32_t pme_grid[3], double ewald_alpha,
+                                     double electric, double *d_phi, double *d_energy, void *stream);
+
 #ifdef __cplusplus
 }
 #endif

@@ -1,0 +1,72 @@
+"""The allocation-free reciprocal-space entry point against the handle-based path.
+
+ffxg_pme_recip_permanent_noalloc serves callers that may not allocate device
+memory (their GPU memory belongs to another allocator, or they must not pay
+cudaMalloc's synchronisation).  This test plays such a caller: it owns every
+buffer, makes two calls in a row through the C ABI, and checks each against the
+permanent reciprocal energy that ffxg_energy computes for the same coordinates and
+multipoles, within the parity tolerance of the other GPU tests.  The file sorts
+last so a run that stops at the first failure has run every other test already.
+"""
+import ctypes
+
+import numpy as np
+import pytest
+
+from forcefieldx_b200 import cabi
+from forcefieldx_b200.energy import ForceFieldEnergy, library
+from forcefieldx_b200.system import water_box, water_params
+
+pytestmark = pytest.mark.gpu
+
+E_REL = 1.0e-8
+
+
+def _call(lib, d_xyz, d_mp, n, box, grid, alpha, electric, d_phi, d_e):
+    b = (ctypes.c_double * 3)(*box)
+    g = (ctypes.c_int32 * 3)(*grid)
+    return lib.ffxg_pme_recip_permanent_noalloc(ctypes.c_void_p(d_xyz), ctypes.c_void_p(d_mp), n, b, g, alpha,
+                                                electric, ctypes.c_void_p(d_phi) if d_phi else None,
+                                                ctypes.c_void_p(d_e), None)
+
+
+def test_no_alloc_matches_handle_path_twice():
+    import torch
+
+    edge = 24.8
+    s = water_box(8, edge, seed=31)
+    p = water_params(edge, pme_grid=(30, 30, 30), vdw_cutoff=9.0, ewald_cutoff=7.0, list_buffer=2.0)
+    with ForceFieldEnergy(s, p) as ffe:
+        ffe.energy(s.xyz)
+        ref = ffe.term("perm_recip")
+        gm = ffe.get_global_multipoles()
+    lib = library()
+    n = s.n_atoms
+    d_xyz = torch.tensor(s.xyz, dtype=torch.float64, device="cuda")
+    d_mp = torch.tensor(gm, dtype=torch.float64, device="cuda")
+    d_phi = torch.empty((n, 10), dtype=torch.float64, device="cuda")
+    d_e = torch.empty(1, dtype=torch.float64, device="cuda")
+    phis = []
+    for _ in range(2):
+        d_phi.fill_(float("nan"))
+        d_e.fill_(float("nan"))
+        st = _call(lib, d_xyz.data_ptr(), d_mp.data_ptr(), n, p.box, p.grid(), p.ewald_alpha, p.electric,
+                   d_phi.data_ptr(), d_e.data_ptr())
+        torch.cuda.synchronize()
+        assert st == 0
+        e = float(d_e.item())
+        assert abs(e - ref) <= E_REL * max(1.0, abs(ref)), (e, ref)
+        phis.append(d_phi.cpu().numpy())
+    assert np.all(np.isfinite(phis[0]))
+    assert np.max(np.abs(phis[0] - phis[1])) <= 1e-12 * max(1.0, np.max(np.abs(phis[0])))
+
+
+def test_no_alloc_rejects_sizes_beyond_its_maximum():
+    import torch
+
+    lib = library()
+    d = torch.zeros(16, dtype=torch.float64, device="cuda")
+    ptr = d.data_ptr()
+    assert _call(lib, ptr, ptr, 40000, (40.0, 40.0, 40.0), (32, 32, 32), 0.545, 332.0637133, 0, ptr) == 6
+    assert _call(lib, ptr, ptr, 100, (40.0, 40.0, 40.0), (80, 32, 32), 0.545, 332.0637133, 0, ptr) == 6
+    assert _call(lib, ptr, ptr, 100, (40.0, 40.0, 40.0), (22, 32, 32), 0.545, 332.0637133, 0, ptr) == 1
