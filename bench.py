@@ -103,8 +103,9 @@ def algorithmic_traffic(stage: str, n: int, pairs_half: int, vdw_list_full: int)
     """Compulsory HBM bytes of one launch of a stage's kernel: every input read once,
     every output written once (list entries 4 B, FP64 per-atom data)."""
     full = 2 * pairs_half
-    if stage == "ind_field":      # list + x,y,z,u(3),p(3),ipdamp,thole,phi(2x3) in; 6 field out
-        return 4.0 * full + n * (4 + 8 * (3 + 3 + 3 + 2 + 6) + 8 * 6)
+    if stage == "ind_field":      # per entry: index 4 B + coefficients (A, B) 16 B; per atom:
+        # x,y,z, p(3), pP(3), phi(2x3), polarizability, r(3), rP(3), z(3), zP(3) in; vec(6) out; count
+        return 20.0 * full + n * (4 + 8 * (3 + 6 + 6 + 1 + 12) + 8 * 6)
     if stage == "real_energy":    # list + x,y,z,gm(10),u,p,ipdamp,thole in; e(2),count,grad,torque out
         return 4.0 * full + n * (4 + 8 * (3 + 10 + 6 + 2) + 8 * 2 + 8 + 8 * 6)
     if stage == "vdw":

@@ -134,6 +134,9 @@ struct Handle {
   int *d_nbr = nullptr, *d_nbr_cnt = nullptr;
   int *d_ewl = nullptr, *d_ewl_cnt = nullptr;
   int *d_prl = nullptr, *d_prl_cnt = nullptr;
+  double2 *d_coefE = nullptr, *d_coefP = nullptr;   // cached dipole-field pair coefficients (A, B)
+  double *d_part2 = nullptr;                        // PCG partial sums of the fixed-grid kernels
+  unsigned *d_counter = nullptr;                    // last-block counter (returns to 0 after each use)
 
   // ---- electrostatics work arrays
   double *d_gm = nullptr;                     // [10][n]
@@ -196,6 +199,7 @@ void launch_fft_convolution(Handle &h);
 void launch_phi_permanent(Handle &h);
 void launch_phi_induced(Handle &h, bool full);
 void launch_permanent_field(Handle &h);
+void launch_realspace_field(Handle &h);
 void launch_direct(Handle &h);
 void launch_induced_recip(Handle &h, const double *ud, const double *up);
 void launch_induced_real(Handle &h, const double *ud, const double *up, double *outD, double *outP);

@@ -51,10 +51,15 @@ static int alloc_lists(Handle &h) {
   if (h.d_nbr) cudaFree(h.d_nbr);
   if (h.d_ewl) cudaFree(h.d_ewl);
   if (h.d_prl) cudaFree(h.d_prl);
+  if (h.d_coefE) cudaFree(h.d_coefE);
+  if (h.d_coefP) cudaFree(h.d_coefP);
   h.d_nbr = h.d_ewl = h.d_prl = nullptr;
+  h.d_coefE = h.d_coefP = nullptr;
   CK(dalloc(&h.d_nbr, (size_t)h.n * h.cap_nbr));
   CK(dalloc(&h.d_ewl, (size_t)h.n * h.cap_ewl));
   CK(dalloc(&h.d_prl, (size_t)h.n * h.cap_prl));
+  CK(dalloc(&h.d_coefE, (size_t)h.n * h.cap_ewl));
+  CK(dalloc(&h.d_coefP, (size_t)h.n * h.cap_prl));
   h.list_valid = false;
   return FFXG_OK;
 }
@@ -213,6 +218,9 @@ static int create_impl(const ffxg_system *s, const ffxg_params *p, Handle &h) {
   CK(dalloc(&h.d_p, 3 * N)); CK(dalloc(&h.d_pP, 3 * N)); CK(dalloc(&h.d_vec, 3 * N)); CK(dalloc(&h.d_vecP, 3 * N));
   const size_t nparts = std::max<size_t>((size_t)nblocks(n, 256) * 8, 148 * 16) + 64;
   CK(dalloc(&h.d_partials, nparts));
+  CK(dalloc(&h.d_part2, 4096 * 8));
+  CK(dalloc(&h.d_counter, 4));
+  CK(cudaMemset(h.d_counter, 0, 4 * sizeof(unsigned)));
   CK(dalloc(&h.d_scalars, 16));
   CK(cudaMallocHost((void **)&h.h_scalars, 16 * sizeof(double)));
   const int nfx = p->pme_grid[0], nfy = p->pme_grid[1], nfz = p->pme_grid[2];
@@ -293,7 +301,8 @@ static void free_all(Handle &h) {
                   h.d_cphi, h.d_fphi, h.d_cphiI, h.d_fphiI, h.d_cphiP, h.d_fphiP, h.d_fieldD, h.d_fieldP, h.d_uD,
                   h.d_uP, h.d_udirD, h.d_udirP, h.d_r, h.d_rP, h.d_zpre, h.d_zpreP, h.d_p, h.d_pP, h.d_vec, h.d_vecP,
                   h.d_partials, h.d_scalars, h.d_grid, h.d_influence, h.d_twiddle, h.d_grad, h.d_torque, h.d_gred,
-                  h.d_eatom, h.d_catom, h.d_result, h.d_cresult, h.d_flags, h.d_xyz_in, h.d_grad_out};
+                  h.d_eatom, h.d_catom, h.d_result, h.d_cresult, h.d_flags, h.d_xyz_in, h.d_grad_out,
+                  h.d_coefE, h.d_coefP, h.d_part2, h.d_counter};
   for (void *q : ptrs)
     if (q) cudaFree(q);
   if (h.h_scalars) cudaFreeHost(h.h_scalars);
@@ -315,10 +324,24 @@ static int evaluate(Handle &h, const double *d_xyz, double *d_grad_xyz, bool gra
     FFX_LAUNCHED(h);
     launch_set_coordinates(h, d_xyz);
     launch_neighbor_list(h, false);
-    launch_realspace_lists(h);
+    timer_end(h, tk);
+    tk = timer_begin(h, FFXG_STAGE_VDW);
+    launch_vdw(h, grad);
+    timer_end(h, tk);
+    tk = timer_begin(h, FFXG_STAGE_MULTIPOLES);
+    launch_rotate(h);
+    launch_bsplines(h);
+    timer_end(h, tk);
+    tk = timer_begin(h, FFXG_STAGE_PERM_RECIP);
+    launch_spread_permanent(h);
+    launch_fft_convolution(h);
+    launch_phi_permanent(h);
+    timer_end(h, tk);
+    tk = timer_begin(h, FFXG_STAGE_PERM_FIELD);
+    launch_realspace_field(h);   // sub-lists, permanent field, pair coefficients, direct dipoles
     timer_end(h, tk);
     // List overflow invalidates everything downstream and non-finite coordinates
-    // make the evaluation meaningless: check both before the expensive stages.
+    // make the evaluation meaningless: check both before the solver.
     cudaMemcpyAsync(h.h_flags, h.d_flags, sizeof(int), cudaMemcpyDeviceToHost, h.stream);
     if (cudaStreamSynchronize(h.stream) != cudaSuccess) {
       h.err = std::string("CUDA error: ") + cudaGetErrorString(cudaGetLastError());
@@ -336,24 +359,8 @@ static int evaluate(Handle &h, const double *d_xyz, double *d_grad_xyz, bool gra
     const bool rebuilt = (f & FLAG_REBUILD) != 0;
     if (rebuilt) h.list_builds++;
     h.list_valid = true;
-    tk = timer_begin(h, FFXG_STAGE_VDW);
-    launch_vdw(h, grad);
-    timer_end(h, tk);
-    tk = timer_begin(h, FFXG_STAGE_MULTIPOLES);
-    launch_rotate(h);
-    launch_bsplines(h);
-    timer_end(h, tk);
-    tk = timer_begin(h, FFXG_STAGE_PERM_RECIP);
-    launch_spread_permanent(h);
-    launch_fft_convolution(h);
-    launch_phi_permanent(h);
-    timer_end(h, tk);
-    tk = timer_begin(h, FFXG_STAGE_PERM_FIELD);
-    launch_permanent_field(h);
     int st = FFXG_OK;
     h.scf_iter = 0;
-    if (h.prm.polarization != FFXG_POLAR_NONE) launch_direct(h);
-    timer_end(h, tk);
     if (h.prm.polarization != FFXG_POLAR_NONE) {
       if (h.prm.polarization == FFXG_POLAR_MUTUAL) st = run_pcg(h);
       if (st == FFXG_OK) {

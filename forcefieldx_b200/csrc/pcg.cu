@@ -3,125 +3,193 @@
 // PCGSolver.scfByPCG (pme/PCGSolver.java:487-602) with InitResidualRegion (:609-663),
 // InitConjugateRegion (:670-770), UpdateResidualRegion (:773-985) and
 // UpdateConjugateRegion (:991-1180, Fletcher-Reeves).  The D and CR systems advance
-// together with separate scalars.  Vectors are FP64 [3][n]; every dot product is a
-// fixed-order two-level sum (per-block partials, then a fixed-order total), so runs
-// are bitwise reproducible.  The host reads back one 16-byte pair of residual norms
-// per iteration to apply the reference's stopping rules.
+// together with separate scalars.
+//
+// The real-space part of every dipole field reuses the per-pair coefficients
+// (A, B) that k_realspace_field stored for this evaluation: the field at i of a dipole
+// set u is sum_k -A_ik u_k + B_ik (u_k . r_ik) r_ik.  So each field costs one
+// streamed pass over the Ewald (or preconditioner) row plus the minimum image of the
+// pair, with no erfc, exp or sqrt.  The field kernels fold in the PCG vector work
+// (A p = p / alpha - T p with its dot products, or z = alpha (E_precond + s r) with
+// r . z).  Vectors are FP64 [3][n]; every dot product is a fixed-order sum over the
+// blocks of a fixed-size grid, so runs are bitwise reproducible.  The residual norms
+// are finished by the last block and read back once per iteration (16 bytes) to apply
+// the reference's stopping rules.
 #include <cmath>
 
 #include "ffx_internal.cuh"
 
 namespace ffx {
 
-constexpr int kPcgThreads = 256;
-enum { P_PAP = 0, P_PAPP, P_RZ, P_RZP, P_EPS, P_EPSP, P_RZN, P_RZNP, P_NCOL };
+constexpr int kFieldThreads = 128;               // 4 warps, one atom per warp per step
+constexpr int kFieldBlocks = 148 * 8;            // fixed grid: deterministic partials
+constexpr int kVecThreads = 256;
+constexpr int kVecBlocks = 148 * 2;
+// Columns of the partial-sum table d_part2[block][8].
+enum { C_PAP = 0, C_PAPP, C_RZ, C_RZP, C_RZN, C_RZNP, C_EPS, C_EPSP };
 
-__device__ __forceinline__ void block_sums(double *vals, int nv, double *part) {
-  __shared__ double sh[P_NCOL][kPcgThreads / 32];
-  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
-  for (int v = 0; v < nv; v++) {
-    const double s = warp_sum(vals[v]);
-    if (lane == 0) sh[v][wid] = s;
+// Fixed-order total of column c over nb blocks by one warp (lane l sums l, l+32, ...).
+__device__ __forceinline__ double warp_total(const double *__restrict__ part, int nb, int c) {
+  const int lane = threadIdx.x & 31;
+  double s = 0.0;
+  for (int b = lane; b < nb; b += 32) s += part[b * 8 + c];
+  return warp_sum(s);
+}
+
+// Block sum of up to 4 per-warp values, written to part[blockIdx.x][c0 .. c0+nv).
+template <int NV>
+__device__ __forceinline__ void block_store(const double *v, double *part, int c0) {
+  __shared__ double sh[NV][32];
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = blockDim.x >> 5;
+#pragma unroll
+  for (int q = 0; q < NV; q++) {
+    const double s = warp_sum(v[q]);
+    if (lane == 0) sh[q][wid] = s;
   }
   __syncthreads();
-  if (threadIdx.x < nv) {
+  if (threadIdx.x < NV) {
     double s = 0.0;
-    for (int w = 0; w < kPcgThreads / 32; w++) s += sh[threadIdx.x][w];
-    part[threadIdx.x] = s;
+    for (int w = 0; w < nw; w++) s += sh[threadIdx.x][w];
+    part[blockIdx.x * 8 + c0 + threadIdx.x] = s;
   }
 }
 
-// Fixed-order total of column c over nb blocks; computed by every block identically.
-__device__ __forceinline__ double total(const double *__restrict__ part, int nb, int c) {
-  double s = 0.0;
-  for (int b = 0; b < nb; b++) s += part[b * P_NCOL + c];
-  return s;
-}
-
-__global__ void k_pcg_residual_init(int n, const double *__restrict__ polar, const double *__restrict__ udD,
-                                    const double *__restrict__ udP, const double *__restrict__ uD,
-                                    const double *__restrict__ uP, const double *__restrict__ fD,
-                                    const double *__restrict__ fP, double *r, double *rP) {
-  const int i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= n) return;
-  const double a = polar[i];
-  const bool ok = a > 0.0;
-  const double ip = ok ? 1.0 / a : 0.0;
-  for (int d = 0; d < 3; d++) {
-    const size_t j = (size_t)d * n + i;
-    r[j] = ok ? (udD[j] - uD[j]) * ip + fD[j] : 0.0;
-    rP[j] = ok ? (udP[j] - uP[j]) * ip + fP[j] : 0.0;
+// Dipole field at atom i from the cached coefficient row (warp cooperative).
+__device__ __forceinline__ void coef_field(int i, int n, const double *__restrict__ x, const double *__restrict__ y,
+                                           const double *__restrict__ z, const Box &bx, const int *__restrict__ lst,
+                                           const int *__restrict__ lst_cnt, int cap,
+                                           const double2 *__restrict__ coef, const double *__restrict__ ud,
+                                           const double *__restrict__ up, const double *__restrict__ scale_by,
+                                           double *f) {
+  const int lane = threadIdx.x & 31;
+  const double xi = x[i], yi = y[i], zi = z[i];
+  double fx = 0, fy = 0, fz = 0, px = 0, py = 0, pz = 0;
+  const int cnt = min(lst_cnt[i], cap);
+  const int *row = lst + (size_t)i * cap;
+  const double2 *crow = coef + (size_t)i * cap;
+  for (int a = lane; a < cnt; a += 32) {
+    const int k = row[a];
+    const double2 c = crow[a];
+    double xr = __dsub_rn(x[k], xi), yr = __dsub_rn(y[k], yi), zr = __dsub_rn(z[k], zi);
+    image_exact(xr, yr, zr, bx);
+    const double sk = scale_by ? scale_by[k] : 1.0;
+    const double ukx = sk * ud[k], uky = sk * ud[n + k], ukz = sk * ud[2 * n + k];
+    const double pkx = sk * up[k], pky = sk * up[n + k], pkz = sk * up[2 * n + k];
+    const double ukr = c.y * (ukx * xr + uky * yr + ukz * zr);
+    const double pkr = c.y * (pkx * xr + pky * yr + pkz * zr);
+    fx += -c.x * ukx + ukr * xr; fy += -c.x * uky + ukr * yr; fz += -c.x * ukz + ukr * zr;
+    px += -c.x * pkx + pkr * xr; py += -c.x * pky + pkr * yr; pz += -c.x * pkz + pkr * zr;
   }
+  f[0] = warp_sum(fx); f[1] = warp_sum(fy); f[2] = warp_sum(fz);
+  f[3] = warp_sum(px); f[4] = warp_sum(py); f[5] = warp_sum(pz);
 }
 
-// z = alpha (E_precond + s r); optionally p = z (first iteration) and partial r.z_new.
+// MODE 0: field of (ud, up) into outD/outP (used for the final field of the solution).
+// MODE 1: initial residual r = (u_dir - u) / alpha + E(u) with u == u_dir (InitResidualRegion).
+// MODE 2: vec = p / alpha - E(p) and partials of p . vec and r . z (UpdateApLoop).
+template <int MODE>
+__global__ void __launch_bounds__(kFieldThreads) k_pcg_field(
+    int n, const double *__restrict__ x, const double *__restrict__ y, const double *__restrict__ z, Box bx,
+    const int *__restrict__ ewl, const int *__restrict__ ewl_cnt, int capE, const double2 *__restrict__ coefE,
+    const double *__restrict__ ud, const double *__restrict__ up, const double *__restrict__ cphiD,
+    const double *__restrict__ cphiP, double aewald3, const double *__restrict__ polar,
+    const double *__restrict__ udirD, const double *__restrict__ udirP, const double *__restrict__ r,
+    const double *__restrict__ rP, const double *__restrict__ zz, const double *__restrict__ zP, double *outD,
+    double *outP, double *part) {
+  const int lane = threadIdx.x & 31;
+  const int wstride = gridDim.x * (blockDim.x >> 5);
+  double acc[4] = {0, 0, 0, 0};
+  for (int i = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5); i < n; i += wstride) {
+    double f[6];
+    coef_field(i, n, x, y, z, bx, ewl, ewl_cnt, capE, coefE, ud, up, nullptr, f);
+    if (lane == 0) {
+      for (int d = 0; d < 3; d++) {
+        f[d] += aewald3 * ud[d * n + i] - cphiD[(1 + d) * n + i];
+        f[3 + d] += aewald3 * up[d * n + i] - cphiP[(1 + d) * n + i];
+      }
+      const double a = polar[i];
+      const bool ok = a > 0.0;
+      const double ip = ok ? 1.0 / a : 0.0;
+      for (int d = 0; d < 3; d++) {
+        const size_t j = (size_t)d * n + i;
+        if (MODE == 0) {
+          outD[j] = f[d];
+          outP[j] = f[3 + d];
+        } else if (MODE == 1) {
+          outD[j] = ok ? (udirD[j] - ud[j]) * ip + f[d] : 0.0;
+          outP[j] = ok ? (udirP[j] - up[j]) * ip + f[3 + d] : 0.0;
+        } else {
+          const double vv = ok ? ud[j] * ip - f[d] : 0.0;
+          const double vp = ok ? up[j] * ip - f[3 + d] : 0.0;
+          outD[j] = vv;
+          outP[j] = vp;
+          acc[0] += ud[j] * vv;
+          acc[1] += up[j] * vp;
+          acc[2] += r[j] * zz[j];
+          acc[3] += rP[j] * zP[j];
+        }
+      }
+    }
+  }
+  if (MODE == 2) block_store<4>(acc, part, C_PAP);
+}
+
+// z = alpha (E_precond(alpha r) + s r) (InitConjugateRegion / UpdatePreconditionerLoop);
+// INIT also sets p = z, otherwise the partials of r . z_new are stored.
 template <bool INIT>
-__global__ void __launch_bounds__(kPcgThreads) k_pcg_z(int n, const double *__restrict__ polar,
-                                                       const double *__restrict__ preD,
-                                                       const double *__restrict__ preP, const double *__restrict__ r,
-                                                       const double *__restrict__ rP, double s, double *z, double *zP,
-                                                       double *p, double *pP, double *part) {
-  const int i = blockIdx.x * blockDim.x + threadIdx.x;
-  double v[2] = {0.0, 0.0};
-  if (i < n) {
-    const double a = polar[i];
-    for (int d = 0; d < 3; d++) {
-      const size_t j = (size_t)d * n + i;
-      const double zz = a * (preD[j] + s * r[j]);
-      const double zp = a * (preP[j] + s * rP[j]);
-      z[j] = zz; zP[j] = zp;
-      if (INIT) { p[j] = zz; pP[j] = zp; }
-      v[0] += r[j] * zz;
-      v[1] += rP[j] * zp;
+__global__ void __launch_bounds__(kFieldThreads) k_pcg_precond(
+    int n, const double *__restrict__ x, const double *__restrict__ y, const double *__restrict__ z, Box bx,
+    const int *__restrict__ prl, const int *__restrict__ prl_cnt, int capP, const double2 *__restrict__ coefP,
+    const double *__restrict__ polar, const double *__restrict__ r, const double *__restrict__ rP, double s,
+    double *zz, double *zP, double *p, double *pP, double *part) {
+  const int lane = threadIdx.x & 31;
+  const int wstride = gridDim.x * (blockDim.x >> 5);
+  double acc[2] = {0, 0};
+  for (int i = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5); i < n; i += wstride) {
+    double f[6];
+    coef_field(i, n, x, y, z, bx, prl, prl_cnt, capP, coefP, r, rP, polar, f);
+    if (lane == 0) {
+      const double a = polar[i];
+      for (int d = 0; d < 3; d++) {
+        const size_t j = (size_t)d * n + i;
+        const double vz = a * (f[d] + s * r[j]);
+        const double vp = a * (f[3 + d] + s * rP[j]);
+        zz[j] = vz;
+        zP[j] = vp;
+        if (INIT) {
+          p[j] = vz;
+          pP[j] = vp;
+        }
+        acc[0] += r[j] * vz;
+        acc[1] += rP[j] * vp;
+      }
     }
   }
-  if (!INIT) block_sums(v, 2, part + blockIdx.x * P_NCOL + P_RZN);
+  if (!INIT) block_store<2>(acc, part, C_RZN);
 }
 
-// vec = p / alpha - T p; partials of p.Ap and r.z (UpdateApLoop).
-__global__ void __launch_bounds__(kPcgThreads) k_pcg_ap(int n, const double *__restrict__ polar,
-                                                        const double *__restrict__ p, const double *__restrict__ pP,
-                                                        const double *__restrict__ fD, const double *__restrict__ fP,
-                                                        const double *__restrict__ r, const double *__restrict__ rP,
-                                                        const double *__restrict__ z, const double *__restrict__ zP,
-                                                        double *vec, double *vecP, double *part) {
-  const int i = blockIdx.x * blockDim.x + threadIdx.x;
-  double v[4] = {0, 0, 0, 0};
-  if (i < n) {
-    const double a = polar[i];
-    const bool ok = a > 0.0;
-    const double ip = ok ? 1.0 / a : 0.0;
-    for (int d = 0; d < 3; d++) {
-      const size_t j = (size_t)d * n + i;
-      const double vv = ok ? p[j] * ip - fD[j] : 0.0;
-      const double vp = ok ? pP[j] * ip - fP[j] : 0.0;
-      vec[j] = vv; vecP[j] = vp;
-      v[0] += p[j] * vv;
-      v[1] += pP[j] * vp;
-      v[2] += r[j] * z[j];
-      v[3] += rP[j] * zP[j];
-    }
-  }
-  block_sums(v, 4, part + blockIdx.x * P_NCOL + P_PAP);
-}
-
-// r -= alpha vec; u += alpha p; partial |r|^2 (UpdateResidualAndInducedLoop).
-__global__ void __launch_bounds__(kPcgThreads) k_pcg_update(int n, int nb, const double *__restrict__ vec,
+// alpha = r.z / p.Ap; r -= alpha vec; u += alpha p; |r|^2 partials; the last block
+// finishes both norms into out[0..1] and re-arms the counter.
+__global__ void __launch_bounds__(kVecThreads) k_pcg_update(int n, int nbf, const double *__restrict__ vec,
                                                             const double *__restrict__ vecP,
                                                             const double *__restrict__ p,
                                                             const double *__restrict__ pP, double *r, double *rP,
-                                                            double *uD, double *uP, double *part) {
+                                                            double *uD, double *uP, const double *__restrict__ partF,
+                                                            double *partE, unsigned *counter, double *out) {
   __shared__ double alpha[2];
-  if (threadIdx.x == 0) {
-    const double pap = total(part, nb, P_PAP), papP = total(part, nb, P_PAPP);
-    const double rz = total(part, nb, P_RZ), rzP = total(part, nb, P_RZP);
-    alpha[0] = (pap != 0.0) ? rz / pap : rz;
-    alpha[1] = (papP != 0.0) ? rzP / papP : rzP;
+  __shared__ bool last;
+  if (threadIdx.x < 32) {
+    const double pap = warp_total(partF, nbf, C_PAP), papP = warp_total(partF, nbf, C_PAPP);
+    const double rz = warp_total(partF, nbf, C_RZ), rzP = warp_total(partF, nbf, C_RZP);
+    if (threadIdx.x == 0) {
+      alpha[0] = (pap != 0.0) ? rz / pap : rz;
+      alpha[1] = (papP != 0.0) ? rzP / papP : rzP;
+    }
   }
   __syncthreads();
-  const int i = blockIdx.x * blockDim.x + threadIdx.x;
   double v[2] = {0.0, 0.0};
-  if (i < n) {
+  const int stride = gridDim.x * blockDim.x;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) {
     for (int d = 0; d < 3; d++) {
       const size_t j = (size_t)d * n + i;
       const double rr = r[j] - alpha[0] * vec[j];
@@ -133,82 +201,97 @@ __global__ void __launch_bounds__(kPcgThreads) k_pcg_update(int n, int nb, const
       v[1] += rp * rp;
     }
   }
+  block_store<2>(v, partE, C_EPS);
+  __threadfence();
+  if (threadIdx.x == 0) last = (atomicAdd(counter, 1u) == gridDim.x - 1);
   __syncthreads();
-  block_sums(v, 2, part + blockIdx.x * P_NCOL + P_EPS);
-}
-
-__global__ void k_pcg_eps(int nb, const double *__restrict__ part, double *out) {
-  if (threadIdx.x == 0) {
-    out[0] = total(part, nb, P_EPS);
-    out[1] = total(part, nb, P_EPSP);
+  if (last && threadIdx.x < 32) {
+    __threadfence();
+    const double e0 = warp_total(partE, gridDim.x, C_EPS), e1 = warp_total(partE, gridDim.x, C_EPSP);
+    if (threadIdx.x == 0) {
+      out[0] = e0;
+      out[1] = e1;
+      *counter = 0u;
+    }
   }
 }
 
-// beta = r.z_new / r.z_old; p = z + beta p (UpdateConjugateLoop).
-__global__ void __launch_bounds__(kPcgThreads) k_pcg_p(int n, int nb, const double *__restrict__ part,
-                                                       const double *__restrict__ z, const double *__restrict__ zP,
+// beta = r.z_new / r.z_old; p = z + beta p (UpdateConjugateLoop, Fletcher-Reeves).
+__global__ void __launch_bounds__(kVecThreads) k_pcg_p(int n, int nbf, const double *__restrict__ part,
+                                                       const double *__restrict__ zz, const double *__restrict__ zP,
                                                        double *p, double *pP) {
   __shared__ double beta[2];
-  if (threadIdx.x == 0) {
-    double old = total(part, nb, P_RZ), oldP = total(part, nb, P_RZP);
-    if (old == 0.0) old = 1.0;
-    if (oldP == 0.0) oldP = 1.0;
-    beta[0] = total(part, nb, P_RZN) / old;
-    beta[1] = total(part, nb, P_RZNP) / oldP;
+  if (threadIdx.x < 32) {
+    double old = warp_total(part, nbf, C_RZ), oldP = warp_total(part, nbf, C_RZP);
+    const double nw = warp_total(part, nbf, C_RZN), nwP = warp_total(part, nbf, C_RZNP);
+    if (threadIdx.x == 0) {
+      if (old == 0.0) old = 1.0;
+      if (oldP == 0.0) oldP = 1.0;
+      beta[0] = nw / old;
+      beta[1] = nwP / oldP;
+    }
   }
   __syncthreads();
-  const int i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= n) return;
-  for (int d = 0; d < 3; d++) {
-    const size_t j = (size_t)d * n + i;
-    p[j] = z[j] + beta[0] * p[j];
-    pP[j] = zP[j] + beta[1] * pP[j];
+  const int stride = gridDim.x * blockDim.x;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) {
+    for (int d = 0; d < 3; d++) {
+      const size_t j = (size_t)d * n + i;
+      p[j] = zz[j] + beta[0] * p[j];
+      pP[j] = zP[j] + beta[1] * pP[j];
+    }
   }
 }
 
-// Reciprocal (spread, FFT, potential) and real-space parts of one induced field, timed separately.
-static void induced_field_timed(Handle &h, const double *ud, const double *up, double *outD, double *outP) {
-  int tk = timer_begin(h, FFXG_STAGE_IND_RECIP);
-  launch_induced_recip(h, ud, up);
-  timer_end(h, tk);
-  tk = timer_begin(h, FFXG_STAGE_IND_FIELD);
-  launch_induced_real(h, ud, up, outD, outP);
-  timer_end(h, tk);
+// ---------------------------------------------------------------------------
+static double aewald3_of(const Handle &h) {
+  const double a = h.prm.ewald_alpha;
+  return 4.0 / 3.0 * pow(a, 3.0) / 1.7724538509055160273;
+}
+
+template <int MODE>
+static void launch_field(Handle &h, const double *ud, const double *up, double *outD, double *outP) {
+  k_pcg_field<MODE><<<kFieldBlocks, kFieldThreads, 0, h.stream>>>(
+      h.n, h.d_x, h.d_y, h.d_z, h.box, h.d_ewl, h.d_ewl_cnt, h.cap_ewl, h.d_coefE, ud, up, h.d_cphiI, h.d_cphiP,
+      aewald3_of(h), h.d_polar, h.d_udirD, h.d_udirP, h.d_r, h.d_rP, h.d_zpre, h.d_zpreP, outD, outP, h.d_part2);
+  FFX_LAUNCHED(h);
+}
+
+template <bool INIT>
+static void launch_precond(Handle &h) {
+  k_pcg_precond<INIT><<<kFieldBlocks, kFieldThreads, 0, h.stream>>>(
+      h.n, h.d_x, h.d_y, h.d_z, h.box, h.d_prl, h.d_prl_cnt, h.cap_prl, h.d_coefP, h.d_polar, h.d_r, h.d_rP,
+      h.prm.precond_scale, h.d_zpre, h.d_zpreP, h.d_p, h.d_pP, h.d_part2);
+  FFX_LAUNCHED(h);
 }
 
 int run_pcg(Handle &h) {
   const int n = h.n;
-  const int nb = nblocks(n, kPcgThreads);
-  double *part = h.d_partials;
-  double *fD = h.d_fieldD, *fP = h.d_fieldP;  // reused as T p scratch
-  double *preD = h.d_vec + 0, *preP = h.d_vecP;  // preconditioner field scratch shares vec storage
-  // Field of the direct dipoles: u == udir at entry.
-  induced_field_timed(h, h.d_uD, h.d_uP, fD, fP);
-  int tk = timer_begin(h, FFXG_STAGE_PCG_VECTOR);
-  k_pcg_residual_init<<<nblocks(n, 256), 256, 0, h.stream>>>(n, h.d_polar, h.d_udirD, h.d_udirP, h.d_uD, h.d_uP, fD,
-                                                              fP, h.d_r, h.d_rP);
+  // Field of the direct dipoles (u == u_dir at entry) gives the initial residual.
+  int tk = timer_begin(h, FFXG_STAGE_IND_RECIP);
+  launch_induced_recip(h, h.d_uD, h.d_uP);
+  timer_end(h, tk);
+  tk = timer_begin(h, FFXG_STAGE_IND_FIELD);
+  launch_field<1>(h, h.d_uD, h.d_uP, h.d_r, h.d_rP);
   timer_end(h, tk);
   tk = timer_begin(h, FFXG_STAGE_PRECOND);
-  launch_precond_field(h, h.d_r, h.d_rP, preD, preP);
+  launch_precond<true>(h);
   timer_end(h, tk);
-  tk = timer_begin(h, FFXG_STAGE_PCG_VECTOR);
-  k_pcg_z<true><<<nb, kPcgThreads, 0, h.stream>>>(n, h.d_polar, preD, preP, h.d_r, h.d_rP, h.prm.precond_scale,
-                                                  h.d_zpre, h.d_zpreP, h.d_p, h.d_pP, part);
-  timer_end(h, tk);
-  h.launches += 2;
   int iter = 0;
   double eps = 100.0;
   int status = FFXG_OK;
   while (true) {
-    induced_field_timed(h, h.d_p, h.d_pP, fD, fP);
-    tk = timer_begin(h, FFXG_STAGE_PCG_VECTOR);
-    k_pcg_ap<<<nb, kPcgThreads, 0, h.stream>>>(n, h.d_polar, h.d_p, h.d_pP, fD, fP, h.d_r, h.d_rP, h.d_zpre, h.d_zpreP,
-                                               h.d_vec, h.d_vecP, part);
-    k_pcg_update<<<nb, kPcgThreads, 0, h.stream>>>(n, nb, h.d_vec, h.d_vecP, h.d_p, h.d_pP, h.d_r, h.d_rP, h.d_uD,
-                                                   h.d_uP, part);
-    k_pcg_eps<<<1, 32, 0, h.stream>>>(nb, part, h.d_scalars);
+    tk = timer_begin(h, FFXG_STAGE_IND_RECIP);
+    launch_induced_recip(h, h.d_p, h.d_pP);
     timer_end(h, tk);
-    h.launches += 3;
+    tk = timer_begin(h, FFXG_STAGE_IND_FIELD);
+    launch_field<2>(h, h.d_p, h.d_pP, h.d_vec, h.d_vecP);
+    timer_end(h, tk);
+    tk = timer_begin(h, FFXG_STAGE_PCG_VECTOR);
+    k_pcg_update<<<kVecBlocks, kVecThreads, 0, h.stream>>>(n, kFieldBlocks, h.d_vec, h.d_vecP, h.d_p, h.d_pP, h.d_r,
+                                                           h.d_rP, h.d_uD, h.d_uP, h.d_part2, h.d_part2 + 8 * 2048,
+                                                           h.d_counter, h.d_scalars);
+    timer_end(h, tk);
+    FFX_LAUNCHED(h);
     cudaMemcpyAsync(h.h_scalars, h.d_scalars, 2 * sizeof(double), cudaMemcpyDeviceToHost, h.stream);
     if (cudaStreamSynchronize(h.stream) != cudaSuccess) return FFXG_ERR_CUDA;
     const double previous = eps;
@@ -218,14 +301,12 @@ int run_pcg(Handle &h) {
     if (iter >= h.prm.max_scf_iter) { status = FFXG_ERR_SCF_MAXITER; break; }
     if (eps < h.prm.polar_eps) break;
     tk = timer_begin(h, FFXG_STAGE_PRECOND);
-    launch_precond_field(h, h.d_r, h.d_rP, preD, preP);
+    launch_precond<false>(h);
     timer_end(h, tk);
     tk = timer_begin(h, FFXG_STAGE_PCG_VECTOR);
-    k_pcg_z<false><<<nb, kPcgThreads, 0, h.stream>>>(n, h.d_polar, preD, preP, h.d_r, h.d_rP, h.prm.precond_scale,
-                                                     h.d_zpre, h.d_zpreP, nullptr, nullptr, part);
-    k_pcg_p<<<nb, kPcgThreads, 0, h.stream>>>(n, nb, part, h.d_zpre, h.d_zpreP, h.d_p, h.d_pP);
+    k_pcg_p<<<kVecBlocks, kVecThreads, 0, h.stream>>>(n, kFieldBlocks, h.d_part2, h.d_zpre, h.d_zpreP, h.d_p, h.d_pP);
     timer_end(h, tk);
-    h.launches += 2;
+    FFX_LAUNCHED(h);
   }
   h.scf_iter = iter;
   return status;

@@ -267,6 +267,69 @@ __device__ __forceinline__ double2 cmul(double2 a, double2 b) {
   return make_double2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
 }
 
+// Radix-R Stockham butterfly for one (line, j) pair.  R is a compile-time constant so
+// the R values stay in registers; the small DFTs of R = 2, 3, 4 use their closed
+// forms, R = 5 and 7 use the twiddle table.
+template <int R>
+__device__ __forceinline__ void fft_butterfly(const double2 *in, double2 *out, int j, int l, int L, int nb, int Ns,
+                                              int len, int sg, const double2 *__restrict__ tw) {
+  double2 v[R];
+  const int k = j % Ns;
+  const int tstep = len / (Ns * R);
+#pragma unroll
+  for (int r = 0; r < R; r++) {
+    double2 a = in[(j + r * nb) * L + l];
+    if (r > 0 && k > 0) {
+      double2 w = tw[r * k * tstep];
+      if (sg > 0) w.y = -w.y;
+      a = cmul(a, w);
+    }
+    v[r] = a;
+  }
+  const int idxD = (j / Ns) * Ns * R + k;
+  double2 y[R];
+  if (R == 2) {
+    y[0] = make_double2(v[0].x + v[1].x, v[0].y + v[1].y);
+    y[1] = make_double2(v[0].x - v[1].x, v[0].y - v[1].y);
+  } else if (R == 4) {
+    // W4 = exp(sg * i * pi / 2) = sg * i.
+    const double2 s02 = make_double2(v[0].x + v[2].x, v[0].y + v[2].y);
+    const double2 d02 = make_double2(v[0].x - v[2].x, v[0].y - v[2].y);
+    const double2 s13 = make_double2(v[1].x + v[3].x, v[1].y + v[3].y);
+    const double2 d13 = make_double2(v[1].x - v[3].x, v[1].y - v[3].y);
+    // i * d13 = (-d13.y, d13.x)
+    const double2 id13 = make_double2(-sg * d13.y, sg * d13.x);
+    y[0] = make_double2(s02.x + s13.x, s02.y + s13.y);
+    y[1] = make_double2(d02.x + id13.x, d02.y + id13.y);
+    y[2] = make_double2(s02.x - s13.x, s02.y - s13.y);
+    y[3] = make_double2(d02.x - id13.x, d02.y - id13.y);
+  } else if (R == 3) {
+    const double c = -0.5, s = sg * 0.86602540378443864676;  // cos(2 pi / 3), sg * sin(2 pi / 3)
+    const double2 t = make_double2(v[1].x + v[2].x, v[1].y + v[2].y);
+    const double2 d = make_double2(v[1].x - v[2].x, v[1].y - v[2].y);
+    y[0] = make_double2(v[0].x + t.x, v[0].y + t.y);
+    const double2 m = make_double2(v[0].x + c * t.x, v[0].y + c * t.y);
+    y[1] = make_double2(m.x - s * d.y, m.y + s * d.x);
+    y[2] = make_double2(m.x + s * d.y, m.y - s * d.x);
+  } else {
+    const int wstep = len / R;
+#pragma unroll
+    for (int q = 0; q < R; q++) {
+      double2 acc = v[0];
+#pragma unroll
+      for (int r = 1; r < R; r++) {
+        double2 w = tw[((r * q) % R) * wstep];
+        if (sg > 0) w.y = -w.y;
+        const double2 m = cmul(v[r], w);
+        acc.x += m.x; acc.y += m.y;
+      }
+      y[q] = acc;
+    }
+  }
+#pragma unroll
+  for (int q = 0; q < R; q++) out[(idxD + q * Ns) * L + l] = y[q];
+}
+
 template <bool FUSE_G>
 __global__ void __launch_bounds__(256) k_fft_axis(double2 *grid, FftAxis ax, int sign, const double2 *__restrict__ tw,
                                                   const double *__restrict__ G, int gnx, int gny) {
@@ -292,31 +355,14 @@ __global__ void __launch_bounds__(256) k_fft_axis(double2 *grid, FftAxis ax, int
     for (int st = 0; st < ax.nradix; st++) {
       const int R = ax.radix[st];
       const int nb = len / R;
-      const int tstep = len / (Ns * R);
-      const int wstep = len / R;
       for (int t = threadIdx.x; t < nb * L; t += blockDim.x) {
         const int l = t % L, j = t / L;
-        double2 v[7];
-        const int k = j % Ns;
-        for (int r = 0; r < R; r++) {
-          double2 a = in[(j + r * nb) * L + l];
-          if (r > 0 && k > 0) {
-            double2 w = tw[r * k * tstep];
-            if (sg > 0) w.y = -w.y;
-            a = cmul(a, w);
-          }
-          v[r] = a;
-        }
-        const int idxD = (j / Ns) * Ns * R + k;
-        for (int s = 0; s < R; s++) {
-          double2 acc = v[0];
-          for (int r = 1; r < R; r++) {
-            double2 w = tw[((r * s) % R) * wstep];
-            if (sg > 0) w.y = -w.y;
-            const double2 m = cmul(v[r], w);
-            acc.x += m.x; acc.y += m.y;
-          }
-          out[(idxD + s * Ns) * L + l] = acc;
+        switch (R) {
+          case 4: fft_butterfly<4>(in, out, j, l, L, nb, Ns, len, sg, tw); break;
+          case 2: fft_butterfly<2>(in, out, j, l, L, nb, Ns, len, sg, tw); break;
+          case 3: fft_butterfly<3>(in, out, j, l, L, nb, Ns, len, sg, tw); break;
+          case 5: fft_butterfly<5>(in, out, j, l, L, nb, Ns, len, sg, tw); break;
+          default: fft_butterfly<7>(in, out, j, l, L, nb, Ns, len, sg, tw); break;
         }
       }
       __syncthreads();
@@ -430,6 +476,46 @@ __global__ void k_phi(int n, const double *__restrict__ spl, const int *__restri
   if (cphiI) {
     interp<NT>(i, n, spl, igrid, grid, nfx, nfy, nfz, true, tuv);
     store_phi<NT>(i, n, tuv, fphiI, cphiI, pc);
+  }
+}
+
+// Field terms only (first derivatives of the Re and Im potentials), one warp per atom:
+// lanes walk the 125 support points, then the six partial sums reduce by shuffles.
+// Used inside the PCG loop, where only t100, t010, t001 of the induced potential are read.
+__global__ void k_phi_field(int n, const double *__restrict__ spl, const int *__restrict__ igrid,
+                            const double2 *__restrict__ grid, int nfx, int nfy, int nfz, PmeConst pc,
+                            double *cphiR, double *cphiI) {
+  const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const int lane = threadIdx.x & 31;
+  if (warp >= n) return;
+  const int i = warp;
+  const double *sp = spl + (size_t)i * 3 * kOrder * 4;
+  const double *sx = sp, *sy = sp + kOrder * 4, *sz = sp + 2 * kOrder * 4;
+  const int i0 = igrid[i], j0 = igrid[n + i], k0 = igrid[2 * n + i];
+  double rx = 0, ry = 0, rz = 0, ix = 0, iy = 0, iz = 0;
+  for (int p = lane; p < 125; p += 32) {
+    const int a1 = p % 5, a2 = (p / 5) % 5, a3 = p / 25;
+    const int ii = jmod(i0 + 1 + a1, nfx), jj = jmod(j0 + 1 + a2, nfy), kk = jmod(k0 + 1 + a3, nfz);
+    const double2 g = grid[((size_t)kk * nfy + jj) * nfx + ii];
+    const double x0 = sx[a1 * 4], x1 = sx[a1 * 4 + 1];
+    const double y0 = sy[a2 * 4], y1 = sy[a2 * 4 + 1];
+    const double z0 = sz[a3 * 4], z1 = sz[a3 * 4 + 1];
+    const double wx = x1 * y0 * z0, wy = x0 * y1 * z0, wz = x0 * y0 * z1;
+    rx = fma(g.x, wx, rx); ry = fma(g.x, wy, ry); rz = fma(g.x, wz, rz);
+    ix = fma(g.y, wx, ix); iy = fma(g.y, wy, iy); iz = fma(g.y, wz, iz);
+  }
+  rx = warp_sum(rx); ry = warp_sum(ry); rz = warp_sum(rz);
+  ix = warp_sum(ix); iy = warp_sum(iy); iz = warp_sum(iz);
+  if (lane < 2) {
+    const double f[3] = {lane == 0 ? rx : ix, lane == 0 ? ry : iy, lane == 0 ? rz : iz};
+    double *out = lane == 0 ? cphiR : cphiI;
+#pragma unroll
+    for (int j = 1; j < 4; j++) {
+      double v = 0.0;
+#pragma unroll
+      for (int k = 1; k < 4; k++) v = fma(pc.tfm[j][k], f[k - 1], v);
+      out[j * n + i] = v;
+    }
   }
 }
 
@@ -680,8 +766,9 @@ void launch_phi_induced(Handle &h, bool full) {
     k_phi<20><<<nblocks(h.n, 128), 128, 0, h.stream>>>(h.n, h.d_spl, h.d_igrid, h.d_grid, h.nfft[0], h.nfft[1],
                                                         h.nfft[2], h.d_fphiI, h.d_cphiI, h.d_fphiP, h.d_cphiP, h.pc);
   else
-    k_phi<4><<<nblocks(h.n, 128), 128, 0, h.stream>>>(h.n, h.d_spl, h.d_igrid, h.d_grid, h.nfft[0], h.nfft[1],
-                                                       h.nfft[2], nullptr, h.d_cphiI, nullptr, h.d_cphiP, h.pc);
+    k_phi_field<<<nblocks((int64_t)h.n * 32, 128), 128, 0, h.stream>>>(h.n, h.d_spl, h.d_igrid, h.d_grid, h.nfft[0],
+                                                                        h.nfft[1], h.nfft[2], h.pc, h.d_cphiI,
+                                                                        h.d_cphiP);
   FFX_LAUNCHED(h);
 }
 

@@ -119,6 +119,166 @@ __global__ void k_permanent_field(int n, const double *__restrict__ x, const dou
   }
 }
 
+// Real-space lists, permanent field, cached pair coefficients and direct dipoles in one
+// pass (PermanentRealSpaceFieldLoop, pme/PermanentFieldRegion.java:595-815, which also
+// derives the Ewald and preconditioner lists; DirectLoop, pme/DirectRegion.java:170-243).
+// Phase 1 compacts the buffered row into the Ewald row (r2 <= off2) and the
+// preconditioner row (r < pcut).  Phase 2 walks the Ewald row: it accumulates the D and
+// CR permanent fields and stores, per entry, the two symmetric coefficients of the
+// unmasked Thole-damped dipole field, A = bn1 - (1 - s3) rr3 and B = bn2 - (1 - s5) rr5,
+// so the field of any dipole set is -A u_k + B (u_k . r) r; entries inside the
+// preconditioner cutoff also store the Ewald-free pair (pme/PCGSolver.java:1300-1331).
+__global__ void __launch_bounds__(128) k_realspace_field(
+    int n, const double *__restrict__ x, const double *__restrict__ y, const double *__restrict__ z, Box bx,
+    const double *__restrict__ gm, const double *__restrict__ ipdamp, const double *__restrict__ thole,
+    const int *__restrict__ nbr, const int *__restrict__ nbr_cnt, int cap, double off2, double pcut, int *ewl,
+    int *ewl_cnt, int capE, int *prl, int *prl_cnt, int capP, double2 *coefE, double2 *coefP, Excl ex, EwaldCoef ec,
+    ScaleTables c_scales, const double *__restrict__ cphi, const double *__restrict__ polar, int direct,
+    double *fieldD, double *fieldP, double *uD, double *uP, double *udD, double *udP, int *flags) {
+  const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const int lane = threadIdx.x & 31;
+  if (warp >= n) return;
+  const int i = warp;
+  const unsigned lt = (1u << lane) - 1u;
+  const double xi = x[i], yi = y[i], zi = z[i];
+  // ---- phase 1: sub-lists
+  {
+    const int cnt = min(nbr_cnt[i], cap);
+    const int *row = nbr + (size_t)i * cap;
+    int ce = 0, cp = 0;
+    for (int base = 0; base < cnt; base += 32) {
+      const int a = base + lane;
+      bool ew = false, pr = false;
+      int k = -1;
+      if (a < cnt) {
+        k = row[a];
+        double dx = __dsub_rn(x[k], xi), dy = __dsub_rn(y[k], yi), dz = __dsub_rn(z[k], zi);
+        const double r2 = image_exact(dx, dy, dz, bx);
+        ew = r2 <= off2;
+        pr = ew && (sqrt(r2) < pcut);
+      }
+      const unsigned me = __ballot_sync(0xffffffffu, ew);
+      const unsigned mp = __ballot_sync(0xffffffffu, pr);
+      if (ew) {
+        const int pos = ce + __popc(me & lt);
+        if (pos < capE) ewl[(size_t)i * capE + pos] = k;
+      }
+      if (pr) {
+        const int pos = cp + __popc(mp & lt);
+        if (pos < capP) prl[(size_t)i * capP + pos] = k;
+      }
+      ce += __popc(me);
+      cp += __popc(mp);
+    }
+    if (lane == 0) {
+      ewl_cnt[i] = ce;
+      prl_cnt[i] = cp;
+      if (ce > capE) atomicOr(flags, FLAG_EWALD_OVERFLOW);
+      if (cp > capP) atomicOr(flags, FLAG_PRECOND_OVERFLOW);
+    }
+  }
+  __syncwarp();
+  // ---- phase 2: permanent field and coefficients
+  const double pdi = ipdamp[i], pti = thole[i];
+  double fx = 0, fy = 0, fz = 0, px = 0, py = 0, pz = 0;
+  const int cnt = min(ewl_cnt[i], capE);
+  const int *row = ewl + (size_t)i * capE;
+  int cp = 0;
+  for (int base = 0; base < cnt; base += 32) {
+    const int a = base + lane;
+    const bool act = a < cnt;
+    bool pr = false;
+    double2 cpre = make_double2(0.0, 0.0);
+    if (act) {
+      const int k = row[a];
+      double xr = __dsub_rn(x[k], xi), yr = __dsub_rn(y[k], yi), zr = __dsub_rn(z[k], zi);
+      const double r2 = image_exact(xr, yr, zr, bx);
+      const double ck = gm[t000 * n + k], dkx = gm[t100 * n + k], dky = gm[t010 * n + k], dkz = gm[t001 * n + k];
+      const double qkxx = gm[t200 * n + k] * (1.0 / 3.0), qkyy = gm[t020 * n + k] * (1.0 / 3.0);
+      const double qkzz = gm[t002 * n + k] * (1.0 / 3.0), qkxy = gm[t110 * n + k] * (1.0 / 3.0);
+      const double qkxz = gm[t101 * n + k] * (1.0 / 3.0), qkyz = gm[t011 * n + k] * (1.0 / 3.0);
+      const double r = sqrt(r2);
+      const double ralpha = ec.aewald * r;
+      const double exp2a = exp(-ralpha * ralpha);
+      const double rr1 = 1.0 / r, rr2 = rr1 * rr1;
+      const double bn0 = erfc(ralpha) * rr1;
+      const double bn1 = (bn0 + ec.an0 * exp2a) * rr2;
+      const double bn2 = (3.0 * bn1 + ec.an1 * exp2a) * rr2;
+      const double bn3 = (5.0 * bn2 + ec.an2 * exp2a) * rr2;
+      double scale3 = 1.0, scale5 = 1.0, scale7 = 1.0;
+      double damp = pdi * ipdamp[k];
+      const double pgamma = fmin(pti, thole[k]);
+      const double rdamp = r * damp;
+      damp = -pgamma * rdamp * rdamp * rdamp;
+      if (damp > -50.0) {
+        const double expdamp = exp(damp);
+        scale3 = 1.0 - expdamp;
+        scale5 = 1.0 - expdamp * (1.0 - damp);
+        scale7 = 1.0 - expdamp * (1.0 - damp + 0.6 * damp * damp);
+      }
+      const unsigned code = excl_code(i, k, ex.ptr, ex.k, ex.code, ex.lo, ex.hi);
+      const double scale = c_scales.d[(code >> 6) & 1u];
+      const double scalep = c_scales.p[(code >> 3) & 7u];
+      const double dsc3 = scale3 * scale, dsc5 = scale5 * scale, dsc7 = scale7 * scale;
+      const double psc3 = scale3 * scalep, psc5 = scale5 * scalep, psc7 = scale7 * scalep;
+      const double rr3 = rr1 * rr2, rr5 = 3.0 * rr3 * rr2, rr7 = 5.0 * rr5 * rr2;
+      const double drr3 = (1.0 - dsc3) * rr3, drr5 = (1.0 - dsc5) * rr5, drr7 = (1.0 - dsc7) * rr7;
+      const double prr3 = (1.0 - psc3) * rr3, prr5 = (1.0 - psc5) * rr5, prr7 = (1.0 - psc7) * rr7;
+      const double dkr = dkx * xr + dky * yr + dkz * zr;
+      const double qkx = 2.0 * (qkxx * xr + qkxy * yr + qkxz * zr);
+      const double qky = 2.0 * (qkxy * xr + qkyy * yr + qkyz * zr);
+      const double qkz = 2.0 * (qkxz * xr + qkyz * yr + qkzz * zr);
+      const double qkr = (qkx * xr + qky * yr + qkz * zr) * 0.5;
+      const double bn123k = bn1 * ck - bn2 * dkr + bn3 * qkr;
+      const double fimx = -xr * bn123k - bn1 * dkx + bn2 * qkx;
+      const double fimy = -yr * bn123k - bn1 * dky + bn2 * qky;
+      const double fimz = -zr * bn123k - bn1 * dkz + bn2 * qkz;
+      const double drr357k = drr3 * ck - drr5 * dkr + drr7 * qkr;
+      const double fidx = -xr * drr357k - drr3 * dkx + drr5 * qkx;
+      const double fidy = -yr * drr357k - drr3 * dky + drr5 * qky;
+      const double fidz = -zr * drr357k - drr3 * dkz + drr5 * qkz;
+      fx += fimx - fidx; fy += fimy - fidy; fz += fimz - fidz;
+      const double prr357k = prr3 * ck - prr5 * dkr + prr7 * qkr;
+      const double fipx = -xr * prr357k - prr3 * dkx + prr5 * qkx;
+      const double fipy = -yr * prr357k - prr3 * dky + prr5 * qky;
+      const double fipz = -zr * prr357k - prr3 * dkz + prr5 * qkz;
+      px += fimx - fipx; py += fimy - fipy; pz += fimz - fipz;
+      // Induced-field coefficients (no masks), InducedDipoleFieldRegion.java:383-404.
+      const double urr3 = (1.0 - scale3) * rr3, urr5 = (1.0 - scale5) * rr5;
+      if (a < capE) coefE[(size_t)i * capE + a] = make_double2(bn1 - urr3, bn2 - urr5);
+      pr = r < pcut;
+      if (pr) {
+        const double b1 = rr1 * rr2, b2 = 3.0 * b1 * rr2;   // Ewald off: bn0 = 1/r
+        cpre = make_double2(b1 - urr3, b2 - urr5);
+      }
+    }
+    const unsigned mp = __ballot_sync(0xffffffffu, pr);
+    if (pr) {
+      const int pos = cp + __popc(mp & lt);
+      if (pos < capP) coefP[(size_t)i * capP + pos] = cpre;
+    }
+    cp += __popc(mp);
+  }
+  fx = warp_sum(fx); fy = warp_sum(fy); fz = warp_sum(fz);
+  px = warp_sum(px); py = warp_sum(py); pz = warp_sum(pz);
+  if (lane == 0) {
+    if (direct) {
+      const double a = polar[i];
+      const double f0 = ec.aewald3 * gm[t100 * n + i] - cphi[1 * n + i];
+      const double f1 = ec.aewald3 * gm[t010 * n + i] - cphi[2 * n + i];
+      const double f2 = ec.aewald3 * gm[t001 * n + i] - cphi[3 * n + i];
+      fx += f0; fy += f1; fz += f2;
+      px += f0; py += f1; pz += f2;
+      uD[i] = a * fx; uD[n + i] = a * fy; uD[2 * n + i] = a * fz;
+      uP[i] = a * px; uP[n + i] = a * py; uP[2 * n + i] = a * pz;
+      udD[i] = a * fx; udD[n + i] = a * fy; udD[2 * n + i] = a * fz;
+      udP[i] = a * px; udP[n + i] = a * py; udP[2 * n + i] = a * pz;
+    }
+    fieldD[i] = fx; fieldD[n + i] = fy; fieldD[2 * n + i] = fz;
+    fieldP[i] = px; fieldP[n + i] = py; fieldP[2 * n + i] = pz;
+  }
+}
+
 // field += aewald3 * d_i - phi_recip (DirectLoop); u = alpha * field.
 __global__ void k_direct(int n, const double *__restrict__ gm, const double *__restrict__ cphi,
                          const double *__restrict__ polar, double aewald3, double *fieldD, double *fieldP, double *uD,
@@ -580,6 +740,19 @@ static Excl excl(const Handle &h) {
   return e;
 }
 
+
+void launch_realspace_field(Handle &h) {
+  const double off2 = h.prm.ewald_cutoff * h.prm.ewald_cutoff;
+  k_realspace_field<<<nblocks((int64_t)h.n * 32, 128), 128, 0, h.stream>>>(
+      h.n, h.d_x, h.d_y, h.d_z, h.box, h.d_gm, h.d_ipdamp, h.d_thole, h.d_nbr, h.d_nbr_cnt, h.cap_nbr, off2,
+      h.prm.precond_cutoff, h.d_ewl, h.d_ewl_cnt, h.cap_ewl, h.d_prl, h.d_prl_cnt, h.cap_prl, h.d_coefE, h.d_coefP,
+      excl(h), ewald_coef(h, h.prm.ewald_alpha), h.scales, h.d_cphi, h.d_polar,
+      h.prm.polarization != FFXG_POLAR_NONE ? 1 : 0, h.d_fieldD, h.d_fieldP, h.d_uD, h.d_uP, h.d_udirD, h.d_udirP,
+      h.d_flags);
+  FFX_LAUNCHED(h);
+}
+
+EwaldCoef ewald_coef_public(const Handle &h) { return ewald_coef(h, h.prm.ewald_alpha); }
 
 void launch_permanent_field(Handle &h) {
   k_permanent_field<<<nblocks((int64_t)h.n * 32, 128), 128, 0, h.stream>>>(
