@@ -7,7 +7,10 @@ polarization solved by PCG to 1e-6 D RMS + torques) of 8,000 AMOEBA waters in a
 shard (a 24k-atom PME evaluation is latency-bound on one GPU), so N GPUs run N
 independent replicas: value = N * steps / (max over ranks of the timed seconds).
 
-  python bench.py [--gpus N] [--steps K] [--warmup W] [--precision fp64|mixed]
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--precision both|fp64|mixed]
+
+By default both forms run; the headline value is the mixed-precision form and the
+plain FP64 form is reported beside it under "fp64".
   python bench.py --impl reference ...   # the CPU FP64 restatement on the host cores
 """
 from __future__ import annotations
@@ -99,13 +102,14 @@ class ClockSampler:
 
 
 # ---------------------------------------------------------------------------
-def algorithmic_traffic(stage: str, n: int, pairs_half: int, vdw_list_full: int) -> float:
+def algorithmic_traffic(stage: str, n: int, pairs_half: int, vdw_list_full: int, mixed: bool) -> float:
     """Compulsory HBM bytes of one launch of a stage's kernel: every input read once,
-    every output written once (list entries 4 B, FP64 per-atom data)."""
+    every output written once (list entries 4 B, FP64 per-atom data; the mixed form
+    caches the pair coefficients in FP32)."""
     full = 2 * pairs_half
-    if stage == "ind_field":      # per entry: index 4 B + coefficients (A, B) 16 B; per atom:
+    if stage == "ind_field":      # per entry: index 4 B + coefficients (A, B) 16 B (8 B mixed); per atom:
         # x,y,z, p(3), pP(3), phi(2x3), polarizability, r(3), rP(3), z(3), zP(3) in; vec(6) out; count
-        return 20.0 * full + n * (4 + 8 * (3 + 6 + 6 + 1 + 12) + 8 * 6)
+        return (12.0 if mixed else 20.0) * full + n * (4 + 8 * (3 + 6 + 6 + 1 + 12) + 8 * 6)
     if stage == "real_energy":    # list + x,y,z,gm(10),u,p,ipdamp,thole in; e(2),count,grad,torque out
         return 4.0 * full + n * (4 + 8 * (3 + 10 + 6 + 2) + 8 * 2 + 8 + 8 * 6)
     if stage == "vdw":
@@ -113,24 +117,13 @@ def algorithmic_traffic(stage: str, n: int, pairs_half: int, vdw_list_full: int)
     return float("nan")
 
 
-def run_mine(args):
+def measure(args, precision, system, dist, world, local):
+    """Device-resident timing of one precision form, plus the end-to-end host-buffer run."""
     import torch
-
-    rank = int(os.environ.get("RANK", "0"))
-    world = int(os.environ.get("WORLD_SIZE", "1"))
-    local = int(os.environ.get("LOCAL_RANK", "0"))
-    torch.cuda.set_device(local)
-    dist = None
-    if world > 1:
-        import datetime
-        import torch.distributed as dist
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
-
     from forcefieldx_b200.energy import ForceFieldEnergy
     from forcefieldx_b200 import cabi
 
-    precision = PRECISION_MIXED if args.precision == "mixed" else PRECISION_FP64
-    system = build_system()
+    mixed = precision == PRECISION_MIXED
     params = build_params(precision)
     n = system.n_atoms
     ffe = ForceFieldEnergy(system, params)
@@ -144,7 +137,7 @@ def run_mine(args):
     torch.cuda.synchronize()
     scf = ffe.count("scf_iter")
     pairs_half = ffe.count("permanent") - n
-    e_ref = float(ffe.terms[9])
+    terms = [float(t) for t in ffe.terms]
 
     sampler = ClockSampler(local)
     sampler.start()
@@ -179,21 +172,18 @@ def run_mine(args):
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         t_max = float(t.item())
     value = world * args.steps / (t_max / 1000.0)
-    ms_per_step = t_max / args.steps
 
     # Dominant stage and its roofline (algorithmic bytes / measured average launch time).
     kernel_stages = ["vdw", "ind_field", "real_energy"]
     per_stage = {cabi.STAGE_NAMES[i]: {"ms_total": float(stage_ms[i]), "launches": int(stage_n[i])}
                  for i in range(12)}
-    dom = max(kernel_stages, key=lambda s: per_stage[s]["ms_total"])
+    dom = max(kernel_stages, key=lambda st: per_stage[st]["ms_total"])
     avg_ms = per_stage[dom]["ms_total"] / max(1, per_stage[dom]["launches"])
-    import json as _json
     peaks_path = os.path.join(ROOT, "MEASURED_PEAKS.json")
     peak, peak_src = 6650.0, "fallback"
     if os.path.exists(peaks_path):
-        peak, peak_src = float(_json.load(open(peaks_path))["hbm_gbs"]), "measured"
-    vdw_full = 2 * ffe.count("vdw")
-    traffic_alg = algorithmic_traffic(dom, n, pairs_half, vdw_full)
+        peak, peak_src = float(json.load(open(peaks_path))["hbm_gbs"]), "measured"
+    traffic_alg = algorithmic_traffic(dom, n, pairs_half, 2 * ffe.count("vdw"), mixed)
     achieved = traffic_alg / (avg_ms * 1e-3) / 1e9
 
     # End to end through the public API with host buffers (H2D coordinates, D2H gradient).
@@ -214,30 +204,71 @@ def run_mine(args):
     e2e = {"value": world * e2e_steps / e2e_s, "unit": UNIT, "h2d_bytes_per_step": int(n * 3 * 8),
            "d2h_bytes_per_step": int(n * 3 * 8 + 8 * cabi.N_TERMS + 8 * cabi.N_COUNTS),
            "api": "ffxg_energy_and_gradient (host xyz in, host gradient out)"}
-
-    cpu = None
-    if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        cpu = cpu_baseline(system, params, samples=args.cpu_samples)
-
-    result = {
-        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
-        "warmup": args.warmup, "ms_per_step": ms_per_step, "higher_is_better": True, "scaling": "weak",
-        "vs_baseline": None, "dtype": "f64" if precision == PRECISION_FP64 else "f32 pair math + f64 accumulation",
-        "data": "synthetic (seeded AMOEBA water box)",
-        "config": {"workload": WORKLOAD, "atoms": n, "precision": args.precision, "pcg_iterations": scf,
-                   "energy_kcal_mol": e_ref, "parallelism": f"replicas x{world}",
-                   "l2": "flushed between steps (256 MB write, untimed)", "ns_per_day_2fs": value / world * 2e-6 * 86400},
+    ffe.close()
+    del flush
+    return {
+        "value": value, "ms_per_step": t_max / args.steps, "pcg_iterations": scf, "terms": terms,
+        "launches": int(launches), "clocks": clocks, "e2e": e2e,
+        "stages_ms_per_step": {k: v["ms_total"] / args.steps for k, v in per_stage.items()},
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                      "frac": achieved / peak, "traffic": None, "kernel_stage": dom,
                      "algorithmic_bytes_per_launch": traffic_alg, "avg_launch_ms": avg_ms,
                      "peak_source": peak_src,
-                     "note": "FP64 pair kernels are bound by the FP64 pipe, not HBM; see profiles/"},
-        "stages_ms_per_step": {k: v["ms_total"] / args.steps for k, v in per_stage.items()},
-        "e2e": e2e, "gpu_launches": int(launches), "clocks": clocks,
+                     "note": "pair kernels are bound by FP issue and gather latency, not HBM; see profiles/"},
     }
+
+
+def run_mine(args):
+    import torch
+
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+
+    system = build_system()
+    n = system.n_atoms
+    forms = {"fp64": PRECISION_FP64, "mixed": PRECISION_MIXED}
+    order = ["fp64", "mixed"] if args.precision == "both" else [args.precision]
+    runs = {name: measure(args, forms[name], system, dist, world, local) for name in order}
+    head_name = order[-1]
+    head = runs[head_name]
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        cpu = cpu_baseline(system, build_params(PRECISION_FP64), samples=args.cpu_samples)
+
+    dtype = "f64" if head_name == "fp64" else "mixed: f32 pair/mesh/FFT math, f64 + 64-bit fixed-point accumulation"
+    result = {
+        "metric": METRIC, "value": head["value"], "unit": UNIT, "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": head["ms_per_step"], "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": dtype, "data": "synthetic (seeded AMOEBA water box)",
+        "config": {"workload": WORKLOAD, "atoms": n, "precision": head_name,
+                   "pcg_iterations": head["pcg_iterations"], "energy_kcal_mol": head["terms"][9],
+                   "parallelism": f"replicas x{world}", "l2": "flushed between steps (256 MB write, untimed)",
+                   "ns_per_day_2fs": head["value"] / world * 2e-6 * 86400},
+        "roofline": head["roofline"],
+        "stages_ms_per_step": head["stages_ms_per_step"],
+        "e2e": head["e2e"], "gpu_launches": head["launches"], "clocks": head["clocks"],
+    }
+    if "fp64" in runs and head_name != "fp64":
+        f = runs["fp64"]
+        ref_terms = np.array(f["terms"])
+        result["fp64"] = {"value": f["value"], "ms_per_step": f["ms_per_step"], "e2e": f["e2e"]["value"],
+                          "pcg_iterations": f["pcg_iterations"], "roofline_frac": f["roofline"]["frac"],
+                          "stages_ms_per_step": f["stages_ms_per_step"], "clocks": f["clocks"],
+                          "gpu_launches": f["launches"]}
+        result["mixed_over_fp64"] = head["value"] / f["value"]
+        result["mixed_energy_error_vs_fp64_gpu"] = {
+            "total_rel": abs(head["terms"][9] - f["terms"][9]) / abs(f["terms"][9]),
+            "terms_abs": [abs(a - b) for a, b in zip(head["terms"], ref_terms)]}
     if cpu:
         result["cpu_baseline"] = cpu
-    ffe.close()
     if dist:
         dist.barrier()
         dist.destroy_process_group()
@@ -292,7 +323,7 @@ def main():
     ap.add_argument("--steps", type=int, default=20)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="mine", choices=["mine", "reference"])
-    ap.add_argument("--precision", default="fp64", choices=["fp64", "mixed"])
+    ap.add_argument("--precision", default="both", choices=["both", "fp64", "mixed"])
     ap.add_argument("--cpu-samples", type=int, default=2)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     args = ap.parse_args()

@@ -70,6 +70,24 @@ __device__ __forceinline__ double image_exact(double &x, double &y, double &z, c
   return __dadd_rn(__dadd_rn(__dmul_rn(x, x), __dmul_rn(y, y)), __dmul_rn(z, z));
 }
 
+// Arithmetic of the two precision forms.  Pair kernels are templates on the pair-math
+// type R: double for the plain FP64 form, float for the mixed form (displacements,
+// list tests, reductions and accumulators stay FP64 in both).
+template <typename R> struct Vec2;
+template <> struct Vec2<double> { using type = double2; };
+template <> struct Vec2<float> { using type = float2; };
+template <typename R> __device__ __forceinline__ typename Vec2<R>::type mk2(R a, R b);
+template <> __device__ __forceinline__ double2 mk2<double>(double a, double b) { return make_double2(a, b); }
+template <> __device__ __forceinline__ float2 mk2<float>(float a, float b) { return make_float2(a, b); }
+__device__ __forceinline__ double m_sqrt(double v) { return sqrt(v); }
+__device__ __forceinline__ float m_sqrt(float v) { return sqrtf(v); }
+__device__ __forceinline__ double m_exp(double v) { return exp(v); }
+__device__ __forceinline__ float m_exp(float v) { return expf(v); }
+__device__ __forceinline__ double m_erfc(double v) { return erfc(v); }
+__device__ __forceinline__ float m_erfc(float v) { return erfcf(v); }
+__device__ __forceinline__ double m_min(double a, double b) { return fmin(a, b); }
+__device__ __forceinline__ float m_min(float a, float b) { return fminf(a, b); }
+
 template <typename T>
 __device__ __forceinline__ T warp_sum(T v) {
 #pragma unroll
@@ -101,6 +119,7 @@ struct Handle {
   // ---- configuration
   int n = 0;
   ffxg_params prm{};
+  bool mixed = false;            // FFXG_PRECISION_MIXED: FP32 pair math, B-splines, mesh and FFT
   Box box{};
   int device = 0;
   cudaStream_t stream = nullptr;
@@ -159,6 +178,11 @@ struct Handle {
   double2 *d_grid = nullptr;
   double *d_influence = nullptr;
   double2 *d_twiddle = nullptr;               // per-axis twiddle tables (3 x max n)
+  // Mixed form: d_grid and d_spl hold float2 / float data; spreading accumulates in
+  // the 64-bit fixed-point mesh d_gridq [points][2].
+  unsigned long long *d_gridq = nullptr;
+  float *d_influencef = nullptr;
+  float2 *d_twiddlef = nullptr;
   PmeConst pc{};
   FftAxis axes[3]{};
 
@@ -189,7 +213,6 @@ struct Handle {
 // ---- kernels / launchers (defined in the .cu files)
 void launch_set_coordinates(Handle &h, const double *d_xyz);
 void launch_neighbor_list(Handle &h, bool force);
-void launch_realspace_lists(Handle &h);
 void launch_vdw(Handle &h, bool grad);
 void launch_rotate(Handle &h);
 void launch_bsplines(Handle &h);
@@ -198,12 +221,8 @@ void launch_spread_induced(Handle &h, const double *ud, const double *up);
 void launch_fft_convolution(Handle &h);
 void launch_phi_permanent(Handle &h);
 void launch_phi_induced(Handle &h, bool full);
-void launch_permanent_field(Handle &h);
 void launch_realspace_field(Handle &h);
-void launch_direct(Handle &h);
 void launch_induced_recip(Handle &h, const double *ud, const double *up);
-void launch_induced_real(Handle &h, const double *ud, const double *up, double *outD, double *outP);
-void launch_precond_field(Handle &h, const double *rD, const double *rP, double *outD, double *outP);
 int run_pcg(Handle &h);
 void launch_recip_energy(Handle &h, bool grad);
 void launch_real_energy(Handle &h, bool grad);

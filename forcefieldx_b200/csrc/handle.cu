@@ -89,6 +89,7 @@ static int create_impl(const ffxg_system *s, const ffxg_params *p, Handle &h) {
   if (p->precision != FFXG_PRECISION_FP64 && p->precision != FFXG_PRECISION_MIXED) {
     h.err = "unknown precision"; return FFXG_ERR_BAD_ARG;
   }
+  h.mixed = (p->precision == FFXG_PRECISION_MIXED);
   if (p->polarization < FFXG_POLAR_NONE || p->polarization > FFXG_POLAR_MUTUAL) {
     h.err = "unknown polarization"; return FFXG_ERR_BAD_ARG;
   }
@@ -227,6 +228,12 @@ static int create_impl(const ffxg_system *s, const ffxg_params *p, Handle &h) {
   const size_t ng = (size_t)nfx * nfy * nfz;
   CK(dalloc(&h.d_grid, ng)); CK(dalloc(&h.d_influence, ng));
   CK(dalloc(&h.d_twiddle, 3 * (size_t)std::max(nfx, std::max(nfy, nfz))));
+  if (h.mixed) {
+    CK(dalloc(&h.d_gridq, 2 * ng));
+    CK(cudaMemset(h.d_gridq, 0, 2 * ng * sizeof(unsigned long long)));
+    CK(dalloc(&h.d_influencef, ng));
+    CK(dalloc(&h.d_twiddlef, 3 * (size_t)std::max(nfx, std::max(nfy, nfz))));
+  }
   CK(dalloc(&h.d_grad, 3 * N)); CK(dalloc(&h.d_torque, 3 * N)); CK(dalloc(&h.d_gred, 6 * N));
   CK(dalloc(&h.d_eatom, 8 * N)); CK(dalloc(&h.d_catom, 2 * N));
   CK(dalloc(&h.d_result, 16)); CK(dalloc(&h.d_cresult, 8));
@@ -300,7 +307,7 @@ static void free_all(Handle &h) {
                   h.d_nbr_cnt, h.d_ewl, h.d_ewl_cnt, h.d_prl, h.d_prl_cnt, h.d_gm, h.d_fm, h.d_spl, h.d_igrid,
                   h.d_cphi, h.d_fphi, h.d_cphiI, h.d_fphiI, h.d_cphiP, h.d_fphiP, h.d_fieldD, h.d_fieldP, h.d_uD,
                   h.d_uP, h.d_udirD, h.d_udirP, h.d_r, h.d_rP, h.d_zpre, h.d_zpreP, h.d_p, h.d_pP, h.d_vec, h.d_vecP,
-                  h.d_partials, h.d_scalars, h.d_grid, h.d_influence, h.d_twiddle, h.d_grad, h.d_torque, h.d_gred,
+                  h.d_partials, h.d_scalars, h.d_grid, h.d_influence, h.d_twiddle, h.d_gridq, h.d_influencef, h.d_twiddlef, h.d_grad, h.d_torque, h.d_gred,
                   h.d_eatom, h.d_catom, h.d_result, h.d_cresult, h.d_flags, h.d_xyz_in, h.d_grad_out,
                   h.d_coefE, h.d_coefP, h.d_part2, h.d_counter};
   for (void *q : ptrs)

@@ -202,53 +202,6 @@ __global__ void k_list_done(int n, double *refx, double *refy, double *refz, con
   refx[i] = rx[i]; refy[i] = ry[i]; refz[i] = rz[i];
 }
 
-// Real-space (Ewald) and preconditioner sub-lists on the actual coordinates, as
-// PermanentRealSpaceFieldLoop derives them (pme/PermanentFieldRegion.java:669-717).
-__global__ void k_realspace_lists(int n, const double *__restrict__ x, const double *__restrict__ y,
-                                  const double *__restrict__ z, Box bx, const int *__restrict__ nbr,
-                                  const int *__restrict__ nbr_cnt, int cap, double off2, double pcut,
-                                  int *ewl, int *ewl_cnt, int capE, int *prl, int *prl_cnt, int capP, int *flags) {
-  const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-  const int lane = threadIdx.x & 31;
-  if (warp >= n) return;
-  const int i = warp;
-  const double xi = x[i], yi = y[i], zi = z[i];
-  const int cnt = min(nbr_cnt[i], cap);
-  const int *row = nbr + (size_t)i * cap;
-  int ce = 0, cp = 0;
-  for (int base = 0; base < cnt; base += 32) {
-    const int a = base + lane;
-    bool ew = false, pr = false;
-    int k = -1;
-    if (a < cnt) {
-      k = row[a];
-      double dx = __dsub_rn(x[k], xi), dy = __dsub_rn(y[k], yi), dz = __dsub_rn(z[k], zi);
-      const double r2 = image_exact(dx, dy, dz, bx);
-      ew = r2 <= off2;
-      pr = ew && (sqrt(r2) < pcut);
-    }
-    const unsigned me = __ballot_sync(0xffffffffu, ew);
-    const unsigned mp = __ballot_sync(0xffffffffu, pr);
-    const unsigned lt = (1u << lane) - 1u;
-    if (ew) {
-      const int pos = ce + __popc(me & lt);
-      if (pos < capE) ewl[(size_t)i * capE + pos] = k;
-    }
-    if (pr) {
-      const int pos = cp + __popc(mp & lt);
-      if (pos < capP) prl[(size_t)i * capP + pos] = k;
-    }
-    ce += __popc(me);
-    cp += __popc(mp);
-  }
-  if (lane == 0) {
-    ewl_cnt[i] = ce;
-    prl_cnt[i] = cp;
-    if (ce > capE) atomicOr(flags, FLAG_EWALD_OVERFLOW);
-    if (cp > capP) atomicOr(flags, FLAG_PRECOND_OVERFLOW);
-  }
-}
-
 // ---------------------------------------------------------------------------
 void launch_set_coordinates(Handle &h, const double *d_xyz) {
   const int n = h.n;
@@ -298,15 +251,6 @@ void launch_neighbor_list(Handle &h, bool force) {
   k_list_done<<<nblocks(n, 256), 256, 0, h.stream>>>(n, h.d_refx, h.d_refy, h.d_refz, h.d_rx, h.d_ry, h.d_rz,
                                                       h.d_flags);
   h.launches += 6;
-}
-
-void launch_realspace_lists(Handle &h) {
-  const int n = h.n;
-  const double off2 = h.prm.ewald_cutoff * h.prm.ewald_cutoff;
-  k_realspace_lists<<<nblocks((int64_t)n * 32, 256), 256, 0, h.stream>>>(
-      n, h.d_x, h.d_y, h.d_z, h.box, h.d_nbr, h.d_nbr_cnt, h.cap_nbr, off2, h.prm.precond_cutoff, h.d_ewl,
-      h.d_ewl_cnt, h.cap_ewl, h.d_prl, h.d_prl_cnt, h.cap_prl, h.d_flags);
-  FFX_LAUNCHED(h);
 }
 
 }  // namespace ffx

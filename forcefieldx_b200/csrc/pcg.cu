@@ -54,11 +54,13 @@ __device__ __forceinline__ void block_store(const double *v, double *part, int c
   }
 }
 
-// Dipole field at atom i from the cached coefficient row (warp cooperative).
+// Dipole field at atom i from the cached coefficient row (warp cooperative).  C2 is
+// double2 (plain form) or float2 (mixed form: FP32 coefficients, FP64 accumulation).
+template <typename C2>
 __device__ __forceinline__ void coef_field(int i, int n, const double *__restrict__ x, const double *__restrict__ y,
                                            const double *__restrict__ z, const Box &bx, const int *__restrict__ lst,
                                            const int *__restrict__ lst_cnt, int cap,
-                                           const double2 *__restrict__ coef, const double *__restrict__ ud,
+                                           const C2 *__restrict__ coef, const double *__restrict__ ud,
                                            const double *__restrict__ up, const double *__restrict__ scale_by,
                                            double *f) {
   const int lane = threadIdx.x & 31;
@@ -66,10 +68,11 @@ __device__ __forceinline__ void coef_field(int i, int n, const double *__restric
   double fx = 0, fy = 0, fz = 0, px = 0, py = 0, pz = 0;
   const int cnt = min(lst_cnt[i], cap);
   const int *row = lst + (size_t)i * cap;
-  const double2 *crow = coef + (size_t)i * cap;
+  const C2 *crow = coef + (size_t)i * cap;
   for (int a = lane; a < cnt; a += 32) {
     const int k = row[a];
-    const double2 c = crow[a];
+    const C2 cc = crow[a];
+    const double2 c = make_double2((double)cc.x, (double)cc.y);
     double xr = __dsub_rn(x[k], xi), yr = __dsub_rn(y[k], yi), zr = __dsub_rn(z[k], zi);
     image_exact(xr, yr, zr, bx);
     const double sk = scale_by ? scale_by[k] : 1.0;
@@ -87,10 +90,10 @@ __device__ __forceinline__ void coef_field(int i, int n, const double *__restric
 // MODE 0: field of (ud, up) into outD/outP (used for the final field of the solution).
 // MODE 1: initial residual r = (u_dir - u) / alpha + E(u) with u == u_dir (InitResidualRegion).
 // MODE 2: vec = p / alpha - E(p) and partials of p . vec and r . z (UpdateApLoop).
-template <int MODE>
+template <int MODE, typename C2>
 __global__ void __launch_bounds__(kFieldThreads) k_pcg_field(
     int n, const double *__restrict__ x, const double *__restrict__ y, const double *__restrict__ z, Box bx,
-    const int *__restrict__ ewl, const int *__restrict__ ewl_cnt, int capE, const double2 *__restrict__ coefE,
+    const int *__restrict__ ewl, const int *__restrict__ ewl_cnt, int capE, const C2 *__restrict__ coefE,
     const double *__restrict__ ud, const double *__restrict__ up, const double *__restrict__ cphiD,
     const double *__restrict__ cphiP, double aewald3, const double *__restrict__ polar,
     const double *__restrict__ udirD, const double *__restrict__ udirP, const double *__restrict__ r,
@@ -136,10 +139,10 @@ __global__ void __launch_bounds__(kFieldThreads) k_pcg_field(
 
 // z = alpha (E_precond(alpha r) + s r) (InitConjugateRegion / UpdatePreconditionerLoop);
 // INIT also sets p = z, otherwise the partials of r . z_new are stored.
-template <bool INIT>
+template <bool INIT, typename C2>
 __global__ void __launch_bounds__(kFieldThreads) k_pcg_precond(
     int n, const double *__restrict__ x, const double *__restrict__ y, const double *__restrict__ z, Box bx,
-    const int *__restrict__ prl, const int *__restrict__ prl_cnt, int capP, const double2 *__restrict__ coefP,
+    const int *__restrict__ prl, const int *__restrict__ prl_cnt, int capP, const C2 *__restrict__ coefP,
     const double *__restrict__ polar, const double *__restrict__ r, const double *__restrict__ rP, double s,
     double *zz, double *zP, double *p, double *pP, double *part) {
   const int lane = threadIdx.x & 31;
@@ -248,20 +251,31 @@ static double aewald3_of(const Handle &h) {
   return 4.0 / 3.0 * pow(a, 3.0) / 1.7724538509055160273;
 }
 
+template <int MODE, typename C2>
+static void field(Handle &h, const double *ud, const double *up, double *outD, double *outP) {
+  k_pcg_field<MODE, C2><<<kFieldBlocks, kFieldThreads, 0, h.stream>>>(
+      h.n, h.d_x, h.d_y, h.d_z, h.box, h.d_ewl, h.d_ewl_cnt, h.cap_ewl, reinterpret_cast<const C2 *>(h.d_coefE), ud,
+      up, h.d_cphiI, h.d_cphiP, aewald3_of(h), h.d_polar, h.d_udirD, h.d_udirP, h.d_r, h.d_rP, h.d_zpre, h.d_zpreP,
+      outD, outP, h.d_part2);
+  FFX_LAUNCHED(h);
+}
+
 template <int MODE>
 static void launch_field(Handle &h, const double *ud, const double *up, double *outD, double *outP) {
-  k_pcg_field<MODE><<<kFieldBlocks, kFieldThreads, 0, h.stream>>>(
-      h.n, h.d_x, h.d_y, h.d_z, h.box, h.d_ewl, h.d_ewl_cnt, h.cap_ewl, h.d_coefE, ud, up, h.d_cphiI, h.d_cphiP,
-      aewald3_of(h), h.d_polar, h.d_udirD, h.d_udirP, h.d_r, h.d_rP, h.d_zpre, h.d_zpreP, outD, outP, h.d_part2);
+  if (h.mixed) field<MODE, float2>(h, ud, up, outD, outP); else field<MODE, double2>(h, ud, up, outD, outP);
+}
+
+template <bool INIT, typename C2>
+static void precond(Handle &h) {
+  k_pcg_precond<INIT, C2><<<kFieldBlocks, kFieldThreads, 0, h.stream>>>(
+      h.n, h.d_x, h.d_y, h.d_z, h.box, h.d_prl, h.d_prl_cnt, h.cap_prl, reinterpret_cast<const C2 *>(h.d_coefP),
+      h.d_polar, h.d_r, h.d_rP, h.prm.precond_scale, h.d_zpre, h.d_zpreP, h.d_p, h.d_pP, h.d_part2);
   FFX_LAUNCHED(h);
 }
 
 template <bool INIT>
 static void launch_precond(Handle &h) {
-  k_pcg_precond<INIT><<<kFieldBlocks, kFieldThreads, 0, h.stream>>>(
-      h.n, h.d_x, h.d_y, h.d_z, h.box, h.d_prl, h.d_prl_cnt, h.cap_prl, h.d_coefP, h.d_polar, h.d_r, h.d_rP,
-      h.prm.precond_scale, h.d_zpre, h.d_zpreP, h.d_p, h.d_pP, h.d_part2);
-  FFX_LAUNCHED(h);
+  if (h.mixed) precond<INIT, float2>(h); else precond<INIT, double2>(h);
 }
 
 int run_pcg(Handle &h) {

@@ -114,29 +114,31 @@ __global__ void k_rotate(int n, const double *__restrict__ x, const double *__re
 }
 
 // ---------------------------------------------------------------------------
-// Order-5 B-spline values and three derivatives (UniformBSpline.bSplineDerivatives).
-__device__ __forceinline__ void bspline5(double x, double *out /* [5][4] */) {
-  double w[5][6];
+// Order-5 B-spline values and three derivatives (UniformBSpline.bSplineDerivatives),
+// in the mesh precision S.
+template <typename S>
+__device__ __forceinline__ void bspline5(S x, S *out /* [5][4] */) {
+  S w[5][6];
 #pragma unroll
   for (int a = 0; a < 5; a++)
 #pragma unroll
-    for (int b = 0; b < 6; b++) w[a][b] = 0.0;
-  w[1][0] = 1.0 - x;
+    for (int b = 0; b < 6; b++) w[a][b] = S(0);
+  w[1][0] = S(1) - x;
   w[1][1] = x;
-  w[2][0] = 0.5 * (1.0 - x) * w[1][0];
-  w[2][1] = 0.5 * ((x + 1.0) * w[1][0] + (2.0 - x) * w[1][1]);
-  w[2][2] = 0.5 * x * w[1][1];
+  w[2][0] = S(0.5) * (S(1) - x) * w[1][0];
+  w[2][1] = S(0.5) * ((x + S(1)) * w[1][0] + (S(2) - x) * w[1][1]);
+  w[2][2] = S(0.5) * x * w[1][1];
 #pragma unroll
   for (int k = 3; k < 5; k++) {
-    const double div = 1.0 / (double)k;
-    const double k1mw = k + (1.0 - x);
+    const S div = S(1) / (S)k;
+    const S k1mw = (S)k + (S(1) - x);
     w[k][k] = div * x * w[k - 1][k - 1];
 #pragma unroll
-    for (int i = 1; i < k; i++) w[k][k - i] = div * ((x + (double)i) * w[k - 1][k - 1 - i] + (k1mw - (double)i) * w[k - 1][k - i]);
-    w[k][0] = div * (1.0 - x) * w[k - 1][0];
+    for (int i = 1; i < k; i++) w[k][k - i] = div * ((x + (S)i) * w[k - 1][k - 1 - i] + (k1mw - (S)i) * w[k - 1][k - i]);
+    w[k][0] = div * (S(1) - x) * w[k - 1][0];
   }
   // bSplineDiff(work[o2], o1); (work[o3], o2), (o3, o1); (o4, o3), (o4, o2), (o4, o1) with order 5.
-  auto diff = [](double *c, int order) {
+  auto diff = [](S *c, int order) {
     const int o1 = order - 1;
     c[order] = c[o1];
     for (int i = o1; i > 0; i--) c[i] = c[i - 1] - c[i];
@@ -151,9 +153,10 @@ __device__ __forceinline__ void bspline5(double x, double *out /* [5][4] */) {
     for (int j = 0; j < 4; j++) out[k * 4 + j] = w[4 - j][k];
 }
 
+template <typename S>
 __global__ void k_bsplines(int n, const double *__restrict__ x, const double *__restrict__ y,
                            const double *__restrict__ z, const double *__restrict__ gm, int nfx, int nfy, int nfz,
-                           double *spl, int *igrid, double *fm, PmeConst pc) {
+                           S *spl, int *igrid, double *fm, PmeConst pc) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
   const double xi = x[i], yi = y[i], zi = z[i];
@@ -167,7 +170,7 @@ __global__ void k_bsplines(int n, const double *__restrict__ x, const double *__
     const double fr = nf[d] * u;
     const int ifr = (int)fr;
     igrid[d * n + i] = ifr - kOrder;
-    bspline5(fr - ifr, spl + ((size_t)i * 3 + d) * kOrder * 4);
+    bspline5<S>((S)(fr - ifr), spl + ((size_t)i * 3 + d) * kOrder * 4);
   }
   double g[10];
 #pragma unroll
@@ -196,65 +199,92 @@ __device__ __forceinline__ int jmod(int a, int m) {
   return r < 0 ? r + m : r;
 }
 
+// Mesh accumulation.  Plain form: FP64 atomics into the complex double mesh.  Mixed
+// form: 64-bit fixed-point integer atomics (2^32 units per unit of density) into a
+// separate accumulation mesh [points][2]; integer addition is associative, so the
+// accumulated mesh has the same bits whatever order the atoms arrive in.  The first
+// FFT pass converts it to FP32 and clears it for the next spread.
+constexpr float kMeshFix = 4294967296.0f;        // 2^32
+constexpr float kMeshUnfix = 2.3283064365386963e-10f;  // 2^-32
+
+__device__ __forceinline__ unsigned long long to_fix(float v) {
+  return (unsigned long long)__float2ll_rn(v * kMeshFix);
+}
+__device__ __forceinline__ void mesh_add(double2 *grid, unsigned long long *, size_t idx, double re) {
+  atomicAdd(&grid[idx].x, re);
+}
+__device__ __forceinline__ void mesh_add(double2 *, unsigned long long *gq, size_t idx, float re) {
+  atomicAdd(&gq[2 * idx], to_fix(re));
+}
+__device__ __forceinline__ void mesh_add(double2 *grid, unsigned long long *, size_t idx, double re, double im) {
+  atomicAdd(&grid[idx].x, re);
+  atomicAdd(&grid[idx].y, im);
+}
+__device__ __forceinline__ void mesh_add(double2 *, unsigned long long *gq, size_t idx, float re, float im) {
+  atomicAdd(&gq[2 * idx], to_fix(re));
+  atomicAdd(&gq[2 * idx + 1], to_fix(im));
+}
+
 // One warp per atom; lanes walk the 125 mesh points of the atom's support.
-__global__ void k_spread_permanent(int n, const double *__restrict__ fm, const double *__restrict__ spl,
-                                   const int *__restrict__ igrid, int nfx, int nfy, int nfz, double2 *grid) {
+template <typename S>
+__global__ void k_spread_permanent(int n, const double *__restrict__ fm, const S *__restrict__ spl,
+                                   const int *__restrict__ igrid, int nfx, int nfy, int nfz, double2 *grid,
+                                   unsigned long long *gq) {
   const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const int lane = threadIdx.x & 31;
   if (warp >= n) return;
   const int i = warp;
-  const double *s = spl + (size_t)i * 3 * kOrder * 4;
-  const double *sx = s, *sy = s + kOrder * 4, *sz = s + 2 * kOrder * 4;
+  const S *s = spl + (size_t)i * 3 * kOrder * 4;
+  const S *sx = s, *sy = s + kOrder * 4, *sz = s + 2 * kOrder * 4;
   const int i0 = igrid[i], j0 = igrid[n + i], k0 = igrid[2 * n + i];
-  double f[10];
+  S f[10];
 #pragma unroll
-  for (int j = 0; j < 10; j++) f[j] = fm[j * n + i];
+  for (int j = 0; j < 10; j++) f[j] = (S)fm[j * n + i];
   for (int p = lane; p < 125; p += 32) {
     const int a1 = p % 5, a2 = (p / 5) % 5, a3 = p / 25;
-    const double v0 = sz[a3 * 4], v1 = sz[a3 * 4 + 1], v2 = sz[a3 * 4 + 2];
-    const double u0 = sy[a2 * 4], u1 = sy[a2 * 4 + 1], u2 = sy[a2 * 4 + 2];
-    const double c0dz1qzz2 = f[t000] * v0 + f[t001] * v1 + f[t002] * v2;
-    const double dy0qyz1 = f[t010] * v0 + f[t011] * v1;
-    const double dx0qxz1 = f[t100] * v0 + f[t101] * v1;
-    const double term0 = fma(c0dz1qzz2, u0, fma(dy0qyz1, u1, f[t020] * v0 * u2));
-    const double term1 = fma(dx0qxz1, u0, f[t110] * v0 * u1);
-    const double term2 = f[t200] * v0 * u0;
-    const double val = fma(sx[a1 * 4], term0, fma(sx[a1 * 4 + 1], term1, sx[a1 * 4 + 2] * term2));
+    const S v0 = sz[a3 * 4], v1 = sz[a3 * 4 + 1], v2 = sz[a3 * 4 + 2];
+    const S u0 = sy[a2 * 4], u1 = sy[a2 * 4 + 1], u2 = sy[a2 * 4 + 2];
+    const S c0dz1qzz2 = f[t000] * v0 + f[t001] * v1 + f[t002] * v2;
+    const S dy0qyz1 = f[t010] * v0 + f[t011] * v1;
+    const S dx0qxz1 = f[t100] * v0 + f[t101] * v1;
+    const S term0 = fma(c0dz1qzz2, u0, fma(dy0qyz1, u1, f[t020] * v0 * u2));
+    const S term1 = fma(dx0qxz1, u0, f[t110] * v0 * u1);
+    const S term2 = f[t200] * v0 * u0;
+    const S val = fma(sx[a1 * 4], term0, fma(sx[a1 * 4 + 1], term1, sx[a1 * 4 + 2] * term2));
     const int ii = jmod(i0 + 1 + a1, nfx), jj = jmod(j0 + 1 + a2, nfy), kk = jmod(k0 + 1 + a3, nfz);
-    atomicAdd(&grid[((size_t)kk * nfy + jj) * nfx + ii].x, val);
+    mesh_add(grid, gq, ((size_t)kk * nfy + jj) * nfx + ii, val);
   }
 }
 
+template <typename S>
 __global__ void k_spread_induced(int n, const double *__restrict__ ud, const double *__restrict__ up,
-                                 const double *__restrict__ spl, const int *__restrict__ igrid, int nfx, int nfy,
-                                 int nfz, double2 *grid, PmeConst pc) {
+                                 const S *__restrict__ spl, const int *__restrict__ igrid, int nfx, int nfy,
+                                 int nfz, double2 *grid, unsigned long long *gq, PmeConst pc) {
   const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const int lane = threadIdx.x & 31;
   if (warp >= n) return;
   const int i = warp;
-  const double *s = spl + (size_t)i * 3 * kOrder * 4;
-  const double *sx = s, *sy = s + kOrder * 4, *sz = s + 2 * kOrder * 4;
+  const S *s = spl + (size_t)i * 3 * kOrder * 4;
+  const S *sx = s, *sy = s + kOrder * 4, *sz = s + 2 * kOrder * 4;
   const int i0 = igrid[i], j0 = igrid[n + i], k0 = igrid[2 * n + i];
-  double u[3], q[3];
+  S u[3], q[3];
   const double c[3] = {ud[i], ud[n + i], ud[2 * n + i]};
   const double cp[3] = {up[i], up[n + i], up[2 * n + i]};
 #pragma unroll
   for (int a = 0; a < 3; a++) {
-    u[a] = pc.afrac[a][0] * c[0] + pc.afrac[a][1] * c[1] + pc.afrac[a][2] * c[2];
-    q[a] = pc.afrac[a][0] * cp[0] + pc.afrac[a][1] * cp[1] + pc.afrac[a][2] * cp[2];
+    u[a] = (S)(pc.afrac[a][0] * c[0] + pc.afrac[a][1] * c[1] + pc.afrac[a][2] * c[2]);
+    q[a] = (S)(pc.afrac[a][0] * cp[0] + pc.afrac[a][1] * cp[1] + pc.afrac[a][2] * cp[2]);
   }
   for (int p = lane; p < 125; p += 32) {
     const int a1 = p % 5, a2 = (p / 5) % 5, a3 = p / 25;
-    const double v0 = sz[a3 * 4], v1 = sz[a3 * 4 + 1];
-    const double u0 = sy[a2 * 4], u1 = sy[a2 * 4 + 1];
-    const double t0 = fma(u[2] * v1, u0, u[1] * v0 * u1), t1 = u[0] * v0 * u0;
-    const double tp0 = fma(q[2] * v1, u0, q[1] * v0 * u1), tp1 = q[0] * v0 * u0;
-    const double re = fma(sx[a1 * 4], t0, sx[a1 * 4 + 1] * t1);
-    const double im = fma(sx[a1 * 4], tp0, sx[a1 * 4 + 1] * tp1);
+    const S v0 = sz[a3 * 4], v1 = sz[a3 * 4 + 1];
+    const S u0 = sy[a2 * 4], u1 = sy[a2 * 4 + 1];
+    const S t0 = fma(u[2] * v1, u0, u[1] * v0 * u1), t1 = u[0] * v0 * u0;
+    const S tp0 = fma(q[2] * v1, u0, q[1] * v0 * u1), tp1 = q[0] * v0 * u0;
+    const S re = fma(sx[a1 * 4], t0, sx[a1 * 4 + 1] * t1);
+    const S im = fma(sx[a1 * 4], tp0, sx[a1 * 4 + 1] * tp1);
     const int ii = jmod(i0 + 1 + a1, nfx), jj = jmod(j0 + 1 + a2, nfy), kk = jmod(k0 + 1 + a3, nfz);
-    double2 *g = &grid[((size_t)kk * nfy + jj) * nfx + ii];
-    atomicAdd(&g->x, re);
-    atomicAdd(&g->y, im);
+    mesh_add(grid, gq, ((size_t)kk * nfy + jj) * nfx + ii, re, im);
   }
 }
 
@@ -263,64 +293,70 @@ __global__ void k_spread_induced(int n, const double *__restrict__ ud, const dou
 // Stockham self-sorting mixed-radix passes (radices 4, 2, 3, 5, 7), ping-pong
 // between two shared buffers.  `tw` holds exp(-2*pi*i*j/len), j < len.
 
-__device__ __forceinline__ double2 cmul(double2 a, double2 b) {
-  return make_double2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
+template <typename V2>
+__device__ __forceinline__ V2 cmul(V2 a, V2 b) {
+  V2 r;
+  r.x = a.x * b.x - a.y * b.y;
+  r.y = a.x * b.y + a.y * b.x;
+  return r;
 }
 
 // Radix-R Stockham butterfly for one (line, j) pair.  R is a compile-time constant so
 // the R values stay in registers; the small DFTs of R = 2, 3, 4 use their closed
 // forms, R = 5 and 7 use the twiddle table.
-template <int R>
-__device__ __forceinline__ void fft_butterfly(const double2 *in, double2 *out, int j, int l, int L, int nb, int Ns,
-                                              int len, int sg, const double2 *__restrict__ tw) {
-  double2 v[R];
+template <int R, typename S>
+__device__ __forceinline__ void fft_butterfly(const typename Vec2<S>::type *in, typename Vec2<S>::type *out, int j,
+                                              int l, int L, int nb, int Ns, int len, int sg,
+                                              const typename Vec2<S>::type *__restrict__ tw) {
+  using V2 = typename Vec2<S>::type;
+  V2 v[R];
   const int k = j % Ns;
   const int tstep = len / (Ns * R);
 #pragma unroll
   for (int r = 0; r < R; r++) {
-    double2 a = in[(j + r * nb) * L + l];
+    V2 a = in[(j + r * nb) * L + l];
     if (r > 0 && k > 0) {
-      double2 w = tw[r * k * tstep];
+      V2 w = tw[r * k * tstep];
       if (sg > 0) w.y = -w.y;
       a = cmul(a, w);
     }
     v[r] = a;
   }
   const int idxD = (j / Ns) * Ns * R + k;
-  double2 y[R];
+  V2 y[R];
   if (R == 2) {
-    y[0] = make_double2(v[0].x + v[1].x, v[0].y + v[1].y);
-    y[1] = make_double2(v[0].x - v[1].x, v[0].y - v[1].y);
+    y[0] = mk2<S>(v[0].x + v[1].x, v[0].y + v[1].y);
+    y[1] = mk2<S>(v[0].x - v[1].x, v[0].y - v[1].y);
   } else if (R == 4) {
     // W4 = exp(sg * i * pi / 2) = sg * i.
-    const double2 s02 = make_double2(v[0].x + v[2].x, v[0].y + v[2].y);
-    const double2 d02 = make_double2(v[0].x - v[2].x, v[0].y - v[2].y);
-    const double2 s13 = make_double2(v[1].x + v[3].x, v[1].y + v[3].y);
-    const double2 d13 = make_double2(v[1].x - v[3].x, v[1].y - v[3].y);
+    const V2 s02 = mk2<S>(v[0].x + v[2].x, v[0].y + v[2].y);
+    const V2 d02 = mk2<S>(v[0].x - v[2].x, v[0].y - v[2].y);
+    const V2 s13 = mk2<S>(v[1].x + v[3].x, v[1].y + v[3].y);
+    const V2 d13 = mk2<S>(v[1].x - v[3].x, v[1].y - v[3].y);
     // i * d13 = (-d13.y, d13.x)
-    const double2 id13 = make_double2(-sg * d13.y, sg * d13.x);
-    y[0] = make_double2(s02.x + s13.x, s02.y + s13.y);
-    y[1] = make_double2(d02.x + id13.x, d02.y + id13.y);
-    y[2] = make_double2(s02.x - s13.x, s02.y - s13.y);
-    y[3] = make_double2(d02.x - id13.x, d02.y - id13.y);
+    const V2 id13 = mk2<S>((S)(-sg) * d13.y, (S)sg * d13.x);
+    y[0] = mk2<S>(s02.x + s13.x, s02.y + s13.y);
+    y[1] = mk2<S>(d02.x + id13.x, d02.y + id13.y);
+    y[2] = mk2<S>(s02.x - s13.x, s02.y - s13.y);
+    y[3] = mk2<S>(d02.x - id13.x, d02.y - id13.y);
   } else if (R == 3) {
-    const double c = -0.5, s = sg * 0.86602540378443864676;  // cos(2 pi / 3), sg * sin(2 pi / 3)
-    const double2 t = make_double2(v[1].x + v[2].x, v[1].y + v[2].y);
-    const double2 d = make_double2(v[1].x - v[2].x, v[1].y - v[2].y);
-    y[0] = make_double2(v[0].x + t.x, v[0].y + t.y);
-    const double2 m = make_double2(v[0].x + c * t.x, v[0].y + c * t.y);
-    y[1] = make_double2(m.x - s * d.y, m.y + s * d.x);
-    y[2] = make_double2(m.x + s * d.y, m.y - s * d.x);
+    const S c = S(-0.5), s = (S)sg * S(0.86602540378443864676);  // cos(2 pi / 3), sg * sin(2 pi / 3)
+    const V2 t = mk2<S>(v[1].x + v[2].x, v[1].y + v[2].y);
+    const V2 d = mk2<S>(v[1].x - v[2].x, v[1].y - v[2].y);
+    y[0] = mk2<S>(v[0].x + t.x, v[0].y + t.y);
+    const V2 m = mk2<S>(v[0].x + c * t.x, v[0].y + c * t.y);
+    y[1] = mk2<S>(m.x - s * d.y, m.y + s * d.x);
+    y[2] = mk2<S>(m.x + s * d.y, m.y - s * d.x);
   } else {
     const int wstep = len / R;
 #pragma unroll
     for (int q = 0; q < R; q++) {
-      double2 acc = v[0];
+      V2 acc = v[0];
 #pragma unroll
       for (int r = 1; r < R; r++) {
-        double2 w = tw[((r * q) % R) * wstep];
+        V2 w = tw[((r * q) % R) * wstep];
         if (sg > 0) w.y = -w.y;
-        const double2 m = cmul(v[r], w);
+        const V2 m = cmul(v[r], w);
         acc.x += m.x; acc.y += m.y;
       }
       y[q] = acc;
@@ -330,24 +366,37 @@ __device__ __forceinline__ void fft_butterfly(const double2 *in, double2 *out, i
   for (int q = 0; q < R; q++) out[(idxD + q * Ns) * L + l] = y[q];
 }
 
-template <bool FUSE_G>
-__global__ void __launch_bounds__(256) k_fft_axis(double2 *grid, FftAxis ax, int sign, const double2 *__restrict__ tw,
-                                                  const double *__restrict__ G, int gnx, int gny) {
+// FROMQ (mixed form, first pass only): the input is the 64-bit fixed-point
+// accumulation mesh, converted to FP32 on load and cleared for the next spread.
+template <bool FUSE_G, typename S, bool FROMQ>
+__global__ void __launch_bounds__(256) k_fft_axis(typename Vec2<S>::type *grid, FftAxis ax, int sign,
+                                                  const typename Vec2<S>::type *__restrict__ tw,
+                                                  const S *__restrict__ G, int gnx, int gny,
+                                                  unsigned long long *gq) {
+  using V2 = typename Vec2<S>::type;
   // Shared layout is element-major, line-minor: buf[j * L + l].  Consecutive threads
   // take consecutive lines, so butterflies are bank-conflict free and the Y and Z
   // passes (adjacent lines adjacent in memory) load and store coalesced.
-  extern __shared__ double2 sm[];
+  extern __shared__ __align__(16) unsigned char sm_raw[];
+  V2 *sm = reinterpret_cast<V2 *>(sm_raw);
   const int len = ax.len, L = ax.L;
-  double2 *buf0 = sm, *buf1 = sm + (size_t)len * L;
+  V2 *buf0 = sm, *buf1 = sm + (size_t)len * L;
   const int gi = blockIdx.x % ax.groups_inner, go = blockIdx.x / ax.groups_inner;
   const size_t base = (size_t)gi * ax.group_step_inner + (size_t)go * ax.group_step_outer;
   const bool contiguous = (ax.stride == 1);
   for (int t = threadIdx.x; t < len * L; t += blockDim.x) {
     const int l = contiguous ? t / len : t % L, j = contiguous ? t % len : t / L;
-    buf0[j * L + l] = grid[base + (size_t)l * ax.line_step + (size_t)j * ax.stride];
+    const size_t g = base + (size_t)l * ax.line_step + (size_t)j * ax.stride;
+    if (FROMQ) {
+      const longlong2 q = reinterpret_cast<const longlong2 *>(gq)[g];
+      reinterpret_cast<longlong2 *>(gq)[g] = make_longlong2(0, 0);
+      buf0[j * L + l] = mk2<S>((S)q.x * (S)kMeshUnfix, (S)q.y * (S)kMeshUnfix);
+    } else {
+      buf0[j * L + l] = grid[g];
+    }
   }
   __syncthreads();
-  double2 *in = buf0, *out = buf1;
+  V2 *in = buf0, *out = buf1;
   const int npass = FUSE_G ? 2 : 1;
   for (int pass = 0; pass < npass; pass++) {
     const int sg = (pass == 0) ? sign : -sign;
@@ -358,22 +407,22 @@ __global__ void __launch_bounds__(256) k_fft_axis(double2 *grid, FftAxis ax, int
       for (int t = threadIdx.x; t < nb * L; t += blockDim.x) {
         const int l = t % L, j = t / L;
         switch (R) {
-          case 4: fft_butterfly<4>(in, out, j, l, L, nb, Ns, len, sg, tw); break;
-          case 2: fft_butterfly<2>(in, out, j, l, L, nb, Ns, len, sg, tw); break;
-          case 3: fft_butterfly<3>(in, out, j, l, L, nb, Ns, len, sg, tw); break;
-          case 5: fft_butterfly<5>(in, out, j, l, L, nb, Ns, len, sg, tw); break;
-          default: fft_butterfly<7>(in, out, j, l, L, nb, Ns, len, sg, tw); break;
+          case 4: fft_butterfly<4, S>(in, out, j, l, L, nb, Ns, len, sg, tw); break;
+          case 2: fft_butterfly<2, S>(in, out, j, l, L, nb, Ns, len, sg, tw); break;
+          case 3: fft_butterfly<3, S>(in, out, j, l, L, nb, Ns, len, sg, tw); break;
+          case 5: fft_butterfly<5, S>(in, out, j, l, L, nb, Ns, len, sg, tw); break;
+          default: fft_butterfly<7, S>(in, out, j, l, L, nb, Ns, len, sg, tw); break;
         }
       }
       __syncthreads();
-      double2 *tmp = in; in = out; out = tmp;
+      V2 *tmp = in; in = out; out = tmp;
       Ns *= R;
     }
     if (FUSE_G && pass == 0) {
       // Influence function: lines run along z at fixed (x, y) = base + l (line_step 1).
       for (int t = threadIdx.x; t < len * L; t += blockDim.x) {
         const int l = t % L, j = t / L;
-        const double g = G[(size_t)j * gnx * gny + base + (size_t)l * ax.line_step];
+        const S g = G[(size_t)j * gnx * gny + base + (size_t)l * ax.line_step];
         in[j * L + l].x *= g;
         in[j * L + l].y *= g;
       }
@@ -388,26 +437,26 @@ __global__ void __launch_bounds__(256) k_fft_axis(double2 *grid, FftAxis ax, int
 
 // ---------------------------------------------------------------------------
 // Potential and derivatives at each atom (20 fractional terms -> Cartesian).
-template <int NT>
-__device__ __forceinline__ void interp(int i, int n, const double *__restrict__ spl, const int *__restrict__ igrid,
-                                       const double2 *__restrict__ grid, int nfx, int nfy, int nfz, bool imag,
-                                       double *tuv) {
-  const double *s = spl + (size_t)i * 3 * kOrder * 4;
-  const double *sx = s, *sy = s + kOrder * 4, *sz = s + 2 * kOrder * 4;
+template <int NT, typename S>
+__device__ __forceinline__ void interp(int i, int n, const S *__restrict__ spl, const int *__restrict__ igrid,
+                                       const typename Vec2<S>::type *__restrict__ grid, int nfx, int nfy, int nfz,
+                                       bool imag, S *tuv) {
+  const S *s = spl + (size_t)i * 3 * kOrder * 4;
+  const S *sx = s, *sy = s + kOrder * 4, *sz = s + 2 * kOrder * 4;
   const int i0 = igrid[i], j0 = igrid[n + i], k0 = igrid[2 * n + i];
 #pragma unroll
-  for (int t = 0; t < NT; t++) tuv[t] = 0.0;
+  for (int t = 0; t < NT; t++) tuv[t] = S(0);
   for (int a3 = 0; a3 < kOrder; a3++) {
     const int kk = jmod(k0 + 1 + a3, nfz);
-    double tu00 = 0, tu10 = 0, tu01 = 0, tu20 = 0, tu11 = 0, tu02 = 0, tu30 = 0, tu21 = 0, tu12 = 0, tu03 = 0;
+    S tu00 = 0, tu10 = 0, tu01 = 0, tu20 = 0, tu11 = 0, tu02 = 0, tu30 = 0, tu21 = 0, tu12 = 0, tu03 = 0;
     for (int a2 = 0; a2 < kOrder; a2++) {
       const int jj = jmod(j0 + 1 + a2, nfy);
-      double t0 = 0, t1 = 0, t2 = 0, t3 = 0;
+      S t0 = 0, t1 = 0, t2 = 0, t3 = 0;
 #pragma unroll
       for (int a1 = 0; a1 < kOrder; a1++) {
         const int ii = jmod(i0 + 1 + a1, nfx);
-        const double2 gv = grid[((size_t)kk * nfy + jj) * nfx + ii];
-        const double tq = imag ? gv.y : gv.x;
+        const auto gv = grid[((size_t)kk * nfy + jj) * nfx + ii];
+        const S tq = imag ? gv.y : gv.x;
         t0 = fma(tq, sx[a1 * 4], t0);
         t1 = fma(tq, sx[a1 * 4 + 1], t1);
         if (NT > 4) {
@@ -415,14 +464,14 @@ __device__ __forceinline__ void interp(int i, int n, const double *__restrict__ 
           t3 = fma(tq, sx[a1 * 4 + 3], t3);
         }
       }
-      const double u0 = sy[a2 * 4], u1 = sy[a2 * 4 + 1], u2 = sy[a2 * 4 + 2], u3 = sy[a2 * 4 + 3];
+      const S u0 = sy[a2 * 4], u1 = sy[a2 * 4 + 1], u2 = sy[a2 * 4 + 2], u3 = sy[a2 * 4 + 3];
       tu00 = fma(t0, u0, tu00); tu10 = fma(t1, u0, tu10); tu01 = fma(t0, u1, tu01);
       if (NT > 4) {
         tu20 = fma(t2, u0, tu20); tu11 = fma(t1, u1, tu11); tu02 = fma(t0, u2, tu02);
         tu30 = fma(t3, u0, tu30); tu21 = fma(t2, u1, tu21); tu12 = fma(t1, u2, tu12); tu03 = fma(t0, u3, tu03);
       }
     }
-    const double v0 = sz[a3 * 4], v1 = sz[a3 * 4 + 1], v2 = sz[a3 * 4 + 2], v3 = sz[a3 * 4 + 3];
+    const S v0 = sz[a3 * 4], v1 = sz[a3 * 4 + 1], v2 = sz[a3 * 4 + 2], v3 = sz[a3 * 4 + 3];
     tuv[t000] = fma(tu00, v0, tuv[t000]); tuv[t100] = fma(tu10, v0, tuv[t100]);
     tuv[t010] = fma(tu01, v0, tuv[t010]); tuv[t001] = fma(tu00, v1, tuv[t001]);
     if (NT > 4) {
@@ -464,50 +513,56 @@ __device__ __forceinline__ void store_phi(int i, int n, const double *tuv, doubl
   }
 }
 
-template <int NT>
-__global__ void k_phi(int n, const double *__restrict__ spl, const int *__restrict__ igrid,
-                      const double2 *__restrict__ grid, int nfx, int nfy, int nfz, double *fphiR, double *cphiR,
-                      double *fphiI, double *cphiI, PmeConst pc) {
+template <int NT, typename S>
+__global__ void k_phi(int n, const S *__restrict__ spl, const int *__restrict__ igrid,
+                      const typename Vec2<S>::type *__restrict__ grid, int nfx, int nfy, int nfz, double *fphiR,
+                      double *cphiR, double *fphiI, double *cphiI, PmeConst pc) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
-  double tuv[NT];
-  interp<NT>(i, n, spl, igrid, grid, nfx, nfy, nfz, false, tuv);
-  store_phi<NT>(i, n, tuv, fphiR, cphiR, pc);
+  S tuv[NT];
+  double td[NT];
+  interp<NT, S>(i, n, spl, igrid, grid, nfx, nfy, nfz, false, tuv);
+#pragma unroll
+  for (int t = 0; t < NT; t++) td[t] = (double)tuv[t];
+  store_phi<NT>(i, n, td, fphiR, cphiR, pc);
   if (cphiI) {
-    interp<NT>(i, n, spl, igrid, grid, nfx, nfy, nfz, true, tuv);
-    store_phi<NT>(i, n, tuv, fphiI, cphiI, pc);
+    interp<NT, S>(i, n, spl, igrid, grid, nfx, nfy, nfz, true, tuv);
+#pragma unroll
+    for (int t = 0; t < NT; t++) td[t] = (double)tuv[t];
+    store_phi<NT>(i, n, td, fphiI, cphiI, pc);
   }
 }
 
 // Field terms only (first derivatives of the Re and Im potentials), one warp per atom:
 // lanes walk the 125 support points, then the six partial sums reduce by shuffles.
 // Used inside the PCG loop, where only t100, t010, t001 of the induced potential are read.
-__global__ void k_phi_field(int n, const double *__restrict__ spl, const int *__restrict__ igrid,
-                            const double2 *__restrict__ grid, int nfx, int nfy, int nfz, PmeConst pc,
+template <typename S>
+__global__ void k_phi_field(int n, const S *__restrict__ spl, const int *__restrict__ igrid,
+                            const typename Vec2<S>::type *__restrict__ grid, int nfx, int nfy, int nfz, PmeConst pc,
                             double *cphiR, double *cphiI) {
   const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const int lane = threadIdx.x & 31;
   if (warp >= n) return;
   const int i = warp;
-  const double *sp = spl + (size_t)i * 3 * kOrder * 4;
-  const double *sx = sp, *sy = sp + kOrder * 4, *sz = sp + 2 * kOrder * 4;
+  const S *sp = spl + (size_t)i * 3 * kOrder * 4;
+  const S *sx = sp, *sy = sp + kOrder * 4, *sz = sp + 2 * kOrder * 4;
   const int i0 = igrid[i], j0 = igrid[n + i], k0 = igrid[2 * n + i];
-  double rx = 0, ry = 0, rz = 0, ix = 0, iy = 0, iz = 0;
+  S rx = 0, ry = 0, rz = 0, ix = 0, iy = 0, iz = 0;
   for (int p = lane; p < 125; p += 32) {
     const int a1 = p % 5, a2 = (p / 5) % 5, a3 = p / 25;
     const int ii = jmod(i0 + 1 + a1, nfx), jj = jmod(j0 + 1 + a2, nfy), kk = jmod(k0 + 1 + a3, nfz);
-    const double2 g = grid[((size_t)kk * nfy + jj) * nfx + ii];
-    const double x0 = sx[a1 * 4], x1 = sx[a1 * 4 + 1];
-    const double y0 = sy[a2 * 4], y1 = sy[a2 * 4 + 1];
-    const double z0 = sz[a3 * 4], z1 = sz[a3 * 4 + 1];
-    const double wx = x1 * y0 * z0, wy = x0 * y1 * z0, wz = x0 * y0 * z1;
+    const auto g = grid[((size_t)kk * nfy + jj) * nfx + ii];
+    const S x0 = sx[a1 * 4], x1 = sx[a1 * 4 + 1];
+    const S y0 = sy[a2 * 4], y1 = sy[a2 * 4 + 1];
+    const S z0 = sz[a3 * 4], z1 = sz[a3 * 4 + 1];
+    const S wx = x1 * y0 * z0, wy = x0 * y1 * z0, wz = x0 * y0 * z1;
     rx = fma(g.x, wx, rx); ry = fma(g.x, wy, ry); rz = fma(g.x, wz, rz);
     ix = fma(g.y, wx, ix); iy = fma(g.y, wy, iy); iz = fma(g.y, wz, iz);
   }
-  rx = warp_sum(rx); ry = warp_sum(ry); rz = warp_sum(rz);
-  ix = warp_sum(ix); iy = warp_sum(iy); iz = warp_sum(iz);
+  const double Rx = warp_sum((double)rx), Ry = warp_sum((double)ry), Rz = warp_sum((double)rz);
+  const double Ix = warp_sum((double)ix), Iy = warp_sum((double)iy), Iz = warp_sum((double)iz);
   if (lane < 2) {
-    const double f[3] = {lane == 0 ? rx : ix, lane == 0 ? ry : iy, lane == 0 ? rz : iz};
+    const double f[3] = {lane == 0 ? Rx : Ix, lane == 0 ? Ry : Iy, lane == 0 ? Rz : Iz};
     double *out = lane == 0 ? cphiR : cphiI;
 #pragma unroll
     for (int j = 1; j < 4; j++) {
@@ -698,11 +753,23 @@ void setup_pme(Handle &h) {
       tw[(size_t)d * maxn + j] = make_double2(std::cos(ang), -std::sin(ang));
     }
   cudaMemcpy(h.d_twiddle, tw.data(), tw.size() * sizeof(double2), cudaMemcpyHostToDevice);
+  if (h.mixed) {
+    // The influence function and twiddles are computed in FP64 and rounded once.
+    std::vector<float> Gf(G.size());
+    for (size_t q = 0; q < G.size(); q++) Gf[q] = (float)G[q];
+    std::vector<float2> twf(tw.size());
+    for (size_t q = 0; q < tw.size(); q++) twf[q] = make_float2((float)tw[q].x, (float)tw[q].y);
+    cudaMemcpy(h.d_influencef, Gf.data(), Gf.size() * sizeof(float), cudaMemcpyHostToDevice);
+    cudaMemcpy(h.d_twiddlef, twf.data(), twf.size() * sizeof(float2), cudaMemcpyHostToDevice);
+  }
   for (int d = 0; d < 3; d++) h.axes[d] = make_axis(d, nf);
   for (int d = 0; d < 3; d++) {
-    const size_t smem = 2 * (size_t)h.axes[d].len * h.axes[d].L * sizeof(double2);
-    cudaFuncSetAttribute(k_fft_axis<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)std::max<size_t>(smem, 48 * 1024));
-    cudaFuncSetAttribute(k_fft_axis<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)std::max<size_t>(smem, 48 * 1024));
+    const int smem = (int)std::max<size_t>(2 * (size_t)h.axes[d].len * h.axes[d].L * sizeof(double2), 48 * 1024);
+    cudaFuncSetAttribute(k_fft_axis<false, double, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+    cudaFuncSetAttribute(k_fft_axis<true, double, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+    cudaFuncSetAttribute(k_fft_axis<false, float, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+    cudaFuncSetAttribute(k_fft_axis<false, float, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+    cudaFuncSetAttribute(k_fft_axis<true, float, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
   }
 }
 
@@ -713,63 +780,102 @@ void launch_rotate(Handle &h) {
 }
 
 void launch_bsplines(Handle &h) {
-  k_bsplines<<<nblocks(h.n, 128), 128, 0, h.stream>>>(h.n, h.d_x, h.d_y, h.d_z, h.d_gm, h.nfft[0], h.nfft[1],
-                                                       h.nfft[2], h.d_spl, h.d_igrid, h.d_fm, h.pc);
+  if (h.mixed)
+    k_bsplines<float><<<nblocks(h.n, 128), 128, 0, h.stream>>>(h.n, h.d_x, h.d_y, h.d_z, h.d_gm, h.nfft[0], h.nfft[1],
+                                                              h.nfft[2], reinterpret_cast<float *>(h.d_spl), h.d_igrid,
+                                                              h.d_fm, h.pc);
+  else
+    k_bsplines<double><<<nblocks(h.n, 128), 128, 0, h.stream>>>(h.n, h.d_x, h.d_y, h.d_z, h.d_gm, h.nfft[0], h.nfft[1],
+                                                               h.nfft[2], h.d_spl, h.d_igrid, h.d_fm, h.pc);
   FFX_LAUNCHED(h);
 }
 
 static size_t grid_points(const Handle &h) { return (size_t)h.nfft[0] * h.nfft[1] * h.nfft[2]; }
 
+// The mixed form's accumulation mesh is cleared by the FFT pass that consumes it.
 void launch_spread_permanent(Handle &h) {
-  cudaMemsetAsync(h.d_grid, 0, grid_points(h) * sizeof(double2), h.stream);
-  k_spread_permanent<<<nblocks((int64_t)h.n * 32, 256), 256, 0, h.stream>>>(h.n, h.d_fm, h.d_spl, h.d_igrid,
-                                                                             h.nfft[0], h.nfft[1], h.nfft[2], h.d_grid);
+  const int nb = nblocks((int64_t)h.n * 32, 256);
+  if (h.mixed) {
+    k_spread_permanent<float><<<nb, 256, 0, h.stream>>>(h.n, h.d_fm, reinterpret_cast<const float *>(h.d_spl),
+                                                        h.d_igrid, h.nfft[0], h.nfft[1], h.nfft[2], nullptr, h.d_gridq);
+  } else {
+    cudaMemsetAsync(h.d_grid, 0, grid_points(h) * sizeof(double2), h.stream);
+    k_spread_permanent<double><<<nb, 256, 0, h.stream>>>(h.n, h.d_fm, h.d_spl, h.d_igrid, h.nfft[0], h.nfft[1],
+                                                         h.nfft[2], h.d_grid, nullptr);
+  }
   FFX_LAUNCHED(h);
 }
 
 void launch_spread_induced(Handle &h, const double *ud, const double *up) {
-  cudaMemsetAsync(h.d_grid, 0, grid_points(h) * sizeof(double2), h.stream);
-  k_spread_induced<<<nblocks((int64_t)h.n * 32, 256), 256, 0, h.stream>>>(h.n, ud, up, h.d_spl, h.d_igrid, h.nfft[0],
-                                                                           h.nfft[1], h.nfft[2], h.d_grid, h.pc);
+  const int nb = nblocks((int64_t)h.n * 32, 256);
+  if (h.mixed) {
+    k_spread_induced<float><<<nb, 256, 0, h.stream>>>(h.n, ud, up, reinterpret_cast<const float *>(h.d_spl), h.d_igrid,
+                                                      h.nfft[0], h.nfft[1], h.nfft[2], nullptr, h.d_gridq, h.pc);
+  } else {
+    cudaMemsetAsync(h.d_grid, 0, grid_points(h) * sizeof(double2), h.stream);
+    k_spread_induced<double><<<nb, 256, 0, h.stream>>>(h.n, ud, up, h.d_spl, h.d_igrid, h.nfft[0], h.nfft[1],
+                                                       h.nfft[2], h.d_grid, nullptr, h.pc);
+  }
   FFX_LAUNCHED(h);
 }
 
-void launch_fft_convolution(Handle &h) {
+template <typename S>
+static void fft_convolution(Handle &h, typename Vec2<S>::type *grid, const typename Vec2<S>::type *twiddle,
+                            const S *influence) {
   const int nfx = h.nfft[0], nfy = h.nfft[1], nfz = h.nfft[2];
   const int maxn = std::max(nfx, std::max(nfy, nfz));
-  auto run = [&](int d, int sign, bool fuse) {
+  auto run = [&](int d, int sign, bool fuse, bool fromq) {
     const FftAxis &a = h.axes[d];
     const int outer = (d == 0) ? nfz : ((d == 1) ? nfz : nfy);
     const int blocks = a.groups_inner * outer;
-    const size_t smem = 2 * (size_t)a.len * a.L * sizeof(double2);
+    const size_t smem = 2 * (size_t)a.len * a.L * sizeof(typename Vec2<S>::type);
+    const auto *tw = twiddle + (size_t)d * maxn;
     if (fuse)
-      k_fft_axis<true><<<blocks, 256, smem, h.stream>>>(h.d_grid, a, sign, h.d_twiddle + (size_t)d * maxn, h.d_influence, nfx, nfy);
+      k_fft_axis<true, S, false><<<blocks, 256, smem, h.stream>>>(grid, a, sign, tw, influence, nfx, nfy, nullptr);
+    else if (fromq)
+      k_fft_axis<false, S, true><<<blocks, 256, smem, h.stream>>>(grid, a, sign, tw, nullptr, nfx, nfy, h.d_gridq);
     else
-      k_fft_axis<false><<<blocks, 256, smem, h.stream>>>(h.d_grid, a, sign, h.d_twiddle + (size_t)d * maxn, nullptr, nfx, nfy);
+      k_fft_axis<false, S, false><<<blocks, 256, smem, h.stream>>>(grid, a, sign, tw, nullptr, nfx, nfy, nullptr);
     FFX_LAUNCHED(h);
   };
-  run(0, -1, false);
-  run(1, -1, false);
-  run(2, -1, true);
-  run(1, +1, false);
-  run(0, +1, false);
+  const bool fromq = (sizeof(S) == 4);
+  run(0, -1, false, fromq);
+  run(1, -1, false, false);
+  run(2, -1, true, false);
+  run(1, +1, false, false);
+  run(0, +1, false, false);
+}
+
+void launch_fft_convolution(Handle &h) {
+  if (h.mixed)
+    fft_convolution<float>(h, reinterpret_cast<float2 *>(h.d_grid), h.d_twiddlef, h.d_influencef);
+  else
+    fft_convolution<double>(h, h.d_grid, h.d_twiddle, h.d_influence);
+}
+
+template <typename S>
+static void phi(Handle &h, int which) {
+  const S *spl = reinterpret_cast<const S *>(h.d_spl);
+  const auto *grid = reinterpret_cast<const typename Vec2<S>::type *>(h.d_grid);
+  if (which == 0)
+    k_phi<20, S><<<nblocks(h.n, 128), 128, 0, h.stream>>>(h.n, spl, h.d_igrid, grid, h.nfft[0], h.nfft[1], h.nfft[2],
+                                                         h.d_fphi, h.d_cphi, nullptr, nullptr, h.pc);
+  else if (which == 1)
+    k_phi<20, S><<<nblocks(h.n, 128), 128, 0, h.stream>>>(h.n, spl, h.d_igrid, grid, h.nfft[0], h.nfft[1], h.nfft[2],
+                                                         h.d_fphiI, h.d_cphiI, h.d_fphiP, h.d_cphiP, h.pc);
+  else
+    k_phi_field<S><<<nblocks((int64_t)h.n * 32, 128), 128, 0, h.stream>>>(h.n, spl, h.d_igrid, grid, h.nfft[0],
+                                                                          h.nfft[1], h.nfft[2], h.pc, h.d_cphiI,
+                                                                          h.d_cphiP);
+  FFX_LAUNCHED(h);
 }
 
 void launch_phi_permanent(Handle &h) {
-  k_phi<20><<<nblocks(h.n, 128), 128, 0, h.stream>>>(h.n, h.d_spl, h.d_igrid, h.d_grid, h.nfft[0], h.nfft[1],
-                                                      h.nfft[2], h.d_fphi, h.d_cphi, nullptr, nullptr, h.pc);
-  FFX_LAUNCHED(h);
+  if (h.mixed) phi<float>(h, 0); else phi<double>(h, 0);
 }
 
 void launch_phi_induced(Handle &h, bool full) {
-  if (full)
-    k_phi<20><<<nblocks(h.n, 128), 128, 0, h.stream>>>(h.n, h.d_spl, h.d_igrid, h.d_grid, h.nfft[0], h.nfft[1],
-                                                        h.nfft[2], h.d_fphiI, h.d_cphiI, h.d_fphiP, h.d_cphiP, h.pc);
-  else
-    k_phi_field<<<nblocks((int64_t)h.n * 32, 128), 128, 0, h.stream>>>(h.n, h.d_spl, h.d_igrid, h.d_grid, h.nfft[0],
-                                                                        h.nfft[1], h.nfft[2], h.pc, h.d_cphiI,
-                                                                        h.d_cphiP);
-  FFX_LAUNCHED(h);
+  if (h.mixed) phi<float>(h, full ? 1 : 2); else phi<double>(h, full ? 1 : 2);
 }
 
 
@@ -906,7 +1012,7 @@ __device__ __forceinline__ int na_spline(double w, int nf, double *out) {
   const double u = w - floor(w + 0.5) + 0.5;
   const double fr = nf * u;
   const int ifr = (int)fr;
-  bspline5(fr - ifr, out);
+  bspline5<double>(fr - ifr, out);
   return ifr - kOrder;
 }
 
@@ -1114,11 +1220,11 @@ extern "C" int ffxg_pme_recip_permanent_noalloc(const double *d_xyz, const doubl
     const int outer = (d == 2) ? nf[1] : nf[2];
     const size_t smem = 2 * (size_t)ax.len * ax.L * sizeof(double2);
     if (pass == 2)
-      k_fft_axis<true><<<ax.groups_inner * outer, 256, smem, st>>>(grid, ax, sign, s->twiddle + d * kNaMaxDim,
-                                                                   s->influence, nf[0], nf[1]);
+      k_fft_axis<true, double, false><<<ax.groups_inner * outer, 256, smem, st>>>(
+          grid, ax, sign, s->twiddle + d * kNaMaxDim, s->influence, nf[0], nf[1], nullptr);
     else
-      k_fft_axis<false><<<ax.groups_inner * outer, 256, smem, st>>>(grid, ax, sign, s->twiddle + d * kNaMaxDim,
-                                                                    nullptr, nf[0], nf[1]);
+      k_fft_axis<false, double, false><<<ax.groups_inner * outer, 256, smem, st>>>(
+          grid, ax, sign, s->twiddle + d * kNaMaxDim, nullptr, nf[0], nf[1], nullptr);
   }
   const int nb = nblocks(n_atoms, kNaThreads);
   k_na_phi<<<nb, kNaThreads, 0, st>>>(n_atoms, d_xyz, d_mpole, nf[0], nf[1], nf[2], pc, d_phi, s);

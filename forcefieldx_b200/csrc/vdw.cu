@@ -15,6 +15,7 @@ namespace ffx {
 struct VdwForm {
   double off2, cut2, t1n, gamma1, delta, gamma;
   double c0, c1, c2, c3, c4, c5;
+  double cut, iwidth;   // taper start and 1 / (cutoff - taper start)
 };
 
 __device__ __forceinline__ unsigned vexcl_code(int i, int k, const int *__restrict__ ptr, const int *__restrict__ ek,
@@ -27,6 +28,7 @@ __device__ __forceinline__ unsigned vexcl_code(int i, int k, const int *__restri
   return 0u;
 }
 
+template <typename R>
 __global__ void __launch_bounds__(256) k_vdw(int n, const double *__restrict__ rx, const double *__restrict__ ry,
                                              const double *__restrict__ rz, Box bx, const int *__restrict__ vtype,
                                              int ntypes, const double *__restrict__ vrad,
@@ -41,62 +43,75 @@ __global__ void __launch_bounds__(256) k_vdw(int n, const double *__restrict__ r
   const int i = warp;
   const double xi = rx[i], yi = ry[i], zi = rz[i];
   const int ti = vtype[i];
-  double e = 0.0, gx = 0.0, gy = 0.0, gz = 0.0;
+  const R delta = vf.delta, gamma = vf.gamma, gamma1 = vf.gamma1, t1n = vf.t1n;
+  const R c0 = vf.c0, c1 = vf.c1, c2 = vf.c2, c3 = vf.c3, c4 = vf.c4, c5 = vf.c5;
+  const R cut = vf.cut, iwidth = vf.iwidth;
+  double e = 0.0;
+  R gx = 0, gy = 0, gz = 0;
   long long cnt = 0;
   const int m = min(nbr_cnt[i], cap);
   const int *row = nbr + (size_t)i * cap;
   for (int a = lane; a < m; a += 32) {
     const int k = row[a];
-    double dx = __dsub_rn(xi, rx[k]), dy = __dsub_rn(yi, ry[k]), dz = __dsub_rn(zi, rz[k]);
-    const double r2 = image_exact(dx, dy, dz, bx);
+    double dxd = __dsub_rn(xi, rx[k]), dyd = __dsub_rn(yi, ry[k]), dzd = __dsub_rn(zi, rz[k]);
+    const double r2d = image_exact(dxd, dyd, dzd, bx);
     const int tk = vtype[k];
-    const double irv = vrad[ti * ntypes + tk];
-    if (!(r2 <= vf.off2) || !(irv > 0.0)) continue;
+    const R irv = vrad[ti * ntypes + tk];
+    if (!(r2d <= vf.off2) || !(irv > R(0.0))) continue;
     const unsigned code = vexcl_code(i, k, eptr, ek, ecode, elo, ehi);
-    const double mask = c_vscales.v[(code >> 7) & 3u];
-    if (!(mask > 0.0)) continue;
-    const double r = sqrt(r2);
-    const double ev = mask * veps[ti * ntypes + tk];
-    const double rho = r * irv;
-    const double rho2 = rho * rho;
-    const double rhoDisp1 = rho2 * rho2 * rho2;
-    const double rhoDisp = rhoDisp1 * rho;
-    const double rd = rho + vf.delta, rd2 = rd * rd;
-    const double rhoDelta1 = rd2 * rd2 * rd2;
-    const double rhoDelta = rhoDelta1 * rd;
-    const double t1d = 1.0 / rhoDelta;
-    const double t2d = 1.0 / (rhoDisp + vf.gamma);
-    const double t1 = vf.t1n * t1d;
-    const double t2a = vf.gamma1 * t2d;
-    const double t2 = t2a - 2.0;
-    const double eik = ev * t1 * t2;
-    double taper = 1.0, dtaper = 0.0;
-    if (r2 > vf.cut2) {
-      const double r3 = r2 * r, r4 = r2 * r2, r5 = r2 * r3;
-      taper = vf.c5 * r5 + vf.c4 * r4 + vf.c3 * r3 + vf.c2 * r2 + vf.c1 * r + vf.c0;
-      dtaper = 5.0 * vf.c5 * r4 + 4.0 * vf.c4 * r3 + 3.0 * vf.c3 * r2 + 2.0 * vf.c2 * r + vf.c1;
+    const R mask = c_vscales.v[(code >> 7) & 3u];
+    if (!(mask > R(0.0))) continue;
+    const R dx = (R)dxd, dy = (R)dyd, dz = (R)dzd, r2 = (R)r2d;
+    const R r = m_sqrt(r2);
+    const R ev = mask * veps[ti * ntypes + tk];
+    const R rho = r * irv;
+    const R rho2 = rho * rho;
+    const R rhoDisp1 = rho2 * rho2 * rho2;
+    const R rhoDisp = rhoDisp1 * rho;
+    const R rd = rho + delta, rd2 = rd * rd;
+    const R rhoDelta1 = rd2 * rd2 * rd2;
+    const R rhoDelta = rhoDelta1 * rd;
+    const R t1d = R(1.0) / rhoDelta;
+    const R t2d = R(1.0) / (rhoDisp + gamma);
+    const R t1 = t1n * t1d;
+    const R t2a = gamma1 * t2d;
+    const R t2 = t2a - R(2.0);
+    const R eik = ev * t1 * t2;
+    R taper = R(1.0), dtaper = R(0.0);
+    if (r2d > vf.cut2) {
+      if (sizeof(R) == 8) {
+        const R r3 = r2 * r, r4 = r2 * r2, r5 = r2 * r3;
+        taper = c5 * r5 + c4 * r4 + c3 * r3 + c2 * r2 + c1 * r + c0;
+        dtaper = R(5.0) * c5 * r4 + R(4.0) * c4 * r3 + R(3.0) * c3 * r2 + R(2.0) * c2 * r + c1;
+      } else {
+        // The same quintic in t = (r - cut) / (off - cut): 1 - 10 t^3 + 15 t^4 - 6 t^5.
+        // The power form above cancels ~1e6-sized terms and is unusable in FP32.
+        const R t = (r - cut) * iwidth, t2 = t * t;
+        taper = R(1) + t2 * t * (R(-10) + t * (R(15) - R(6) * t));
+        dtaper = t2 * (R(-30) + t * (R(60) - R(30) * t)) * iwidth;
+      }
     }
-    e += 0.5 * eik * taper;
+    e += R(0.5) * eik * taper;
     if (k > i) cnt++;
     if (gradient) {
-      const double dt1d_dr = 7.0 * rhoDelta1 * irv;
-      const double dt2d_dr = 7.0 * rhoDisp1 * irv;
-      const double dt1_dr = t1 * dt1d_dr * t1d;
-      const double dt2_dr = t2a * dt2d_dr * t2d;
-      const double dedr = -ev * (dt1_dr * t2 + t1 * dt2_dr);
-      const double ir = 1.0 / r;
-      const double dsw = eik * dtaper + dedr * taper;
+      const R dt1d_dr = R(7.0) * rhoDelta1 * irv;
+      const R dt2d_dr = R(7.0) * rhoDisp1 * irv;
+      const R dt1_dr = t1 * dt1d_dr * t1d;
+      const R dt2_dr = t2a * dt2d_dr * t2d;
+      const R dedr = -ev * (dt1_dr * t2 + t1 * dt2_dr);
+      const R ir = R(1.0) / r;
+      const R dsw = eik * dtaper + dedr * taper;
       gx += dsw * dx * ir; gy += dsw * dy * ir; gz += dsw * dz * ir;
     }
   }
   e = warp_sum(e);
-  gx = warp_sum(gx); gy = warp_sum(gy); gz = warp_sum(gz);
+  const double Gx = warp_sum((double)gx), Gy = warp_sum((double)gy), Gz = warp_sum((double)gz);
 #pragma unroll
   for (int o = 16; o > 0; o >>= 1) cnt += __shfl_xor_sync(0xffffffffu, cnt, o);
   if (lane == 0) {
     eatom[i] = e;
     catom[i] = cnt;
-    if (gradient) { gred[i] = gx; gred[n + i] = gy; gred[2 * n + i] = gz; }
+    if (gradient) { gred[i] = Gx; gred[n + i] = Gy; gred[2 * n + i] = Gz; }
   }
 }
 
@@ -134,7 +149,10 @@ void launch_vdw(Handle &h, bool grad) {
   vf.c3 = -10.0 * (a2 + 4.0 * a * b + b2) / den;
   vf.c4 = 15.0 * (a + b) / den;
   vf.c5 = -6.0 / den;
-  k_vdw<<<nblocks((int64_t)h.n * 32, 256), 256, 0, h.stream>>>(
+  vf.cut = cut;
+  vf.iwidth = 1.0 / (off - cut);
+  auto kern = h.mixed ? k_vdw<float> : k_vdw<double>;
+  kern<<<nblocks((int64_t)h.n * 32, 256), 256, 0, h.stream>>>(
       h.n, h.d_rx, h.d_ry, h.d_rz, h.box, h.d_vtype, h.ntypes, h.d_vrad, h.d_veps, h.d_nbr, h.d_nbr_cnt, h.cap_nbr,
       h.d_excl_ptr, h.d_excl_k, h.d_excl_code, h.d_excl_lo, h.d_excl_hi, vf, h.scales, grad ? 1 : 0, h.d_eatom, h.d_catom,
       h.d_gred);
