@@ -65,6 +65,7 @@ PROTOTYPES = {
     "ffxg_stream": (ctypes.c_void_p, [ctypes.c_void_p]),
     "ffxg_last_launch_count": (ctypes.c_int64, [ctypes.c_void_p]),
     "ffxg_set_timing": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int]),
+    "ffxg_set_graph_mode": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int]),
     "ffxg_get_timings": (ctypes.c_int, [ctypes.c_void_p, _D, _L, ctypes.c_int]),
     "ffxg_pme_recip_permanent_noalloc": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int32, _D, _I,
                                                         ctypes.c_double, ctypes.c_double, ctypes.c_void_p,

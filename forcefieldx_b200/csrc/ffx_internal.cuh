@@ -115,6 +115,15 @@ struct FftAxis {
   int radix[12];
 };
 
+// Device-side state of the PCG solve (read by the host after the loop).
+struct PcgState {
+  double eps;     // last convergence measure, Debye
+  int iter;       // completed iterations
+  int status;     // FFXG_OK or the SCF error status
+  int cont;       // 1 while the loop should continue
+  int pad;
+};
+
 struct Handle {
   // ---- configuration
   int n = 0;
@@ -199,6 +208,14 @@ struct Handle {
   double *h_xyz_pin = nullptr, *h_grad_pin = nullptr;
 
   int scf_iter = 0;
+  PcgState *d_pcg = nullptr, *h_pcg = nullptr;
+  // Graph execution: the whole evaluation captured once per gradient mode and replayed.
+  bool use_graphs = true;
+  bool want_grad = true;                            // gradient requested by the current call
+  cudaStream_t side = nullptr;                      // captures the PCG while-node body
+  cudaGraphExec_t graph_exec[2] = {nullptr, nullptr};
+  int64_t graph_launches[2] = {0, 0};               // kernels outside the PCG body
+  int64_t graph_body_launches = 0;
   double e_charge_correction = 0.0;
   // Stage timers (PMETimings counterpart).
   bool timing = false;
@@ -223,7 +240,7 @@ void launch_phi_permanent(Handle &h);
 void launch_phi_induced(Handle &h, bool full);
 void launch_realspace_field(Handle &h);
 void launch_induced_recip(Handle &h, const double *ud, const double *up);
-int run_pcg(Handle &h);
+int run_pcg(Handle &h, bool capture);
 void launch_recip_energy(Handle &h, bool grad);
 void launch_real_energy(Handle &h, bool grad);
 void launch_torque(Handle &h);

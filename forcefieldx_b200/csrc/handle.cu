@@ -47,7 +47,13 @@ static bool fft_supported(int n) {
 
 __global__ void k_set_flags(int *flags, int v) { *flags = v; }
 
+static void drop_graphs(Handle &h) {
+  for (cudaGraphExec_t &g : h.graph_exec)
+    if (g) { cudaGraphExecDestroy(g); g = nullptr; }
+}
+
 static int alloc_lists(Handle &h) {
+  drop_graphs(h);   // the captured kernels hold the old list pointers
   if (h.d_nbr) cudaFree(h.d_nbr);
   if (h.d_ewl) cudaFree(h.d_ewl);
   if (h.d_prl) cudaFree(h.d_prl);
@@ -101,6 +107,7 @@ static int create_impl(const ffxg_system *s, const ffxg_params *p, Handle &h) {
   if (prop.major < 10) { h.err = "requires an sm_100 (Blackwell) device"; return FFXG_ERR_CUDA; }
   h.device = dev;
   CK(cudaStreamCreateWithFlags(&h.stream, cudaStreamNonBlocking));
+  CK(cudaStreamCreateWithFlags(&h.side, cudaStreamNonBlocking));
 
   h.box.a = p->box[0]; h.box.b = p->box[1]; h.box.c = p->box[2];
   h.box.A00 = 1.0 / h.box.a; h.box.A11 = 1.0 / h.box.b; h.box.A22 = 1.0 / h.box.c;
@@ -224,6 +231,8 @@ static int create_impl(const ffxg_system *s, const ffxg_params *p, Handle &h) {
   CK(cudaMemset(h.d_counter, 0, 4 * sizeof(unsigned)));
   CK(dalloc(&h.d_scalars, 16));
   CK(cudaMallocHost((void **)&h.h_scalars, 16 * sizeof(double)));
+  CK(cudaMalloc((void **)&h.d_pcg, sizeof(PcgState)));
+  CK(cudaMallocHost((void **)&h.h_pcg, sizeof(PcgState)));
   const int nfx = p->pme_grid[0], nfy = p->pme_grid[1], nfz = p->pme_grid[2];
   const size_t ng = (size_t)nfx * nfy * nfz;
   CK(dalloc(&h.d_grid, ng)); CK(dalloc(&h.d_influence, ng));
@@ -317,36 +326,127 @@ static void free_all(Handle &h) {
   if (h.h_xyz_pin) cudaFreeHost(h.h_xyz_pin);
   if (h.h_grad_pin) cudaFreeHost(h.h_grad_pin);
   for (cudaEvent_t e : h.ev_pool) cudaEventDestroy(e);
+  drop_graphs(h);
+  if (h.d_pcg) cudaFree(h.d_pcg);
+  if (h.h_pcg) cudaFreeHost(h.h_pcg);
+  if (h.side) cudaStreamDestroy(h.side);
   if (h.stream) cudaStreamDestroy(h.stream);
 }
 
-// One evaluation on device-resident coordinates; grows list capacities and repeats on overflow.
-static int evaluate(Handle &h, const double *d_xyz, double *d_grad_xyz, bool grad, double *terms, int64_t *counts) {
-  h.launches = 0;
+// ---------------------------------------------------------------------------
+// Evaluation.  emit_front (coordinates .. permanent field) and emit_back (energies,
+// torques, gradient, reductions) are shared by the direct path and the captured graph.
+static void emit_front(Handle &h, const double *d_xyz) {
+  int tk = timer_begin(h, FFXG_STAGE_LISTS);
+  k_set_flags<<<1, 1, 0, h.stream>>>(h.d_flags, h.list_valid ? 0 : FLAG_REBUILD);
+  FFX_LAUNCHED(h);
+  launch_set_coordinates(h, d_xyz);
+  launch_neighbor_list(h, false);
+  timer_end(h, tk);
+  tk = timer_begin(h, FFXG_STAGE_VDW);
+  launch_vdw(h, h.want_grad);
+  timer_end(h, tk);
+  tk = timer_begin(h, FFXG_STAGE_MULTIPOLES);
+  launch_rotate(h);
+  launch_bsplines(h);
+  timer_end(h, tk);
+  tk = timer_begin(h, FFXG_STAGE_PERM_RECIP);
+  launch_spread_permanent(h);
+  launch_fft_convolution(h);
+  launch_phi_permanent(h);
+  timer_end(h, tk);
+  tk = timer_begin(h, FFXG_STAGE_PERM_FIELD);
+  launch_realspace_field(h);   // sub-lists, permanent field, pair coefficients, direct dipoles
+  timer_end(h, tk);
+}
+
+static void emit_final_induced(Handle &h) {
+  const int tk = timer_begin(h, FFXG_STAGE_IND_RECIP);
+  launch_spread_induced(h, h.d_uD, h.d_uP);
+  launch_fft_convolution(h);
+  launch_phi_induced(h, true);
+  timer_end(h, tk);
+}
+
+static void emit_no_polarization(Handle &h) {
+  cudaMemsetAsync(h.d_uD, 0, 3 * (size_t)h.n * sizeof(double), h.stream);
+  cudaMemsetAsync(h.d_uP, 0, 3 * (size_t)h.n * sizeof(double), h.stream);
+}
+
+static void emit_back(Handle &h, double *d_grad_xyz) {
+  int tk = timer_begin(h, FFXG_STAGE_REAL_ENERGY);
+  launch_real_energy(h, h.want_grad);
+  timer_end(h, tk);
+  tk = timer_begin(h, FFXG_STAGE_RECIP_ENERGY);
+  launch_recip_energy(h, h.want_grad);
+  timer_end(h, tk);
+  tk = timer_begin(h, FFXG_STAGE_GRADIENT);
+  if (h.want_grad) {
+    launch_torque(h);
+    launch_assemble(h, d_grad_xyz);
+  }
+  launch_reduce_results(h);
+  timer_end(h, tk);
+  cudaMemcpyAsync(h.h_scalars, h.d_result, 7 * sizeof(double), cudaMemcpyDeviceToHost, h.stream);
+  cudaMemcpyAsync(h.h_flags + 2, h.d_cresult, 2 * sizeof(long long), cudaMemcpyDeviceToHost, h.stream);
+  cudaMemcpyAsync(h.h_flags, h.d_flags, sizeof(int), cudaMemcpyDeviceToHost, h.stream);
+}
+
+static const char *scf_message(int st) {
+  return (st == FFXG_ERR_SCF_DIVERGED) ? "SCF convergence failure (residual grew)"
+         : (st == FFXG_ERR_SCF_MAXITER) ? "maximum SCF iterations reached"
+                                        : "non-finite SCF residual";
+}
+
+// Terms and counts from the pinned copies written by emit_back.
+static int finish(Handle &h, bool rebuilt, double *terms, int64_t *counts) {
+  double res[7];
+  long long cres[2];
+  std::memcpy(res, h.h_scalars, 7 * sizeof(double));
+  std::memcpy(cres, h.h_flags + 2, 2 * sizeof(long long));
+  const double eCorr = h.e_charge_correction;
+  if (terms) {
+    terms[FFXG_TERM_VDW] = res[0];
+    terms[FFXG_TERM_PERM_REAL] = res[1];
+    terms[FFXG_TERM_POL_REAL] = res[2];
+    terms[FFXG_TERM_PERM_SELF] = res[3];
+    terms[FFXG_TERM_PERM_RECIP] = res[4] + eCorr;
+    terms[FFXG_TERM_POL_SELF] = res[5];
+    terms[FFXG_TERM_POL_RECIP] = res[6];
+    terms[FFXG_TERM_PERMANENT] = res[1] + res[3] + res[4] + eCorr;
+    terms[FFXG_TERM_POLARIZATION] = res[2] + res[5] + res[6];
+    terms[FFXG_TERM_TOTAL] = res[0] + terms[FFXG_TERM_PERMANENT] + terms[FFXG_TERM_POLARIZATION];
+  }
+  if (counts) {
+    counts[FFXG_COUNT_VDW] = cres[0];
+    counts[FFXG_COUNT_PERMANENT] = cres[1] + h.n;
+    counts[FFXG_COUNT_SCF_ITER] = h.scf_iter;
+    counts[FFXG_COUNT_LIST_BUILDS] = rebuilt ? 1 : 0;
+    counts[FFXG_COUNT_LIST_PAIRS] = -1;
+  }
+  if (h.h_flags[0] & FLAG_NONFINITE) { h.err = "non-finite energy, torque or gradient"; return FFXG_ERR_NONFINITE; }
+  for (int t = 0; t < 7; t++)
+    if (!std::isfinite(res[t])) { h.err = "non-finite energy"; return FFXG_ERR_NONFINITE; }
+  return FFXG_OK;
+}
+
+static int grow_lists(Handle &h, int f) {
+  if (f & FLAG_NBR_OVERFLOW) h.cap_nbr = round32(h.cap_nbr * 1.5);
+  if (f & FLAG_EWALD_OVERFLOW) h.cap_ewl = round32(h.cap_ewl * 1.5);
+  if (f & FLAG_PRECOND_OVERFLOW) h.cap_prl = round32(h.cap_prl * 1.5);
+  return alloc_lists(h);
+}
+
+static constexpr int kOverflow = FLAG_NBR_OVERFLOW | FLAG_EWALD_OVERFLOW | FLAG_PRECOND_OVERFLOW;
+
+// Direct execution: one host check of the list and coordinate flags before the solver,
+// the solver's stopping test read back per iteration.  Grows list capacities and repeats
+// on overflow.
+static int evaluate_direct(Handle &h, const double *d_xyz, double *d_grad_xyz, double *terms, int64_t *counts) {
   for (int attempt = 0; attempt < 4; attempt++) {
     h.ev_stage.clear();
     h.ev_used = 0;
-    int tk = timer_begin(h, FFXG_STAGE_LISTS);
-    k_set_flags<<<1, 1, 0, h.stream>>>(h.d_flags, h.list_valid ? 0 : FLAG_REBUILD);
-    FFX_LAUNCHED(h);
-    launch_set_coordinates(h, d_xyz);
-    launch_neighbor_list(h, false);
-    timer_end(h, tk);
-    tk = timer_begin(h, FFXG_STAGE_VDW);
-    launch_vdw(h, grad);
-    timer_end(h, tk);
-    tk = timer_begin(h, FFXG_STAGE_MULTIPOLES);
-    launch_rotate(h);
-    launch_bsplines(h);
-    timer_end(h, tk);
-    tk = timer_begin(h, FFXG_STAGE_PERM_RECIP);
-    launch_spread_permanent(h);
-    launch_fft_convolution(h);
-    launch_phi_permanent(h);
-    timer_end(h, tk);
-    tk = timer_begin(h, FFXG_STAGE_PERM_FIELD);
-    launch_realspace_field(h);   // sub-lists, permanent field, pair coefficients, direct dipoles
-    timer_end(h, tk);
+    emit_front(h, d_xyz);
     // List overflow invalidates everything downstream and non-finite coordinates
     // make the evaluation meaningless: check both before the solver.
     cudaMemcpyAsync(h.h_flags, h.d_flags, sizeof(int), cudaMemcpyDeviceToHost, h.stream);
@@ -356,11 +456,8 @@ static int evaluate(Handle &h, const double *d_xyz, double *d_grad_xyz, bool gra
     }
     const int f = h.h_flags[0];
     if (f & FLAG_NONFINITE) { h.err = "non-finite coordinates"; return FFXG_ERR_NONFINITE; }
-    if (f & (FLAG_NBR_OVERFLOW | FLAG_EWALD_OVERFLOW | FLAG_PRECOND_OVERFLOW)) {
-      if (f & FLAG_NBR_OVERFLOW) h.cap_nbr = round32(h.cap_nbr * 1.5);
-      if (f & FLAG_EWALD_OVERFLOW) h.cap_ewl = round32(h.cap_ewl * 1.5);
-      if (f & FLAG_PRECOND_OVERFLOW) h.cap_prl = round32(h.cap_prl * 1.5);
-      if (int a = alloc_lists(h)) return a;
+    if (f & kOverflow) {
+      if (int a = grow_lists(h, f)) return a;
       continue;
     }
     const bool rebuilt = (f & FLAG_REBUILD) != 0;
@@ -369,76 +466,111 @@ static int evaluate(Handle &h, const double *d_xyz, double *d_grad_xyz, bool gra
     int st = FFXG_OK;
     h.scf_iter = 0;
     if (h.prm.polarization != FFXG_POLAR_NONE) {
-      if (h.prm.polarization == FFXG_POLAR_MUTUAL) st = run_pcg(h);
-      if (st == FFXG_OK) {
-        tk = timer_begin(h, FFXG_STAGE_IND_RECIP);
-        launch_spread_induced(h, h.d_uD, h.d_uP);
-        launch_fft_convolution(h);
-        launch_phi_induced(h, true);
-        timer_end(h, tk);
-      }
+      if (h.prm.polarization == FFXG_POLAR_MUTUAL) st = run_pcg(h, false);
+      if (st == FFXG_OK) emit_final_induced(h);
     } else {
-      cudaMemsetAsync(h.d_uD, 0, 3 * (size_t)h.n * sizeof(double), h.stream);
-      cudaMemsetAsync(h.d_uP, 0, 3 * (size_t)h.n * sizeof(double), h.stream);
+      emit_no_polarization(h);
     }
-    if (st != FFXG_OK) {
-      h.err = (st == FFXG_ERR_SCF_DIVERGED) ? "SCF convergence failure (residual grew)"
-              : (st == FFXG_ERR_SCF_MAXITER) ? "maximum SCF iterations reached"
-                                             : "non-finite SCF residual";
-      return st;
-    }
-    tk = timer_begin(h, FFXG_STAGE_REAL_ENERGY);
-    launch_real_energy(h, grad);
-    timer_end(h, tk);
-    tk = timer_begin(h, FFXG_STAGE_RECIP_ENERGY);
-    launch_recip_energy(h, grad);
-    timer_end(h, tk);
-    tk = timer_begin(h, FFXG_STAGE_GRADIENT);
-    if (grad) {
-      launch_torque(h);
-      launch_assemble(h, d_grad_xyz);
-    }
-    launch_reduce_results(h);
-    timer_end(h, tk);
-    double res[8];
-    long long cres[2];
-    cudaMemcpyAsync(h.h_scalars, h.d_result, 7 * sizeof(double), cudaMemcpyDeviceToHost, h.stream);
-    cudaMemcpyAsync(h.h_flags + 2, h.d_cresult, 2 * sizeof(long long), cudaMemcpyDeviceToHost, h.stream);
-    cudaMemcpyAsync(h.h_flags, h.d_flags, sizeof(int), cudaMemcpyDeviceToHost, h.stream);
+    if (st != FFXG_OK) { h.err = scf_message(st); return st; }
+    emit_back(h, d_grad_xyz);
     if (cudaStreamSynchronize(h.stream) != cudaSuccess) {
       h.err = std::string("CUDA error: ") + cudaGetErrorString(cudaGetLastError());
       return FFXG_ERR_CUDA;
     }
-    std::memcpy(res, h.h_scalars, 7 * sizeof(double));
     if (h.timing) timer_collect(h);
-    std::memcpy(cres, h.h_flags + 2, 2 * sizeof(long long));
-    const double eCorr = h.e_charge_correction;
-    if (terms) {
-      terms[FFXG_TERM_VDW] = res[0];
-      terms[FFXG_TERM_PERM_REAL] = res[1];
-      terms[FFXG_TERM_POL_REAL] = res[2];
-      terms[FFXG_TERM_PERM_SELF] = res[3];
-      terms[FFXG_TERM_PERM_RECIP] = res[4] + eCorr;
-      terms[FFXG_TERM_POL_SELF] = res[5];
-      terms[FFXG_TERM_POL_RECIP] = res[6];
-      terms[FFXG_TERM_PERMANENT] = res[1] + res[3] + res[4] + eCorr;
-      terms[FFXG_TERM_POLARIZATION] = res[2] + res[5] + res[6];
-      terms[FFXG_TERM_TOTAL] = res[0] + terms[FFXG_TERM_PERMANENT] + terms[FFXG_TERM_POLARIZATION];
-    }
-    if (counts) {
-      counts[FFXG_COUNT_VDW] = cres[0];
-      counts[FFXG_COUNT_PERMANENT] = cres[1] + h.n;
-      counts[FFXG_COUNT_SCF_ITER] = h.scf_iter;
-      counts[FFXG_COUNT_LIST_BUILDS] = rebuilt ? 1 : 0;
-      counts[FFXG_COUNT_LIST_PAIRS] = -1;
-    }
-    if (h.h_flags[0] & FLAG_NONFINITE) { h.err = "non-finite energy, torque or gradient"; return FFXG_ERR_NONFINITE; }
-    for (int t = 0; t < 7; t++)
-      if (!std::isfinite(res[t])) { h.err = "non-finite energy"; return FFXG_ERR_NONFINITE; }
-    return FFXG_OK;
+    return finish(h, rebuilt, terms, counts);
   }
   h.err = "neighbour capacity could not be satisfied";
   return FFXG_ERR_CAPACITY;
+}
+
+// Capture the whole evaluation (internal coordinate and gradient buffers) as one graph.
+static int capture_graph(Handle &h) {
+  const int key = h.want_grad ? 1 : 0;
+  const int64_t before = h.launches;
+  if (cudaStreamBeginCapture(h.stream, cudaStreamCaptureModeThreadLocal) != cudaSuccess) return FFXG_ERR_CUDA;
+  emit_front(h, h.d_xyz_in);
+  int st = FFXG_OK;
+  if (h.prm.polarization != FFXG_POLAR_NONE) {
+    if (h.prm.polarization == FFXG_POLAR_MUTUAL) st = run_pcg(h, true);
+    emit_final_induced(h);
+  } else {
+    emit_no_polarization(h);
+  }
+  emit_back(h, h.d_grad_out);
+  cudaMemcpyAsync(h.h_pcg, h.d_pcg, sizeof(PcgState), cudaMemcpyDeviceToHost, h.stream);
+  cudaGraph_t graph = nullptr;
+  const cudaError_t ec = cudaStreamEndCapture(h.stream, &graph);
+  if (st != FFXG_OK || ec != cudaSuccess) {
+    if (graph) cudaGraphDestroy(graph);
+    cudaGetLastError();
+    return FFXG_ERR_CUDA;
+  }
+  const cudaError_t ei = cudaGraphInstantiate(&h.graph_exec[key], graph, 0);
+  cudaGraphDestroy(graph);
+  if (ei != cudaSuccess) {
+    h.graph_exec[key] = nullptr;
+    cudaGetLastError();
+    return FFXG_ERR_CUDA;
+  }
+  h.graph_launches[key] = h.launches - before - h.graph_body_launches;
+  return FFXG_OK;
+}
+
+// Graph execution: one launch, one synchronisation.  Returns -1 when the evaluation must
+// be repeated directly (list overflow, or the graph could not be built).
+static int evaluate_graph(Handle &h, const double *d_xyz, double *d_grad_xyz, double *terms, int64_t *counts) {
+  const int key = h.want_grad ? 1 : 0;
+  if (!h.graph_exec[key] && capture_graph(h) != FFXG_OK) {
+    h.use_graphs = false;   // fall back to direct launches for this handle
+    return -1;
+  }
+  if (d_xyz != h.d_xyz_in)
+    cudaMemcpyAsync(h.d_xyz_in, d_xyz, 3 * (size_t)h.n * sizeof(double), cudaMemcpyDeviceToDevice, h.stream);
+  if (cudaGraphLaunch(h.graph_exec[key], h.stream) != cudaSuccess) {
+    h.err = std::string("CUDA error: ") + cudaGetErrorString(cudaGetLastError());
+    return FFXG_ERR_CUDA;
+  }
+  if (h.want_grad && d_grad_xyz != h.d_grad_out)
+    cudaMemcpyAsync(d_grad_xyz, h.d_grad_out, 3 * (size_t)h.n * sizeof(double), cudaMemcpyDeviceToDevice, h.stream);
+  if (cudaStreamSynchronize(h.stream) != cudaSuccess) {
+    h.err = std::string("CUDA error: ") + cudaGetErrorString(cudaGetLastError());
+    return FFXG_ERR_CUDA;
+  }
+  const int f = h.h_flags[0];
+  if (f & kOverflow) {
+    if (int a = grow_lists(h, f)) return a;   // also drops the graphs
+    return -1;
+  }
+  if (f & FLAG_NONFINITE) {
+    // k_reduce_coordinates raises the flag for non-finite input coordinates.
+    h.err = "non-finite coordinates or energy";
+    return FFXG_ERR_NONFINITE;
+  }
+  const bool rebuilt = (f & FLAG_REBUILD) != 0;
+  if (rebuilt) h.list_builds++;
+  h.scf_iter = 0;
+  h.launches = h.graph_launches[key];
+  if (h.prm.polarization == FFXG_POLAR_MUTUAL) {
+    h.scf_iter = h.h_pcg->iter;
+    h.launches += h.graph_body_launches * (int64_t)std::max(0, h.scf_iter - 1);
+    if (h.h_pcg->status != FFXG_OK) { h.err = scf_message(h.h_pcg->status); return h.h_pcg->status; }
+  }
+  return finish(h, rebuilt, terms, counts);
+}
+
+// One evaluation on device-resident coordinates.  The graph path is used once the
+// neighbour list exists (its first build and any regrowth run directly) and when stage
+// timing is off.
+static int evaluate(Handle &h, const double *d_xyz, double *d_grad_xyz, bool grad, double *terms, int64_t *counts) {
+  h.launches = 0;
+  h.want_grad = grad;
+  if (h.use_graphs && h.list_valid && !h.timing) {
+    const int st = evaluate_graph(h, d_xyz, d_grad_xyz, terms, counts);
+    if (st != -1) return st;
+    h.launches = 0;
+  }
+  return evaluate_direct(h, d_xyz, d_grad_xyz, terms, counts);
 }
 
 extern "C" {
@@ -550,6 +682,14 @@ int ffxg_get_neighbor_pairs(ffxg_handle *hh, int32_t *pairs, int64_t *n_pairs) {
 void *ffxg_stream(ffxg_handle *hh) { return hh ? (void *)hh->h.stream : nullptr; }
 
 int64_t ffxg_last_launch_count(const ffxg_handle *hh) { return hh ? hh->h.launches : 0; }
+
+int ffxg_set_graph_mode(ffxg_handle *hh, int on) {
+  if (!hh) return FFXG_ERR_BAD_ARG;
+  Handle &h = hh->h;
+  h.use_graphs = on != 0;
+  if (!h.use_graphs) drop_graphs(h);
+  return FFXG_OK;
+}
 
 int ffxg_set_timing(ffxg_handle *hh, int on) {
   if (!hh) return FFXG_ERR_BAD_ARG;

@@ -171,14 +171,29 @@ __global__ void __launch_bounds__(kFieldThreads) k_pcg_precond(
   if (!INIT) block_store<2>(acc, part, C_RZN);
 }
 
+// PCGSolver.scfByPCG stopping rules (pme/PCGSolver.java:541-570) applied on the device:
+// eps = 4.80321 sqrt(max(|r_D|^2, |r_CR|^2) / n); stop with an error when eps grew (or
+// is not finite) or the iteration limit is reached, stop converged when eps < polar-eps.
+// A list overflow seen earlier in the evaluation also stops the loop (the host repeats
+// the evaluation with larger lists).
+__global__ void k_pcg_reset(PcgState *st) {
+  st->eps = 100.0;
+  st->iter = 0;
+  st->status = FFXG_OK;
+  st->cont = 1;
+}
+
 // alpha = r.z / p.Ap; r -= alpha vec; u += alpha p; |r|^2 partials; the last block
-// finishes both norms into out[0..1] and re-arms the counter.
+// finishes both norms, applies the stopping rules to PcgState, re-arms the counter and,
+// inside a captured graph, sets the condition of the PCG while node.
 __global__ void __launch_bounds__(kVecThreads) k_pcg_update(int n, int nbf, const double *__restrict__ vec,
                                                             const double *__restrict__ vecP,
                                                             const double *__restrict__ p,
                                                             const double *__restrict__ pP, double *r, double *rP,
                                                             double *uD, double *uP, const double *__restrict__ partF,
-                                                            double *partE, unsigned *counter, double *out) {
+                                                            double *partE, unsigned *counter, PcgState *st,
+                                                            int max_iter, double polar_eps, const int *flags,
+                                                            cudaGraphConditionalHandle cond, int use_cond) {
   __shared__ double alpha[2];
   __shared__ bool last;
   if (threadIdx.x < 32) {
@@ -212,9 +227,27 @@ __global__ void __launch_bounds__(kVecThreads) k_pcg_update(int n, int nbf, cons
     __threadfence();
     const double e0 = warp_total(partE, gridDim.x, C_EPS), e1 = warp_total(partE, gridDim.x, C_EPSP);
     if (threadIdx.x == 0) {
-      out[0] = e0;
-      out[1] = e1;
+      const double m = (e0 < e1) ? e1 : e0;
+      const double eps = kElecAngToDebye * sqrt(m / (double)n);
+      const double previous = st->eps;
+      const int iter = st->iter + 1;
+      int status = FFXG_OK, cont = 1;
+      if (!(eps <= previous)) {
+        status = isfinite(eps) ? FFXG_ERR_SCF_DIVERGED : FFXG_ERR_NONFINITE;
+        cont = 0;
+      } else if (iter >= max_iter) {
+        status = FFXG_ERR_SCF_MAXITER;
+        cont = 0;
+      } else if (eps < polar_eps) {
+        cont = 0;
+      }
+      if (*flags & (FLAG_NBR_OVERFLOW | FLAG_EWALD_OVERFLOW | FLAG_PRECOND_OVERFLOW | FLAG_NONFINITE)) cont = 0;
+      st->eps = eps;
+      st->iter = iter;
+      st->status = status;
+      st->cont = cont;
       *counter = 0u;
+      if (use_cond) cudaGraphSetConditional(cond, (unsigned)cont);
     }
   }
 }
@@ -278,8 +311,42 @@ static void launch_precond(Handle &h) {
   if (h.mixed) precond<INIT, float2>(h); else precond<INIT, double2>(h);
 }
 
-int run_pcg(Handle &h) {
-  const int n = h.n;
+// One PCG step up to the stopping test: recip field of p, A p with its dot products, update.
+static void pcg_step(Handle &h, cudaGraphConditionalHandle cond, int use_cond) {
+  int tk = timer_begin(h, FFXG_STAGE_IND_RECIP);
+  launch_induced_recip(h, h.d_p, h.d_pP);
+  timer_end(h, tk);
+  tk = timer_begin(h, FFXG_STAGE_IND_FIELD);
+  launch_field<2>(h, h.d_p, h.d_pP, h.d_vec, h.d_vecP);
+  timer_end(h, tk);
+  tk = timer_begin(h, FFXG_STAGE_PCG_VECTOR);
+  k_pcg_update<<<kVecBlocks, kVecThreads, 0, h.stream>>>(h.n, kFieldBlocks, h.d_vec, h.d_vecP, h.d_p, h.d_pP, h.d_r,
+                                                         h.d_rP, h.d_uD, h.d_uP, h.d_part2, h.d_part2 + 8 * 2048,
+                                                         h.d_counter, h.d_pcg, h.prm.max_scf_iter, h.prm.polar_eps,
+                                                         h.d_flags, cond, use_cond);
+  timer_end(h, tk);
+  FFX_LAUNCHED(h);
+}
+
+// New search direction: z = M r (with r . z partials), then p = z + beta p.
+static void pcg_direction(Handle &h) {
+  int tk = timer_begin(h, FFXG_STAGE_PRECOND);
+  launch_precond<false>(h);
+  timer_end(h, tk);
+  tk = timer_begin(h, FFXG_STAGE_PCG_VECTOR);
+  k_pcg_p<<<kVecBlocks, kVecThreads, 0, h.stream>>>(h.n, kFieldBlocks, h.d_part2, h.d_zpre, h.d_zpreP, h.d_p, h.d_pP);
+  timer_end(h, tk);
+  FFX_LAUNCHED(h);
+}
+
+// The solve.  Directly (capture false): the host reads the device's stopping decision
+// after every update (24 bytes).  Under stream capture (capture true): the first step is
+// recorded in line and the rest as a conditional WHILE node whose body (direction, step)
+// the update kernel re-arms on the device, so the loop runs with no host round trip.
+// Either way the loop ends by max_scf_iter at the latest.
+int run_pcg(Handle &h, bool capture) {
+  k_pcg_reset<<<1, 1, 0, h.stream>>>(h.d_pcg);
+  FFX_LAUNCHED(h);
   // Field of the direct dipoles (u == u_dir at entry) gives the initial residual.
   int tk = timer_begin(h, FFXG_STAGE_IND_RECIP);
   launch_induced_recip(h, h.d_uD, h.d_uP);
@@ -290,40 +357,49 @@ int run_pcg(Handle &h) {
   tk = timer_begin(h, FFXG_STAGE_PRECOND);
   launch_precond<true>(h);
   timer_end(h, tk);
-  int iter = 0;
-  double eps = 100.0;
-  int status = FFXG_OK;
-  while (true) {
-    tk = timer_begin(h, FFXG_STAGE_IND_RECIP);
-    launch_induced_recip(h, h.d_p, h.d_pP);
-    timer_end(h, tk);
-    tk = timer_begin(h, FFXG_STAGE_IND_FIELD);
-    launch_field<2>(h, h.d_p, h.d_pP, h.d_vec, h.d_vecP);
-    timer_end(h, tk);
-    tk = timer_begin(h, FFXG_STAGE_PCG_VECTOR);
-    k_pcg_update<<<kVecBlocks, kVecThreads, 0, h.stream>>>(n, kFieldBlocks, h.d_vec, h.d_vecP, h.d_p, h.d_pP, h.d_r,
-                                                           h.d_rP, h.d_uD, h.d_uP, h.d_part2, h.d_part2 + 8 * 2048,
-                                                           h.d_counter, h.d_scalars);
-    timer_end(h, tk);
-    FFX_LAUNCHED(h);
-    cudaMemcpyAsync(h.h_scalars, h.d_scalars, 2 * sizeof(double), cudaMemcpyDeviceToHost, h.stream);
-    if (cudaStreamSynchronize(h.stream) != cudaSuccess) return FFXG_ERR_CUDA;
-    const double previous = eps;
-    eps = kElecAngToDebye * std::sqrt(std::max(h.h_scalars[0], h.h_scalars[1]) / (double)n);
-    iter++;
-    if (!(eps <= previous)) { status = std::isfinite(eps) ? FFXG_ERR_SCF_DIVERGED : FFXG_ERR_NONFINITE; break; }
-    if (iter >= h.prm.max_scf_iter) { status = FFXG_ERR_SCF_MAXITER; break; }
-    if (eps < h.prm.polar_eps) break;
-    tk = timer_begin(h, FFXG_STAGE_PRECOND);
-    launch_precond<false>(h);
-    timer_end(h, tk);
-    tk = timer_begin(h, FFXG_STAGE_PCG_VECTOR);
-    k_pcg_p<<<kVecBlocks, kVecThreads, 0, h.stream>>>(n, kFieldBlocks, h.d_part2, h.d_zpre, h.d_zpreP, h.d_p, h.d_pP);
-    timer_end(h, tk);
-    FFX_LAUNCHED(h);
+  if (!capture) {
+    while (true) {
+      pcg_step(h, 0, 0);
+      cudaMemcpyAsync(h.h_pcg, h.d_pcg, sizeof(PcgState), cudaMemcpyDeviceToHost, h.stream);
+      if (cudaStreamSynchronize(h.stream) != cudaSuccess) return FFXG_ERR_CUDA;
+      if (!h.h_pcg->cont) break;
+      pcg_direction(h);
+    }
+    h.scf_iter = h.h_pcg->iter;
+    return h.h_pcg->status;
   }
-  h.scf_iter = iter;
-  return status;
+  cudaStreamCaptureStatus cs;
+  cudaGraph_t g = nullptr;
+  const cudaGraphNode_t *deps = nullptr;
+  size_t ndeps = 0;
+  if (cudaStreamGetCaptureInfo(h.stream, &cs, nullptr, &g, &deps, &ndeps) != cudaSuccess ||
+      cs != cudaStreamCaptureStatusActive)
+    return FFXG_ERR_CUDA;
+  cudaGraphConditionalHandle cond;
+  if (cudaGraphConditionalHandleCreate(&cond, g, 0, cudaGraphCondAssignDefault) != cudaSuccess) return FFXG_ERR_CUDA;
+  pcg_step(h, cond, 1);
+  if (cudaStreamGetCaptureInfo(h.stream, &cs, nullptr, &g, &deps, &ndeps) != cudaSuccess) return FFXG_ERR_CUDA;
+  cudaGraphNodeParams cp = {};
+  cp.type = cudaGraphNodeTypeConditional;
+  cp.conditional.handle = cond;
+  cp.conditional.type = cudaGraphCondTypeWhile;
+  cp.conditional.size = 1;
+  cudaGraphNode_t node;
+  if (cudaGraphAddNode(&node, g, deps, ndeps, &cp) != cudaSuccess) return FFXG_ERR_CUDA;
+  if (cudaStreamUpdateCaptureDependencies(h.stream, &node, 1, cudaStreamSetCaptureDependencies) != cudaSuccess)
+    return FFXG_ERR_CUDA;
+  cudaGraph_t body = cp.conditional.phGraph_out[0];
+  if (cudaStreamBeginCaptureToGraph(h.side, body, nullptr, nullptr, 0, cudaStreamCaptureModeRelaxed) != cudaSuccess)
+    return FFXG_ERR_CUDA;
+  cudaStream_t main = h.stream;
+  h.stream = h.side;
+  const int64_t before = h.launches;
+  pcg_direction(h);
+  pcg_step(h, cond, 1);
+  h.graph_body_launches = h.launches - before;
+  h.stream = main;
+  if (cudaStreamEndCapture(h.side, &body) != cudaSuccess) return FFXG_ERR_CUDA;
+  return FFXG_OK;
 }
 
 }  // namespace ffx

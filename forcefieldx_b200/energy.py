@@ -168,5 +168,9 @@ class ForceFieldEnergy:
     def stream(self) -> int:
         return int(self.lib.ffxg_stream(self._h) or 0)
 
+    def set_graph_mode(self, on: bool) -> None:
+        """Replay the evaluation as one captured CUDA graph (default) or launch directly."""
+        self._check(self.lib.ffxg_set_graph_mode(self._h, 1 if on else 0))
+
     def launch_count(self) -> int:
         return int(self.lib.ffxg_last_launch_count(self._h))

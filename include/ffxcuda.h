@@ -215,6 +215,15 @@ enum {
 int ffxg_set_timing(ffxg_handle *h, int on);
 int ffxg_get_timings(ffxg_handle *h, double *ms, int64_t *launches, int n);
 
+/* Execution mode (no counterpart in the reference, which has no GPU path).  With graph
+ * mode on (the default) the first evaluation after the neighbour list exists captures
+ * the whole evaluation, the PCG loop included as a conditional while node that the
+ * solver re-arms on the device, and later evaluations replay it with one launch and
+ * one synchronisation.  Off: every kernel is launched directly and the host reads the
+ * solver's stopping decision after each iteration.  Results are the same either way;
+ * stage timing (ffxg_set_timing) always uses direct launches. */
+int ffxg_set_graph_mode(ffxg_handle *h, int on);
+
 /* Permanent-multipole reciprocal-space potential and energy without any device
  * allocation.  This entry point has no counterpart in the reference; it is for
  * callers that may not allocate device memory themselves or through this library:

@@ -127,3 +127,40 @@ def test_error_status_codes():
     with pytest.raises(EnergyException) as ei:
         ForceFieldEnergy(s, p)                                            # 22 = 2 * 11: radix 11 unsupported
     assert ei.value.status == 1
+
+
+@pytest.mark.parametrize("precision", [0, 1])
+def test_graph_replay_matches_direct_launches(precision):
+    """The captured graph (PCG loop as a device-side while node) gives the direct path's
+    results: bitwise in the mixed form, to FP64 rounding in the plain form (its mesh
+    spreading uses floating-point atomics)."""
+    s = water_box(6, 18.643, seed=5)
+    p = water_params(18.643, vdw_cutoff=7.0, ewald_cutoff=7.0, pme_grid=(20, 20, 20), precision=precision)
+    rng = np.random.default_rng(7)
+    xs = [s.xyz + rng.normal(0.0, 0.05, s.xyz.shape) for _ in range(3)]
+    res = {}
+    for mode in (True, False):
+        with ForceFieldEnergy(s, p) as ffe:
+            ffe.set_graph_mode(mode)
+            out = []
+            for x in [s.xyz] + xs:
+                e, g = ffe.energy_and_gradient(x)
+                out.append((ffe.terms.copy(), g.copy(), int(ffe.count("scf_iter"))))
+            res[mode] = out
+    for (ta, ga, ia), (tb, gb, ib) in zip(res[True], res[False]):
+        assert ia == ib
+        if precision == 1:
+            assert np.array_equal(ta, tb) and np.array_equal(ga, gb)
+        else:
+            assert np.max(np.abs(ta - tb) / np.maximum(np.abs(tb), 1.0)) < 1e-11
+            assert np.max(np.abs(ga - gb)) < 1e-9
+
+
+def test_graph_replay_reports_scf_errors():
+    s = water_box(6, 18.643, seed=2)
+    p = water_params(18.643, vdw_cutoff=7.0, ewald_cutoff=7.0, pme_grid=(20, 20, 20), max_scf_iter=2)
+    with ForceFieldEnergy(s, p) as ffe:
+        for _ in range(3):                      # the first call builds the list; later ones replay
+            with pytest.raises(EnergyException) as ei:
+                ffe.energy(s.xyz)
+            assert ei.value.status == 4         # SCF_MAXITER, decided on the device
