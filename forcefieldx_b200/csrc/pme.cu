@@ -225,34 +225,43 @@ __device__ __forceinline__ void mesh_add(double2 *, unsigned long long *gq, size
   atomicAdd(&gq[2 * idx + 1], to_fix(im));
 }
 
-// One warp per atom; lanes walk the 125 mesh points of the atom's support.
+// Wrap a support index (within one period of the mesh) into [0, m).
+__device__ __forceinline__ int wrap1(int v, int m) { return v < 0 ? v + m : (v >= m ? v - m : v); }
+
+// One warp per atom.  Lane l < 25 owns the (x, y) point (l % 5, l / 5) of the atom's
+// support and walks the five z layers, so the per-point work is the B-spline product and
+// the atomic add (no integer division in the loop).
 template <typename S>
 __global__ void k_spread_permanent(int n, const double *__restrict__ fm, const S *__restrict__ spl,
                                    const int *__restrict__ igrid, int nfx, int nfy, int nfz, double2 *grid,
                                    unsigned long long *gq) {
   const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const int lane = threadIdx.x & 31;
-  if (warp >= n) return;
+  if (warp >= n || lane >= 25) return;
   const int i = warp;
   const S *s = spl + (size_t)i * 3 * kOrder * 4;
   const S *sx = s, *sy = s + kOrder * 4, *sz = s + 2 * kOrder * 4;
-  const int i0 = igrid[i], j0 = igrid[n + i], k0 = igrid[2 * n + i];
+  const int a1 = lane % 5, a2 = lane / 5;
+  const int ii = wrap1(igrid[i] + 1 + a1, nfx), jj = wrap1(igrid[n + i] + 1 + a2, nfy);
+  const int k0 = igrid[2 * n + i] + 1;
   S f[10];
 #pragma unroll
   for (int j = 0; j < 10; j++) f[j] = (S)fm[j * n + i];
-  for (int p = lane; p < 125; p += 32) {
-    const int a1 = p % 5, a2 = (p / 5) % 5, a3 = p / 25;
+  const S x0 = sx[a1 * 4], x1 = sx[a1 * 4 + 1], x2 = sx[a1 * 4 + 2];
+  const S u0 = sy[a2 * 4], u1 = sy[a2 * 4 + 1], u2 = sy[a2 * 4 + 2];
+  const size_t row = (size_t)jj * nfx + ii;
+#pragma unroll
+  for (int a3 = 0; a3 < 5; a3++) {
     const S v0 = sz[a3 * 4], v1 = sz[a3 * 4 + 1], v2 = sz[a3 * 4 + 2];
-    const S u0 = sy[a2 * 4], u1 = sy[a2 * 4 + 1], u2 = sy[a2 * 4 + 2];
     const S c0dz1qzz2 = f[t000] * v0 + f[t001] * v1 + f[t002] * v2;
     const S dy0qyz1 = f[t010] * v0 + f[t011] * v1;
     const S dx0qxz1 = f[t100] * v0 + f[t101] * v1;
     const S term0 = fma(c0dz1qzz2, u0, fma(dy0qyz1, u1, f[t020] * v0 * u2));
     const S term1 = fma(dx0qxz1, u0, f[t110] * v0 * u1);
     const S term2 = f[t200] * v0 * u0;
-    const S val = fma(sx[a1 * 4], term0, fma(sx[a1 * 4 + 1], term1, sx[a1 * 4 + 2] * term2));
-    const int ii = jmod(i0 + 1 + a1, nfx), jj = jmod(j0 + 1 + a2, nfy), kk = jmod(k0 + 1 + a3, nfz);
-    mesh_add(grid, gq, ((size_t)kk * nfy + jj) * nfx + ii, val);
+    const S val = fma(x0, term0, fma(x1, term1, x2 * term2));
+    const int kk = wrap1(k0 + a3, nfz);
+    mesh_add(grid, gq, (size_t)kk * nfy * nfx + row, val);
   }
 }
 
@@ -262,11 +271,13 @@ __global__ void k_spread_induced(int n, const double *__restrict__ ud, const dou
                                  int nfz, double2 *grid, unsigned long long *gq, PmeConst pc) {
   const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const int lane = threadIdx.x & 31;
-  if (warp >= n) return;
+  if (warp >= n || lane >= 25) return;
   const int i = warp;
   const S *s = spl + (size_t)i * 3 * kOrder * 4;
   const S *sx = s, *sy = s + kOrder * 4, *sz = s + 2 * kOrder * 4;
-  const int i0 = igrid[i], j0 = igrid[n + i], k0 = igrid[2 * n + i];
+  const int a1 = lane % 5, a2 = lane / 5;
+  const int ii = wrap1(igrid[i] + 1 + a1, nfx), jj = wrap1(igrid[n + i] + 1 + a2, nfy);
+  const int k0 = igrid[2 * n + i] + 1;
   S u[3], q[3];
   const double c[3] = {ud[i], ud[n + i], ud[2 * n + i]};
   const double cp[3] = {up[i], up[n + i], up[2 * n + i]};
@@ -275,16 +286,19 @@ __global__ void k_spread_induced(int n, const double *__restrict__ ud, const dou
     u[a] = (S)(pc.afrac[a][0] * c[0] + pc.afrac[a][1] * c[1] + pc.afrac[a][2] * c[2]);
     q[a] = (S)(pc.afrac[a][0] * cp[0] + pc.afrac[a][1] * cp[1] + pc.afrac[a][2] * cp[2]);
   }
-  for (int p = lane; p < 125; p += 32) {
-    const int a1 = p % 5, a2 = (p / 5) % 5, a3 = p / 25;
+  const S x0 = sx[a1 * 4], x1 = sx[a1 * 4 + 1];
+  const S u0 = sy[a2 * 4], u1 = sy[a2 * 4 + 1];
+  // Per (x, y) point the z-layer value is  v0 * A + v1 * B  for each set.
+  const S Ad = x0 * u[1] * u1 + x1 * u[0] * u0, Bd = x0 * u[2] * u0;
+  const S Ap = x0 * q[1] * u1 + x1 * q[0] * u0, Bp = x0 * q[2] * u0;
+  const size_t row = (size_t)jj * nfx + ii;
+#pragma unroll
+  for (int a3 = 0; a3 < 5; a3++) {
     const S v0 = sz[a3 * 4], v1 = sz[a3 * 4 + 1];
-    const S u0 = sy[a2 * 4], u1 = sy[a2 * 4 + 1];
-    const S t0 = fma(u[2] * v1, u0, u[1] * v0 * u1), t1 = u[0] * v0 * u0;
-    const S tp0 = fma(q[2] * v1, u0, q[1] * v0 * u1), tp1 = q[0] * v0 * u0;
-    const S re = fma(sx[a1 * 4], t0, sx[a1 * 4 + 1] * t1);
-    const S im = fma(sx[a1 * 4], tp0, sx[a1 * 4 + 1] * tp1);
-    const int ii = jmod(i0 + 1 + a1, nfx), jj = jmod(j0 + 1 + a2, nfy), kk = jmod(k0 + 1 + a3, nfz);
-    mesh_add(grid, gq, ((size_t)kk * nfy + jj) * nfx + ii, re, im);
+    const S re = fma(v0, Ad, v1 * Bd);
+    const S im = fma(v0, Ap, v1 * Bp);
+    const int kk = wrap1(k0 + a3, nfz);
+    mesh_add(grid, gq, (size_t)kk * nfy * nfx + row, re, im);
   }
 }
 
@@ -435,6 +449,82 @@ __global__ void __launch_bounds__(256) k_fft_axis(typename Vec2<S>::type *grid, 
   }
 }
 
+// Fixed-length line FFT (length LEN known at compile time, L lines per CTA, 256
+// threads).  The same Stockham passes as k_fft_axis, but every index division is by a
+// constant and the twiddle table sits in shared memory: at 64^3 the runtime-length
+// kernel spends most of its issue slots on integer division.
+__host__ __device__ constexpr int plan_radix(int len, int st) {
+  int m = len;
+  const int f[5] = {4, 2, 3, 5, 7};
+  for (int q = 0; q < 5; q++)
+    while (m % f[q] == 0) {
+      if (st == 0) return f[q];
+      st--;
+      m /= f[q];
+    }
+  return 0;
+}
+
+template <int LEN, int ST, int NS, int L, typename S>
+__device__ __forceinline__ void fixed_stages(typename Vec2<S>::type *&in, typename Vec2<S>::type *&out,
+                                             const typename Vec2<S>::type *tw, int sg) {
+  constexpr int R = plan_radix(LEN, ST);
+  if constexpr (R != 0) {
+    constexpr int NB = LEN / R;
+    for (int t = threadIdx.x; t < NB * L; t += 256) {
+      const int l = t % L, j = t / L;
+      fft_butterfly<R, S>(in, out, j, l, L, NB, NS, LEN, sg, tw);
+    }
+    __syncthreads();
+    typename Vec2<S>::type *tmp = in;
+    in = out;
+    out = tmp;
+    fixed_stages<LEN, ST + 1, NS * R, L, S>(in, out, tw, sg);
+  }
+}
+
+template <int LEN, int L, bool FUSE_G, typename S, bool FROMQ>
+__global__ void __launch_bounds__(256) k_fft_fixed(typename Vec2<S>::type *grid, FftAxis ax, int sign,
+                                                   const typename Vec2<S>::type *__restrict__ twg,
+                                                   const S *__restrict__ G, int gnx, int gny,
+                                                   unsigned long long *gq) {
+  using V2 = typename Vec2<S>::type;
+  __shared__ V2 buf[2][LEN * L];
+  __shared__ V2 tw[LEN];
+  for (int t = threadIdx.x; t < LEN; t += 256) tw[t] = twg[t];
+  const int gi = blockIdx.x % ax.groups_inner, go = blockIdx.x / ax.groups_inner;
+  const size_t base = (size_t)gi * ax.group_step_inner + (size_t)go * ax.group_step_outer;
+  const bool contiguous = (ax.stride == 1);
+  for (int t = threadIdx.x; t < LEN * L; t += 256) {
+    const int l = contiguous ? t / LEN : t % L, j = contiguous ? t % LEN : t / L;
+    const size_t g = base + (size_t)l * ax.line_step + (size_t)j * ax.stride;
+    if (FROMQ) {
+      const longlong2 q = reinterpret_cast<const longlong2 *>(gq)[g];
+      reinterpret_cast<longlong2 *>(gq)[g] = make_longlong2(0, 0);
+      buf[0][j * L + l] = mk2<S>((S)q.x * (S)kMeshUnfix, (S)q.y * (S)kMeshUnfix);
+    } else {
+      buf[0][j * L + l] = grid[g];
+    }
+  }
+  __syncthreads();
+  V2 *in = buf[0], *out = buf[1];
+  fixed_stages<LEN, 0, 1, L, S>(in, out, tw, sign);
+  if (FUSE_G) {
+    for (int t = threadIdx.x; t < LEN * L; t += 256) {
+      const int l = t % L, j = t / L;
+      const S gv = G[(size_t)j * gnx * gny + base + (size_t)l * ax.line_step];
+      in[j * L + l].x *= gv;
+      in[j * L + l].y *= gv;
+    }
+    __syncthreads();
+    fixed_stages<LEN, 0, 1, L, S>(in, out, tw, -sign);
+  }
+  for (int t = threadIdx.x; t < LEN * L; t += 256) {
+    const int l = contiguous ? t / LEN : t % L, j = contiguous ? t % LEN : t / L;
+    grid[base + (size_t)l * ax.line_step + (size_t)j * ax.stride] = in[j * L + l];
+  }
+}
+
 // ---------------------------------------------------------------------------
 // Potential and derivatives at each atom (20 fractional terms -> Cartesian).
 template <int NT, typename S>
@@ -546,31 +636,38 @@ __global__ void k_phi_field(int n, const S *__restrict__ spl, const int *__restr
   const int i = warp;
   const S *sp = spl + (size_t)i * 3 * kOrder * 4;
   const S *sx = sp, *sy = sp + kOrder * 4, *sz = sp + 2 * kOrder * 4;
-  const int i0 = igrid[i], j0 = igrid[n + i], k0 = igrid[2 * n + i];
   S rx = 0, ry = 0, rz = 0, ix = 0, iy = 0, iz = 0;
-  for (int p = lane; p < 125; p += 32) {
-    const int a1 = p % 5, a2 = (p / 5) % 5, a3 = p / 25;
-    const int ii = jmod(i0 + 1 + a1, nfx), jj = jmod(j0 + 1 + a2, nfy), kk = jmod(k0 + 1 + a3, nfz);
-    const auto g = grid[((size_t)kk * nfy + jj) * nfx + ii];
+  if (lane < 25) {
+    // Lane owns the (x, y) point (lane % 5, lane / 5) and walks the five z layers.
+    const int a1 = lane % 5, a2 = lane / 5;
+    const int ii = wrap1(igrid[i] + 1 + a1, nfx), jj = wrap1(igrid[n + i] + 1 + a2, nfy);
+    const int k0 = igrid[2 * n + i] + 1;
     const S x0 = sx[a1 * 4], x1 = sx[a1 * 4 + 1];
     const S y0 = sy[a2 * 4], y1 = sy[a2 * 4 + 1];
-    const S z0 = sz[a3 * 4], z1 = sz[a3 * 4 + 1];
-    const S wx = x1 * y0 * z0, wy = x0 * y1 * z0, wz = x0 * y0 * z1;
-    rx = fma(g.x, wx, rx); ry = fma(g.x, wy, ry); rz = fma(g.x, wz, rz);
-    ix = fma(g.y, wx, ix); iy = fma(g.y, wy, iy); iz = fma(g.y, wz, iz);
+    const S w10 = x1 * y0, w01 = x0 * y1, w00 = x0 * y0;
+    const auto *row = grid + (size_t)jj * nfx + ii;
+    S gr[5], gi[5];
+#pragma unroll
+    for (int a3 = 0; a3 < 5; a3++) {
+      const auto g = row[(size_t)wrap1(k0 + a3, nfz) * nfy * nfx];
+      gr[a3] = g.x;
+      gi[a3] = g.y;
+    }
+#pragma unroll
+    for (int a3 = 0; a3 < 5; a3++) {
+      const S z0 = sz[a3 * 4], z1 = sz[a3 * 4 + 1];
+      const S wx = w10 * z0, wy = w01 * z0, wz = w00 * z1;
+      rx = fma(gr[a3], wx, rx); ry = fma(gr[a3], wy, ry); rz = fma(gr[a3], wz, rz);
+      ix = fma(gi[a3], wx, ix); iy = fma(gi[a3], wy, iy); iz = fma(gi[a3], wz, iz);
+    }
   }
   const double Rx = warp_sum((double)rx), Ry = warp_sum((double)ry), Rz = warp_sum((double)rz);
   const double Ix = warp_sum((double)ix), Iy = warp_sum((double)iy), Iz = warp_sum((double)iz);
   if (lane < 2) {
-    const double f[3] = {lane == 0 ? Rx : Ix, lane == 0 ? Ry : Iy, lane == 0 ? Rz : Iz};
+    const double f0 = lane == 0 ? Rx : Ix, f1 = lane == 0 ? Ry : Iy, f2 = lane == 0 ? Rz : Iz;
     double *out = lane == 0 ? cphiR : cphiI;
 #pragma unroll
-    for (int j = 1; j < 4; j++) {
-      double v = 0.0;
-#pragma unroll
-      for (int k = 1; k < 4; k++) v = fma(pc.tfm[j][k], f[k - 1], v);
-      out[j * n + i] = v;
-    }
+    for (int j = 1; j < 4; j++) out[j * n + i] = fma(pc.tfm[j][1], f0, fma(pc.tfm[j][2], f1, pc.tfm[j][3] * f2));
   }
 }
 
@@ -830,6 +927,19 @@ static void fft_convolution(Handle &h, typename Vec2<S>::type *grid, const typen
     const int blocks = a.groups_inner * outer;
     const size_t smem = 2 * (size_t)a.len * a.L * sizeof(typename Vec2<S>::type);
     const auto *tw = twiddle + (size_t)d * maxn;
+    if (a.len == 64 && a.L == 16) {
+      if (fuse)
+        k_fft_fixed<64, 16, true, S, false><<<blocks, 256, 0, h.stream>>>(grid, a, sign, tw, influence, nfx, nfy,
+                                                                          nullptr);
+      else if (fromq)
+        k_fft_fixed<64, 16, false, S, true><<<blocks, 256, 0, h.stream>>>(grid, a, sign, tw, nullptr, nfx, nfy,
+                                                                          h.d_gridq);
+      else
+        k_fft_fixed<64, 16, false, S, false><<<blocks, 256, 0, h.stream>>>(grid, a, sign, tw, nullptr, nfx, nfy,
+                                                                           nullptr);
+      FFX_LAUNCHED(h);
+      return;
+    }
     if (fuse)
       k_fft_axis<true, S, false><<<blocks, 256, smem, h.stream>>>(grid, a, sign, tw, influence, nfx, nfy, nullptr);
     else if (fromq)
