@@ -95,6 +95,38 @@ __device__ __forceinline__ T warp_sum(T v) {
   return v;
 }
 
+// Packed per-atom source records for the field gathers: T[8] per atom = (D xyz, CR xyz,
+// pad), T = double (plain form) or float (mixed form), so a neighbour costs one 64- or
+// 32-byte record instead of six scattered loads.  Positions are packed as double2
+// pairs (x, y), (z, 0).
+template <typename T>
+__device__ __forceinline__ void put_rec(T *rec, int i, double d0, double d1, double d2, double p0, double p1,
+                                        double p2) {
+  T *q = rec + 8 * (size_t)i;
+  if constexpr (sizeof(T) == 8) {
+    reinterpret_cast<double2 *>(q)[0] = make_double2(d0, d1);
+    reinterpret_cast<double2 *>(q)[1] = make_double2(d2, p0);
+    reinterpret_cast<double2 *>(q)[2] = make_double2(p1, p2);
+  } else {
+    reinterpret_cast<float4 *>(q)[0] = make_float4((float)d0, (float)d1, (float)d2, (float)p0);
+    reinterpret_cast<float2 *>(q)[2] = make_float2((float)p1, (float)p2);
+  }
+}
+
+template <typename T>
+__device__ __forceinline__ void get_rec(const T *__restrict__ rec, int k, T *v) {
+  const T *q = rec + 8 * (size_t)k;
+  if constexpr (sizeof(T) == 8) {
+    const double2 a = reinterpret_cast<const double2 *>(q)[0], b = reinterpret_cast<const double2 *>(q)[1],
+                  c = reinterpret_cast<const double2 *>(q)[2];
+    v[0] = a.x; v[1] = a.y; v[2] = b.x; v[3] = b.y; v[4] = c.x; v[5] = c.y;
+  } else {
+    const float4 a = reinterpret_cast<const float4 *>(q)[0];
+    const float2 b = reinterpret_cast<const float2 *>(q)[2];
+    v[0] = a.x; v[1] = a.y; v[2] = a.z; v[3] = a.w; v[4] = b.x; v[5] = b.y;
+  }
+}
+
 // PME transforms of one handle (passed to kernels by value).
 struct PmeConst {
   double tmm[10][10];   // ReciprocalSpace.transformMultipoleMatrix
@@ -179,6 +211,11 @@ struct Handle {
   // PCG vectors [3][n]
   double *d_r = nullptr, *d_rP = nullptr, *d_zpre = nullptr, *d_zpreP = nullptr, *d_p = nullptr, *d_pP = nullptr;
   double *d_vec = nullptr, *d_vecP = nullptr;
+  // Packed gather records: positions (x, y), (z, 0) per atom, and the field source
+  // dipoles of the PCG fields, [n][8] of double (plain) or float (mixed): d_recF holds
+  // the dipoles whose field is taken (u, then p), d_recP holds alpha r.
+  double2 *d_pos = nullptr;
+  void *d_recF = nullptr, *d_recP = nullptr;
   double *d_partials = nullptr;               // block partial sums [nblk][8]
   double *d_scalars = nullptr;                // PCG scalars on device
   double *h_scalars = nullptr;                // pinned mirror
@@ -187,9 +224,9 @@ struct Handle {
   double2 *d_grid = nullptr;
   double *d_influence = nullptr;
   double2 *d_twiddle = nullptr;               // per-axis twiddle tables (3 x max n)
-  // Mixed form: d_grid and d_spl hold float2 / float data; spreading accumulates in
-  // the 64-bit fixed-point mesh d_gridq [points][2].
-  unsigned long long *d_gridq = nullptr;
+  // Mixed form: d_spl holds float data; spreading accumulates (exactly) in the double
+  // mesh d_grid and the FFT and interpolation run on the FP32 mesh d_gridf.
+  float2 *d_gridf = nullptr;
   float *d_influencef = nullptr;
   float2 *d_twiddlef = nullptr;
   PmeConst pc{};

@@ -223,7 +223,10 @@ static int create_impl(const ffxg_system *s, const ffxg_params *p, Handle &h) {
   CK(dalloc(&h.d_fieldD, 3 * N)); CK(dalloc(&h.d_fieldP, 3 * N));
   CK(dalloc(&h.d_uD, 3 * N)); CK(dalloc(&h.d_uP, 3 * N)); CK(dalloc(&h.d_udirD, 3 * N)); CK(dalloc(&h.d_udirP, 3 * N));
   CK(dalloc(&h.d_r, 3 * N)); CK(dalloc(&h.d_rP, 3 * N)); CK(dalloc(&h.d_zpre, 3 * N)); CK(dalloc(&h.d_zpreP, 3 * N));
-  CK(dalloc(&h.d_p, 3 * N)); CK(dalloc(&h.d_pP, 3 * N)); CK(dalloc(&h.d_vec, 3 * N)); CK(dalloc(&h.d_vecP, 3 * N));
+  CK(dalloc(&h.d_p, 3 * N)); CK(dalloc(&h.d_pP, 3 * N));
+  CK(dalloc(&h.d_pos, 2 * N));
+  CK(cudaMalloc(&h.d_recF, 8 * N * sizeof(double)));
+  CK(cudaMalloc(&h.d_recP, 8 * N * sizeof(double))); CK(dalloc(&h.d_vec, 3 * N)); CK(dalloc(&h.d_vecP, 3 * N));
   const size_t nparts = std::max<size_t>((size_t)nblocks(n, 256) * 8, 148 * 16) + 64;
   CK(dalloc(&h.d_partials, nparts));
   CK(dalloc(&h.d_part2, 4096 * 8));
@@ -238,8 +241,7 @@ static int create_impl(const ffxg_system *s, const ffxg_params *p, Handle &h) {
   CK(dalloc(&h.d_grid, ng)); CK(dalloc(&h.d_influence, ng));
   CK(dalloc(&h.d_twiddle, 3 * (size_t)std::max(nfx, std::max(nfy, nfz))));
   if (h.mixed) {
-    CK(dalloc(&h.d_gridq, 2 * ng));
-    CK(cudaMemset(h.d_gridq, 0, 2 * ng * sizeof(unsigned long long)));
+    CK(dalloc(&h.d_gridf, ng));
     CK(dalloc(&h.d_influencef, ng));
     CK(dalloc(&h.d_twiddlef, 3 * (size_t)std::max(nfx, std::max(nfy, nfz))));
   }
@@ -316,9 +318,9 @@ static void free_all(Handle &h) {
                   h.d_nbr_cnt, h.d_ewl, h.d_ewl_cnt, h.d_prl, h.d_prl_cnt, h.d_gm, h.d_fm, h.d_spl, h.d_igrid,
                   h.d_cphi, h.d_fphi, h.d_cphiI, h.d_fphiI, h.d_cphiP, h.d_fphiP, h.d_fieldD, h.d_fieldP, h.d_uD,
                   h.d_uP, h.d_udirD, h.d_udirP, h.d_r, h.d_rP, h.d_zpre, h.d_zpreP, h.d_p, h.d_pP, h.d_vec, h.d_vecP,
-                  h.d_partials, h.d_scalars, h.d_grid, h.d_influence, h.d_twiddle, h.d_gridq, h.d_influencef, h.d_twiddlef, h.d_grad, h.d_torque, h.d_gred,
+                  h.d_partials, h.d_scalars, h.d_grid, h.d_influence, h.d_twiddle, h.d_gridf, h.d_influencef, h.d_twiddlef, h.d_grad, h.d_torque, h.d_gred,
                   h.d_eatom, h.d_catom, h.d_result, h.d_cresult, h.d_flags, h.d_xyz_in, h.d_grad_out,
-                  h.d_coefE, h.d_coefP, h.d_part2, h.d_counter};
+                  h.d_coefE, h.d_coefP, h.d_part2, h.d_counter, h.d_pos, h.d_recF, h.d_recP};
   for (void *q : ptrs)
     if (q) cudaFree(q);
   if (h.h_scalars) cudaFreeHost(h.h_scalars);

@@ -20,12 +20,15 @@ struct CellOffsets {
 // without contraction like Java (VanDerWaals.java:1521-1527).
 __global__ void k_set_coordinates(int n, const double *__restrict__ xyz, const int *__restrict__ redp,
                                   const double *__restrict__ redf, double *x, double *y, double *z,
-                                  double *rx, double *ry, double *rz) {
+                                  double *rx, double *ry, double *rz, double2 *pos) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
-  x[i] = xyz[3 * i];
-  y[i] = xyz[3 * i + 1];
-  z[i] = xyz[3 * i + 2];
+  const double a = xyz[3 * i], b = xyz[3 * i + 1], c = xyz[3 * i + 2];
+  x[i] = a;
+  y[i] = b;
+  z[i] = c;
+  pos[2 * i] = make_double2(a, b);
+  pos[2 * i + 1] = make_double2(c, 0.0);
 }
 
 __global__ void k_reduce_coordinates(int n, const double *__restrict__ x, const double *__restrict__ y,
@@ -206,7 +209,7 @@ __global__ void k_list_done(int n, double *refx, double *refy, double *refz, con
 void launch_set_coordinates(Handle &h, const double *d_xyz) {
   const int n = h.n;
   k_set_coordinates<<<nblocks(n, 256), 256, 0, h.stream>>>(n, d_xyz, h.d_redp, h.d_redf, h.d_x, h.d_y, h.d_z,
-                                                            h.d_rx, h.d_ry, h.d_rz);
+                                                            h.d_rx, h.d_ry, h.d_rz, h.d_pos);
   FFX_LAUNCHED(h);
   const double hb = 0.5 * h.prm.list_buffer;
   k_reduce_coordinates<<<nblocks(n, 256), 256, 0, h.stream>>>(n, h.d_x, h.d_y, h.d_z, h.d_redp, h.d_redf, h.d_rx,

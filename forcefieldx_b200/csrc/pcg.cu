@@ -54,57 +54,69 @@ __device__ __forceinline__ void block_store(const double *v, double *part, int c
   }
 }
 
+// Contribution of one neighbour: -A u_k + B (u_k . r) r for both sets.
+template <typename C2, typename T>
+__device__ __forceinline__ void field_term(double xi, double yi, double zi, double2 qa, double2 qb, C2 c,
+                                           const T *s, const Box &bx, T *acc) {
+  double xd = __dsub_rn(qa.x, xi), yd = __dsub_rn(qa.y, yi), zd = __dsub_rn(qb.x, zi);
+  image_exact(xd, yd, zd, bx);
+  const T xr = (T)xd, yr = (T)yd, zr = (T)zd, A = (T)c.x, B = (T)c.y;
+  const T ukr = B * (s[0] * xr + s[1] * yr + s[2] * zr);
+  const T pkr = B * (s[3] * xr + s[4] * yr + s[5] * zr);
+  acc[0] += -A * s[0] + ukr * xr; acc[1] += -A * s[1] + ukr * yr; acc[2] += -A * s[2] + ukr * zr;
+  acc[3] += -A * s[3] + pkr * xr; acc[4] += -A * s[4] + pkr * yr; acc[5] += -A * s[5] + pkr * zr;
+}
+
 // Dipole field at atom i from the cached coefficient row (warp cooperative).  C2 is
-// double2 (plain form) or float2 (mixed form: FP32 coefficients, FP64 accumulation).
-template <typename C2>
-__device__ __forceinline__ void coef_field(int i, int n, const double *__restrict__ x, const double *__restrict__ y,
-                                           const double *__restrict__ z, const Box &bx, const int *__restrict__ lst,
-                                           const int *__restrict__ lst_cnt, int cap,
-                                           const C2 *__restrict__ coef, const double *__restrict__ ud,
-                                           const double *__restrict__ up, const double *__restrict__ scale_by,
-                                           double *f) {
+// double2 (plain form) or float2 (mixed form: FP32 coefficients and sources, FP64
+// reduction).  Each lane handles entries a and a + 32 together so that both entries'
+// loads are in flight at once; the summation order stays a, a + 32, a + 64, ...
+template <typename C2, typename T>
+__device__ __forceinline__ void coef_field(int i, const double2 *__restrict__ pos, const Box &bx,
+                                           const int *__restrict__ lst, const int *__restrict__ lst_cnt, int cap,
+                                           const C2 *__restrict__ coef, const T *__restrict__ rec, double *f) {
   const int lane = threadIdx.x & 31;
-  const double xi = x[i], yi = y[i], zi = z[i];
-  double fx = 0, fy = 0, fz = 0, px = 0, py = 0, pz = 0;
+  const double2 pa = pos[2 * i], pb = pos[2 * i + 1];
+  T acc[6] = {0, 0, 0, 0, 0, 0};
   const int cnt = min(lst_cnt[i], cap);
   const int *row = lst + (size_t)i * cap;
   const C2 *crow = coef + (size_t)i * cap;
-  for (int a = lane; a < cnt; a += 32) {
-    const int k = row[a];
-    const C2 cc = crow[a];
-    const double2 c = make_double2((double)cc.x, (double)cc.y);
-    double xr = __dsub_rn(x[k], xi), yr = __dsub_rn(y[k], yi), zr = __dsub_rn(z[k], zi);
-    image_exact(xr, yr, zr, bx);
-    const double sk = scale_by ? scale_by[k] : 1.0;
-    const double ukx = sk * ud[k], uky = sk * ud[n + k], ukz = sk * ud[2 * n + k];
-    const double pkx = sk * up[k], pky = sk * up[n + k], pkz = sk * up[2 * n + k];
-    const double ukr = c.y * (ukx * xr + uky * yr + ukz * zr);
-    const double pkr = c.y * (pkx * xr + pky * yr + pkz * zr);
-    fx += -c.x * ukx + ukr * xr; fy += -c.x * uky + ukr * yr; fz += -c.x * ukz + ukr * zr;
-    px += -c.x * pkx + pkr * xr; py += -c.x * pky + pkr * yr; pz += -c.x * pkz + pkr * zr;
+  for (int a = lane; a < cnt; a += 64) {
+    const bool two = a + 32 < cnt;
+    const int k0 = row[a];
+    const int k1 = two ? row[a + 32] : k0;
+    const C2 c0 = crow[a];
+    const C2 c1 = two ? crow[a + 32] : c0;
+    const double2 q0a = pos[2 * k0], q0b = pos[2 * k0 + 1];
+    const double2 q1a = pos[2 * k1], q1b = pos[2 * k1 + 1];
+    T s0[6], s1[6];
+    get_rec(rec, k0, s0);
+    get_rec(rec, k1, s1);
+    field_term(pa.x, pa.y, pb.x, q0a, q0b, c0, s0, bx, acc);
+    if (two) field_term(pa.x, pa.y, pb.x, q1a, q1b, c1, s1, bx, acc);
   }
-  f[0] = warp_sum(fx); f[1] = warp_sum(fy); f[2] = warp_sum(fz);
-  f[3] = warp_sum(px); f[4] = warp_sum(py); f[5] = warp_sum(pz);
+#pragma unroll
+  for (int q = 0; q < 6; q++) f[q] = warp_sum((double)acc[q]);
 }
 
-// MODE 0: field of (ud, up) into outD/outP (used for the final field of the solution).
-// MODE 1: initial residual r = (u_dir - u) / alpha + E(u) with u == u_dir (InitResidualRegion).
+// MODE 1: initial residual r = (u_dir - u) / alpha + E(u) with u == u_dir (InitResidualRegion);
+//         also writes the preconditioner source record alpha r.
 // MODE 2: vec = p / alpha - E(p) and partials of p . vec and r . z (UpdateApLoop).
-template <int MODE, typename C2>
+template <int MODE, typename C2, typename T>
 __global__ void __launch_bounds__(kFieldThreads) k_pcg_field(
-    int n, const double *__restrict__ x, const double *__restrict__ y, const double *__restrict__ z, Box bx,
-    const int *__restrict__ ewl, const int *__restrict__ ewl_cnt, int capE, const C2 *__restrict__ coefE,
-    const double *__restrict__ ud, const double *__restrict__ up, const double *__restrict__ cphiD,
-    const double *__restrict__ cphiP, double aewald3, const double *__restrict__ polar,
-    const double *__restrict__ udirD, const double *__restrict__ udirP, const double *__restrict__ r,
-    const double *__restrict__ rP, const double *__restrict__ zz, const double *__restrict__ zP, double *outD,
-    double *outP, double *part) {
+    int n, const double2 *__restrict__ pos, Box bx, const int *__restrict__ ewl, const int *__restrict__ ewl_cnt,
+    int capE, const C2 *__restrict__ coefE, const T *__restrict__ rec, const double *__restrict__ ud,
+    const double *__restrict__ up, const double *__restrict__ cphiD, const double *__restrict__ cphiP,
+    double aewald3, const double *__restrict__ polar, const double *__restrict__ udirD,
+    const double *__restrict__ udirP, const double *__restrict__ r, const double *__restrict__ rP,
+    const double *__restrict__ zz, const double *__restrict__ zP, double *outD, double *outP, T *recP,
+    double *part) {
   const int lane = threadIdx.x & 31;
   const int wstride = gridDim.x * (blockDim.x >> 5);
   double acc[4] = {0, 0, 0, 0};
   for (int i = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5); i < n; i += wstride) {
     double f[6];
-    coef_field(i, n, x, y, z, bx, ewl, ewl_cnt, capE, coefE, ud, up, nullptr, f);
+    coef_field(i, pos, bx, ewl, ewl_cnt, capE, coefE, rec, f);
     if (lane == 0) {
       for (int d = 0; d < 3; d++) {
         f[d] += aewald3 * ud[d * n + i] - cphiD[(1 + d) * n + i];
@@ -113,14 +125,16 @@ __global__ void __launch_bounds__(kFieldThreads) k_pcg_field(
       const double a = polar[i];
       const bool ok = a > 0.0;
       const double ip = ok ? 1.0 / a : 0.0;
+      double nr[6];
       for (int d = 0; d < 3; d++) {
         const size_t j = (size_t)d * n + i;
-        if (MODE == 0) {
-          outD[j] = f[d];
-          outP[j] = f[3 + d];
-        } else if (MODE == 1) {
-          outD[j] = ok ? (udirD[j] - ud[j]) * ip + f[d] : 0.0;
-          outP[j] = ok ? (udirP[j] - up[j]) * ip + f[3 + d] : 0.0;
+        if (MODE == 1) {
+          const double rv = ok ? (udirD[j] - ud[j]) * ip + f[d] : 0.0;
+          const double rp = ok ? (udirP[j] - up[j]) * ip + f[3 + d] : 0.0;
+          outD[j] = rv;
+          outP[j] = rp;
+          nr[d] = a * rv;
+          nr[3 + d] = a * rp;
         } else {
           const double vv = ok ? ud[j] * ip - f[d] : 0.0;
           const double vp = ok ? up[j] * ip - f[3 + d] : 0.0;
@@ -132,27 +146,30 @@ __global__ void __launch_bounds__(kFieldThreads) k_pcg_field(
           acc[3] += rP[j] * zP[j];
         }
       }
+      if (MODE == 1) put_rec(recP, i, nr[0], nr[1], nr[2], nr[3], nr[4], nr[5]);
     }
   }
   if (MODE == 2) block_store<4>(acc, part, C_PAP);
 }
 
 // z = alpha (E_precond(alpha r) + s r) (InitConjugateRegion / UpdatePreconditionerLoop);
-// INIT also sets p = z, otherwise the partials of r . z_new are stored.
-template <bool INIT, typename C2>
+// INIT also sets p = z (and its source record), otherwise the partials of r . z_new are
+// stored.  The source record holds alpha r.
+template <bool INIT, typename C2, typename T>
 __global__ void __launch_bounds__(kFieldThreads) k_pcg_precond(
-    int n, const double *__restrict__ x, const double *__restrict__ y, const double *__restrict__ z, Box bx,
-    const int *__restrict__ prl, const int *__restrict__ prl_cnt, int capP, const C2 *__restrict__ coefP,
-    const double *__restrict__ polar, const double *__restrict__ r, const double *__restrict__ rP, double s,
-    double *zz, double *zP, double *p, double *pP, double *part) {
+    int n, const double2 *__restrict__ pos, Box bx, const int *__restrict__ prl, const int *__restrict__ prl_cnt,
+    int capP, const C2 *__restrict__ coefP, const T *__restrict__ recP, const double *__restrict__ polar,
+    const double *__restrict__ r, const double *__restrict__ rP, double s, double *zz, double *zP, double *p,
+    double *pP, T *recF, double *part) {
   const int lane = threadIdx.x & 31;
   const int wstride = gridDim.x * (blockDim.x >> 5);
   double acc[2] = {0, 0};
   for (int i = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5); i < n; i += wstride) {
     double f[6];
-    coef_field(i, n, x, y, z, bx, prl, prl_cnt, capP, coefP, r, rP, polar, f);
+    coef_field(i, pos, bx, prl, prl_cnt, capP, coefP, recP, f);
     if (lane == 0) {
       const double a = polar[i];
+      double nz[6];
       for (int d = 0; d < 3; d++) {
         const size_t j = (size_t)d * n + i;
         const double vz = a * (f[d] + s * r[j]);
@@ -163,9 +180,12 @@ __global__ void __launch_bounds__(kFieldThreads) k_pcg_precond(
           p[j] = vz;
           pP[j] = vp;
         }
+        nz[d] = vz;
+        nz[3 + d] = vp;
         acc[0] += r[j] * vz;
         acc[1] += rP[j] * vp;
       }
+      if (INIT) put_rec(recF, i, nz[0], nz[1], nz[2], nz[3], nz[4], nz[5]);
     }
   }
   if (!INIT) block_store<2>(acc, part, C_RZN);
@@ -186,6 +206,7 @@ __global__ void k_pcg_reset(PcgState *st) {
 // alpha = r.z / p.Ap; r -= alpha vec; u += alpha p; |r|^2 partials; the last block
 // finishes both norms, applies the stopping rules to PcgState, re-arms the counter and,
 // inside a captured graph, sets the condition of the PCG while node.
+template <typename T>
 __global__ void __launch_bounds__(kVecThreads) k_pcg_update(int n, int nbf, const double *__restrict__ vec,
                                                             const double *__restrict__ vecP,
                                                             const double *__restrict__ p,
@@ -193,7 +214,8 @@ __global__ void __launch_bounds__(kVecThreads) k_pcg_update(int n, int nbf, cons
                                                             double *uD, double *uP, const double *__restrict__ partF,
                                                             double *partE, unsigned *counter, PcgState *st,
                                                             int max_iter, double polar_eps, const int *flags,
-                                                            cudaGraphConditionalHandle cond, int use_cond) {
+                                                            cudaGraphConditionalHandle cond, int use_cond,
+                                                            const double *__restrict__ polar, T *recP) {
   __shared__ double alpha[2];
   __shared__ bool last;
   if (threadIdx.x < 32) {
@@ -208,6 +230,7 @@ __global__ void __launch_bounds__(kVecThreads) k_pcg_update(int n, int nbf, cons
   double v[2] = {0.0, 0.0};
   const int stride = gridDim.x * blockDim.x;
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) {
+    double nr[6];
     for (int d = 0; d < 3; d++) {
       const size_t j = (size_t)d * n + i;
       const double rr = r[j] - alpha[0] * vec[j];
@@ -217,7 +240,11 @@ __global__ void __launch_bounds__(kVecThreads) k_pcg_update(int n, int nbf, cons
       uP[j] += alpha[1] * pP[j];
       v[0] += rr * rr;
       v[1] += rp * rp;
+      nr[d] = rr;
+      nr[3 + d] = rp;
     }
+    const double a = polar[i];
+    put_rec(recP, i, a * nr[0], a * nr[1], a * nr[2], a * nr[3], a * nr[4], a * nr[5]);
   }
   block_store<2>(v, partE, C_EPS);
   __threadfence();
@@ -252,10 +279,12 @@ __global__ void __launch_bounds__(kVecThreads) k_pcg_update(int n, int nbf, cons
   }
 }
 
-// beta = r.z_new / r.z_old; p = z + beta p (UpdateConjugateLoop, Fletcher-Reeves).
+// beta = r.z_new / r.z_old; p = z + beta p (UpdateConjugateLoop, Fletcher-Reeves); also
+// writes p's source record.
+template <typename T>
 __global__ void __launch_bounds__(kVecThreads) k_pcg_p(int n, int nbf, const double *__restrict__ part,
                                                        const double *__restrict__ zz, const double *__restrict__ zP,
-                                                       double *p, double *pP) {
+                                                       double *p, double *pP, T *recF) {
   __shared__ double beta[2];
   if (threadIdx.x < 32) {
     double old = warp_total(part, nbf, C_RZ), oldP = warp_total(part, nbf, C_RZP);
@@ -270,11 +299,17 @@ __global__ void __launch_bounds__(kVecThreads) k_pcg_p(int n, int nbf, const dou
   __syncthreads();
   const int stride = gridDim.x * blockDim.x;
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) {
+    double np[6];
     for (int d = 0; d < 3; d++) {
       const size_t j = (size_t)d * n + i;
-      p[j] = zz[j] + beta[0] * p[j];
-      pP[j] = zP[j] + beta[1] * pP[j];
+      const double a = zz[j] + beta[0] * p[j];
+      const double b = zP[j] + beta[1] * pP[j];
+      p[j] = a;
+      pP[j] = b;
+      np[d] = a;
+      np[3 + d] = b;
     }
+    put_rec(recF, i, np[0], np[1], np[2], np[3], np[4], np[5]);
   }
 }
 
@@ -284,31 +319,48 @@ static double aewald3_of(const Handle &h) {
   return 4.0 / 3.0 * pow(a, 3.0) / 1.7724538509055160273;
 }
 
-template <int MODE, typename C2>
+template <int MODE, typename C2, typename T>
 static void field(Handle &h, const double *ud, const double *up, double *outD, double *outP) {
-  k_pcg_field<MODE, C2><<<kFieldBlocks, kFieldThreads, 0, h.stream>>>(
-      h.n, h.d_x, h.d_y, h.d_z, h.box, h.d_ewl, h.d_ewl_cnt, h.cap_ewl, reinterpret_cast<const C2 *>(h.d_coefE), ud,
-      up, h.d_cphiI, h.d_cphiP, aewald3_of(h), h.d_polar, h.d_udirD, h.d_udirP, h.d_r, h.d_rP, h.d_zpre, h.d_zpreP,
-      outD, outP, h.d_part2);
+  k_pcg_field<MODE, C2, T><<<kFieldBlocks, kFieldThreads, 0, h.stream>>>(
+      h.n, h.d_pos, h.box, h.d_ewl, h.d_ewl_cnt, h.cap_ewl, reinterpret_cast<const C2 *>(h.d_coefE),
+      reinterpret_cast<const T *>(h.d_recF), ud, up, h.d_cphiI, h.d_cphiP, aewald3_of(h), h.d_polar, h.d_udirD,
+      h.d_udirP, h.d_r, h.d_rP, h.d_zpre, h.d_zpreP, outD, outP, reinterpret_cast<T *>(h.d_recP), h.d_part2);
   FFX_LAUNCHED(h);
 }
 
 template <int MODE>
 static void launch_field(Handle &h, const double *ud, const double *up, double *outD, double *outP) {
-  if (h.mixed) field<MODE, float2>(h, ud, up, outD, outP); else field<MODE, double2>(h, ud, up, outD, outP);
+  if (h.mixed) field<MODE, float2, float>(h, ud, up, outD, outP); else field<MODE, double2, double>(h, ud, up, outD, outP);
 }
 
-template <bool INIT, typename C2>
+template <bool INIT, typename C2, typename T>
 static void precond(Handle &h) {
-  k_pcg_precond<INIT, C2><<<kFieldBlocks, kFieldThreads, 0, h.stream>>>(
-      h.n, h.d_x, h.d_y, h.d_z, h.box, h.d_prl, h.d_prl_cnt, h.cap_prl, reinterpret_cast<const C2 *>(h.d_coefP),
-      h.d_polar, h.d_r, h.d_rP, h.prm.precond_scale, h.d_zpre, h.d_zpreP, h.d_p, h.d_pP, h.d_part2);
+  k_pcg_precond<INIT, C2, T><<<kFieldBlocks, kFieldThreads, 0, h.stream>>>(
+      h.n, h.d_pos, h.box, h.d_prl, h.d_prl_cnt, h.cap_prl, reinterpret_cast<const C2 *>(h.d_coefP),
+      reinterpret_cast<const T *>(h.d_recP), h.d_polar, h.d_r, h.d_rP, h.prm.precond_scale, h.d_zpre, h.d_zpreP,
+      h.d_p, h.d_pP, reinterpret_cast<T *>(h.d_recF), h.d_part2);
   FFX_LAUNCHED(h);
 }
 
 template <bool INIT>
 static void launch_precond(Handle &h) {
-  if (h.mixed) precond<INIT, float2>(h); else precond<INIT, double2>(h);
+  if (h.mixed) precond<INIT, float2, float>(h); else precond<INIT, double2, double>(h);
+}
+
+template <typename T>
+static void update(Handle &h, cudaGraphConditionalHandle cond, int use_cond) {
+  k_pcg_update<T><<<kVecBlocks, kVecThreads, 0, h.stream>>>(
+      h.n, kFieldBlocks, h.d_vec, h.d_vecP, h.d_p, h.d_pP, h.d_r, h.d_rP, h.d_uD, h.d_uP, h.d_part2,
+      h.d_part2 + 8 * 2048, h.d_counter, h.d_pcg, h.prm.max_scf_iter, h.prm.polar_eps, h.d_flags, cond, use_cond,
+      h.d_polar, reinterpret_cast<T *>(h.d_recP));
+  FFX_LAUNCHED(h);
+}
+
+template <typename T>
+static void new_direction(Handle &h) {
+  k_pcg_p<T><<<kVecBlocks, kVecThreads, 0, h.stream>>>(h.n, kFieldBlocks, h.d_part2, h.d_zpre, h.d_zpreP, h.d_p,
+                                                       h.d_pP, reinterpret_cast<T *>(h.d_recF));
+  FFX_LAUNCHED(h);
 }
 
 // One PCG step up to the stopping test: recip field of p, A p with its dot products, update.
@@ -320,12 +372,8 @@ static void pcg_step(Handle &h, cudaGraphConditionalHandle cond, int use_cond) {
   launch_field<2>(h, h.d_p, h.d_pP, h.d_vec, h.d_vecP);
   timer_end(h, tk);
   tk = timer_begin(h, FFXG_STAGE_PCG_VECTOR);
-  k_pcg_update<<<kVecBlocks, kVecThreads, 0, h.stream>>>(h.n, kFieldBlocks, h.d_vec, h.d_vecP, h.d_p, h.d_pP, h.d_r,
-                                                         h.d_rP, h.d_uD, h.d_uP, h.d_part2, h.d_part2 + 8 * 2048,
-                                                         h.d_counter, h.d_pcg, h.prm.max_scf_iter, h.prm.polar_eps,
-                                                         h.d_flags, cond, use_cond);
+  if (h.mixed) update<float>(h, cond, use_cond); else update<double>(h, cond, use_cond);
   timer_end(h, tk);
-  FFX_LAUNCHED(h);
 }
 
 // New search direction: z = M r (with r . z partials), then p = z + beta p.
@@ -334,9 +382,8 @@ static void pcg_direction(Handle &h) {
   launch_precond<false>(h);
   timer_end(h, tk);
   tk = timer_begin(h, FFXG_STAGE_PCG_VECTOR);
-  k_pcg_p<<<kVecBlocks, kVecThreads, 0, h.stream>>>(h.n, kFieldBlocks, h.d_part2, h.d_zpre, h.d_zpreP, h.d_p, h.d_pP);
+  if (h.mixed) new_direction<float>(h); else new_direction<double>(h);
   timer_end(h, tk);
-  FFX_LAUNCHED(h);
 }
 
 // The solve.  Directly (capture false): the host reads the device's stopping decision

@@ -199,30 +199,25 @@ __device__ __forceinline__ int jmod(int a, int m) {
   return r < 0 ? r + m : r;
 }
 
-// Mesh accumulation.  Plain form: FP64 atomics into the complex double mesh.  Mixed
-// form: 64-bit fixed-point integer atomics (2^32 units per unit of density) into a
-// separate accumulation mesh [points][2]; integer addition is associative, so the
-// accumulated mesh has the same bits whatever order the atoms arrive in.  The first
-// FFT pass converts it to FP32 and clears it for the next spread.
-constexpr float kMeshFix = 4294967296.0f;        // 2^32
-constexpr float kMeshUnfix = 2.3283064365386963e-10f;  // 2^-32
-
-__device__ __forceinline__ unsigned long long to_fix(float v) {
-  return (unsigned long long)__float2ll_rn(v * kMeshFix);
+// Mesh accumulation: FP64 atomics into the complex double mesh in both forms.  The
+// mixed form first rounds each FP32 contribution to a multiple of 2^-32; sums of such
+// values are exact in FP64 (below 2^21 in magnitude), so the accumulated mesh has the
+// same bits whatever order the atoms arrive in.  The first FFT pass reads the double
+// mesh and continues in FP32.
+__device__ __forceinline__ double mesh_quantize(float v) {
+  return rint((double)v * 4294967296.0) * 2.3283064365386962890625e-10;
 }
-__device__ __forceinline__ void mesh_add(double2 *grid, unsigned long long *, size_t idx, double re) {
-  atomicAdd(&grid[idx].x, re);
+__device__ __forceinline__ void mesh_add(double2 *grid, size_t idx, double re) { atomicAdd(&grid[idx].x, re); }
+__device__ __forceinline__ void mesh_add(double2 *grid, size_t idx, float re) {
+  atomicAdd(&grid[idx].x, mesh_quantize(re));
 }
-__device__ __forceinline__ void mesh_add(double2 *, unsigned long long *gq, size_t idx, float re) {
-  atomicAdd(&gq[2 * idx], to_fix(re));
-}
-__device__ __forceinline__ void mesh_add(double2 *grid, unsigned long long *, size_t idx, double re, double im) {
+__device__ __forceinline__ void mesh_add(double2 *grid, size_t idx, double re, double im) {
   atomicAdd(&grid[idx].x, re);
   atomicAdd(&grid[idx].y, im);
 }
-__device__ __forceinline__ void mesh_add(double2 *, unsigned long long *gq, size_t idx, float re, float im) {
-  atomicAdd(&gq[2 * idx], to_fix(re));
-  atomicAdd(&gq[2 * idx + 1], to_fix(im));
+__device__ __forceinline__ void mesh_add(double2 *grid, size_t idx, float re, float im) {
+  atomicAdd(&grid[idx].x, mesh_quantize(re));
+  atomicAdd(&grid[idx].y, mesh_quantize(im));
 }
 
 // Wrap a support index (within one period of the mesh) into [0, m).
@@ -233,8 +228,7 @@ __device__ __forceinline__ int wrap1(int v, int m) { return v < 0 ? v + m : (v >
 // the atomic add (no integer division in the loop).
 template <typename S>
 __global__ void k_spread_permanent(int n, const double *__restrict__ fm, const S *__restrict__ spl,
-                                   const int *__restrict__ igrid, int nfx, int nfy, int nfz, double2 *grid,
-                                   unsigned long long *gq) {
+                                   const int *__restrict__ igrid, int nfx, int nfy, int nfz, double2 *grid) {
   const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const int lane = threadIdx.x & 31;
   if (warp >= n || lane >= 25) return;
@@ -261,14 +255,14 @@ __global__ void k_spread_permanent(int n, const double *__restrict__ fm, const S
     const S term2 = f[t200] * v0 * u0;
     const S val = fma(x0, term0, fma(x1, term1, x2 * term2));
     const int kk = wrap1(k0 + a3, nfz);
-    mesh_add(grid, gq, (size_t)kk * nfy * nfx + row, val);
+    mesh_add(grid, (size_t)kk * nfy * nfx + row, val);
   }
 }
 
 template <typename S>
 __global__ void k_spread_induced(int n, const double *__restrict__ ud, const double *__restrict__ up,
                                  const S *__restrict__ spl, const int *__restrict__ igrid, int nfx, int nfy,
-                                 int nfz, double2 *grid, unsigned long long *gq, PmeConst pc) {
+                                 int nfz, double2 *grid, PmeConst pc) {
   const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const int lane = threadIdx.x & 31;
   if (warp >= n || lane >= 25) return;
@@ -298,7 +292,7 @@ __global__ void k_spread_induced(int n, const double *__restrict__ ud, const dou
     const S re = fma(v0, Ad, v1 * Bd);
     const S im = fma(v0, Ap, v1 * Bp);
     const int kk = wrap1(k0 + a3, nfz);
-    mesh_add(grid, gq, (size_t)kk * nfy * nfx + row, re, im);
+    mesh_add(grid, (size_t)kk * nfy * nfx + row, re, im);
   }
 }
 
@@ -380,13 +374,13 @@ __device__ __forceinline__ void fft_butterfly(const typename Vec2<S>::type *in, 
   for (int q = 0; q < R; q++) out[(idxD + q * Ns) * L + l] = y[q];
 }
 
-// FROMQ (mixed form, first pass only): the input is the 64-bit fixed-point
-// accumulation mesh, converted to FP32 on load and cleared for the next spread.
-template <bool FUSE_G, typename S, bool FROMQ>
+// FROMD (mixed form, first pass only): the input is the double accumulation mesh `src`,
+// converted to FP32 on load.
+template <bool FUSE_G, typename S, bool FROMD>
 __global__ void __launch_bounds__(256) k_fft_axis(typename Vec2<S>::type *grid, FftAxis ax, int sign,
                                                   const typename Vec2<S>::type *__restrict__ tw,
                                                   const S *__restrict__ G, int gnx, int gny,
-                                                  unsigned long long *gq) {
+                                                  const double2 *__restrict__ src) {
   using V2 = typename Vec2<S>::type;
   // Shared layout is element-major, line-minor: buf[j * L + l].  Consecutive threads
   // take consecutive lines, so butterflies are bank-conflict free and the Y and Z
@@ -401,10 +395,9 @@ __global__ void __launch_bounds__(256) k_fft_axis(typename Vec2<S>::type *grid, 
   for (int t = threadIdx.x; t < len * L; t += blockDim.x) {
     const int l = contiguous ? t / len : t % L, j = contiguous ? t % len : t / L;
     const size_t g = base + (size_t)l * ax.line_step + (size_t)j * ax.stride;
-    if (FROMQ) {
-      const longlong2 q = reinterpret_cast<const longlong2 *>(gq)[g];
-      reinterpret_cast<longlong2 *>(gq)[g] = make_longlong2(0, 0);
-      buf0[j * L + l] = mk2<S>((S)q.x * (S)kMeshUnfix, (S)q.y * (S)kMeshUnfix);
+    if (FROMD) {
+      const double2 q = src[g];
+      buf0[j * L + l] = mk2<S>((S)q.x, (S)q.y);
     } else {
       buf0[j * L + l] = grid[g];
     }
@@ -483,11 +476,11 @@ __device__ __forceinline__ void fixed_stages(typename Vec2<S>::type *&in, typena
   }
 }
 
-template <int LEN, int L, bool FUSE_G, typename S, bool FROMQ>
+template <int LEN, int L, bool FUSE_G, typename S, bool FROMD>
 __global__ void __launch_bounds__(256) k_fft_fixed(typename Vec2<S>::type *grid, FftAxis ax, int sign,
                                                    const typename Vec2<S>::type *__restrict__ twg,
                                                    const S *__restrict__ G, int gnx, int gny,
-                                                   unsigned long long *gq) {
+                                                   const double2 *__restrict__ src) {
   using V2 = typename Vec2<S>::type;
   __shared__ V2 buf[2][LEN * L];
   __shared__ V2 tw[LEN];
@@ -498,10 +491,9 @@ __global__ void __launch_bounds__(256) k_fft_fixed(typename Vec2<S>::type *grid,
   for (int t = threadIdx.x; t < LEN * L; t += 256) {
     const int l = contiguous ? t / LEN : t % L, j = contiguous ? t % LEN : t / L;
     const size_t g = base + (size_t)l * ax.line_step + (size_t)j * ax.stride;
-    if (FROMQ) {
-      const longlong2 q = reinterpret_cast<const longlong2 *>(gq)[g];
-      reinterpret_cast<longlong2 *>(gq)[g] = make_longlong2(0, 0);
-      buf[0][j * L + l] = mk2<S>((S)q.x * (S)kMeshUnfix, (S)q.y * (S)kMeshUnfix);
+    if (FROMD) {
+      const double2 q = src[g];
+      buf[0][j * L + l] = mk2<S>((S)q.x, (S)q.y);
     } else {
       buf[0][j * L + l] = grid[g];
     }
@@ -889,30 +881,29 @@ void launch_bsplines(Handle &h) {
 
 static size_t grid_points(const Handle &h) { return (size_t)h.nfft[0] * h.nfft[1] * h.nfft[2]; }
 
-// The mixed form's accumulation mesh is cleared by the FFT pass that consumes it.
+// Both forms accumulate into the double mesh d_grid (cleared first); the mixed form's
+// FFT continues in the FP32 mesh d_gridf.
 void launch_spread_permanent(Handle &h) {
   const int nb = nblocks((int64_t)h.n * 32, 256);
-  if (h.mixed) {
+  cudaMemsetAsync(h.d_grid, 0, grid_points(h) * sizeof(double2), h.stream);
+  if (h.mixed)
     k_spread_permanent<float><<<nb, 256, 0, h.stream>>>(h.n, h.d_fm, reinterpret_cast<const float *>(h.d_spl),
-                                                        h.d_igrid, h.nfft[0], h.nfft[1], h.nfft[2], nullptr, h.d_gridq);
-  } else {
-    cudaMemsetAsync(h.d_grid, 0, grid_points(h) * sizeof(double2), h.stream);
+                                                        h.d_igrid, h.nfft[0], h.nfft[1], h.nfft[2], h.d_grid);
+  else
     k_spread_permanent<double><<<nb, 256, 0, h.stream>>>(h.n, h.d_fm, h.d_spl, h.d_igrid, h.nfft[0], h.nfft[1],
-                                                         h.nfft[2], h.d_grid, nullptr);
-  }
+                                                         h.nfft[2], h.d_grid);
   FFX_LAUNCHED(h);
 }
 
 void launch_spread_induced(Handle &h, const double *ud, const double *up) {
   const int nb = nblocks((int64_t)h.n * 32, 256);
-  if (h.mixed) {
+  cudaMemsetAsync(h.d_grid, 0, grid_points(h) * sizeof(double2), h.stream);
+  if (h.mixed)
     k_spread_induced<float><<<nb, 256, 0, h.stream>>>(h.n, ud, up, reinterpret_cast<const float *>(h.d_spl), h.d_igrid,
-                                                      h.nfft[0], h.nfft[1], h.nfft[2], nullptr, h.d_gridq, h.pc);
-  } else {
-    cudaMemsetAsync(h.d_grid, 0, grid_points(h) * sizeof(double2), h.stream);
+                                                      h.nfft[0], h.nfft[1], h.nfft[2], h.d_grid, h.pc);
+  else
     k_spread_induced<double><<<nb, 256, 0, h.stream>>>(h.n, ud, up, h.d_spl, h.d_igrid, h.nfft[0], h.nfft[1],
-                                                       h.nfft[2], h.d_grid, nullptr, h.pc);
-  }
+                                                       h.nfft[2], h.d_grid, h.pc);
   FFX_LAUNCHED(h);
 }
 
@@ -921,7 +912,7 @@ static void fft_convolution(Handle &h, typename Vec2<S>::type *grid, const typen
                             const S *influence) {
   const int nfx = h.nfft[0], nfy = h.nfft[1], nfz = h.nfft[2];
   const int maxn = std::max(nfx, std::max(nfy, nfz));
-  auto run = [&](int d, int sign, bool fuse, bool fromq) {
+  auto run = [&](int d, int sign, bool fuse, bool fromd) {
     const FftAxis &a = h.axes[d];
     const int outer = (d == 0) ? nfz : ((d == 1) ? nfz : nfy);
     const int blocks = a.groups_inner * outer;
@@ -931,9 +922,9 @@ static void fft_convolution(Handle &h, typename Vec2<S>::type *grid, const typen
       if (fuse)
         k_fft_fixed<64, 16, true, S, false><<<blocks, 256, 0, h.stream>>>(grid, a, sign, tw, influence, nfx, nfy,
                                                                           nullptr);
-      else if (fromq)
+      else if (fromd)
         k_fft_fixed<64, 16, false, S, true><<<blocks, 256, 0, h.stream>>>(grid, a, sign, tw, nullptr, nfx, nfy,
-                                                                          h.d_gridq);
+                                                                          h.d_grid);
       else
         k_fft_fixed<64, 16, false, S, false><<<blocks, 256, 0, h.stream>>>(grid, a, sign, tw, nullptr, nfx, nfy,
                                                                            nullptr);
@@ -942,14 +933,14 @@ static void fft_convolution(Handle &h, typename Vec2<S>::type *grid, const typen
     }
     if (fuse)
       k_fft_axis<true, S, false><<<blocks, 256, smem, h.stream>>>(grid, a, sign, tw, influence, nfx, nfy, nullptr);
-    else if (fromq)
-      k_fft_axis<false, S, true><<<blocks, 256, smem, h.stream>>>(grid, a, sign, tw, nullptr, nfx, nfy, h.d_gridq);
+    else if (fromd)
+      k_fft_axis<false, S, true><<<blocks, 256, smem, h.stream>>>(grid, a, sign, tw, nullptr, nfx, nfy, h.d_grid);
     else
       k_fft_axis<false, S, false><<<blocks, 256, smem, h.stream>>>(grid, a, sign, tw, nullptr, nfx, nfy, nullptr);
     FFX_LAUNCHED(h);
   };
-  const bool fromq = (sizeof(S) == 4);
-  run(0, -1, false, fromq);
+  const bool fromd = (sizeof(S) == 4);   // mixed: the first pass reads the double mesh
+  run(0, -1, false, fromd);
   run(1, -1, false, false);
   run(2, -1, true, false);
   run(1, +1, false, false);
@@ -958,7 +949,7 @@ static void fft_convolution(Handle &h, typename Vec2<S>::type *grid, const typen
 
 void launch_fft_convolution(Handle &h) {
   if (h.mixed)
-    fft_convolution<float>(h, reinterpret_cast<float2 *>(h.d_grid), h.d_twiddlef, h.d_influencef);
+    fft_convolution<float>(h, h.d_gridf, h.d_twiddlef, h.d_influencef);
   else
     fft_convolution<double>(h, h.d_grid, h.d_twiddle, h.d_influence);
 }
@@ -966,7 +957,7 @@ void launch_fft_convolution(Handle &h) {
 template <typename S>
 static void phi(Handle &h, int which) {
   const S *spl = reinterpret_cast<const S *>(h.d_spl);
-  const auto *grid = reinterpret_cast<const typename Vec2<S>::type *>(h.d_grid);
+  const auto *grid = reinterpret_cast<const typename Vec2<S>::type *>(h.mixed ? (void *)h.d_gridf : (void *)h.d_grid);
   if (which == 0)
     k_phi<20, S><<<nblocks(h.n, 128), 128, 0, h.stream>>>(h.n, spl, h.d_igrid, grid, h.nfft[0], h.nfft[1], h.nfft[2],
                                                          h.d_fphi, h.d_cphi, nullptr, nullptr, h.pc);

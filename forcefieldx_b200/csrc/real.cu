@@ -59,7 +59,7 @@ __global__ void __launch_bounds__(128) k_realspace_field(
     int *ewl_cnt, int capE, int *prl, int *prl_cnt, int capP, typename Vec2<R>::type *coefE,
     typename Vec2<R>::type *coefP, Excl ex, EwaldCoef ec, ScaleTables c_scales, const double *__restrict__ cphi,
     const double *__restrict__ polar, int direct, double *fieldD, double *fieldP, double *uD, double *uP,
-    double *udD, double *udP, int *flags) {
+    double *udD, double *udP, R *recF, int *flags) {
   using V2 = typename Vec2<R>::type;
   const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const int lane = threadIdx.x & 31;
@@ -201,6 +201,7 @@ __global__ void __launch_bounds__(128) k_realspace_field(
       uP[i] = a * Px; uP[n + i] = a * Py; uP[2 * n + i] = a * Pz;
       udD[i] = a * Fx; udD[n + i] = a * Fy; udD[2 * n + i] = a * Fz;
       udP[i] = a * Px; udP[n + i] = a * Py; udP[2 * n + i] = a * Pz;
+      put_rec(recF, i, a * Fx, a * Fy, a * Fz, a * Px, a * Py, a * Pz);
     }
     fieldD[i] = Fx; fieldD[n + i] = Fy; fieldD[2 * n + i] = Fz;
     fieldP[i] = Px; fieldP[n + i] = Py; fieldP[2 * n + i] = Pz;
@@ -586,7 +587,7 @@ static void realspace_field(Handle &h) {
       h.prm.precond_cutoff, h.d_ewl, h.d_ewl_cnt, h.cap_ewl, h.d_prl, h.d_prl_cnt, h.cap_prl,
       reinterpret_cast<V2 *>(h.d_coefE), reinterpret_cast<V2 *>(h.d_coefP), excl(h),
       ewald_coef(h, h.prm.ewald_alpha), h.scales, h.d_cphi, h.d_polar, h.prm.polarization != FFXG_POLAR_NONE ? 1 : 0,
-      h.d_fieldD, h.d_fieldP, h.d_uD, h.d_uP, h.d_udirD, h.d_udirP, h.d_flags);
+      h.d_fieldD, h.d_fieldP, h.d_uD, h.d_uP, h.d_udirD, h.d_udirP, reinterpret_cast<R *>(h.d_recF), h.d_flags);
   FFX_LAUNCHED(h);
 }
 
