@@ -127,6 +127,32 @@ __device__ __forceinline__ void get_rec(const T *__restrict__ rec, int k, T *v) 
   }
 }
 
+// One cached pair of the dipole-field lists: the minimum-image displacement r = x_k - x_i
+// and the coefficients A (scalar part) and B (dyadic part) of the field -A u + B (u.r) r.
+// Plain form: FP64, 40 bytes; mixed form: FP32, 20 bytes.  Stored as a 32- or 16-byte
+// record (x, y, z, A) plus B in a parallel array, both read as coalesced streams.
+template <typename T> struct PairRec;
+template <> struct alignas(32) PairRec<double> { double2 xy, za; };
+template <> struct alignas(16) PairRec<float> { float4 v; };
+
+__device__ __forceinline__ void store_pair(PairRec<double> *p, size_t e, double x, double y, double z, double a) {
+  p[e].xy = make_double2(x, y);
+  p[e].za = make_double2(z, a);
+}
+__device__ __forceinline__ void store_pair(PairRec<float> *p, size_t e, float x, float y, float z, float a) {
+  p[e].v = make_float4(x, y, z, a);
+}
+__device__ __forceinline__ void load_pair(const PairRec<double> *__restrict__ p, size_t e, double &x, double &y,
+                                          double &z, double &a) {
+  const double2 u = p[e].xy, v = p[e].za;
+  x = u.x; y = u.y; z = v.x; a = v.y;
+}
+__device__ __forceinline__ void load_pair(const PairRec<float> *__restrict__ p, size_t e, float &x, float &y,
+                                          float &z, float &a) {
+  const float4 u = p[e].v;
+  x = u.x; y = u.y; z = u.z; a = u.w;
+}
+
 // PME transforms of one handle (passed to kernels by value).
 struct PmeConst {
   double tmm[10][10];   // ReciprocalSpace.transformMultipoleMatrix
@@ -194,7 +220,10 @@ struct Handle {
   int *d_nbr = nullptr, *d_nbr_cnt = nullptr;
   int *d_ewl = nullptr, *d_ewl_cnt = nullptr;
   int *d_prl = nullptr, *d_prl_cnt = nullptr;
-  double2 *d_coefE = nullptr, *d_coefP = nullptr;   // cached dipole-field pair coefficients (A, B)
+  // Cached dipole-field pairs of the Ewald and preconditioner rows (PairRec + B), sized
+  // for the FP64 records; the mixed form uses the leading half.
+  PairRec<double> *d_coefE = nullptr, *d_coefP = nullptr;
+  double *d_coefEB = nullptr, *d_coefPB = nullptr;
   double *d_part2 = nullptr;                        // PCG partial sums of the fixed-grid kernels
   unsigned *d_counter = nullptr;                    // last-block counter (returns to 0 after each use)
 

@@ -59,13 +59,18 @@ static int alloc_lists(Handle &h) {
   if (h.d_prl) cudaFree(h.d_prl);
   if (h.d_coefE) cudaFree(h.d_coefE);
   if (h.d_coefP) cudaFree(h.d_coefP);
+  if (h.d_coefEB) cudaFree(h.d_coefEB);
+  if (h.d_coefPB) cudaFree(h.d_coefPB);
   h.d_nbr = h.d_ewl = h.d_prl = nullptr;
   h.d_coefE = h.d_coefP = nullptr;
+  h.d_coefEB = h.d_coefPB = nullptr;
   CK(dalloc(&h.d_nbr, (size_t)h.n * h.cap_nbr));
   CK(dalloc(&h.d_ewl, (size_t)h.n * h.cap_ewl));
   CK(dalloc(&h.d_prl, (size_t)h.n * h.cap_prl));
   CK(dalloc(&h.d_coefE, (size_t)h.n * h.cap_ewl));
   CK(dalloc(&h.d_coefP, (size_t)h.n * h.cap_prl));
+  CK(dalloc(&h.d_coefEB, (size_t)h.n * h.cap_ewl));
+  CK(dalloc(&h.d_coefPB, (size_t)h.n * h.cap_prl));
   h.list_valid = false;
   return FFXG_OK;
 }
@@ -320,7 +325,7 @@ static void free_all(Handle &h) {
                   h.d_uP, h.d_udirD, h.d_udirP, h.d_r, h.d_rP, h.d_zpre, h.d_zpreP, h.d_p, h.d_pP, h.d_vec, h.d_vecP,
                   h.d_partials, h.d_scalars, h.d_grid, h.d_influence, h.d_twiddle, h.d_gridf, h.d_influencef, h.d_twiddlef, h.d_grad, h.d_torque, h.d_gred,
                   h.d_eatom, h.d_catom, h.d_result, h.d_cresult, h.d_flags, h.d_xyz_in, h.d_grad_out,
-                  h.d_coefE, h.d_coefP, h.d_part2, h.d_counter, h.d_pos, h.d_recF, h.d_recP};
+                  h.d_coefE, h.d_coefP, h.d_coefEB, h.d_coefPB, h.d_part2, h.d_counter, h.d_pos, h.d_recF, h.d_recP};
   for (void *q : ptrs)
     if (q) cudaFree(q);
   if (h.h_scalars) cudaFreeHost(h.h_scalars);

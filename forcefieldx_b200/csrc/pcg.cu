@@ -5,11 +5,11 @@
 // UpdateConjugateRegion (:991-1180, Fletcher-Reeves).  The D and CR systems advance
 // together with separate scalars.
 //
-// The real-space part of every dipole field reuses the per-pair coefficients
-// (A, B) that k_realspace_field stored for this evaluation: the field at i of a dipole
-// set u is sum_k -A_ik u_k + B_ik (u_k . r_ik) r_ik.  So each field costs one
-// streamed pass over the Ewald (or preconditioner) row plus the minimum image of the
-// pair, with no erfc, exp or sqrt.  The field kernels fold in the PCG vector work
+// The real-space part of every dipole field reuses the pairs that k_realspace_field
+// cached for this evaluation (displacement r_ik and coefficients A_ik, B_ik): the field
+// at i of a dipole set u is sum_k -A_ik u_k + B_ik (u_k . r_ik) r_ik.  So each field
+// costs one streamed pass over the Ewald (or preconditioner) row plus one gathered
+// source record per pair, with no minimum image, erfc, exp or sqrt.  The field kernels fold in the PCG vector work
 // (A p = p / alpha - T p with its dot products, or z = alpha (E_precond + s r) with
 // r . z).  Vectors are FP64 [3][n]; every dot product is a fixed-order sum over the
 // blocks of a fixed-size grid, so runs are bitwise reproducible.  The residual norms
@@ -55,45 +55,41 @@ __device__ __forceinline__ void block_store(const double *v, double *part, int c
 }
 
 // Contribution of one neighbour: -A u_k + B (u_k . r) r for both sets.
-template <typename C2, typename T>
-__device__ __forceinline__ void field_term(double xi, double yi, double zi, double2 qa, double2 qb, C2 c,
-                                           const T *s, const Box &bx, T *acc) {
-  double xd = __dsub_rn(qa.x, xi), yd = __dsub_rn(qa.y, yi), zd = __dsub_rn(qb.x, zi);
-  image_exact(xd, yd, zd, bx);
-  const T xr = (T)xd, yr = (T)yd, zr = (T)zd, A = (T)c.x, B = (T)c.y;
+template <typename T>
+__device__ __forceinline__ void field_term(T xr, T yr, T zr, T A, T B, const T *s, T *acc) {
   const T ukr = B * (s[0] * xr + s[1] * yr + s[2] * zr);
   const T pkr = B * (s[3] * xr + s[4] * yr + s[5] * zr);
   acc[0] += -A * s[0] + ukr * xr; acc[1] += -A * s[1] + ukr * yr; acc[2] += -A * s[2] + ukr * zr;
   acc[3] += -A * s[3] + pkr * xr; acc[4] += -A * s[4] + pkr * yr; acc[5] += -A * s[5] + pkr * zr;
 }
 
-// Dipole field at atom i from the cached coefficient row (warp cooperative).  C2 is
-// double2 (plain form) or float2 (mixed form: FP32 coefficients and sources, FP64
-// reduction).  Each lane handles entries a and a + 32 together so that both entries'
-// loads are in flight at once; the summation order stays a, a + 32, a + 64, ...
-template <typename C2, typename T>
-__device__ __forceinline__ void coef_field(int i, const double2 *__restrict__ pos, const Box &bx,
-                                           const int *__restrict__ lst, const int *__restrict__ lst_cnt, int cap,
-                                           const C2 *__restrict__ coef, const T *__restrict__ rec, double *f) {
+// Dipole field at atom i from the cached pair row (warp cooperative): the displacement
+// and A, B of each pair stream in coalesced; only the neighbour's source record is
+// gathered.  T is double (plain form) or float (mixed form, FP64 reduction).  Each lane
+// handles entries a and a + 32 together so that both entries' loads are in flight; the
+// summation order stays a, a + 32, a + 64, ...
+template <typename T>
+__device__ __forceinline__ void coef_field(int i, const int *__restrict__ lst, const int *__restrict__ lst_cnt,
+                                           int cap, const PairRec<T> *__restrict__ pr, const T *__restrict__ pb,
+                                           const T *__restrict__ rec, double *f) {
   const int lane = threadIdx.x & 31;
-  const double2 pa = pos[2 * i], pb = pos[2 * i + 1];
   T acc[6] = {0, 0, 0, 0, 0, 0};
   const int cnt = min(lst_cnt[i], cap);
-  const int *row = lst + (size_t)i * cap;
-  const C2 *crow = coef + (size_t)i * cap;
+  const size_t e0 = (size_t)i * cap;
+  const int *row = lst + e0;
   for (int a = lane; a < cnt; a += 64) {
     const bool two = a + 32 < cnt;
-    const int k0 = row[a];
-    const int k1 = two ? row[a + 32] : k0;
-    const C2 c0 = crow[a];
-    const C2 c1 = two ? crow[a + 32] : c0;
-    const double2 q0a = pos[2 * k0], q0b = pos[2 * k0 + 1];
-    const double2 q1a = pos[2 * k1], q1b = pos[2 * k1 + 1];
+    const int a1 = two ? a + 32 : a;
+    const int k0 = row[a], k1 = row[a1];
+    T x0, y0, z0, A0, x1, y1, z1, A1;
+    load_pair(pr, e0 + a, x0, y0, z0, A0);
+    load_pair(pr, e0 + a1, x1, y1, z1, A1);
+    const T B0 = pb[e0 + a], B1 = pb[e0 + a1];
     T s0[6], s1[6];
     get_rec(rec, k0, s0);
     get_rec(rec, k1, s1);
-    field_term(pa.x, pa.y, pb.x, q0a, q0b, c0, s0, bx, acc);
-    if (two) field_term(pa.x, pa.y, pb.x, q1a, q1b, c1, s1, bx, acc);
+    field_term(x0, y0, z0, A0, B0, s0, acc);
+    if (two) field_term(x1, y1, z1, A1, B1, s1, acc);
   }
 #pragma unroll
   for (int q = 0; q < 6; q++) f[q] = warp_sum((double)acc[q]);
@@ -102,10 +98,10 @@ __device__ __forceinline__ void coef_field(int i, const double2 *__restrict__ po
 // MODE 1: initial residual r = (u_dir - u) / alpha + E(u) with u == u_dir (InitResidualRegion);
 //         also writes the preconditioner source record alpha r.
 // MODE 2: vec = p / alpha - E(p) and partials of p . vec and r . z (UpdateApLoop).
-template <int MODE, typename C2, typename T>
+template <int MODE, typename T>
 __global__ void __launch_bounds__(kFieldThreads) k_pcg_field(
-    int n, const double2 *__restrict__ pos, Box bx, const int *__restrict__ ewl, const int *__restrict__ ewl_cnt,
-    int capE, const C2 *__restrict__ coefE, const T *__restrict__ rec, const double *__restrict__ ud,
+    int n, const int *__restrict__ ewl, const int *__restrict__ ewl_cnt, int capE,
+    const PairRec<T> *__restrict__ coefE, const T *__restrict__ coefEB, const T *__restrict__ rec, const double *__restrict__ ud,
     const double *__restrict__ up, const double *__restrict__ cphiD, const double *__restrict__ cphiP,
     double aewald3, const double *__restrict__ polar, const double *__restrict__ udirD,
     const double *__restrict__ udirP, const double *__restrict__ r, const double *__restrict__ rP,
@@ -116,7 +112,7 @@ __global__ void __launch_bounds__(kFieldThreads) k_pcg_field(
   double acc[4] = {0, 0, 0, 0};
   for (int i = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5); i < n; i += wstride) {
     double f[6];
-    coef_field(i, pos, bx, ewl, ewl_cnt, capE, coefE, rec, f);
+    coef_field(i, ewl, ewl_cnt, capE, coefE, coefEB, rec, f);
     if (lane == 0) {
       for (int d = 0; d < 3; d++) {
         f[d] += aewald3 * ud[d * n + i] - cphiD[(1 + d) * n + i];
@@ -155,10 +151,10 @@ __global__ void __launch_bounds__(kFieldThreads) k_pcg_field(
 // z = alpha (E_precond(alpha r) + s r) (InitConjugateRegion / UpdatePreconditionerLoop);
 // INIT also sets p = z (and its source record), otherwise the partials of r . z_new are
 // stored.  The source record holds alpha r.
-template <bool INIT, typename C2, typename T>
+template <bool INIT, typename T>
 __global__ void __launch_bounds__(kFieldThreads) k_pcg_precond(
-    int n, const double2 *__restrict__ pos, Box bx, const int *__restrict__ prl, const int *__restrict__ prl_cnt,
-    int capP, const C2 *__restrict__ coefP, const T *__restrict__ recP, const double *__restrict__ polar,
+    int n, const int *__restrict__ prl, const int *__restrict__ prl_cnt, int capP,
+    const PairRec<T> *__restrict__ coefP, const T *__restrict__ coefPB, const T *__restrict__ recP, const double *__restrict__ polar,
     const double *__restrict__ r, const double *__restrict__ rP, double s, double *zz, double *zP, double *p,
     double *pP, T *recF, double *part) {
   const int lane = threadIdx.x & 31;
@@ -166,7 +162,7 @@ __global__ void __launch_bounds__(kFieldThreads) k_pcg_precond(
   double acc[2] = {0, 0};
   for (int i = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5); i < n; i += wstride) {
     double f[6];
-    coef_field(i, pos, bx, prl, prl_cnt, capP, coefP, recP, f);
+    coef_field(i, prl, prl_cnt, capP, coefP, coefPB, recP, f);
     if (lane == 0) {
       const double a = polar[i];
       double nz[6];
@@ -319,32 +315,33 @@ static double aewald3_of(const Handle &h) {
   return 4.0 / 3.0 * pow(a, 3.0) / 1.7724538509055160273;
 }
 
-template <int MODE, typename C2, typename T>
+template <int MODE, typename T>
 static void field(Handle &h, const double *ud, const double *up, double *outD, double *outP) {
-  k_pcg_field<MODE, C2, T><<<kFieldBlocks, kFieldThreads, 0, h.stream>>>(
-      h.n, h.d_pos, h.box, h.d_ewl, h.d_ewl_cnt, h.cap_ewl, reinterpret_cast<const C2 *>(h.d_coefE),
-      reinterpret_cast<const T *>(h.d_recF), ud, up, h.d_cphiI, h.d_cphiP, aewald3_of(h), h.d_polar, h.d_udirD,
-      h.d_udirP, h.d_r, h.d_rP, h.d_zpre, h.d_zpreP, outD, outP, reinterpret_cast<T *>(h.d_recP), h.d_part2);
+  k_pcg_field<MODE, T><<<kFieldBlocks, kFieldThreads, 0, h.stream>>>(
+      h.n, h.d_ewl, h.d_ewl_cnt, h.cap_ewl, reinterpret_cast<const PairRec<T> *>(h.d_coefE),
+      reinterpret_cast<const T *>(h.d_coefEB), reinterpret_cast<const T *>(h.d_recF), ud, up, h.d_cphiI, h.d_cphiP,
+      aewald3_of(h), h.d_polar, h.d_udirD, h.d_udirP, h.d_r, h.d_rP, h.d_zpre, h.d_zpreP, outD, outP,
+      reinterpret_cast<T *>(h.d_recP), h.d_part2);
   FFX_LAUNCHED(h);
 }
 
 template <int MODE>
 static void launch_field(Handle &h, const double *ud, const double *up, double *outD, double *outP) {
-  if (h.mixed) field<MODE, float2, float>(h, ud, up, outD, outP); else field<MODE, double2, double>(h, ud, up, outD, outP);
+  if (h.mixed) field<MODE, float>(h, ud, up, outD, outP); else field<MODE, double>(h, ud, up, outD, outP);
 }
 
-template <bool INIT, typename C2, typename T>
+template <bool INIT, typename T>
 static void precond(Handle &h) {
-  k_pcg_precond<INIT, C2, T><<<kFieldBlocks, kFieldThreads, 0, h.stream>>>(
-      h.n, h.d_pos, h.box, h.d_prl, h.d_prl_cnt, h.cap_prl, reinterpret_cast<const C2 *>(h.d_coefP),
-      reinterpret_cast<const T *>(h.d_recP), h.d_polar, h.d_r, h.d_rP, h.prm.precond_scale, h.d_zpre, h.d_zpreP,
-      h.d_p, h.d_pP, reinterpret_cast<T *>(h.d_recF), h.d_part2);
+  k_pcg_precond<INIT, T><<<kFieldBlocks, kFieldThreads, 0, h.stream>>>(
+      h.n, h.d_prl, h.d_prl_cnt, h.cap_prl, reinterpret_cast<const PairRec<T> *>(h.d_coefP),
+      reinterpret_cast<const T *>(h.d_coefPB), reinterpret_cast<const T *>(h.d_recP), h.d_polar, h.d_r, h.d_rP,
+      h.prm.precond_scale, h.d_zpre, h.d_zpreP, h.d_p, h.d_pP, reinterpret_cast<T *>(h.d_recF), h.d_part2);
   FFX_LAUNCHED(h);
 }
 
 template <bool INIT>
 static void launch_precond(Handle &h) {
-  if (h.mixed) precond<INIT, float2, float>(h); else precond<INIT, double2, double>(h);
+  if (h.mixed) precond<INIT, float>(h); else precond<INIT, double>(h);
 }
 
 template <typename T>

@@ -56,8 +56,8 @@ __global__ void __launch_bounds__(128) k_realspace_field(
     int n, const double *__restrict__ x, const double *__restrict__ y, const double *__restrict__ z, Box bx,
     const double *__restrict__ gm, const double *__restrict__ ipdamp, const double *__restrict__ thole,
     const int *__restrict__ nbr, const int *__restrict__ nbr_cnt, int cap, double off2, double pcut, int *ewl,
-    int *ewl_cnt, int capE, int *prl, int *prl_cnt, int capP, typename Vec2<R>::type *coefE,
-    typename Vec2<R>::type *coefP, Excl ex, EwaldCoef ec, ScaleTables c_scales, const double *__restrict__ cphi,
+    int *ewl_cnt, int capE, int *prl, int *prl_cnt, int capP, PairRec<R> *coefE, R *coefEB,
+    PairRec<R> *coefP, R *coefPB, Excl ex, EwaldCoef ec, ScaleTables c_scales, const double *__restrict__ cphi,
     const double *__restrict__ polar, int direct, double *fieldD, double *fieldP, double *uD, double *uP,
     double *udD, double *udP, R *recF, int *flags) {
   using V2 = typename Vec2<R>::type;
@@ -115,7 +115,7 @@ __global__ void __launch_bounds__(128) k_realspace_field(
     const int a = base + lane;
     const bool act = a < cnt;
     bool pr = false;
-    V2 cpre = mk2<R>(R(0.0), R(0.0));
+    R pA = R(0), pB = R(0), px_ = R(0), py_ = R(0), pz_ = R(0);
     if (act) {
       const int k = row[a];
       double xd = __dsub_rn(x[k], xi), yd = __dsub_rn(y[k], yi), zd = __dsub_rn(z[k], zi);
@@ -173,17 +173,25 @@ __global__ void __launch_bounds__(128) k_realspace_field(
       px += fimx - fipx; py += fimy - fipy; pz += fimz - fipz;
       // Induced-field coefficients (no masks), InducedDipoleFieldRegion.java:383-404.
       const R urr3 = (R(1.0) - scale3) * rr3, urr5 = (R(1.0) - scale5) * rr5;
-      if (a < capE) coefE[(size_t)i * capE + a] = mk2<R>(bn1 - urr3, bn2 - urr5);
+      if (a < capE) {
+        store_pair(coefE, (size_t)i * capE + a, xr, yr, zr, bn1 - urr3);
+        coefEB[(size_t)i * capE + a] = bn2 - urr5;
+      }
       pr = sqrt(r2d) < pcut;   // the same test, in FP64, that selected the preconditioner row
       if (pr) {
         const R b1 = rr1 * rr2, b2 = R(3.0) * b1 * rr2;   // Ewald off: bn0 = 1/r
-        cpre = mk2<R>(b1 - urr3, b2 - urr5);
+        pA = b1 - urr3;
+        pB = b2 - urr5;
+        px_ = xr; py_ = yr; pz_ = zr;
       }
     }
     const unsigned mp = __ballot_sync(0xffffffffu, pr);
     if (pr) {
       const int pos = cp + __popc(mp & lt);
-      if (pos < capP) coefP[(size_t)i * capP + pos] = cpre;
+      if (pos < capP) {
+        store_pair(coefP, (size_t)i * capP + pos, px_, py_, pz_, pA);
+        coefPB[(size_t)i * capP + pos] = pB;
+      }
     }
     cp += __popc(mp);
   }
@@ -585,7 +593,8 @@ static void realspace_field(Handle &h) {
   k_realspace_field<R><<<nblocks((int64_t)h.n * 32, 128), 128, 0, h.stream>>>(
       h.n, h.d_x, h.d_y, h.d_z, h.box, h.d_gm, h.d_ipdamp, h.d_thole, h.d_nbr, h.d_nbr_cnt, h.cap_nbr, off2,
       h.prm.precond_cutoff, h.d_ewl, h.d_ewl_cnt, h.cap_ewl, h.d_prl, h.d_prl_cnt, h.cap_prl,
-      reinterpret_cast<V2 *>(h.d_coefE), reinterpret_cast<V2 *>(h.d_coefP), excl(h),
+      reinterpret_cast<PairRec<R> *>(h.d_coefE), reinterpret_cast<R *>(h.d_coefEB),
+      reinterpret_cast<PairRec<R> *>(h.d_coefP), reinterpret_cast<R *>(h.d_coefPB), excl(h),
       ewald_coef(h, h.prm.ewald_alpha), h.scales, h.d_cphi, h.d_polar, h.prm.polarization != FFXG_POLAR_NONE ? 1 : 0,
       h.d_fieldD, h.d_fieldP, h.d_uD, h.d_uP, h.d_udirD, h.d_udirP, reinterpret_cast<R *>(h.d_recF), h.d_flags);
   FFX_LAUNCHED(h);
