@@ -245,7 +245,14 @@ struct Handle {
   // the dipoles whose field is taken (u, then p), d_recP holds alpha r.
   double2 *d_pos = nullptr;
   void *d_recF = nullptr, *d_recP = nullptr;
+  double *d_tpair = nullptr;                  // [6][n] pair field of the current source
+  double *d_tp = nullptr;                     // [6][n] field of the PCG direction p
+  cudaStream_t aux = nullptr;                 // runs the pair field beside spread + FFT
+  cudaStream_t aux_side = nullptr;            // the same inside the PCG while-node body capture
+                                              // (a stream forked into a capture stays in it)
+  cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
   double *d_partials = nullptr;               // block partial sums [nblk][8]
+  int part_rows = 0;                          // rows of each PCG partial-sum region of d_part2
   double *d_scalars = nullptr;                // PCG scalars on device
   double *h_scalars = nullptr;                // pinned mirror
   // PME
@@ -303,10 +310,10 @@ void launch_spread_permanent(Handle &h);
 void launch_spread_induced(Handle &h, const double *ud, const double *up);
 void launch_fft_convolution(Handle &h);
 void launch_phi_permanent(Handle &h);
-void launch_phi_induced(Handle &h, bool full);
+void launch_phi_induced(Handle &h);
 void launch_realspace_field(Handle &h);
-void launch_induced_recip(Handle &h, const double *ud, const double *up);
 int run_pcg(Handle &h, bool capture);
+int pcg_partial_rows();
 void launch_recip_energy(Handle &h, bool grad);
 void launch_real_energy(Handle &h, bool grad);
 void launch_torque(Handle &h);
@@ -334,6 +341,17 @@ inline int timer_begin(Handle &h, int stage) {
 }
 inline void timer_end(Handle &h, int tok) {
   if (tok >= 0) cudaEventRecord(h.ev_pool[tok + 1], h.stream);
+}
+// The same on another stream of the handle.
+inline int timer_begin_on(Handle &h, int stage, cudaStream_t st) {
+  cudaStream_t keep = h.stream;
+  h.stream = st;
+  const int tok = timer_begin(h, stage);
+  h.stream = keep;
+  return tok;
+}
+inline void timer_end_on(Handle &h, int tok, cudaStream_t st) {
+  if (tok >= 0) cudaEventRecord(h.ev_pool[tok + 1], st);
 }
 // Accumulate the recorded pairs (stream must be synchronised).
 inline void timer_collect(Handle &h) {

@@ -113,6 +113,10 @@ static int create_impl(const ffxg_system *s, const ffxg_params *p, Handle &h) {
   h.device = dev;
   CK(cudaStreamCreateWithFlags(&h.stream, cudaStreamNonBlocking));
   CK(cudaStreamCreateWithFlags(&h.side, cudaStreamNonBlocking));
+  CK(cudaStreamCreateWithFlags(&h.aux, cudaStreamNonBlocking));
+  CK(cudaStreamCreateWithFlags(&h.aux_side, cudaStreamNonBlocking));
+  CK(cudaEventCreateWithFlags(&h.ev_fork, cudaEventDisableTiming));
+  CK(cudaEventCreateWithFlags(&h.ev_join, cudaEventDisableTiming));
 
   h.box.a = p->box[0]; h.box.b = p->box[1]; h.box.c = p->box[2];
   h.box.A00 = 1.0 / h.box.a; h.box.A11 = 1.0 / h.box.b; h.box.A22 = 1.0 / h.box.c;
@@ -230,11 +234,13 @@ static int create_impl(const ffxg_system *s, const ffxg_params *p, Handle &h) {
   CK(dalloc(&h.d_r, 3 * N)); CK(dalloc(&h.d_rP, 3 * N)); CK(dalloc(&h.d_zpre, 3 * N)); CK(dalloc(&h.d_zpreP, 3 * N));
   CK(dalloc(&h.d_p, 3 * N)); CK(dalloc(&h.d_pP, 3 * N));
   CK(dalloc(&h.d_pos, 2 * N));
+  CK(dalloc(&h.d_tpair, 6 * N)); CK(dalloc(&h.d_tp, 6 * N));
   CK(cudaMalloc(&h.d_recF, 8 * N * sizeof(double)));
   CK(cudaMalloc(&h.d_recP, 8 * N * sizeof(double))); CK(dalloc(&h.d_vec, 3 * N)); CK(dalloc(&h.d_vecP, 3 * N));
   const size_t nparts = std::max<size_t>((size_t)nblocks(n, 256) * 8, 148 * 16) + 64;
   CK(dalloc(&h.d_partials, nparts));
-  CK(dalloc(&h.d_part2, 4096 * 8));
+  h.part_rows = pcg_partial_rows();
+  CK(dalloc(&h.d_part2, 3 * (size_t)h.part_rows * 8));
   CK(dalloc(&h.d_counter, 4));
   CK(cudaMemset(h.d_counter, 0, 4 * sizeof(unsigned)));
   CK(dalloc(&h.d_scalars, 16));
@@ -325,7 +331,7 @@ static void free_all(Handle &h) {
                   h.d_uP, h.d_udirD, h.d_udirP, h.d_r, h.d_rP, h.d_zpre, h.d_zpreP, h.d_p, h.d_pP, h.d_vec, h.d_vecP,
                   h.d_partials, h.d_scalars, h.d_grid, h.d_influence, h.d_twiddle, h.d_gridf, h.d_influencef, h.d_twiddlef, h.d_grad, h.d_torque, h.d_gred,
                   h.d_eatom, h.d_catom, h.d_result, h.d_cresult, h.d_flags, h.d_xyz_in, h.d_grad_out,
-                  h.d_coefE, h.d_coefP, h.d_coefEB, h.d_coefPB, h.d_part2, h.d_counter, h.d_pos, h.d_recF, h.d_recP};
+                  h.d_coefE, h.d_coefP, h.d_coefEB, h.d_coefPB, h.d_part2, h.d_counter, h.d_pos, h.d_recF, h.d_recP, h.d_tpair, h.d_tp};
   for (void *q : ptrs)
     if (q) cudaFree(q);
   if (h.h_scalars) cudaFreeHost(h.h_scalars);
@@ -337,6 +343,10 @@ static void free_all(Handle &h) {
   if (h.d_pcg) cudaFree(h.d_pcg);
   if (h.h_pcg) cudaFreeHost(h.h_pcg);
   if (h.side) cudaStreamDestroy(h.side);
+  if (h.aux) cudaStreamDestroy(h.aux);
+  if (h.aux_side) cudaStreamDestroy(h.aux_side);
+  if (h.ev_fork) cudaEventDestroy(h.ev_fork);
+  if (h.ev_join) cudaEventDestroy(h.ev_join);
   if (h.stream) cudaStreamDestroy(h.stream);
 }
 
@@ -371,7 +381,7 @@ static void emit_final_induced(Handle &h) {
   const int tk = timer_begin(h, FFXG_STAGE_IND_RECIP);
   launch_spread_induced(h, h.d_uD, h.d_uP);
   launch_fft_convolution(h);
-  launch_phi_induced(h, true);
+  launch_phi_induced(h);
   timer_end(h, tk);
 }
 

@@ -21,14 +21,16 @@
 
 namespace ffx {
 
-constexpr int kFieldThreads = 128;               // 4 warps, one atom per warp per step
-constexpr int kFieldBlocks = 148 * 8;            // fixed grid: deterministic partials
+constexpr int kFieldThreads = 128;               // 4 warps; each warp takes one atom at a time
+constexpr int kFieldBlocks = 148 * 8;            // fixed grid (grid-stride over atoms)
 constexpr int kVecThreads = 256;
 constexpr int kVecBlocks = 148 * 2;
-// Columns of the partial-sum table d_part2[block][8].
-enum { C_PAP = 0, C_PAPP, C_RZ, C_RZP, C_RZN, C_RZNP, C_EPS, C_EPSP };
+// Totals of the PCG scalars in Handle::d_scalars.
+enum { T_PAP = 0, T_PAPP, T_RZ, T_RZP, T_RZN, T_RZNP, T_BETA, T_BETAP };
+// Counters (each returns to 0 after use) in Handle::d_counter.
+enum { K_UPDATE = 0, K_FIELD, K_PRECOND };
 
-// Fixed-order total of column c over nb blocks by one warp (lane l sums l, l+32, ...).
+// Fixed-order total of column c over nb rows by one warp (lane l sums l, l+32, ...).
 __device__ __forceinline__ double warp_total(const double *__restrict__ part, int nb, int c) {
   const int lane = threadIdx.x & 31;
   double s = 0.0;
@@ -36,10 +38,14 @@ __device__ __forceinline__ double warp_total(const double *__restrict__ part, in
   return warp_sum(s);
 }
 
-// Block sum of up to 4 per-warp values, written to part[blockIdx.x][c0 .. c0+nv).
+// Block sum of NV per-thread values into part[blockIdx.x][0 .. NV); the last block to
+// finish sums all rows in block order into tot[t0 .. t0 + NV) and re-arms the counter.
+// Returns true in the last block (all threads).
 template <int NV>
-__device__ __forceinline__ void block_store(const double *v, double *part, int c0) {
+__device__ __forceinline__ bool block_partials(const double *v, double *part, unsigned *counter, double *tot,
+                                               int t0) {
   __shared__ double sh[NV][32];
+  __shared__ bool last;
   const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = blockDim.x >> 5;
 #pragma unroll
   for (int q = 0; q < NV; q++) {
@@ -50,8 +56,22 @@ __device__ __forceinline__ void block_store(const double *v, double *part, int c
   if (threadIdx.x < NV) {
     double s = 0.0;
     for (int w = 0; w < nw; w++) s += sh[threadIdx.x][w];
-    part[blockIdx.x * 8 + c0 + threadIdx.x] = s;
+    part[blockIdx.x * 8 + threadIdx.x] = s;
   }
+  __threadfence();
+  __syncthreads();
+  if (threadIdx.x == 0) last = (atomicAdd(counter, 1u) == gridDim.x - 1);
+  __syncthreads();
+  if (last && threadIdx.x < 32) {
+    __threadfence();
+#pragma unroll
+    for (int q = 0; q < NV; q++) {
+      const double t = warp_total(part, gridDim.x, q);
+      if (threadIdx.x == 0) tot[t0 + q] = t;
+    }
+    if (threadIdx.x == 0) *counter = 0u;
+  }
+  return last;
 }
 
 // Contribution of one neighbour: -A u_k + B (u_k . r) r for both sets.
@@ -63,17 +83,16 @@ __device__ __forceinline__ void field_term(T xr, T yr, T zr, T A, T B, const T *
   acc[3] += -A * s[3] + pkr * xr; acc[4] += -A * s[4] + pkr * yr; acc[5] += -A * s[5] + pkr * zr;
 }
 
-// Dipole field at atom i from the cached pair row (warp cooperative): the displacement
+// Lane partials of the dipole field at atom i from the cached pair row: the displacement
 // and A, B of each pair stream in coalesced; only the neighbour's source record is
-// gathered.  T is double (plain form) or float (mixed form, FP64 reduction).  Each lane
-// handles entries a and a + 32 together so that both entries' loads are in flight; the
-// summation order stays a, a + 32, a + 64, ...
+// gathered.  T is double (plain form) or float (mixed form).  Each lane handles entries
+// a and a + 32 together so that both entries' loads are in flight; the summation order
+// stays a, a + 32, a + 64, ...
 template <typename T>
-__device__ __forceinline__ void coef_field(int i, const int *__restrict__ lst, const int *__restrict__ lst_cnt,
-                                           int cap, const PairRec<T> *__restrict__ pr, const T *__restrict__ pb,
-                                           const T *__restrict__ rec, double *f) {
+__device__ __forceinline__ void pair_field(int i, const int *__restrict__ lst, const int *__restrict__ lst_cnt, int cap,
+                                           const PairRec<T> *__restrict__ pr, const T *__restrict__ pb,
+                                           const T *__restrict__ rec, T *acc) {
   const int lane = threadIdx.x & 31;
-  T acc[6] = {0, 0, 0, 0, 0, 0};
   const int cnt = min(lst_cnt[i], cap);
   const size_t e0 = (size_t)i * cap;
   const int *row = lst + e0;
@@ -91,32 +110,106 @@ __device__ __forceinline__ void coef_field(int i, const int *__restrict__ lst, c
     field_term(x0, y0, z0, A0, B0, s0, acc);
     if (two) field_term(x1, y1, z1, A1, B1, s1, acc);
   }
-#pragma unroll
-  for (int q = 0; q < 6; q++) f[q] = warp_sum((double)acc[q]);
 }
 
-// MODE 1: initial residual r = (u_dir - u) / alpha + E(u) with u == u_dir (InitResidualRegion);
-//         also writes the preconditioner source record alpha r.
-// MODE 2: vec = p / alpha - E(p) and partials of p . vec and r . z (UpdateApLoop).
+// Fractional-to-Cartesian transform of the potential gradient (rows and columns 1-3 of
+// ReciprocalSpace.transformFieldMatrix).
+struct FieldXform {
+  double m[3][3];
+};
+
+// Lane partials of the reciprocal-space field (minus the potential gradient) of the
+// (Re, Im) mesh at atom i: lane l < 25 owns the (x, y) support point (l % 5, l / 5) and
+// walks the five z layers (InducedPhiLoop, ReciprocalSpace.java:2506-2775, first
+// derivatives only); the lane's gradient is transformed to Cartesian before the warp sum.
+template <typename T>
+__device__ __forceinline__ void mesh_field(int i, int n, const int *__restrict__ igrid, const T *__restrict__ spl,
+                                           const typename Vec2<T>::type *__restrict__ mesh, int nfx, int nfy, int nfz,
+                                           const FieldXform &xf, T *acc) {
+  const int lane = threadIdx.x & 31;
+  if (lane >= 25) return;
+  const T *sp = spl + (size_t)i * 3 * kOrder * 4;
+  const T *sx = sp, *sy = sp + kOrder * 4, *sz = sp + 2 * kOrder * 4;
+  const int a1 = lane % 5, a2 = lane / 5;
+  int ii = igrid[i] + 1 + a1, jj = igrid[n + i] + 1 + a2;
+  ii += (ii < 0) ? nfx : ((ii >= nfx) ? -nfx : 0);
+  jj += (jj < 0) ? nfy : ((jj >= nfy) ? -nfy : 0);
+  const int k0 = igrid[2 * n + i] + 1;
+  const T x0 = sx[a1 * 4], x1 = sx[a1 * 4 + 1];
+  const T y0 = sy[a2 * 4], y1 = sy[a2 * 4 + 1];
+  const T w10 = x1 * y0, w01 = x0 * y1, w00 = x0 * y0;
+  const auto *col = mesh + (size_t)jj * nfx + ii;
+  T g[6] = {0, 0, 0, 0, 0, 0};
+#pragma unroll
+  for (int a3 = 0; a3 < 5; a3++) {
+    int kk = k0 + a3;
+    kk += (kk < 0) ? nfz : ((kk >= nfz) ? -nfz : 0);
+    const auto m = col[(size_t)kk * nfy * nfx];
+    const T z0 = sz[a3 * 4], z1 = sz[a3 * 4 + 1];
+    const T wx = w10 * z0, wy = w01 * z0, wz = w00 * z1;
+    g[0] = fma(m.x, wx, g[0]); g[1] = fma(m.x, wy, g[1]); g[2] = fma(m.x, wz, g[2]);
+    g[3] = fma(m.y, wx, g[3]); g[4] = fma(m.y, wy, g[4]); g[5] = fma(m.y, wz, g[5]);
+  }
+#pragma unroll
+  for (int d = 0; d < 3; d++) {
+    acc[d] -= (T)xf.m[d][0] * g[0] + (T)xf.m[d][1] * g[1] + (T)xf.m[d][2] * g[2];
+    acc[3 + d] -= (T)xf.m[d][0] * g[3] + (T)xf.m[d][1] * g[4] + (T)xf.m[d][2] * g[5];
+  }
+}
+
+// Real-space pair field of the source records `rec` (u, then z) at every atom, into
+// out[6][n] (D xyz, CR xyz).
+template <typename T>
+__global__ void __launch_bounds__(kFieldThreads) k_pair_field(int n, const int *__restrict__ ewl,
+                                                              const int *__restrict__ ewl_cnt, int capE,
+                                                              const PairRec<T> *__restrict__ coefE,
+                                                              const T *__restrict__ coefEB,
+                                                              const T *__restrict__ rec, double *out) {
+  const int lane = threadIdx.x & 31;
+  const int wstride = gridDim.x * (blockDim.x >> 5);
+  for (int i = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5); i < n; i += wstride) {
+    T a6[6] = {0, 0, 0, 0, 0, 0};
+    pair_field(i, ewl, ewl_cnt, capE, coefE, coefEB, rec, a6);
+    double f[6];
+#pragma unroll
+    for (int q = 0; q < 6; q++) f[q] = warp_sum((double)a6[q]);
+    if (lane == 0) {
+#pragma unroll
+      for (int q = 0; q < 6; q++) out[(size_t)q * n + i] = f[q];
+    }
+  }
+}
+
+// E(v) = pair field (tpair) + reciprocal field from the mesh + self field aewald3 v,
+// for the source v = (vD, vP), then
+// MODE 1: initial residual r = (u_dir - u) / alpha + E(u) with u == u_dir
+//         (InitResidualRegion) and the preconditioner source record alpha r.
+// MODE 2: v = z.  T p = E(z) + beta T p_old and p = z + beta p_old (first: T p = E(z),
+//         p = z); vec = p / alpha - T p; p . vec and r . z finished into d_scalars
+//         (UpdateApLoop).
 template <int MODE, typename T>
-__global__ void __launch_bounds__(kFieldThreads) k_pcg_field(
-    int n, const int *__restrict__ ewl, const int *__restrict__ ewl_cnt, int capE,
-    const PairRec<T> *__restrict__ coefE, const T *__restrict__ coefEB, const T *__restrict__ rec, const double *__restrict__ ud,
-    const double *__restrict__ up, const double *__restrict__ cphiD, const double *__restrict__ cphiP,
-    double aewald3, const double *__restrict__ polar, const double *__restrict__ udirD,
-    const double *__restrict__ udirP, const double *__restrict__ r, const double *__restrict__ rP,
-    const double *__restrict__ zz, const double *__restrict__ zP, double *outD, double *outP, T *recP,
-    double *part) {
+__global__ void __launch_bounds__(kFieldThreads) k_pcg_combine(
+    int n, const int *__restrict__ igrid, const T *__restrict__ spl, const typename Vec2<T>::type *__restrict__ mesh,
+    int nfx, int nfy, int nfz, FieldXform xf, const double *__restrict__ tpair, const double *__restrict__ vD,
+    const double *__restrict__ vP, double aewald3, const double *__restrict__ polar,
+    const double *__restrict__ udirD, const double *__restrict__ udirP, double *p, double *pP, double *tp,
+    int first, const double *__restrict__ r, const double *__restrict__ rP, double *outD, double *outP, T *recP,
+    double *part, unsigned *counter, double *tot) {
   const int lane = threadIdx.x & 31;
   const int wstride = gridDim.x * (blockDim.x >> 5);
   double acc[4] = {0, 0, 0, 0};
+  const double b0 = (MODE == 2 && !first) ? tot[T_BETA] : 0.0;
+  const double b1 = (MODE == 2 && !first) ? tot[T_BETAP] : 0.0;
   for (int i = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5); i < n; i += wstride) {
+    T a6[6] = {0, 0, 0, 0, 0, 0};
+    mesh_field(i, n, igrid, spl, mesh, nfx, nfy, nfz, xf, a6);
     double f[6];
-    coef_field(i, ewl, ewl_cnt, capE, coefE, coefEB, rec, f);
+#pragma unroll
+    for (int q = 0; q < 6; q++) f[q] = warp_sum((double)a6[q]);
     if (lane == 0) {
       for (int d = 0; d < 3; d++) {
-        f[d] += aewald3 * ud[d * n + i] - cphiD[(1 + d) * n + i];
-        f[3 + d] += aewald3 * up[d * n + i] - cphiP[(1 + d) * n + i];
+        f[d] += tpair[(size_t)d * n + i] + aewald3 * vD[d * n + i];
+        f[3 + d] += tpair[(size_t)(3 + d) * n + i] + aewald3 * vP[d * n + i];
       }
       const double a = polar[i];
       const bool ok = a > 0.0;
@@ -125,44 +218,60 @@ __global__ void __launch_bounds__(kFieldThreads) k_pcg_field(
       for (int d = 0; d < 3; d++) {
         const size_t j = (size_t)d * n + i;
         if (MODE == 1) {
-          const double rv = ok ? (udirD[j] - ud[j]) * ip + f[d] : 0.0;
-          const double rp = ok ? (udirP[j] - up[j]) * ip + f[3 + d] : 0.0;
+          const double rv = ok ? (udirD[j] - vD[j]) * ip + f[d] : 0.0;
+          const double rp = ok ? (udirP[j] - vP[j]) * ip + f[3 + d] : 0.0;
           outD[j] = rv;
           outP[j] = rp;
           nr[d] = a * rv;
           nr[3 + d] = a * rp;
         } else {
-          const double vv = ok ? ud[j] * ip - f[d] : 0.0;
-          const double vp = ok ? up[j] * ip - f[3 + d] : 0.0;
+          const size_t jp = (size_t)(3 + d) * n + i;
+          double tD = f[d], tP = f[3 + d], pd = vD[j], pp = vP[j];
+          if (!first) {
+            tD += b0 * tp[j];
+            tP += b1 * tp[jp];
+            pd += b0 * p[j];
+            pp += b1 * pP[j];
+          }
+          tp[j] = tD;
+          tp[jp] = tP;
+          p[j] = pd;
+          pP[j] = pp;
+          const double vv = ok ? pd * ip - tD : 0.0;
+          const double vp = ok ? pp * ip - tP : 0.0;
           outD[j] = vv;
           outP[j] = vp;
-          acc[0] += ud[j] * vv;
-          acc[1] += up[j] * vp;
-          acc[2] += r[j] * zz[j];
-          acc[3] += rP[j] * zP[j];
+          acc[0] += pd * vv;
+          acc[1] += pp * vp;
+          acc[2] += r[j] * vD[j];
+          acc[3] += rP[j] * vP[j];
         }
       }
       if (MODE == 1) put_rec(recP, i, nr[0], nr[1], nr[2], nr[3], nr[4], nr[5]);
     }
   }
-  if (MODE == 2) block_store<4>(acc, part, C_PAP);
+  if (MODE == 2) block_partials<4>(acc, part, counter, tot, T_PAP);
 }
 
-// z = alpha (E_precond(alpha r) + s r) (InitConjugateRegion / UpdatePreconditionerLoop);
-// INIT also sets p = z (and its source record), otherwise the partials of r . z_new are
-// stored.  The source record holds alpha r.
+// z = alpha (E_precond(alpha r) + s r) (InitConjugateRegion / UpdatePreconditionerLoop)
+// and z's source record for the next field.  INIT also sets p = z; otherwise r . z_new
+// is finished into d_scalars and the last block forms beta = r.z_new / r.z_old
+// (UpdateConjugateLoop, Fletcher-Reeves; a zero r.z_old counts as 1).
 template <bool INIT, typename T>
 __global__ void __launch_bounds__(kFieldThreads) k_pcg_precond(
     int n, const int *__restrict__ prl, const int *__restrict__ prl_cnt, int capP,
-    const PairRec<T> *__restrict__ coefP, const T *__restrict__ coefPB, const T *__restrict__ recP, const double *__restrict__ polar,
-    const double *__restrict__ r, const double *__restrict__ rP, double s, double *zz, double *zP, double *p,
-    double *pP, T *recF, double *part) {
+    const PairRec<T> *__restrict__ coefP, const T *__restrict__ coefPB, const T *__restrict__ recP,
+    const double *__restrict__ polar, const double *__restrict__ r, const double *__restrict__ rP, double s,
+    double *zz, double *zP, double *p, double *pP, T *recF, double *part, unsigned *counter, double *tot) {
   const int lane = threadIdx.x & 31;
   const int wstride = gridDim.x * (blockDim.x >> 5);
   double acc[2] = {0, 0};
   for (int i = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5); i < n; i += wstride) {
+    T a6[6] = {0, 0, 0, 0, 0, 0};
+    pair_field(i, prl, prl_cnt, capP, coefP, coefPB, recP, a6);
     double f[6];
-    coef_field(i, prl, prl_cnt, capP, coefP, coefPB, recP, f);
+#pragma unroll
+    for (int q = 0; q < 6; q++) f[q] = warp_sum((double)a6[q]);
     if (lane == 0) {
       const double a = polar[i];
       double nz[6];
@@ -181,10 +290,18 @@ __global__ void __launch_bounds__(kFieldThreads) k_pcg_precond(
         acc[0] += r[j] * vz;
         acc[1] += rP[j] * vp;
       }
-      if (INIT) put_rec(recF, i, nz[0], nz[1], nz[2], nz[3], nz[4], nz[5]);
+      put_rec(recF, i, nz[0], nz[1], nz[2], nz[3], nz[4], nz[5]);
     }
   }
-  if (!INIT) block_store<2>(acc, part, C_RZN);
+  if (!INIT) {
+    if (block_partials<2>(acc, part, counter, tot, T_RZN) && threadIdx.x == 0) {
+      double old = tot[T_RZ], oldP = tot[T_RZP];
+      if (old == 0.0) old = 1.0;
+      if (oldP == 0.0) oldP = 1.0;
+      tot[T_BETA] = tot[T_RZN] / old;
+      tot[T_BETAP] = tot[T_RZNP] / oldP;
+    }
+  }
 }
 
 // PCGSolver.scfByPCG stopping rules (pme/PCGSolver.java:541-570) applied on the device:
@@ -199,41 +316,30 @@ __global__ void k_pcg_reset(PcgState *st) {
   st->cont = 1;
 }
 
-// alpha = r.z / p.Ap; r -= alpha vec; u += alpha p; |r|^2 partials; the last block
-// finishes both norms, applies the stopping rules to PcgState, re-arms the counter and,
-// inside a captured graph, sets the condition of the PCG while node.
+// alpha = r.z / p.Ap; r -= alpha vec; u += alpha p; the preconditioner source record
+// alpha_pol r; |r|^2 partials.  The last block finishes both norms, applies the stopping
+// rules to PcgState, re-arms the counter and, inside a captured graph, sets the
+// condition of the PCG while node.
 template <typename T>
-__global__ void __launch_bounds__(kVecThreads) k_pcg_update(int n, int nbf, const double *__restrict__ vec,
-                                                            const double *__restrict__ vecP,
-                                                            const double *__restrict__ p,
-                                                            const double *__restrict__ pP, double *r, double *rP,
-                                                            double *uD, double *uP, const double *__restrict__ partF,
-                                                            double *partE, unsigned *counter, PcgState *st,
-                                                            int max_iter, double polar_eps, const int *flags,
-                                                            cudaGraphConditionalHandle cond, int use_cond,
-                                                            const double *__restrict__ polar, T *recP) {
-  __shared__ double alpha[2];
-  __shared__ bool last;
-  if (threadIdx.x < 32) {
-    const double pap = warp_total(partF, nbf, C_PAP), papP = warp_total(partF, nbf, C_PAPP);
-    const double rz = warp_total(partF, nbf, C_RZ), rzP = warp_total(partF, nbf, C_RZP);
-    if (threadIdx.x == 0) {
-      alpha[0] = (pap != 0.0) ? rz / pap : rz;
-      alpha[1] = (papP != 0.0) ? rzP / papP : rzP;
-    }
-  }
-  __syncthreads();
+__global__ void __launch_bounds__(kVecThreads) k_pcg_update(
+    int n, const double *__restrict__ vec, const double *__restrict__ vecP, const double *__restrict__ p,
+    const double *__restrict__ pP, double *r, double *rP, double *uD, double *uP, const double *__restrict__ tot,
+    double *partE, unsigned *counter, PcgState *st, int max_iter, double polar_eps, const int *flags,
+    cudaGraphConditionalHandle cond, int use_cond, const double *__restrict__ polar, T *recP) {
+  const double pap = tot[T_PAP], papP = tot[T_PAPP], rz = tot[T_RZ], rzP = tot[T_RZP];
+  const double alpha0 = (pap != 0.0) ? rz / pap : rz;
+  const double alpha1 = (papP != 0.0) ? rzP / papP : rzP;
   double v[2] = {0.0, 0.0};
   const int stride = gridDim.x * blockDim.x;
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) {
     double nr[6];
     for (int d = 0; d < 3; d++) {
       const size_t j = (size_t)d * n + i;
-      const double rr = r[j] - alpha[0] * vec[j];
-      const double rp = rP[j] - alpha[1] * vecP[j];
+      const double rr = r[j] - alpha0 * vec[j];
+      const double rp = rP[j] - alpha1 * vecP[j];
       r[j] = rr; rP[j] = rp;
-      uD[j] += alpha[0] * p[j];
-      uP[j] += alpha[1] * pP[j];
+      uD[j] += alpha0 * p[j];
+      uP[j] += alpha1 * pP[j];
       v[0] += rr * rr;
       v[1] += rp * rp;
       nr[d] = rr;
@@ -242,70 +348,29 @@ __global__ void __launch_bounds__(kVecThreads) k_pcg_update(int n, int nbf, cons
     const double a = polar[i];
     put_rec(recP, i, a * nr[0], a * nr[1], a * nr[2], a * nr[3], a * nr[4], a * nr[5]);
   }
-  block_store<2>(v, partE, C_EPS);
-  __threadfence();
-  if (threadIdx.x == 0) last = (atomicAdd(counter, 1u) == gridDim.x - 1);
-  __syncthreads();
-  if (last && threadIdx.x < 32) {
-    __threadfence();
-    const double e0 = warp_total(partE, gridDim.x, C_EPS), e1 = warp_total(partE, gridDim.x, C_EPSP);
-    if (threadIdx.x == 0) {
-      const double m = (e0 < e1) ? e1 : e0;
-      const double eps = kElecAngToDebye * sqrt(m / (double)n);
-      const double previous = st->eps;
-      const int iter = st->iter + 1;
-      int status = FFXG_OK, cont = 1;
-      if (!(eps <= previous)) {
-        status = isfinite(eps) ? FFXG_ERR_SCF_DIVERGED : FFXG_ERR_NONFINITE;
-        cont = 0;
-      } else if (iter >= max_iter) {
-        status = FFXG_ERR_SCF_MAXITER;
-        cont = 0;
-      } else if (eps < polar_eps) {
-        cont = 0;
-      }
-      if (*flags & (FLAG_NBR_OVERFLOW | FLAG_EWALD_OVERFLOW | FLAG_PRECOND_OVERFLOW | FLAG_NONFINITE)) cont = 0;
-      st->eps = eps;
-      st->iter = iter;
-      st->status = status;
-      st->cont = cont;
-      *counter = 0u;
-      if (use_cond) cudaGraphSetConditional(cond, (unsigned)cont);
+  __shared__ double norms[2];
+  if (block_partials<2>(v, partE, counter, norms, 0) && threadIdx.x == 0) {
+    const double e0 = norms[0], e1 = norms[1];
+    const double m = (e0 < e1) ? e1 : e0;
+    const double eps = kElecAngToDebye * sqrt(m / (double)n);
+    const double previous = st->eps;
+    const int iter = st->iter + 1;
+    int status = FFXG_OK, cont = 1;
+    if (!(eps <= previous)) {
+      status = isfinite(eps) ? FFXG_ERR_SCF_DIVERGED : FFXG_ERR_NONFINITE;
+      cont = 0;
+    } else if (iter >= max_iter) {
+      status = FFXG_ERR_SCF_MAXITER;
+      cont = 0;
+    } else if (eps < polar_eps) {
+      cont = 0;
     }
-  }
-}
-
-// beta = r.z_new / r.z_old; p = z + beta p (UpdateConjugateLoop, Fletcher-Reeves); also
-// writes p's source record.
-template <typename T>
-__global__ void __launch_bounds__(kVecThreads) k_pcg_p(int n, int nbf, const double *__restrict__ part,
-                                                       const double *__restrict__ zz, const double *__restrict__ zP,
-                                                       double *p, double *pP, T *recF) {
-  __shared__ double beta[2];
-  if (threadIdx.x < 32) {
-    double old = warp_total(part, nbf, C_RZ), oldP = warp_total(part, nbf, C_RZP);
-    const double nw = warp_total(part, nbf, C_RZN), nwP = warp_total(part, nbf, C_RZNP);
-    if (threadIdx.x == 0) {
-      if (old == 0.0) old = 1.0;
-      if (oldP == 0.0) oldP = 1.0;
-      beta[0] = nw / old;
-      beta[1] = nwP / oldP;
-    }
-  }
-  __syncthreads();
-  const int stride = gridDim.x * blockDim.x;
-  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) {
-    double np[6];
-    for (int d = 0; d < 3; d++) {
-      const size_t j = (size_t)d * n + i;
-      const double a = zz[j] + beta[0] * p[j];
-      const double b = zP[j] + beta[1] * pP[j];
-      p[j] = a;
-      pP[j] = b;
-      np[d] = a;
-      np[3 + d] = b;
-    }
-    put_rec(recF, i, np[0], np[1], np[2], np[3], np[4], np[5]);
+    if (*flags & (FLAG_NBR_OVERFLOW | FLAG_EWALD_OVERFLOW | FLAG_PRECOND_OVERFLOW | FLAG_NONFINITE)) cont = 0;
+    st->eps = eps;
+    st->iter = iter;
+    st->status = status;
+    st->cont = cont;
+    if (use_cond) cudaGraphSetConditional(cond, (unsigned)cont);
   }
 }
 
@@ -315,19 +380,53 @@ static double aewald3_of(const Handle &h) {
   return 4.0 / 3.0 * pow(a, 3.0) / 1.7724538509055160273;
 }
 
-template <int MODE, typename T>
-static void field(Handle &h, const double *ud, const double *up, double *outD, double *outP) {
-  k_pcg_field<MODE, T><<<kFieldBlocks, kFieldThreads, 0, h.stream>>>(
+// Partial-sum regions of d_part2 (combine, preconditioner, update): one row of 8 per
+// block of the largest grid that writes them.
+int pcg_partial_rows() { return kFieldBlocks > kVecBlocks ? kFieldBlocks : kVecBlocks; }
+static double *part_region(const Handle &h, int k) { return h.d_part2 + (size_t)k * h.part_rows * 8; }
+
+template <typename T>
+static void pair_field_launch(Handle &h, cudaStream_t st) {
+  k_pair_field<T><<<kFieldBlocks, kFieldThreads, 0, st>>>(
       h.n, h.d_ewl, h.d_ewl_cnt, h.cap_ewl, reinterpret_cast<const PairRec<T> *>(h.d_coefE),
-      reinterpret_cast<const T *>(h.d_coefEB), reinterpret_cast<const T *>(h.d_recF), ud, up, h.d_cphiI, h.d_cphiP,
-      aewald3_of(h), h.d_polar, h.d_udirD, h.d_udirP, h.d_r, h.d_rP, h.d_zpre, h.d_zpreP, outD, outP,
-      reinterpret_cast<T *>(h.d_recP), h.d_part2);
+      reinterpret_cast<const T *>(h.d_coefEB), reinterpret_cast<const T *>(h.d_recF), h.d_tpair);
   FFX_LAUNCHED(h);
 }
 
+template <int MODE, typename T>
+static void combine(Handle &h, const double *vD, const double *vP, bool first, double *outD, double *outP) {
+  using V2 = typename Vec2<T>::type;
+  FieldXform xf;
+  for (int a = 0; a < 3; a++)
+    for (int b = 0; b < 3; b++) xf.m[a][b] = h.pc.tfm[1 + a][1 + b];
+  const V2 *mesh = reinterpret_cast<const V2 *>(h.mixed ? (const void *)h.d_gridf : (const void *)h.d_grid);
+  k_pcg_combine<MODE, T><<<kFieldBlocks, kFieldThreads, 0, h.stream>>>(
+      h.n, h.d_igrid, reinterpret_cast<const T *>(h.d_spl), mesh, h.nfft[0], h.nfft[1], h.nfft[2], xf, h.d_tpair, vD,
+      vP, aewald3_of(h), h.d_polar, h.d_udirD, h.d_udirP, h.d_p, h.d_pP, h.d_tp, first ? 1 : 0, h.d_r, h.d_rP, outD,
+      outP, reinterpret_cast<T *>(h.d_recP), part_region(h, 0), h.d_counter + K_FIELD, h.d_scalars);
+  FFX_LAUNCHED(h);
+}
+
+// The full field of (vD, vP), whose source record is in d_recF: the pair field on the
+// auxiliary stream, concurrently with spread + FFT on the main stream, then the combine.
 template <int MODE>
-static void launch_field(Handle &h, const double *ud, const double *up, double *outD, double *outP) {
-  if (h.mixed) field<MODE, float>(h, ud, up, outD, outP); else field<MODE, double>(h, ud, up, outD, outP);
+static void field_of(Handle &h, const double *vD, const double *vP, bool first, double *outD, double *outP) {
+  cudaStream_t ax = (h.stream == h.side) ? h.aux_side : h.aux;
+  cudaEventRecord(h.ev_fork, h.stream);
+  cudaStreamWaitEvent(ax, h.ev_fork, 0);
+  int tk = timer_begin_on(h, FFXG_STAGE_IND_FIELD, ax);
+  if (h.mixed) pair_field_launch<float>(h, ax); else pair_field_launch<double>(h, ax);
+  timer_end_on(h, tk, ax);
+  cudaEventRecord(h.ev_join, ax);
+  tk = timer_begin(h, FFXG_STAGE_IND_RECIP);
+  launch_spread_induced(h, vD, vP);
+  launch_fft_convolution(h);
+  timer_end(h, tk);
+  cudaStreamWaitEvent(h.stream, h.ev_join, 0);
+  tk = timer_begin(h, FFXG_STAGE_PCG_VECTOR);
+  if (h.mixed) combine<MODE, float>(h, vD, vP, first, outD, outP);
+  else combine<MODE, double>(h, vD, vP, first, outD, outP);
+  timer_end(h, tk);
 }
 
 template <bool INIT, typename T>
@@ -335,7 +434,8 @@ static void precond(Handle &h) {
   k_pcg_precond<INIT, T><<<kFieldBlocks, kFieldThreads, 0, h.stream>>>(
       h.n, h.d_prl, h.d_prl_cnt, h.cap_prl, reinterpret_cast<const PairRec<T> *>(h.d_coefP),
       reinterpret_cast<const T *>(h.d_coefPB), reinterpret_cast<const T *>(h.d_recP), h.d_polar, h.d_r, h.d_rP,
-      h.prm.precond_scale, h.d_zpre, h.d_zpreP, h.d_p, h.d_pP, reinterpret_cast<T *>(h.d_recF), h.d_part2);
+      h.prm.precond_scale, h.d_zpre, h.d_zpreP, h.d_p, h.d_pP, reinterpret_cast<T *>(h.d_recF), part_region(h, 1),
+      h.d_counter + K_PRECOND, h.d_scalars);
   FFX_LAUNCHED(h);
 }
 
@@ -347,67 +447,48 @@ static void launch_precond(Handle &h) {
 template <typename T>
 static void update(Handle &h, cudaGraphConditionalHandle cond, int use_cond) {
   k_pcg_update<T><<<kVecBlocks, kVecThreads, 0, h.stream>>>(
-      h.n, kFieldBlocks, h.d_vec, h.d_vecP, h.d_p, h.d_pP, h.d_r, h.d_rP, h.d_uD, h.d_uP, h.d_part2,
-      h.d_part2 + 8 * 2048, h.d_counter, h.d_pcg, h.prm.max_scf_iter, h.prm.polar_eps, h.d_flags, cond, use_cond,
-      h.d_polar, reinterpret_cast<T *>(h.d_recP));
+      h.n, h.d_vec, h.d_vecP, h.d_p, h.d_pP, h.d_r, h.d_rP, h.d_uD, h.d_uP, h.d_scalars, part_region(h, 2),
+      h.d_counter + K_UPDATE, h.d_pcg, h.prm.max_scf_iter, h.prm.polar_eps, h.d_flags, cond, use_cond, h.d_polar,
+      reinterpret_cast<T *>(h.d_recP));
   FFX_LAUNCHED(h);
 }
 
-template <typename T>
-static void new_direction(Handle &h) {
-  k_pcg_p<T><<<kVecBlocks, kVecThreads, 0, h.stream>>>(h.n, kFieldBlocks, h.d_part2, h.d_zpre, h.d_zpreP, h.d_p,
-                                                       h.d_pP, reinterpret_cast<T *>(h.d_recF));
-  FFX_LAUNCHED(h);
-}
-
-// One PCG step up to the stopping test: recip field of p, A p with its dot products, update.
-static void pcg_step(Handle &h, cudaGraphConditionalHandle cond, int use_cond) {
-  int tk = timer_begin(h, FFXG_STAGE_IND_RECIP);
-  launch_induced_recip(h, h.d_p, h.d_pP);
-  timer_end(h, tk);
-  tk = timer_begin(h, FFXG_STAGE_IND_FIELD);
-  launch_field<2>(h, h.d_p, h.d_pP, h.d_vec, h.d_vecP);
-  timer_end(h, tk);
-  tk = timer_begin(h, FFXG_STAGE_PCG_VECTOR);
+// One PCG step up to the stopping test: T p from T z, A p with its dot products, update.
+static void pcg_step(Handle &h, bool first, cudaGraphConditionalHandle cond, int use_cond) {
+  field_of<2>(h, h.d_zpre, h.d_zpreP, first, h.d_vec, h.d_vecP);
+  const int tk = timer_begin(h, FFXG_STAGE_PCG_VECTOR);
   if (h.mixed) update<float>(h, cond, use_cond); else update<double>(h, cond, use_cond);
   timer_end(h, tk);
 }
 
-// New search direction: z = M r (with r . z partials), then p = z + beta p.
-static void pcg_direction(Handle &h) {
-  int tk = timer_begin(h, FFXG_STAGE_PRECOND);
+static void pcg_precond(Handle &h) {
+  const int tk = timer_begin(h, FFXG_STAGE_PRECOND);
   launch_precond<false>(h);
-  timer_end(h, tk);
-  tk = timer_begin(h, FFXG_STAGE_PCG_VECTOR);
-  if (h.mixed) new_direction<float>(h); else new_direction<double>(h);
   timer_end(h, tk);
 }
 
 // The solve.  Directly (capture false): the host reads the device's stopping decision
 // after every update (24 bytes).  Under stream capture (capture true): the first step is
-// recorded in line and the rest as a conditional WHILE node whose body (direction, step)
-// the update kernel re-arms on the device, so the loop runs with no host round trip.
-// Either way the loop ends by max_scf_iter at the latest.
+// recorded in line and the rest as a conditional WHILE node whose body (preconditioner,
+// step) the update kernel re-arms on the device, so the loop runs with no host round
+// trip.  Either way the loop ends by max_scf_iter at the latest.
 int run_pcg(Handle &h, bool capture) {
   k_pcg_reset<<<1, 1, 0, h.stream>>>(h.d_pcg);
   FFX_LAUNCHED(h);
   // Field of the direct dipoles (u == u_dir at entry) gives the initial residual.
-  int tk = timer_begin(h, FFXG_STAGE_IND_RECIP);
-  launch_induced_recip(h, h.d_uD, h.d_uP);
-  timer_end(h, tk);
-  tk = timer_begin(h, FFXG_STAGE_IND_FIELD);
-  launch_field<1>(h, h.d_uD, h.d_uP, h.d_r, h.d_rP);
-  timer_end(h, tk);
-  tk = timer_begin(h, FFXG_STAGE_PRECOND);
+  field_of<1>(h, h.d_uD, h.d_uP, true, h.d_r, h.d_rP);
+  int tk = timer_begin(h, FFXG_STAGE_PRECOND);
   launch_precond<true>(h);
   timer_end(h, tk);
   if (!capture) {
+    bool first = true;
     while (true) {
-      pcg_step(h, 0, 0);
+      pcg_step(h, first, 0, 0);
+      first = false;
       cudaMemcpyAsync(h.h_pcg, h.d_pcg, sizeof(PcgState), cudaMemcpyDeviceToHost, h.stream);
       if (cudaStreamSynchronize(h.stream) != cudaSuccess) return FFXG_ERR_CUDA;
       if (!h.h_pcg->cont) break;
-      pcg_direction(h);
+      pcg_precond(h);
     }
     h.scf_iter = h.h_pcg->iter;
     return h.h_pcg->status;
@@ -421,7 +502,7 @@ int run_pcg(Handle &h, bool capture) {
     return FFXG_ERR_CUDA;
   cudaGraphConditionalHandle cond;
   if (cudaGraphConditionalHandleCreate(&cond, g, 0, cudaGraphCondAssignDefault) != cudaSuccess) return FFXG_ERR_CUDA;
-  pcg_step(h, cond, 1);
+  pcg_step(h, true, cond, 1);
   if (cudaStreamGetCaptureInfo(h.stream, &cs, nullptr, &g, &deps, &ndeps) != cudaSuccess) return FFXG_ERR_CUDA;
   cudaGraphNodeParams cp = {};
   cp.type = cudaGraphNodeTypeConditional;
@@ -438,8 +519,8 @@ int run_pcg(Handle &h, bool capture) {
   cudaStream_t main = h.stream;
   h.stream = h.side;
   const int64_t before = h.launches;
-  pcg_direction(h);
-  pcg_step(h, cond, 1);
+  pcg_precond(h);
+  pcg_step(h, false, cond, 1);
   h.graph_body_launches = h.launches - before;
   h.stream = main;
   if (cudaStreamEndCapture(h.side, &body) != cudaSuccess) return FFXG_ERR_CUDA;

@@ -615,54 +615,6 @@ __global__ void k_phi(int n, const S *__restrict__ spl, const int *__restrict__ 
   }
 }
 
-// Field terms only (first derivatives of the Re and Im potentials), one warp per atom:
-// lanes walk the 125 support points, then the six partial sums reduce by shuffles.
-// Used inside the PCG loop, where only t100, t010, t001 of the induced potential are read.
-template <typename S>
-__global__ void k_phi_field(int n, const S *__restrict__ spl, const int *__restrict__ igrid,
-                            const typename Vec2<S>::type *__restrict__ grid, int nfx, int nfy, int nfz, PmeConst pc,
-                            double *cphiR, double *cphiI) {
-  const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-  const int lane = threadIdx.x & 31;
-  if (warp >= n) return;
-  const int i = warp;
-  const S *sp = spl + (size_t)i * 3 * kOrder * 4;
-  const S *sx = sp, *sy = sp + kOrder * 4, *sz = sp + 2 * kOrder * 4;
-  S rx = 0, ry = 0, rz = 0, ix = 0, iy = 0, iz = 0;
-  if (lane < 25) {
-    // Lane owns the (x, y) point (lane % 5, lane / 5) and walks the five z layers.
-    const int a1 = lane % 5, a2 = lane / 5;
-    const int ii = wrap1(igrid[i] + 1 + a1, nfx), jj = wrap1(igrid[n + i] + 1 + a2, nfy);
-    const int k0 = igrid[2 * n + i] + 1;
-    const S x0 = sx[a1 * 4], x1 = sx[a1 * 4 + 1];
-    const S y0 = sy[a2 * 4], y1 = sy[a2 * 4 + 1];
-    const S w10 = x1 * y0, w01 = x0 * y1, w00 = x0 * y0;
-    const auto *row = grid + (size_t)jj * nfx + ii;
-    S gr[5], gi[5];
-#pragma unroll
-    for (int a3 = 0; a3 < 5; a3++) {
-      const auto g = row[(size_t)wrap1(k0 + a3, nfz) * nfy * nfx];
-      gr[a3] = g.x;
-      gi[a3] = g.y;
-    }
-#pragma unroll
-    for (int a3 = 0; a3 < 5; a3++) {
-      const S z0 = sz[a3 * 4], z1 = sz[a3 * 4 + 1];
-      const S wx = w10 * z0, wy = w01 * z0, wz = w00 * z1;
-      rx = fma(gr[a3], wx, rx); ry = fma(gr[a3], wy, ry); rz = fma(gr[a3], wz, rz);
-      ix = fma(gi[a3], wx, ix); iy = fma(gi[a3], wy, iy); iz = fma(gi[a3], wz, iz);
-    }
-  }
-  const double Rx = warp_sum((double)rx), Ry = warp_sum((double)ry), Rz = warp_sum((double)rz);
-  const double Ix = warp_sum((double)ix), Iy = warp_sum((double)iy), Iz = warp_sum((double)iz);
-  if (lane < 2) {
-    const double f0 = lane == 0 ? Rx : Ix, f1 = lane == 0 ? Ry : Iy, f2 = lane == 0 ? Rz : Iz;
-    double *out = lane == 0 ? cphiR : cphiI;
-#pragma unroll
-    for (int j = 1; j < 4; j++) out[j * n + i] = fma(pc.tfm[j][1], f0, fma(pc.tfm[j][2], f1, pc.tfm[j][3] * f2));
-  }
-}
-
 // ---------------------------------------------------------------------------
 // Host set-up: transform matrices (ReciprocalSpace.java:1123-1210), twiddles and the
 // generalized influence function with zeta-corrected B-spline moduli (:435-492, :1045-1121).
@@ -961,13 +913,9 @@ static void phi(Handle &h, int which) {
   if (which == 0)
     k_phi<20, S><<<nblocks(h.n, 128), 128, 0, h.stream>>>(h.n, spl, h.d_igrid, grid, h.nfft[0], h.nfft[1], h.nfft[2],
                                                          h.d_fphi, h.d_cphi, nullptr, nullptr, h.pc);
-  else if (which == 1)
+  else
     k_phi<20, S><<<nblocks(h.n, 128), 128, 0, h.stream>>>(h.n, spl, h.d_igrid, grid, h.nfft[0], h.nfft[1], h.nfft[2],
                                                          h.d_fphiI, h.d_cphiI, h.d_fphiP, h.d_cphiP, h.pc);
-  else
-    k_phi_field<S><<<nblocks((int64_t)h.n * 32, 128), 128, 0, h.stream>>>(h.n, spl, h.d_igrid, grid, h.nfft[0],
-                                                                          h.nfft[1], h.nfft[2], h.pc, h.d_cphiI,
-                                                                          h.d_cphiP);
   FFX_LAUNCHED(h);
 }
 
@@ -975,8 +923,8 @@ void launch_phi_permanent(Handle &h) {
   if (h.mixed) phi<float>(h, 0); else phi<double>(h, 0);
 }
 
-void launch_phi_induced(Handle &h, bool full) {
-  if (h.mixed) phi<float>(h, full ? 1 : 2); else phi<double>(h, full ? 1 : 2);
+void launch_phi_induced(Handle &h) {
+  if (h.mixed) phi<float>(h, 1); else phi<double>(h, 1);
 }
 
 

@@ -607,12 +607,6 @@ void launch_realspace_field(Handle &h) {
     realspace_field<double>(h);
 }
 
-void launch_induced_recip(Handle &h, const double *ud, const double *up) {
-  // Spread both sets (Re = D, Im = CR), convolve, interpolate the field terms.
-  launch_spread_induced(h, ud, up);
-  launch_fft_convolution(h);
-  launch_phi_induced(h, false);
-}
 
 
 template <typename R>
