@@ -313,7 +313,7 @@ void launch_phi_permanent(Handle &h);
 void launch_phi_induced(Handle &h);
 void launch_realspace_field(Handle &h);
 int run_pcg(Handle &h, bool capture);
-int pcg_partial_rows();
+int pcg_partial_rows(int n);
 void launch_recip_energy(Handle &h, bool grad);
 void launch_real_energy(Handle &h, bool grad);
 void launch_torque(Handle &h);

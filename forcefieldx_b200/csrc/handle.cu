@@ -239,7 +239,7 @@ static int create_impl(const ffxg_system *s, const ffxg_params *p, Handle &h) {
   CK(cudaMalloc(&h.d_recP, 8 * N * sizeof(double))); CK(dalloc(&h.d_vec, 3 * N)); CK(dalloc(&h.d_vecP, 3 * N));
   const size_t nparts = std::max<size_t>((size_t)nblocks(n, 256) * 8, 148 * 16) + 64;
   CK(dalloc(&h.d_partials, nparts));
-  h.part_rows = pcg_partial_rows();
+  h.part_rows = pcg_partial_rows(n);
   CK(dalloc(&h.d_part2, 3 * (size_t)h.part_rows * 8));
   CK(dalloc(&h.d_counter, 4));
   CK(cudaMemset(h.d_counter, 0, 4 * sizeof(unsigned)));

@@ -15,6 +15,7 @@
 // blocks of a fixed-size grid, so runs are bitwise reproducible.  The residual norms
 // are finished by the last block and read back once per iteration (16 bytes) to apply
 // the reference's stopping rules.
+#include <algorithm>
 #include <cmath>
 
 #include "ffx_internal.cuh"
@@ -74,6 +75,56 @@ __device__ __forceinline__ bool block_partials(const double *v, double *part, un
   return last;
 }
 
+// Block sum of NV values already reduced to lane 0 of each warp, stored as
+// part[blockIdx.x][0 .. NV) (no atomics; k_pcg_totals finishes the sum).
+template <int NV>
+__device__ __forceinline__ void block_store_lane0(const double *v, double *part) {
+  __shared__ double sh[NV][32];
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = blockDim.x >> 5;
+  if (lane == 0) {
+#pragma unroll
+    for (int q = 0; q < NV; q++) sh[q][wid] = v[q];
+  }
+  __syncthreads();
+  if (threadIdx.x < NV) {
+    double s = 0.0;
+    for (int w = 0; w < nw; w++) s += sh[threadIdx.x][w];
+    part[blockIdx.x * 8 + threadIdx.x] = s;
+  }
+}
+
+// Fixed-order totals of the first NV columns of nrows partial rows into tot[t0 ..], by
+// one block (thread t sums rows t, t + 256, ...; the 256 sums are added in thread order).
+// BETA: then beta = r.z_new / r.z_old for both systems (a zero r.z_old counts as 1).
+template <int NV, bool BETA>
+__global__ void __launch_bounds__(256) k_pcg_totals(const double *__restrict__ part, int nrows, double *tot, int t0) {
+  __shared__ double sh[NV][256];
+  double s[NV];
+#pragma unroll
+  for (int q = 0; q < NV; q++) s[q] = 0.0;
+  for (int b = threadIdx.x; b < nrows; b += 256)
+#pragma unroll
+    for (int q = 0; q < NV; q++) s[q] += part[b * 8 + q];
+#pragma unroll
+  for (int q = 0; q < NV; q++) sh[q][threadIdx.x] = s[q];
+  __syncthreads();
+  if (threadIdx.x < NV) {
+    double t = 0.0;
+    for (int k = 0; k < 256; k++) t += sh[threadIdx.x][k];
+    tot[t0 + threadIdx.x] = t;
+  }
+  if (BETA) {
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      double old = tot[T_RZ], oldP = tot[T_RZP];
+      if (old == 0.0) old = 1.0;
+      if (oldP == 0.0) oldP = 1.0;
+      tot[T_BETA] = tot[T_RZN] / old;
+      tot[T_BETAP] = tot[T_RZNP] / oldP;
+    }
+  }
+}
+
 // Contribution of one neighbour: -A u_k + B (u_k . r) r for both sets.
 template <typename T>
 __device__ __forceinline__ void field_term(T xr, T yr, T zr, T A, T B, const T *s, T *acc) {
@@ -118,14 +169,14 @@ struct FieldXform {
   double m[3][3];
 };
 
-// Lane partials of the reciprocal-space field (minus the potential gradient) of the
-// (Re, Im) mesh at atom i: lane l < 25 owns the (x, y) support point (l % 5, l / 5) and
-// walks the five z layers (InducedPhiLoop, ReciprocalSpace.java:2506-2775, first
-// derivatives only); the lane's gradient is transformed to Cartesian before the warp sum.
+// Lane partials of the fractional potential gradient of the (Re, Im) mesh at atom i:
+// lane l < 25 owns the (x, y) support point (l % 5, l / 5) and walks the five z layers
+// (InducedPhiLoop, ReciprocalSpace.java:2506-2775, first derivatives only).  The caller
+// sums the lanes and applies the fractional-to-Cartesian transform.
 template <typename T>
 __device__ __forceinline__ void mesh_field(int i, int n, const int *__restrict__ igrid, const T *__restrict__ spl,
                                            const typename Vec2<T>::type *__restrict__ mesh, int nfx, int nfy, int nfz,
-                                           const FieldXform &xf, T *acc) {
+                                           T *acc) {
   const int lane = threadIdx.x & 31;
   if (lane >= 25) return;
   const T *sp = spl + (size_t)i * 3 * kOrder * 4;
@@ -151,10 +202,7 @@ __device__ __forceinline__ void mesh_field(int i, int n, const int *__restrict__
     g[3] = fma(m.y, wx, g[3]); g[4] = fma(m.y, wy, g[4]); g[5] = fma(m.y, wz, g[5]);
   }
 #pragma unroll
-  for (int d = 0; d < 3; d++) {
-    acc[d] -= (T)xf.m[d][0] * g[0] + (T)xf.m[d][1] * g[1] + (T)xf.m[d][2] * g[2];
-    acc[3 + d] -= (T)xf.m[d][0] * g[3] + (T)xf.m[d][1] * g[4] + (T)xf.m[d][2] * g[5];
-  }
+  for (int q = 0; q < 6; q++) acc[q] += g[q];
 }
 
 // Real-space pair field of the source records `rec` (u, then z) at every atom, into
@@ -187,8 +235,10 @@ __global__ void __launch_bounds__(kFieldThreads) k_pair_field(int n, const int *
 // MODE 2: v = z.  T p = E(z) + beta T p_old and p = z + beta p_old (first: T p = E(z),
 //         p = z); vec = p / alpha - T p; p . vec and r . z finished into d_scalars
 //         (UpdateApLoop).
+// One warp per atom: all lanes interpolate the mesh, then lane q < 6 finishes component
+// q (D x, y, z, CR x, y, z).
 template <int MODE, typename T>
-__global__ void __launch_bounds__(kFieldThreads) k_pcg_combine(
+__global__ void __launch_bounds__(256) k_pcg_combine(
     int n, const int *__restrict__ igrid, const T *__restrict__ spl, const typename Vec2<T>::type *__restrict__ mesh,
     int nfx, int nfy, int nfz, FieldXform xf, const double *__restrict__ tpair, const double *__restrict__ vD,
     const double *__restrict__ vP, double aewald3, const double *__restrict__ polar,
@@ -196,61 +246,64 @@ __global__ void __launch_bounds__(kFieldThreads) k_pcg_combine(
     int first, const double *__restrict__ r, const double *__restrict__ rP, double *outD, double *outP, T *recP,
     double *part, unsigned *counter, double *tot) {
   const int lane = threadIdx.x & 31;
-  const int wstride = gridDim.x * (blockDim.x >> 5);
+  const int i = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   double acc[4] = {0, 0, 0, 0};
-  const double b0 = (MODE == 2 && !first) ? tot[T_BETA] : 0.0;
-  const double b1 = (MODE == 2 && !first) ? tot[T_BETAP] : 0.0;
-  for (int i = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5); i < n; i += wstride) {
+  if (i < n) {
     T a6[6] = {0, 0, 0, 0, 0, 0};
-    mesh_field(i, n, igrid, spl, mesh, nfx, nfy, nfz, xf, a6);
-    double f[6];
+    mesh_field(i, n, igrid, spl, mesh, nfx, nfy, nfz, a6);
+    T g[6];
 #pragma unroll
-    for (int q = 0; q < 6; q++) f[q] = warp_sum((double)a6[q]);
-    if (lane == 0) {
-      for (int d = 0; d < 3; d++) {
-        f[d] += tpair[(size_t)d * n + i] + aewald3 * vD[d * n + i];
-        f[3 + d] += tpair[(size_t)(3 + d) * n + i] + aewald3 * vP[d * n + i];
-      }
+    for (int q = 0; q < 6; q++) g[q] = warp_sum(a6[q]);
+    // Lane q < 6 takes Cartesian field component q: -(xf . gradient) of its set.
+    const int d = lane % 3, set = lane / 3;
+    const double *row = xf.m[lane < 6 ? d : 0];
+    const double mine = (lane < 6) ? -(row[0] * (double)(set ? g[3] : g[0]) + row[1] * (double)(set ? g[4] : g[1]) +
+                                       row[2] * (double)(set ? g[5] : g[2]))
+                                   : 0.0;
+    double rec_v = 0.0;
+    if (lane < 6) {
+      const size_t j = (size_t)d * n + i, jt = (size_t)lane * n + i;
+      const double *v = set ? vP : vD;
+      const double vj = v[j];
+      const double e = mine + tpair[jt] + aewald3 * vj;
       const double a = polar[i];
       const bool ok = a > 0.0;
       const double ip = ok ? 1.0 / a : 0.0;
-      double nr[6];
-      for (int d = 0; d < 3; d++) {
-        const size_t j = (size_t)d * n + i;
-        if (MODE == 1) {
-          const double rv = ok ? (udirD[j] - vD[j]) * ip + f[d] : 0.0;
-          const double rp = ok ? (udirP[j] - vP[j]) * ip + f[3 + d] : 0.0;
-          outD[j] = rv;
-          outP[j] = rp;
-          nr[d] = a * rv;
-          nr[3 + d] = a * rp;
-        } else {
-          const size_t jp = (size_t)(3 + d) * n + i;
-          double tD = f[d], tP = f[3 + d], pd = vD[j], pp = vP[j];
-          if (!first) {
-            tD += b0 * tp[j];
-            tP += b1 * tp[jp];
-            pd += b0 * p[j];
-            pp += b1 * pP[j];
-          }
-          tp[j] = tD;
-          tp[jp] = tP;
-          p[j] = pd;
-          pP[j] = pp;
-          const double vv = ok ? pd * ip - tD : 0.0;
-          const double vp = ok ? pp * ip - tP : 0.0;
-          outD[j] = vv;
-          outP[j] = vp;
-          acc[0] += pd * vv;
-          acc[1] += pp * vp;
-          acc[2] += r[j] * vD[j];
-          acc[3] += rP[j] * vP[j];
+      if (MODE == 1) {
+        const double *ud = set ? udirP : udirD;
+        const double rv = ok ? (ud[j] - vj) * ip + e : 0.0;
+        (set ? outP : outD)[j] = rv;
+        rec_v = a * rv;
+      } else {
+        const double b = first ? 0.0 : tot[set ? T_BETAP : T_BETA];
+        double *pp = set ? pP : p;
+        double t = e, pv = vj;
+        if (!first) {
+          t += b * tp[jt];
+          pv += b * pp[j];
         }
+        tp[jt] = t;
+        pp[j] = pv;
+        const double vv = ok ? pv * ip - t : 0.0;
+        (set ? outP : outD)[j] = vv;
+        acc[set] = pv * vv;
+        acc[2 + set] = (set ? rP : r)[j] * vj;
       }
-      if (MODE == 1) put_rec(recP, i, nr[0], nr[1], nr[2], nr[3], nr[4], nr[5]);
+    }
+    if (MODE == 1) {
+      double w[6];
+#pragma unroll
+      for (int q = 0; q < 6; q++) w[q] = __shfl_sync(0xffffffffu, rec_v, q);
+      if (lane == 0) put_rec(recP, i, w[0], w[1], w[2], w[3], w[4], w[5]);
     }
   }
-  if (MODE == 2) block_partials<4>(acc, part, counter, tot, T_PAP);
+  if (MODE == 2) {
+#pragma unroll
+    for (int q = 0; q < 4; q++)
+#pragma unroll
+      for (int o = 4; o > 0; o >>= 1) acc[q] += __shfl_xor_sync(0xffffffffu, acc[q], o);
+    block_store_lane0<4>(acc, part);
+  }
 }
 
 // z = alpha (E_precond(alpha r) + s r) (InitConjugateRegion / UpdatePreconditionerLoop)
@@ -272,35 +325,31 @@ __global__ void __launch_bounds__(kFieldThreads) k_pcg_precond(
     double f[6];
 #pragma unroll
     for (int q = 0; q < 6; q++) f[q] = warp_sum((double)a6[q]);
-    if (lane == 0) {
-      const double a = polar[i];
-      double nz[6];
-      for (int d = 0; d < 3; d++) {
-        const size_t j = (size_t)d * n + i;
-        const double vz = a * (f[d] + s * r[j]);
-        const double vp = a * (f[3 + d] + s * rP[j]);
-        zz[j] = vz;
-        zP[j] = vp;
-        if (INIT) {
-          p[j] = vz;
-          pP[j] = vp;
-        }
-        nz[d] = vz;
-        nz[3 + d] = vp;
-        acc[0] += r[j] * vz;
-        acc[1] += rP[j] * vp;
-      }
-      put_rec(recF, i, nz[0], nz[1], nz[2], nz[3], nz[4], nz[5]);
+    double mine = f[0];
+#pragma unroll
+    for (int q = 1; q < 6; q++)
+      if (lane == q) mine = f[q];
+    double zv = 0.0;
+    if (lane < 6) {
+      const int d = lane % 3, set = lane / 3;
+      const size_t j = (size_t)d * n + i;
+      const double rj = (set ? rP : r)[j];
+      zv = polar[i] * (mine + s * rj);
+      (set ? zP : zz)[j] = zv;
+      if (INIT) (set ? pP : p)[j] = zv;
+      acc[set] += rj * zv;
     }
+    double w[6];
+#pragma unroll
+    for (int q = 0; q < 6; q++) w[q] = __shfl_sync(0xffffffffu, zv, q);
+    if (lane == 0) put_rec(recF, i, w[0], w[1], w[2], w[3], w[4], w[5]);
   }
   if (!INIT) {
-    if (block_partials<2>(acc, part, counter, tot, T_RZN) && threadIdx.x == 0) {
-      double old = tot[T_RZ], oldP = tot[T_RZP];
-      if (old == 0.0) old = 1.0;
-      if (oldP == 0.0) oldP = 1.0;
-      tot[T_BETA] = tot[T_RZN] / old;
-      tot[T_BETAP] = tot[T_RZNP] / oldP;
-    }
+#pragma unroll
+    for (int q = 0; q < 2; q++)
+#pragma unroll
+      for (int o = 4; o > 0; o >>= 1) acc[q] += __shfl_xor_sync(0xffffffffu, acc[q], o);
+    block_store_lane0<2>(acc, part);
   }
 }
 
@@ -382,7 +431,10 @@ static double aewald3_of(const Handle &h) {
 
 // Partial-sum regions of d_part2 (combine, preconditioner, update): one row of 8 per
 // block of the largest grid that writes them.
-int pcg_partial_rows() { return kFieldBlocks > kVecBlocks ? kFieldBlocks : kVecBlocks; }
+int pcg_partial_rows(int n) {
+  const int per_atom = nblocks((int64_t)n * 32, 256);   // k_pcg_combine
+  return std::max(std::max(kFieldBlocks, kVecBlocks), per_atom);
+}
 static double *part_region(const Handle &h, int k) { return h.d_part2 + (size_t)k * h.part_rows * 8; }
 
 template <typename T>
@@ -400,11 +452,16 @@ static void combine(Handle &h, const double *vD, const double *vP, bool first, d
   for (int a = 0; a < 3; a++)
     for (int b = 0; b < 3; b++) xf.m[a][b] = h.pc.tfm[1 + a][1 + b];
   const V2 *mesh = reinterpret_cast<const V2 *>(h.mixed ? (const void *)h.d_gridf : (const void *)h.d_grid);
-  k_pcg_combine<MODE, T><<<kFieldBlocks, kFieldThreads, 0, h.stream>>>(
+  k_pcg_combine<MODE, T><<<nblocks((int64_t)h.n * 32, 256), 256, 0, h.stream>>>(
       h.n, h.d_igrid, reinterpret_cast<const T *>(h.d_spl), mesh, h.nfft[0], h.nfft[1], h.nfft[2], xf, h.d_tpair, vD,
       vP, aewald3_of(h), h.d_polar, h.d_udirD, h.d_udirP, h.d_p, h.d_pP, h.d_tp, first ? 1 : 0, h.d_r, h.d_rP, outD,
       outP, reinterpret_cast<T *>(h.d_recP), part_region(h, 0), h.d_counter + K_FIELD, h.d_scalars);
   FFX_LAUNCHED(h);
+  if (MODE == 2) {
+    k_pcg_totals<4, false><<<1, 256, 0, h.stream>>>(part_region(h, 0), nblocks((int64_t)h.n * 32, 256), h.d_scalars,
+                                                   T_PAP);
+    FFX_LAUNCHED(h);
+  }
 }
 
 // The full field of (vD, vP), whose source record is in d_recF: the pair field on the
@@ -437,6 +494,10 @@ static void precond(Handle &h) {
       h.prm.precond_scale, h.d_zpre, h.d_zpreP, h.d_p, h.d_pP, reinterpret_cast<T *>(h.d_recF), part_region(h, 1),
       h.d_counter + K_PRECOND, h.d_scalars);
   FFX_LAUNCHED(h);
+  if (!INIT) {
+    k_pcg_totals<2, true><<<1, 256, 0, h.stream>>>(part_region(h, 1), kFieldBlocks, h.d_scalars, T_RZN);
+    FFX_LAUNCHED(h);
+  }
 }
 
 template <bool INIT>
