@@ -103,13 +103,14 @@ class ClockSampler:
 
 # ---------------------------------------------------------------------------
 def algorithmic_traffic(stage: str, n: int, pairs_half: int, vdw_list_full: int, mixed: bool) -> float:
-    """Compulsory HBM bytes of one launch of a stage's kernel: every input read once,
-    every output written once (list entries 4 B, FP64 per-atom data; the mixed form
-    caches the pair coefficients in FP32)."""
+    """Compulsory HBM bytes of one launch of a stage's dominant kernel: every input read
+    once, every output written once."""
     full = 2 * pairs_half
-    if stage == "ind_field":      # per entry: index 4 B + coefficients (A, B) 16 B (8 B mixed); per atom:
-        # x,y,z, p(3), pP(3), phi(2x3), polarizability, r(3), rP(3), z(3), zP(3) in; vec(6) out; count
-        return (12.0 if mixed else 20.0) * full + n * (4 + 8 * (3 + 6 + 6 + 1 + 12) + 8 * 6)
+    if stage == "ind_field":      # k_pair_field: per directed pair index 4 B + displacement and A
+        # (16 B mixed, 32 B FP64) + B (4 B / 8 B); per atom one source record (32 B / 64 B) and
+        # the six-component output (48 B)
+        per_pair = 24.0 if mixed else 44.0
+        return per_pair * full + n * ((32 if mixed else 64) + 48)
     if stage == "real_energy":    # list + x,y,z,gm(10),u,p,ipdamp,thole in; e(2),count,grad,torque out
         return 4.0 * full + n * (4 + 8 * (3 + 10 + 6 + 2) + 8 * 2 + 8 + 8 * 6)
     if stage == "vdw":
@@ -221,7 +222,7 @@ def measure(args, precision, system, dist, world, local):
                      "frac": achieved / peak, "traffic": None, "kernel_stage": dom,
                      "algorithmic_bytes_per_launch": traffic_alg, "avg_launch_ms": avg_ms,
                      "peak_source": peak_src,
-                     "note": "pair kernels are bound by FP issue and gather latency, not HBM; see profiles/"},
+                     "note": "stage timed with direct launches; the pair kernels are bound by gather latency, not HBM (profiles/pcg_kernels_water24k_mixed.md)"},
     }
 
 
