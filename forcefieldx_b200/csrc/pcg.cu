@@ -7,14 +7,19 @@
 //
 // The real-space part of every dipole field reuses the pairs that k_realspace_field
 // cached for this evaluation (displacement r_ik and coefficients A_ik, B_ik): the field
-// at i of a dipole set u is sum_k -A_ik u_k + B_ik (u_k . r_ik) r_ik.  So each field
-// costs one streamed pass over the Ewald (or preconditioner) row plus one gathered
-// source record per pair, with no minimum image, erfc, exp or sqrt.  The field kernels fold in the PCG vector work
-// (A p = p / alpha - T p with its dot products, or z = alpha (E_precond + s r) with
-// r . z).  Vectors are FP64 [3][n]; every dot product is a fixed-order sum over the
-// blocks of a fixed-size grid, so runs are bitwise reproducible.  The residual norms
-// are finished by the last block and read back once per iteration (16 bytes) to apply
-// the reference's stopping rules.
+// at i of a dipole set u is sum_k -A_ik u_k + B_ik (u_k . r_ik) r_ik, so each field costs
+// one streamed pass over the Ewald (or preconditioner) row plus one gathered source
+// record per pair, with no minimum image, erfc, exp or sqrt.
+//
+// The field operator T is linear, so with p = z + beta p_old an iteration only needs
+// T z: T p = T z + beta T p_old, with T p_old kept from the previous iteration.  T z is
+// available as soon as the preconditioner has produced z, and its real-space part
+// (k_pair_field) runs on a second stream beside the spread and FFT convolution of z,
+// which leave most SMs idle.  One iteration: k_pcg_precond (z, r . z, beta), {spread z,
+// FFT} || k_pair_field, k_pcg_combine (mesh field of z, self term, T p, p, A p and its
+// dot products), k_pcg_update (r, u, norms; its last block applies the reference's
+// stopping rules on the device).  Vectors are FP64 [3][n]; every dot product is a
+// fixed-order sum of per-block partials (k_pcg_totals, or k_pcg_update's last block).
 #include <algorithm>
 #include <cmath>
 
