@@ -90,12 +90,19 @@ static int create_impl(const ffxg_system *s, const ffxg_params *p, Handle &h) {
       return FFXG_ERR_BAD_ARG;
     }
   }
-  const double rlist = std::max(p->vdw_cutoff, p->ewald_cutoff) + p->list_buffer;
+  // ReplicatesCrystal (C/ReplicatesCrystal.java:172-202) switches to a supercell of
+  // replicate cells when an edge is shorter than twice the buffered list cutoff.  While
+  // every interaction cutoff stays below half of each edge, each pair has exactly one
+  // image within any cutoff, so the minimum image on the unit cell (with the buffered
+  // list, whose extra images lie beyond every cutoff) gives the same energy; that case is
+  // handled here.  A cutoff of half an edge or more needs true multi-image lists.
+  const double rcut = std::max(std::max(p->vdw_cutoff, p->ewald_cutoff), p->precond_cutoff);
   for (int d = 0; d < 3; d++)
-    if (p->box[d] < 2.0 * rlist) {
-      h.err = "box edge shorter than twice the buffered cutoff: replicate cells (nSymm > 1) are not supported";
+    if (p->box[d] <= 2.0 * rcut) {
+      h.err = "box edge not longer than twice an interaction cutoff: multi-image replicate lists are not supported";
       return FFXG_ERR_BAD_ARG;
     }
+  const double rlist = std::max(p->vdw_cutoff, p->ewald_cutoff) + p->list_buffer;
   if (p->ewald_alpha <= 0.0) { h.err = "ewald-alpha must be positive"; return FFXG_ERR_BAD_ARG; }
   if (p->precision != FFXG_PRECISION_FP64 && p->precision != FFXG_PRECISION_MIXED) {
     h.err = "unknown precision"; return FFXG_ERR_BAD_ARG;

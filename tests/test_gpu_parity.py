@@ -10,7 +10,7 @@ import numpy as np
 import pytest
 
 from forcefieldx_b200.energy import EnergyException, ForceFieldEnergy
-from forcefieldx_b200.system import WATER_24K, water_box, water_params
+from forcefieldx_b200.system import WATER_24K, WATER_648, water_box, water_params
 from oracle import binding as ob
 from tests.common import golden_system
 
@@ -50,6 +50,15 @@ def compare(system, params, check_pairs=True):
 def test_water_648():
     s = water_box(6, 18.643, seed=21)
     p = water_params(18.643, vdw_cutoff=7.0, ewald_cutoff=7.0, pme_grid=(20, 20, 20))
+    compare(s, p)
+
+
+def test_water_648_buffered_list_beyond_half_box():
+    """The reference's CPU-runnable case (216 waters, 18.643 A, 9 A vdW, 7 A Ewald, PME 20^3):
+    the 11 A buffered list is longer than half the edge, where the reference switches to
+    replicate cells; every interaction cutoff is shorter, so each pair has one image."""
+    s = water_box(WATER_648["n_side"], WATER_648["edge"], seed=3)
+    p = water_params(WATER_648["edge"], pme_grid=WATER_648["grid"])
     compare(s, p)
 
 
@@ -110,7 +119,7 @@ def test_fd_gradient_gpu():
 def test_error_status_codes():
     s = water_box(4, 12.4, seed=2)
     with pytest.raises(EnergyException) as ei:
-        ForceFieldEnergy(s, water_params(12.4, pme_grid=(16, 16, 16)))   # box < 2 * (9 + 2)
+        ForceFieldEnergy(s, water_params(12.4, pme_grid=(16, 16, 16)))   # box edge < 2 * 9 A vdW cutoff
     assert ei.value.status == 1
     s = water_box(6, 18.643, seed=2)
     p = water_params(18.643, vdw_cutoff=7.0, ewald_cutoff=7.0, pme_grid=(20, 20, 20), max_scf_iter=1)

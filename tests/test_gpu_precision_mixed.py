@@ -48,7 +48,7 @@ def compare_mixed(system, params, xyz=None):
 
 def test_mixed_water_648():
     s = water_box(6, 18.643, seed=21)
-    p = water_params(18.643, vdw_cutoff=7.0, ewald_cutoff=7.0, pme_grid=(20, 20, 20), precision=PRECISION_MIXED)
+    p = water_params(18.643, pme_grid=(20, 20, 20), precision=PRECISION_MIXED)
     compare_mixed(s, p)
 
 
