@@ -49,6 +49,15 @@ class FfxgParams(ctypes.Structure):
     ]
 
 
+class FfxgAlchemy(ctypes.Structure):
+    _fields_ = [
+        ("soft", _I), ("molecule", _I),
+        ("vdw_lambda_alpha", ctypes.c_double), ("vdw_lambda_exponent", ctypes.c_double),
+        ("vdw_lambda_end", ctypes.c_double),
+        ("intermolecular_softcore", ctypes.c_int32), ("intramolecular_softcore", ctypes.c_int32),
+    ]
+
+
 # Every symbol include/ffxcuda.h declares, with its ctypes signature.
 PROTOTYPES = {
     "ffxg_create": (ctypes.c_int, [ctypes.POINTER(FfxgSystem), ctypes.POINTER(FfxgParams),
@@ -62,6 +71,9 @@ PROTOTYPES = {
     "ffxg_get_induced_dipoles": (ctypes.c_int, [ctypes.c_void_p, _D, _D]),
     "ffxg_get_global_multipoles": (ctypes.c_int, [ctypes.c_void_p, _D]),
     "ffxg_get_neighbor_pairs": (ctypes.c_int, [ctypes.c_void_p, _I, _L]),
+    "ffxg_set_alchemy": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(FfxgAlchemy)]),
+    "ffxg_set_lambda": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_double]),
+    "ffxg_get_dEdL": (ctypes.c_int, [ctypes.c_void_p, _D, _D, _D]),
     "ffxg_stream": (ctypes.c_void_p, [ctypes.c_void_p]),
     "ffxg_last_launch_count": (ctypes.c_int64, [ctypes.c_void_p]),
     "ffxg_set_timing": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int]),

@@ -182,6 +182,12 @@ struct PcgState {
   int pad;
 };
 
+// vdW softcore constants of the current lambda (VanDerWaals.setLambda).
+struct AlchConst {
+  double sc1, dsc1dL, d2sc1dL2, sc2, dsc2dL, d2sc2dL2;
+  int active, inter, intra;
+};
+
 struct Handle {
   // ---- configuration
   int n = 0;
@@ -281,6 +287,14 @@ struct Handle {
   double *h_xyz_pin = nullptr, *h_grad_pin = nullptr;
 
   int scf_iter = 0;
+  // Alchemical state (vdW softcore): soft flags, molecule ids, keys, lambda and the
+  // lambda derivatives of the last evaluation.
+  AlchConst alch{0, 0, 0, 1, 0, 0, 0, 0, 0};
+  double alch_alpha = 0.25, alch_exponent = 3.0, alch_end = 1.0, lambda = 1.0;
+  int *d_soft = nullptr, *d_mol = nullptr;
+  double *d_lgred = nullptr;                       // [6][n]: reduced-site and distributed dU/dX dL
+  double dEdL = 0.0, d2EdL2 = 0.0;
+  bool lgrad_valid = false;
   PcgState *d_pcg = nullptr, *h_pcg = nullptr;
   // Graph execution: the whole evaluation captured once per gradient mode and replayed.
   bool use_graphs = true;

@@ -264,7 +264,7 @@ static int create_impl(const ffxg_system *s, const ffxg_params *p, Handle &h) {
     CK(dalloc(&h.d_twiddlef, 3 * (size_t)std::max(nfx, std::max(nfy, nfz))));
   }
   CK(dalloc(&h.d_grad, 3 * N)); CK(dalloc(&h.d_torque, 3 * N)); CK(dalloc(&h.d_gred, 6 * N));
-  CK(dalloc(&h.d_eatom, 8 * N)); CK(dalloc(&h.d_catom, 2 * N));
+  CK(dalloc(&h.d_eatom, 10 * N)); CK(dalloc(&h.d_catom, 2 * N));
   CK(dalloc(&h.d_result, 16)); CK(dalloc(&h.d_cresult, 8));
   CK(dalloc(&h.d_flags, 1));
   CK(cudaMallocHost((void **)&h.h_flags, 64));
@@ -309,7 +309,7 @@ static int create_impl(const ffxg_system *s, const ffxg_params *p, Handle &h) {
   CK(cudaMemset(h.d_grad, 0, 3 * N * sizeof(double)));
   CK(cudaMemset(h.d_torque, 0, 3 * N * sizeof(double)));
   CK(cudaMemset(h.d_gred, 0, 6 * N * sizeof(double)));
-  CK(cudaMemset(h.d_eatom, 0, 8 * N * sizeof(double)));
+  CK(cudaMemset(h.d_eatom, 0, 10 * N * sizeof(double)));
   CK(cudaMemset(h.d_catom, 0, 2 * N * sizeof(long long)));
   CK(cudaMemset(h.d_uD, 0, 3 * N * sizeof(double)));
   CK(cudaMemset(h.d_uP, 0, 3 * N * sizeof(double)));
@@ -338,7 +338,7 @@ static void free_all(Handle &h) {
                   h.d_uP, h.d_udirD, h.d_udirP, h.d_r, h.d_rP, h.d_zpre, h.d_zpreP, h.d_p, h.d_pP, h.d_vec, h.d_vecP,
                   h.d_partials, h.d_scalars, h.d_grid, h.d_influence, h.d_twiddle, h.d_gridf, h.d_influencef, h.d_twiddlef, h.d_grad, h.d_torque, h.d_gred,
                   h.d_eatom, h.d_catom, h.d_result, h.d_cresult, h.d_flags, h.d_xyz_in, h.d_grad_out,
-                  h.d_coefE, h.d_coefP, h.d_coefEB, h.d_coefPB, h.d_part2, h.d_counter, h.d_pos, h.d_recF, h.d_recP, h.d_tpair, h.d_tp};
+                  h.d_coefE, h.d_coefP, h.d_coefEB, h.d_coefPB, h.d_part2, h.d_counter, h.d_pos, h.d_recF, h.d_recP, h.d_tpair, h.d_tp, h.d_soft, h.d_mol, h.d_lgred};
   for (void *q : ptrs)
     if (q) cudaFree(q);
   if (h.h_scalars) cudaFreeHost(h.h_scalars);
@@ -411,7 +411,7 @@ static void emit_back(Handle &h, double *d_grad_xyz) {
   }
   launch_reduce_results(h);
   timer_end(h, tk);
-  cudaMemcpyAsync(h.h_scalars, h.d_result, 7 * sizeof(double), cudaMemcpyDeviceToHost, h.stream);
+  cudaMemcpyAsync(h.h_scalars, h.d_result, 9 * sizeof(double), cudaMemcpyDeviceToHost, h.stream);
   cudaMemcpyAsync(h.h_flags + 2, h.d_cresult, 2 * sizeof(long long), cudaMemcpyDeviceToHost, h.stream);
   cudaMemcpyAsync(h.h_flags, h.d_flags, sizeof(int), cudaMemcpyDeviceToHost, h.stream);
 }
@@ -424,9 +424,12 @@ static const char *scf_message(int st) {
 
 // Terms and counts from the pinned copies written by emit_back.
 static int finish(Handle &h, bool rebuilt, double *terms, int64_t *counts) {
-  double res[7];
+  double res[9];
   long long cres[2];
-  std::memcpy(res, h.h_scalars, 7 * sizeof(double));
+  std::memcpy(res, h.h_scalars, 9 * sizeof(double));
+  h.dEdL = res[7];
+  h.d2EdL2 = res[8];
+  h.lgrad_valid = h.alch.active && h.want_grad;
   std::memcpy(cres, h.h_flags + 2, 2 * sizeof(long long));
   const double eCorr = h.e_charge_correction;
   if (terms) {
@@ -700,6 +703,84 @@ int ffxg_get_neighbor_pairs(ffxg_handle *hh, int32_t *pairs, int64_t *n_pairs) {
       }
     }
   *n_pairs = c;
+  return FFXG_OK;
+}
+
+// VanDerWaals.setLambda (VanDerWaals.java:599-628): softcore constants at lambda.
+static void update_alchemy(Handle &h) {
+  double l = h.lambda;
+  if (l > h.alch_end) l = 1.0; else l = l / h.alch_end;
+  const double a = h.alch_alpha, ex = h.alch_exponent;
+  h.alch.sc1 = a * (1.0 - l) * (1.0 - l);
+  h.alch.dsc1dL = -2.0 * a * (1.0 - l);
+  h.alch.d2sc1dL2 = 2.0 * a;
+  h.alch.sc2 = std::pow(l, ex);
+  h.alch.dsc2dL = ex * std::pow(l, ex - 1.0);
+  h.alch.d2sc2dL2 = (ex >= 2.0) ? ex * (ex - 1.0) * std::pow(l, ex - 2.0) : 0.0;
+  drop_graphs(h);   // the captured vdW launch holds the constants
+}
+
+int ffxg_set_alchemy(ffxg_handle *hh, const ffxg_alchemy *a) {
+  if (!hh) return FFXG_ERR_BAD_ARG;
+  Handle &h = hh->h;
+  if (!a) {
+    h.alch.active = 0;
+    update_alchemy(h);
+    return FFXG_OK;
+  }
+  if (!a->soft || !(a->vdw_lambda_alpha >= 0.0) || !(a->vdw_lambda_exponent >= 1.0) ||
+      !(a->vdw_lambda_end > 0.0 && a->vdw_lambda_end <= 1.0)) {
+    h.err = "alchemy: soft flags required, vdw-lambda-alpha >= 0, vdw-lambda-exponent >= 1, 0 < vdw-lambda-end <= 1";
+    return FFXG_ERR_BAD_ARG;
+  }
+  const size_t N = h.n;
+  if (!h.d_soft) {
+    CK(dalloc(&h.d_soft, N));
+    CK(dalloc(&h.d_mol, N));
+    CK(dalloc(&h.d_lgred, 6 * N));
+  }
+  std::vector<int> soft(N), mol(N);
+  for (size_t i = 0; i < N; i++) {
+    soft[i] = a->soft[i] != 0;
+    mol[i] = a->molecule ? a->molecule[i] : (int)i;
+  }
+  CK(cudaMemcpy(h.d_soft, soft.data(), N * sizeof(int), cudaMemcpyHostToDevice));
+  CK(cudaMemcpy(h.d_mol, mol.data(), N * sizeof(int), cudaMemcpyHostToDevice));
+  h.alch_alpha = a->vdw_lambda_alpha;
+  h.alch_exponent = a->vdw_lambda_exponent;
+  h.alch_end = a->vdw_lambda_end;
+  h.alch.inter = a->intermolecular_softcore != 0;
+  h.alch.intra = a->intramolecular_softcore != 0;
+  h.alch.active = 1;
+  update_alchemy(h);
+  return FFXG_OK;
+}
+
+int ffxg_set_lambda(ffxg_handle *hh, double lambda) {
+  if (!hh) return FFXG_ERR_BAD_ARG;
+  Handle &h = hh->h;
+  if (!(lambda >= 0.0 && lambda <= 1.0)) { h.err = "lambda must lie in [0, 1]"; return FFXG_ERR_BAD_ARG; }
+  h.lambda = lambda;
+  update_alchemy(h);
+  return FFXG_OK;
+}
+
+int ffxg_get_dEdL(ffxg_handle *hh, double *dEdL, double *d2EdL2, double *dEdXdL) {
+  if (!hh) return FFXG_ERR_BAD_ARG;
+  Handle &h = hh->h;
+  if (dEdL) *dEdL = h.alch.active ? h.dEdL : 0.0;
+  if (d2EdL2) *d2EdL2 = h.alch.active ? h.d2EdL2 : 0.0;
+  if (dEdXdL) {
+    const size_t N = h.n;
+    if (!h.lgrad_valid) {
+      std::memset(dEdXdL, 0, 3 * N * sizeof(double));
+      return FFXG_OK;
+    }
+    std::vector<double> a(3 * N);
+    CK(cudaMemcpy(a.data(), h.d_lgred + 3 * N, 3 * N * sizeof(double), cudaMemcpyDeviceToHost));
+    for (size_t i = 0; i < N; i++)
+      for (int d = 0; d < 3; d++) dEdXdL[3 * i + d] = a[d * N + i];
+  }
   return FFXG_OK;
 }
 

@@ -299,7 +299,7 @@ __global__ void k_assemble(int n, const double *__restrict__ grad, const double 
 
 // Two-level deterministic sums: blocks reduce contiguous chunks in a fixed order.
 constexpr int kSumBlocks = 148;
-constexpr int kNE = 7, kNC = 2;
+constexpr int kNE = 9, kNC = 2;   // energy rows: vdW, perm real, pol real, 4 recip/self, dU/dL, d2U/dL2
 
 __global__ void k_sum_partial(int n, const double *__restrict__ eatom, const long long *__restrict__ catom,
                               double *pe, long long *pc) {

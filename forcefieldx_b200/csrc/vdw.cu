@@ -36,7 +36,9 @@ __global__ void __launch_bounds__(256) k_vdw(int n, const double *__restrict__ r
                                              const int *__restrict__ nbr_cnt, int cap, const int *__restrict__ eptr,
                                              const int *__restrict__ ek, const unsigned *__restrict__ ecode,
                                              const int *__restrict__ elo, const int *__restrict__ ehi, VdwForm vf,
-                                             ScaleTables c_vscales, int gradient, double *eatom, long long *catom, double *gred) {
+                                             ScaleTables c_vscales, int gradient, double *eatom, long long *catom, double *gred,
+                                             const int *__restrict__ soft, const int *__restrict__ mol, AlchConst al,
+                                             double *edl, double *ed2l, double *lgred) {
   const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const int lane = threadIdx.x & 31;
   if (warp >= n) return;
@@ -46,9 +48,11 @@ __global__ void __launch_bounds__(256) k_vdw(int n, const double *__restrict__ r
   const R delta = vf.delta, gamma = vf.gamma, gamma1 = vf.gamma1, t1n = vf.t1n;
   const R c0 = vf.c0, c1 = vf.c1, c2 = vf.c2, c3 = vf.c3, c4 = vf.c4, c5 = vf.c5;
   const R cut = vf.cut, iwidth = vf.iwidth;
-  double e = 0.0;
-  R gx = 0, gy = 0, gz = 0;
+  double e = 0.0, dl = 0.0, d2l = 0.0;
+  R gx = 0, gy = 0, gz = 0, lx = 0, ly = 0, lz = 0;
   long long cnt = 0;
+  const int soft_i = al.active ? soft[i] : 0;
+  const int mol_i = al.active ? mol[i] : 0;
   const int m = min(nbr_cnt[i], cap);
   const int *row = nbr + (size_t)i * cap;
   for (int a = lane; a < m; a += 32) {
@@ -63,7 +67,22 @@ __global__ void __launch_bounds__(256) k_vdw(int n, const double *__restrict__ r
     if (!(mask > R(0.0))) continue;
     const R dx = (R)dxd, dy = (R)dyd, dz = (R)dzd, r2 = (R)r2d;
     const R r = m_sqrt(r2);
+    // Softcore pair (VanDerWaals.java:1728-1761): exactly one atom soft, or both soft under
+    // the intermolecular / intramolecular softcore options.
+    bool spair = false;
+    if (al.active) {
+      const int sk = soft[k];
+      spair = (soft_i != sk);
+      if (soft_i && sk) {
+        const bool same = (mol_i == mol[k]);
+        if (al.inter && !same) spair = true;
+        else if (al.intra && same) spair = true;
+      }
+    }
+    const R alpha = spair ? (R)al.sc1 : R(0);
+    const R lambda5 = spair ? (R)al.sc2 : R(1);
     const R ev = mask * veps[ti * ntypes + tk];
+    const R eps_lambda = ev * lambda5;
     const R rho = r * irv;
     const R rho2 = rho * rho;
     const R rhoDisp1 = rho2 * rho2 * rho2;
@@ -71,12 +90,12 @@ __global__ void __launch_bounds__(256) k_vdw(int n, const double *__restrict__ r
     const R rd = rho + delta, rd2 = rd * rd;
     const R rhoDelta1 = rd2 * rd2 * rd2;
     const R rhoDelta = rhoDelta1 * rd;
-    const R t1d = R(1.0) / rhoDelta;
-    const R t2d = R(1.0) / (rhoDisp + gamma);
+    const R t1d = R(1.0) / (alpha + rhoDelta);
+    const R t2d = R(1.0) / (alpha + rhoDisp + gamma);
     const R t1 = t1n * t1d;
     const R t2a = gamma1 * t2d;
     const R t2 = t2a - R(2.0);
-    const R eik = ev * t1 * t2;
+    const R eik = eps_lambda * t1 * t2;
     R taper = R(1.0), dtaper = R(0.0);
     if (r2d > vf.cut2) {
       if (sizeof(R) == 8) {
@@ -93,25 +112,67 @@ __global__ void __launch_bounds__(256) k_vdw(int n, const double *__restrict__ r
     }
     e += R(0.5) * eik * taper;
     if (k > i) cnt++;
-    if (gradient) {
+    if (gradient || spair) {
       const R dt1d_dr = R(7.0) * rhoDelta1 * irv;
       const R dt2d_dr = R(7.0) * rhoDisp1 * irv;
       const R dt1_dr = t1 * dt1d_dr * t1d;
       const R dt2_dr = t2a * dt2d_dr * t2d;
-      const R dedr = -ev * (dt1_dr * t2 + t1 * dt2_dr);
+      const R dedr = -eps_lambda * (dt1_dr * t2 + t1 * dt2_dr);
       const R ir = R(1.0) / r;
-      const R dsw = eik * dtaper + dedr * taper;
-      gx += dsw * dx * ir; gy += dsw * dy * ir; gz += dsw * dz * ir;
+      if (gradient) {
+        const R dsw = eik * dtaper + dedr * taper;
+        gx += dsw * dx * ir; gy += dsw * dy * ir; gz += dsw * dz * ir;
+      }
+      if (spair) {
+        // dU/dL, d2U/dL2 and dU/dX dL of the softcore pair (VanDerWaals.java:1842-1880); each
+        // direction of the full list carries half of the pair's lambda derivatives.
+        const R dsc1 = (R)al.dsc1dL, d2sc1 = (R)al.d2sc1dL2, sc2 = (R)al.sc2, dsc2 = (R)al.dsc2dL;
+        const R d2sc2 = (R)al.d2sc2dL2;
+        const R dt1 = -t1 * t1d * dsc1;
+        const R dt2 = -t2a * t2d * dsc1;
+        const R dedl = ev * (dsc2 * t1 * t2 + sc2 * dt1 * t2 + sc2 * t1 * dt2);
+        dl += 0.5 * (double)(dedl * taper);
+        const R t1d2 = -dsc1 * t1d * t1d;
+        const R t2d2 = -dsc1 * t2d * t2d;
+        const R d2t1 = -dt1 * t1d * dsc1 - t1 * t1d * d2sc1 - t1 * t1d2 * dsc1;
+        const R d2t2 = -dt2 * t2d * dsc1 - t2a * t2d * d2sc1 - t2a * t2d2 * dsc1;
+        const R df1 = d2sc2 * t1 * t2 + dsc2 * dt1 * t2 + dsc2 * t1 * dt2;
+        const R df2 = dsc2 * dt1 * t2 + sc2 * d2t1 * t2 + sc2 * dt1 * dt2;
+        const R df3 = dsc2 * t1 * dt2 + sc2 * dt1 * dt2 + sc2 * t1 * d2t2;
+        d2l += 0.5 * (double)(ev * (df1 + df2 + df3) * taper);
+        if (gradient) {
+          const R t11 = -dsc2 * t2 * dt1_dr;
+          const R t21 = -dsc2 * t1 * dt2_dr;
+          const R t13 = R(2.0) * sc2 * t2 * dt1_dr * dsc1 * t1d;
+          const R t23 = R(2.0) * sc2 * t1 * dt2_dr * dsc1 * t2d;
+          const R t12 = -sc2 * dt2 * dt1_dr;
+          const R t22 = -sc2 * dt1 * dt2_dr;
+          const R dedldr = ev * (t11 + t12 + t13 + t21 + t22 + t23);
+          const R lsw = dedl * dtaper + dedldr * taper;
+          lx += lsw * dx * ir; ly += lsw * dy * ir; lz += lsw * dz * ir;
+        }
+      }
     }
   }
   e = warp_sum(e);
   const double Gx = warp_sum((double)gx), Gy = warp_sum((double)gy), Gz = warp_sum((double)gz);
 #pragma unroll
   for (int o = 16; o > 0; o >>= 1) cnt += __shfl_xor_sync(0xffffffffu, cnt, o);
+  if (al.active) {
+    dl = warp_sum(dl);
+    d2l = warp_sum(d2l);
+  }
+  double Lx = 0.0, Ly = 0.0, Lz = 0.0;
+  if (al.active && gradient) {
+    Lx = warp_sum((double)lx); Ly = warp_sum((double)ly); Lz = warp_sum((double)lz);
+  }
   if (lane == 0) {
     eatom[i] = e;
     catom[i] = cnt;
+    edl[i] = dl;
+    ed2l[i] = d2l;
     if (gradient) { gred[i] = Gx; gred[n + i] = Gy; gred[2 * n + i] = Gz; }
+    if (al.active && gradient) { lgred[i] = Lx; lgred[n + i] = Ly; lgred[2 * n + i] = Lz; }
   }
 }
 
@@ -155,13 +216,18 @@ void launch_vdw(Handle &h, bool grad) {
   kern<<<nblocks((int64_t)h.n * 32, 256), 256, 0, h.stream>>>(
       h.n, h.d_rx, h.d_ry, h.d_rz, h.box, h.d_vtype, h.ntypes, h.d_vrad, h.d_veps, h.d_nbr, h.d_nbr_cnt, h.cap_nbr,
       h.d_excl_ptr, h.d_excl_k, h.d_excl_code, h.d_excl_lo, h.d_excl_hi, vf, h.scales, grad ? 1 : 0, h.d_eatom, h.d_catom,
-      h.d_gred);
+      h.d_gred, h.d_soft, h.d_mol, h.alch, h.d_eatom + 7 * (size_t)h.n, h.d_eatom + 8 * (size_t)h.n, h.d_lgred);
   FFX_LAUNCHED(h);
   if (grad) {
     // Rows 3-5 of d_gred hold the distributed per-atom vdW gradient.
     k_vdw_distribute<<<nblocks(h.n, 256), 256, 0, h.stream>>>(h.n, h.d_gred, h.d_redp, h.d_redf, h.d_red_ptr,
                                                                h.d_red_child, h.d_gred + 3 * (size_t)h.n);
     FFX_LAUNCHED(h);
+    if (h.alch.active) {   // dU/dX dL rows 3-5 of d_lgred, distributed the same way
+      k_vdw_distribute<<<nblocks(h.n, 256), 256, 0, h.stream>>>(h.n, h.d_lgred, h.d_redp, h.d_redf, h.d_red_ptr,
+                                                                 h.d_red_child, h.d_lgred + 3 * (size_t)h.n);
+      FFX_LAUNCHED(h);
+    }
   }
 }
 

@@ -168,6 +168,26 @@ class ForceFieldEnergy:
     def stream(self) -> int:
         return int(self.lib.ffxg_stream(self._h) or 0)
 
+    def set_alchemy(self, alchemy) -> None:
+        """Soft atoms and vdW softcore keys (an Alchemy, or None to clear)."""
+        if alchemy is None:
+            self._check(self.lib.ffxg_set_alchemy(self._h, None))
+            return
+        a, keep = alchemy.c_struct(cabi)
+        self._check(self.lib.ffxg_set_alchemy(self._h, ctypes.byref(a)))
+
+    def set_lambda(self, lam: float) -> None:
+        """LambdaInterface.setLambda for the vdW softcore."""
+        self._check(self.lib.ffxg_set_lambda(self._h, float(lam)))
+
+    def get_dEdL(self):
+        """(dU/dL, d2U/dL2, dU/dX dL [n, 3]) of the last evaluation."""
+        d1 = ctypes.c_double()
+        d2 = ctypes.c_double()
+        g = np.zeros((self.n, 3))
+        self._check(self.lib.ffxg_get_dEdL(self._h, ctypes.byref(d1), ctypes.byref(d2), _dp(g)))
+        return d1.value, d2.value, g
+
     def set_graph_mode(self, on: bool) -> None:
         """Replay the evaluation as one captured CUDA graph (default) or launch directly."""
         self._check(self.lib.ffxg_set_graph_mode(self._h, 1 if on else 0))

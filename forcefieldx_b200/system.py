@@ -369,6 +369,28 @@ def water_params(edge: float, **kw) -> AmoebaParams:
     return AmoebaParams(**base)
 
 
+@dataclasses.dataclass
+class Alchemy:
+    """Soft atoms and vdW softcore keys (the reference's Atom.applyLambda flags and the
+    vdw-lambda-* / *-softcore keys, VanDerWaals.java:336-357)."""
+    soft: np.ndarray                      # [n] bool / 0-1
+    molecule: Optional[np.ndarray] = None  # [n] molecule index, or None (every atom its own)
+    vdw_lambda_alpha: float = 0.25
+    vdw_lambda_exponent: float = 3.0
+    vdw_lambda_end: float = 1.0
+    intermolecular_softcore: bool = False
+    intramolecular_softcore: bool = False
+
+    def c_struct(self, cabi):
+        soft = np.ascontiguousarray(self.soft, dtype=np.int32)
+        mol = None if self.molecule is None else np.ascontiguousarray(self.molecule, dtype=np.int32)
+        ptr = lambda a: a.ctypes.data_as(cabi._I) if a is not None else cabi._I()  # noqa: E731
+        a = cabi.FfxgAlchemy(ptr(soft), ptr(mol), float(self.vdw_lambda_alpha), float(self.vdw_lambda_exponent),
+                             float(self.vdw_lambda_end), int(self.intermolecular_softcore),
+                             int(self.intramolecular_softcore))
+        return a, (soft, mol)
+
+
 # The two named water workloads.
 WATER_24K = dict(n_side=20, edge=62.08, grid=(64, 64, 64))   # 8,000 waters, 24,000 atoms
 WATER_648 = dict(n_side=6, edge=18.643, grid=(20, 20, 20))  # 216 waters, 648 atoms

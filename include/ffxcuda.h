@@ -186,6 +186,38 @@ int ffxg_get_global_multipoles(ffxg_handle *h, double *mpole);
  * unordered (i, k) with i < k.  With pairs == NULL only *n_pairs is written. */
 int ffxg_get_neighbor_pairs(ffxg_handle *h, int32_t *pairs, int64_t *n_pairs);
 
+/* Alchemical state of the van der Waals term: which atoms carry lambda (Atom.applyLambda)
+ * and the softcore keys read by VanDerWaals (VanDerWaals.java:336-357).  soft[n] is
+ * 0/1; molecule[n] (may be NULL: every atom its own molecule) decides the both-soft
+ * intermolecular / intramolecular softcore options.  Defaults of the reference:
+ * vdw-lambda-alpha 0.25, vdw-lambda-exponent 3, vdw-lambda-end 1, both options off.
+ * A pair is softcore when exactly one atom is soft (or both, per the options); its
+ * energy is eps * L^n * t1 * t2 with alpha (1 - L)^2 added to both denominators
+ * (VanDerWaalsLoop, VanDerWaals.java:1723-1880).  Electrostatic lambda (permanent
+ * softcore and the OST polarization pieces) is not part of this library. */
+typedef struct ffxg_alchemy {
+  const int32_t *soft;
+  const int32_t *molecule;
+  double vdw_lambda_alpha;
+  double vdw_lambda_exponent;
+  double vdw_lambda_end;
+  int32_t intermolecular_softcore;
+  int32_t intramolecular_softcore;
+} ffxg_alchemy;
+
+/* Set (or, with a == NULL, clear) the soft atoms and softcore keys.  The state starts
+ * cleared and lambda at 1. */
+int ffxg_set_alchemy(ffxg_handle *h, const ffxg_alchemy *a);
+
+/* LambdaInterface.setLambda (P/bonded/LambdaInterface.java:47-99) for the vdW term:
+ * lambda in [0, 1], rescaled by vdw-lambda-end as VanDerWaals.setLambda (:599-647). */
+int ffxg_set_lambda(ffxg_handle *h, double lambda);
+
+/* dU/dL, d2U/dL2 and dU/dX dL (LambdaInterface getdEdL / getd2EdL2 / getdEdXdL) of the
+ * last evaluation: the vdW softcore contributions.  dEdXdL[n][3] (may be NULL) is filled
+ * only when that evaluation computed a gradient. */
+int ffxg_get_dEdL(ffxg_handle *h, double *dEdL, double *d2EdL2, double *dEdXdL);
+
 /* The CUDA stream (cudaStream_t) the handle launches on, for event timing. */
 void *ffxg_stream(ffxg_handle *h);
 

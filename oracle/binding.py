@@ -38,6 +38,10 @@ def lib():
         L.oracle_neighbor_pairs.restype = ctypes.c_int64
         L.oracle_neighbor_pairs.argtypes = [ctypes.POINTER(cabi.FfxgSystem), ctypes.POINTER(cabi.FfxgParams), D,
                                             ctypes.POINTER(ctypes.c_int32)]
+        L.oracle_set_alchemy.restype = None
+        L.oracle_set_alchemy.argtypes = [ctypes.POINTER(cabi.FfxgAlchemy), ctypes.c_int, ctypes.c_double]
+        L.oracle_get_dEdL.restype = None
+        L.oracle_get_dEdL.argtypes = [D, D, D]
         L.oracle_erfc.restype = ctypes.c_double
         L.oracle_erfc.argtypes = [ctypes.c_double]
         L.oracle_bspline.restype = None
@@ -52,9 +56,16 @@ def _dp(a):
     return a.ctypes.data_as(ctypes.POINTER(ctypes.c_double))
 
 
-def energy(system: AmoebaSystem, params: AmoebaParams, xyz=None, gradient=True, nthreads=0):
-    """Returns dict(terms, grad, counts, induced, induced_cr, global_mpole, status)."""
+def energy(system: AmoebaSystem, params: AmoebaParams, xyz=None, gradient=True, nthreads=0, alchemy=None,
+           lam=1.0):
+    """Returns dict(terms, grad, counts, induced, induced_cr, global_mpole, status), and with
+    an Alchemy also dEdL, d2EdL2 and dEdXdL (the vdW softcore at lambda `lam`)."""
     L = lib()
+    if alchemy is not None:
+        a, keep_a = alchemy.c_struct(cabi)
+        L.oracle_set_alchemy(ctypes.byref(a), system.n_atoms, float(lam))
+    else:
+        L.oracle_set_alchemy(None, system.n_atoms, 1.0)
     s, keep = system.c_struct(cabi)
     p = params_struct(params, cabi)
     n = system.n_atoms
@@ -68,8 +79,16 @@ def energy(system: AmoebaSystem, params: AmoebaParams, xyz=None, gradient=True, 
     st = L.oracle_energy(ctypes.byref(s), ctypes.byref(p), _dp(x), 1 if gradient else 0, int(nthreads),
                          _dp(terms), _dp(grad), counts.ctypes.data_as(ctypes.POINTER(ctypes.c_int64)),
                          _dp(ind), _dp(indcr), _dp(gm))
-    return dict(terms=terms, grad=grad, counts=counts, induced=ind, induced_cr=indcr,
-                global_mpole=gm, status=int(st))
+    out = dict(terms=terms, grad=grad, counts=counts, induced=ind, induced_cr=indcr, global_mpole=gm,
+               status=int(st))
+    if alchemy is not None:
+        d1 = ctypes.c_double()
+        d2 = ctypes.c_double()
+        lg = np.zeros((n, 3))
+        L.oracle_get_dEdL(ctypes.byref(d1), ctypes.byref(d2), _dp(lg))
+        out.update(dEdL=d1.value, d2EdL2=d2.value, dEdXdL=lg)
+        L.oracle_set_alchemy(None, n, 1.0)
+    return out
 
 
 def neighbor_pairs(system: AmoebaSystem, params: AmoebaParams, xyz=None) -> np.ndarray:

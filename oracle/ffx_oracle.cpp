@@ -206,6 +206,18 @@ void fft3d(std::vector<std::complex<double>> &g, int nx, int ny, int nz, int sig
 }
 
 // ---------------------------------------------------------------------------
+// Alchemical state of the vdW term (VanDerWaals.setLambda, :599-647; initSoftCore,
+// :1150-1180).  Set through oracle_set_alchemy, read by Oracle::vdw.
+struct Alchemy {
+  bool on = false;
+  std::vector<int> soft, mol;
+  double sc1 = 0, dsc1dL = 0, d2sc1dL2 = 0, sc2 = 1, dsc2dL = 0, d2sc2dL2 = 0;
+  bool inter = false, intra = false;
+  double dEdL = 0, d2EdL2 = 0;
+  std::vector<double> lgrad;   // [n][3] dU/dX dL
+};
+Alchemy g_alch;
+
 struct Oracle {
   // ---- inputs
   int n = 0;
@@ -376,10 +388,12 @@ struct Oracle {
     const double c3 = -10.0 * (a2 + 4.0 * a * b + b2) / den;
     const double c4 = 15.0 * (a + b) / den;
     const double c5 = -6.0 / den;
-    double energy = 0.0;
+    double energy = 0.0, dEdL = 0.0, d2EdL2 = 0.0;
     int64_t cnt = 0;
+    const Alchemy &al = g_alch;
     std::vector<std::vector<double>> tg(nthreads, std::vector<double>(3 * (size_t)n, 0.0));
-#pragma omp parallel reduction(+ : energy, cnt)
+    std::vector<std::vector<double>> tl(al.on ? nthreads : 0, std::vector<double>(3 * (size_t)n, 0.0));
+#pragma omp parallel reduction(+ : energy, cnt, dEdL, d2EdL2)
     {
       int tid = 0;
 #ifdef _OPENMP
@@ -403,7 +417,22 @@ struct Oracle {
           const double irv = vrad[(size_t)ti * ntypes + tk];
           if (!(r2 <= off2v && mask[k] > 0.0 && irv > 0.0)) continue;
           const double r = std::sqrt(r2);
+          // Softcore pair (VanDerWaals.java:1728-1761): exactly one atom soft, or both
+          // soft under the intermolecular / intramolecular softcore options.
+          bool soft = false;
+          if (al.on) {
+            const int si = al.soft[i], sk = al.soft[k];
+            soft = (si != sk);
+            if (si && sk) {
+              const bool same = al.mol[i] == al.mol[k];
+              if (al.inter && !same) soft = true;
+              else if (al.intra && same) soft = true;
+            }
+          }
+          const double alpha = soft ? al.sc1 : 0.0;
+          const double lambda5 = soft ? al.sc2 : 1.0;
           const double ev = mask[k] * veps[(size_t)ti * ntypes + tk];
+          const double eps_lambda = ev * lambda5;
           const double rho = r * irv;
           const double rho2 = rho * rho;
           const double rhoDisp1 = rho2 * rho2 * rho2;
@@ -411,12 +440,12 @@ struct Oracle {
           const double rd = rho + delta, rd2 = rd * rd;
           const double rhoDelta1 = rd2 * rd2 * rd2;
           const double rhoDelta = rhoDelta1 * rd;
-          const double t1d = 1.0 / (0.0 + rhoDelta);
-          const double t2d = 1.0 / (0.0 + rhoDisp + gamma);
+          const double t1d = 1.0 / (alpha + rhoDelta);
+          const double t2d = 1.0 / (alpha + rhoDisp + gamma);
           const double t1 = t1n * t1d;
           const double t2a = gamma1 * t2d;
           const double t2 = t2a - 2.0;
-          const double eik = ev * t1 * t2;
+          const double eik = eps_lambda * t1 * t2;
           double taper = 1.0, dtaper = 0.0;
           if (r2 > cut2) {
             const double r3 = r2 * r, r4 = r2 * r2, r5 = r2 * r3;
@@ -425,13 +454,50 @@ struct Oracle {
           }
           energy += eik * taper;
           cnt++;
-          if (!gradient) continue;
+          if (!gradient && !soft) continue;
           const double dt1d_dr = 7.0 * rhoDelta1 * irv;
           const double dt2d_dr = 7.0 * rhoDisp1 * irv;
           const double dt1_dr = t1 * dt1d_dr * t1d;
           const double dt2_dr = t2a * dt2d_dr * t2d;
-          const double dedr = -ev * (dt1_dr * t2 + t1 * dt2_dr);
+          const double dedr = -eps_lambda * (dt1_dr * t2 + t1 * dt2_dr);
           const double ir = 1.0 / r;
+          if (soft) {
+            // dU/dL, d2U/dL2 and dU/dX dL of the softcore pair (VanDerWaals.java:1842-1880).
+            const double dt1 = -t1 * t1d * al.dsc1dL;
+            const double dt2 = -t2a * t2d * al.dsc1dL;
+            const double f1 = al.dsc2dL * t1 * t2;
+            const double f2 = al.sc2 * dt1 * t2;
+            const double f3 = al.sc2 * t1 * dt2;
+            const double dedl = ev * (f1 + f2 + f3);
+            dEdL += dedl * taper;
+            const double t1d2 = -al.dsc1dL * t1d * t1d;
+            const double t2d2 = -al.dsc1dL * t2d * t2d;
+            const double d2t1 = -dt1 * t1d * al.dsc1dL - t1 * t1d * al.d2sc1dL2 - t1 * t1d2 * al.dsc1dL;
+            const double d2t2 = -dt2 * t2d * al.dsc1dL - t2a * t2d * al.d2sc1dL2 - t2a * t2d2 * al.dsc1dL;
+            const double df1 = al.d2sc2dL2 * t1 * t2 + al.dsc2dL * dt1 * t2 + al.dsc2dL * t1 * dt2;
+            const double df2 = al.dsc2dL * dt1 * t2 + al.sc2 * d2t1 * t2 + al.sc2 * dt1 * dt2;
+            const double df3 = al.dsc2dL * t1 * dt2 + al.sc2 * dt1 * dt2 + al.sc2 * t1 * d2t2;
+            d2EdL2 += ev * (df1 + df2 + df3) * taper;
+            if (gradient) {
+              const double t11 = -al.dsc2dL * t2 * dt1_dr;
+              const double t21 = -al.dsc2dL * t1 * dt2_dr;
+              const double t13 = 2.0 * al.sc2 * t2 * dt1_dr * al.dsc1dL * t1d;
+              const double t23 = 2.0 * al.sc2 * t1 * dt2_dr * al.dsc1dL * t2d;
+              const double t12 = -al.sc2 * dt2 * dt1_dr;
+              const double t22 = -al.sc2 * dt1 * dt2_dr;
+              const double dedldr = ev * (t11 + t12 + t13 + t21 + t22 + t23);
+              const double lsw = dedl * dtaper + dedldr * taper;
+              const double lx = lsw * dx * ir, ly = lsw * dy * ir, lz = lsw * dz * ir;
+              std::vector<double> &lg = tl[tid];
+              lg[3 * i] += lx * rv; lg[3 * i + 1] += ly * rv; lg[3 * i + 2] += lz * rv;
+              lg[3 * ri] += lx * rdv; lg[3 * ri + 1] += ly * rdv; lg[3 * ri + 2] += lz * rdv;
+              const int rk = redi[k];
+              const double red = redv[k], redk = 1.0 - red;
+              lg[3 * k] -= red * lx; lg[3 * k + 1] -= red * ly; lg[3 * k + 2] -= red * lz;
+              lg[3 * rk] -= redk * lx; lg[3 * rk + 1] -= redk * ly; lg[3 * rk + 2] -= redk * lz;
+            }
+          }
+          if (!gradient) continue;
           const double dswitch = eik * dtaper + dedr * taper;
           const double dedx = dswitch * dx * ir, dedy = dswitch * dy * ir, dedz = dswitch * dz * ir;
           g[3 * i] += dedx * rv; g[3 * i + 1] += dedy * rv; g[3 * i + 2] += dedz * rv;
@@ -449,6 +515,14 @@ struct Oracle {
     if (gradient)
       for (int t = 0; t < nthreads; t++)
         for (size_t j = 0; j < 3 * (size_t)n; j++) grad[j] += tg[t][j];
+    if (al.on) {
+      g_alch.dEdL = dEdL;
+      g_alch.d2EdL2 = d2EdL2;
+      g_alch.lgrad.assign(3 * (size_t)n, 0.0);
+      if (gradient)
+        for (int t = 0; t < nthreads; t++)
+          for (size_t j = 0; j < 3 * (size_t)n; j++) g_alch.lgrad[j] += tl[t][j];
+    }
     count = cnt;
     return energy;
   }
@@ -1966,6 +2040,35 @@ int64_t oracle_neighbor_pairs(const ffxg_system *sys, const ffxg_params *prm, co
       c++;
     }
   return c;
+}
+
+// Soft atoms and softcore keys for the next oracle_energy calls (NULL clears), at lambda.
+void oracle_set_alchemy(const ffxg_alchemy *a, int n, double lambda) {
+  g_alch = Alchemy();
+  if (!a) return;
+  g_alch.on = true;
+  g_alch.soft.assign(a->soft, a->soft + n);
+  g_alch.mol.resize(n);
+  for (int i = 0; i < n; i++) g_alch.mol[i] = a->molecule ? a->molecule[i] : i;
+  g_alch.inter = a->intermolecular_softcore != 0;
+  g_alch.intra = a->intramolecular_softcore != 0;
+  // VanDerWaals.setLambda (VanDerWaals.java:599-628).
+  double l = lambda;
+  if (l > a->vdw_lambda_end) l = 1.0; else l = l / a->vdw_lambda_end;
+  const double al = a->vdw_lambda_alpha, ex = a->vdw_lambda_exponent;
+  g_alch.sc1 = al * (1.0 - l) * (1.0 - l);
+  g_alch.dsc1dL = -2.0 * al * (1.0 - l);
+  g_alch.d2sc1dL2 = 2.0 * al;
+  g_alch.sc2 = std::pow(l, ex);
+  g_alch.dsc2dL = ex * std::pow(l, ex - 1.0);
+  g_alch.d2sc2dL2 = (ex >= 2.0) ? ex * (ex - 1.0) * std::pow(l, ex - 2.0) : 0.0;
+}
+
+// dU/dL, d2U/dL2 and dU/dX dL [n][3] of the last oracle_energy call.
+void oracle_get_dEdL(double *dEdL, double *d2EdL2, double *dEdXdL) {
+  if (dEdL) *dEdL = g_alch.dEdL;
+  if (d2EdL2) *d2EdL2 = g_alch.d2EdL2;
+  if (dEdXdL && !g_alch.lgrad.empty()) std::memcpy(dEdXdL, g_alch.lgrad.data(), g_alch.lgrad.size() * sizeof(double));
 }
 
 // Known-answer hooks for the numerics unit tests.

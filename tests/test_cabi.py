@@ -10,7 +10,7 @@ ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 
 def declared_symbols():
     text = open(os.path.join(ROOT, "include", "ffxcuda.h")).read()
-    return sorted(set(re.findall(r"\b(ffxg_[a-z_]+)\s*\(", text)))
+    return sorted(set(re.findall(r"\b(ffxg_[A-Za-z0-9_]+)\s*\(", text)))
 
 
 def test_header_and_binding_agree():
