@@ -58,6 +58,11 @@ class FfxgAlchemy(ctypes.Structure):
     ]
 
 
+class FfxgMd(ctypes.Structure):
+    _fields_ = [("mass", _D), ("n_settle", ctypes.c_int32), ("settle", _I), ("settle_d1", ctypes.c_double),
+                ("settle_d2", ctypes.c_double)]
+
+
 # Every symbol include/ffxcuda.h declares, with its ctypes signature.
 PROTOTYPES = {
     "ffxg_create": (ctypes.c_int, [ctypes.POINTER(FfxgSystem), ctypes.POINTER(FfxgParams),
@@ -74,6 +79,8 @@ PROTOTYPES = {
     "ffxg_set_alchemy": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(FfxgAlchemy)]),
     "ffxg_set_lambda": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_double]),
     "ffxg_get_dEdL": (ctypes.c_int, [ctypes.c_void_p, _D, _D, _D]),
+    "ffxg_md_setup": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(FfxgMd)]),
+    "ffxg_md_run": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_double, ctypes.c_int32, _D, _D, _D, _D]),
     "ffxg_stream": (ctypes.c_void_p, [ctypes.c_void_p]),
     "ffxg_last_launch_count": (ctypes.c_int64, [ctypes.c_void_p]),
     "ffxg_set_timing": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int]),

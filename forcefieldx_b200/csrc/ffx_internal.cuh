@@ -295,6 +295,14 @@ struct Handle {
   double *d_lgred = nullptr;                       // [6][n]: reduced-site and distributed dU/dX dL
   double dEdL = 0.0, d2EdL2 = 0.0;
   bool lgrad_valid = false;
+  // Molecular dynamics state (md.cu): masses, SETTLE molecules and the trajectory arrays
+  // (interleaved [n][3]): positions, velocities, accelerations, prior positions, gradient.
+  bool md_ready = false;
+  double *d_mass = nullptr, *d_mdx = nullptr, *d_mdv = nullptr, *d_mda = nullptr, *d_mdxp = nullptr;
+  double *d_mdg = nullptr, *d_mdke = nullptr;
+  int *d_settle = nullptr;
+  int n_settle = 0;
+  double settle_d1 = 0.0, settle_d2 = 0.0;
   PcgState *d_pcg = nullptr, *h_pcg = nullptr;
   // Graph execution: the whole evaluation captured once per gradient mode and replayed.
   bool use_graphs = true;
@@ -328,6 +336,9 @@ void launch_phi_induced(Handle &h);
 void launch_realspace_field(Handle &h);
 int run_pcg(Handle &h, bool capture);
 int pcg_partial_rows(int n);
+int md_setup(Handle &h, const ffxg_md *md);
+int md_run(Handle &h, double dt, int steps, double *xyz, double *vel, double *epot, double *ekin,
+           int (*force)(Handle &, const double *, double *, double *));
 void launch_recip_energy(Handle &h, bool grad);
 void launch_real_energy(Handle &h, bool grad);
 void launch_torque(Handle &h);

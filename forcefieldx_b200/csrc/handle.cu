@@ -338,7 +338,7 @@ static void free_all(Handle &h) {
                   h.d_uP, h.d_udirD, h.d_udirP, h.d_r, h.d_rP, h.d_zpre, h.d_zpreP, h.d_p, h.d_pP, h.d_vec, h.d_vecP,
                   h.d_partials, h.d_scalars, h.d_grid, h.d_influence, h.d_twiddle, h.d_gridf, h.d_influencef, h.d_twiddlef, h.d_grad, h.d_torque, h.d_gred,
                   h.d_eatom, h.d_catom, h.d_result, h.d_cresult, h.d_flags, h.d_xyz_in, h.d_grad_out,
-                  h.d_coefE, h.d_coefP, h.d_coefEB, h.d_coefPB, h.d_part2, h.d_counter, h.d_pos, h.d_recF, h.d_recP, h.d_tpair, h.d_tp, h.d_soft, h.d_mol, h.d_lgred};
+                  h.d_coefE, h.d_coefP, h.d_coefEB, h.d_coefPB, h.d_part2, h.d_counter, h.d_pos, h.d_recF, h.d_recP, h.d_tpair, h.d_tp, h.d_soft, h.d_mol, h.d_lgred, h.d_mass, h.d_mdx, h.d_mdv, h.d_mda, h.d_mdxp, h.d_mdg, h.d_mdke, h.d_settle};
   for (void *q : ptrs)
     if (q) cudaFree(q);
   if (h.h_scalars) cudaFreeHost(h.h_scalars);
@@ -782,6 +782,20 @@ int ffxg_get_dEdL(ffxg_handle *hh, double *dEdL, double *d2EdL2, double *dEdXdL)
       for (int d = 0; d < 3; d++) dEdXdL[3 * i + d] = a[d * N + i];
   }
   return FFXG_OK;
+}
+
+static int md_force(Handle &h, const double *d_xyz, double *d_grad, double *terms) {
+  return evaluate(h, d_xyz, d_grad, true, terms, nullptr);
+}
+
+int ffxg_md_setup(ffxg_handle *hh, const ffxg_md *md) {
+  if (!hh) return FFXG_ERR_BAD_ARG;
+  return md_setup(hh->h, md);
+}
+
+int ffxg_md_run(ffxg_handle *hh, double dt, int32_t n_steps, double *xyz, double *vel, double *epot, double *ekin) {
+  if (!hh) return FFXG_ERR_BAD_ARG;
+  return md_run(hh->h, dt, n_steps, xyz, vel, epot, ekin, md_force);
 }
 
 void *ffxg_stream(ffxg_handle *hh) { return hh ? (void *)hh->h.stream : nullptr; }

@@ -28,7 +28,8 @@ __device__ __forceinline__ unsigned vexcl_code(int i, int k, const int *__restri
   return 0u;
 }
 
-template <typename R>
+// ALCH: the softcore variant (launched only while soft atoms are set).
+template <typename R, bool ALCH>
 __global__ void __launch_bounds__(256) k_vdw(int n, const double *__restrict__ rx, const double *__restrict__ ry,
                                              const double *__restrict__ rz, Box bx, const int *__restrict__ vtype,
                                              int ntypes, const double *__restrict__ vrad,
@@ -51,8 +52,8 @@ __global__ void __launch_bounds__(256) k_vdw(int n, const double *__restrict__ r
   double e = 0.0, dl = 0.0, d2l = 0.0;
   R gx = 0, gy = 0, gz = 0, lx = 0, ly = 0, lz = 0;
   long long cnt = 0;
-  const int soft_i = al.active ? soft[i] : 0;
-  const int mol_i = al.active ? mol[i] : 0;
+  const int soft_i = ALCH ? soft[i] : 0;
+  const int mol_i = ALCH ? mol[i] : 0;
   const int m = min(nbr_cnt[i], cap);
   const int *row = nbr + (size_t)i * cap;
   for (int a = lane; a < m; a += 32) {
@@ -70,7 +71,7 @@ __global__ void __launch_bounds__(256) k_vdw(int n, const double *__restrict__ r
     // Softcore pair (VanDerWaals.java:1728-1761): exactly one atom soft, or both soft under
     // the intermolecular / intramolecular softcore options.
     bool spair = false;
-    if (al.active) {
+    if (ALCH) {
       const int sk = soft[k];
       spair = (soft_i != sk);
       if (soft_i && sk) {
@@ -112,7 +113,7 @@ __global__ void __launch_bounds__(256) k_vdw(int n, const double *__restrict__ r
     }
     e += R(0.5) * eik * taper;
     if (k > i) cnt++;
-    if (gradient || spair) {
+    if (gradient || (ALCH && spair)) {
       const R dt1d_dr = R(7.0) * rhoDelta1 * irv;
       const R dt2d_dr = R(7.0) * rhoDisp1 * irv;
       const R dt1_dr = t1 * dt1d_dr * t1d;
@@ -123,7 +124,7 @@ __global__ void __launch_bounds__(256) k_vdw(int n, const double *__restrict__ r
         const R dsw = eik * dtaper + dedr * taper;
         gx += dsw * dx * ir; gy += dsw * dy * ir; gz += dsw * dz * ir;
       }
-      if (spair) {
+      if (ALCH && spair) {
         // dU/dL, d2U/dL2 and dU/dX dL of the softcore pair (VanDerWaals.java:1842-1880); each
         // direction of the full list carries half of the pair's lambda derivatives.
         const R dsc1 = (R)al.dsc1dL, d2sc1 = (R)al.d2sc1dL2, sc2 = (R)al.sc2, dsc2 = (R)al.dsc2dL;
@@ -158,12 +159,12 @@ __global__ void __launch_bounds__(256) k_vdw(int n, const double *__restrict__ r
   const double Gx = warp_sum((double)gx), Gy = warp_sum((double)gy), Gz = warp_sum((double)gz);
 #pragma unroll
   for (int o = 16; o > 0; o >>= 1) cnt += __shfl_xor_sync(0xffffffffu, cnt, o);
-  if (al.active) {
+  if (ALCH) {
     dl = warp_sum(dl);
     d2l = warp_sum(d2l);
   }
   double Lx = 0.0, Ly = 0.0, Lz = 0.0;
-  if (al.active && gradient) {
+  if (ALCH && gradient) {
     Lx = warp_sum((double)lx); Ly = warp_sum((double)ly); Lz = warp_sum((double)lz);
   }
   if (lane == 0) {
@@ -172,7 +173,7 @@ __global__ void __launch_bounds__(256) k_vdw(int n, const double *__restrict__ r
     edl[i] = dl;
     ed2l[i] = d2l;
     if (gradient) { gred[i] = Gx; gred[n + i] = Gy; gred[2 * n + i] = Gz; }
-    if (al.active && gradient) { lgred[i] = Lx; lgred[n + i] = Ly; lgred[2 * n + i] = Lz; }
+    if (ALCH && gradient) { lgred[i] = Lx; lgred[n + i] = Ly; lgred[2 * n + i] = Lz; }
   }
 }
 
@@ -212,7 +213,8 @@ void launch_vdw(Handle &h, bool grad) {
   vf.c5 = -6.0 / den;
   vf.cut = cut;
   vf.iwidth = 1.0 / (off - cut);
-  auto kern = h.mixed ? k_vdw<float> : k_vdw<double>;
+  auto kern = h.alch.active ? (h.mixed ? k_vdw<float, true> : k_vdw<double, true>)
+                            : (h.mixed ? k_vdw<float, false> : k_vdw<double, false>);
   kern<<<nblocks((int64_t)h.n * 32, 256), 256, 0, h.stream>>>(
       h.n, h.d_rx, h.d_ry, h.d_rz, h.box, h.d_vtype, h.ntypes, h.d_vrad, h.d_veps, h.d_nbr, h.d_nbr_cnt, h.cap_nbr,
       h.d_excl_ptr, h.d_excl_k, h.d_excl_code, h.d_excl_lo, h.d_excl_hi, vf, h.scales, grad ? 1 : 0, h.d_eatom, h.d_catom,

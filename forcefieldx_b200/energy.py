@@ -188,6 +188,24 @@ class ForceFieldEnergy:
         self._check(self.lib.ffxg_get_dEdL(self._h, ctypes.byref(d1), ctypes.byref(d2), _dp(g)))
         return d1.value, d2.value, g
 
+    def md_setup(self, mass, settle=None, d1: float = 0.0, d2: float = 0.0) -> None:
+        """Masses (amu) and rigid three-site molecules [(centre, partner, partner), ...] for md_run."""
+        self._md_mass = np.ascontiguousarray(mass, dtype=np.float64)
+        self._md_settle = None if settle is None else np.ascontiguousarray(settle, dtype=np.int32).reshape(-1, 3)
+        ns = 0 if self._md_settle is None else self._md_settle.shape[0]
+        md = cabi.FfxgMd(_dp(self._md_mass), ns,
+                         self._md_settle.ctypes.data_as(cabi._I) if ns else cabi._I(), float(d1), float(d2))
+        self._check(self.lib.ffxg_md_setup(self._h, ctypes.byref(md)))
+
+    def md_run(self, xyz, vel, dt: float, n_steps: int):
+        """Velocity Verlet on the device; returns (xyz, vel, epot[n_steps], ekin[n_steps])."""
+        x = np.ascontiguousarray(xyz, dtype=np.float64).copy()
+        v = np.ascontiguousarray(vel, dtype=np.float64).copy()
+        ep = np.zeros(n_steps)
+        ek = np.zeros(n_steps)
+        self._check(self.lib.ffxg_md_run(self._h, float(dt), int(n_steps), _dp(x), _dp(v), _dp(ep), _dp(ek)))
+        return x, v, ep, ek
+
     def set_graph_mode(self, on: bool) -> None:
         """Replay the evaluation as one captured CUDA graph (default) or launch directly."""
         self._check(self.lib.ffxg_set_graph_mode(self._h, 1 if on else 0))

@@ -218,6 +218,29 @@ int ffxg_set_lambda(ffxg_handle *h, double lambda);
  * only when that evaluation computed a gradient. */
 int ffxg_get_dEdL(ffxg_handle *h, double *dEdL, double *d2EdL2, double *dEdXdL);
 
+/* Molecular dynamics on the device: VelocityVerlet (algorithms/.../integrators/
+ * VelocityVerlet.java:73-120) with SettleConstraint rigid three-site molecules
+ * (P/constraint/SettleConstraint.java), the counterpart of MolecularDynamics.mainLoop
+ * (MolecularDynamics.java:1488-1560) for this library's vdW + PME potential.  mass[n]
+ * in amu (0 freezes an atom); settle[n_settle][3] lists each rigid molecule as its
+ * centre atom and two partners at distance settle_d1 from the centre and settle_d2 from
+ * each other (water: O, H, H; 0.9572 A and 1.5139 A for 104.52 degrees). */
+typedef struct ffxg_md {
+  const double *mass;
+  int32_t n_settle;
+  const int32_t *settle;
+  double settle_d1;
+  double settle_d2;
+} ffxg_md;
+int ffxg_md_setup(ffxg_handle *h, const ffxg_md *md);
+
+/* Integrate n_steps of dt (ps) from xyz[n][3] (A) and vel[n][3] (A/ps), both updated in
+ * place.  Forces are this library's energy gradient; units follow the reference
+ * (a = -418.4 g / m).  epot[n_steps] and ekin[n_steps] (kcal/mol, may be NULL) receive
+ * the potential energy after each step's force evaluation and the kinetic energy after
+ * its closing half kick.  Positions and velocities stay on the device between steps. */
+int ffxg_md_run(ffxg_handle *h, double dt, int32_t n_steps, double *xyz, double *vel, double *epot, double *ekin);
+
 /* The CUDA stream (cudaStream_t) the handle launches on, for event timing. */
 void *ffxg_stream(ffxg_handle *h);
 
