@@ -325,6 +325,72 @@ def run_reference(args):
     }))
 
 
+def run_accuracy(args):
+    """Mixed form vs FP64 on frames of a 300 K trajectory of the 24k box.
+
+    The trajectory is run on the device (velocity Verlet + SETTLE, 2 fs, FP64 forces,
+    velocity rescaling to 300 K every 10 steps after a hot lattice start); every 10th step
+    after equilibration is a frame.  Each frame is evaluated in both forms; the FP64 form
+    is itself checked against the CPU oracle on the first and last frames.  Prints one JSON
+    line with per-term absolute and relative errors and the force RMS error."""
+    import math
+    from forcefieldx_b200.energy import ForceFieldEnergy
+    from oracle import binding as ob
+
+    system = build_system()
+    n = system.n_atoms
+    kcal, kb = 418.4, 0.0019872041
+    mass = np.where(np.arange(n) % 3 == 0, 15.999, 1.008)
+    settle = np.arange(n).reshape(-1, 3)
+    roh, theta = 0.9572, math.radians(104.52)
+    rhh = 2.0 * roh * math.sin(theta / 2.0)
+    dof = 2.0 * n                     # 9 - 3 constraints per water
+    rng = np.random.default_rng(300)
+    vel = rng.normal(size=(n, 3)) * np.sqrt(kb * 300.0 * kcal / mass)[:, None]
+    x = system.xyz.copy()
+    frames = []
+    with ForceFieldEnergy(system, build_params(PRECISION_FP64)) as md:
+        md.md_setup(mass, settle, roh, rhh)
+        for chunk in range(args.accuracy_equil // 10 + 10 * args.accuracy_frames // 10):
+            x, vel, ep, ek = md.md_run(x, vel, 0.002, 10)
+            temp = 2.0 * ek[-1] / (dof * kb)
+            vel *= math.sqrt(300.0 / temp)
+            if chunk >= args.accuracy_equil // 10:
+                frames.append(x.copy())
+    frames = frames[:args.accuracy_frames]
+    f64 = ForceFieldEnergy(system, build_params(PRECISION_FP64))
+    mix = ForceFieldEnergy(system, build_params(PRECISION_MIXED))
+    err_terms, rel_total, grad_rms, pins = [], [], [], []
+    for k, xf in enumerate(frames):
+        _, g64 = f64.energy_and_gradient(xf)
+        t64 = f64.terms.copy()
+        _, gm = mix.energy_and_gradient(xf)
+        tm = mix.terms.copy()
+        err_terms.append(np.abs(tm - t64))
+        rel_total.append(abs(tm[9] - t64[9]) / abs(t64[9]))
+        grad_rms.append(float(np.sqrt(np.mean((gm - g64) ** 2))))
+        if k in (0, len(frames) - 1):
+            ref = ob.energy(system, build_params(PRECISION_FP64), xyz=xf)
+            pins.append({"frame": k, "fp64_vs_oracle_total_rel": abs(t64[9] - ref["terms"][9]) / abs(ref["terms"][9]),
+                         "fp64_vs_oracle_grad_rms": float(np.sqrt(np.mean((g64 - ref["grad"]) ** 2))),
+                         "mixed_vs_oracle_total_rel": abs(tm[9] - ref["terms"][9]) / abs(ref["terms"][9]),
+                         "mixed_vs_oracle_grad_rms": float(np.sqrt(np.mean((gm - ref["grad"]) ** 2)))})
+    f64.close()
+    mix.close()
+    et = np.array(err_terms)
+    names = ["vdw", "permanent", "polarization", "perm_real", "perm_self", "perm_recip", "pol_real", "pol_self",
+             "pol_recip", "total"]
+    print(json.dumps({
+        "metric": "mixed-precision error vs FP64, 24k-atom water box, frames of a 300 K trajectory",
+        "frames": len(frames), "trajectory": "2 fs velocity Verlet + SETTLE on the device, FP64 forces, rescaled "
+                                             "to 300 K every 10 steps, frame every 10 steps after equilibration",
+        "term_abs_error_max": dict(zip(names, et.max(0).tolist())),
+        "term_abs_error_mean": dict(zip(names, et.mean(0).tolist())),
+        "total_rel_error_max": float(max(rel_total)), "total_rel_error_mean": float(np.mean(rel_total)),
+        "grad_rms_error_max": float(max(grad_rms)), "grad_rms_error_mean": float(np.mean(grad_rms)),
+        "oracle_pins": pins}))
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -334,7 +400,13 @@ def main():
     ap.add_argument("--precision", default="both", choices=["both", "fp64", "mixed"])
     ap.add_argument("--cpu-samples", type=int, default=2)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--accuracy-frames", type=int, default=0,
+                    help="instead of timing, report the mixed form's error on this many trajectory frames")
+    ap.add_argument("--accuracy-equil", type=int, default=200, help="equilibration steps before the first frame")
     args = ap.parse_args()
+    if args.accuracy_frames > 0:
+        run_accuracy(args)
+        return
     if args.warmup < 3 and args.impl == "mine":
         args.warmup = 3
     if args.impl == "reference":

@@ -304,6 +304,9 @@ struct Handle {
   int n_settle = 0;
   double settle_d1 = 0.0, settle_d2 = 0.0;
   PcgState *d_pcg = nullptr, *h_pcg = nullptr;
+  int scf_predictor = FFXG_PREDICTOR_NONE;
+  double *d_aspc = nullptr;                         // [6][6][n] ASPC ring of u - u_dir
+  int *d_aspc_state = nullptr;                      // most recent slot, slots stored
   // Graph execution: the whole evaluation captured once per gradient mode and replayed.
   bool use_graphs = true;
   bool want_grad = true;                            // gradient requested by the current call

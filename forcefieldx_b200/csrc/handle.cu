@@ -338,7 +338,7 @@ static void free_all(Handle &h) {
                   h.d_uP, h.d_udirD, h.d_udirP, h.d_r, h.d_rP, h.d_zpre, h.d_zpreP, h.d_p, h.d_pP, h.d_vec, h.d_vecP,
                   h.d_partials, h.d_scalars, h.d_grid, h.d_influence, h.d_twiddle, h.d_gridf, h.d_influencef, h.d_twiddlef, h.d_grad, h.d_torque, h.d_gred,
                   h.d_eatom, h.d_catom, h.d_result, h.d_cresult, h.d_flags, h.d_xyz_in, h.d_grad_out,
-                  h.d_coefE, h.d_coefP, h.d_coefEB, h.d_coefPB, h.d_part2, h.d_counter, h.d_pos, h.d_recF, h.d_recP, h.d_tpair, h.d_tp, h.d_soft, h.d_mol, h.d_lgred, h.d_mass, h.d_mdx, h.d_mdv, h.d_mda, h.d_mdxp, h.d_mdg, h.d_mdke, h.d_settle};
+                  h.d_coefE, h.d_coefP, h.d_coefEB, h.d_coefPB, h.d_part2, h.d_counter, h.d_pos, h.d_recF, h.d_recP, h.d_tpair, h.d_tp, h.d_soft, h.d_mol, h.d_lgred, h.d_mass, h.d_mdx, h.d_mdv, h.d_mda, h.d_mdxp, h.d_mdg, h.d_mdke, h.d_settle, h.d_aspc, h.d_aspc_state};
   for (void *q : ptrs)
     if (q) cudaFree(q);
   if (h.h_scalars) cudaFreeHost(h.h_scalars);
@@ -781,6 +781,23 @@ int ffxg_get_dEdL(ffxg_handle *hh, double *dEdL, double *d2EdL2, double *dEdXdL)
     for (size_t i = 0; i < N; i++)
       for (int d = 0; d < 3; d++) dEdXdL[3 * i + d] = a[d * N + i];
   }
+  return FFXG_OK;
+}
+
+int ffxg_set_scf_predictor(ffxg_handle *hh, int predictor) {
+  if (!hh) return FFXG_ERR_BAD_ARG;
+  Handle &h = hh->h;
+  if (predictor != FFXG_PREDICTOR_NONE && predictor != FFXG_PREDICTOR_ASPC) {
+    h.err = "unknown SCF predictor";
+    return FFXG_ERR_BAD_ARG;
+  }
+  if (predictor == FFXG_PREDICTOR_ASPC && !h.d_aspc) {
+    CK(dalloc(&h.d_aspc, 36 * (size_t)h.n));
+    CK(dalloc(&h.d_aspc_state, 2));
+  }
+  if (h.d_aspc_state) CK(cudaMemset(h.d_aspc_state, 0, 2 * sizeof(int)));
+  h.scf_predictor = predictor;
+  drop_graphs(h);
   return FFXG_OK;
 }
 

@@ -99,28 +99,32 @@ __device__ __forceinline__ void block_store_lane0(const double *v, double *part)
 }
 
 // Fixed-order totals of the first NV columns of nrows partial rows into tot[t0 ..], by
-// one block (thread t sums rows t, t + 256, ...; the 256 sums are added in thread order).
+// one block of 1024 threads (thread t sums rows t, t + 1024, ...; the per-thread sums are
+// added in thread order by a fixed warp tree).
 // BETA: then beta = r.z_new / r.z_old for both systems (a zero r.z_old counts as 1).
 template <int NV, bool BETA>
-__global__ void __launch_bounds__(256) k_pcg_totals(const double *__restrict__ part, int nrows, double *tot, int t0) {
-  __shared__ double sh[NV][256];
+__global__ void __launch_bounds__(1024) k_pcg_totals(const double *__restrict__ part, int nrows, double *tot, int t0) {
+  __shared__ double sh[NV][32];
   double s[NV];
 #pragma unroll
   for (int q = 0; q < NV; q++) s[q] = 0.0;
-  for (int b = threadIdx.x; b < nrows; b += 256)
+  for (int b = threadIdx.x; b < nrows; b += 1024)
 #pragma unroll
     for (int q = 0; q < NV; q++) s[q] += part[b * 8 + q];
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
 #pragma unroll
-  for (int q = 0; q < NV; q++) sh[q][threadIdx.x] = s[q];
-  __syncthreads();
-  if (threadIdx.x < NV) {
-    double t = 0.0;
-    for (int k = 0; k < 256; k++) t += sh[threadIdx.x][k];
-    tot[t0 + threadIdx.x] = t;
+  for (int q = 0; q < NV; q++) {
+    const double w = warp_sum(s[q]);
+    if (lane == 0) sh[q][wid] = w;
   }
-  if (BETA) {
-    __syncthreads();
-    if (threadIdx.x == 0) {
+  __syncthreads();
+  if (wid == 0) {
+#pragma unroll
+    for (int q = 0; q < NV; q++) {
+      const double t = warp_sum(sh[q][lane]);
+      if (lane == 0) tot[t0 + q] = t;
+    }
+    if (BETA && lane == 0) {
       double old = tot[T_RZ], oldP = tot[T_RZP];
       if (old == 0.0) old = 1.0;
       if (oldP == 0.0) oldP = 1.0;
@@ -429,6 +433,69 @@ __global__ void __launch_bounds__(kVecThreads) k_pcg_update(
 }
 
 // ---------------------------------------------------------------------------
+// Always-stable predictor-corrector initial guess (SCFPredictorParameters.aspcPredictor,
+// pme/SCFPredictorParameters.java:80-123; saveMutualInducedDipoles, :269-303).  The ring
+// ring[6][6][n] holds u - u_dir (D xyz, CR xyz) of the last six converged solves; state[0]
+// is the slot of the most recent one and state[1] how many are stored.  With six stored,
+// the solve starts from u = u_dir + sum_k c_k ring[(state[0] + k) % 6].
+__global__ void k_aspc_predict(int n, const double *__restrict__ ring, const int *__restrict__ state,
+                               const double *__restrict__ udD, const double *__restrict__ udP, double *uD, double *uP,
+                               void *recF, int mixed) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n || state[1] < 6) return;
+  const double c[6] = {22.0 / 7.0, -55.0 / 14.0, 55.0 / 21.0, -22.0 / 21.0, 5.0 / 21.0, -1.0 / 42.0};
+  double u[6];
+  for (int q = 0; q < 6; q++) u[q] = (q < 3) ? udD[q * n + i] : udP[(q - 3) * n + i];
+  int slot = state[0];
+  for (int k = 0; k < 6; k++) {
+    for (int q = 0; q < 6; q++) u[q] += c[k] * ring[((size_t)slot * 6 + q) * n + i];
+    slot = (slot + 1 == 6) ? 0 : slot + 1;
+  }
+  for (int d = 0; d < 3; d++) {
+    uD[d * n + i] = u[d];
+    uP[d * n + i] = u[3 + d];
+  }
+  if (mixed) put_rec(reinterpret_cast<float *>(recF), i, u[0], u[1], u[2], u[3], u[4], u[5]);
+  else put_rec(reinterpret_cast<double *>(recF), i, u[0], u[1], u[2], u[3], u[4], u[5]);
+}
+
+// Store u - u_dir of a converged solve in the slot before state[0] (k_aspc_commit then
+// advances the state); nothing is stored after a failed solve or a list overflow.
+__global__ void k_aspc_save(int n, double *ring, const int *__restrict__ state, const double *__restrict__ uD,
+                            const double *__restrict__ uP, const double *__restrict__ udD,
+                            const double *__restrict__ udP, const PcgState *__restrict__ st, const int *flags) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n || st->status != FFXG_OK) return;
+  if (*flags & (FLAG_NBR_OVERFLOW | FLAG_EWALD_OVERFLOW | FLAG_PRECOND_OVERFLOW | FLAG_NONFINITE)) return;
+  const int slot = (state[0] + 5) % 6;
+  for (int d = 0; d < 3; d++) {
+    ring[((size_t)slot * 6 + d) * n + i] = uD[d * n + i] - udD[d * n + i];
+    ring[((size_t)slot * 6 + 3 + d) * n + i] = uP[d * n + i] - udP[d * n + i];
+  }
+}
+
+__global__ void k_aspc_commit(int *state, const PcgState *__restrict__ st, const int *flags) {
+  if (st->status != FFXG_OK) return;
+  if (*flags & (FLAG_NBR_OVERFLOW | FLAG_EWALD_OVERFLOW | FLAG_PRECOND_OVERFLOW | FLAG_NONFINITE)) return;
+  state[0] = (state[0] + 5) % 6;
+  if (state[1] < 6) state[1] += 1;
+}
+
+static void aspc_predict(Handle &h) {
+  if (h.scf_predictor != FFXG_PREDICTOR_ASPC) return;
+  k_aspc_predict<<<nblocks(h.n, 256), 256, 0, h.stream>>>(h.n, h.d_aspc, h.d_aspc_state, h.d_udirD, h.d_udirP, h.d_uD,
+                                                           h.d_uP, h.d_recF, h.mixed ? 1 : 0);
+  FFX_LAUNCHED(h);
+}
+
+static void aspc_save(Handle &h) {
+  if (h.scf_predictor != FFXG_PREDICTOR_ASPC) return;
+  k_aspc_save<<<nblocks(h.n, 256), 256, 0, h.stream>>>(h.n, h.d_aspc, h.d_aspc_state, h.d_uD, h.d_uP, h.d_udirD,
+                                                        h.d_udirP, h.d_pcg, h.d_flags);
+  k_aspc_commit<<<1, 1, 0, h.stream>>>(h.d_aspc_state, h.d_pcg, h.d_flags);
+  h.launches += 2;
+}
+
 static double aewald3_of(const Handle &h) {
   const double a = h.prm.ewald_alpha;
   return 4.0 / 3.0 * pow(a, 3.0) / 1.7724538509055160273;
@@ -463,7 +530,7 @@ static void combine(Handle &h, const double *vD, const double *vP, bool first, d
       outP, reinterpret_cast<T *>(h.d_recP), part_region(h, 0), h.d_counter + K_FIELD, h.d_scalars);
   FFX_LAUNCHED(h);
   if (MODE == 2) {
-    k_pcg_totals<4, false><<<1, 256, 0, h.stream>>>(part_region(h, 0), nblocks((int64_t)h.n * 32, 256), h.d_scalars,
+    k_pcg_totals<4, false><<<1, 1024, 0, h.stream>>>(part_region(h, 0), nblocks((int64_t)h.n * 32, 256), h.d_scalars,
                                                    T_PAP);
     FFX_LAUNCHED(h);
   }
@@ -500,7 +567,7 @@ static void precond(Handle &h) {
       h.d_counter + K_PRECOND, h.d_scalars);
   FFX_LAUNCHED(h);
   if (!INIT) {
-    k_pcg_totals<2, true><<<1, 256, 0, h.stream>>>(part_region(h, 1), kFieldBlocks, h.d_scalars, T_RZN);
+    k_pcg_totals<2, true><<<1, 1024, 0, h.stream>>>(part_region(h, 1), kFieldBlocks, h.d_scalars, T_RZN);
     FFX_LAUNCHED(h);
   }
 }
@@ -541,6 +608,7 @@ static void pcg_precond(Handle &h) {
 int run_pcg(Handle &h, bool capture) {
   k_pcg_reset<<<1, 1, 0, h.stream>>>(h.d_pcg);
   FFX_LAUNCHED(h);
+  aspc_predict(h);
   // Field of the direct dipoles (u == u_dir at entry) gives the initial residual.
   field_of<1>(h, h.d_uD, h.d_uP, true, h.d_r, h.d_rP);
   int tk = timer_begin(h, FFXG_STAGE_PRECOND);
@@ -556,6 +624,7 @@ int run_pcg(Handle &h, bool capture) {
       if (!h.h_pcg->cont) break;
       pcg_precond(h);
     }
+    aspc_save(h);
     h.scf_iter = h.h_pcg->iter;
     return h.h_pcg->status;
   }
@@ -590,6 +659,7 @@ int run_pcg(Handle &h, bool capture) {
   h.graph_body_launches = h.launches - before;
   h.stream = main;
   if (cudaStreamEndCapture(h.side, &body) != cudaSuccess) return FFXG_ERR_CUDA;
+  aspc_save(h);   // after the while node
   return FFXG_OK;
 }
 

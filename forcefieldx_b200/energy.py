@@ -206,6 +206,10 @@ class ForceFieldEnergy:
         self._check(self.lib.ffxg_md_run(self._h, float(dt), int(n_steps), _dp(x), _dp(v), _dp(ep), _dp(ek)))
         return x, v, ep, ek
 
+    def set_scf_predictor(self, aspc: bool) -> None:
+        """Start each PCG solve from the ASPC prediction (the scf-predictor key) or not."""
+        self._check(self.lib.ffxg_set_scf_predictor(self._h, 1 if aspc else 0))
+
     def set_graph_mode(self, on: bool) -> None:
         """Replay the evaluation as one captured CUDA graph (default) or launch directly."""
         self._check(self.lib.ffxg_set_graph_mode(self._h, 1 if on else 0))

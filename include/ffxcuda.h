@@ -241,6 +241,15 @@ int ffxg_md_setup(ffxg_handle *h, const ffxg_md *md);
  * its closing half kick.  Positions and velocities stay on the device between steps. */
 int ffxg_md_run(ffxg_handle *h, double dt, int32_t n_steps, double *xyz, double *vel, double *epot, double *ekin);
 
+/* SCF predictor for the PCG starting guess (the scf-predictor key, ParticleMeshEwald.java:
+ * 540-550): FFXG_PREDICTOR_ASPC is the always-stable predictor of
+ * SCFPredictorParameters.aspcPredictor (pme/SCFPredictorParameters.java:80-123), which
+ * starts each solve from the direct dipoles plus a fixed combination of the last six
+ * converged (u - u_direct); it applies once six solves are stored and leaves the
+ * converged result unchanged up to polar-eps.  Setting a predictor clears the history. */
+enum { FFXG_PREDICTOR_NONE = 0, FFXG_PREDICTOR_ASPC = 1 };
+int ffxg_set_scf_predictor(ffxg_handle *h, int predictor);
+
 /* The CUDA stream (cudaStream_t) the handle launches on, for event timing. */
 void *ffxg_stream(ffxg_handle *h);
 

@@ -122,3 +122,32 @@ def test_md_nve_conserves_energy_and_geometry():
     drift = np.abs(etot - etot[0]).max()
     print(f"NVE 200 x 1 fs: E0={etot[0]:.4f} max|E-E0|={drift:.4f} kcal/mol, mean KE={ek.mean():.2f}")
     assert drift < 1e-3 * ek.mean() * 10, drift
+
+
+def test_aspc_predictor_cuts_iterations_and_keeps_the_solution():
+    """Along a smooth path of configurations the ASPC guess (after six stored solves)
+    lowers the PCG iteration count; every result still agrees with the oracle's solve
+    from the direct dipoles to the convergence tolerance."""
+    s, p, mass, settle, vel = _system(seed=2)
+    with ForceFieldEnergy(s, p) as ffe:
+        ffe.md_setup(mass, settle, ROH, RHH)
+        path = [s.xyz]
+        x, v = s.xyz, vel
+        for _ in range(9):
+            x, v, _, _ = ffe.md_run(x, v, 0.001, 1)
+            path.append(x)
+    iters = {}
+    for aspc in (False, True):
+        with ForceFieldEnergy(s, p) as ffe:
+            ffe.set_scf_predictor(aspc)
+            iters[aspc] = []
+            for k, x in enumerate(path):
+                e, g = ffe.energy_and_gradient(x)
+                iters[aspc].append(int(ffe.count("scf_iter")))
+                if aspc and k >= 6:
+                    ref = ob.energy(s, p, xyz=x)
+                    assert abs(ffe.terms[2] - ref["terms"][2]) < 1e-6 * abs(ref["terms"][2])
+                    assert float(np.sqrt(np.mean((g - ref["grad"]) ** 2))) < 1e-4
+    print("PCG iterations without / with ASPC:", iters[False], iters[True])
+    assert iters[True][:6] == iters[False][:6]
+    assert sum(iters[True][6:]) < sum(iters[False][6:])
