@@ -20,7 +20,7 @@ from __future__ import annotations
 import ctypes
 import dataclasses
 import math
-from typing import List, Optional, Sequence
+from typing import List, Optional, Sequence, Tuple
 
 import numpy as np
 
@@ -305,11 +305,20 @@ def _random_rotation(rng: np.random.Generator) -> np.ndarray:
                      [2 * (x * z - y * w), 2 * (y * z + x * w), 1 - 2 * (x * x + y * y)]])
 
 
-def water_box(n_side: int, edge: float, seed: int = 2026, jitter: float = 0.15) -> AmoebaSystem:
+def water_box(n_side: int, edge: float, seed: int = 2026, jitter: float = 0.15,
+              n_waters: Optional[int] = None) -> AmoebaSystem:
     """``n_side``^3 rigid AMOEBA waters on a seeded jittered cubic lattice in a cube
-    of ``edge`` A, uniform random orientations, O-H 0.9572 A, H-O-H 104.52 deg."""
+    of ``edge`` A, uniform random orientations, O-H 0.9572 A, H-O-H 104.52 deg.
+    With ``n_waters`` set, that many sites of the lattice are drawn without replacement
+    (``n_side`` is then the lattice size, at least the cube root of ``n_waters``)."""
     rng = np.random.default_rng(seed)
     nw = n_side ** 3
+    sites = None
+    if n_waters is not None:
+        if n_waters > nw:
+            raise ValueError("n_waters exceeds the lattice")
+        sites = set(rng.choice(nw, size=n_waters, replace=False).tolist())
+        nw = n_waters
     spacing = edge / n_side
     roh, theta = 0.9572, math.radians(104.52)
     local = np.array([[0.0, 0.0, 0.0],
@@ -317,9 +326,13 @@ def water_box(n_side: int, edge: float, seed: int = 2026, jitter: float = 0.15) 
                       [-roh * math.sin(theta / 2), 0.0, roh * math.cos(theta / 2)]])
     xyz = np.zeros((3 * nw, 3))
     m = 0
+    site = -1
     for a in range(n_side):
         for b in range(n_side):
             for c in range(n_side):
+                site += 1
+                if sites is not None and site not in sites:
+                    continue
                 origin = (np.array([a, b, c]) + 0.5) * spacing - 0.5 * edge
                 origin = origin + rng.uniform(-jitter, jitter, size=3)
                 rot = _random_rotation(rng)
@@ -359,6 +372,44 @@ def water_box(n_side: int, edge: float, seed: int = 2026, jitter: float = 0.15) 
                         red_factor=red_factor, vdw_inv_rmin=inv, vdw_eps=ee, n12=n12, n13=n13,
                         n14=n14, n15=n15, ip11=ip11, molecule=np.arange(n) // 3,
                         name=f"water{nw}")
+
+
+def small_water_box(n_atoms: int, seed: int = 2026) -> Tuple[AmoebaSystem, float]:
+    """A water box of ``n_atoms`` (a multiple of 3) at 29.915 A^3 per molecule, the
+    density of the batched small-system workload: returns (system, edge)."""
+    if n_atoms % 3:
+        raise ValueError("n_atoms must be a multiple of 3")
+    nw = n_atoms // 3
+    edge = (nw * 29.915) ** (1.0 / 3.0)
+    n_side = int(math.ceil(nw ** (1.0 / 3.0) - 1e-9))
+    return water_box(n_side, edge, seed=seed, n_waters=nw, jitter=0.1), edge
+
+
+def replicate(system: AmoebaSystem, edge, reps=(2, 2, 2)) -> AmoebaSystem:
+    """The replicate supercell of an orthorhombic box: copies of every atom at lattice
+    translations t = (i a, j b, k c), 0 <= i < reps[0] ..., with connectivity and frame
+    indices offset per copy (the expansion C/ReplicatesCrystal.java:172-202 describes).
+    Copy m = (k * reps[1] + j) * reps[0] + i holds atoms m*n .. m*n + n - 1."""
+    edge = np.broadcast_to(np.asarray(edge, dtype=np.float64), (3,))
+    n = system.n_atoms
+    copies = [(i, j, k) for k in range(reps[2]) for j in range(reps[1]) for i in range(reps[0])]
+    nc = len(copies)
+    xyz = np.concatenate([system.xyz + np.array(c) * edge for c in copies])
+    tile = lambda a: np.concatenate([a] * nc)  # noqa: E731
+    axis = np.concatenate([np.where(system.axis >= 0, system.axis + m * n, -1) for m in range(nc)]).astype(np.int32)
+    red_parent = np.concatenate([system.red_parent + m * n for m in range(nc)]).astype(np.int32)
+    shift_lists = lambda L: [[k + m * n for k in row] for m in range(nc) for row in L]  # noqa: E731
+    mol = None
+    if system.molecule is not None:
+        nm = int(np.max(system.molecule)) + 1
+        mol = np.concatenate([system.molecule + m * nm for m in range(nc)])
+    return AmoebaSystem(xyz=xyz, multipole=tile(system.multipole), frame=tile(system.frame), axis=axis,
+                        polarizability=tile(system.polarizability), thole=tile(system.thole),
+                        pdamp=tile(system.pdamp), vdw_type=tile(system.vdw_type), red_parent=red_parent,
+                        red_factor=tile(system.red_factor), vdw_inv_rmin=system.vdw_inv_rmin,
+                        vdw_eps=system.vdw_eps, n12=shift_lists(system.n12), n13=shift_lists(system.n13),
+                        n14=shift_lists(system.n14), n15=shift_lists(system.n15), ip11=shift_lists(system.ip11),
+                        molecule=mol, name=f"{system.name}x{nc}")
 
 
 def water_params(edge: float, **kw) -> AmoebaParams:

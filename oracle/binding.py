@@ -38,6 +38,11 @@ def lib():
         L.oracle_neighbor_pairs.restype = ctypes.c_int64
         L.oracle_neighbor_pairs.argtypes = [ctypes.POINTER(cabi.FfxgSystem), ctypes.POINTER(cabi.FfxgParams), D,
                                             ctypes.POINTER(ctypes.c_int32)]
+        L.oracle_neighbor_images.restype = ctypes.c_int64
+        L.oracle_neighbor_images.argtypes = [ctypes.POINTER(cabi.FfxgSystem), ctypes.POINTER(cabi.FfxgParams), D,
+                                             ctypes.POINTER(ctypes.c_int32)]
+        L.oracle_set_images.restype = None
+        L.oracle_set_images.argtypes = [ctypes.c_int]
         L.oracle_set_alchemy.restype = None
         L.oracle_set_alchemy.argtypes = [ctypes.POINTER(cabi.FfxgAlchemy), ctypes.c_int, ctypes.c_double]
         L.oracle_get_dEdL.restype = None
@@ -57,10 +62,12 @@ def _dp(a):
 
 
 def energy(system: AmoebaSystem, params: AmoebaParams, xyz=None, gradient=True, nthreads=0, alchemy=None,
-           lam=1.0):
+           lam=1.0, all_images=False):
     """Returns dict(terms, grad, counts, induced, induced_cr, global_mpole, status), and with
-    an Alchemy also dEdL, d2EdL2 and dEdXdL (the vdW softcore at lambda `lam`)."""
+    an Alchemy also dEdL, d2EdL2 and dEdXdL (the vdW softcore at lambda `lam`).
+    all_images=True forces multi-image lists where the minimum image would suffice."""
     L = lib()
+    L.oracle_set_images(1 if all_images else 0)
     if alchemy is not None:
         a, keep_a = alchemy.c_struct(cabi)
         L.oracle_set_alchemy(ctypes.byref(a), system.n_atoms, float(lam))
@@ -81,6 +88,7 @@ def energy(system: AmoebaSystem, params: AmoebaParams, xyz=None, gradient=True, 
                          _dp(ind), _dp(indcr), _dp(gm))
     out = dict(terms=terms, grad=grad, counts=counts, induced=ind, induced_cr=indcr, global_mpole=gm,
                status=int(st))
+    L.oracle_set_images(0)
     if alchemy is not None:
         d1 = ctypes.c_double()
         d2 = ctypes.c_double()
@@ -100,6 +108,22 @@ def neighbor_pairs(system: AmoebaSystem, params: AmoebaParams, xyz=None) -> np.n
     out = np.zeros((n, 2), dtype=np.int32)
     L.oracle_neighbor_pairs(ctypes.byref(s), ctypes.byref(p), _dp(x),
                             out.ctypes.data_as(ctypes.POINTER(ctypes.c_int32)))
+    return out
+
+
+def neighbor_images(system: AmoebaSystem, params: AmoebaParams, xyz=None, all_images=False) -> np.ndarray:
+    """Rows (i, k, nx, ny, nz): one per image pair of the buffered list (i < k, or i == k
+    with n > 0), n the lattice shift of x_k + n L - x_i (zero outside multi-image mode)."""
+    L = lib()
+    L.oracle_set_images(1 if all_images else 0)
+    s, keep = system.c_struct(cabi)
+    p = params_struct(params, cabi)
+    x = np.ascontiguousarray(system.xyz if xyz is None else xyz, dtype=np.float64)
+    n = L.oracle_neighbor_images(ctypes.byref(s), ctypes.byref(p), _dp(x), None)
+    out = np.zeros((n, 5), dtype=np.int32)
+    L.oracle_neighbor_images(ctypes.byref(s), ctypes.byref(p), _dp(x),
+                             out.ctypes.data_as(ctypes.POINTER(ctypes.c_int32)))
+    L.oracle_set_images(0)
     return out
 
 

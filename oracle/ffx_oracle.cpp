@@ -218,6 +218,17 @@ struct Alchemy {
 };
 Alchemy g_alch;
 
+// Multi-image lists forced on for boxes where the minimum image would also do (a
+// consistency hook for tests; oracle_set_images).
+int g_force_images = 0;
+
+// Packed lattice shift of a multi-image list entry: n = (nx, ny, nz) in 10-bit fields
+// offset by 512, bit 30 set on the minimum-image entry of the pair (the only one the
+// bonded masks touch).
+inline int pack_shift(int nx, int ny, int nz, bool primary) {
+  return (nx + 512) | ((ny + 512) << 10) | ((nz + 512) << 20) | (primary ? (1 << 30) : 0);
+}
+
 struct Oracle {
   // ---- inputs
   int n = 0;
@@ -239,6 +250,29 @@ struct Oracle {
   std::vector<std::vector<int>> nlist;   // half list (i < k) at cutoff + buffer
   std::vector<std::vector<int>> ewald;   // realSpaceLists
   std::vector<std::vector<int>> precond; // preconditionerLists
+  // Multi-image mode: the box is at most twice an interaction cutoff, so a pair may
+  // interact through several lattice images (the reference's ReplicatesCrystal,
+  // C/ReplicatesCrystal.java:172-202, whose replicate supercell sums the same images).
+  // Each list entry then carries a packed shift (pack_shift) in the parallel lists below.
+  bool multi_image = false;
+  std::vector<std::vector<int>> nsh, esh, psh;
+
+  // Displacement of list entry e of atom i, given x_k - x_i on entry: the minimum image
+  // (Crystal.image) or, in multi-image mode, x_k + n L - x_i.  sign = -1 for the vdW
+  // convention x_i - x_k.  Returns r^2 in Crystal.image's operation order.
+  double disp(double &dx, double &dy, double &dz, const std::vector<std::vector<int>> &sh, int i, size_t e,
+              double sign = 1.0) const {
+    if (!multi_image) return image(dx, dy, dz, cell);
+    const int c = sh[i][e];
+    dx += sign * ((double)((c & 1023) - 512) * cell.a);
+    dy += sign * ((double)(((c >> 10) & 1023) - 512) * cell.b);
+    dz += sign * ((double)(((c >> 20) & 1023) - 512) * cell.c);
+    return dx * dx + dy * dy + dz * dz;
+  }
+  // Whether entry e of atom i is the pair's minimum image (masks apply only there).
+  bool primary(const std::vector<std::vector<int>> &sh, int i, size_t e) const {
+    return !multi_image || ((sh[i][e] >> 30) & 1);
+  }
   std::vector<double> gm;                // [n][10] global multipoles
   std::vector<double> fm;                // [n][10] fractional multipoles
   int nfx = 0, nfy = 0, nfz = 0, order = 5;
@@ -297,6 +331,10 @@ struct Oracle {
     }
     nfx = p.pme_grid[0]; nfy = p.pme_grid[1]; nfz = p.pme_grid[2];
     order = p.pme_order;
+    const double maxcut = std::max(std::max(p.vdw_cutoff, p.ewald_cutoff), p.precond_cutoff);
+    multi_image = g_force_images != 0;
+    for (int d = 0; d < 3; d++)
+      if (p.box[d] <= 2.0 * maxcut) multi_image = true;
     setup_recip();
   }
 
@@ -319,11 +357,51 @@ struct Oracle {
     }
   }
 
+  // Multi-image list: every image k + n L (k >= i; n > 0 in (z, y, x) lexicographic order
+  // for k == i) within the buffered cutoff.  n runs over n0 + m, n0 the minimum-image
+  // shift of the raw difference and |m_d| <= floor(rlist / L_d + 1/2), which covers every
+  // image inside rlist.  Brute force over atom pairs: boxes this small hold few atoms.
+  void build_list_images(const std::vector<double> &rx, const std::vector<double> &ry,
+                         const std::vector<double> &rz, double rlist) {
+    const double rl2 = rlist * rlist;
+    const int R[3] = {(int)std::floor(rlist / cell.a + 0.5), (int)std::floor(rlist / cell.b + 0.5),
+                      (int)std::floor(rlist / cell.c + 0.5)};
+    nlist.assign(n, {});
+    nsh.assign(n, {});
+#pragma omp parallel for schedule(dynamic, 16)
+    for (int i = 0; i < n; i++) {
+      for (int k = i; k < n; k++) {
+        const double dx = rx[k] - rx[i], dy = ry[k] - ry[i], dz = rz[k] - rz[i];
+        const double fx = dx * cell.A00, fy = dy * cell.A11, fz = dz * cell.A22;
+        const int n0x = (int)(std::floor(std::fabs(fx) + 0.5) * jsignum(-fx));
+        const int n0y = (int)(std::floor(std::fabs(fy) + 0.5) * jsignum(-fy));
+        const int n0z = (int)(std::floor(std::fabs(fz) + 0.5) * jsignum(-fz));
+        for (int mz = -R[2]; mz <= R[2]; mz++)
+          for (int my = -R[1]; my <= R[1]; my++)
+            for (int mx = -R[0]; mx <= R[0]; mx++) {
+              const int nx = n0x + mx, ny = n0y + my, nz = n0z + mz;
+              if (k == i && !(nz > 0 || (nz == 0 && (ny > 0 || (ny == 0 && nx > 0))))) continue;
+              const double ex = dx + (double)nx * cell.a, ey = dy + (double)ny * cell.b,
+                           ez = dz + (double)nz * cell.c;
+              const double d2 = ex * ex + ey * ey + ez * ez;
+              if (d2 <= rl2) {
+                nlist[i].push_back(k);
+                nsh[i].push_back(pack_shift(nx, ny, nz, mx == 0 && my == 0 && mz == 0));
+              }
+            }
+      }
+    }
+  }
+
   void build_list() {
     std::vector<double> rx, ry, rz;
     reduced_coords(rx, ry, rz);
     const double rlist = std::max(p.vdw_cutoff, p.ewald_cutoff) + p.list_buffer;
     const double rl2 = rlist * rlist;
+    if (multi_image) {
+      build_list_images(rx, ry, rz, rlist);
+      return;
+    }
     // Cells at least rlist/2 wide; search +-2 cells (nEdge = 2, NeighborList.java:1296-1345).
     const int nca = std::max(1, (int)std::floor(cell.a / (rlist * 0.5)));
     const int ncb = std::max(1, (int)std::floor(cell.b / (rlist * 0.5)));
@@ -410,12 +488,14 @@ struct Oracle {
         const double rv = redv[i], rdv = 1.0 - rv;
         const int ri = redi[i];
         const int ti = vtype[i];
-        for (int k : nlist[i]) {
+        for (size_t e = 0; e < nlist[i].size(); e++) {
+          const int k = nlist[i][e];
           double dx = xi - rx[k], dy = yi - ry[k], dz = zi - rz[k];
-          const double r2 = image(dx, dy, dz, cell);
+          const double r2 = disp(dx, dy, dz, nsh, i, e, -1.0);
           const int tk = vtype[k];
           const double irv = vrad[(size_t)ti * ntypes + tk];
-          if (!(r2 <= off2v && mask[k] > 0.0 && irv > 0.0)) continue;
+          const double mk = primary(nsh, i, e) ? mask[k] : 1.0;
+          if (!(r2 <= off2v && mk > 0.0 && irv > 0.0)) continue;
           const double r = std::sqrt(r2);
           // Softcore pair (VanDerWaals.java:1728-1761): exactly one atom soft, or both
           // soft under the intermolecular / intramolecular softcore options.
@@ -431,7 +511,7 @@ struct Oracle {
           }
           const double alpha = soft ? al.sc1 : 0.0;
           const double lambda5 = soft ? al.sc2 : 1.0;
-          const double ev = mask[k] * veps[(size_t)ti * ntypes + tk];
+          const double ev = mk * veps[(size_t)ti * ntypes + tk];
           const double eps_lambda = ev * lambda5;
           const double rho = r * irv;
           const double rho2 = rho * rho;
@@ -995,6 +1075,8 @@ struct Oracle {
     fieldP.assign(3 * (size_t)n, 0.0);
     ewald.assign(n, {});
     precond.assign(n, {});
+    esh.assign(multi_image ? n : 0, {});
+    psh.assign(multi_image ? n : 0, {});
     std::vector<std::vector<double>> tD(nthreads, std::vector<double>(3 * (size_t)n, 0.0));
     std::vector<std::vector<double>> tP(nthreads, std::vector<double>(3 * (size_t)n, 0.0));
 #pragma omp parallel
@@ -1021,18 +1103,24 @@ struct Oracle {
           for (int g : ip11[i]) if (g == k) { emask[k] = p.intra14 * p.p14; break; }
         }
         for (int g : ip11[i]) imask[g] = p.d11;
-        for (int k : nlist[i]) {
+        for (size_t e = 0; e < nlist[i].size(); e++) {
+          const int k = nlist[i][e];
           double xr = x[k] - xi, yr = y[k] - yi, zr = z[k] - zi;
-          const double r2 = image(xr, yr, zr, cell);
+          const double r2 = disp(xr, yr, zr, nsh, i, e);
           if (!(r2 <= off2)) continue;
           ewald[i].push_back(k);
+          if (multi_image) esh[i].push_back(nsh[i][e]);
+          const bool prim = primary(nsh, i, e);
           const double pdk = ipdamp[k], ptk = thole[k];
           const double *mk = &gm[10 * (size_t)k];
           const double ck = mk[t000], dkx = mk[t100], dky = mk[t010], dkz = mk[t001];
           const double qkxx = mk[t200] / 3.0, qkyy = mk[t020] / 3.0, qkzz = mk[t002] / 3.0;
           const double qkxy = mk[t110] / 3.0, qkxz = mk[t101] / 3.0, qkyz = mk[t011] / 3.0;
           const double r = std::sqrt(r2);
-          if (r < p.precond_cutoff) precond[i].push_back(k);
+          if (r < p.precond_cutoff) {
+            precond[i].push_back(k);
+            if (multi_image) psh[i].push_back(nsh[i][e]);
+          }
           const double ralpha = aewald * r;
           const double exp2a = std::exp(-ralpha * ralpha);
           const double rr1 = 1.0 / r, rr2 = rr1 * rr1;
@@ -1051,7 +1139,7 @@ struct Oracle {
             scale5 = 1.0 - expdamp * (1.0 - damp);
             scale7 = 1.0 - expdamp * (1.0 - damp + 0.6 * damp * damp);
           }
-          const double scale = imask[k], scalep = emask[k];
+          const double scale = prim ? imask[k] : 1.0, scalep = prim ? emask[k] : 1.0;
           const double dsc3 = scale3 * scale, dsc5 = scale5 * scale, dsc7 = scale7 * scale;
           const double psc3 = scale3 * scalep, psc5 = scale5 * scalep, psc7 = scale7 * scalep;
           const double rr3 = rr1 * rr2, rr5 = 3.0 * rr3 * rr2, rr7 = 5.0 * rr5 * rr2;
@@ -1112,7 +1200,8 @@ struct Oracle {
   // Ewald list with the given Ewald coefficient (0 plus the short list gives the
   // preconditioner field, PCGSolver.java:1254-1400).
   void dipole_field(const std::vector<double> &ud, const std::vector<double> &up,
-                    const std::vector<std::vector<int>> &lists, double alpha,
+                    const std::vector<std::vector<int>> &lists, const std::vector<std::vector<int>> &shifts,
+                    double alpha,
                     std::vector<double> &outD, std::vector<double> &outP) {
     outD.assign(3 * (size_t)n, 0.0);
     outP.assign(3 * (size_t)n, 0.0);
@@ -1138,9 +1227,10 @@ struct Oracle {
         const double pdi = ipdamp[i], pti = thole[i];
         const double uix = ud[3 * i], uiy = ud[3 * i + 1], uiz = ud[3 * i + 2];
         const double pix = up[3 * i], piy = up[3 * i + 1], piz = up[3 * i + 2];
-        for (int k : lists[i]) {
+        for (size_t e = 0; e < lists[i].size(); e++) {
+          const int k = lists[i][e];
           double xr = x[k] - xi, yr = y[k] - yi, zr = z[k] - zi;
-          const double r2 = image(xr, yr, zr, cell);
+          const double r2 = disp(xr, yr, zr, shifts, i, e);
           const double r = std::sqrt(r2);
           const double rr1 = 1.0 / r, rr2 = rr1 * rr1;
           const double ralpha = alpha * r;
@@ -1202,7 +1292,7 @@ struct Oracle {
     convolve(grid);
     interpolate(grid, 0, fphiI, cphiI);
     interpolate(grid, 1, fphiP, cphiP);
-    dipole_field(ud, up, ewald, aewald, outD, outP);
+    dipole_field(ud, up, ewald, esh, aewald, outD, outP);
     for (int i = 0; i < n; i++)
       for (int a = 0; a < 3; a++) {
         outD[3 * i + a] += aewald3 * ud[3 * i + a] - cphiI[20 * (size_t)i + 1 + a];
@@ -1233,7 +1323,7 @@ struct Oracle {
           ur[3 * i + a] = polar[i] * r[3 * i + a];
           pr[3 * i + a] = polar[i] * rCR[3 * i + a];
         }
-      dipole_field(ur, pr, precond, 0.0, preD, preP);
+      dipole_field(ur, pr, precond, psh, 0.0, preD, preP);
     };
     precondition();
     for (int i = 0; i < n; i++)
@@ -1472,16 +1562,19 @@ struct Oracle {
         const double uix = uD[3 * i], uiy = uD[3 * i + 1], uiz = uD[3 * i + 2];
         const double pix = uP[3 * i], piy = uP[3 * i + 1], piz = uP[3 * i + 2];
         const double pdi = ipdamp[i], pti = thole[i];
-        for (int k : ewald[i]) {
+        for (size_t e = 0; e < ewald[i].size(); e++) {
+          const int k = ewald[i][e];
           double xr = x[k] - xi, yr = y[k] - yi, zr = z[k] - zi;
-          const double r2 = image(xr, yr, zr, cell);
+          const double r2 = disp(xr, yr, zr, esh, i, e);
+          const bool prim = primary(esh, i, e);
           const double *mk = &gm[10 * (size_t)k];
           const double ck = mk[t000], dkx = mk[t100], dky = mk[t010], dkz = mk[t001];
           const double qkxx = mk[t200] / 3.0, qkyy = mk[t020] / 3.0, qkzz = mk[t002] / 3.0;
           const double qkxy = mk[t110] / 3.0, qkxz = mk[t101] / 3.0, qkyz = mk[t011] / 3.0;
           const double ukx = uD[3 * k], uky = uD[3 * k + 1], ukz = uD[3 * k + 2];
           const double pkx = uP[3 * k], pky = uP[3 * k + 1], pkz = uP[3 * k + 2];
-          const double scale = mmask[k], scalep = pmask[k], scaled = dmask[k];
+          const double scale = prim ? mmask[k] : 1.0, scalep = prim ? pmask[k] : 1.0;
+          const double scaled = prim ? dmask[k] : 1.0;
           const double r = std::sqrt(r2);
           const double ralpha = aewald * r;
           const double exp2a = std::exp(-ralpha * ralpha);
@@ -2041,6 +2134,39 @@ int64_t oracle_neighbor_pairs(const ffxg_system *sys, const ffxg_params *prm, co
     }
   return c;
 }
+
+// Image pairs of the buffered list, one line per pair image: (i, k, nx, ny, nz) with the
+// lattice shift n of x_k + n L - x_i (minimum image: n from Crystal.image's rounding),
+// i < k, or i == k with n > 0.  out may be NULL to count.
+int64_t oracle_neighbor_images(const ffxg_system *sys, const ffxg_params *prm, const double *xyz,
+                               int32_t *out) {
+  Oracle o;
+  o.nthreads = 1;
+#ifdef _OPENMP
+  o.nthreads = omp_get_max_threads();
+#endif
+  o.setup(sys, prm, xyz ? xyz : sys->xyz);
+  o.build_list();
+  int64_t c = 0;
+  for (int i = 0; i < o.n; i++)
+    for (size_t e = 0; e < o.nlist[i].size(); e++) {
+      if (out) {
+        const int k = o.nlist[i][e];
+        int nx = 0, ny = 0, nz = 0;
+        if (o.multi_image) {
+          const int code = o.nsh[i][e];
+          nx = (code & 1023) - 512; ny = ((code >> 10) & 1023) - 512; nz = ((code >> 20) & 1023) - 512;
+        }
+        int32_t *q = out + 5 * c;
+        q[0] = i; q[1] = k; q[2] = nx; q[3] = ny; q[4] = nz;
+      }
+      c++;
+    }
+  return c;
+}
+
+// Force (1) or release (0) multi-image lists for boxes where the minimum image suffices.
+void oracle_set_images(int force_all) { g_force_images = force_all; }
 
 // Soft atoms and softcore keys for the next oracle_energy calls (NULL clears), at lambda.
 void oracle_set_alchemy(const ffxg_alchemy *a, int n, double lambda) {
