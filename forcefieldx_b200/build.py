@@ -6,7 +6,7 @@ import subprocess
 import sys
 
 HERE = os.path.dirname(os.path.abspath(__file__))
-SOURCES = ["handle.cu", "nlist.cu", "pme.cu", "real.cu", "vdw.cu", "recip.cu", "pcg.cu", "md.cu"]
+SOURCES = ["handle.cu", "nlist.cu", "pme.cu", "real.cu", "vdw.cu", "recip.cu", "pcg.cu", "md.cu", "batch.cu"]
 LIB = os.path.join(HERE, "libffxcuda.so")
 NVCC_FLAGS = ["-gencode", "arch=compute_100a,code=sm_100a", "-O3", "-lineinfo", "-std=c++17",
               "-Xcompiler", "-fPIC", "-shared", "-diag-suppress", "177"]

@@ -76,6 +76,17 @@ PROTOTYPES = {
     "ffxg_get_induced_dipoles": (ctypes.c_int, [ctypes.c_void_p, _D, _D]),
     "ffxg_get_global_multipoles": (ctypes.c_int, [ctypes.c_void_p, _D]),
     "ffxg_get_neighbor_pairs": (ctypes.c_int, [ctypes.c_void_p, _I, _L]),
+    "ffxg_get_neighbor_images": (ctypes.c_int, [ctypes.c_void_p, _I, _L]),
+    "ffxg_set_image_mode": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int]),
+    "ffxg_batch_create": (ctypes.c_int, [ctypes.c_int32, ctypes.POINTER(FfxgSystem), ctypes.POINTER(FfxgParams),
+                                         ctypes.POINTER(ctypes.c_void_p)]),
+    "ffxg_batch_energy": (ctypes.c_int, [ctypes.c_void_p, _D, ctypes.c_int, _D, _D, _L, _I]),
+    "ffxg_batch_set_mode": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int]),
+    "ffxg_batch_atoms": (ctypes.c_int64, [ctypes.c_void_p, _L]),
+    "ffxg_batch_system": (ctypes.c_void_p, [ctypes.c_void_p, ctypes.c_int32]),
+    "ffxg_batch_graph_builds": (ctypes.c_int64, [ctypes.c_void_p]),
+    "ffxg_batch_last_error": (ctypes.c_char_p, [ctypes.c_void_p]),
+    "ffxg_batch_destroy": (None, [ctypes.c_void_p]),
     "ffxg_set_alchemy": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(FfxgAlchemy)]),
     "ffxg_set_lambda": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_double]),
     "ffxg_get_dEdL": (ctypes.c_int, [ctypes.c_void_p, _D, _D, _D]),

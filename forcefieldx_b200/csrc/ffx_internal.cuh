@@ -33,6 +33,7 @@ enum : int {
   FLAG_PRECOND_OVERFLOW = 4,
   FLAG_NONFINITE = 8,
   FLAG_REBUILD = 16,
+  FLAG_IMAGE_RANGE = 32,   // a multi-image shift beyond the 10-bit packing (|n| > 511)
 };
 
 // Exclusion codes: bits 0-2 mpole class, 3-5 polar class, 6 same polarization group,
@@ -68,6 +69,42 @@ __device__ __forceinline__ double image_exact(double &x, double &y, double &z, c
   y = __dmul_rn(yf, bx.Ai11);
   z = __dmul_rn(zf, bx.Ai22);
   return __dadd_rn(__dadd_rn(__dmul_rn(x, x), __dmul_rn(y, y)), __dmul_rn(z, z));
+}
+
+// Multi-image lists (boxes at most twice an interaction cutoff; the reference's
+// ReplicatesCrystal case, C/ReplicatesCrystal.java:172-202): each list entry carries the
+// lattice shift n of its image x_k + n L in a parallel int array, packed as three 10-bit
+// fields offset by 512 with bit 30 set on the pair's minimum-image entry (the only one the
+// bonded masks touch).  sh == nullptr selects the minimum image.
+__device__ __host__ __forceinline__ int pack_shift(int nx, int ny, int nz, bool primary) {
+  return (nx + 512) | ((ny + 512) << 10) | ((nz + 512) << 20) | (primary ? (1 << 30) : 0);
+}
+
+// r = (x_k - x_i) + sign * n L for entry e (sign = -1 for the vdW convention x_i - x_k),
+// else Crystal.image; r^2 in Crystal.image's operation order, without contraction.
+__device__ __forceinline__ double pair_image(double &x, double &y, double &z, const Box &bx,
+                                             const int *__restrict__ sh, size_t e, double sign) {
+  if (sh == nullptr) return image_exact(x, y, z, bx);
+  const int c = sh[e];
+  x = __dadd_rn(x, sign * __dmul_rn((double)((c & 1023) - 512), bx.Ai00));
+  y = __dadd_rn(y, sign * __dmul_rn((double)(((c >> 10) & 1023) - 512), bx.Ai11));
+  z = __dadd_rn(z, sign * __dmul_rn((double)(((c >> 20) & 1023) - 512), bx.Ai22));
+  return __dadd_rn(__dadd_rn(__dmul_rn(x, x), __dmul_rn(y, y)), __dmul_rn(z, z));
+}
+
+// Whether entry e is its pair's minimum image (always, outside multi-image mode).
+__device__ __forceinline__ bool pair_primary(const int *__restrict__ sh, size_t e) {
+  return sh == nullptr || ((sh[e] >> 30) & 1);
+}
+
+// Whether entry e (atom i, partner k) is the one that counts an image pair once: k > i, or
+// k == i with n > 0 in (z, y, x) lexicographic order.
+__device__ __forceinline__ bool pair_counted(int i, int k, const int *__restrict__ sh, size_t e) {
+  if (k != i) return k > i;
+  if (sh == nullptr) return false;
+  const int c = sh[e];
+  const int nx = (c & 1023) - 512, ny = ((c >> 10) & 1023) - 512, nz = ((c >> 20) & 1023) - 512;
+  return nz > 0 || (nz == 0 && (ny > 0 || (ny == 0 && nx > 0)));
 }
 
 // Arithmetic of the two precision forms.  Pair kernels are templates on the pair-math
@@ -226,6 +263,13 @@ struct Handle {
   int *d_nbr = nullptr, *d_nbr_cnt = nullptr;
   int *d_ewl = nullptr, *d_ewl_cnt = nullptr;
   int *d_prl = nullptr, *d_prl_cnt = nullptr;
+  // Multi-image lists: on when an edge is at most twice an interaction cutoff (or forced
+  // with ffxg_set_image_mode); then every buffered and Ewald entry has a packed shift.
+  int64_t graph_gen = 0;                             // bumped whenever captured graphs go stale
+  bool images = false;
+  int image_mode = 0;                                // FFXG_IMAGES_AUTO / FFXG_IMAGES_ALL
+  int img_range[3] = {0, 0, 0};                      // |n - n0| bound per axis of the builder
+  int *d_nbr_sh = nullptr, *d_ewl_sh = nullptr;
   // Cached dipole-field pairs of the Ewald and preconditioner rows (PairRec + B), sized
   // for the FP64 records; the mixed form uses the leading half.
   PairRec<double> *d_coefE = nullptr, *d_coefP = nullptr;
@@ -338,6 +382,11 @@ void launch_phi_permanent(Handle &h);
 void launch_phi_induced(Handle &h);
 void launch_realspace_field(Handle &h);
 int run_pcg(Handle &h, bool capture);
+// Evaluation entry points shared by the single-system ABI and batches (handle.cu).
+int evaluate(Handle &h, const double *d_xyz, double *d_grad_xyz, bool grad, double *terms, int64_t *counts);
+int eval_capture_body(Handle &h, const double *d_xyz, double *d_grad);
+int eval_after_graph(Handle &h, double *terms, int64_t *counts);
+Handle &handle_of(ffxg_handle *hh);
 int pcg_partial_rows(int n);
 int md_setup(Handle &h, const ffxg_md *md);
 int md_run(Handle &h, double dt, int steps, double *xyz, double *vel, double *epot, double *ekin,

@@ -50,6 +50,7 @@ __global__ void k_set_flags(int *flags, int v) { *flags = v; }
 static void drop_graphs(Handle &h) {
   for (cudaGraphExec_t &g : h.graph_exec)
     if (g) { cudaGraphExecDestroy(g); g = nullptr; }
+  h.graph_gen++;   // batches holding this handle's evaluation recapture
 }
 
 static int alloc_lists(Handle &h) {
@@ -61,6 +62,9 @@ static int alloc_lists(Handle &h) {
   if (h.d_coefP) cudaFree(h.d_coefP);
   if (h.d_coefEB) cudaFree(h.d_coefEB);
   if (h.d_coefPB) cudaFree(h.d_coefPB);
+  if (h.d_nbr_sh) cudaFree(h.d_nbr_sh);
+  if (h.d_ewl_sh) cudaFree(h.d_ewl_sh);
+  h.d_nbr_sh = h.d_ewl_sh = nullptr;
   h.d_nbr = h.d_ewl = h.d_prl = nullptr;
   h.d_coefE = h.d_coefP = nullptr;
   h.d_coefEB = h.d_coefPB = nullptr;
@@ -71,11 +75,28 @@ static int alloc_lists(Handle &h) {
   CK(dalloc(&h.d_coefP, (size_t)h.n * h.cap_prl));
   CK(dalloc(&h.d_coefEB, (size_t)h.n * h.cap_ewl));
   CK(dalloc(&h.d_coefPB, (size_t)h.n * h.cap_prl));
+  if (h.images) {
+    CK(dalloc(&h.d_nbr_sh, (size_t)h.n * h.cap_nbr));
+    CK(dalloc(&h.d_ewl_sh, (size_t)h.n * h.cap_ewl));
+  }
   h.list_valid = false;
   return FFXG_OK;
 }
 
 static int round32(double v) { return ((int)std::ceil(v) + 31) / 32 * 32; }
+
+// Multi-image mode and the shift range of its list builder: |n_d - n0_d| <=
+// floor(rlist / L_d + 1/2), n0 the minimum-image shift, covers every image within rlist.
+static void configure_images(Handle &h) {
+  const ffxg_params *p = &h.prm;
+  const double rcut = std::max(std::max(p->vdw_cutoff, p->ewald_cutoff), p->precond_cutoff);
+  const double rlist = std::max(p->vdw_cutoff, p->ewald_cutoff) + p->list_buffer;
+  h.images = h.image_mode == FFXG_IMAGES_ALL;
+  for (int d = 0; d < 3; d++) {
+    if (p->box[d] <= 2.0 * rcut) h.images = true;
+    h.img_range[d] = (int)std::floor(rlist / p->box[d] + 0.5);
+  }
+}
 
 static int create_impl(const ffxg_system *s, const ffxg_params *p, Handle &h) {
   const int n = s->n_atoms;
@@ -94,14 +115,11 @@ static int create_impl(const ffxg_system *s, const ffxg_params *p, Handle &h) {
   // replicate cells when an edge is shorter than twice the buffered list cutoff.  While
   // every interaction cutoff stays below half of each edge, each pair has exactly one
   // image within any cutoff, so the minimum image on the unit cell (with the buffered
-  // list, whose extra images lie beyond every cutoff) gives the same energy; that case is
-  // handled here.  A cutoff of half an edge or more needs true multi-image lists.
-  const double rcut = std::max(std::max(p->vdw_cutoff, p->ewald_cutoff), p->precond_cutoff);
-  for (int d = 0; d < 3; d++)
-    if (p->box[d] <= 2.0 * rcut) {
-      h.err = "box edge not longer than twice an interaction cutoff: multi-image replicate lists are not supported";
-      return FFXG_ERR_BAD_ARG;
-    }
+  // list, whose extra images lie beyond every cutoff) gives the same energy.  A cutoff of
+  // half an edge or more takes multi-image lists: every lattice image inside the cutoffs,
+  // the sum the replicate supercell forms.
+  h.image_mode = FFXG_IMAGES_AUTO;
+  configure_images(h);
   const double rlist = std::max(p->vdw_cutoff, p->ewald_cutoff) + p->list_buffer;
   if (p->ewald_alpha <= 0.0) { h.err = "ewald-alpha must be positive"; return FFXG_ERR_BAD_ARG; }
   if (p->precision != FFXG_PRECISION_FP64 && p->precision != FFXG_PRECISION_MIXED) {
@@ -338,7 +356,7 @@ static void free_all(Handle &h) {
                   h.d_uP, h.d_udirD, h.d_udirP, h.d_r, h.d_rP, h.d_zpre, h.d_zpreP, h.d_p, h.d_pP, h.d_vec, h.d_vecP,
                   h.d_partials, h.d_scalars, h.d_grid, h.d_influence, h.d_twiddle, h.d_gridf, h.d_influencef, h.d_twiddlef, h.d_grad, h.d_torque, h.d_gred,
                   h.d_eatom, h.d_catom, h.d_result, h.d_cresult, h.d_flags, h.d_xyz_in, h.d_grad_out,
-                  h.d_coefE, h.d_coefP, h.d_coefEB, h.d_coefPB, h.d_part2, h.d_counter, h.d_pos, h.d_recF, h.d_recP, h.d_tpair, h.d_tp, h.d_soft, h.d_mol, h.d_lgred, h.d_mass, h.d_mdx, h.d_mdv, h.d_mda, h.d_mdxp, h.d_mdg, h.d_mdke, h.d_settle, h.d_aspc, h.d_aspc_state};
+                  h.d_coefE, h.d_coefP, h.d_coefEB, h.d_coefPB, h.d_part2, h.d_counter, h.d_pos, h.d_recF, h.d_recP, h.d_tpair, h.d_tp, h.d_soft, h.d_mol, h.d_lgred, h.d_mass, h.d_mdx, h.d_mdv, h.d_mda, h.d_mdxp, h.d_mdg, h.d_mdke, h.d_settle, h.d_aspc, h.d_aspc_state, h.d_nbr_sh, h.d_ewl_sh};
   for (void *q : ptrs)
     if (q) cudaFree(q);
   if (h.h_scalars) cudaFreeHost(h.h_scalars);
@@ -483,6 +501,7 @@ static int evaluate_direct(Handle &h, const double *d_xyz, double *d_grad_xyz, d
     }
     const int f = h.h_flags[0];
     if (f & FLAG_NONFINITE) { h.err = "non-finite coordinates"; return FFXG_ERR_NONFINITE; }
+    if (f & FLAG_IMAGE_RANGE) { h.err = "atoms more than 500 box edges apart"; return FFXG_ERR_BAD_ARG; }
     if (f & kOverflow) {
       if (int a = grow_lists(h, f)) return a;
       continue;
@@ -511,12 +530,15 @@ static int evaluate_direct(Handle &h, const double *d_xyz, double *d_grad_xyz, d
   return FFXG_ERR_CAPACITY;
 }
 
-// Capture the whole evaluation (internal coordinate and gradient buffers) as one graph.
-static int capture_graph(Handle &h) {
+namespace ffx {
+
+// The whole evaluation issued onto h.stream, which is capturing (alone, or as one branch
+// of a batch capture): inputs from d_xyz, gradient into d_grad, and the pinned copies of
+// scalars, flags and solver state that eval_after_graph reads.
+int eval_capture_body(Handle &h, const double *d_xyz, double *d_grad) {
   const int key = h.want_grad ? 1 : 0;
   const int64_t before = h.launches;
-  if (cudaStreamBeginCapture(h.stream, cudaStreamCaptureModeThreadLocal) != cudaSuccess) return FFXG_ERR_CUDA;
-  emit_front(h, h.d_xyz_in);
+  emit_front(h, d_xyz);
   int st = FFXG_OK;
   if (h.prm.polarization != FFXG_POLAR_NONE) {
     if (h.prm.polarization == FFXG_POLAR_MUTUAL) st = run_pcg(h, true);
@@ -524,8 +546,19 @@ static int capture_graph(Handle &h) {
   } else {
     emit_no_polarization(h);
   }
-  emit_back(h, h.d_grad_out);
+  emit_back(h, d_grad);
   cudaMemcpyAsync(h.h_pcg, h.d_pcg, sizeof(PcgState), cudaMemcpyDeviceToHost, h.stream);
+  h.graph_launches[key] = h.launches - before - h.graph_body_launches;
+  return st;
+}
+
+}  // namespace ffx
+
+// Capture the whole evaluation (internal coordinate and gradient buffers) as one graph.
+static int capture_graph(Handle &h) {
+  const int key = h.want_grad ? 1 : 0;
+  if (cudaStreamBeginCapture(h.stream, cudaStreamCaptureModeThreadLocal) != cudaSuccess) return FFXG_ERR_CUDA;
+  const int st = eval_capture_body(h, h.d_xyz_in, h.d_grad_out);
   cudaGraph_t graph = nullptr;
   const cudaError_t ec = cudaStreamEndCapture(h.stream, &graph);
   if (st != FFXG_OK || ec != cudaSuccess) {
@@ -540,7 +573,6 @@ static int capture_graph(Handle &h) {
     cudaGetLastError();
     return FFXG_ERR_CUDA;
   }
-  h.graph_launches[key] = h.launches - before - h.graph_body_launches;
   return FFXG_OK;
 }
 
@@ -564,11 +596,22 @@ static int evaluate_graph(Handle &h, const double *d_xyz, double *d_grad_xyz, do
     h.err = std::string("CUDA error: ") + cudaGetErrorString(cudaGetLastError());
     return FFXG_ERR_CUDA;
   }
+  return eval_after_graph(h, terms, counts);
+}
+
+namespace ffx {
+
+// Results of a finished graph replay (the handle's own or a batch's) from the pinned copies.
+// Returns -1 when a list overflowed: capacities grew, the handle's graphs are gone, and the
+// evaluation must be repeated directly.
+int eval_after_graph(Handle &h, double *terms, int64_t *counts) {
+  const int key = h.want_grad ? 1 : 0;
   const int f = h.h_flags[0];
   if (f & kOverflow) {
     if (int a = grow_lists(h, f)) return a;   // also drops the graphs
     return -1;
   }
+  if (f & FLAG_IMAGE_RANGE) { h.err = "atoms more than 500 box edges apart"; return FFXG_ERR_BAD_ARG; }
   if (f & FLAG_NONFINITE) {
     // k_reduce_coordinates raises the flag for non-finite input coordinates.
     h.err = "non-finite coordinates or energy";
@@ -586,10 +629,13 @@ static int evaluate_graph(Handle &h, const double *d_xyz, double *d_grad_xyz, do
   return finish(h, rebuilt, terms, counts);
 }
 
+}  // namespace ffx
+
 // One evaluation on device-resident coordinates.  The graph path is used once the
 // neighbour list exists (its first build and any regrowth run directly) and when stage
 // timing is off.
-static int evaluate(Handle &h, const double *d_xyz, double *d_grad_xyz, bool grad, double *terms, int64_t *counts) {
+namespace ffx {
+int evaluate(Handle &h, const double *d_xyz, double *d_grad_xyz, bool grad, double *terms, int64_t *counts) {
   h.launches = 0;
   h.want_grad = grad;
   if (h.use_graphs && h.list_valid && !h.timing) {
@@ -599,6 +645,9 @@ static int evaluate(Handle &h, const double *d_xyz, double *d_grad_xyz, bool gra
   }
   return evaluate_direct(h, d_xyz, d_grad_xyz, terms, counts);
 }
+
+Handle &handle_of(ffxg_handle *hh) { return hh->h; }
+}  // namespace ffx
 
 extern "C" {
 
@@ -685,25 +734,58 @@ int ffxg_get_global_multipoles(ffxg_handle *hh, double *mpole) {
   return FFXG_OK;
 }
 
-int ffxg_get_neighbor_pairs(ffxg_handle *hh, int32_t *pairs, int64_t *n_pairs) {
-  if (!hh || !n_pairs) return FFXG_ERR_BAD_ARG;
-  Handle &h = hh->h;
+// Image pairs of the buffered list, each once: rows (i, k, nx, ny, nz) with k > i, or
+// k == i and n > 0 in (z, y, x) lexicographic order; n = 0 outside multi-image mode.
+static int list_images(Handle &h, int32_t *rows, int stride, int64_t *n_rows) {
   if (!h.list_valid) { h.err = "no neighbour list yet: call ffxg_energy first"; return FFXG_ERR_BAD_ARG; }
   const size_t N = h.n;
-  std::vector<int> cnt(N), lst(N * h.cap_nbr);
+  std::vector<int> cnt(N), lst(N * h.cap_nbr), sh;
   CK(cudaMemcpy(cnt.data(), h.d_nbr_cnt, N * sizeof(int), cudaMemcpyDeviceToHost));
   CK(cudaMemcpy(lst.data(), h.d_nbr, N * h.cap_nbr * sizeof(int), cudaMemcpyDeviceToHost));
+  if (h.images) {
+    sh.resize(N * h.cap_nbr);
+    CK(cudaMemcpy(sh.data(), h.d_nbr_sh, N * h.cap_nbr * sizeof(int), cudaMemcpyDeviceToHost));
+  }
   int64_t c = 0;
   for (size_t i = 0; i < N; i++)
     for (int a = 0; a < std::min(cnt[i], h.cap_nbr); a++) {
-      const int k = lst[i * h.cap_nbr + a];
-      if (k > (int)i) {
-        if (pairs) { pairs[2 * c] = (int32_t)i; pairs[2 * c + 1] = k; }
+      const size_t e = i * h.cap_nbr + a;
+      const int k = lst[e];
+      int n3[3] = {0, 0, 0};
+      if (h.images) {
+        n3[0] = (sh[e] & 1023) - 512; n3[1] = ((sh[e] >> 10) & 1023) - 512; n3[2] = ((sh[e] >> 20) & 1023) - 512;
+      }
+      const bool pos = n3[2] > 0 || (n3[2] == 0 && (n3[1] > 0 || (n3[1] == 0 && n3[0] > 0)));
+      if (k > (int)i || (k == (int)i && pos)) {
+        if (rows) {
+          int32_t *q = rows + stride * c;
+          q[0] = (int32_t)i; q[1] = k;
+          if (stride == 5) { q[2] = n3[0]; q[3] = n3[1]; q[4] = n3[2]; }
+        }
         c++;
       }
     }
-  *n_pairs = c;
+  *n_rows = c;
   return FFXG_OK;
+}
+
+int ffxg_get_neighbor_pairs(ffxg_handle *hh, int32_t *pairs, int64_t *n_pairs) {
+  if (!hh || !n_pairs) return FFXG_ERR_BAD_ARG;
+  return list_images(hh->h, pairs, 2, n_pairs);
+}
+
+int ffxg_get_neighbor_images(ffxg_handle *hh, int32_t *rows, int64_t *n_rows) {
+  if (!hh || !n_rows) return FFXG_ERR_BAD_ARG;
+  return list_images(hh->h, rows, 5, n_rows);
+}
+
+int ffxg_set_image_mode(ffxg_handle *hh, int mode) {
+  if (!hh) return FFXG_ERR_BAD_ARG;
+  Handle &h = hh->h;
+  if (mode != FFXG_IMAGES_AUTO && mode != FFXG_IMAGES_ALL) { h.err = "unknown image mode"; return FFXG_ERR_BAD_ARG; }
+  h.image_mode = mode;
+  configure_images(h);
+  return alloc_lists(h);
 }
 
 // VanDerWaals.setLambda (VanDerWaals.java:599-628): softcore constants at lambda.

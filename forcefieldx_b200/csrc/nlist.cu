@@ -197,6 +197,70 @@ __global__ void k_verlet(int n, const double *__restrict__ rx, const double *__r
   }
 }
 
+// Multi-image list: one warp per atom i, lanes over every atom k, and every shift
+// n = n0 + m (n0 the minimum-image shift of the reduced-coordinate difference, |m_d| <=
+// R_d) with |x_k + n L - x_i|^2 <= rl2, except k == i at n = 0.  Entries keep k and the
+// packed shift; the order (k chunk, then m) is fixed, so lists are reproducible.
+__global__ void k_verlet_images(int n, const double *__restrict__ rx, const double *__restrict__ ry,
+                                const double *__restrict__ rz, Box bx, int R0, int R1, int R2, double rl2,
+                                int cap, int *nbr, int *nbr_sh, int *nbr_cnt, int *flags) {
+  if (!(*flags & FLAG_REBUILD)) return;
+  const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const int lane = threadIdx.x & 31;
+  if (warp >= n) return;
+  const int i = warp;
+  const double xi = rx[i], yi = ry[i], zi = rz[i];
+  int count = 0;
+  int *row = nbr + (size_t)i * cap;
+  int *rsh = nbr_sh + (size_t)i * cap;
+  for (int base = 0; base < n; base += 32) {
+    const int k = base + lane;
+    const bool valid = k < n;
+    double dx = 0.0, dy = 0.0, dz = 0.0;
+    int n0x = 0, n0y = 0, n0z = 0;
+    bool ok = valid;
+    if (valid) {
+      dx = __dsub_rn(rx[k], xi); dy = __dsub_rn(ry[k], yi); dz = __dsub_rn(rz[k], zi);
+      const double fx = __dmul_rn(dx, bx.A00), fy = __dmul_rn(dy, bx.A11), fz = __dmul_rn(dz, bx.A22);
+      const double gx = floor(__dadd_rn(fabs(fx), 0.5)) * jsignum(-fx);
+      const double gy = floor(__dadd_rn(fabs(fy), 0.5)) * jsignum(-fy);
+      const double gz = floor(__dadd_rn(fabs(fz), 0.5)) * jsignum(-fz);
+      if (fabs(gx) + R0 > 511.0 || fabs(gy) + R1 > 511.0 || fabs(gz) + R2 > 511.0) {
+        atomicOr(flags, FLAG_IMAGE_RANGE);
+        ok = false;
+      } else {
+        n0x = (int)gx; n0y = (int)gy; n0z = (int)gz;
+      }
+    }
+    for (int mz = -R2; mz <= R2; mz++)
+      for (int my = -R1; my <= R1; my++)
+        for (int mx = -R0; mx <= R0; mx++) {
+          const int nx = n0x + mx, ny = n0y + my, nz = n0z + mz;
+          bool pass = false;
+          if (ok && !(k == i && nx == 0 && ny == 0 && nz == 0)) {
+            const double ex = __dadd_rn(dx, __dmul_rn((double)nx, bx.Ai00));
+            const double ey = __dadd_rn(dy, __dmul_rn((double)ny, bx.Ai11));
+            const double ez = __dadd_rn(dz, __dmul_rn((double)nz, bx.Ai22));
+            const double d2 = __dadd_rn(__dadd_rn(__dmul_rn(ex, ex), __dmul_rn(ey, ey)), __dmul_rn(ez, ez));
+            pass = d2 <= rl2;
+          }
+          const unsigned m = __ballot_sync(0xffffffffu, pass);
+          if (pass) {
+            const int pos = count + __popc(m & ((1u << lane) - 1u));
+            if (pos < cap) {
+              row[pos] = k;
+              rsh[pos] = pack_shift(nx, ny, nz, mx == 0 && my == 0 && mz == 0);
+            }
+          }
+          count += __popc(m);
+        }
+  }
+  if (lane == 0) {
+    nbr_cnt[i] = count;
+    if (count > cap) atomicOr(flags, FLAG_NBR_OVERFLOW);
+  }
+}
+
 __global__ void k_list_done(int n, double *refx, double *refy, double *refz, const double *__restrict__ rx,
                             const double *__restrict__ ry, const double *__restrict__ rz, const int *flags) {
   if (!(*flags & FLAG_REBUILD)) return;
@@ -239,6 +303,16 @@ void launch_neighbor_list(Handle &h, bool force) {
     cudaMemcpyAsync(h.d_flags, &f, sizeof(int), cudaMemcpyHostToDevice, h.stream);
     cudaStreamSynchronize(h.stream);
   }
+  const double rl = fmax(h.prm.vdw_cutoff, h.prm.ewald_cutoff) + h.prm.list_buffer;
+  if (h.images) {
+    k_verlet_images<<<nblocks((int64_t)n * 32, 256), 256, 0, h.stream>>>(
+        n, h.d_rx, h.d_ry, h.d_rz, h.box, h.img_range[0], h.img_range[1], h.img_range[2], rl * rl, h.cap_nbr,
+        h.d_nbr, h.d_nbr_sh, h.d_nbr_cnt, h.d_flags);
+    k_list_done<<<nblocks(n, 256), 256, 0, h.stream>>>(n, h.d_refx, h.d_refy, h.d_refz, h.d_rx, h.d_ry, h.d_rz,
+                                                        h.d_flags);
+    h.launches += 2;
+    return;
+  }
   const int ncells = h.ncell[0] * h.ncell[1] * h.ncell[2];
   cudaMemsetAsync(h.d_cell_cnt, 0, sizeof(int) * (size_t)ncells * 2, h.stream);  // counts and cursors
   k_cell_count<<<nblocks(n, 256), 256, 0, h.stream>>>(n, h.d_rx, h.d_ry, h.d_rz, h.box, h.ncell[0], h.ncell[1],
@@ -247,7 +321,6 @@ void launch_neighbor_list(Handle &h, bool force) {
   k_cell_fill<<<nblocks(n, 256), 256, 0, h.stream>>>(n, h.d_atom_cell, h.d_cell_start, h.d_cell_atoms,
                                                       h.d_cell_cnt + ncells, h.d_flags);
   k_cell_sort<<<nblocks(ncells, 128), 128, 0, h.stream>>>(ncells, h.d_cell_start, h.d_cell_atoms, h.d_flags);
-  const double rl = fmax(h.prm.vdw_cutoff, h.prm.ewald_cutoff) + h.prm.list_buffer;
   k_verlet<<<nblocks((int64_t)n * 32, 256), 256, 0, h.stream>>>(
       n, h.d_rx, h.d_ry, h.d_rz, h.box, cell_offsets(h.ncell), h.d_atom_cell, h.d_cell_start, h.d_cell_atoms,
       rl * rl, h.cap_nbr, h.d_nbr, h.d_nbr_cnt, h.d_flags);

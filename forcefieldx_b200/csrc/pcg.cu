@@ -31,6 +31,11 @@ constexpr int kFieldThreads = 128;               // 4 warps; each warp takes one
 constexpr int kFieldBlocks = 148 * 8;            // fixed grid (grid-stride over atoms)
 constexpr int kVecThreads = 256;
 constexpr int kVecBlocks = 148 * 2;
+// Grids of the grid-stride kernels: the fixed sizes above for large systems, fewer blocks
+// for small ones (a 96-atom box needs 24 warps-per-atom blocks, not 1,184), so the kernels
+// of many small systems can share the device (batches).
+static int field_blocks(int n) { return std::min(kFieldBlocks, std::max(1, (n + 3) / 4)); }
+static int vec_blocks(int n) { return std::min(kVecBlocks, std::max(1, (n + kVecThreads - 1) / kVecThreads)); }
 // Totals of the PCG scalars in Handle::d_scalars.
 enum { T_PAP = 0, T_PAPP, T_RZ, T_RZP, T_RZN, T_RZNP, T_BETA, T_BETAP };
 // Counters (each returns to 0 after use) in Handle::d_counter.
@@ -511,7 +516,7 @@ static double *part_region(const Handle &h, int k) { return h.d_part2 + (size_t)
 
 template <typename T>
 static void pair_field_launch(Handle &h, cudaStream_t st) {
-  k_pair_field<T><<<kFieldBlocks, kFieldThreads, 0, st>>>(
+  k_pair_field<T><<<field_blocks(h.n), kFieldThreads, 0, st>>>(
       h.n, h.d_ewl, h.d_ewl_cnt, h.cap_ewl, reinterpret_cast<const PairRec<T> *>(h.d_coefE),
       reinterpret_cast<const T *>(h.d_coefEB), reinterpret_cast<const T *>(h.d_recF), h.d_tpair);
   FFX_LAUNCHED(h);
@@ -560,14 +565,14 @@ static void field_of(Handle &h, const double *vD, const double *vP, bool first, 
 
 template <bool INIT, typename T>
 static void precond(Handle &h) {
-  k_pcg_precond<INIT, T><<<kFieldBlocks, kFieldThreads, 0, h.stream>>>(
+  k_pcg_precond<INIT, T><<<field_blocks(h.n), kFieldThreads, 0, h.stream>>>(
       h.n, h.d_prl, h.d_prl_cnt, h.cap_prl, reinterpret_cast<const PairRec<T> *>(h.d_coefP),
       reinterpret_cast<const T *>(h.d_coefPB), reinterpret_cast<const T *>(h.d_recP), h.d_polar, h.d_r, h.d_rP,
       h.prm.precond_scale, h.d_zpre, h.d_zpreP, h.d_p, h.d_pP, reinterpret_cast<T *>(h.d_recF), part_region(h, 1),
       h.d_counter + K_PRECOND, h.d_scalars);
   FFX_LAUNCHED(h);
   if (!INIT) {
-    k_pcg_totals<2, true><<<1, 1024, 0, h.stream>>>(part_region(h, 1), kFieldBlocks, h.d_scalars, T_RZN);
+    k_pcg_totals<2, true><<<1, 1024, 0, h.stream>>>(part_region(h, 1), field_blocks(h.n), h.d_scalars, T_RZN);
     FFX_LAUNCHED(h);
   }
 }
@@ -579,7 +584,7 @@ static void launch_precond(Handle &h) {
 
 template <typename T>
 static void update(Handle &h, cudaGraphConditionalHandle cond, int use_cond) {
-  k_pcg_update<T><<<kVecBlocks, kVecThreads, 0, h.stream>>>(
+  k_pcg_update<T><<<vec_blocks(h.n), kVecThreads, 0, h.stream>>>(
       h.n, h.d_vec, h.d_vecP, h.d_p, h.d_pP, h.d_r, h.d_rP, h.d_uD, h.d_uP, h.d_scalars, part_region(h, 2),
       h.d_counter + K_UPDATE, h.d_pcg, h.prm.max_scf_iter, h.prm.polar_eps, h.d_flags, cond, use_cond, h.d_polar,
       reinterpret_cast<T *>(h.d_recP));

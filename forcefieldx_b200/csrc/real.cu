@@ -55,8 +55,9 @@ template <typename R>
 __global__ void __launch_bounds__(128) k_realspace_field(
     int n, const double *__restrict__ x, const double *__restrict__ y, const double *__restrict__ z, Box bx,
     const double *__restrict__ gm, const double *__restrict__ ipdamp, const double *__restrict__ thole,
-    const int *__restrict__ nbr, const int *__restrict__ nbr_cnt, int cap, double off2, double pcut, int *ewl,
-    int *ewl_cnt, int capE, int *prl, int *prl_cnt, int capP, PairRec<R> *coefE, R *coefEB,
+    const int *__restrict__ nbr, const int *__restrict__ nbr_cnt, int cap, const int *__restrict__ nbr_sh,
+    double off2, double pcut, int *ewl, int *ewl_cnt, int capE, int *ewl_sh, int *prl, int *prl_cnt, int capP,
+    PairRec<R> *coefE, R *coefEB,
     PairRec<R> *coefP, R *coefPB, Excl ex, EwaldCoef ec, ScaleTables c_scales, const double *__restrict__ cphi,
     const double *__restrict__ polar, int direct, double *fieldD, double *fieldP, double *uD, double *uP,
     double *udD, double *udP, R *recF, int *flags) {
@@ -79,7 +80,7 @@ __global__ void __launch_bounds__(128) k_realspace_field(
       if (a < cnt) {
         k = row[a];
         double dx = __dsub_rn(x[k], xi), dy = __dsub_rn(y[k], yi), dz = __dsub_rn(z[k], zi);
-        const double r2 = image_exact(dx, dy, dz, bx);
+        const double r2 = pair_image(dx, dy, dz, bx, nbr_sh, (size_t)i * cap + a, 1.0);
         ew = r2 <= off2;
         pr = ew && (sqrt(r2) < pcut);
       }
@@ -87,7 +88,10 @@ __global__ void __launch_bounds__(128) k_realspace_field(
       const unsigned mp = __ballot_sync(0xffffffffu, pr);
       if (ew) {
         const int pos = ce + __popc(me & lt);
-        if (pos < capE) ewl[(size_t)i * capE + pos] = k;
+        if (pos < capE) {
+          ewl[(size_t)i * capE + pos] = k;
+          if (nbr_sh) ewl_sh[(size_t)i * capE + pos] = nbr_sh[(size_t)i * cap + a];
+        }
       }
       if (pr) {
         const int pos = cp + __popc(mp & lt);
@@ -118,8 +122,9 @@ __global__ void __launch_bounds__(128) k_realspace_field(
     R pA = R(0), pB = R(0), px_ = R(0), py_ = R(0), pz_ = R(0);
     if (act) {
       const int k = row[a];
+      const size_t ent = (size_t)i * capE + a;
       double xd = __dsub_rn(x[k], xi), yd = __dsub_rn(y[k], yi), zd = __dsub_rn(z[k], zi);
-      const double r2d = image_exact(xd, yd, zd, bx);
+      const double r2d = pair_image(xd, yd, zd, bx, ewl_sh, ent, 1.0);
       const R xr = (R)xd, yr = (R)yd, zr = (R)zd, r2 = (R)r2d;
       const R ck = gm[t000 * n + k], dkx = gm[t100 * n + k], dky = gm[t010 * n + k], dkz = gm[t001 * n + k];
       const R qkxx = gm[t200 * n + k] * (R(1.0) / R(3.0)), qkyy = gm[t020 * n + k] * (R(1.0) / R(3.0));
@@ -144,7 +149,7 @@ __global__ void __launch_bounds__(128) k_realspace_field(
         scale5 = R(1.0) - expdamp * (R(1.0) - damp);
         scale7 = R(1.0) - expdamp * (R(1.0) - damp + R(0.6) * damp * damp);
       }
-      const unsigned code = excl_code(i, k, ex.ptr, ex.k, ex.code, ex.lo, ex.hi);
+      const unsigned code = pair_primary(ewl_sh, ent) ? excl_code(i, k, ex.ptr, ex.k, ex.code, ex.lo, ex.hi) : 0u;
       const R scale = c_scales.d[(code >> 6) & 1u];
       const R scalep = c_scales.p[(code >> 3) & 7u];
       const R dsc3 = scale3 * scale, dsc5 = scale5 * scale, dsc7 = scale7 * scale;
@@ -224,7 +229,7 @@ __global__ void __launch_bounds__(128) k_real_energy(
     int n, const double *__restrict__ x, const double *__restrict__ y, const double *__restrict__ z, Box bx,
     const double *__restrict__ gm, const double *__restrict__ uD, const double *__restrict__ uP,
     const double *__restrict__ ipdamp, const double *__restrict__ thole, const int *__restrict__ ewl,
-    const int *__restrict__ ewl_cnt, int capE, Excl ex, EwaldCoef ec, ScaleTables c_scales, int polarization, int gradient,
+    const int *__restrict__ ewl_cnt, int capE, const int *__restrict__ ewl_sh, Excl ex, EwaldCoef ec, ScaleTables c_scales, int polarization, int gradient,
     double *eatom_perm, double *eatom_pol, long long *catom, double *grad, double *torque) {
   const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const int lane = threadIdx.x & 31;
@@ -248,8 +253,9 @@ __global__ void __launch_bounds__(128) k_real_energy(
   const int *row = ewl + (size_t)i * capE;
   for (int a = lane; a < cnt; a += 32) {
     const int k = row[a];
+    const size_t ent = (size_t)i * capE + a;
     double xd = __dsub_rn(x[k], xi), yd = __dsub_rn(y[k], yi), zd = __dsub_rn(z[k], zi);
-    const double r2d = image_exact(xd, yd, zd, bx);
+    const double r2d = pair_image(xd, yd, zd, bx, ewl_sh, ent, 1.0);
     const R xr = (R)xd, yr = (R)yd, zr = (R)zd, r2 = (R)r2d;
     const R ck = gm[t000 * n + k], dkx = gm[t100 * n + k], dky = gm[t010 * n + k], dkz = gm[t001 * n + k];
     const R qkxx = gm[t200 * n + k] * (R(1.0) / R(3.0)), qkyy = gm[t020 * n + k] * (R(1.0) / R(3.0));
@@ -257,7 +263,7 @@ __global__ void __launch_bounds__(128) k_real_energy(
     const R qkxz = gm[t101 * n + k] * (R(1.0) / R(3.0)), qkyz = gm[t011 * n + k] * (R(1.0) / R(3.0));
     const R ukx = uD[k], uky = uD[n + k], ukz = uD[2 * n + k];
     const R pkx = uP[k], pky = uP[n + k], pkz = uP[2 * n + k];
-    const unsigned code = excl_code(i, k, ex.ptr, ex.k, ex.code, ex.lo, ex.hi);
+    const unsigned code = pair_primary(ewl_sh, ent) ? excl_code(i, k, ex.ptr, ex.k, ex.code, ex.lo, ex.hi) : 0u;
     const R scale = c_scales.m[code & 7u];
     const R scalep = c_scales.p[(code >> 3) & 7u];
     const R scaled = c_scales.d[(code >> 6) & 1u];
@@ -342,7 +348,7 @@ __global__ void __launch_bounds__(128) k_real_energy(
       const R ereal = gl0 * bn0 + (gl1 + gl6) * bn1 + (gl2 + gl7 + gl8) * bn2 + (gl3 + gl5) * bn3 + gl4 * bn4;
       const R efix = scale1 * (gl0 * rr1 + (gl1 + gl6) * rr3 + (gl2 + gl7 + gl8) * rr5 + (gl3 + gl5) * rr7 + gl4 * rr9);
       const R e = ereal - efix;
-      if (e != R(0.0)) { eP += R(0.5) * e; if (k > i) cnt_pairs++; }
+      if (e != R(0.0)) { eP += R(0.5) * e; if (pair_counted(i, k, ewl_sh, ent)) cnt_pairs++; }
       if (gradient) {
         const R gf1 = bn1 * gl0 + bn2 * (gl1 + gl6) + bn3 * (gl2 + gl7 + gl8) + bn4 * (gl3 + gl5) + bn5 * gl4;
         const R gf2 = -ck * bn1 + sc4 * bn2 - sc6 * bn3;
@@ -591,8 +597,9 @@ static void realspace_field(Handle &h) {
   using V2 = typename Vec2<R>::type;
   const double off2 = h.prm.ewald_cutoff * h.prm.ewald_cutoff;
   k_realspace_field<R><<<nblocks((int64_t)h.n * 32, 128), 128, 0, h.stream>>>(
-      h.n, h.d_x, h.d_y, h.d_z, h.box, h.d_gm, h.d_ipdamp, h.d_thole, h.d_nbr, h.d_nbr_cnt, h.cap_nbr, off2,
-      h.prm.precond_cutoff, h.d_ewl, h.d_ewl_cnt, h.cap_ewl, h.d_prl, h.d_prl_cnt, h.cap_prl,
+      h.n, h.d_x, h.d_y, h.d_z, h.box, h.d_gm, h.d_ipdamp, h.d_thole, h.d_nbr, h.d_nbr_cnt, h.cap_nbr,
+      h.d_nbr_sh, off2, h.prm.precond_cutoff, h.d_ewl, h.d_ewl_cnt, h.cap_ewl, h.d_ewl_sh, h.d_prl, h.d_prl_cnt,
+      h.cap_prl,
       reinterpret_cast<PairRec<R> *>(h.d_coefE), reinterpret_cast<R *>(h.d_coefEB),
       reinterpret_cast<PairRec<R> *>(h.d_coefP), reinterpret_cast<R *>(h.d_coefPB), excl(h),
       ewald_coef(h, h.prm.ewald_alpha), h.scales, h.d_cphi, h.d_polar, h.prm.polarization != FFXG_POLAR_NONE ? 1 : 0,
@@ -613,7 +620,7 @@ template <typename R>
 static void real_energy(Handle &h, bool grad) {
   k_real_energy<R><<<nblocks((int64_t)h.n * 32, 128), 128, 0, h.stream>>>(
       h.n, h.d_x, h.d_y, h.d_z, h.box, h.d_gm, h.d_uD, h.d_uP, h.d_ipdamp, h.d_thole, h.d_ewl, h.d_ewl_cnt,
-      h.cap_ewl, excl(h), ewald_coef(h, h.prm.ewald_alpha), h.scales, h.prm.polarization, grad ? 1 : 0,
+      h.cap_ewl, h.d_ewl_sh, excl(h), ewald_coef(h, h.prm.ewald_alpha), h.scales, h.prm.polarization, grad ? 1 : 0,
       h.d_eatom + 1 * (size_t)h.n, h.d_eatom + 2 * (size_t)h.n, h.d_catom + (size_t)h.n, h.d_grad, h.d_torque);
   FFX_LAUNCHED(h);
 }

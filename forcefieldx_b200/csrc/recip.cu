@@ -7,6 +7,8 @@
 //                   frame-atom forces of every atom whose frame it defines.
 //  k_assemble       ForceFieldEnergy.fillGradient (ForceFieldEnergy.java:2848): vdW + PME.
 //  k_sum_*          deterministic two-level sums of the per-atom energies and counts.
+#include <algorithm>
+
 #include "ffx_internal.cuh"
 
 namespace ffx {
@@ -378,8 +380,9 @@ void launch_assemble(Handle &h, double *d_grad_xyz) {
 void launch_reduce_results(Handle &h) {
   double *pe = h.d_partials;
   long long *pc = reinterpret_cast<long long *>(h.d_partials + kSumBlocks * kNE);
-  k_sum_partial<<<kSumBlocks, 256, 0, h.stream>>>(h.n, h.d_eatom, h.d_catom, pe, pc);
-  k_sum_final<<<1, 32, 0, h.stream>>>(kSumBlocks, pe, pc, h.d_result, h.d_cresult);
+  const int nb = std::min(kSumBlocks, std::max(1, (h.n + 255) / 256));   // fewer blocks for small systems
+  k_sum_partial<<<nb, 256, 0, h.stream>>>(h.n, h.d_eatom, h.d_catom, pe, pc);
+  k_sum_final<<<1, 32, 0, h.stream>>>(nb, pe, pc, h.d_result, h.d_cresult);
   h.launches += 2;
 }
 

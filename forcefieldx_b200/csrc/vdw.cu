@@ -34,7 +34,8 @@ __global__ void __launch_bounds__(256) k_vdw(int n, const double *__restrict__ r
                                              const double *__restrict__ rz, Box bx, const int *__restrict__ vtype,
                                              int ntypes, const double *__restrict__ vrad,
                                              const double *__restrict__ veps, const int *__restrict__ nbr,
-                                             const int *__restrict__ nbr_cnt, int cap, const int *__restrict__ eptr,
+                                             const int *__restrict__ nbr_cnt, int cap, const int *__restrict__ nbr_sh,
+                                             const int *__restrict__ eptr,
                                              const int *__restrict__ ek, const unsigned *__restrict__ ecode,
                                              const int *__restrict__ elo, const int *__restrict__ ehi, VdwForm vf,
                                              ScaleTables c_vscales, int gradient, double *eatom, long long *catom, double *gred,
@@ -58,12 +59,13 @@ __global__ void __launch_bounds__(256) k_vdw(int n, const double *__restrict__ r
   const int *row = nbr + (size_t)i * cap;
   for (int a = lane; a < m; a += 32) {
     const int k = row[a];
+    const size_t ent = (size_t)i * cap + a;
     double dxd = __dsub_rn(xi, rx[k]), dyd = __dsub_rn(yi, ry[k]), dzd = __dsub_rn(zi, rz[k]);
-    const double r2d = image_exact(dxd, dyd, dzd, bx);
+    const double r2d = pair_image(dxd, dyd, dzd, bx, nbr_sh, ent, -1.0);
     const int tk = vtype[k];
     const R irv = vrad[ti * ntypes + tk];
     if (!(r2d <= vf.off2) || !(irv > R(0.0))) continue;
-    const unsigned code = vexcl_code(i, k, eptr, ek, ecode, elo, ehi);
+    const unsigned code = pair_primary(nbr_sh, ent) ? vexcl_code(i, k, eptr, ek, ecode, elo, ehi) : 0u;
     const R mask = c_vscales.v[(code >> 7) & 3u];
     if (!(mask > R(0.0))) continue;
     const R dx = (R)dxd, dy = (R)dyd, dz = (R)dzd, r2 = (R)r2d;
@@ -112,7 +114,7 @@ __global__ void __launch_bounds__(256) k_vdw(int n, const double *__restrict__ r
       }
     }
     e += R(0.5) * eik * taper;
-    if (k > i) cnt++;
+    if (pair_counted(i, k, nbr_sh, ent)) cnt++;
     if (gradient || (ALCH && spair)) {
       const R dt1d_dr = R(7.0) * rhoDelta1 * irv;
       const R dt2d_dr = R(7.0) * rhoDisp1 * irv;
@@ -217,7 +219,7 @@ void launch_vdw(Handle &h, bool grad) {
                             : (h.mixed ? k_vdw<float, false> : k_vdw<double, false>);
   kern<<<nblocks((int64_t)h.n * 32, 256), 256, 0, h.stream>>>(
       h.n, h.d_rx, h.d_ry, h.d_rz, h.box, h.d_vtype, h.ntypes, h.d_vrad, h.d_veps, h.d_nbr, h.d_nbr_cnt, h.cap_nbr,
-      h.d_excl_ptr, h.d_excl_k, h.d_excl_code, h.d_excl_lo, h.d_excl_hi, vf, h.scales, grad ? 1 : 0, h.d_eatom, h.d_catom,
+      h.d_nbr_sh, h.d_excl_ptr, h.d_excl_k, h.d_excl_code, h.d_excl_lo, h.d_excl_hi, vf, h.scales, grad ? 1 : 0, h.d_eatom, h.d_catom,
       h.d_gred, h.d_soft, h.d_mol, h.alch, h.d_eatom + 7 * (size_t)h.n, h.d_eatom + 8 * (size_t)h.n, h.d_lgred);
   FFX_LAUNCHED(h);
   if (grad) {

@@ -56,17 +56,21 @@ def _dp(a: np.ndarray):
 class ForceFieldEnergy:
     """AMOEBA vdW + PME energy and gradient on one B200 (one handle, one CUDA stream)."""
 
-    def __init__(self, system: AmoebaSystem, params: AmoebaParams):
+    def __init__(self, system: AmoebaSystem, params: AmoebaParams, _handle=None):
         self.lib = library()
         self.system = system
         self.params = params
         self.n = system.n_atoms
-        s, self._keep = system.c_struct(cabi)
-        p = params_struct(params, cabi)
-        h = ctypes.c_void_p()
-        st = self.lib.ffxg_create(ctypes.byref(s), ctypes.byref(p), ctypes.byref(h))
-        if st != 0:
-            raise EnergyException(st, self.lib.ffxg_last_error(None).decode())
+        self._owned = _handle is None
+        if _handle is None:
+            s, self._keep = system.c_struct(cabi)
+            p = params_struct(params, cabi)
+            h = ctypes.c_void_p()
+            st = self.lib.ffxg_create(ctypes.byref(s), ctypes.byref(p), ctypes.byref(h))
+            if st != 0:
+                raise EnergyException(st, self.lib.ffxg_last_error(None).decode())
+        else:
+            h = ctypes.c_void_p(_handle)      # a batch's system handle, owned by the batch
         self._h = h
         self.terms = np.zeros(cabi.N_TERMS)
         self.counts = np.zeros(cabi.N_COUNTS, dtype=np.int64)
@@ -79,7 +83,8 @@ class ForceFieldEnergy:
 
     def close(self):
         if getattr(self, "_h", None):
-            self.lib.ffxg_destroy(self._h)
+            if self._owned:
+                self.lib.ffxg_destroy(self._h)
             self._h = None
 
     def __del__(self):
@@ -163,6 +168,20 @@ class ForceFieldEnergy:
         self._check(self.lib.ffxg_get_neighbor_pairs(self._h, out.ctypes.data_as(ctypes.POINTER(ctypes.c_int32)),
                                                      ctypes.byref(cnt)))
         return out
+
+    def neighbor_images(self) -> np.ndarray:
+        """Rows (i, k, nx, ny, nz), one per image pair of the buffered list (k > i, or k == i
+        with n > 0); n is the lattice shift of x_k + n L - x_i, zero for minimum-image lists."""
+        cnt = ctypes.c_int64(0)
+        self._check(self.lib.ffxg_get_neighbor_images(self._h, None, ctypes.byref(cnt)))
+        out = np.zeros((cnt.value, 5), dtype=np.int32)
+        self._check(self.lib.ffxg_get_neighbor_images(self._h, out.ctypes.data_as(ctypes.POINTER(ctypes.c_int32)),
+                                                      ctypes.byref(cnt)))
+        return out
+
+    def set_image_mode(self, all_images: bool) -> None:
+        """Force lists of every lattice image (True) or return to the automatic choice."""
+        self._check(self.lib.ffxg_set_image_mode(self._h, 1 if all_images else 0))
 
     @property
     def stream(self) -> int:

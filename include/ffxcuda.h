@@ -186,6 +186,49 @@ int ffxg_get_global_multipoles(ffxg_handle *h, double *mpole);
  * unordered (i, k) with i < k.  With pairs == NULL only *n_pairs is written. */
 int ffxg_get_neighbor_pairs(ffxg_handle *h, int32_t *pairs, int64_t *n_pairs);
 
+/* Image pairs of the buffered list, one row per image: (i, k, nx, ny, nz) with the lattice
+ * shift n of x_k + n L - x_i, for k > i, or k == i and n > 0 in (z, y, x) lexicographic
+ * order; n = 0 outside multi-image mode.  rows may be NULL to count. */
+int ffxg_get_neighbor_images(ffxg_handle *h, int32_t *rows, int64_t *n_rows);
+
+/* Lists of every lattice image inside the cutoffs.  AUTO (the default) uses them when an
+ * edge is at most twice an interaction cutoff (max of vdW, real-space and preconditioner
+ * cutoffs), the boxes the reference expands into a replicate supercell
+ * (ReplicatesCrystal.replicatesCrystalFactory, C/ReplicatesCrystal.java:172-202: the same
+ * sum); the minimum image otherwise.  ALL forces them.  The list builder of this mode is
+ * a brute-force O(N^2) pass, meant for the small boxes that need it. */
+enum { FFXG_IMAGES_AUTO = 0, FFXG_IMAGES_ALL = 1 };
+int ffxg_set_image_mode(ffxg_handle *h, int mode);
+
+/* ---- Batches of independent systems --------------------------------------------------
+ * Many small periodic systems of uneven size (conformer, rotamer or lambda-window
+ * energies) evaluated together.  The reference evaluates such sets one ForceFieldEnergy
+ * at a time (ForceFieldEnergy.energyAndGradient, P/ForceFieldEnergy.java:1843-1890, in a
+ * caller's loop); here each system keeps its own handle and one batch evaluation replays
+ * every system's captured evaluation as a branch of one CUDA graph (GRAPH mode, one
+ * launch), or loops over single-system launches (LOOP mode, for comparison).  Results are
+ * those of the single-system path bit for bit.
+ *   systems[n_systems], params[n_systems]: as for ffxg_create, one per system.
+ *   xyz, grad: all systems' coordinates / gradients concatenated in system order
+ *     ([total atoms][3]; xyz may be NULL to reuse the last coordinates).
+ *   terms[n_systems][FFXG_N_TERMS]; counts[n_systems][FFXG_N_COUNTS] and
+ *   status[n_systems] may be NULL.  Returns the first nonzero status, if any. */
+typedef struct ffxg_batch ffxg_batch;
+enum { FFXG_BATCH_GRAPH = 0, FFXG_BATCH_LOOP = 1 };
+int ffxg_batch_create(int32_t n_systems, const ffxg_system *systems, const ffxg_params *params, ffxg_batch **out);
+int ffxg_batch_energy(ffxg_batch *b, const double *xyz, int want_grad, double *terms, double *grad, int64_t *counts,
+                      int32_t *status);
+int ffxg_batch_set_mode(ffxg_batch *b, int mode);
+/* Total atoms; offsets[n_systems + 1] (may be NULL) receives each system's first atom. */
+int64_t ffxg_batch_atoms(const ffxg_batch *b, int64_t *offsets);
+/* The handle of system i (induced dipoles, lambda, image mode ...); owned by the batch. */
+ffxg_handle *ffxg_batch_system(ffxg_batch *b, int32_t i);
+/* How many times the batch graph was captured (a new capture follows list growth or a
+ * change of a system's lambda or modes). */
+int64_t ffxg_batch_graph_builds(const ffxg_batch *b);
+const char *ffxg_batch_last_error(const ffxg_batch *b);
+void ffxg_batch_destroy(ffxg_batch *b);
+
 /* Alchemical state of the van der Waals term: which atoms carry lambda (Atom.applyLambda)
  * and the softcore keys read by VanDerWaals (VanDerWaals.java:336-357).  soft[n] is
  * 0/1; molecule[n] (may be NULL: every atom its own molecule) decides the both-soft

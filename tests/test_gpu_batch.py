@@ -1,0 +1,90 @@
+"""Batches (ffxg_batch_*) on the device.
+
+1. Every system of a batch (multi-image and minimum-image boxes, 96-1,200 atoms, odd and
+   even PME grids) gives the energy terms and gradient of its own single-system handle,
+   in GRAPH mode (one launch) and in LOOP mode, on first and repeated calls and after the
+   coordinates move: bit for bit in the mixed form, to rounding (1e-11) in the plain FP64
+   form, whose mesh atomics add in arrival order.
+2. The plain FP64 batch against the oracle at the parity bar (1e-8 relative per term,
+   1e-6 gradient RMS).
+3. A lambda change on one system's handle makes the batch recapture its graph.
+"""
+import numpy as np
+import pytest
+
+from forcefieldx_b200.batch import BatchEnergy, batch_workload
+from forcefieldx_b200.energy import ForceFieldEnergy
+from forcefieldx_b200.system import PRECISION_FP64, PRECISION_MIXED, Alchemy
+from oracle import binding as ob
+
+pytestmark = pytest.mark.gpu
+
+
+def _single(s, p, xs):
+    """Results of one handle over the coordinate history xs (lists built at xs[0], as in
+    the batch: the moves stay inside the list buffer, so summation orders agree)."""
+    out = []
+    with ForceFieldEnergy(s, p) as f:
+        for x in xs:
+            e, g = f.energy_and_gradient(x)
+            out.append((f.terms.copy(), g.copy()))
+    return out
+
+
+@pytest.mark.parametrize("precision", [PRECISION_MIXED, PRECISION_FP64])
+def test_batch_matches_single_system_handles(precision):
+    w = batch_workload(n_systems=10, seed=31, n_min=96, n_max=1200, precision=precision)
+    systems, params = [s for s, _ in w], [p for _, p in w]
+    rng = np.random.default_rng(4)
+    moved = [s.xyz + rng.normal(scale=0.05, size=s.xyz.shape) for s in systems]
+    hist = [_single(s, p, [s.xyz, s.xyz, x]) for s, p, x in zip(systems, params, moved)]
+    with BatchEnergy(systems, params) as b:
+        for loop in (False, True, False):
+            b.set_mode(loop)
+            for k, xs in enumerate(([s.xyz for s in systems], moved, moved)):
+                e, grads = b.energy_and_gradient(xs)
+                for j in range(len(systems)):
+                    ref = hist[j][1 if k == 0 else 2]
+                    if precision == PRECISION_MIXED:     # deterministic form: bit for bit
+                        assert np.array_equal(b.terms[j], ref[0]), (loop, k, j, b.terms[j], ref[0])
+                        assert np.array_equal(grads[j], ref[1]), (loop, k, j)
+                    else:   # FP64 mesh atomics add in arrival order: rounding-level differences
+                        rel = np.abs(b.terms[j] - ref[0]) / np.maximum(np.abs(ref[0]), 1.0)
+                        assert rel.max() < 1e-11, (loop, k, j, rel)
+                        assert np.abs(grads[j] - ref[1]).max() < 1e-9
+        assert b.graph_builds >= 1
+
+
+def test_batch_fp64_against_oracle():
+    w = batch_workload(n_systems=6, seed=7, n_min=96, n_max=600, precision=PRECISION_FP64)
+    systems, params = [s for s, _ in w], [p for _, p in w]
+    with BatchEnergy(systems, params) as b:
+        for _ in range(2):
+            e, grads = b.energy_and_gradient()
+            for j, (s, p) in enumerate(w):
+                ref = ob.energy(s, p)
+                rel = np.abs(b.terms[j] - ref["terms"]) / np.maximum(np.abs(ref["terms"]), 1.0)
+                assert rel.max() < 1e-8, (j, rel)
+                assert float(np.sqrt(np.mean((grads[j] - ref["grad"]) ** 2))) < 1e-6
+                assert b.counts[j][2] == ref["counts"][2]
+
+
+def test_lambda_change_recaptures_batch_graph():
+    w = batch_workload(n_systems=4, seed=17, n_min=96, n_max=300, precision=PRECISION_FP64)
+    systems, params = [s for s, _ in w], [p for _, p in w]
+    with BatchEnergy(systems, params) as b:
+        b.energy_and_gradient()
+        e0, _ = b.energy_and_gradient()
+        builds = b.graph_builds
+        s0 = systems[0]
+        soft = np.zeros(s0.n_atoms, dtype=np.int32)
+        soft[:6] = 1
+        a = Alchemy(soft=soft, molecule=np.arange(s0.n_atoms) // 3)
+        f = b.system_energy(0)
+        f.set_alchemy(a)
+        f.set_lambda(0.5)
+        e1, g1 = b.energy_and_gradient()
+        assert b.graph_builds == builds + 1
+        ref = ob.energy(s0, params[0], alchemy=a, lam=0.5)
+        assert abs(e1[0] - ref["terms"][9]) < 1e-8 * abs(ref["terms"][9])
+        assert np.all(np.abs(e1[1:] - e0[1:]) < 1e-11 * np.abs(e0[1:]))   # the other systems unchanged

@@ -119,7 +119,7 @@ def test_fd_gradient_gpu():
 def test_error_status_codes():
     s = water_box(4, 12.4, seed=2)
     with pytest.raises(EnergyException) as ei:
-        ForceFieldEnergy(s, water_params(12.4, pme_grid=(16, 16, 16)))   # box edge < 2 * 9 A vdW cutoff
+        ForceFieldEnergy(s, water_params(12.4, pme_grid=(16, 16, 16), pme_order=4))   # only order 5
     assert ei.value.status == 1
     s = water_box(6, 18.643, seed=2)
     p = water_params(18.643, vdw_cutoff=7.0, ewald_cutoff=7.0, pme_grid=(20, 20, 20), max_scf_iter=1)
