@@ -10,7 +10,9 @@ independent replicas: value = N * steps / (max over ranks of the timed seconds).
   python bench.py [--gpus N] [--steps K] [--warmup W] [--precision both|fp64|mixed]
 
 By default both forms run; the headline value is the mixed-precision form and the
-plain FP64 form is reported beside it under "fp64".
+plain FP64 form is reported beside it under "fp64".  A batch of 512 small systems
+(96-3,000 atoms each) is timed beside it under "batch" (one-graph batch vs a loop of
+single-system launches; --batch-systems 0 skips it).
   python bench.py --impl reference ...   # the CPU FP64 restatement on the host cores
 """
 from __future__ import annotations
@@ -247,6 +249,13 @@ def run_mine(args):
     head_name = order[-1]
     head = runs[head_name]
 
+    batch = None
+    if args.batch_systems > 0:
+        try:
+            batch = measure_batch(args, dist, world, rank)
+        except Exception as exc:     # the headline stands without it
+            batch = {"error": repr(exc)}
+
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         cpu = cpu_baseline(system, build_params(PRECISION_FP64), samples=args.cpu_samples)
@@ -275,6 +284,8 @@ def run_mine(args):
         result["mixed_energy_error_vs_fp64_gpu"] = {
             "total_rel": abs(head["terms"][9] - f["terms"][9]) / abs(f["terms"][9]),
             "terms_abs": [abs(a - b) for a, b in zip(head["terms"], ref_terms)]}
+    if batch:
+        result["batch"] = batch
     if cpu:
         result["cpu_baseline"] = cpu
     if dist:
@@ -282,6 +293,47 @@ def run_mine(args):
         dist.destroy_process_group()
     if rank == 0:
         print(json.dumps(result))
+
+
+def measure_batch(args, dist, world, rank):
+    """Many small systems: ``--batch-systems`` water boxes of 96-3,000 atoms (uniform in
+    multiples of 3, 29.915 A^3 per molecule, PME grid per system at <= 1.2 A rounded up to
+    2,3,5-smooth), mixed precision, energy + gradient of all of them per step through
+    BatchEnergy (host coordinates in, host gradients out).  Systems are split over ranks by
+    the longest-processing-time rule; one all-reduce gathers the per-system energies.  Both
+    the one-graph batch and the loop of single-system launches are timed."""
+    import torch
+    from forcefieldx_b200.batch import BatchEnergy, batch_workload, partition_lpt, torch_all_reduce
+    nsys = args.batch_systems
+    w = batch_workload(n_systems=nsys, seed=2026)
+    parts = partition_lpt([s.n_atoms for s, _ in w], world)
+    mine = parts[rank]
+    reduce_sum = torch_all_reduce() if dist else (lambda a: a)
+    out = {"systems": nsys, "atoms": int(sum(s.n_atoms for s, _ in w)), "steps": args.batch_steps,
+           "metric": "energy+gradient systems/s (e2e: host coordinates in, host gradients out)"}
+    with BatchEnergy([w[j][0] for j in mine], [w[j][1] for j in mine]) as b:
+        for mode in ("graph", "loop"):
+            b.set_mode(mode == "loop")
+            for _ in range(3):
+                b.energy_and_gradient()
+            if dist:
+                dist.barrier()
+            t0 = time.perf_counter()
+            for _ in range(args.batch_steps):
+                e, _ = b.energy_and_gradient()
+            dt = time.perf_counter() - t0
+            if dist:
+                t = torch.tensor([dt], dtype=torch.float64, device="cuda")
+                dist.all_reduce(t, op=dist.ReduceOp.MAX)
+                dt = float(t.item())
+            out[mode] = {"systems_per_s": nsys * args.batch_steps / dt, "ms_per_batch": 1e3 * dt / args.batch_steps}
+        table = np.zeros(nsys)
+        table[mine] = b.terms[:, 9]
+        table = reduce_sum(table)
+        out["pcg_iterations_mean"] = float(np.mean(b.counts[:, 2]))
+        out["graph_over_loop"] = out["graph"]["systems_per_s"] / out["loop"]["systems_per_s"]
+        out["energy_sum_kcal_mol"] = float(np.sum(table))
+    return out
 
 
 def cpu_baseline(system, params, samples=2):
@@ -400,6 +452,9 @@ def main():
     ap.add_argument("--precision", default="both", choices=["both", "fp64", "mixed"])
     ap.add_argument("--cpu-samples", type=int, default=2)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--batch-systems", type=int, default=512,
+                    help="also time a batch of this many small systems (0: skip)")
+    ap.add_argument("--batch-steps", type=int, default=5)
     ap.add_argument("--accuracy-frames", type=int, default=0,
                     help="instead of timing, report the mixed form's error on this many trajectory frames")
     ap.add_argument("--accuracy-equil", type=int, default=200, help="equilibration steps before the first frame")
