@@ -55,6 +55,12 @@ class FfxgAlchemy(ctypes.Structure):
         ("vdw_lambda_alpha", ctypes.c_double), ("vdw_lambda_exponent", ctypes.c_double),
         ("vdw_lambda_end", ctypes.c_double),
         ("intermolecular_softcore", ctypes.c_int32), ("intramolecular_softcore", ctypes.c_int32),
+        ("elec", ctypes.c_int32),
+        ("permanent_lambda_alpha", ctypes.c_double), ("permanent_lambda_exponent", ctypes.c_double),
+        ("permanent_lambda_start", ctypes.c_double), ("permanent_lambda_end", ctypes.c_double),
+        ("polarization_lambda_start", ctypes.c_double), ("polarization_lambda_end", ctypes.c_double),
+        ("polarization_lambda_exponent", ctypes.c_double),
+        ("ligand_vapor_elec", ctypes.c_int32), ("no_ligand_condensed_scf", ctypes.c_int32),
     ]
 
 

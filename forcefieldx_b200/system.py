@@ -431,6 +431,17 @@ class Alchemy:
     vdw_lambda_end: float = 1.0
     intermolecular_softcore: bool = False
     intramolecular_softcore: bool = False
+    # Electrostatics (elec-lambdaterm, OST mode; AlchemicalParameters.java:60-190 defaults).
+    elec: bool = False
+    permanent_lambda_alpha: float = 2.0
+    permanent_lambda_exponent: float = 3.0
+    permanent_lambda_start: float = 0.4
+    permanent_lambda_end: float = 1.0
+    polarization_lambda_start: float = 0.75
+    polarization_lambda_end: float = 1.0
+    polarization_lambda_exponent: float = 3.0
+    ligand_vapor_elec: bool = True
+    no_ligand_condensed_scf: bool = True
 
     def c_struct(self, cabi):
         soft = np.ascontiguousarray(self.soft, dtype=np.int32)
@@ -438,7 +449,12 @@ class Alchemy:
         ptr = lambda a: a.ctypes.data_as(cabi._I) if a is not None else cabi._I()  # noqa: E731
         a = cabi.FfxgAlchemy(ptr(soft), ptr(mol), float(self.vdw_lambda_alpha), float(self.vdw_lambda_exponent),
                              float(self.vdw_lambda_end), int(self.intermolecular_softcore),
-                             int(self.intramolecular_softcore))
+                             int(self.intramolecular_softcore), int(self.elec),
+                             float(self.permanent_lambda_alpha), float(self.permanent_lambda_exponent),
+                             float(self.permanent_lambda_start), float(self.permanent_lambda_end),
+                             float(self.polarization_lambda_start), float(self.polarization_lambda_end),
+                             float(self.polarization_lambda_exponent), int(self.ligand_vapor_elec),
+                             int(self.no_ligand_condensed_scf))
         return a, (soft, mol)
 
 

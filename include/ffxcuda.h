@@ -236,8 +236,22 @@ void ffxg_batch_destroy(ffxg_batch *b);
  * vdw-lambda-alpha 0.25, vdw-lambda-exponent 3, vdw-lambda-end 1, both options off.
  * A pair is softcore when exactly one atom is soft (or both, per the options); its
  * energy is eps * L^n * t1 * t2 with alpha (1 - L)^2 added to both denominators
- * (VanDerWaalsLoop, VanDerWaals.java:1723-1880).  Electrostatic lambda (permanent
- * softcore and the OST polarization pieces) is not part of this library. */
+ * (VanDerWaalsLoop, VanDerWaals.java:1723-1880).
+ *
+ * elec != 0 also decouples the soft atoms' electrostatics as the reference's
+ * elec-lambdaterm in OST mode (ParticleMeshEwald.java:897-935, 1609-1796): the energy is
+ * the sum of (1) the whole system with softcore permanent real-space pairs involving a
+ * soft atom (r^2 + alpha (1 - L_p)^2, scaled by L_p^n), permanent reciprocal space scaled
+ * by L_p^n and polarization scaled by the polarization window's power; (2) the system
+ * without the soft atoms, reciprocal permanent and polarization scaled by the
+ * complements; (3) the soft atoms alone in vacuum (no Ewald, no cutoff), scaled by the
+ * complements.  L_p is lambda mapped into [permanent_lambda_start, _end], the
+ * polarization window likewise (AlchemicalParameters.update, pme/AlchemicalParameters.
+ * java:306-380).  Reference defaults: permanent-lambda-alpha 2, -exponent 3, -start 0.4,
+ * -end 1; polarization-lambda-start 0.75, -end 1, -exponent 3; ligand-vapor-elec and
+ * no-ligand-condensed-scf on.  The vacuum step solves its dipoles with the same PCG as
+ * the periodic steps (the reference uses SOR there): the two agree to the SCF
+ * tolerance. */
 typedef struct ffxg_alchemy {
   const int32_t *soft;
   const int32_t *molecule;
@@ -246,6 +260,16 @@ typedef struct ffxg_alchemy {
   double vdw_lambda_end;
   int32_t intermolecular_softcore;
   int32_t intramolecular_softcore;
+  int32_t elec;
+  double permanent_lambda_alpha;
+  double permanent_lambda_exponent;
+  double permanent_lambda_start;
+  double permanent_lambda_end;
+  double polarization_lambda_start;
+  double polarization_lambda_end;
+  double polarization_lambda_exponent;
+  int32_t ligand_vapor_elec;
+  int32_t no_ligand_condensed_scf;
 } ffxg_alchemy;
 
 /* Set (or, with a == NULL, clear) the soft atoms and softcore keys.  The state starts
@@ -257,7 +281,8 @@ int ffxg_set_alchemy(ffxg_handle *h, const ffxg_alchemy *a);
 int ffxg_set_lambda(ffxg_handle *h, double lambda);
 
 /* dU/dL, d2U/dL2 and dU/dX dL (LambdaInterface getdEdL / getd2EdL2 / getdEdXdL) of the
- * last evaluation: the vdW softcore contributions.  dEdXdL[n][3] (may be NULL) is filled
+ * last evaluation: the vdW softcore contributions, plus the electrostatic ones with
+ * elec set.  dEdXdL[n][3] (may be NULL) is filled
  * only when that evaluation computed a gradient. */
 int ffxg_get_dEdL(ffxg_handle *h, double *dEdL, double *d2EdL2, double *dEdXdL);
 

@@ -215,6 +215,55 @@ struct Alchemy {
   bool inter = false, intra = false;
   double dEdL = 0, d2EdL2 = 0;
   std::vector<double> lgrad;   // [n][3] dU/dX dL
+  // Electrostatics (elec-lambdaterm, OST mode): keys of AlchemicalParameters
+  // (pme/AlchemicalParameters.java:60-190) and their values at lambda (update, :306-380).
+  bool elec = false;
+  double permAlpha = 2.0, permExp = 3.0, permStart = 0.4, permEnd = 1.0;
+  double polStart = 0.75, polEnd = 1.0, polExp = 3.0;
+  bool vaporElec = true, noLigandSCF = true;
+  double lambda = 1.0;
+  double lAlpha = 0, dlAlpha = 0, d2lAlpha = 0;
+  double lPowPerm = 1, dlPowPerm = 0, d2lPowPerm = 0;
+  double lPowPol = 1, dlPowPol = 0, d2lPowPol = 0;
+
+  void update_elec(double l) {
+    lambda = l;
+    lPowPerm = 1.0; dlPowPerm = 0.0; d2lPowPerm = 0.0;
+    lAlpha = 0.0; dlAlpha = 0.0; d2lAlpha = 0.0;
+    if (l < permStart) {
+      lPowPerm = 0.0;
+    } else if (l <= permEnd) {
+      const double scale = 1.0 / (permEnd - permStart);
+      const double pl = scale * (l - permStart);
+      lAlpha = permAlpha * (1.0 - pl) * (1.0 - pl);
+      dlAlpha = permAlpha * (1.0 - pl);
+      d2lAlpha = -permAlpha;
+      lPowPerm = std::pow(pl, permExp);
+      dlPowPerm = permExp * std::pow(pl, permExp - 1.0);
+      d2lPowPerm = 0.0;
+      if (permExp >= 2.0) d2lPowPerm = permExp * (permExp - 1.0) * std::pow(pl, permExp - 2.0);
+      dlAlpha *= scale;
+      d2lAlpha *= scale * scale;
+      dlPowPerm *= scale;
+      d2lPowPerm *= scale * scale;
+    }
+    lPowPol = 1.0; dlPowPol = 0.0; d2lPowPol = 0.0;
+    if (l < polStart) {
+      lPowPol = 0.0;
+    } else if (l <= polEnd) {
+      const double scale = 1.0 / (polEnd - polStart);
+      const double pl = scale * (l - polStart);
+      if (polExp > 0.0) {
+        lPowPol = std::pow(pl, polExp);
+        if (polExp >= 1.0) {
+          dlPowPol = polExp * std::pow(pl, polExp - 1.0);
+          if (polExp >= 2.0) d2lPowPol = polExp * (polExp - 1.0) * std::pow(pl, polExp - 2.0);
+        }
+      }
+      dlPowPol *= scale;
+      d2lPowPol *= scale * scale;
+    }
+  }
 };
 Alchemy g_alch;
 
@@ -257,6 +306,29 @@ struct Oracle {
   bool multi_image = false;
   std::vector<std::vector<int>> nsh, esh, psh;
 
+  // ---- one electrostatics evaluation of the lambda scheme (ParticleMeshEwald
+  // condensedEnergy / condensedNoLigandSCF / ligandElec, PME:1609-1796): which atoms take
+  // part (use), the scales of the permanent and polarization parts, and the lambda
+  // derivative accumulators (dU/dL, d2U/dL2, dU/dX dL with its torque).
+  std::vector<char> use;                 // empty: every atom
+  std::vector<double> pol_eff;           // polarizability, 0 for atoms not in use (PCG)
+  bool lam = false;                      // lambdaTerm
+  bool vapor = false;                    // LambdaMode.VAPOR
+  bool recip_on = true;                  // reciprocal space (off with Ewald alpha 0)
+  bool doPermReal = true, doPol = true;
+  double permScale = 1.0, polScale = 1.0, dEdLSign = 1.0;
+  double stepAlpha = 0.0, stepDlAlpha = 0.0, stepD2lAlpha = 0.0;
+  double eDL = 0.0, eD2L = 0.0;
+  std::vector<double> lgE, ltE;          // [n][3]
+  bool used(int i) const { return use.empty() || use[i]; }
+  // VAPOR pairs skipped by the inter/intramolecular softcore options
+  // (PermanentFieldRegion.java:665-670, RealSpaceEnergyRegion.java:865-870).
+  bool vapor_skip(int i, int k) const {
+    if (!vapor) return false;
+    const bool same = g_alch.mol.empty() ? (i == k) : (g_alch.mol[i] == g_alch.mol[k]);
+    return (g_alch.inter && !same) || (g_alch.intra && same);
+  }
+
   // Displacement of list entry e of atom i, given x_k - x_i on entry: the minimum image
   // (Crystal.image) or, in multi-image mode, x_k + n L - x_i.  sign = -1 for the vdW
   // convention x_i - x_k.  Returns r^2 in Crystal.image's operation order.
@@ -285,7 +357,7 @@ struct Oracle {
   std::vector<double> fieldD, fieldP;    // [n][3]
   std::vector<double> uD, uP, udir, udirP;  // [n][3]
   std::vector<double> grad, torque;      // [n][3]
-  int scf_iter = 0;
+  int scf_iter = 0, scf_total = 0;
   int status = FFXG_OK;
 
   void setup(const ffxg_system *s, const ffxg_params *prm, const double *xyz) {
@@ -914,6 +986,7 @@ struct Oracle {
     }
     grid.assign((size_t)nfx * nfy * nfz, 0.0);
     for (int i = 0; i < n; i++) {
+      if (!used(i)) continue;   // atoms not in use are not spread (ReciprocalSpace.java:2821, 2884)
       const double *f = &fm[10 * (size_t)i];
       const double *sx = &splx[(size_t)i * order * 4], *sy = &sply[(size_t)i * order * 4],
                    *sz = &splz[(size_t)i * order * 4];
@@ -1026,6 +1099,7 @@ struct Oracle {
                       std::vector<std::complex<double>> &grid) {
     grid.assign((size_t)nfx * nfy * nfz, 0.0);
     for (int i = 0; i < n; i++) {
+      if (!used(i)) continue;   // atoms not in use are not spread (ReciprocalSpace.java:2821, 2884)
       double u[3], q[3];
       for (int a = 0; a < 3; a++) {
         u[a] = afrac[a][0] * d[3 * i] + afrac[a][1] * d[3 * i + 1] + afrac[a][2] * d[3 * i + 2];
@@ -1089,6 +1163,7 @@ struct Oracle {
       std::vector<double> emask(n, 1.0), imask(n, 1.0);
 #pragma omp for schedule(dynamic, 64)
       for (int i = 0; i < n; i++) {
+        if (!used(i)) continue;
         double fix = 0, fiy = 0, fiz = 0, fixCR = 0, fiyCR = 0, fizCR = 0;
         const double pdi = ipdamp[i], pti = thole[i];
         const double xi = x[i], yi = y[i], zi = z[i];
@@ -1105,6 +1180,7 @@ struct Oracle {
         for (int g : ip11[i]) imask[g] = p.d11;
         for (size_t e = 0; e < nlist[i].size(); e++) {
           const int k = nlist[i][e];
+          if (!used(k) || vapor_skip(i, k)) continue;
           double xr = x[k] - xi, yr = y[k] - yi, zr = z[k] - zi;
           const double r2 = disp(xr, yr, zr, nsh, i, e);
           if (!(r2 <= off2)) continue;
@@ -1222,6 +1298,7 @@ struct Oracle {
       std::vector<double> &fd = tD[tid], &fp = tP[tid];
 #pragma omp for schedule(dynamic, 64)
       for (int i = 0; i < n; i++) {
+        if (!used(i)) continue;
         double fx = 0, fy = 0, fz = 0, px = 0, py = 0, pz = 0;
         const double xi = x[i], yi = y[i], zi = z[i];
         const double pdi = ipdamp[i], pti = thole[i];
@@ -1229,6 +1306,7 @@ struct Oracle {
         const double pix = up[3 * i], piy = up[3 * i + 1], piz = up[3 * i + 2];
         for (size_t e = 0; e < lists[i].size(); e++) {
           const int k = lists[i][e];
+          if (!used(k) || vapor_skip(i, k)) continue;
           double xr = x[k] - xi, yr = y[k] - yi, zr = z[k] - zi;
           const double r2 = disp(xr, yr, zr, shifts, i, e);
           const double r = std::sqrt(r2);
@@ -1287,11 +1365,16 @@ struct Oracle {
   // InducedDipoleFieldReduceRegion (pme/InducedDipoleFieldReduceRegion.java:159-207).
   void induced_field(const std::vector<double> &ud, const std::vector<double> &up,
                      std::vector<double> &outD, std::vector<double> &outP) {
-    std::vector<std::complex<double>> grid;
-    spread_induced(ud, up, grid);
-    convolve(grid);
-    interpolate(grid, 0, fphiI, cphiI);
-    interpolate(grid, 1, fphiP, cphiP);
+    if (recip_on) {
+      std::vector<std::complex<double>> grid;
+      spread_induced(ud, up, grid);
+      convolve(grid);
+      interpolate(grid, 0, fphiI, cphiI);
+      interpolate(grid, 1, fphiP, cphiP);
+    } else {
+      cphiI.assign(20 * (size_t)n, 0.0); cphiP.assign(20 * (size_t)n, 0.0);
+      fphiI.assign(20 * (size_t)n, 0.0); fphiP.assign(20 * (size_t)n, 0.0);
+    }
     dipole_field(ud, up, ewald, esh, aewald, outD, outP);
     for (int i = 0; i < n; i++)
       for (int a = 0; a < 3; a++) {
@@ -1308,8 +1391,8 @@ struct Oracle {
     // Field of the direct dipoles.
     induced_field(uD, uP, fD, fP);
     for (int i = 0; i < n; i++) {
-      const bool ok = polar[i] > 0.0;
-      const double ip = ok ? 1.0 / polar[i] : 0.0;
+      const bool ok = pol_eff[i] > 0.0;
+      const double ip = ok ? 1.0 / pol_eff[i] : 0.0;
       for (int a = 0; a < 3; a++) {
         const size_t j = 3 * (size_t)i + a;
         r[j] = ok ? (udir[j] - uD[j]) * ip + fD[j] : 0.0;
@@ -1320,8 +1403,8 @@ struct Oracle {
       std::vector<double> ur(m), pr(m);
       for (int i = 0; i < n; i++)
         for (int a = 0; a < 3; a++) {
-          ur[3 * i + a] = polar[i] * r[3 * i + a];
-          pr[3 * i + a] = polar[i] * rCR[3 * i + a];
+          ur[3 * i + a] = pol_eff[i] * r[3 * i + a];
+          pr[3 * i + a] = pol_eff[i] * rCR[3 * i + a];
         }
       dipole_field(ur, pr, precond, psh, 0.0, preD, preP);
     };
@@ -1329,8 +1412,8 @@ struct Oracle {
     for (int i = 0; i < n; i++)
       for (int a = 0; a < 3; a++) {
         const size_t j = 3 * (size_t)i + a;
-        z[j] = polar[i] * (preD[j] + p.precond_scale * r[j]);
-        zCR[j] = polar[i] * (preP[j] + p.precond_scale * rCR[j]);
+        z[j] = pol_eff[i] * (preD[j] + p.precond_scale * r[j]);
+        zCR[j] = pol_eff[i] * (preP[j] + p.precond_scale * rCR[j]);
         pv[j] = z[j]; pCR[j] = zCR[j];
       }
     int iter = 0;
@@ -1340,8 +1423,8 @@ struct Oracle {
       induced_field(pv, pCR, Ap, ApCR);
       double pAp = 0, pApCR = 0, rz = 0, rzCR = 0;
       for (int i = 0; i < n; i++) {
-        const bool ok = polar[i] > 0.0;
-        const double ip = ok ? 1.0 / polar[i] : 0.0;
+        const bool ok = pol_eff[i] > 0.0;
+        const double ip = ok ? 1.0 / pol_eff[i] : 0.0;
         for (int a = 0; a < 3; a++) {
           const size_t j = 3 * (size_t)i + a;
           vec[j] = ok ? pv[j] * ip - Ap[j] : 0.0;
@@ -1374,8 +1457,8 @@ struct Oracle {
       for (int i = 0; i < n; i++)
         for (int a = 0; a < 3; a++) {
           const size_t j = 3 * (size_t)i + a;
-          z[j] = polar[i] * (preD[j] + p.precond_scale * r[j]);
-          zCR[j] = polar[i] * (preP[j] + p.precond_scale * rCR[j]);
+          z[j] = pol_eff[i] * (preD[j] + p.precond_scale * r[j]);
+          zCR[j] = pol_eff[i] * (preP[j] + p.precond_scale * rCR[j]);
           rzNew += r[j] * z[j];
           rzNewCR += rCR[j] * zCR[j];
         }
@@ -1400,8 +1483,15 @@ struct Oracle {
     const double aw3 = -2.0 / 3.0 * electric * aewald * aewald * aewald / kSqrtPi;
     const double aw4 = -2.0 * aw3;
     eSelf = eRecip = eSelfI = eRecipI = 0.0;
+    const bool gr = gradient || lam;      // lambda derivatives need the forces (PME:940)
+    // Scales of the lambda scheme (ReciprocalEnergyRegion.java:230-255, 385-530, 545-740):
+    // permanent parts x permScale, induced parts x polScale; dU/dL picks up
+    // dEdLSign * dlPow * (the unscaled contribution).
+    const double lP = lam ? dEdLSign * g_alch.dlPowPerm : 0.0, l2P = lam ? dEdLSign * g_alch.d2lPowPerm : 0.0;
+    const double lI = lam ? dEdLSign * g_alch.dlPowPol : 0.0, l2I = lam ? dEdLSign * g_alch.d2lPowPol : 0.0;
     double qtot = 0.0;
     for (int i = 0; i < n; i++) {
+      if (!used(i)) continue;
       const double *in = &gm[10 * (size_t)i];
       qtot += in[t000];
       const double cii = in[t000] * in[t000];
@@ -1410,8 +1500,13 @@ struct Oracle {
                          2.0 * (in[t110] * in[t110] + in[t101] * in[t101] + in[t011] * in[t011]);
       eSelf += aewald1 * (cii + aewald2 * (dii / 3.0 + 2.0 * aewald2 * qii / 45.0));
     }
+    eDL += lP * eSelf;
+    eD2L += l2P * eSelf;
+    eSelf *= permScale;
     const int nf[3] = {nfx, nfy, nfz};
+    double dUdL = 0.0, d2UdL2 = 0.0;
     for (int i = 0; i < n; i++) {
+      if (!used(i)) continue;
       const double *ph = &cphi[20 * (size_t)i];
       const double *mp = &gm[10 * (size_t)i];
       const double *f = &fm[10 * (size_t)i];
@@ -1419,7 +1514,9 @@ struct Oracle {
                        (1.0 / 3.0) * (mp[t200] * ph[t200] + mp[t020] * ph[t020] + mp[t002] * ph[t002] +
                                       2.0 * (mp[t110] * ph[t110] + mp[t101] * ph[t101] + mp[t011] * ph[t011]));
       eRecip += e;
-      if (!gradient) continue;
+      dUdL += lP * e;
+      d2UdL2 += l2P * e;
+      if (!gr) continue;
       const double *fp = &fphi[20 * (size_t)i];
       double gx = f[t000] * fp[t100] + f[t100] * fp[t200] + f[t010] * fp[t110] + f[t001] * fp[t101] +
                   f[t200] * fp[t300] + f[t020] * fp[t120] + f[t002] * fp[t102] + f[t110] * fp[t210] +
@@ -1443,31 +1540,51 @@ struct Oracle {
                             mp[t200] * ph[t101] - mp[t110] * ph[t011] - mp[t101] * ph[t002]);
       tqz -= (2.0 / 3.0) * (mp[t200] * ph[t110] + mp[t110] * ph[t020] + mp[t101] * ph[t011] -
                             mp[t110] * ph[t200] - mp[t020] * ph[t110] - mp[t011] * ph[t101]);
-      grad[3 * i] += electric * dfx; grad[3 * i + 1] += electric * dfy; grad[3 * i + 2] += electric * dfz;
-      torque[3 * i] += electric * tqx; torque[3 * i + 1] += electric * tqy; torque[3 * i + 2] += electric * tqz;
+      const double fs = permScale * electric;
+      grad[3 * i] += fs * dfx; grad[3 * i + 1] += fs * dfy; grad[3 * i + 2] += fs * dfz;
+      torque[3 * i] += fs * tqx; torque[3 * i + 1] += fs * tqy; torque[3 * i + 2] += fs * tqz;
+      if (lam) {
+        const double fl = lP * electric;
+        lgE[3 * i] += fl * dfx; lgE[3 * i + 1] += fl * dfy; lgE[3 * i + 2] += fl * dfz;
+        ltE[3 * i] += fl * tqx; ltE[3 * i + 1] += fl * tqy; ltE[3 * i + 2] += fl * tqz;
+      }
     }
-    eRecip *= 0.5 * electric;
+    eDL += 0.5 * dUdL * electric;
+    eD2L += 0.5 * d2UdL2 * electric;
+    eRecip *= permScale * 0.5 * electric;
     eCorr = 0.0;
-    if (qtot != 0.0) eCorr = -0.5 * electric * kPi * (qtot * qtot) / (cell.volume * aewald * aewald);
-    if (p.polarization == FFXG_POLAR_NONE) return;
+    if (qtot != 0.0) {
+      eCorr = -0.5 * electric * kPi * (qtot * qtot) / (cell.volume * aewald * aewald);
+      eDL += lP * eCorr;
+      eD2L += l2P * eCorr;
+      eCorr *= permScale;
+    }
+    if (p.polarization == FFXG_POLAR_NONE || !doPol) return;
     for (int i = 0; i < n; i++) {
+      if (!used(i)) continue;
       const double *mp = &gm[10 * (size_t)i];
       const double dii = uD[3 * i] * mp[t100] + uD[3 * i + 1] * mp[t010] + uD[3 * i + 2] * mp[t001];
       eSelfI += aw3 * dii;
     }
-    if (gradient) {
+    eDL += lI * eSelfI;
+    eD2L += l2I * eSelfI;
+    eSelfI *= polScale;
+    if (gr) {
       for (int i = 0; i < n; i++) {
+        if (!used(i)) continue;
         const double *mp = &gm[10 * (size_t)i];
         const double dix = mp[t100], diy = mp[t010], diz = mp[t001];
         const double uix = 0.5 * (uD[3 * i] + uP[3 * i]);
         const double uiy = 0.5 * (uD[3 * i + 1] + uP[3 * i + 1]);
         const double uiz = 0.5 * (uD[3 * i + 2] + uP[3 * i + 2]);
-        torque[3 * i] += aw4 * (diy * uiz - diz * uiy);
-        torque[3 * i + 1] += aw4 * (diz * uix - dix * uiz);
-        torque[3 * i + 2] += aw4 * (dix * uiy - diy * uix);
+        const double tx = aw4 * (diy * uiz - diz * uiy), ty = aw4 * (diz * uix - dix * uiz),
+                     tz = aw4 * (dix * uiy - diy * uix);
+        torque[3 * i] += polScale * tx; torque[3 * i + 1] += polScale * ty; torque[3 * i + 2] += polScale * tz;
+        if (lam) { ltE[3 * i] += lI * tx; ltE[3 * i + 1] += lI * ty; ltE[3 * i + 2] += lI * tz; }
       }
     }
     for (int i = 0; i < n; i++) {
+      if (!used(i)) continue;
       const double *fP = &fphi[20 * (size_t)i];
       double fi[3], fiCR[3];
       for (int a = 0; a < 3; a++) {
@@ -1476,7 +1593,7 @@ struct Oracle {
       }
       const double indx = fi[0], indy = fi[1], indz = fi[2];
       eRecipI += indx * fP[t100] + indy * fP[t010] + indz * fP[t001];
-      if (!gradient) continue;
+      if (!gr) continue;
       const double *iPhi = &cphiI[20 * (size_t)i], *iCRPhi = &cphiP[20 * (size_t)i];
       const double *fiPhi = &fphiI[20 * (size_t)i], *fiCRPhi = &fphiP[20 * (size_t)i];
       const double *mp = &gm[10 * (size_t)i];
@@ -1519,10 +1636,19 @@ struct Oracle {
                             mp[t200] * sPhi[t101] - mp[t110] * sPhi[t011] - mp[t101] * sPhi[t002]);
       tqz -= (2.0 / 3.0) * (mp[t200] * sPhi[t110] + mp[t110] * sPhi[t020] + mp[t101] * sPhi[t011] -
                             mp[t110] * sPhi[t200] - mp[t020] * sPhi[t110] - mp[t011] * sPhi[t101]);
-      grad[3 * i] += dfx; grad[3 * i + 1] += dfy; grad[3 * i + 2] += dfz;
-      torque[3 * i] += electric * tqx; torque[3 * i + 1] += electric * tqy; torque[3 * i + 2] += electric * tqz;
+      grad[3 * i] += polScale * dfx; grad[3 * i + 1] += polScale * dfy; grad[3 * i + 2] += polScale * dfz;
+      const double ft = polScale * electric;
+      torque[3 * i] += ft * tqx; torque[3 * i + 1] += ft * tqy; torque[3 * i + 2] += ft * tqz;
+      if (lam) {
+        lgE[3 * i] += lI * dfx; lgE[3 * i + 1] += lI * dfy; lgE[3 * i + 2] += lI * dfz;
+        const double fl = lI * electric;
+        ltE[3 * i] += fl * tqx; ltE[3 * i + 1] += fl * tqy; ltE[3 * i + 2] += fl * tqz;
+      }
     }
     eRecipI *= 0.5 * electric;
+    eDL += lI * eRecipI;
+    eD2L += l2I * eRecipI;
+    eRecipI *= polScale;
   }
 
   // ---------------------------------------------------------------------------
@@ -1531,21 +1657,26 @@ struct Oracle {
   // :1700-2177 (polarizationPair).  Returns energies in kcal/mol.
   void real_energy(bool gradient, double &ePerm, double &ePol, int64_t &count) {
     const double electric = p.electric;
-    double eP = 0.0, eI = 0.0;
+    double eP = 0.0, eI = 0.0, eDLt = 0.0, eD2Lt = 0.0;
     int64_t cnt = 0;
-    const bool doPol = p.polarization != FFXG_POLAR_NONE;
+    const bool polOn = p.polarization != FFXG_POLAR_NONE && doPol;
+    const bool gr = gradient || lam;
     std::vector<std::vector<double>> tg(nthreads, std::vector<double>(3 * (size_t)n, 0.0));
     std::vector<std::vector<double>> tt(nthreads, std::vector<double>(3 * (size_t)n, 0.0));
-#pragma omp parallel reduction(+ : eP, eI, cnt)
+    std::vector<std::vector<double>> tlg(lam ? nthreads : 0, std::vector<double>(3 * (size_t)n, 0.0));
+    std::vector<std::vector<double>> tlt(lam ? nthreads : 0, std::vector<double>(3 * (size_t)n, 0.0));
+#pragma omp parallel reduction(+ : eP, eI, cnt, eDLt, eD2Lt)
     {
       int tid = 0;
 #ifdef _OPENMP
       tid = omp_get_thread_num();
 #endif
       std::vector<double> &g = tg[tid], &tq = tt[tid];
+      std::vector<double> *lgp = lam ? &tlg[tid] : nullptr, *ltp = lam ? &tlt[tid] : nullptr;
       std::vector<double> mmask(n, 1.0), pmask(n, 1.0), dmask(n, 1.0);
 #pragma omp for schedule(dynamic, 64)
       for (int i = 0; i < n; i++) {
+        if (!used(i)) continue;
         for (int k : m12[i]) { pmask[k] = p.p12; mmask[k] = p.m12; }
         for (int k : m13[i]) { pmask[k] = p.p13; mmask[k] = p.m13; }
         for (int k : m14[i]) {
@@ -1564,9 +1695,15 @@ struct Oracle {
         const double pdi = ipdamp[i], pti = thole[i];
         for (size_t e = 0; e < ewald[i].size(); e++) {
           const int k = ewald[i][e];
+          if (!used(k) || vapor_skip(i, k)) continue;
           double xr = x[k] - xi, yr = y[k] - yi, zr = z[k] - zi;
           const double r2 = disp(xr, yr, zr, esh, i, e);
           const bool prim = primary(esh, i, e);
+          // Softcore pairs (RealSpaceEnergyRegion.java:873-883): a soft atom in the pair and
+          // permanent real space on: r^2 + lAlpha and the permanent scale l2.
+          const bool soft = lam && (g_alch.soft[i] || g_alch.soft[k]);
+          double beta = 0.0, l2 = 1.0;
+          if (soft && doPermReal) { beta = stepAlpha; l2 = permScale; }
           const double *mk = &gm[10 * (size_t)k];
           const double ck = mk[t000], dkx = mk[t100], dky = mk[t010], dkz = mk[t001];
           const double qkxx = mk[t200] / 3.0, qkyy = mk[t020] / 3.0, qkzz = mk[t002] / 3.0;
@@ -1575,7 +1712,7 @@ struct Oracle {
           const double pkx = uP[3 * k], pky = uP[3 * k + 1], pkz = uP[3 * k + 2];
           const double scale = prim ? mmask[k] : 1.0, scalep = prim ? pmask[k] : 1.0;
           const double scaled = prim ? dmask[k] : 1.0;
-          const double r = std::sqrt(r2);
+          const double r = std::sqrt(r2 + beta);
           const double ralpha = aewald * r;
           const double exp2a = std::exp(-ralpha * ralpha);
           const double rr1 = 1.0 / r, rr2 = rr1 * rr1;
@@ -1585,8 +1722,9 @@ struct Oracle {
           const double bn3 = (5.0 * bn2 + an2 * exp2a) * rr2;
           const double bn4 = (7.0 * bn3 + an3 * exp2a) * rr2;
           const double bn5 = (9.0 * bn4 + an4 * exp2a) * rr2;
+          const double bn6 = (11.0 * bn5 + an5 * exp2a) * rr2;
           const double rr3 = rr1 * rr2, rr5 = 3.0 * rr3 * rr2, rr7 = 5.0 * rr5 * rr2;
-          const double rr9 = 7.0 * rr7 * rr2, rr11 = 9.0 * rr9 * rr2;
+          const double rr9 = 7.0 * rr7 * rr2, rr11 = 9.0 * rr9 * rr2, rr13 = 11.0 * rr11 * rr2;
           double scale3 = 1.0, scale5 = 1.0, scale7 = 1.0;
           double ddsc3x = 0, ddsc3y = 0, ddsc3z = 0, ddsc5x = 0, ddsc5y = 0, ddsc5z = 0, ddsc7x = 0, ddsc7y = 0, ddsc7z = 0;
           double damp = pdi * ipdamp[k];
@@ -1606,7 +1744,7 @@ struct Oracle {
             ddsc7x = temp7 * ddsc5x; ddsc7y = temp7 * ddsc5y; ddsc7z = temp7 * ddsc5z;
           }
           // ---- permanentPair
-          {
+          if (doPermReal) {
             const double dixdkx = diy * dkz - diz * dky, dixdky = diz * dkx - dix * dkz, dixdkz = dix * dky - diy * dkx;
             const double dixrx = diy * zr - diz * yr, dixry = diz * xr - dix * zr, dixrz = dix * yr - diy * xr;
             const double dkxrx = dky * zr - dkz * yr, dkxry = dkz * xr - dkx * zr, dkxrz = dkx * yr - dky * xr;
@@ -1656,8 +1794,8 @@ struct Oracle {
             const double ereal = gl0 * bn0 + (gl1 + gl6) * bn1 + (gl2 + gl7 + gl8) * bn2 + (gl3 + gl5) * bn3 + gl4 * bn4;
             const double efix = scale1 * (gl0 * rr1 + (gl1 + gl6) * rr3 + (gl2 + gl7 + gl8) * rr5 + (gl3 + gl5) * rr7 + gl4 * rr9);
             const double e = ereal - efix;
-            if (e != 0.0) { eP += e; cnt++; }
-            if (gradient) {
+            if (e != 0.0) { eP += l2 * e; cnt++; }
+            if (gr) {
               const double gf1 = bn1 * gl0 + bn2 * (gl1 + gl6) + bn3 * (gl2 + gl7 + gl8) + bn4 * (gl3 + gl5) + bn5 * gl4;
               const double gf2 = -ck * bn1 + sc4 * bn2 - sc6 * bn3;
               const double gf3 = ci * bn1 + sc3 * bn2 + sc5 * bn3;
@@ -1695,14 +1833,79 @@ struct Oracle {
                 ttm2x -= scale1 * ttm2rx; ttm2y -= scale1 * ttm2ry; ttm2z -= scale1 * ttm2rz;
                 ttm3x -= scale1 * ttm3rx; ttm3y -= scale1 * ttm3ry; ttm3z -= scale1 * ttm3rz;
               }
-              const double pre = electric;
+              const double pre = electric * l2;
               g[3 * i] += pre * ftm2x; g[3 * i + 1] += pre * ftm2y; g[3 * i + 2] += pre * ftm2z;
               tq[3 * i] += pre * ttm2x; tq[3 * i + 1] += pre * ttm2y; tq[3 * i + 2] += pre * ttm2z;
               g[3 * k] -= pre * ftm2x; g[3 * k + 1] -= pre * ftm2y; g[3 * k + 2] -= pre * ftm2z;
               tq[3 * k] += pre * ttm3x; tq[3 * k + 1] += pre * ttm3y; tq[3 * k + 2] += pre * ttm3z;
+              if (soft) {   // dU/dL/dX of the first term, d[dlPow * ereal]/dX (:1465-1475)
+                const double pf = electric * dEdLSign * g_alch.dlPowPerm;
+                std::vector<double> &lg = *lgp, &lt = *ltp;
+                lg[3 * i] += pf * ftm2x; lg[3 * i + 1] += pf * ftm2y; lg[3 * i + 2] += pf * ftm2z;
+                lt[3 * i] += pf * ttm2x; lt[3 * i + 1] += pf * ttm2y; lt[3 * i + 2] += pf * ttm2z;
+                lg[3 * k] -= pf * ftm2x; lg[3 * k + 1] -= pf * ftm2y; lg[3 * k + 2] -= pf * ftm2z;
+                lt[3 * k] += pf * ttm3x; lt[3 * k + 1] += pf * ttm3y; lt[3 * k + 2] += pf * ttm3z;
+              }
+            }
+            if (soft) {
+              // dU/dL and d2U/dL2 of the pair through the scale and the softcore shift, and
+              // dU/dL/dX of the second term with every radial order one higher (:1477-1690).
+              const double dRealdL = gl0 * bn1 + (gl1 + gl6) * bn2 + (gl2 + gl7 + gl8) * bn3 + (gl3 + gl5) * bn4 + gl4 * bn5;
+              const double d2RealdL2 = gl0 * bn2 + (gl1 + gl6) * bn3 + (gl2 + gl7 + gl8) * bn4 + (gl3 + gl5) * bn5 + gl4 * bn6;
+              const double dlP = g_alch.dlPowPerm, d2lP = g_alch.d2lPowPerm;
+              eDLt += dEdLSign * dlP * ereal + l2 * stepDlAlpha * dRealdL;
+              eD2Lt += dEdLSign * (d2lP * ereal + dlP * stepDlAlpha * dRealdL + dlP * stepDlAlpha * dRealdL) +
+                       l2 * stepD2lAlpha * dRealdL + l2 * stepDlAlpha * stepDlAlpha * d2RealdL2;
+              double dFixdL = gl0 * rr3 + (gl1 + gl6) * rr5 + (gl2 + gl7 + gl8) * rr7 + (gl3 + gl5) * rr9 + gl4 * rr11;
+              double d2FixdL2 = gl0 * rr5 + (gl1 + gl6) * rr7 + (gl2 + gl7 + gl8) * rr9 + (gl3 + gl5) * rr11 + gl4 * rr13;
+              dFixdL *= scale1;
+              d2FixdL2 *= scale1;
+              eDLt -= dEdLSign * dlP * efix + l2 * stepDlAlpha * dFixdL;
+              eD2Lt -= dEdLSign * (d2lP * efix + dlP * stepDlAlpha * dFixdL + dlP * stepDlAlpha * dFixdL) +
+                       l2 * stepD2lAlpha * dFixdL + l2 * stepDlAlpha * stepDlAlpha * d2FixdL2;
+              const double gf1 = bn2 * gl0 + bn3 * (gl1 + gl6) + bn4 * (gl2 + gl7 + gl8) + bn5 * (gl3 + gl5) + bn6 * gl4;
+              const double gf2 = -ck * bn2 + sc4 * bn3 - sc6 * bn4;
+              const double gf3 = ci * bn2 + sc3 * bn3 + sc5 * bn4;
+              const double gf4 = 2.0 * bn3;
+              const double gf5 = 2.0 * (-ck * bn3 + sc4 * bn4 - sc6 * bn5);
+              const double gf6 = 2.0 * (-ci * bn3 - sc3 * bn4 - sc5 * bn5);
+              const double gf7 = 4.0 * bn4;
+              double ftm2x = gf1 * xr + gf2 * dix + gf3 * dkx + gf4 * (qkdix - qidkx) + gf5 * qirx + gf6 * qkrx + gf7 * (qiqkrx + qkqirx);
+              double ftm2y = gf1 * yr + gf2 * diy + gf3 * dky + gf4 * (qkdiy - qidky) + gf5 * qiry + gf6 * qkry + gf7 * (qiqkry + qkqiry);
+              double ftm2z = gf1 * zr + gf2 * diz + gf3 * dkz + gf4 * (qkdiz - qidkz) + gf5 * qirz + gf6 * qkrz + gf7 * (qiqkrz + qkqirz);
+              double ttm2x = -bn2 * dixdkx + gf2 * dixrx + gf4 * (dixqkrx + dkxqirx + rxqidkx - 2.0 * qixqkx) - gf5 * rxqirx - gf7 * (rxqikrx + qkrxqirx);
+              double ttm2y = -bn2 * dixdky + gf2 * dixry + gf4 * (dixqkry + dkxqiry + rxqidky - 2.0 * qixqky) - gf5 * rxqiry - gf7 * (rxqikry + qkrxqiry);
+              double ttm2z = -bn2 * dixdkz + gf2 * dixrz + gf4 * (dixqkrz + dkxqirz + rxqidkz - 2.0 * qixqkz) - gf5 * rxqirz - gf7 * (rxqikrz + qkrxqirz);
+              double ttm3x = bn2 * dixdkx + gf3 * dkxrx - gf4 * (dixqkrx + dkxqirx + rxqkdix - 2.0 * qixqkx) - gf6 * rxqkrx - gf7 * (rxqkirx - qkrxqirx);
+              double ttm3y = bn2 * dixdky + gf3 * dkxry - gf4 * (dixqkry + dkxqiry + rxqkdiy - 2.0 * qixqky) - gf6 * rxqkry - gf7 * (rxqkiry - qkrxqiry);
+              double ttm3z = bn2 * dixdkz + gf3 * dkxrz - gf4 * (dixqkrz + dkxqirz + rxqkdiz - 2.0 * qixqkz) - gf6 * rxqkrz - gf7 * (rxqkirz - qkrxqirz);
+              if (scale1 != 0.0) {
+                const double gfr1 = rr5 * gl0 + rr7 * (gl1 + gl6) + rr9 * (gl2 + gl7 + gl8) + rr11 * (gl3 + gl5) + rr13 * gl4;
+                const double gfr2 = -ck * rr5 + sc4 * rr7 - sc6 * rr9;
+                const double gfr3 = ci * rr5 + sc3 * rr7 + sc5 * rr9;
+                const double gfr4 = 2.0 * rr7;
+                const double gfr5 = 2.0 * (-ck * rr7 + sc4 * rr9 - sc6 * rr11);
+                const double gfr6 = 2.0 * (-ci * rr7 - sc3 * rr9 - sc5 * rr11);
+                const double gfr7 = 4.0 * rr9;
+                ftm2x -= scale1 * (gfr1 * xr + gfr2 * dix + gfr3 * dkx + gfr4 * (qkdix - qidkx) + gfr5 * qirx + gfr6 * qkrx + gfr7 * (qiqkrx + qkqirx));
+                ftm2y -= scale1 * (gfr1 * yr + gfr2 * diy + gfr3 * dky + gfr4 * (qkdiy - qidky) + gfr5 * qiry + gfr6 * qkry + gfr7 * (qiqkry + qkqiry));
+                ftm2z -= scale1 * (gfr1 * zr + gfr2 * diz + gfr3 * dkz + gfr4 * (qkdiz - qidkz) + gfr5 * qirz + gfr6 * qkrz + gfr7 * (qiqkrz + qkqirz));
+                ttm2x -= scale1 * (-rr5 * dixdkx + gfr2 * dixrx + gfr4 * (dixqkrx + dkxqirx + rxqidkx - 2.0 * qixqkx) - gfr5 * rxqirx - gfr7 * (rxqikrx + qkrxqirx));
+                ttm2y -= scale1 * (-rr5 * dixdky + gfr2 * dixry + gfr4 * (dixqkry + dkxqiry + rxqidky - 2.0 * qixqky) - gfr5 * rxqiry - gfr7 * (rxqikry + qkrxqiry));
+                ttm2z -= scale1 * (-rr5 * dixdkz + gfr2 * dixrz + gfr4 * (dixqkrz + dkxqirz + rxqidkz - 2.0 * qixqkz) - gfr5 * rxqirz - gfr7 * (rxqikrz + qkrxqirz));
+                ttm3x -= scale1 * (rr5 * dixdkx + gfr3 * dkxrx - gfr4 * (dixqkrx + dkxqirx + rxqkdix - 2.0 * qixqkx) - gfr6 * rxqkrx - gfr7 * (rxqkirx - qkrxqirx));
+                ttm3y -= scale1 * (rr5 * dixdky + gfr3 * dkxry - gfr4 * (dixqkry + dkxqiry + rxqkdiy - 2.0 * qixqky) - gfr6 * rxqkry - gfr7 * (rxqkiry - qkrxqiry));
+                ttm3z -= scale1 * (rr5 * dixdkz + gfr3 * dkxrz - gfr4 * (dixqkrz + dkxqirz + rxqkdiz - 2.0 * qixqkz) - gfr6 * rxqkrz - gfr7 * (rxqkirz - qkrxqirz));
+              }
+              const double pf = electric * l2 * stepDlAlpha;
+              std::vector<double> &lg = *lgp, &lt = *ltp;
+              lg[3 * i] += pf * ftm2x; lg[3 * i + 1] += pf * ftm2y; lg[3 * i + 2] += pf * ftm2z;
+              lt[3 * i] += pf * ttm2x; lt[3 * i + 1] += pf * ttm2y; lt[3 * i + 2] += pf * ttm2z;
+              lg[3 * k] -= pf * ftm2x; lg[3 * k + 1] -= pf * ftm2y; lg[3 * k + 2] -= pf * ftm2z;
+              lt[3 * k] += pf * ttm3x; lt[3 * k + 1] += pf * ttm3y; lt[3 * k + 2] += pf * ttm3z;
             }
           }
-          if (!doPol) continue;
+          if (!polOn) continue;
           // ---- polarizationPair
           {
             const double dsc3 = 1.0 - scale3 * scaled, dsc5 = 1.0 - scale5 * scaled, dsc7 = 1.0 - scale7 * scaled;
@@ -1763,8 +1966,13 @@ struct Oracle {
             const double glip6 = scip1, glip7 = 2.0 * (scip7 - scip8);
             const double ereal = (gli1 + gli6) * bn1 + (gli2 + gli7) * bn2 + gli3 * bn3;
             const double efix = (gli1 + gli6) * rr3 * psc3 + (gli2 + gli7) * rr5 * psc5 + gli3 * rr7 * psc7;
-            eI += 0.5 * (ereal - efix);
-            if (!gradient) continue;
+            const double epol = 0.5 * (ereal - efix);
+            eI += polScale * epol;
+            if (lam) {
+              eDLt += dEdLSign * g_alch.dlPowPol * epol;
+              eD2Lt += dEdLSign * g_alch.d2lPowPol * epol;
+            }
+            if (!gr) continue;
             const bool dorli = (psc3 != 0.0 || dsc3 != 0.0 || usc3 != 0.0);
             const double gfi1 = 0.5 * bn2 * (gli1 + glip1 + gli6 + glip6) + 0.5 * bn2 * scip2 +
                                 0.5 * bn3 * (gli2 + glip2 + gli7 + glip7) - 0.5 * bn3 * (sci3 * scip4 + scip3 * sci4) +
@@ -1857,11 +2065,19 @@ struct Oracle {
             ftm2ix -= ftm2rix; ftm2iy -= ftm2riy; ftm2iz -= ftm2riz;
             ttm2ix -= ttm2rix; ttm2iy -= ttm2riy; ttm2iz -= ttm2riz;
             ttm3ix -= ttm3rix; ttm3iy -= ttm3riy; ttm3iz -= ttm3riz;
-            const double sc = electric;
+            const double sc = electric * polScale;
             g[3 * i] += sc * ftm2ix; g[3 * i + 1] += sc * ftm2iy; g[3 * i + 2] += sc * ftm2iz;
             tq[3 * i] += sc * ttm2ix; tq[3 * i + 1] += sc * ttm2iy; tq[3 * i + 2] += sc * ttm2iz;
             g[3 * k] -= sc * ftm2ix; g[3 * k + 1] -= sc * ftm2iy; g[3 * k + 2] -= sc * ftm2iz;
             tq[3 * k] += sc * ttm3ix; tq[3 * k + 1] += sc * ttm3iy; tq[3 * k + 2] += sc * ttm3iz;
+            if (lam) {   // RealSpaceEnergyRegion.java:2163-2174
+              const double sl = electric * dEdLSign * g_alch.dlPowPol;
+              std::vector<double> &lg = *lgp, &lt = *ltp;
+              lg[3 * i] += sl * ftm2ix; lg[3 * i + 1] += sl * ftm2iy; lg[3 * i + 2] += sl * ftm2iz;
+              lt[3 * i] += sl * ttm2ix; lt[3 * i + 1] += sl * ttm2iy; lt[3 * i + 2] += sl * ttm2iz;
+              lg[3 * k] -= sl * ftm2ix; lg[3 * k + 1] -= sl * ftm2iy; lg[3 * k + 2] -= sl * ftm2iz;
+              lt[3 * k] += sl * ttm3ix; lt[3 * k + 1] += sl * ttm3iy; lt[3 * k + 2] += sl * ttm3iz;
+            }
           }
         }
         for (int k : m12[i]) { pmask[k] = 1.0; mmask[k] = 1.0; }
@@ -1871,9 +2087,15 @@ struct Oracle {
         for (int gg : ip11[i]) dmask[gg] = 1.0;
       }
     }
-    if (gradient)
+    if (gr)
       for (int t = 0; t < nthreads; t++)
         for (size_t j = 0; j < 3 * (size_t)n; j++) { grad[j] += tg[t][j]; torque[j] += tt[t][j]; }
+    if (lam) {
+      for (int t = 0; t < nthreads; t++)
+        for (size_t j = 0; j < 3 * (size_t)n; j++) { lgE[j] += tlg[t][j]; ltE[j] += tlt[t][j]; }
+      eDL += eDLt * electric;
+      eD2L += eD2Lt * electric;
+    }
     ePerm = eP * electric;
     ePol = eI * electric;
     count = cnt;
@@ -2015,15 +2237,145 @@ struct Oracle {
     }
   }
 
-  void torque_to_gradient() {
+  void torque_to_gradient() { torque_to_gradient(torque, grad); }
+
+  void torque_to_gradient(const std::vector<double> &tq, std::vector<double> &gr) {
     for (int i = 0; i < n; i++) {
       int idx[4];
       double g[4][3];
-      torque_one(i, &torque[3 * (size_t)i], idx, g);
+      torque_one(i, &tq[3 * (size_t)i], idx, g);
       for (int a = 0; a < 4; a++)
         if (idx[a] >= 0)
-          for (int d = 0; d < 3; d++) grad[3 * (size_t)idx[a] + d] += g[a][d];
+          for (int d = 0; d < 3; d++) gr[3 * (size_t)idx[a] + d] += g[a][d];
     }
+  }
+
+  // Per-term electrostatic energies of one evaluation.
+  struct ElecTerms {
+    double eSelf = 0, eRecip = 0, eCorr = 0, eSelfI = 0, eRecipI = 0, eReal = 0, eRealI = 0;
+    int64_t nreal = 0;
+    void add(const ElecTerms &o) {
+      eSelf += o.eSelf; eRecip += o.eRecip; eCorr += o.eCorr; eSelfI += o.eSelfI; eRecipI += o.eRecipI;
+      eReal += o.eReal; eRealI += o.eRealI;
+    }
+  };
+
+  // ParticleMeshEwald.computeEnergy (ParticleMeshEwald.java:1871-2183) for the current
+  // step state: permanent field, SCF, reciprocal and real-space energy and gradient.
+  int electrostatics_step(bool gradient, ElecTerms &t) {
+    if (recip_on) {
+      std::vector<std::complex<double>> grid;
+      spread_permanent(grid);
+      convolve(grid);
+      interpolate(grid, 0, fphi, cphi);
+    } else {
+      cphi.assign(20 * (size_t)n, 0.0);
+      fphi.assign(20 * (size_t)n, 0.0);
+    }
+    permanent_field();
+    uD.assign(3 * (size_t)n, 0.0); uP.assign(3 * (size_t)n, 0.0);
+    udir.assign(3 * (size_t)n, 0.0); udirP.assign(3 * (size_t)n, 0.0);
+    int st = FFXG_OK;
+    if (p.polarization != FFXG_POLAR_NONE && doPol) {
+      // DirectRegion (pme/DirectRegion.java:170-243).
+      for (int i = 0; i < n; i++)
+        for (int a = 0; a < 3; a++) {
+          const size_t j = 3 * (size_t)i + a;
+          const double f = aewald3 * gm[10 * (size_t)i + 1 + a] - cphi[20 * (size_t)i + 1 + a];
+          fieldD[j] += f; fieldP[j] += f;
+          uD[j] = polar[i] * fieldD[j]; udir[j] = uD[j];
+          uP[j] = polar[i] * fieldP[j]; udirP[j] = uP[j];
+        }
+      int it = 0;
+      if (p.polarization == FFXG_POLAR_MUTUAL) {
+        st = pcg();
+        it = scf_iter;
+      }
+      scf_total += it;
+      if (st != FFXG_OK) return st;
+      std::vector<double> fD, fP;
+      induced_field(uD, uP, fD, fP);  // final field (PCGSolver.java:601)
+    }
+    if (recip_on) recip_energy(gradient, t.eSelf, t.eRecip, t.eCorr, t.eSelfI, t.eRecipI);
+    real_energy(gradient, t.eReal, t.eRealI, t.nreal);
+    return st;
+  }
+
+  // The three evaluations of elec-lambdaterm in OST mode (ParticleMeshEwald.energy,
+  // PME:897-935): condensedEnergy (:1609-1640), condensedNoLigandSCF (:1650-1700) and
+  // ligandElec (:1704-1796).  The vacuum step solves by PCG (the reference: SOR).
+  int lambda_electrostatics(bool gradient, ElecTerms &sum, int64_t &nreal) {
+    const Alchemy &al = g_alch;
+    const double l = al.lambda;
+    lgE.assign(3 * (size_t)n, 0.0);
+    ltE.assign(3 * (size_t)n, 0.0);
+    eDL = eD2L = 0.0;
+    lam = true;
+    // 1. Everything, softcore permanent real space, scaled reciprocal and polarization.
+    use.clear();
+    pol_eff = polar;
+    vapor = false; recip_on = true; doPermReal = true;
+    permScale = al.lPowPerm; dEdLSign = 1.0;
+    stepAlpha = al.lAlpha; stepDlAlpha = al.dlAlpha; stepD2lAlpha = al.d2lAlpha;
+    if (l < al.polStart) { doPol = false; polScale = 0.0; }
+    else if (l <= al.polEnd) { doPol = true; polScale = al.lPowPol; }
+    else { doPol = true; polScale = 1.0; }
+    ElecTerms t1;
+    int st = electrostatics_step(gradient, t1);
+    if (st != FFXG_OK) return st;
+    sum.add(t1);
+    nreal = t1.nreal;
+    // 2. Without the soft atoms: reciprocal permanent and polarization, complements.
+    use.assign(n, 1);
+    bool any = false;
+    for (int i = 0; i < n; i++) { use[i] = !al.soft[i]; any = any || use[i]; }
+    for (int i = 0; i < n; i++) pol_eff[i] = use[i] ? polar[i] : 0.0;
+    doPermReal = false;
+    permScale = 1.0 - al.lPowPerm; dEdLSign = -1.0;
+    if (l <= al.polEnd && al.noLigandSCF) { doPol = true; polScale = 1.0 - al.lPowPol; }
+    else { doPol = false; polScale = 0.0; }
+    if (any) {
+      ElecTerms t2;
+      st = electrostatics_step(gradient, t2);
+      if (st != FFXG_OK) return st;
+      sum.add(t2);
+    }
+    // 3. The soft atoms alone in vacuum: no Ewald screening, no cutoff, no images.
+    if (al.vaporElec) {
+      for (int i = 0; i < n; i++) { use[i] = al.soft[i] != 0; pol_eff[i] = use[i] ? polar[i] : 0.0; }
+      vapor = true; doPermReal = true;
+      permScale = 1.0 - al.lPowPerm; dEdLSign = -1.0;
+      stepAlpha = stepDlAlpha = stepD2lAlpha = 0.0;
+      if (l <= al.polEnd) { doPol = true; polScale = 1.0 - al.lPowPol; }
+      else { doPol = false; polScale = 0.0; }
+      const double sv[9] = {aewald, an0, an1, an2, an3, an4, an5, aewald3, off2};
+      const bool mi = multi_image;
+      std::vector<std::vector<int>> nl = nlist, ns = nsh;
+      aewald = an0 = an1 = an2 = an3 = an4 = an5 = aewald3 = 0.0;
+      off2 = INFINITY;
+      recip_on = false;
+      multi_image = true;
+      nlist.assign(n, {});
+      nsh.assign(n, {});
+      for (int i = 0; i < n; i++)
+        if (use[i])
+          for (int k = i + 1; k < n; k++)
+            if (use[k]) { nlist[i].push_back(k); nsh[i].push_back(pack_shift(0, 0, 0, true)); }
+      ElecTerms t3;
+      st = electrostatics_step(gradient, t3);
+      aewald = sv[0]; an0 = sv[1]; an1 = sv[2]; an2 = sv[3]; an3 = sv[4]; an4 = sv[5]; an5 = sv[6];
+      aewald3 = sv[7]; off2 = sv[8];
+      multi_image = mi;
+      nlist.swap(nl);
+      nsh.swap(ns);
+      recip_on = true;
+      if (st != FFXG_OK) return st;
+      sum.add(t3);
+    }
+    lam = false; vapor = false; use.clear(); pol_eff = polar;
+    doPermReal = true; doPol = true; permScale = polScale = dEdLSign = 1.0;
+    stepAlpha = stepDlAlpha = stepD2lAlpha = 0.0;
+    return FFXG_OK;
   }
 
   // ---------------------------------------------------------------------------
@@ -2037,34 +2389,29 @@ struct Oracle {
     const double evdw = vdw(gradient, nv);
     rotate_multipoles();
     compute_bsplines();
-    std::vector<std::complex<double>> grid;
-    spread_permanent(grid);
-    convolve(grid);
-    interpolate(grid, 0, fphi, cphi);
-    permanent_field();
-    uD.assign(3 * (size_t)n, 0.0); uP.assign(3 * (size_t)n, 0.0);
-    udir.assign(3 * (size_t)n, 0.0); udirP.assign(3 * (size_t)n, 0.0);
     scf_iter = 0;
+    scf_total = 0;
     int st = FFXG_OK;
-    if (p.polarization != FFXG_POLAR_NONE) {
-      // DirectRegion (pme/DirectRegion.java:170-243).
-      for (int i = 0; i < n; i++)
-        for (int a = 0; a < 3; a++) {
-          const size_t j = 3 * (size_t)i + a;
-          const double f = aewald3 * gm[10 * (size_t)i + 1 + a] - cphi[20 * (size_t)i + 1 + a];
-          fieldD[j] += f; fieldP[j] += f;
-          uD[j] = polar[i] * fieldD[j]; udir[j] = uD[j];
-          uP[j] = polar[i] * fieldP[j]; udirP[j] = uP[j];
-        }
-      if (p.polarization == FFXG_POLAR_MUTUAL) st = pcg();
-      if (st != FFXG_OK) return st;
-      std::vector<double> fD, fP;
-      induced_field(uD, uP, fD, fP);  // final field (PCGSolver.java:601)
-    }
-    double eSelf, eRecip, eCorr, eSelfI, eRecipI, eReal, eRealI;
-    recip_energy(gradient, eSelf, eRecip, eCorr, eSelfI, eRecipI);
+    ElecTerms et;
     int64_t nreal = 0;
-    real_energy(gradient, eReal, eRealI, nreal);
+    if (g_alch.on && g_alch.elec) {
+      st = lambda_electrostatics(gradient, et, nreal);
+      if (st != FFXG_OK) return st;
+      torque_to_gradient(ltE, lgE);
+      g_alch.dEdL += eDL;
+      g_alch.d2EdL2 += eD2L;
+      if (g_alch.lgrad.size() == lgE.size())
+        for (size_t j = 0; j < lgE.size(); j++) g_alch.lgrad[j] += lgE[j];
+    } else {
+      use.clear();
+      pol_eff = polar;
+      st = electrostatics_step(gradient, et);
+      if (st != FFXG_OK) return st;
+      nreal = et.nreal;
+    }
+    scf_iter = scf_total;
+    const double eSelf = et.eSelf, eRecip = et.eRecip, eCorr = et.eCorr, eSelfI = et.eSelfI,
+                 eRecipI = et.eRecipI, eReal = et.eReal, eRealI = et.eRealI;
     if (gradient) torque_to_gradient();
     if (terms) {
       terms[FFXG_TERM_VDW] = evdw;
@@ -2188,6 +2535,19 @@ void oracle_set_alchemy(const ffxg_alchemy *a, int n, double lambda) {
   g_alch.sc2 = std::pow(l, ex);
   g_alch.dsc2dL = ex * std::pow(l, ex - 1.0);
   g_alch.d2sc2dL2 = (ex >= 2.0) ? ex * (ex - 1.0) * std::pow(l, ex - 2.0) : 0.0;
+  g_alch.elec = a->elec != 0;
+  if (g_alch.elec) {
+    g_alch.permAlpha = a->permanent_lambda_alpha;
+    g_alch.permExp = a->permanent_lambda_exponent;
+    g_alch.permStart = a->permanent_lambda_start;
+    g_alch.permEnd = a->permanent_lambda_end;
+    g_alch.polStart = a->polarization_lambda_start;
+    g_alch.polEnd = a->polarization_lambda_end;
+    g_alch.polExp = a->polarization_lambda_exponent;
+    g_alch.vaporElec = a->ligand_vapor_elec != 0;
+    g_alch.noLigandSCF = a->no_ligand_condensed_scf != 0;
+    g_alch.update_elec(lambda);
+  }
 }
 
 // dU/dL, d2U/dL2 and dU/dX dL [n][3] of the last oracle_energy call.
