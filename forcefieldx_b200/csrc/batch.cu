@@ -101,6 +101,7 @@ static bool batch_graph_ready(ffxg_batch &b) {
   for (size_t s = 0; s < b.sys.size(); s++) {
     const Handle &h = handle_of(b.sys[s]);
     if (!h.list_valid || !h.use_graphs || h.timing) return false;
+    if (h.elec.on && h.alch.active) return false;   // electrostatic lambda runs as direct launches
     if (!stale && b.gen[s] != h.graph_gen) stale = true;
   }
   if (stale) batch_drop_graphs(b);

@@ -225,6 +225,42 @@ struct AlchConst {
   int active, inter, intra;
 };
 
+// One electrostatics evaluation of the lambda scheme (ParticleMeshEwald condensedEnergy /
+// condensedNoLigandSCF / ligandElec, PME:1609-1796): which parts run, their scales, the
+// softcore shift of pairs with a soft atom and the lambda derivatives to accumulate.
+// The default is the plain evaluation.
+struct ElecStep {
+  int lam;                 // accumulate dU/dL, d2U/dL2, dU/dX dL
+  int doPermReal;          // permanent real space
+  int doPol;               // polarization
+  double permScale;        // reciprocal/self permanent scale; real-space scale of soft pairs
+  double polScale;
+  double dEdLSign;
+  double beta, dlAlpha, d2lAlpha;               // softcore shift and its lambda derivatives
+  double dlPowPerm, d2lPowPerm, dlPowPol, d2lPowPol;
+};
+inline ElecStep plain_step() { return ElecStep{0, 1, 1, 1.0, 1.0, 1.0, 0, 0, 0, 0, 0, 0, 0}; }
+
+// Electrostatic lambda keys and their values at lambda (AlchemicalParameters,
+// pme/AlchemicalParameters.java:60-190, update :306-380).
+struct ElecAlchemy {
+  bool on = false;
+  double permAlpha = 2.0, permExp = 3.0, permStart = 0.4, permEnd = 1.0;
+  double polStart = 0.75, polEnd = 1.0, polExp = 3.0;
+  bool vaporElec = true, noLigandSCF = true;
+  double lAlpha = 0, dlAlpha = 0, d2lAlpha = 0;
+  double lPowPerm = 1, dlPowPerm = 0, d2lPowPerm = 0;
+  double lPowPol = 1, dlPowPol = 0, d2lPowPol = 0;
+};
+
+// Host copy of the system inputs (kept to build sub-systems, e.g. the vacuum ligand).
+struct SystemCopy {
+  int n = 0, n_vdw_types = 0;
+  std::vector<double> xyz, multipole, polarizability, thole, pdamp, red_factor, vdw_inv_rmin, vdw_eps;
+  std::vector<int> frame, axis, vdw_type, red_parent;
+  std::vector<std::vector<int>> m12, m13, m14, m15, ip11;
+};
+
 struct Handle {
   // ---- configuration
   int n = 0;
@@ -321,7 +357,7 @@ struct Handle {
   // ---- outputs
   double *d_grad = nullptr, *d_torque = nullptr;  // [3][n]
   double *d_gred = nullptr;                        // [3][n] vdW reduced-site force
-  double *d_eatom = nullptr;                       // [8][n] per-atom energy terms
+  double *d_eatom = nullptr;                       // [kEnergyRows][n] per-atom energy terms
   long long *d_catom = nullptr;                    // [2][n] per-atom counts
   double *d_result = nullptr;                      // reduced terms
   long long *d_cresult = nullptr;
@@ -339,6 +375,23 @@ struct Handle {
   double *d_lgred = nullptr;                       // [6][n]: reduced-site and distributed dU/dX dL
   double dEdL = 0.0, d2EdL2 = 0.0;
   bool lgrad_valid = false;
+  // Electrostatic lambda (elec-lambdaterm): keys, the current step, the lambda gradient and
+  // torque of the electrostatics, per-step accumulators, the polarizabilities with the soft
+  // atoms removed, the charge corrections of the whole and soft-free systems, and the
+  // vacuum sub-system of the soft atoms (lig[j] = its atom j in this system).
+  ElecAlchemy elec;
+  ElecStep step = plain_step();
+  double *d_lg = nullptr, *d_lt = nullptr;          // [3][n] each
+  double *d_acc = nullptr;                          // [3+3+8+3+3][n] step accumulators
+  double *d_polar_all = nullptr, *d_polar_env = nullptr;
+  double e_corr_env = 0.0;
+  Handle *vac = nullptr;
+  std::vector<int> lig;
+  int *d_lig = nullptr;
+  bool vacuum = false;                              // this handle is a vacuum sub-system
+  int eps_atoms = 0;                                // atom count of the PCG residual norm (0: n);
+                                                    // a sub-system uses its parent's (PCGSolver.java:546)
+  SystemCopy sys;
   // Molecular dynamics state (md.cu): masses, SETTLE molecules and the trajectory arrays
   // (interleaved [n][3]): positions, velocities, accelerations, prior positions, gradient.
   bool md_ready = false;
@@ -369,6 +422,14 @@ struct Handle {
   int64_t list_builds = 0;
 };
 
+// Ewald coefficient of the evaluation: 0 for a vacuum sub-system (no screening).
+inline double ewald_alpha_of(const Handle &h) { return h.vacuum ? 0.0 : h.prm.ewald_alpha; }
+
+// Rows of Handle::d_eatom: vdW, permanent real, polarization real, permanent self,
+// permanent reciprocal, polarization self, polarization reciprocal, vdW dU/dL, vdW d2U/dL2,
+// electrostatic dU/dL, electrostatic d2U/dL2.
+constexpr int kEnergyRows = 11;
+
 // ---- kernels / launchers (defined in the .cu files)
 void launch_set_coordinates(Handle &h, const double *d_xyz);
 void launch_neighbor_list(Handle &h, bool force);
@@ -394,6 +455,11 @@ int md_run(Handle &h, double dt, int steps, double *xyz, double *vel, double *ep
 void launch_recip_energy(Handle &h, bool grad);
 void launch_real_energy(Handle &h, bool grad);
 void launch_torque(Handle &h);
+void launch_torque_of(Handle &h, const double *torque, double *out);
+void launch_elec_accumulate(Handle &h, bool first);
+void launch_elec_restore(Handle &h);
+void launch_lambda_grad_add(Handle &h, double *out);
+void launch_zero_soft_multipoles(Handle &h);
 void launch_assemble(Handle &h, double *d_grad_xyz);
 void launch_reduce_results(Handle &h);
 void setup_pme(Handle &h);

@@ -24,6 +24,30 @@ using namespace ffx;
 
 static std::string g_create_error;
 
+// Gathers and scatters between a system and its vacuum sub-system (lig[j] = atom j's index).
+__global__ void k_gather_xyz(int m, const int *__restrict__ idx, const double *__restrict__ src, double *dst) {
+  const int j = blockIdx.x * blockDim.x + threadIdx.x;
+  if (j >= m) return;
+  const int i = idx[j];
+  for (int d = 0; d < 3; d++) dst[3 * j + d] = src[3 * i + d];
+}
+
+__global__ void k_scatter_add_xyz(int m, const int *__restrict__ idx, const double *__restrict__ src, double *dst) {
+  const int j = blockIdx.x * blockDim.x + threadIdx.x;
+  if (j >= m) return;
+  const int i = idx[j];
+  for (int d = 0; d < 3; d++) dst[3 * i + d] += src[3 * j + d];
+}
+
+__global__ void k_scatter_add_soa(int m, int n, const int *__restrict__ idx, const double *__restrict__ src,
+                                  double *dst) {
+  const int j = blockIdx.x * blockDim.x + threadIdx.x;
+  if (j >= m) return;
+  const int i = idx[j];
+  for (int d = 0; d < 3; d++) dst[(size_t)d * n + i] += src[(size_t)d * m + j];
+}
+
+
 #define CK(call)                                                                    \
   do {                                                                              \
     cudaError_t e_ = (call);                                                        \
@@ -98,11 +122,46 @@ static void configure_images(Handle &h) {
   }
 }
 
+// Host copy of the inputs (sub-systems are built from it).
+static void copy_system(const ffxg_system *s, SystemCopy &c) {
+  const int n = s->n_atoms;
+  c.n = n;
+  c.n_vdw_types = s->n_vdw_types;
+  c.xyz.assign(s->xyz, s->xyz + 3 * (size_t)n);
+  c.multipole.assign(s->multipole, s->multipole + 10 * (size_t)n);
+  c.frame.assign(s->frame, s->frame + n);
+  c.axis.assign(s->axis, s->axis + 3 * (size_t)n);
+  c.polarizability.assign(s->polarizability, s->polarizability + n);
+  c.thole.assign(s->thole, s->thole + n);
+  c.pdamp.assign(s->pdamp, s->pdamp + n);
+  c.vdw_type.assign(s->vdw_type, s->vdw_type + n);
+  c.red_parent.assign(s->red_parent, s->red_parent + n);
+  c.red_factor.assign(s->red_factor, s->red_factor + n);
+  const size_t t2 = (size_t)s->n_vdw_types * s->n_vdw_types;
+  c.vdw_inv_rmin.assign(s->vdw_inv_rmin, s->vdw_inv_rmin + t2);
+  c.vdw_eps.assign(s->vdw_eps, s->vdw_eps + t2);
+  auto csr = [&](const int32_t *ptr, const int32_t *idx, std::vector<std::vector<int>> &out) {
+    out.assign(n, {});
+    if (!ptr) return;
+    for (int i = 0; i < n; i++) out[i].assign(idx + ptr[i], idx + ptr[i + 1]);
+  };
+  csr(s->mask12_ptr, s->mask12_idx, c.m12);
+  csr(s->mask13_ptr, s->mask13_idx, c.m13);
+  csr(s->mask14_ptr, s->mask14_idx, c.m14);
+  csr(s->mask15_ptr, s->mask15_idx, c.m15);
+  csr(s->ip11_ptr, s->ip11_idx, c.ip11);
+}
+
 static int create_impl(const ffxg_system *s, const ffxg_params *p, Handle &h) {
   const int n = s->n_atoms;
   h.n = n;
   h.prm = *p;
   if (n <= 0) { h.err = "n_atoms must be positive"; return FFXG_ERR_BAD_ARG; }
+  if (!s->xyz || !s->multipole || !s->frame || !s->axis || !s->polarizability || !s->thole || !s->pdamp ||
+      !s->vdw_type || !s->red_parent || !s->red_factor || !s->vdw_inv_rmin || !s->vdw_eps) {
+    h.err = "null per-atom array"; return FFXG_ERR_BAD_ARG;
+  }
+  copy_system(s, h.sys);
   if (p->pme_order != kOrder) { h.err = "only pme-order 5 is supported"; return FFXG_ERR_BAD_ARG; }
   for (int d = 0; d < 3; d++) {
     if (!(p->box[d] > 0.0)) { h.err = "box edges must be positive"; return FFXG_ERR_BAD_ARG; }
@@ -282,7 +341,8 @@ static int create_impl(const ffxg_system *s, const ffxg_params *p, Handle &h) {
     CK(dalloc(&h.d_twiddlef, 3 * (size_t)std::max(nfx, std::max(nfy, nfz))));
   }
   CK(dalloc(&h.d_grad, 3 * N)); CK(dalloc(&h.d_torque, 3 * N)); CK(dalloc(&h.d_gred, 6 * N));
-  CK(dalloc(&h.d_eatom, 10 * N)); CK(dalloc(&h.d_catom, 2 * N));
+  CK(dalloc(&h.d_eatom, (size_t)kEnergyRows * N)); CK(dalloc(&h.d_catom, 2 * N));
+  CK(cudaMemset(h.d_eatom, 0, (size_t)kEnergyRows * N * sizeof(double)));
   CK(dalloc(&h.d_result, 16)); CK(dalloc(&h.d_cresult, 8));
   CK(dalloc(&h.d_flags, 1));
   CK(cudaMallocHost((void **)&h.h_flags, 64));
@@ -346,7 +406,19 @@ static int create_impl(const ffxg_system *s, const ffxg_params *p, Handle &h) {
   return FFXG_OK;
 }
 
+static void free_all(Handle &h);
+
+static void drop_vacuum(Handle &h) {
+  if (h.vac) {
+    free_all(*h.vac);
+    delete h.vac;
+    h.vac = nullptr;
+  }
+}
+
 static void free_all(Handle &h) {
+  drop_vacuum(h);
+  if (h.d_polar_all) h.d_polar = h.d_polar_all;   // the step-2 swap never outlives a call
   void *ptrs[] = {h.d_lmp, h.d_frame, h.d_axis, h.d_polar, h.d_thole, h.d_ipdamp, h.d_vtype, h.d_redp, h.d_redf,
                   h.d_vrad, h.d_veps, h.d_excl_ptr, h.d_excl_k, h.d_excl_code, h.d_excl_lo, h.d_excl_hi, h.d_tq_ptr,
                   h.d_tq_ent, h.d_red_ptr, h.d_red_child, h.d_x, h.d_y, h.d_z, h.d_rx, h.d_ry, h.d_rz, h.d_refx,
@@ -356,7 +428,7 @@ static void free_all(Handle &h) {
                   h.d_uP, h.d_udirD, h.d_udirP, h.d_r, h.d_rP, h.d_zpre, h.d_zpreP, h.d_p, h.d_pP, h.d_vec, h.d_vecP,
                   h.d_partials, h.d_scalars, h.d_grid, h.d_influence, h.d_twiddle, h.d_gridf, h.d_influencef, h.d_twiddlef, h.d_grad, h.d_torque, h.d_gred,
                   h.d_eatom, h.d_catom, h.d_result, h.d_cresult, h.d_flags, h.d_xyz_in, h.d_grad_out,
-                  h.d_coefE, h.d_coefP, h.d_coefEB, h.d_coefPB, h.d_part2, h.d_counter, h.d_pos, h.d_recF, h.d_recP, h.d_tpair, h.d_tp, h.d_soft, h.d_mol, h.d_lgred, h.d_mass, h.d_mdx, h.d_mdv, h.d_mda, h.d_mdxp, h.d_mdg, h.d_mdke, h.d_settle, h.d_aspc, h.d_aspc_state, h.d_nbr_sh, h.d_ewl_sh};
+                  h.d_coefE, h.d_coefP, h.d_coefEB, h.d_coefPB, h.d_part2, h.d_counter, h.d_pos, h.d_recF, h.d_recP, h.d_tpair, h.d_tp, h.d_soft, h.d_mol, h.d_lgred, h.d_mass, h.d_mdx, h.d_mdv, h.d_mda, h.d_mdxp, h.d_mdg, h.d_mdke, h.d_settle, h.d_aspc, h.d_aspc_state, h.d_nbr_sh, h.d_ewl_sh, h.d_lg, h.d_lt, h.d_acc, h.d_polar_env, h.d_lig};
   for (void *q : ptrs)
     if (q) cudaFree(q);
   if (h.h_scalars) cudaFreeHost(h.h_scalars);
@@ -427,9 +499,13 @@ static void emit_back(Handle &h, double *d_grad_xyz) {
     launch_torque(h);
     launch_assemble(h, d_grad_xyz);
   }
+  if (h.step.lam) {   // electrostatic lambda gradient into the dU/dX dL rows (after the vdW part)
+    if (h.vacuum) cudaMemsetAsync(h.d_lgred + 3 * (size_t)h.n, 0, 3 * (size_t)h.n * sizeof(double), h.stream);
+    launch_lambda_grad_add(h, h.d_lgred + 3 * (size_t)h.n);
+  }
   launch_reduce_results(h);
   timer_end(h, tk);
-  cudaMemcpyAsync(h.h_scalars, h.d_result, 9 * sizeof(double), cudaMemcpyDeviceToHost, h.stream);
+  cudaMemcpyAsync(h.h_scalars, h.d_result, kEnergyRows * sizeof(double), cudaMemcpyDeviceToHost, h.stream);
   cudaMemcpyAsync(h.h_flags + 2, h.d_cresult, 2 * sizeof(long long), cudaMemcpyDeviceToHost, h.stream);
   cudaMemcpyAsync(h.h_flags, h.d_flags, sizeof(int), cudaMemcpyDeviceToHost, h.stream);
 }
@@ -442,14 +518,23 @@ static const char *scf_message(int st) {
 
 // Terms and counts from the pinned copies written by emit_back.
 static int finish(Handle &h, bool rebuilt, double *terms, int64_t *counts) {
-  double res[9];
+  double res[kEnergyRows];
   long long cres[2];
-  std::memcpy(res, h.h_scalars, 9 * sizeof(double));
-  h.dEdL = res[7];
-  h.d2EdL2 = res[8];
-  h.lgrad_valid = h.alch.active && h.want_grad;
+  std::memcpy(res, h.h_scalars, kEnergyRows * sizeof(double));
+  h.dEdL = res[7] + res[9];
+  h.d2EdL2 = res[8] + res[10];
+  h.lgrad_valid = (h.alch.active && h.want_grad) || h.step.lam;
   std::memcpy(cres, h.h_flags + 2, 2 * sizeof(long long));
-  const double eCorr = h.e_charge_correction;
+  double eCorr = h.vacuum ? 0.0 : h.e_charge_correction;
+  if (h.step.lam && !h.vacuum) {
+    // Charge corrections of the whole system (step 1, x lPowPerm) and of the system without
+    // the soft atoms (step 2, x (1 - lPowPerm)); ReciprocalEnergyRegion.java:230-255.
+    const ElecAlchemy &el = h.elec;
+    const double ca = h.e_charge_correction, ce = h.e_corr_env;
+    eCorr = el.lPowPerm * ca + (1.0 - el.lPowPerm) * ce;
+    h.dEdL += el.dlPowPerm * ca - el.dlPowPerm * ce;
+    h.d2EdL2 += el.d2lPowPerm * ca - el.d2lPowPerm * ce;
+  }
   if (terms) {
     terms[FFXG_TERM_VDW] = res[0];
     terms[FFXG_TERM_PERM_REAL] = res[1];
@@ -511,7 +596,7 @@ static int evaluate_direct(Handle &h, const double *d_xyz, double *d_grad_xyz, d
     h.list_valid = true;
     int st = FFXG_OK;
     h.scf_iter = 0;
-    if (h.prm.polarization != FFXG_POLAR_NONE) {
+    if (h.prm.polarization != FFXG_POLAR_NONE && h.step.doPol) {
       if (h.prm.polarization == FFXG_POLAR_MUTUAL) st = run_pcg(h, false);
       if (st == FFXG_OK) emit_final_induced(h);
     } else {
@@ -634,8 +719,172 @@ int eval_after_graph(Handle &h, double *terms, int64_t *counts) {
 // One evaluation on device-resident coordinates.  The graph path is used once the
 // neighbour list exists (its first build and any regrowth run directly) and when stage
 // timing is off.
+// Electrostatic lambda (elec-lambdaterm, OST; ParticleMeshEwald.energy, PME:897-935) as
+// direct launches: (1) every atom, softcore permanent real space, reciprocal and
+// polarization scaled (condensedEnergy, :1609-1640); (2) without the soft atoms -- their
+// multipoles and polarizabilities zeroed, which removes them exactly as use[] does --
+// reciprocal permanent and polarization by the complements (condensedNoLigandSCF,
+// :1650-1700); (3) the soft atoms alone in vacuum by the sub-system (ligandElec,
+// :1704-1796).  The steps' results are summed before the torques become forces.
+static int evaluate_elec(Handle &h, const double *d_xyz, double *d_grad_xyz, double *terms, int64_t *counts) {
+  const ElecAlchemy &el = h.elec;
+  const double L = h.lambda;
+  const bool mutual = h.prm.polarization == FFXG_POLAR_MUTUAL;
+  const bool anyPol = h.prm.polarization != FFXG_POLAR_NONE;
+  h.want_grad = true;
+  for (int attempt = 0; attempt < 4; attempt++) {
+    h.ev_stage.clear();
+    h.ev_used = 0;
+    h.step = plain_step();
+    h.step.lam = 1;
+    h.step.permScale = el.lPowPerm;
+    h.step.dEdLSign = 1.0;
+    h.step.beta = el.lAlpha; h.step.dlAlpha = el.dlAlpha; h.step.d2lAlpha = el.d2lAlpha;
+    h.step.dlPowPerm = el.dlPowPerm; h.step.d2lPowPerm = el.d2lPowPerm;
+    h.step.dlPowPol = el.dlPowPol; h.step.d2lPowPol = el.d2lPowPol;
+    if (L < el.polStart) { h.step.doPol = 0; h.step.polScale = 0.0; }
+    else if (L <= el.polEnd) { h.step.doPol = 1; h.step.polScale = el.lPowPol; }
+    else { h.step.doPol = 1; h.step.polScale = 1.0; }
+    emit_front(h, d_xyz);
+    cudaMemcpyAsync(h.h_flags, h.d_flags, sizeof(int), cudaMemcpyDeviceToHost, h.stream);
+    if (cudaStreamSynchronize(h.stream) != cudaSuccess) {
+      h.err = std::string("CUDA error: ") + cudaGetErrorString(cudaGetLastError());
+      h.step = plain_step();
+      return FFXG_ERR_CUDA;
+    }
+    const int f = h.h_flags[0];
+    if (f & FLAG_NONFINITE) { h.err = "non-finite coordinates"; h.step = plain_step(); return FFXG_ERR_NONFINITE; }
+    if (f & FLAG_IMAGE_RANGE) { h.err = "atoms more than 500 box edges apart"; h.step = plain_step(); return FFXG_ERR_BAD_ARG; }
+    if (f & kOverflow) {
+      if (int a = grow_lists(h, f)) { h.step = plain_step(); return a; }
+      continue;
+    }
+    const bool rebuilt = (f & FLAG_REBUILD) != 0;
+    if (rebuilt) h.list_builds++;
+    h.list_valid = true;
+    int st = FFXG_OK, iters = 0;
+    // 1.
+    if (anyPol && h.step.doPol) {
+      if (mutual) st = run_pcg(h, false);
+      iters += h.scf_iter;
+      if (st == FFXG_OK) emit_final_induced(h);
+    } else {
+      emit_no_polarization(h);
+    }
+    if (st != FFXG_OK) { h.err = scf_message(st); h.step = plain_step(); return st; }
+    launch_real_energy(h, true);
+    launch_recip_energy(h, true);
+    launch_elec_accumulate(h, true);
+    // 2.
+    bool any_env = false;
+    for (int i = 0; i < h.n && !any_env; i++) any_env = !std::binary_search(h.lig.begin(), h.lig.end(), i);
+    if (any_env) {
+      h.step.doPermReal = 0;
+      h.step.permScale = 1.0 - el.lPowPerm;
+      h.step.dEdLSign = -1.0;
+      h.step.beta = h.step.dlAlpha = h.step.d2lAlpha = 0.0;
+      if (L <= el.polEnd && el.noLigandSCF) { h.step.doPol = 1; h.step.polScale = 1.0 - el.lPowPol; }
+      else { h.step.doPol = 0; h.step.polScale = 0.0; }
+      launch_zero_soft_multipoles(h);
+      h.d_polar = h.d_polar_env;
+      launch_spread_permanent(h);
+      launch_fft_convolution(h);
+      launch_phi_permanent(h);
+      launch_realspace_field(h);
+      h.scf_iter = 0;
+      if (anyPol && h.step.doPol) {
+        if (mutual) st = run_pcg(h, false);
+        iters += h.scf_iter;
+        if (st == FFXG_OK) emit_final_induced(h);
+      } else {
+        emit_no_polarization(h);
+      }
+      if (st == FFXG_OK) {
+        launch_real_energy(h, true);
+        launch_recip_energy(h, true);
+        launch_elec_accumulate(h, false);
+      }
+      h.d_polar = h.d_polar_all;
+      if (st != FFXG_OK) { h.err = scf_message(st); h.step = plain_step(); return st; }
+    }
+    launch_elec_restore(h);
+    // Torques to forces, vdW, the lambda gradient, sums (the reductions of emit_back).
+    launch_torque(h);
+    launch_assemble(h, d_grad_xyz);
+    launch_lambda_grad_add(h, h.d_lgred + 3 * (size_t)h.n);
+    launch_reduce_results(h);
+    cudaMemcpyAsync(h.h_scalars, h.d_result, kEnergyRows * sizeof(double), cudaMemcpyDeviceToHost, h.stream);
+    cudaMemcpyAsync(h.h_flags + 2, h.d_cresult, 2 * sizeof(long long), cudaMemcpyDeviceToHost, h.stream);
+    cudaMemcpyAsync(h.h_flags, h.d_flags, sizeof(int), cudaMemcpyDeviceToHost, h.stream);
+    if (cudaStreamSynchronize(h.stream) != cudaSuccess) {
+      h.err = std::string("CUDA error: ") + cudaGetErrorString(cudaGetLastError());
+      h.step = plain_step();
+      return FFXG_ERR_CUDA;
+    }
+    h.scf_iter = iters;
+    st = finish(h, rebuilt, terms, counts);
+    if (st != FFXG_OK) { h.step = plain_step(); return st; }
+    // 3.
+    if (el.vaporElec && h.vac) {
+      Handle &v = *h.vac;
+      const int m = v.n;
+      v.lambda = h.lambda;
+      v.step = plain_step();
+      v.step.lam = 1;
+      v.step.permScale = 1.0 - el.lPowPerm;
+      v.step.dEdLSign = -1.0;
+      v.step.dlPowPerm = el.dlPowPerm; v.step.d2lPowPerm = el.d2lPowPerm;
+      v.step.dlPowPol = el.dlPowPol; v.step.d2lPowPol = el.d2lPowPol;
+      if (L <= el.polEnd) { v.step.doPol = 1; v.step.polScale = 1.0 - el.lPowPol; }
+      else { v.step.doPol = 0; v.step.polScale = 0.0; }
+      k_gather_xyz<<<nblocks(m, 128), 128, 0, h.stream>>>(m, h.d_lig, d_xyz, v.d_xyz_in);
+      FFX_LAUNCHED(h);
+      if (cudaStreamSynchronize(h.stream) != cudaSuccess) {
+        h.err = std::string("CUDA error: ") + cudaGetErrorString(cudaGetLastError());
+        h.step = plain_step();
+        return FFXG_ERR_CUDA;
+      }
+      double vt[FFXG_N_TERMS];
+      int64_t vc[FFXG_N_COUNTS];
+      v.want_grad = true;
+      st = evaluate_direct(v, v.d_xyz_in, v.d_grad_out, vt, vc);
+      if (st != FFXG_OK) { h.err = "vacuum step: " + v.err; h.step = plain_step(); return st; }
+      k_scatter_add_xyz<<<nblocks(m, 128), 128, 0, h.stream>>>(m, h.d_lig, v.d_grad_out, d_grad_xyz);
+      k_scatter_add_soa<<<nblocks(m, 128), 128, 0, h.stream>>>(m, h.n, h.d_lig, v.d_lgred + 3 * (size_t)m,
+                                                                h.d_lgred + 3 * (size_t)h.n);
+      h.launches += 2;
+      if (cudaStreamSynchronize(h.stream) != cudaSuccess) {
+        h.err = std::string("CUDA error: ") + cudaGetErrorString(cudaGetLastError());
+        h.step = plain_step();
+        return FFXG_ERR_CUDA;
+      }
+      h.dEdL += v.dEdL;
+      h.d2EdL2 += v.d2EdL2;
+      h.scf_iter += v.scf_iter;
+      if (terms) {
+        terms[FFXG_TERM_PERM_REAL] += vt[FFXG_TERM_PERM_REAL];
+        terms[FFXG_TERM_POL_REAL] += vt[FFXG_TERM_POL_REAL];
+        terms[FFXG_TERM_PERMANENT] += vt[FFXG_TERM_PERMANENT];
+        terms[FFXG_TERM_POLARIZATION] += vt[FFXG_TERM_POLARIZATION];
+        terms[FFXG_TERM_TOTAL] += vt[FFXG_TERM_PERMANENT] + vt[FFXG_TERM_POLARIZATION];
+      }
+      if (counts) counts[FFXG_COUNT_SCF_ITER] = h.scf_iter;
+    }
+    h.lgrad_valid = true;
+    h.step = plain_step();
+    return FFXG_OK;
+  }
+  h.step = plain_step();
+  h.err = "neighbour capacity could not be satisfied";
+  return FFXG_ERR_CAPACITY;
+}
+
 namespace ffx {
 int evaluate(Handle &h, const double *d_xyz, double *d_grad_xyz, bool grad, double *terms, int64_t *counts) {
+  if (h.elec.on && h.alch.active && !h.vacuum) {
+    h.launches = 0;
+    return evaluate_elec(h, d_xyz, d_grad_xyz, terms, counts);
+  }
   h.launches = 0;
   h.want_grad = grad;
   if (h.use_graphs && h.list_valid && !h.timing) {
@@ -799,7 +1048,153 @@ static void update_alchemy(Handle &h) {
   h.alch.sc2 = std::pow(l, ex);
   h.alch.dsc2dL = ex * std::pow(l, ex - 1.0);
   h.alch.d2sc2dL2 = (ex >= 2.0) ? ex * (ex - 1.0) * std::pow(l, ex - 2.0) : 0.0;
+  // Electrostatics: AlchemicalParameters.update (pme/AlchemicalParameters.java:306-380).
+  ElecAlchemy &el = h.elec;
+  const double L = h.lambda;
+  el.lPowPerm = 1.0; el.dlPowPerm = 0.0; el.d2lPowPerm = 0.0;
+  el.lAlpha = 0.0; el.dlAlpha = 0.0; el.d2lAlpha = 0.0;
+  if (L < el.permStart) {
+    el.lPowPerm = 0.0;
+  } else if (L <= el.permEnd) {
+    const double sc = 1.0 / (el.permEnd - el.permStart);
+    const double pl = sc * (L - el.permStart);
+    el.lAlpha = el.permAlpha * (1.0 - pl) * (1.0 - pl);
+    el.dlAlpha = el.permAlpha * (1.0 - pl) * sc;
+    el.d2lAlpha = -el.permAlpha * sc * sc;
+    el.lPowPerm = std::pow(pl, el.permExp);
+    el.dlPowPerm = el.permExp * std::pow(pl, el.permExp - 1.0) * sc;
+    el.d2lPowPerm = (el.permExp >= 2.0) ? el.permExp * (el.permExp - 1.0) * std::pow(pl, el.permExp - 2.0) * sc * sc : 0.0;
+  }
+  el.lPowPol = 1.0; el.dlPowPol = 0.0; el.d2lPowPol = 0.0;
+  if (L < el.polStart) {
+    el.lPowPol = 0.0;
+  } else if (L <= el.polEnd) {
+    const double sc = 1.0 / (el.polEnd - el.polStart);
+    const double pl = sc * (L - el.polStart);
+    if (el.polExp > 0.0) {
+      el.lPowPol = std::pow(pl, el.polExp);
+      if (el.polExp >= 1.0) {
+        el.dlPowPol = el.polExp * std::pow(pl, el.polExp - 1.0);
+        if (el.polExp >= 2.0) el.d2lPowPol = el.polExp * (el.polExp - 1.0) * std::pow(pl, el.polExp - 2.0);
+      }
+    }
+    el.dlPowPol *= sc;
+    el.d2lPowPol *= sc * sc;
+  }
   drop_graphs(h);   // the captured vdW launch holds the constants
+}
+
+// ---------------------------------------------------------------------------
+// Vacuum sub-system of the soft atoms (ligandElec, PME:1704-1796): their multipoles,
+// polarizabilities, frames and masks, an all-pairs list without images, Ewald alpha 0
+// and no reciprocal space.
+static int build_vacuum(Handle &h, const std::vector<int> &soft, const std::vector<int> &mol) {
+  drop_vacuum(h);
+  const SystemCopy &c = h.sys;
+  std::vector<int> map(h.n, -1);
+  h.lig.clear();
+  for (int i = 0; i < h.n; i++)
+    if (soft[i]) { map[i] = (int)h.lig.size(); h.lig.push_back(i); }
+  const int m = (int)h.lig.size();
+  if (m == 0) return FFXG_OK;
+  std::vector<double> xyz(3 * (size_t)m), mp(10 * (size_t)m), pol(m), th(m), pd(m), rf(m);
+  std::vector<int> fr(m), ax(3 * (size_t)m, -1), vt(m), rp(m), vmol(m);
+  for (int j = 0; j < m; j++) {
+    const int i = h.lig[j];
+    for (int d = 0; d < 3; d++) xyz[3 * j + d] = c.xyz[3 * (size_t)i + d];
+    for (int t = 0; t < 10; t++) mp[10 * j + t] = c.multipole[10 * (size_t)i + t];
+    pol[j] = c.polarizability[i]; th[j] = c.thole[i]; pd[j] = c.pdamp[i];
+    fr[j] = c.frame[i];
+    for (int a = 0; a < 3; a++) {
+      const int k = c.axis[3 * (size_t)i + a];
+      if (k >= 0 && map[k] < 0) { h.err = "a frame-defining atom of a soft atom is not soft"; return FFXG_ERR_BAD_ARG; }
+      ax[3 * j + a] = k >= 0 ? map[k] : -1;
+    }
+    vt[j] = c.vdw_type[i];
+    rp[j] = map[c.red_parent[i]] >= 0 ? map[c.red_parent[i]] : j;
+    rf[j] = map[c.red_parent[i]] >= 0 ? c.red_factor[i] : 0.0;
+    vmol[j] = mol[i];
+  }
+  auto sub_csr = [&](const std::vector<std::vector<int>> &L, std::vector<int> &ptr, std::vector<int> &idx) {
+    ptr.assign(m + 1, 0);
+    idx.clear();
+    for (int j = 0; j < m; j++) {
+      for (int k : L[h.lig[j]])
+        if (map[k] >= 0) idx.push_back(map[k]);
+      ptr[j + 1] = (int)idx.size();
+    }
+  };
+  std::vector<int> p12, i12, p13, i13, p14, i14, p15, i15, p11, i11;
+  sub_csr(c.m12, p12, i12); sub_csr(c.m13, p13, i13); sub_csr(c.m14, p14, i14); sub_csr(c.m15, p15, i15);
+  sub_csr(c.ip11, p11, i11);
+  ffxg_system sub{};
+  sub.n_atoms = m; sub.xyz = xyz.data(); sub.multipole = mp.data(); sub.frame = fr.data(); sub.axis = ax.data();
+  sub.polarizability = pol.data(); sub.thole = th.data(); sub.pdamp = pd.data(); sub.vdw_type = vt.data();
+  sub.red_parent = rp.data(); sub.red_factor = rf.data(); sub.n_vdw_types = c.n_vdw_types;
+  sub.vdw_inv_rmin = c.vdw_inv_rmin.data(); sub.vdw_eps = c.vdw_eps.data();
+  sub.mask12_ptr = p12.data(); sub.mask12_idx = i12.data(); sub.mask13_ptr = p13.data(); sub.mask13_idx = i13.data();
+  sub.mask14_ptr = p14.data(); sub.mask14_idx = i14.data(); sub.mask15_ptr = p15.data(); sub.mask15_idx = i15.data();
+  sub.ip11_ptr = p11.data(); sub.ip11_idx = i11.data();
+  ffxg_params prm = h.prm;
+  prm.pme_grid[0] = prm.pme_grid[1] = prm.pme_grid[2] = 8;   // unused: no reciprocal space
+  Handle *v = new Handle();
+  int st = create_impl(&sub, &prm, *v);
+  if (st != FFXG_OK) { h.err = "vacuum sub-system: " + v->err; free_all(*v); delete v; return st; }
+  v->vacuum = true;
+  v->use_graphs = false;
+  v->eps_atoms = h.n;
+  v->images = true;
+  v->cap_nbr = v->cap_ewl = v->cap_prl = round32(m);
+  Handle &vh = *v;
+  auto fail = [&](int code) { h.err = "vacuum sub-system: " + vh.err; free_all(vh); delete v; return code; };
+  if ((st = alloc_lists(vh)) != FFXG_OK) return fail(st);
+  const size_t M = m;
+  std::vector<int> ones(M, 1);
+#define VK(call) do { if ((call) != cudaSuccess) { vh.err = #call; return fail(FFXG_ERR_CUDA); } } while (0)
+  VK(dalloc(&vh.d_soft, M)); VK(dalloc(&vh.d_mol, M)); VK(dalloc(&vh.d_lgred, 6 * M));
+  VK(dalloc(&vh.d_lg, 3 * M)); VK(dalloc(&vh.d_lt, 3 * M));
+  VK(cudaMemcpy(vh.d_soft, ones.data(), M * sizeof(int), cudaMemcpyHostToDevice));
+  VK(cudaMemcpy(vh.d_mol, vmol.data(), M * sizeof(int), cudaMemcpyHostToDevice));
+  VK(cudaMemset(vh.d_lgred, 0, 6 * M * sizeof(double)));
+  // No reciprocal space or vdW: the mesh, potentials, their energy rows and the vdW
+  // gradient stay zero.
+  const size_t ng = (size_t)vh.nfft[0] * vh.nfft[1] * vh.nfft[2];
+  VK(cudaMemset(vh.d_grid, 0, ng * sizeof(double2)));
+  if (vh.d_gridf) VK(cudaMemset(vh.d_gridf, 0, ng * sizeof(float2)));
+  for (double *q : {vh.d_cphi, vh.d_fphi, vh.d_cphiI, vh.d_fphiI, vh.d_cphiP, vh.d_fphiP})
+    VK(cudaMemset(q, 0, 20 * M * sizeof(double)));
+  VK(cudaMemset(vh.d_eatom, 0, (size_t)kEnergyRows * M * sizeof(double)));
+  VK(cudaMemset(vh.d_gred, 0, 6 * M * sizeof(double)));
+#undef VK
+  vh.alch = h.alch;
+  vh.alch.active = 0;   // the vdW softcore stays with the full system
+  CK(dalloc(&h.d_lig, M));
+  CK(cudaMemcpy(h.d_lig, h.lig.data(), M * sizeof(int), cudaMemcpyHostToDevice));
+  h.vac = v;
+  return FFXG_OK;
+}
+
+// Electrostatic lambda state: lambda arrays, step accumulators, the polarizabilities
+// without the soft atoms, the charge correction without them, the vacuum sub-system.
+static int setup_elec(Handle &h, const std::vector<int> &soft, const std::vector<int> &mol) {
+  const size_t N = h.n;
+  if (!h.d_lg) {
+    CK(dalloc(&h.d_lg, 3 * N)); CK(dalloc(&h.d_lt, 3 * N));
+    CK(dalloc(&h.d_acc, 20 * N)); CK(dalloc(&h.d_polar_env, N));
+    h.d_polar_all = h.d_polar;
+  }
+  std::vector<double> pe(N);
+  double q = 0.0;
+  for (size_t i = 0; i < N; i++) {
+    pe[i] = soft[i] ? 0.0 : h.sys.polarizability[i];
+    if (!soft[i]) q += h.sys.multipole[10 * i];
+  }
+  CK(cudaMemcpy(h.d_polar_env, pe.data(), N * sizeof(double), cudaMemcpyHostToDevice));
+  // ReciprocalEnergyRegion.java:228-238 for the atoms in use.
+  h.e_corr_env = 0.0;
+  if (q != 0.0) h.e_corr_env = -0.5 * h.prm.electric * 3.14159265358979323846 * q * q /
+                               (h.box.volume * h.prm.ewald_alpha * h.prm.ewald_alpha);
+  return build_vacuum(h, soft, mol);
 }
 
 int ffxg_set_alchemy(ffxg_handle *hh, const ffxg_alchemy *a) {
@@ -807,8 +1202,21 @@ int ffxg_set_alchemy(ffxg_handle *hh, const ffxg_alchemy *a) {
   Handle &h = hh->h;
   if (!a) {
     h.alch.active = 0;
+    h.elec.on = false;
+    drop_vacuum(h);
+    CK(cudaMemset(h.d_eatom + 9 * (size_t)h.n, 0, 2 * (size_t)h.n * sizeof(double)));
     update_alchemy(h);
     return FFXG_OK;
+  }
+  if (a->elec && (!(a->permanent_lambda_alpha >= 0.0) || !(a->permanent_lambda_exponent >= 0.0) ||
+                  !(a->permanent_lambda_start >= 0.0 && a->permanent_lambda_start <= 1.0) ||
+                  !(a->permanent_lambda_end >= a->permanent_lambda_start && a->permanent_lambda_end <= 1.0) ||
+                  !(a->polarization_lambda_start >= 0.0 && a->polarization_lambda_start <= 1.0) ||
+                  !(a->polarization_lambda_end >= a->polarization_lambda_start &&
+                    a->polarization_lambda_end <= 1.0) ||
+                  !(a->polarization_lambda_exponent >= 0.0))) {
+    h.err = "alchemy: electrostatic lambda windows must lie in [0, 1] with start <= end; alpha, exponents >= 0";
+    return FFXG_ERR_BAD_ARG;
   }
   if (!a->soft || !(a->vdw_lambda_alpha >= 0.0) || !(a->vdw_lambda_exponent >= 1.0) ||
       !(a->vdw_lambda_end > 0.0 && a->vdw_lambda_end <= 1.0)) {
@@ -834,6 +1242,20 @@ int ffxg_set_alchemy(ffxg_handle *hh, const ffxg_alchemy *a) {
   h.alch.inter = a->intermolecular_softcore != 0;
   h.alch.intra = a->intramolecular_softcore != 0;
   h.alch.active = 1;
+  ElecAlchemy &el = h.elec;
+  el.on = a->elec != 0;
+  if (el.on) {
+    el.permAlpha = a->permanent_lambda_alpha; el.permExp = a->permanent_lambda_exponent;
+    el.permStart = a->permanent_lambda_start; el.permEnd = a->permanent_lambda_end;
+    el.polStart = a->polarization_lambda_start; el.polEnd = a->polarization_lambda_end;
+    el.polExp = a->polarization_lambda_exponent;
+    el.vaporElec = a->ligand_vapor_elec != 0;
+    el.noLigandSCF = a->no_ligand_condensed_scf != 0;
+    if (int st = setup_elec(h, soft, mol)) { el.on = false; return st; }
+  } else {
+    drop_vacuum(h);
+    CK(cudaMemset(h.d_eatom + 9 * (size_t)h.n, 0, 2 * (size_t)h.n * sizeof(double)));
+  }
   update_alchemy(h);
   return FFXG_OK;
 }

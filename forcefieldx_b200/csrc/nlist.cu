@@ -261,6 +261,40 @@ __global__ void k_verlet_images(int n, const double *__restrict__ rx, const doub
   }
 }
 
+// Vacuum sub-system: every pair (k != i), no images, the shift field zero and marked
+// minimum image; pairs dropped by the vapor softcore options (intermolecular: different
+// molecules; intramolecular: the same molecule; PermanentFieldRegion.java:665-670).
+__global__ void k_vacuum_pairs(int n, const int *__restrict__ mol, int inter, int intra, int cap, int *nbr,
+                               int *nbr_sh, int *nbr_cnt, int *flags) {
+  if (!(*flags & FLAG_REBUILD)) return;
+  const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const int lane = threadIdx.x & 31;
+  if (warp >= n) return;
+  const int i = warp;
+  int count = 0;
+  for (int base = 0; base < n; base += 32) {
+    const int k = base + lane;
+    bool pass = k < n && k != i;
+    if (pass) {
+      const bool same = mol[k] == mol[i];
+      if ((inter && !same) || (intra && same)) pass = false;
+    }
+    const unsigned m = __ballot_sync(0xffffffffu, pass);
+    if (pass) {
+      const int pos = count + __popc(m & ((1u << lane) - 1u));
+      if (pos < cap) {
+        nbr[(size_t)i * cap + pos] = k;
+        nbr_sh[(size_t)i * cap + pos] = pack_shift(0, 0, 0, true);
+      }
+    }
+    count += __popc(m);
+  }
+  if (lane == 0) {
+    nbr_cnt[i] = count;
+    if (count > cap) atomicOr(flags, FLAG_NBR_OVERFLOW);
+  }
+}
+
 __global__ void k_list_done(int n, double *refx, double *refy, double *refz, const double *__restrict__ rx,
                             const double *__restrict__ ry, const double *__restrict__ rz, const int *flags) {
   if (!(*flags & FLAG_REBUILD)) return;
@@ -304,6 +338,15 @@ void launch_neighbor_list(Handle &h, bool force) {
     cudaStreamSynchronize(h.stream);
   }
   const double rl = fmax(h.prm.vdw_cutoff, h.prm.ewald_cutoff) + h.prm.list_buffer;
+  if (h.vacuum) {
+    k_vacuum_pairs<<<nblocks((int64_t)n * 32, 256), 256, 0, h.stream>>>(n, h.d_mol, h.alch.inter, h.alch.intra,
+                                                                        h.cap_nbr, h.d_nbr, h.d_nbr_sh, h.d_nbr_cnt,
+                                                                        h.d_flags);
+    k_list_done<<<nblocks(n, 256), 256, 0, h.stream>>>(n, h.d_refx, h.d_refy, h.d_refz, h.d_rx, h.d_ry, h.d_rz,
+                                                        h.d_flags);
+    h.launches += 2;
+    return;
+  }
   if (h.images) {
     k_verlet_images<<<nblocks((int64_t)n * 32, 256), 256, 0, h.stream>>>(
         n, h.d_rx, h.d_ry, h.d_rz, h.box, h.img_range[0], h.img_range[1], h.img_range[2], rl * rl, h.cap_nbr,

@@ -388,7 +388,7 @@ __global__ void __launch_bounds__(kVecThreads) k_pcg_update(
     int n, const double *__restrict__ vec, const double *__restrict__ vecP, const double *__restrict__ p,
     const double *__restrict__ pP, double *r, double *rP, double *uD, double *uP, const double *__restrict__ tot,
     double *partE, unsigned *counter, PcgState *st, int max_iter, double polar_eps, const int *flags,
-    cudaGraphConditionalHandle cond, int use_cond, const double *__restrict__ polar, T *recP) {
+    cudaGraphConditionalHandle cond, int use_cond, const double *__restrict__ polar, T *recP, int n_eps) {
   const double pap = tot[T_PAP], papP = tot[T_PAPP], rz = tot[T_RZ], rzP = tot[T_RZP];
   const double alpha0 = (pap != 0.0) ? rz / pap : rz;
   const double alpha1 = (papP != 0.0) ? rzP / papP : rzP;
@@ -415,7 +415,7 @@ __global__ void __launch_bounds__(kVecThreads) k_pcg_update(
   if (block_partials<2>(v, partE, counter, norms, 0) && threadIdx.x == 0) {
     const double e0 = norms[0], e1 = norms[1];
     const double m = (e0 < e1) ? e1 : e0;
-    const double eps = kElecAngToDebye * sqrt(m / (double)n);
+    const double eps = kElecAngToDebye * sqrt(m / (double)n_eps);
     const double previous = st->eps;
     const int iter = st->iter + 1;
     int status = FFXG_OK, cont = 1;
@@ -502,7 +502,7 @@ static void aspc_save(Handle &h) {
 }
 
 static double aewald3_of(const Handle &h) {
-  const double a = h.prm.ewald_alpha;
+  const double a = ewald_alpha_of(h);
   return 4.0 / 3.0 * pow(a, 3.0) / 1.7724538509055160273;
 }
 
@@ -587,7 +587,7 @@ static void update(Handle &h, cudaGraphConditionalHandle cond, int use_cond) {
   k_pcg_update<T><<<vec_blocks(h.n), kVecThreads, 0, h.stream>>>(
       h.n, h.d_vec, h.d_vecP, h.d_p, h.d_pP, h.d_r, h.d_rP, h.d_uD, h.d_uP, h.d_scalars, part_region(h, 2),
       h.d_counter + K_UPDATE, h.d_pcg, h.prm.max_scf_iter, h.prm.polar_eps, h.d_flags, cond, use_cond, h.d_polar,
-      reinterpret_cast<T *>(h.d_recP));
+      reinterpret_cast<T *>(h.d_recP), h.eps_atoms > 0 ? h.eps_atoms : h.n);
   FFX_LAUNCHED(h);
 }
 

@@ -836,6 +836,7 @@ static size_t grid_points(const Handle &h) { return (size_t)h.nfft[0] * h.nfft[1
 // Both forms accumulate into the double mesh d_grid (cleared first); the mixed form's
 // FFT continues in the FP32 mesh d_gridf.
 void launch_spread_permanent(Handle &h) {
+  if (h.vacuum) return;   // no reciprocal space: the mesh and potentials stay zero
   const int nb = nblocks((int64_t)h.n * 32, 256);
   cudaMemsetAsync(h.d_grid, 0, grid_points(h) * sizeof(double2), h.stream);
   if (h.mixed)
@@ -848,6 +849,7 @@ void launch_spread_permanent(Handle &h) {
 }
 
 void launch_spread_induced(Handle &h, const double *ud, const double *up) {
+  if (h.vacuum) return;   // no reciprocal space: the mesh and potentials stay zero
   const int nb = nblocks((int64_t)h.n * 32, 256);
   cudaMemsetAsync(h.d_grid, 0, grid_points(h) * sizeof(double2), h.stream);
   if (h.mixed)
@@ -900,6 +902,7 @@ static void fft_convolution(Handle &h, typename Vec2<S>::type *grid, const typen
 }
 
 void launch_fft_convolution(Handle &h) {
+  if (h.vacuum) return;   // no reciprocal space: the mesh and potentials stay zero
   if (h.mixed)
     fft_convolution<float>(h, h.d_gridf, h.d_twiddlef, h.d_influencef);
   else
@@ -920,10 +923,12 @@ static void phi(Handle &h, int which) {
 }
 
 void launch_phi_permanent(Handle &h) {
+  if (h.vacuum) return;   // no reciprocal space: the mesh and potentials stay zero
   if (h.mixed) phi<float>(h, 0); else phi<double>(h, 0);
 }
 
 void launch_phi_induced(Handle &h) {
+  if (h.vacuum) return;   // no reciprocal space: the mesh and potentials stay zero
   if (h.mixed) phi<float>(h, 1); else phi<double>(h, 1);
 }
 

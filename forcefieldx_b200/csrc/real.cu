@@ -224,13 +224,18 @@ __global__ void __launch_bounds__(128) k_realspace_field(
 
 // ---------------------------------------------------------------------------
 // Permanent and polarization real-space energy, i-side force and torque.
-template <typename R>
+// LAM: the electrostatic lambda variant (RealSpaceEnergyRegion.java:873-883, 1190-1690,
+// 2153-2176): pairs with a soft atom take r^2 + beta and the scale permScale in the
+// permanent part, the polarization part is scaled by polScale, and dU/dL, d2U/dL2, the
+// lambda gradient and torque are gathered (written to edl/ed2l/lgrad/ltorque).
+template <typename R, bool LAM>
 __global__ void __launch_bounds__(128) k_real_energy(
     int n, const double *__restrict__ x, const double *__restrict__ y, const double *__restrict__ z, Box bx,
     const double *__restrict__ gm, const double *__restrict__ uD, const double *__restrict__ uP,
     const double *__restrict__ ipdamp, const double *__restrict__ thole, const int *__restrict__ ewl,
     const int *__restrict__ ewl_cnt, int capE, const int *__restrict__ ewl_sh, Excl ex, EwaldCoef ec, ScaleTables c_scales, int polarization, int gradient,
-    double *eatom_perm, double *eatom_pol, long long *catom, double *grad, double *torque) {
+    double *eatom_perm, double *eatom_pol, long long *catom, double *grad, double *torque,
+    const int *__restrict__ soft, ElecStep st, double *edl, double *ed2l, double *lgrad, double *ltorque) {
   const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const int lane = threadIdx.x & 31;
   if (warp >= n) return;
@@ -244,11 +249,17 @@ __global__ void __launch_bounds__(128) k_real_energy(
   const R pix = uP[i], piy = uP[n + i], piz = uP[2 * n + i];
   const R pdi = ipdamp[i], pti = thole[i];
   const R aewald = ec.aewald, an0 = ec.an0, an1 = ec.an1, an2 = ec.an2, an3 = ec.an3, an4 = ec.an4;
+  const R an5 = ec.an5;
   const R electric = ec.electric;
-  const bool doPol = polarization != FFXG_POLAR_NONE;
+  const bool doPol = polarization != FFXG_POLAR_NONE && (!LAM || st.doPol);
+  const bool doPerm = !LAM || st.doPermReal;
+  const bool gr = gradient || LAM;
   double eP = 0, eI = 0;
   long long cnt_pairs = 0;
   R gx = 0, gy = 0, gz = 0, tx = 0, ty = 0, tz = 0;
+  double dl = 0, d2l = 0;
+  R lgx = 0, lgy = 0, lgz = 0, ltx = 0, lty = 0, ltz = 0;
+  const int soft_i = LAM ? soft[i] : 0;
   const int cnt = min(ewl_cnt[i], capE);
   const int *row = ewl + (size_t)i * capE;
   for (int a = lane; a < cnt; a += 32) {
@@ -267,7 +278,14 @@ __global__ void __launch_bounds__(128) k_real_energy(
     const R scale = c_scales.m[code & 7u];
     const R scalep = c_scales.p[(code >> 3) & 7u];
     const R scaled = c_scales.d[(code >> 6) & 1u];
-    const R r = m_sqrt(r2);
+    bool spair = false;
+    R l2 = R(1.0);
+    double r2s = r2d;
+    if (LAM) {
+      spair = soft_i || soft[k];
+      if (spair && st.doPermReal) { r2s = r2d + st.beta; l2 = (R)st.permScale; }
+    }
+    const R r = m_sqrt(LAM ? (R)r2s : r2);
     const R ralpha = aewald * r;
     const R exp2a = m_exp(-ralpha * ralpha);
     const R rr1 = R(1.0) / r, rr2 = rr1 * rr1;
@@ -281,6 +299,7 @@ __global__ void __launch_bounds__(128) k_real_energy(
     const R rr9 = R(7.0) * rr7 * rr2, rr11 = R(9.0) * rr9 * rr2;
     R scale3 = R(1.0), scale5 = R(1.0), scale7 = R(1.0);
     R ddsc3x = 0, ddsc3y = 0, ddsc3z = 0, ddsc5x = 0, ddsc5y = 0, ddsc5z = 0, ddsc7x = 0, ddsc7y = 0, ddsc7z = 0;
+    (void)an5;
     R damp = pdi * ipdamp[k];
     const R tho = m_min(pti, thole[k]);
     const R rdamp = r * damp;
@@ -298,7 +317,7 @@ __global__ void __launch_bounds__(128) k_real_energy(
       ddsc7x = temp7 * ddsc5x; ddsc7y = temp7 * ddsc5y; ddsc7z = temp7 * ddsc5z;
     }
     // ---- permanentPair
-    {
+    if (doPerm) {
       const R dixdkx = diy * dkz - diz * dky, dixdky = diz * dkx - dix * dkz, dixdkz = dix * dky - diy * dkx;
       const R dixrx = diy * zr - diz * yr, dixry = diz * xr - dix * zr, dixrz = dix * yr - diy * xr;
       const R dkxrx = dky * zr - dkz * yr, dkxry = dkz * xr - dkx * zr, dkxrz = dkx * yr - dky * xr;
@@ -348,8 +367,8 @@ __global__ void __launch_bounds__(128) k_real_energy(
       const R ereal = gl0 * bn0 + (gl1 + gl6) * bn1 + (gl2 + gl7 + gl8) * bn2 + (gl3 + gl5) * bn3 + gl4 * bn4;
       const R efix = scale1 * (gl0 * rr1 + (gl1 + gl6) * rr3 + (gl2 + gl7 + gl8) * rr5 + (gl3 + gl5) * rr7 + gl4 * rr9);
       const R e = ereal - efix;
-      if (e != R(0.0)) { eP += R(0.5) * e; if (pair_counted(i, k, ewl_sh, ent)) cnt_pairs++; }
-      if (gradient) {
+      if (e != R(0.0)) { eP += R(0.5) * (LAM ? l2 * e : e); if (pair_counted(i, k, ewl_sh, ent)) cnt_pairs++; }
+      if (gr) {
         const R gf1 = bn1 * gl0 + bn2 * (gl1 + gl6) + bn3 * (gl2 + gl7 + gl8) + bn4 * (gl3 + gl5) + bn5 * gl4;
         const R gf2 = -ck * bn1 + sc4 * bn2 - sc6 * bn3;
         const R gf3 = ci * bn1 + sc3 * bn2 + sc5 * bn3;
@@ -387,9 +406,65 @@ __global__ void __launch_bounds__(128) k_real_energy(
           ttm2x -= scale1 * ttm2rx; ttm2y -= scale1 * ttm2ry; ttm2z -= scale1 * ttm2rz;
           ttm3x -= scale1 * ttm3rx; ttm3y -= scale1 * ttm3ry; ttm3z -= scale1 * ttm3rz;
         }
-        const R pre = electric;
+        const R pre = LAM ? electric * l2 : electric;
         gx += pre * ftm2x; gy += pre * ftm2y; gz += pre * ftm2z;
         tx += pre * ttm2x; ty += pre * ttm2y; tz += pre * ttm2z;
+        if (LAM && spair) {   // d[dlPow * ereal]/dX (:1465-1475)
+          const R pf = electric * (R)(st.dEdLSign * st.dlPowPerm);
+          lgx += pf * ftm2x; lgy += pf * ftm2y; lgz += pf * ftm2z;
+          ltx += pf * ttm2x; lty += pf * ttm2y; ltz += pf * ttm2z;
+        }
+      }
+      if (LAM && spair) {
+        // dU/dL, d2U/dL2 through the scale and the softcore shift; dU/dL/dX of the second
+        // term, every radial order one higher (:1477-1690).  Half weight per direction.
+        const R bn6 = (R(11.0) * bn5 + an5 * exp2a) * rr2;
+        const R rr13 = R(11.0) * rr11 * rr2;
+        const R dRealdL = gl0 * bn1 + (gl1 + gl6) * bn2 + (gl2 + gl7 + gl8) * bn3 + (gl3 + gl5) * bn4 + gl4 * bn5;
+        const R d2RealdL2 = gl0 * bn2 + (gl1 + gl6) * bn3 + (gl2 + gl7 + gl8) * bn4 + (gl3 + gl5) * bn5 + gl4 * bn6;
+        R dFixdL = gl0 * rr3 + (gl1 + gl6) * rr5 + (gl2 + gl7 + gl8) * rr7 + (gl3 + gl5) * rr9 + gl4 * rr11;
+        R d2FixdL2 = gl0 * rr5 + (gl1 + gl6) * rr7 + (gl2 + gl7 + gl8) * rr9 + (gl3 + gl5) * rr11 + gl4 * rr13;
+        dFixdL *= scale1;
+        d2FixdL2 *= scale1;
+        const double sg = st.dEdLSign, dP = st.dlPowPerm, d2P = st.d2lPowPerm, dA = st.dlAlpha, d2A = st.d2lAlpha;
+        const double L2 = (double)l2;
+        dl += 0.5 * (sg * dP * (double)ereal + L2 * dA * (double)dRealdL);
+        d2l += 0.5 * (sg * (d2P * (double)ereal + 2.0 * dP * dA * (double)dRealdL) + L2 * d2A * (double)dRealdL +
+                      L2 * dA * dA * (double)d2RealdL2);
+        dl -= 0.5 * (sg * dP * (double)efix + L2 * dA * (double)dFixdL);
+        d2l -= 0.5 * (sg * (d2P * (double)efix + 2.0 * dP * dA * (double)dFixdL) + L2 * d2A * (double)dFixdL +
+                      L2 * dA * dA * (double)d2FixdL2);
+        const R gf1 = bn2 * gl0 + bn3 * (gl1 + gl6) + bn4 * (gl2 + gl7 + gl8) + bn5 * (gl3 + gl5) + bn6 * gl4;
+        const R gf2 = -ck * bn2 + sc4 * bn3 - sc6 * bn4;
+        const R gf3 = ci * bn2 + sc3 * bn3 + sc5 * bn4;
+        const R gf4 = R(2.0) * bn3;
+        const R gf5 = R(2.0) * (-ck * bn3 + sc4 * bn4 - sc6 * bn5);
+        const R gf6 = R(2.0) * (-ci * bn3 - sc3 * bn4 - sc5 * bn5);
+        const R gf7 = R(4.0) * bn4;
+        R fx = gf1 * xr + gf2 * dix + gf3 * dkx + gf4 * (qkdix - qidkx) + gf5 * qirx + gf6 * qkrx + gf7 * (qiqkrx + qkqirx);
+        R fy = gf1 * yr + gf2 * diy + gf3 * dky + gf4 * (qkdiy - qidky) + gf5 * qiry + gf6 * qkry + gf7 * (qiqkry + qkqiry);
+        R fz = gf1 * zr + gf2 * diz + gf3 * dkz + gf4 * (qkdiz - qidkz) + gf5 * qirz + gf6 * qkrz + gf7 * (qiqkrz + qkqirz);
+        R qx = -bn2 * dixdkx + gf2 * dixrx + gf4 * (dixqkrx + dkxqirx + rxqidkx - R(2.0) * qixqkx) - gf5 * rxqirx - gf7 * (rxqikrx + qkrxqirx);
+        R qy = -bn2 * dixdky + gf2 * dixry + gf4 * (dixqkry + dkxqiry + rxqidky - R(2.0) * qixqky) - gf5 * rxqiry - gf7 * (rxqikry + qkrxqiry);
+        R qz = -bn2 * dixdkz + gf2 * dixrz + gf4 * (dixqkrz + dkxqirz + rxqidkz - R(2.0) * qixqkz) - gf5 * rxqirz - gf7 * (rxqikrz + qkrxqirz);
+        if (scale1 != R(0.0)) {
+          const R gfr1 = rr5 * gl0 + rr7 * (gl1 + gl6) + rr9 * (gl2 + gl7 + gl8) + rr11 * (gl3 + gl5) + rr13 * gl4;
+          const R gfr2 = -ck * rr5 + sc4 * rr7 - sc6 * rr9;
+          const R gfr3 = ci * rr5 + sc3 * rr7 + sc5 * rr9;
+          const R gfr4 = R(2.0) * rr7;
+          const R gfr5 = R(2.0) * (-ck * rr7 + sc4 * rr9 - sc6 * rr11);
+          const R gfr6 = R(2.0) * (-ci * rr7 - sc3 * rr9 - sc5 * rr11);
+          const R gfr7 = R(4.0) * rr9;
+          fx -= scale1 * (gfr1 * xr + gfr2 * dix + gfr3 * dkx + gfr4 * (qkdix - qidkx) + gfr5 * qirx + gfr6 * qkrx + gfr7 * (qiqkrx + qkqirx));
+          fy -= scale1 * (gfr1 * yr + gfr2 * diy + gfr3 * dky + gfr4 * (qkdiy - qidky) + gfr5 * qiry + gfr6 * qkry + gfr7 * (qiqkry + qkqiry));
+          fz -= scale1 * (gfr1 * zr + gfr2 * diz + gfr3 * dkz + gfr4 * (qkdiz - qidkz) + gfr5 * qirz + gfr6 * qkrz + gfr7 * (qiqkrz + qkqirz));
+          qx -= scale1 * (-rr5 * dixdkx + gfr2 * dixrx + gfr4 * (dixqkrx + dkxqirx + rxqidkx - R(2.0) * qixqkx) - gfr5 * rxqirx - gfr7 * (rxqikrx + qkrxqirx));
+          qy -= scale1 * (-rr5 * dixdky + gfr2 * dixry + gfr4 * (dixqkry + dkxqiry + rxqidky - R(2.0) * qixqky) - gfr5 * rxqiry - gfr7 * (rxqikry + qkrxqiry));
+          qz -= scale1 * (-rr5 * dixdkz + gfr2 * dixrz + gfr4 * (dixqkrz + dkxqirz + rxqidkz - R(2.0) * qixqkz) - gfr5 * rxqirz - gfr7 * (rxqikrz + qkrxqirz));
+        }
+        const R pf = electric * l2 * (R)st.dlAlpha;
+        lgx += pf * fx; lgy += pf * fy; lgz += pf * fz;
+        ltx += pf * qx; lty += pf * qy; ltz += pf * qz;
       }
     }
     if (!doPol) continue;
@@ -453,8 +528,13 @@ __global__ void __launch_bounds__(128) k_real_energy(
       const R glip6 = scip1, glip7 = R(2.0) * (scip7 - scip8);
       const R ereal = (gli1 + gli6) * bn1 + (gli2 + gli7) * bn2 + gli3 * bn3;
       const R efix = (gli1 + gli6) * rr3 * psc3 + (gli2 + gli7) * rr5 * psc5 + gli3 * rr7 * psc7;
-      eI += R(0.25) * (ereal - efix);
-      if (!gradient) continue;
+      const R epol = R(0.25) * (ereal - efix);
+      eI += LAM ? (R)st.polScale * epol : epol;
+      if (LAM) {
+        dl += st.dEdLSign * st.dlPowPol * (double)epol;
+        d2l += st.dEdLSign * st.d2lPowPol * (double)epol;
+      }
+      if (!gr) continue;
       const bool dorli = (psc3 != R(0.0) || dsc3 != R(0.0) || usc3 != R(0.0));
       const R gfi1 = R(0.5) * bn2 * (gli1 + glip1 + gli6 + glip6) + R(0.5) * bn2 * scip2 +
                           R(0.5) * bn3 * (gli2 + glip2 + gli7 + glip7) - R(0.5) * bn3 * (sci3 * scip4 + scip3 * sci4) +
@@ -547,9 +627,14 @@ __global__ void __launch_bounds__(128) k_real_energy(
       ftm2ix -= ftm2rix; ftm2iy -= ftm2riy; ftm2iz -= ftm2riz;
       ttm2ix -= ttm2rix; ttm2iy -= ttm2riy; ttm2iz -= ttm2riz;
       ttm3ix -= ttm3rix; ttm3iy -= ttm3riy; ttm3iz -= ttm3riz;
-      const R sc = electric;
+      const R sc = LAM ? electric * (R)st.polScale : electric;
       gx += sc * ftm2ix; gy += sc * ftm2iy; gz += sc * ftm2iz;
       tx += sc * ttm2ix; ty += sc * ttm2iy; tz += sc * ttm2iz;
+      if (LAM) {   // RealSpaceEnergyRegion.java:2163-2174
+        const R sl = electric * (R)(st.dEdLSign * st.dlPowPol);
+        lgx += sl * ftm2ix; lgy += sl * ftm2iy; lgz += sl * ftm2iz;
+        ltx += sl * ttm2ix; lty += sl * ttm2iy; ltz += sl * ttm2iz;
+      }
     }
 
   }
@@ -558,13 +643,25 @@ __global__ void __launch_bounds__(128) k_real_energy(
   const double Tx = warp_sum((double)tx), Ty = warp_sum((double)ty), Tz = warp_sum((double)tz);
 #pragma unroll
   for (int o = 16; o > 0; o >>= 1) cnt_pairs += __shfl_xor_sync(0xffffffffu, cnt_pairs, o);
+  double L[8];
+  if (LAM) {
+    L[0] = warp_sum(dl); L[1] = warp_sum(d2l);
+    L[2] = warp_sum((double)lgx); L[3] = warp_sum((double)lgy); L[4] = warp_sum((double)lgz);
+    L[5] = warp_sum((double)ltx); L[6] = warp_sum((double)lty); L[7] = warp_sum((double)ltz);
+  }
   if (lane == 0) {
     eatom_perm[i] = eP * ec.electric;
     eatom_pol[i] = eI * ec.electric;
     catom[i] = cnt_pairs;
-    if (gradient) {
+    if (gr) {
       grad[i] = Gx; grad[n + i] = Gy; grad[2 * n + i] = Gz;
       torque[i] = Tx; torque[n + i] = Ty; torque[2 * n + i] = Tz;
+    }
+    if (LAM) {
+      edl[i] = L[0] * ec.electric;
+      ed2l[i] = L[1] * ec.electric;
+      lgrad[i] = L[2]; lgrad[n + i] = L[3]; lgrad[2 * n + i] = L[4];
+      ltorque[i] = L[5]; ltorque[n + i] = L[6]; ltorque[2 * n + i] = L[7];
     }
   }
 }
@@ -595,14 +692,14 @@ static Excl excl(const Handle &h) {
 template <typename R>
 static void realspace_field(Handle &h) {
   using V2 = typename Vec2<R>::type;
-  const double off2 = h.prm.ewald_cutoff * h.prm.ewald_cutoff;
+  const double off2 = h.vacuum ? INFINITY : h.prm.ewald_cutoff * h.prm.ewald_cutoff;
   k_realspace_field<R><<<nblocks((int64_t)h.n * 32, 128), 128, 0, h.stream>>>(
       h.n, h.d_x, h.d_y, h.d_z, h.box, h.d_gm, h.d_ipdamp, h.d_thole, h.d_nbr, h.d_nbr_cnt, h.cap_nbr,
       h.d_nbr_sh, off2, h.prm.precond_cutoff, h.d_ewl, h.d_ewl_cnt, h.cap_ewl, h.d_ewl_sh, h.d_prl, h.d_prl_cnt,
       h.cap_prl,
       reinterpret_cast<PairRec<R> *>(h.d_coefE), reinterpret_cast<R *>(h.d_coefEB),
       reinterpret_cast<PairRec<R> *>(h.d_coefP), reinterpret_cast<R *>(h.d_coefPB), excl(h),
-      ewald_coef(h, h.prm.ewald_alpha), h.scales, h.d_cphi, h.d_polar, h.prm.polarization != FFXG_POLAR_NONE ? 1 : 0,
+      ewald_coef(h, ewald_alpha_of(h)), h.scales, h.d_cphi, h.d_polar, h.prm.polarization != FFXG_POLAR_NONE ? 1 : 0,
       h.d_fieldD, h.d_fieldP, h.d_uD, h.d_uP, h.d_udirD, h.d_udirP, reinterpret_cast<R *>(h.d_recF), h.d_flags);
   FFX_LAUNCHED(h);
 }
@@ -618,10 +715,12 @@ void launch_realspace_field(Handle &h) {
 
 template <typename R>
 static void real_energy(Handle &h, bool grad) {
-  k_real_energy<R><<<nblocks((int64_t)h.n * 32, 128), 128, 0, h.stream>>>(
+  auto kern = h.step.lam ? k_real_energy<R, true> : k_real_energy<R, false>;
+  kern<<<nblocks((int64_t)h.n * 32, 128), 128, 0, h.stream>>>(
       h.n, h.d_x, h.d_y, h.d_z, h.box, h.d_gm, h.d_uD, h.d_uP, h.d_ipdamp, h.d_thole, h.d_ewl, h.d_ewl_cnt,
-      h.cap_ewl, h.d_ewl_sh, excl(h), ewald_coef(h, h.prm.ewald_alpha), h.scales, h.prm.polarization, grad ? 1 : 0,
-      h.d_eatom + 1 * (size_t)h.n, h.d_eatom + 2 * (size_t)h.n, h.d_catom + (size_t)h.n, h.d_grad, h.d_torque);
+      h.cap_ewl, h.d_ewl_sh, excl(h), ewald_coef(h, ewald_alpha_of(h)), h.scales, h.prm.polarization, grad ? 1 : 0,
+      h.d_eatom + 1 * (size_t)h.n, h.d_eatom + 2 * (size_t)h.n, h.d_catom + (size_t)h.n, h.d_grad, h.d_torque,
+      h.d_soft, h.step, h.d_eatom + 9 * (size_t)h.n, h.d_eatom + 10 * (size_t)h.n, h.d_lg, h.d_lt);
   FFX_LAUNCHED(h);
 }
 

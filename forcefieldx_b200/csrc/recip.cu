@@ -28,7 +28,8 @@ __global__ void k_recip_energy(int n, const double *__restrict__ gm, const doubl
                                const double *__restrict__ uD, const double *__restrict__ uP,
                                const double *__restrict__ cphiI, const double *__restrict__ cphiP,
                                const double *__restrict__ fphiI, const double *__restrict__ fphiP, RecipCoef rc,
-                               PmeConst pc, int gradient, double *eatom, double *grad, double *torque) {
+                               PmeConst pc, int gradient, double *eatom, double *grad, double *torque, ElecStep st,
+                               double *lgrad, double *ltorque) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
   double mp[10], f[10];
@@ -45,8 +46,12 @@ __global__ void k_recip_energy(int n, const double *__restrict__ gm, const doubl
   const double e = mp[t000] * ph[t000] + mp[t100] * ph[t100] + mp[t010] * ph[t010] + mp[t001] * ph[t001] +
                    (1.0 / 3.0) * (mp[t200] * ph[t200] + mp[t020] * ph[t020] + mp[t002] * ph[t002] +
                                   2.0 * (mp[t110] * ph[t110] + mp[t101] * ph[t101] + mp[t011] * ph[t011]));
-  eatom[3 * (size_t)n + i] = eSelf;
-  eatom[4 * (size_t)n + i] = 0.5 * rc.electric * e;
+  // Lambda scheme (ReciprocalEnergyRegion.java:230-255, 385-530, 545-740): permanent parts x
+  // permScale, induced parts x polScale; dU/dL takes dEdLSign * dlPow * the unscaled parts.
+  const double sP = st.permScale, sI = st.polScale;
+  const double eRecip = 0.5 * rc.electric * e;
+  eatom[3 * (size_t)n + i] = sP * eSelf;
+  eatom[4 * (size_t)n + i] = sP * eRecip;
   double gx = 0, gy = 0, gz = 0, tqx = 0, tqy = 0, tqz = 0;
   if (gradient) {
     double fp[20];
@@ -76,6 +81,8 @@ __global__ void k_recip_energy(int n, const double *__restrict__ gm, const doubl
                          mp[t020] * ph[t110] - mp[t011] * ph[t101]);
     tqx = rc.electric * tx; tqy = rc.electric * ty; tqz = rc.electric * tz;
   }
+  const double gPx = gx, gPy = gy, gPz = gz, tPx = tqx, tPy = tqy, tPz = tqz;
+  gx = gy = gz = tqx = tqy = tqz = 0.0;
   double eSelfI = 0.0, eRecipI = 0.0;
   if (rc.polarization != FFXG_POLAR_NONE) {
     const double u0 = uD[i], u1 = uD[n + i], u2 = uD[2 * n + i];
@@ -141,11 +148,20 @@ __global__ void k_recip_energy(int n, const double *__restrict__ gm, const doubl
       tqx += rc.electric * tx; tqy += rc.electric * ty; tqz += rc.electric * tz;
     }
   }
-  eatom[5 * (size_t)n + i] = eSelfI;
-  eatom[6 * (size_t)n + i] = eRecipI;
+  eatom[5 * (size_t)n + i] = sI * eSelfI;
+  eatom[6 * (size_t)n + i] = sI * eRecipI;
   if (gradient) {
-    grad[i] += gx; grad[n + i] += gy; grad[2 * n + i] += gz;
-    torque[i] += tqx; torque[n + i] += tqy; torque[2 * n + i] += tqz;
+    grad[i] += sP * gPx + sI * gx; grad[n + i] += sP * gPy + sI * gy; grad[2 * n + i] += sP * gPz + sI * gz;
+    torque[i] += sP * tPx + sI * tqx; torque[n + i] += sP * tPy + sI * tqy; torque[2 * n + i] += sP * tPz + sI * tqz;
+  }
+  if (st.lam) {   // adds to the rows and arrays k_real_energy<R, true> wrote
+    const double lP = st.dEdLSign * st.dlPowPerm, l2P = st.dEdLSign * st.d2lPowPerm;
+    const double lI = st.dEdLSign * st.dlPowPol, l2I = st.dEdLSign * st.d2lPowPol;
+    eatom[9 * (size_t)n + i] += lP * (eSelf + eRecip) + lI * (eSelfI + eRecipI);
+    eatom[10 * (size_t)n + i] += l2P * (eSelf + eRecip) + l2I * (eSelfI + eRecipI);
+    lgrad[i] += lP * gPx + lI * gx; lgrad[n + i] += lP * gPy + lI * gy; lgrad[2 * n + i] += lP * gPz + lI * gz;
+    ltorque[i] += lP * tPx + lI * tqx; ltorque[n + i] += lP * tPy + lI * tqy;
+    ltorque[2 * n + i] += lP * tPz + lI * tqz;
   }
 }
 
@@ -301,7 +317,7 @@ __global__ void k_assemble(int n, const double *__restrict__ grad, const double 
 
 // Two-level deterministic sums: blocks reduce contiguous chunks in a fixed order.
 constexpr int kSumBlocks = 148;
-constexpr int kNE = 9, kNC = 2;   // energy rows: vdW, perm real, pol real, 4 recip/self, dU/dL, d2U/dL2
+constexpr int kNE = kEnergyRows, kNC = 2;   // energy rows (kEnergyRows), count rows
 
 __global__ void k_sum_partial(int n, const double *__restrict__ eatom, const long long *__restrict__ catom,
                               double *pe, long long *pc) {
@@ -357,23 +373,100 @@ void launch_recip_energy(Handle &h, bool grad) {
   rc.aw3 = -2.0 / 3.0 * rc.electric * a * a * a / SQRT_PI;
   rc.aw4 = -2.0 * rc.aw3;
   rc.nf[0] = h.nfft[0]; rc.nf[1] = h.nfft[1]; rc.nf[2] = h.nfft[2];
-  rc.polarization = h.prm.polarization;
+  rc.polarization = h.step.doPol ? h.prm.polarization : FFXG_POLAR_NONE;
+  if (h.vacuum) return;   // no reciprocal space and no Ewald self terms (alpha 0)
   k_recip_energy<<<nblocks(h.n, 128), 128, 0, h.stream>>>(h.n, h.d_gm, h.d_fm, h.d_cphi, h.d_fphi, h.d_uD, h.d_uP,
                                                            h.d_cphiI, h.d_cphiP, h.d_fphiI, h.d_fphiP, rc, h.pc,
-                                                           grad ? 1 : 0, h.d_eatom, h.d_grad, h.d_torque);
+                                                           (grad || h.step.lam) ? 1 : 0, h.d_eatom, h.d_grad, h.d_torque,
+                                                           h.step, h.d_lg, h.d_lt);
   FFX_LAUNCHED(h);
 }
 
-void launch_torque(Handle &h) {
-  // The torque-derived gradient reuses the induced-field scratch rows of d_vec.
-  k_torque_gather<<<nblocks(h.n, 128), 128, 0, h.stream>>>(h.n, h.d_x, h.d_y, h.d_z, h.d_frame, h.d_axis, h.d_torque,
-                                                            h.d_tq_ptr, h.d_tq_ent, h.d_vec, h.d_flags);
+void launch_torque(Handle &h) { launch_torque_of(h, h.d_torque, h.d_vec); }
+
+// Torque -> Cartesian gradient of `torque` into out[3][n] (written, not added).
+void launch_torque_of(Handle &h, const double *torque, double *out) {
+  k_torque_gather<<<nblocks(h.n, 128), 128, 0, h.stream>>>(h.n, h.d_x, h.d_y, h.d_z, h.d_frame, h.d_axis, torque,
+                                                            h.d_tq_ptr, h.d_tq_ent, out, h.d_flags);
   FFX_LAUNCHED(h);
 }
 
 void launch_assemble(Handle &h, double *d_grad_xyz) {
   k_assemble<<<nblocks(h.n, 256), 256, 0, h.stream>>>(h.n, h.d_grad, h.d_vec, h.d_gred + 3 * (size_t)h.n, d_grad_xyz,
                                                        h.d_flags);
+  FFX_LAUNCHED(h);
+}
+
+// ---------------------------------------------------------------------------
+// Electrostatic lambda: the steps' results summed in d_acc, rows [0,3) gradient, [3,6)
+// torque, [6,14) energy rows 1-6, 9, 10, [14,17) lambda gradient, [17,20) lambda torque.
+__device__ __constant__ int kAccRows[8] = {1, 2, 3, 4, 5, 6, 9, 10};
+
+__global__ void k_elec_accumulate(int n, int first, const double *__restrict__ grad, const double *__restrict__ torque,
+                                  const double *__restrict__ eatom, const double *__restrict__ lg,
+                                  const double *__restrict__ lt, double *acc) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  double v[20];
+  for (int d = 0; d < 3; d++) {
+    v[d] = grad[d * n + i];
+    v[3 + d] = torque[d * n + i];
+    v[14 + d] = lg[d * n + i];
+    v[17 + d] = lt[d * n + i];
+  }
+  for (int r = 0; r < 8; r++) v[6 + r] = eatom[(size_t)kAccRows[r] * n + i];
+  for (int r = 0; r < 20; r++) acc[(size_t)r * n + i] = first ? v[r] : acc[(size_t)r * n + i] + v[r];
+}
+
+__global__ void k_elec_restore(int n, const double *__restrict__ acc, double *grad, double *torque, double *eatom,
+                               double *lg, double *lt) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  for (int d = 0; d < 3; d++) {
+    grad[d * n + i] = acc[(size_t)d * n + i];
+    torque[d * n + i] = acc[(size_t)(3 + d) * n + i];
+    lg[d * n + i] = acc[(size_t)(14 + d) * n + i];
+    lt[d * n + i] = acc[(size_t)(17 + d) * n + i];
+  }
+  for (int r = 0; r < 8; r++) eatom[(size_t)kAccRows[r] * n + i] = acc[(size_t)(6 + r) * n + i];
+}
+
+// out[3][n] += lg + the torque-derived part of the lambda gradient.
+__global__ void k_lambda_grad_add(int n, const double *__restrict__ lg, const double *__restrict__ lgtq, double *out) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  for (int d = 0; d < 3; d++) out[d * n + i] += lg[d * n + i] + lgtq[d * n + i];
+}
+
+// Zero the global and fractional multipoles of the soft atoms (the condensed step without
+// them: an atom with no multipoles and no polarizability takes no part).
+__global__ void k_zero_soft_multipoles(int n, const int *__restrict__ soft, double *gm, double *fm) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n || !soft[i]) return;
+  for (int t = 0; t < 10; t++) { gm[(size_t)t * n + i] = 0.0; fm[(size_t)t * n + i] = 0.0; }
+}
+
+void launch_elec_accumulate(Handle &h, bool first) {
+  k_elec_accumulate<<<nblocks(h.n, 256), 256, 0, h.stream>>>(h.n, first ? 1 : 0, h.d_grad, h.d_torque, h.d_eatom,
+                                                              h.d_lg, h.d_lt, h.d_acc);
+  FFX_LAUNCHED(h);
+}
+
+void launch_elec_restore(Handle &h) {
+  k_elec_restore<<<nblocks(h.n, 256), 256, 0, h.stream>>>(h.n, h.d_acc, h.d_grad, h.d_torque, h.d_eatom, h.d_lg,
+                                                           h.d_lt);
+  FFX_LAUNCHED(h);
+}
+
+void launch_lambda_grad_add(Handle &h, double *out) {
+  // The torque-derived part goes through d_vec's scratch rows, like launch_torque.
+  launch_torque_of(h, h.d_lt, h.d_vec);
+  k_lambda_grad_add<<<nblocks(h.n, 256), 256, 0, h.stream>>>(h.n, h.d_lg, h.d_vec, out);
+  FFX_LAUNCHED(h);
+}
+
+void launch_zero_soft_multipoles(Handle &h) {
+  k_zero_soft_multipoles<<<nblocks(h.n, 256), 256, 0, h.stream>>>(h.n, h.d_soft, h.d_gm, h.d_fm);
   FFX_LAUNCHED(h);
 }
 

@@ -198,6 +198,7 @@ __global__ void k_vdw_distribute(int n, const double *__restrict__ gred, const i
 
 
 void launch_vdw(Handle &h, bool grad) {
+  if (h.vacuum) return;   // a vacuum sub-system carries electrostatics only
   VdwForm vf{};
   const double off = h.prm.vdw_cutoff, cut = h.prm.vdw_taper * h.prm.vdw_cutoff;
   vf.off2 = off * off;
