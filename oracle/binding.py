@@ -41,6 +41,8 @@ def lib():
         L.oracle_neighbor_images.restype = ctypes.c_int64
         L.oracle_neighbor_images.argtypes = [ctypes.POINTER(cabi.FfxgSystem), ctypes.POINTER(cabi.FfxgParams), D,
                                              ctypes.POINTER(ctypes.c_int32)]
+        L.oracle_param_grad.restype = ctypes.c_int
+        L.oracle_param_grad.argtypes = [ctypes.POINTER(cabi.FfxgSystem), ctypes.POINTER(cabi.FfxgParams), D, D, D]
         L.oracle_set_images.restype = None
         L.oracle_set_images.argtypes = [ctypes.c_int]
         L.oracle_set_alchemy.restype = None
@@ -125,6 +127,21 @@ def neighbor_images(system: AmoebaSystem, params: AmoebaParams, xyz=None, all_im
                              out.ctypes.data_as(ctypes.POINTER(ctypes.c_int32)))
     L.oracle_set_images(0)
     return out
+
+
+def param_gradients(system: AmoebaSystem, params: AmoebaParams, xyz=None):
+    """(dE/dM [n,10] w.r.t. each atom's local multipole, dE/dalpha [n])."""
+    L = lib()
+    L.oracle_set_alchemy(None, system.n_atoms, 1.0)
+    s, keep = system.c_struct(cabi)
+    p = params_struct(params, cabi)
+    x = np.ascontiguousarray(system.xyz if xyz is None else xyz, dtype=np.float64)
+    dM = np.zeros((system.n_atoms, 10))
+    dA = np.zeros(system.n_atoms)
+    st = L.oracle_param_grad(ctypes.byref(s), ctypes.byref(p), _dp(x), _dp(dM), _dp(dA))
+    if st != 0:
+        raise RuntimeError(f"oracle status {st}")
+    return dM, dA
 
 
 def erfc(x: float) -> float:

@@ -2250,6 +2250,179 @@ struct Oracle {
     }
   }
 
+  // ---------------------------------------------------------------------------
+  // Parameter gradients (after energy()): dE/dM for each atom's local-frame multipole
+  // (stored components q, d, Q as in lmp) and dE/dalpha for its polarizability (with the
+  // Thole damping held fixed).  The permanent energy is bilinear in the multipoles, so
+  // dE_perm/dM_i is the potential of all other multipoles at i (real space with its
+  // masks, reciprocal, self, charge correction).  The polarization energy is
+  // E_pol = -1/2 electric E_d^T A^-1 E_p with A = alpha^-1 - T symmetric, u_D = A^-1 E_d and
+  // u_P = A^-1 E_p, so dE_pol/dM = -1/2 electric (F_d^T u_P + F_p^T u_D): the CR dipoles
+  // are the adjoint solution and no further solve is needed; and
+  // dE_pol/dalpha_i = -1/2 electric alpha_i^-2 u_D,i . u_P,i.
+
+  // d e_pair / d M_t (stored components) of the permanent pair energy for the target
+  // multipole t and source Ms at r = x_s - x_t with radial coefficients b[0..4]
+  // (the derivative of RealSpaceEnergyRegion.permanentPair's gl sums, :1190-1290).
+  static void pair_pot(const double *Ms, const double r[3], const double b[5], double out[10]) {
+    const double ck = Ms[t000], dk[3] = {Ms[t100], Ms[t010], Ms[t001]};
+    double qk[3][3];
+    qk[0][0] = Ms[t200] / 3.0; qk[1][1] = Ms[t020] / 3.0; qk[2][2] = Ms[t002] / 3.0;
+    qk[0][1] = qk[1][0] = Ms[t110] / 3.0; qk[0][2] = qk[2][0] = Ms[t101] / 3.0; qk[1][2] = qk[2][1] = Ms[t011] / 3.0;
+    double qkr[3];
+    for (int a = 0; a < 3; a++) qkr[a] = qk[a][0] * r[0] + qk[a][1] * r[1] + qk[a][2] * r[2];
+    const double sc4 = dk[0] * r[0] + dk[1] * r[1] + dk[2] * r[2];
+    const double sc6 = qkr[0] * r[0] + qkr[1] * r[1] + qkr[2] * r[2];
+    out[t000] = ck * b[0] - sc4 * b[1] + sc6 * b[2];
+    const double cd = ck * b[1] - sc4 * b[2] + sc6 * b[3];
+    for (int a = 0; a < 3; a++) out[1 + a] = cd * r[a] + b[1] * dk[a] - 2.0 * b[2] * qkr[a];
+    double G[3][3];
+    for (int a = 0; a < 3; a++)
+      for (int c = 0; c < 3; c++)
+        G[a][c] = (ck * r[a] * r[c] + 2.0 * dk[a] * r[c] + 2.0 * qk[a][c]) * b[2] +
+                  (-sc4 * r[a] * r[c] - 4.0 * qkr[a] * r[c]) * b[3] + sc6 * r[a] * r[c] * b[4];
+    quad_out(G, out);
+  }
+
+  // d (u . E(M_t))/d M_t for a dipole u at r = x_u - x_t from the target multipole, with the
+  // radial coefficients b1..b3 of the field (PermanentFieldRegion.java:703-760: Ewald bn
+  // less the masked, Thole-damped corrections).
+  static void dip_pot(const double u[3], const double r[3], double b1, double b2, double b3, double out[10]) {
+    const double ur = u[0] * r[0] + u[1] * r[1] + u[2] * r[2];
+    out[t000] = ur * b1;
+    for (int a = 0; a < 3; a++) out[1 + a] = ur * b2 * r[a] - b1 * u[a];
+    double G[3][3];
+    for (int a = 0; a < 3; a++)
+      for (int c = 0; c < 3; c++) G[a][c] = ur * b3 * r[a] * r[c] - 2.0 * b2 * u[a] * r[c];
+    quad_out(G, out);
+  }
+
+  // Derivatives w.r.t. q_ab = Q_ab / 3 (full matrix G) as derivatives w.r.t. the stored
+  // quadrupole components (diagonal once, each off-diagonal pair once).
+  static void quad_out(const double G[3][3], double *out) {
+    out[t200] = G[0][0] / 3.0; out[t020] = G[1][1] / 3.0; out[t002] = G[2][2] / 3.0;
+    out[t110] = (G[0][1] + G[1][0]) / 3.0;
+    out[t101] = (G[0][2] + G[2][0]) / 3.0;
+    out[t011] = (G[1][2] + G[2][1]) / 3.0;
+  }
+
+  void param_gradients(std::vector<double> &dM, std::vector<double> &dA) {
+    const double electric = p.electric;
+    std::vector<double> phi(10 * (size_t)n, 0.0);   // dE/dM, global frame
+    const bool pol = p.polarization != FFXG_POLAR_NONE;
+    // Real space, over the Ewald lists (each pair once, both sides).
+    for (int i = 0; i < n; i++) {
+      std::vector<double> mm(n, 1.0), dd(n, 1.0), pp(n, 1.0);
+      for (int k : m12[i]) { mm[k] = p.m12; pp[k] = p.p12; }
+      for (int k : m13[i]) { mm[k] = p.m13; pp[k] = p.p13; }
+      for (int k : m14[i]) {
+        mm[k] = p.m14; pp[k] = p.p14;
+        for (int g : ip11[i]) if (g == k) { pp[k] = p.intra14 * p.p14; break; }
+      }
+      for (int k : m15[i]) mm[k] = p.m15;
+      for (int g : ip11[i]) dd[g] = p.d11;
+      for (size_t e = 0; e < ewald[i].size(); e++) {
+        const int k = ewald[i][e];
+        double xr = x[k] - x[i], yr = y[k] - y[i], zr = z[k] - z[i];
+        const double r2 = disp(xr, yr, zr, esh, i, e);
+        const bool prim = primary(esh, i, e);
+        const double r = std::sqrt(r2);
+        const double ralpha = aewald * r, exp2a = std::exp(-ralpha * ralpha);
+        const double rr1 = 1.0 / r, rr2 = rr1 * rr1;
+        const double bn0 = std::erfc(ralpha) * rr1;
+        const double bn1 = (bn0 + an0 * exp2a) * rr2, bn2 = (3.0 * bn1 + an1 * exp2a) * rr2;
+        const double bn3 = (5.0 * bn2 + an2 * exp2a) * rr2, bn4 = (7.0 * bn3 + an3 * exp2a) * rr2;
+        const double rr3 = rr1 * rr2, rr5 = 3.0 * rr3 * rr2, rr7 = 5.0 * rr5 * rr2, rr9 = 7.0 * rr7 * rr2;
+        const double rik[3] = {xr, yr, zr}, rki[3] = {-xr, -yr, -zr};
+        const double scale1 = 1.0 - (prim ? mm[k] : 1.0);
+        const double bE[5] = {bn0, bn1, bn2, bn3, bn4}, bR[5] = {rr1, rr3, rr5, rr7, rr9};
+        double a[10], c[10];
+        // permanent: target i (source k at r_ik), target k (source i at r_ki)
+        pair_pot(&gm[10 * (size_t)k], rik, bE, a);
+        pair_pot(&gm[10 * (size_t)k], rik, bR, c);
+        for (int t = 0; t < 10; t++) phi[10 * (size_t)i + t] += electric * (a[t] - scale1 * c[t]);
+        pair_pot(&gm[10 * (size_t)i], rki, bE, a);
+        pair_pot(&gm[10 * (size_t)i], rki, bR, c);
+        for (int t = 0; t < 10; t++) phi[10 * (size_t)k + t] += electric * (a[t] - scale1 * c[t]);
+        if (!pol) continue;
+        double scale3 = 1.0, scale5 = 1.0, scale7 = 1.0;
+        double damp = ipdamp[i] * ipdamp[k];
+        const double tho = std::min(thole[i], thole[k]);
+        const double rdamp = r * damp;
+        damp = -tho * rdamp * rdamp * rdamp;
+        if (damp > -50.0) {
+          const double expdamp = std::exp(damp);
+          scale3 = 1.0 - expdamp;
+          scale5 = 1.0 - expdamp * (1.0 - damp);
+          scale7 = 1.0 - expdamp * (1.0 - damp + 0.6 * damp * damp);
+        }
+        const double sd = prim ? dd[k] : 1.0, sp = prim ? pp[k] : 1.0;
+        const double db1 = bn1 - (1.0 - scale3 * sd) * rr3, db2 = bn2 - (1.0 - scale5 * sd) * rr5,
+                     db3 = bn3 - (1.0 - scale7 * sd) * rr7;
+        const double pb1 = bn1 - (1.0 - scale3 * sp) * rr3, pb2 = bn2 - (1.0 - scale5 * sp) * rr5,
+                     pb3 = bn3 - (1.0 - scale7 * sp) * rr7;
+        const double h = -0.5 * electric;
+        // target i: dipoles at k; target k: dipoles at i.
+        dip_pot(&uP[3 * (size_t)k], rik, db1, db2, db3, a);
+        dip_pot(&uD[3 * (size_t)k], rik, pb1, pb2, pb3, c);
+        for (int t = 0; t < 10; t++) phi[10 * (size_t)i + t] += h * (a[t] + c[t]);
+        dip_pot(&uP[3 * (size_t)i], rki, db1, db2, db3, a);
+        dip_pot(&uD[3 * (size_t)i], rki, pb1, pb2, pb3, c);
+        for (int t = 0; t < 10; t++) phi[10 * (size_t)k + t] += h * (a[t] + c[t]);
+      }
+    }
+    // Reciprocal space, self terms, charge correction.
+    const double w[10] = {1.0, 1.0, 1.0, 1.0, 1.0 / 3.0, 1.0 / 3.0, 1.0 / 3.0, 2.0 / 3.0, 2.0 / 3.0, 2.0 / 3.0};
+    const double aewald1 = -electric * aewald / kSqrtPi, aewald2 = 2.0 * aewald * aewald;
+    double qtot = 0.0;
+    for (int i = 0; i < n; i++) qtot += gm[10 * (size_t)i];
+    const double dcorr = (qtot != 0.0) ? -electric * kPi * qtot / (cell.volume * aewald * aewald) : 0.0;
+    for (int i = 0; i < n; i++) {
+      double *f = &phi[10 * (size_t)i];
+      const double *m = &gm[10 * (size_t)i];
+      for (int t = 0; t < 10; t++) f[t] += electric * w[t] * cphi[20 * (size_t)i + t];
+      f[t000] += 2.0 * aewald1 * m[t000] + dcorr;
+      for (int a = 1; a < 4; a++) f[a] += aewald1 * aewald2 * 2.0 * m[a] / 3.0;
+      for (int a = 4; a < 7; a++) f[a] += aewald1 * aewald2 * 2.0 * aewald2 * 2.0 * m[a] / 45.0;
+      for (int a = 7; a < 10; a++) f[a] += aewald1 * aewald2 * 2.0 * aewald2 * 4.0 * m[a] / 45.0;
+      if (pol) {
+        const double h = -0.5 * electric;
+        for (int t = 0; t < 10; t++)
+          f[t] += h * -w[t] * (cphiP[20 * (size_t)i + t] + cphiI[20 * (size_t)i + t]);
+        for (int a = 0; a < 3; a++) f[1 + a] += h * aewald3 * (uP[3 * (size_t)i + a] + uD[3 * (size_t)i + a]);
+      }
+    }
+    // Global -> local frame: d = R d_l, Q = R Q_l R^T (rotate_multipoles).
+    dM.assign(10 * (size_t)n, 0.0);
+    dA.assign(n, 0.0);
+    for (int i = 0; i < n; i++) {
+      double R[3][3];
+      rotation_matrix(i, R);
+      const double *f = &phi[10 * (size_t)i];
+      double *o = &dM[10 * (size_t)i];
+      o[t000] = f[t000];
+      for (int b = 0; b < 3; b++) o[1 + b] = R[0][b] * f[1] + R[1][b] * f[2] + R[2][b] * f[3];
+      double G[3][3];
+      G[0][0] = f[t200]; G[1][1] = f[t020]; G[2][2] = f[t002];
+      G[0][1] = G[1][0] = 0.5 * f[t110]; G[0][2] = G[2][0] = 0.5 * f[t101]; G[1][2] = G[2][1] = 0.5 * f[t011];
+      double L[3][3];
+      for (int a = 0; a < 3; a++)
+        for (int b = 0; b < 3; b++) {
+          double v = 0.0;
+          for (int c = 0; c < 3; c++)
+            for (int d = 0; d < 3; d++) v += R[c][a] * G[c][d] * R[d][b];
+          L[a][b] = v;
+        }
+      o[t200] = L[0][0]; o[t020] = L[1][1]; o[t002] = L[2][2];
+      o[t110] = 2.0 * L[0][1]; o[t101] = 2.0 * L[0][2]; o[t011] = 2.0 * L[1][2];
+      if (pol && polar[i] > 0.0) {
+        const double ud = uD[3 * (size_t)i] * uP[3 * (size_t)i] + uD[3 * (size_t)i + 1] * uP[3 * (size_t)i + 1] +
+                          uD[3 * (size_t)i + 2] * uP[3 * (size_t)i + 2];
+        dA[i] = -0.5 * electric * ud / (polar[i] * polar[i]);
+      }
+    }
+  }
+
   // Per-term electrostatic energies of one evaluation.
   struct ElecTerms {
     double eSelf = 0, eRecip = 0, eCorr = 0, eSelfI = 0, eRecipI = 0, eReal = 0, eRealI = 0;
@@ -2510,6 +2683,25 @@ int64_t oracle_neighbor_images(const ffxg_system *sys, const ffxg_params *prm, c
       c++;
     }
   return c;
+}
+
+// Energy, then the parameter gradients: dEdM[n][10] w.r.t. each atom's local multipole
+// (stored components) and dEdA[n] w.r.t. its polarizability (Thole damping fixed).
+int oracle_param_grad(const ffxg_system *sys, const ffxg_params *prm, const double *xyz, double *dEdM,
+                      double *dEdA) {
+  Oracle o;
+  o.nthreads = 1;
+#ifdef _OPENMP
+  o.nthreads = omp_get_max_threads();
+#endif
+  o.setup(sys, prm, xyz ? xyz : sys->xyz);
+  const int st = o.energy(false, nullptr, nullptr, nullptr);
+  if (st != FFXG_OK) return st;
+  std::vector<double> dM, dA;
+  o.param_gradients(dM, dA);
+  std::memcpy(dEdM, dM.data(), dM.size() * sizeof(double));
+  std::memcpy(dEdA, dA.data(), dA.size() * sizeof(double));
+  return FFXG_OK;
 }
 
 // Force (1) or release (0) multi-image lists for boxes where the minimum image suffices.
