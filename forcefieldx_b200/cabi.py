@@ -84,6 +84,7 @@ PROTOTYPES = {
     "ffxg_get_neighbor_pairs": (ctypes.c_int, [ctypes.c_void_p, _I, _L]),
     "ffxg_get_neighbor_images": (ctypes.c_int, [ctypes.c_void_p, _I, _L]),
     "ffxg_set_image_mode": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int]),
+    "ffxg_param_grad": (ctypes.c_int, [ctypes.c_void_p, _D, _D]),
     "ffxg_batch_create": (ctypes.c_int, [ctypes.c_int32, ctypes.POINTER(FfxgSystem), ctypes.POINTER(FfxgParams),
                                          ctypes.POINTER(ctypes.c_void_p)]),
     "ffxg_batch_energy": (ctypes.c_int, [ctypes.c_void_p, _D, ctypes.c_int, _D, _D, _L, _I]),

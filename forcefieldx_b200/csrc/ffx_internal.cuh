@@ -315,6 +315,7 @@ struct Handle {
 
   // ---- electrostatics work arrays
   double *d_gm = nullptr;                     // [10][n]
+  double *d_rot = nullptr;                    // [9][n] local-to-global rotation (row-major)
   double *d_fm = nullptr;                     // [10][n]
   double *d_spl = nullptr;                    // [n][3][order][4]
   int *d_igrid = nullptr;                     // [3][n]
@@ -462,6 +463,7 @@ void launch_lambda_grad_add(Handle &h, double *out);
 void launch_zero_soft_multipoles(Handle &h);
 void launch_assemble(Handle &h, double *d_grad_xyz);
 void launch_reduce_results(Handle &h);
+int param_gradients(Handle &h, double *dEdM, double *dEdA);
 void setup_pme(Handle &h);
 
 inline int nblocks(int64_t n, int t) { return (int)((n + t - 1) / t); }

@@ -308,7 +308,7 @@ static int create_impl(const ffxg_system *s, const ffxg_params *p, Handle &h) {
   CK(dalloc(&h.d_cell_atoms, N)); CK(dalloc(&h.d_atom_cell, N));
   CK(dalloc(&h.d_nbr_cnt, N)); CK(dalloc(&h.d_ewl_cnt, N)); CK(dalloc(&h.d_prl_cnt, N));
   if (int st = alloc_lists(h)) return st;
-  CK(dalloc(&h.d_gm, 10 * N)); CK(dalloc(&h.d_fm, 10 * N));
+  CK(dalloc(&h.d_gm, 10 * N)); CK(dalloc(&h.d_fm, 10 * N)); CK(dalloc(&h.d_rot, 9 * N));
   CK(dalloc(&h.d_spl, N * 3 * kOrder * 4)); CK(dalloc(&h.d_igrid, 3 * N));
   CK(dalloc(&h.d_cphi, 20 * N)); CK(dalloc(&h.d_fphi, 20 * N));
   CK(dalloc(&h.d_cphiI, 20 * N)); CK(dalloc(&h.d_fphiI, 20 * N));
@@ -428,7 +428,7 @@ static void free_all(Handle &h) {
                   h.d_uP, h.d_udirD, h.d_udirP, h.d_r, h.d_rP, h.d_zpre, h.d_zpreP, h.d_p, h.d_pP, h.d_vec, h.d_vecP,
                   h.d_partials, h.d_scalars, h.d_grid, h.d_influence, h.d_twiddle, h.d_gridf, h.d_influencef, h.d_twiddlef, h.d_grad, h.d_torque, h.d_gred,
                   h.d_eatom, h.d_catom, h.d_result, h.d_cresult, h.d_flags, h.d_xyz_in, h.d_grad_out,
-                  h.d_coefE, h.d_coefP, h.d_coefEB, h.d_coefPB, h.d_part2, h.d_counter, h.d_pos, h.d_recF, h.d_recP, h.d_tpair, h.d_tp, h.d_soft, h.d_mol, h.d_lgred, h.d_mass, h.d_mdx, h.d_mdv, h.d_mda, h.d_mdxp, h.d_mdg, h.d_mdke, h.d_settle, h.d_aspc, h.d_aspc_state, h.d_nbr_sh, h.d_ewl_sh, h.d_lg, h.d_lt, h.d_acc, h.d_polar_env, h.d_lig};
+                  h.d_coefE, h.d_coefP, h.d_coefEB, h.d_coefPB, h.d_part2, h.d_counter, h.d_pos, h.d_recF, h.d_recP, h.d_tpair, h.d_tp, h.d_soft, h.d_mol, h.d_lgred, h.d_mass, h.d_mdx, h.d_mdv, h.d_mda, h.d_mdxp, h.d_mdg, h.d_mdke, h.d_settle, h.d_aspc, h.d_aspc_state, h.d_nbr_sh, h.d_ewl_sh, h.d_lg, h.d_lt, h.d_acc, h.d_polar_env, h.d_lig, h.d_rot};
   for (void *q : ptrs)
     if (q) cudaFree(q);
   if (h.h_scalars) cudaFreeHost(h.h_scalars);
@@ -1026,6 +1026,30 @@ int ffxg_get_neighbor_pairs(ffxg_handle *hh, int32_t *pairs, int64_t *n_pairs) {
 int ffxg_get_neighbor_images(ffxg_handle *hh, int32_t *rows, int64_t *n_rows) {
   if (!hh || !n_rows) return FFXG_ERR_BAD_ARG;
   return list_images(hh->h, rows, 5, n_rows);
+}
+
+int ffxg_param_grad(ffxg_handle *hh, double *dEdM, double *dEdalpha) {
+  if (!hh || !dEdM || !dEdalpha) return FFXG_ERR_BAD_ARG;
+  Handle &h = hh->h;
+  if (!h.list_valid) { h.err = "no evaluation yet: call ffxg_energy first"; return FFXG_ERR_BAD_ARG; }
+  if (h.elec.on && h.alch.active) { h.err = "parameter gradients are not defined under electrostatic lambda"; return FFXG_ERR_BAD_ARG; }
+  const size_t N = h.n;
+  double *d = nullptr;
+  CK(cudaMalloc(&d, 11 * N * sizeof(double)));
+  int st = param_gradients(h, d, d + 10 * N);
+  if (st == FFXG_OK) {
+    std::vector<double> a(11 * N);
+    if (cudaMemcpyAsync(a.data(), d, 11 * N * sizeof(double), cudaMemcpyDeviceToHost, h.stream) != cudaSuccess ||
+        cudaStreamSynchronize(h.stream) != cudaSuccess) {
+      st = FFXG_ERR_CUDA;
+    } else {
+      std::memcpy(dEdM, a.data(), 10 * N * sizeof(double));
+      std::memcpy(dEdalpha, a.data() + 10 * N, N * sizeof(double));
+    }
+  }
+  cudaFree(d);
+  if (st != FFXG_OK) h.err = std::string("CUDA error: ") + cudaGetErrorString(cudaGetLastError());
+  return st;
 }
 
 int ffxg_set_image_mode(ffxg_handle *hh, int mode) {

@@ -31,7 +31,7 @@ __device__ __forceinline__ void d_norm(double *v) {
 
 __global__ void k_rotate(int n, const double *__restrict__ x, const double *__restrict__ y,
                          const double *__restrict__ z, const int *__restrict__ frame, const int *__restrict__ axis,
-                         const double *__restrict__ lmp, double *gm) {
+                         const double *__restrict__ lmp, double *gm, double *rot) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
   double R[3][3] = {{1, 0, 0}, {0, 1, 0}, {0, 0, 1}};
@@ -107,6 +107,8 @@ __global__ void k_rotate(int n, const double *__restrict__ x, const double *__re
       rq[a][b] = s;
     }
   }
+  for (int a = 0; a < 3; a++)
+    for (int b = 0; b < 3; b++) rot[(3 * a + b) * n + i] = R[a][b];   // kept for the parameter gradients
   gm[t000 * n + i] = lmp[i];
   gm[t100 * n + i] = rd[0]; gm[t010 * n + i] = rd[1]; gm[t001 * n + i] = rd[2];
   gm[t200 * n + i] = rq[0][0]; gm[t020 * n + i] = rq[1][1]; gm[t002 * n + i] = rq[2][2];
@@ -816,7 +818,8 @@ void setup_pme(Handle &h) {
 
 // ---------------------------------------------------------------------------
 void launch_rotate(Handle &h) {
-  k_rotate<<<nblocks(h.n, 128), 128, 0, h.stream>>>(h.n, h.d_x, h.d_y, h.d_z, h.d_frame, h.d_axis, h.d_lmp, h.d_gm);
+  k_rotate<<<nblocks(h.n, 128), 128, 0, h.stream>>>(h.n, h.d_x, h.d_y, h.d_z, h.d_frame, h.d_axis, h.d_lmp, h.d_gm,
+                                                     h.d_rot);
   FFX_LAUNCHED(h);
 }
 

@@ -724,6 +724,208 @@ static void real_energy(Handle &h, bool grad) {
   FFX_LAUNCHED(h);
 }
 
+// ---------------------------------------------------------------------------
+// Parameter gradients of the last evaluation: dE/dM of each atom's local-frame multipole
+// (stored components) and dE/dalpha of its polarizability (Thole damping fixed).
+// dE_perm/dM_i is the potential of all other multipoles at i (bilinear energy); with
+// E_pol = -1/2 electric E_d^T A^-1 E_p and A symmetric, the CR dipoles u_P = A^-1 E_p are
+// the adjoint solution: dE_pol/dM = -1/2 electric (F_d^T u_P + F_p^T u_D), and
+// dE_pol/dalpha_i = -1/2 electric alpha_i^-2 u_D,i . u_P,i.  FP64 in both forms.
+
+// d e_pair/d M_t for the source multipole (ck, dk, qk = Q/3) at r = x_s - x_t and radial
+// coefficients b[0..4]: the derivative of permanentPair's gl sums
+// (RealSpaceEnergyRegion.java:1190-1290).  Accumulated into acc with weight wgt.
+__device__ __forceinline__ void quad_acc(const double G[3][3], double wgt, double *acc) {
+  acc[4] += wgt * G[0][0] / 3.0; acc[5] += wgt * G[1][1] / 3.0; acc[6] += wgt * G[2][2] / 3.0;
+  acc[7] += wgt * (G[0][1] + G[1][0]) / 3.0;
+  acc[8] += wgt * (G[0][2] + G[2][0]) / 3.0;
+  acc[9] += wgt * (G[1][2] + G[2][1]) / 3.0;
+}
+
+__device__ __forceinline__ void pair_pot_acc(double ck, const double *dk, const double qk[3][3], const double *r,
+                                             const double *b, double wgt, double *acc) {
+  double qkr[3];
+  for (int a = 0; a < 3; a++) qkr[a] = qk[a][0] * r[0] + qk[a][1] * r[1] + qk[a][2] * r[2];
+  const double sc4 = dk[0] * r[0] + dk[1] * r[1] + dk[2] * r[2];
+  const double sc6 = qkr[0] * r[0] + qkr[1] * r[1] + qkr[2] * r[2];
+  acc[0] += wgt * (ck * b[0] - sc4 * b[1] + sc6 * b[2]);
+  const double cd = ck * b[1] - sc4 * b[2] + sc6 * b[3];
+  for (int a = 0; a < 3; a++) acc[1 + a] += wgt * (cd * r[a] + b[1] * dk[a] - 2.0 * b[2] * qkr[a]);
+  double G[3][3];
+  for (int a = 0; a < 3; a++)
+    for (int c = 0; c < 3; c++)
+      G[a][c] = (ck * r[a] * r[c] + 2.0 * dk[a] * r[c] + 2.0 * qk[a][c]) * b[2] +
+                (-sc4 * r[a] * r[c] - 4.0 * qkr[a] * r[c]) * b[3] + sc6 * r[a] * r[c] * b[4];
+  quad_acc(G, wgt, acc);
+}
+
+// d (u . E(M_t))/d M_t for a dipole u at r = x_u - x_t, field coefficients b1..b3
+// (PermanentFieldRegion.java:703-760).
+__device__ __forceinline__ void dip_pot_acc(const double *u, const double *r, double b1, double b2, double b3,
+                                            double wgt, double *acc) {
+  const double ur = u[0] * r[0] + u[1] * r[1] + u[2] * r[2];
+  acc[0] += wgt * ur * b1;
+  for (int a = 0; a < 3; a++) acc[1 + a] += wgt * (ur * b2 * r[a] - b1 * u[a]);
+  double G[3][3];
+  for (int a = 0; a < 3; a++)
+    for (int c = 0; c < 3; c++) G[a][c] = ur * b3 * r[a] * r[c] - 2.0 * b2 * u[a] * r[c];
+  quad_acc(G, wgt, acc);
+}
+
+// One warp per atom over its Ewald row: the real-space parts of dE/dM_i (global frame)
+// into phi[10][n].
+__global__ void __launch_bounds__(128) k_param_real(
+    int n, const double *__restrict__ x, const double *__restrict__ y, const double *__restrict__ z, Box bx,
+    const double *__restrict__ gm, const double *__restrict__ uD, const double *__restrict__ uP,
+    const double *__restrict__ ipdamp, const double *__restrict__ thole, const int *__restrict__ ewl,
+    const int *__restrict__ ewl_cnt, int capE, const int *__restrict__ ewl_sh, Excl ex, EwaldCoef ec,
+    ScaleTables c_scales, int pol, double *phi) {
+  const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const int lane = threadIdx.x & 31;
+  if (warp >= n) return;
+  const int i = warp;
+  const double xi = x[i], yi = y[i], zi = z[i];
+  const double pdi = ipdamp[i], pti = thole[i];
+  const double electric = ec.electric;
+  double acc[10] = {0, 0, 0, 0, 0, 0, 0, 0, 0, 0};
+  const int cnt = min(ewl_cnt[i], capE);
+  const int *row = ewl + (size_t)i * capE;
+  for (int a = lane; a < cnt; a += 32) {
+    const int k = row[a];
+    const size_t ent = (size_t)i * capE + a;
+    double xr = __dsub_rn(x[k], xi), yr = __dsub_rn(y[k], yi), zr = __dsub_rn(z[k], zi);
+    const double r2 = pair_image(xr, yr, zr, bx, ewl_sh, ent, 1.0);
+    const unsigned code = pair_primary(ewl_sh, ent) ? excl_code(i, k, ex.ptr, ex.k, ex.code, ex.lo, ex.hi) : 0u;
+    const double sm = c_scales.m[code & 7u], sp = c_scales.p[(code >> 3) & 7u], sd = c_scales.d[(code >> 6) & 1u];
+    const double r = sqrt(r2);
+    const double ralpha = ec.aewald * r, exp2a = exp(-ralpha * ralpha);
+    const double rr1 = 1.0 / r, rr2 = rr1 * rr1;
+    const double bn0 = erfc(ralpha) * rr1;
+    const double bn1 = (bn0 + ec.an0 * exp2a) * rr2, bn2 = (3.0 * bn1 + ec.an1 * exp2a) * rr2;
+    const double bn3 = (5.0 * bn2 + ec.an2 * exp2a) * rr2, bn4 = (7.0 * bn3 + ec.an3 * exp2a) * rr2;
+    const double rr3 = rr1 * rr2, rr5 = 3.0 * rr3 * rr2, rr7 = 5.0 * rr5 * rr2, rr9 = 7.0 * rr7 * rr2;
+    const double rv[3] = {xr, yr, zr};
+    const double ck = gm[t000 * n + k];
+    const double dk[3] = {gm[t100 * n + k], gm[t010 * n + k], gm[t001 * n + k]};
+    double qk[3][3];
+    qk[0][0] = gm[t200 * n + k] / 3.0; qk[1][1] = gm[t020 * n + k] / 3.0; qk[2][2] = gm[t002 * n + k] / 3.0;
+    qk[0][1] = qk[1][0] = gm[t110 * n + k] / 3.0;
+    qk[0][2] = qk[2][0] = gm[t101 * n + k] / 3.0;
+    qk[1][2] = qk[2][1] = gm[t011 * n + k] / 3.0;
+    const double bE[5] = {bn0, bn1, bn2, bn3, bn4}, bR[5] = {rr1, rr3, rr5, rr7, rr9};
+    pair_pot_acc(ck, dk, qk, rv, bE, electric, acc);
+    pair_pot_acc(ck, dk, qk, rv, bR, -electric * (1.0 - sm), acc);
+    if (!pol) continue;
+    double scale3 = 1.0, scale5 = 1.0, scale7 = 1.0;
+    double damp = pdi * ipdamp[k];
+    const double tho = fmin(pti, thole[k]);
+    const double rdamp = r * damp;
+    damp = -tho * rdamp * rdamp * rdamp;
+    if (damp > -50.0) {
+      const double expdamp = exp(damp);
+      scale3 = 1.0 - expdamp;
+      scale5 = 1.0 - expdamp * (1.0 - damp);
+      scale7 = 1.0 - expdamp * (1.0 - damp + 0.6 * damp * damp);
+    }
+    const double up[3] = {uP[k], uP[n + k], uP[2 * n + k]}, ud[3] = {uD[k], uD[n + k], uD[2 * n + k]};
+    const double hw = -0.5 * electric;
+    dip_pot_acc(up, rv, bn1 - (1.0 - scale3 * sd) * rr3, bn2 - (1.0 - scale5 * sd) * rr5,
+                bn3 - (1.0 - scale7 * sd) * rr7, hw, acc);
+    dip_pot_acc(ud, rv, bn1 - (1.0 - scale3 * sp) * rr3, bn2 - (1.0 - scale5 * sp) * rr5,
+                bn3 - (1.0 - scale7 * sp) * rr7, hw, acc);
+  }
+#pragma unroll
+  for (int t = 0; t < 10; t++) acc[t] = warp_sum(acc[t]);
+  if (lane == 0)
+    for (int t = 0; t < 10; t++) phi[(size_t)t * n + i] = acc[t];
+}
+
+struct ParamConst {
+  double electric, aewald1, aewald2, aewald3, dcorr;
+  int pol;
+};
+
+// Reciprocal, self and charge-correction parts, then the local frame (d = R d_l,
+// Q = R Q_l R^T) and dE/dalpha; out[n][10], outA[n].
+__global__ void k_param_finish(int n, const double *__restrict__ phi, const double *__restrict__ gm,
+                               const double *__restrict__ cphi, const double *__restrict__ cphiI,
+                               const double *__restrict__ cphiP, const double *__restrict__ uD,
+                               const double *__restrict__ uP, const double *__restrict__ polar,
+                               const double *__restrict__ rot, ParamConst pc, double *out, double *outA) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const double w[10] = {1.0, 1.0, 1.0, 1.0, 1.0 / 3.0, 1.0 / 3.0, 1.0 / 3.0, 2.0 / 3.0, 2.0 / 3.0, 2.0 / 3.0};
+  double f[10], m[10];
+  for (int t = 0; t < 10; t++) {
+    m[t] = gm[(size_t)t * n + i];
+    f[t] = phi[(size_t)t * n + i] + pc.electric * w[t] * cphi[(size_t)t * n + i];
+  }
+  f[0] += 2.0 * pc.aewald1 * m[0] + pc.dcorr;
+  for (int a = 1; a < 4; a++) f[a] += pc.aewald1 * pc.aewald2 * 2.0 * m[a] / 3.0;
+  for (int a = 4; a < 7; a++) f[a] += pc.aewald1 * pc.aewald2 * 2.0 * pc.aewald2 * 2.0 * m[a] / 45.0;
+  for (int a = 7; a < 10; a++) f[a] += pc.aewald1 * pc.aewald2 * 2.0 * pc.aewald2 * 4.0 * m[a] / 45.0;
+  double dA = 0.0;
+  if (pc.pol) {
+    const double h = -0.5 * pc.electric;
+    for (int t = 0; t < 10; t++) f[t] -= h * w[t] * (cphiP[(size_t)t * n + i] + cphiI[(size_t)t * n + i]);
+    double ud = 0.0;
+    for (int a = 0; a < 3; a++) {
+      const double pa = uP[(size_t)a * n + i], da = uD[(size_t)a * n + i];
+      f[1 + a] += h * pc.aewald3 * (pa + da);
+      ud += da * pa;
+    }
+    const double al = polar[i];
+    if (al > 0.0) dA = h * ud / (al * al);
+  }
+  double R[3][3];
+  for (int a = 0; a < 3; a++)
+    for (int b = 0; b < 3; b++) R[a][b] = rot[(size_t)(3 * a + b) * n + i];
+  double *o = out + 10 * (size_t)i;
+  o[0] = f[0];
+  for (int b = 0; b < 3; b++) o[1 + b] = R[0][b] * f[1] + R[1][b] * f[2] + R[2][b] * f[3];
+  double G[3][3];
+  G[0][0] = f[4]; G[1][1] = f[5]; G[2][2] = f[6];
+  G[0][1] = G[1][0] = 0.5 * f[7]; G[0][2] = G[2][0] = 0.5 * f[8]; G[1][2] = G[2][1] = 0.5 * f[9];
+  double L[3][3];
+  for (int a = 0; a < 3; a++)
+    for (int b = 0; b < 3; b++) {
+      double v = 0.0;
+      for (int c = 0; c < 3; c++)
+        for (int d = 0; d < 3; d++) v += R[c][a] * G[c][d] * R[d][b];
+      L[a][b] = v;
+    }
+  o[4] = L[0][0]; o[5] = L[1][1]; o[6] = L[2][2];
+  o[7] = 2.0 * L[0][1]; o[8] = 2.0 * L[0][2]; o[9] = 2.0 * L[1][2];
+  outA[i] = dA;
+}
+
+// dE/dM [n][10] (device) and dE/dalpha [n] (device) of the last evaluation's state.
+int param_gradients(Handle &h, double *d_dM, double *d_dA) {
+  const size_t N = h.n;
+  double *scratch = nullptr;
+  if (cudaMallocAsync(&scratch, 10 * N * sizeof(double), h.stream) != cudaSuccess) return FFXG_ERR_CUDA;
+  const bool pol = h.prm.polarization != FFXG_POLAR_NONE;
+  k_param_real<<<nblocks((int64_t)h.n * 32, 128), 128, 0, h.stream>>>(
+      h.n, h.d_x, h.d_y, h.d_z, h.box, h.d_gm, h.d_uD, h.d_uP, h.d_ipdamp, h.d_thole, h.d_ewl, h.d_ewl_cnt,
+      h.cap_ewl, h.d_ewl_sh, excl(h), ewald_coef(h, ewald_alpha_of(h)), h.scales, pol ? 1 : 0, scratch);
+  ParamConst pc{};
+  const double SQRT_PI = 1.7724538509055160273, PI = 3.14159265358979323846;
+  const double a = ewald_alpha_of(h);
+  pc.electric = h.prm.electric;
+  pc.aewald1 = -pc.electric * a / SQRT_PI;
+  pc.aewald2 = 2.0 * a * a;
+  pc.aewald3 = 4.0 / 3.0 * a * a * a / SQRT_PI;
+  double q = 0.0;
+  for (size_t i = 0; i < N; i++) q += h.sys.multipole[10 * i];
+  pc.dcorr = (q != 0.0 && a > 0.0) ? -pc.electric * PI * q / (h.box.volume * a * a) : 0.0;
+  pc.pol = pol ? 1 : 0;
+  k_param_finish<<<nblocks(h.n, 128), 128, 0, h.stream>>>(h.n, scratch, h.d_gm, h.d_cphi, h.d_cphiI, h.d_cphiP,
+                                                          h.d_uD, h.d_uP, h.d_polar, h.d_rot, pc, d_dM, d_dA);
+  cudaFreeAsync(scratch, h.stream);
+  h.launches += 2;
+  return cudaGetLastError() == cudaSuccess ? FFXG_OK : FFXG_ERR_CUDA;
+}
+
 void launch_real_energy(Handle &h, bool grad) {
   if (h.mixed)
     real_energy<float>(h, grad);

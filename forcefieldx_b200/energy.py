@@ -179,6 +179,20 @@ class ForceFieldEnergy:
                                                       ctypes.byref(cnt)))
         return out
 
+    def param_gradients(self):
+        """(dE/dM [n, 10] of each atom's local-frame multipole, dE/dalpha [n]) of the last
+        evaluation (Thole damping fixed)."""
+        dM = np.zeros((self.n, 10))
+        dA = np.zeros(self.n)
+        self._check(self.lib.ffxg_param_grad(self._h, _dp(dM), _dp(dA)))
+        return dM, dA
+
+    @staticmethod
+    def per_type(values: np.ndarray, types: np.ndarray) -> dict:
+        """Sum per-atom parameter gradients over atoms of each type: {type: sum}."""
+        types = np.asarray(types)
+        return {int(t): values[types == t].sum(axis=0) for t in np.unique(types)}
+
     def set_image_mode(self, all_images: bool) -> None:
         """Force lists of every lattice image (True) or return to the automatic choice."""
         self._check(self.lib.ffxg_set_image_mode(self._h, 1 if all_images else 0))

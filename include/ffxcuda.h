@@ -191,6 +191,17 @@ int ffxg_get_neighbor_pairs(ffxg_handle *h, int32_t *pairs, int64_t *n_pairs);
  * order; n = 0 outside multi-image mode.  rows may be NULL to count. */
 int ffxg_get_neighbor_images(ffxg_handle *h, int32_t *rows, int64_t *n_rows);
 
+/* Parameter gradients of the last evaluation (the differentiation counterpart of the
+ * reference's parameter fitting; it has no analytic equivalent to cite): dEdM[n][10] is
+ * dE/dM of each atom's LOCAL-frame multipole in the component order of
+ * ffxg_system.multipole (charge, dipole x y z, quadrupole xx yy zz xy xz yz, each
+ * off-diagonal element counted once), dEdalpha[n] dE/d(polarizability) with the Thole
+ * damping held fixed.  The permanent energy is bilinear in the multipoles; for
+ * E_pol = -1/2 electric E_d^T A^-1 E_p with A = alpha^-1 - T symmetric, the CR dipoles
+ * A^-1 E_p are the adjoint solution, so no further solve is needed.  Per-type gradients are
+ * sums over the atoms of a type.  Not available under electrostatic lambda. */
+int ffxg_param_grad(ffxg_handle *h, double *dEdM, double *dEdalpha);
+
 /* Lists of every lattice image inside the cutoffs.  AUTO (the default) uses them when an
  * edge is at most twice an interaction cutoff (max of vdW, real-space and preconditioner
  * cutoffs), the boxes the reference expands into a replicate supercell
