@@ -81,7 +81,7 @@ static int batch_capture(ffxg_batch &b, int key) {
     cudaGetLastError();
     return FFXG_ERR_CUDA;
   }
-  const cudaError_t ei = cudaGraphInstantiate(&b.exec[key], graph, 0);
+  const cudaError_t ei = cudaGraphInstantiate(&b.exec[key], graph, cudaGraphInstantiateFlagUseNodePriority);
   cudaGraphDestroy(graph);
   if (ei != cudaSuccess) {
     b.exec[key] = nullptr;

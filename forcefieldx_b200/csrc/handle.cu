@@ -195,10 +195,15 @@ static int create_impl(const ffxg_system *s, const ffxg_params *p, Handle &h) {
   CK(cudaGetDeviceProperties(&prop, dev));
   if (prop.major < 10) { h.err = "requires an sm_100 (Blackwell) device"; return FFXG_ERR_CUDA; }
   h.device = dev;
-  CK(cudaStreamCreateWithFlags(&h.stream, cudaStreamNonBlocking));
-  CK(cudaStreamCreateWithFlags(&h.side, cudaStreamNonBlocking));
-  CK(cudaStreamCreateWithFlags(&h.aux, cudaStreamNonBlocking));
-  CK(cudaStreamCreateWithFlags(&h.aux_side, cudaStreamNonBlocking));
+  // The PCG's mesh chain (spread, FFT, combine) is its critical path; the real-space pair
+  // field beside it runs on lower-priority streams so that it fills the SMs the chain
+  // leaves idle instead of taking them from it.
+  int prio_low = 0, prio_high = 0;
+  CK(cudaDeviceGetStreamPriorityRange(&prio_low, &prio_high));
+  CK(cudaStreamCreateWithPriority(&h.stream, cudaStreamNonBlocking, prio_high));
+  CK(cudaStreamCreateWithPriority(&h.side, cudaStreamNonBlocking, prio_high));
+  CK(cudaStreamCreateWithPriority(&h.aux, cudaStreamNonBlocking, prio_low));
+  CK(cudaStreamCreateWithPriority(&h.aux_side, cudaStreamNonBlocking, prio_low));
   CK(cudaEventCreateWithFlags(&h.ev_fork, cudaEventDisableTiming));
   CK(cudaEventCreateWithFlags(&h.ev_join, cudaEventDisableTiming));
 
@@ -651,7 +656,7 @@ static int capture_graph(Handle &h) {
     cudaGetLastError();
     return FFXG_ERR_CUDA;
   }
-  const cudaError_t ei = cudaGraphInstantiate(&h.graph_exec[key], graph, 0);
+  const cudaError_t ei = cudaGraphInstantiate(&h.graph_exec[key], graph, cudaGraphInstantiateFlagUseNodePriority);
   cudaGraphDestroy(graph);
   if (ei != cudaSuccess) {
     h.graph_exec[key] = nullptr;

@@ -150,10 +150,10 @@ __device__ __forceinline__ void field_term(T xr, T yr, T zr, T A, T B, const T *
 
 // Lane partials of the dipole field at atom i from the cached pair row: the displacement
 // and A, B of each pair stream in coalesced; only the neighbour's source record is
-// gathered.  T is double (plain form) or float (mixed form).  Each lane handles entries
-// a and a + 32 together so that both entries' loads are in flight; the summation order
-// stays a, a + 32, a + 64, ...
-template <typename T>
+// gathered.  T is double (plain form) or float (mixed form).  Each lane handles NU entries
+// (a, a + 32, ...) together so that all their loads are in flight at once (4 for the long
+// Ewald rows in the FP32 form, 2 otherwise); the summation order stays a, a + 32, a + 64, ...
+template <typename T, int NU>
 __device__ __forceinline__ void pair_field(int i, const int *__restrict__ lst, const int *__restrict__ lst_cnt, int cap,
                                            const PairRec<T> *__restrict__ pr, const T *__restrict__ pb,
                                            const T *__restrict__ rec, T *acc) {
@@ -161,19 +161,23 @@ __device__ __forceinline__ void pair_field(int i, const int *__restrict__ lst, c
   const int cnt = min(lst_cnt[i], cap);
   const size_t e0 = (size_t)i * cap;
   const int *row = lst + e0;
-  for (int a = lane; a < cnt; a += 64) {
-    const bool two = a + 32 < cnt;
-    const int a1 = two ? a + 32 : a;
-    const int k0 = row[a], k1 = row[a1];
-    T x0, y0, z0, A0, x1, y1, z1, A1;
-    load_pair(pr, e0 + a, x0, y0, z0, A0);
-    load_pair(pr, e0 + a1, x1, y1, z1, A1);
-    const T B0 = pb[e0 + a], B1 = pb[e0 + a1];
-    T s0[6], s1[6];
-    get_rec(rec, k0, s0);
-    get_rec(rec, k1, s1);
-    field_term(x0, y0, z0, A0, B0, s0, acc);
-    if (two) field_term(x1, y1, z1, A1, B1, s1, acc);
+  for (int a = lane; a < cnt; a += 32 * NU) {
+    int ix[NU], kk[NU];
+    T xx[NU], yy[NU], zz[NU], AA[NU], BB[NU], ss[NU][6];
+#pragma unroll
+    for (int u = 0; u < NU; u++) {
+      ix[u] = (a + 32 * u < cnt) ? a + 32 * u : a;
+      kk[u] = row[ix[u]];
+    }
+#pragma unroll
+    for (int u = 0; u < NU; u++) {
+      load_pair(pr, e0 + ix[u], xx[u], yy[u], zz[u], AA[u]);
+      BB[u] = pb[e0 + ix[u]];
+      get_rec(rec, kk[u], ss[u]);
+    }
+#pragma unroll
+    for (int u = 0; u < NU; u++)
+      if (a + 32 * u < cnt) field_term(xx[u], yy[u], zz[u], AA[u], BB[u], ss[u], acc);
   }
 }
 
@@ -231,7 +235,7 @@ __global__ void __launch_bounds__(kFieldThreads) k_pair_field(int n, const int *
   const int wstride = gridDim.x * (blockDim.x >> 5);
   for (int i = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5); i < n; i += wstride) {
     T a6[6] = {0, 0, 0, 0, 0, 0};
-    pair_field(i, ewl, ewl_cnt, capE, coefE, coefEB, rec, a6);
+    pair_field<T, 2>(i, ewl, ewl_cnt, capE, coefE, coefEB, rec, a6);
     double f[6];
 #pragma unroll
     for (int q = 0; q < 6; q++) f[q] = warp_sum((double)a6[q]);
@@ -335,7 +339,7 @@ __global__ void __launch_bounds__(kFieldThreads) k_pcg_precond(
   double acc[2] = {0, 0};
   for (int i = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5); i < n; i += wstride) {
     T a6[6] = {0, 0, 0, 0, 0, 0};
-    pair_field(i, prl, prl_cnt, capP, coefP, coefPB, recP, a6);
+    pair_field<T, 2>(i, prl, prl_cnt, capP, coefP, coefPB, recP, a6);
     double f[6];
 #pragma unroll
     for (int q = 0; q < 6; q++) f[q] = warp_sum((double)a6[q]);
