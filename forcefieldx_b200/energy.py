@@ -249,3 +249,40 @@ class ForceFieldEnergy:
 
     def launch_count(self) -> int:
         return int(self.lib.ffxg_last_launch_count(self._h))
+
+
+class CrystalEnergy:
+    """Energy and gradient of an asymmetric unit in a space group with an orthorhombic cell,
+    evaluated as the P1 unit cell of its symmetry mates (forcefieldx_b200.ffxio): the
+    reference sums the asymmetric unit's interactions with its mates
+    (ParticleMeshEwald / NeighborList symmetry loops); the cell of mates has the same
+    energy per asymmetric unit, and the asymmetric unit's gradient is the first mate's."""
+
+    def __init__(self, asu_system: AmoebaSystem, params: AmoebaParams, space_group: str):
+        from .ffxio import SPACE_GROUPS, expand_system
+        self.space_group = space_group
+        self.n_asu = asu_system.n_atoms
+        self.n_symm = len(SPACE_GROUPS[space_group])
+        self.box = params.box
+        self.cell = expand_system(asu_system, params.box, space_group)
+        self.ffe = ForceFieldEnergy(self.cell, params)
+
+    def close(self):
+        self.ffe.close()
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    def energy_and_gradient(self, x_asu=None):
+        """(energy per asymmetric unit, gradient [n_asu, 3]) at the asymmetric unit's coordinates."""
+        from .ffxio import expand_coordinates
+        x = None if x_asu is None else expand_coordinates(x_asu, self.box, self.space_group)
+        e, g = self.ffe.energy_and_gradient(x)
+        return e / self.n_symm, g[:self.n_asu].copy()
+
+    @property
+    def terms(self) -> np.ndarray:
+        return self.ffe.terms / self.n_symm

@@ -16,9 +16,13 @@ AMOEBA parameter (.prm) files, resolved into an AmoebaSystem + AmoebaParams.
     vdW          nonbonded/VanDerWaals.java:1421-1433 (reduction toward the single bonded
                  atom), VanDerWaalsForm.java:355-470 (class tables, vdwpr)
     keys         box (a-axis, b-axis, c-axis), vdw-cutoff, ewald-cutoff, ewald-alpha,
-                 pme-order, pme-grid or pme-mesh-density, polar-eps, polarization
-(paths under modules/potential/src/main/java/ffx/potential/).  Only orthorhombic P1
-boxes reach the library; other space groups are rejected.
+                 pme-order, pme-grid or pme-mesh-density / pme-spacing, polar-eps,
+                 polarization, spacegroup
+(paths under modules/potential/src/main/java/ffx/potential/).  Space groups with an
+orthorhombic cell are expanded to the P1 cell of their symmetry mates (unit_cell): the
+reference sums the asymmetric unit's interactions with its mates
+(C/SpaceGroup, ParticleMeshEwald symmetry loops); the cell of mates has the same energy
+per asymmetric unit.
 """
 from __future__ import annotations
 
@@ -30,7 +34,7 @@ import numpy as np
 
 from .system import (FRAME_BISECTOR, FRAME_NONE, FRAME_THREEFOLD, FRAME_ZONLY, FRAME_ZTHENBISECTOR, FRAME_ZTHENX,
                      POLAR_DIRECT, POLAR_MUTUAL, POLAR_NONE, AmoebaParams, AmoebaSystem, combine_vdw,
-                     connectivity_lists, pack_multipole_bohr, pme_grid_dim)
+                     connectivity_lists, pack_multipole_bohr, pme_grid_dim, tile_system)
 
 
 def read_prm(path):
@@ -235,11 +239,55 @@ def write_xyz(path, xyz, types, bonds, names=None, title="") -> None:
             f.write(f"{a + 1:6d}  {name:<3s}{xyz[a, 0]:12.6f}{xyz[a, 1]:12.6f}{xyz[a, 2]:12.6f}{int(types[a]):6d}{links}\n")
 
 
+# Symmetry operators (fractional: x' = R x + t) of the space groups whose unit cell is
+# orthorhombic, the only cells the library takes; standard settings of the International
+# Tables, in the order Force Field X lists them for its P1 expansion of P212121
+# (the reference's 1n7s.P212121 / 1n7s.P1 test pair).
+def _op(r, t):
+    return (np.array(r, dtype=np.float64), np.array(t, dtype=np.float64))
+
+
+SPACE_GROUPS = {
+    "P1": [_op(np.eye(3), (0, 0, 0))],
+    "P222": [_op(np.eye(3), (0, 0, 0)), _op(np.diag([-1, -1, 1]), (0, 0, 0)),
+             _op(np.diag([-1, 1, -1]), (0, 0, 0)), _op(np.diag([1, -1, -1]), (0, 0, 0))],
+    "P2221": [_op(np.eye(3), (0, 0, 0)), _op(np.diag([-1, -1, 1]), (0, 0, 0.5)),
+              _op(np.diag([-1, 1, -1]), (0, 0, 0.5)), _op(np.diag([1, -1, -1]), (0, 0, 0))],
+    "P21212": [_op(np.eye(3), (0, 0, 0)), _op(np.diag([-1, -1, 1]), (0, 0, 0)),
+               _op(np.diag([-1, 1, -1]), (0.5, 0.5, 0)), _op(np.diag([1, -1, -1]), (0.5, 0.5, 0))],
+    "P212121": [_op(np.eye(3), (0, 0, 0)), _op(np.diag([-1, -1, 1]), (0.5, 0, 0.5)),
+                _op(np.diag([1, -1, -1]), (0.5, 0.5, 0)), _op(np.diag([-1, 1, -1]), (0, 0.5, 0.5))],
+}
+
+
+def space_group(key: Dict[str, List[str]]) -> str:
+    sg = key.get("spacegroup", ["P1"])[0].upper().replace(" ", "")
+    if sg not in SPACE_GROUPS:
+        raise ValueError(f"space group {sg}: supported are {sorted(SPACE_GROUPS)} (orthorhombic cells)")
+    return sg
+
+
+def expand_coordinates(xyz, box, sg: str) -> np.ndarray:
+    """Coordinates of the unit cell's symmetry mates of an asymmetric unit, mate after mate
+    (x_frac' = R x_frac + t; no wrapping, the energy is periodic)."""
+    xyz = np.asarray(xyz, dtype=np.float64).reshape(-1, 3)
+    box = np.asarray(box, dtype=np.float64)
+    frac = xyz / box
+    return np.concatenate([((frac @ R.T) + t) * box for R, t in SPACE_GROUPS[sg]])
+
+
+def expand_system(system: AmoebaSystem, box, sg: str) -> AmoebaSystem:
+    """A resolved asymmetric-unit system expanded to the P1 cell of its symmetry mates
+    (attributes n_symm, n_asu set)."""
+    cell = tile_system(system, expand_coordinates(system.xyz, box, sg), len(SPACE_GROUPS[sg]))
+    cell.n_symm = len(SPACE_GROUPS[sg])
+    cell.n_asu = system.n_atoms
+    return cell
+
+
 def params_from_key(key: Dict[str, List[str]], **overrides) -> AmoebaParams:
     """AmoebaParams from a key file's keywords (ForceFieldEnergy / PME defaults otherwise)."""
-    sg = key.get("spacegroup", ["P1"])[0].upper()
-    if sg not in ("P1",):
-        raise ValueError(f"space group {sg}: only P1 boxes are supported")
+    space_group(key)
     for ang in ("alpha", "beta", "gamma"):
         if ang in key and abs(float(key[ang][0]) - 90.0) > 1e-9:
             raise ValueError("only orthorhombic boxes are supported")
@@ -297,11 +345,13 @@ def system_from_types(xyz, types, bonds, prm) -> AmoebaSystem:
                         ip11=ip11)
 
 
-def load_system(xyz_path: str, key_path: str, prm_path: Optional[str] = None,
+def load_system(xyz_path: str, key_path: str, prm_path: Optional[str] = None, expand_symmetry: bool = True,
                 **overrides) -> Tuple[AmoebaSystem, AmoebaParams]:
     """An FFX structure: coordinates and topology from the XYZ file, keys from the key
     file, parameters from ``prm_path`` (else the key file's ``parameters`` keyword,
-    relative to the key file)."""
+    relative to the key file).  A space group other than P1 is expanded to the P1 unit
+    cell of the symmetry mates (see unit_cell); the returned system then carries the
+    attributes n_symm and n_asu."""
     key = read_key(key_path)
     if prm_path is None:
         if "parameters" not in key:
@@ -310,5 +360,26 @@ def load_system(xyz_path: str, key_path: str, prm_path: Optional[str] = None,
         if not os.path.isabs(prm_path):
             prm_path = os.path.join(os.path.dirname(os.path.abspath(key_path)), prm_path)
     xyz, types, bonds = read_xyz(xyz_path)
+    params = params_from_key(key, **overrides)
+    sg = space_group(key)
+    n_asu = len(types)
+    if expand_symmetry and sg != "P1":
+        xyz, types, bonds = unit_cell(xyz, types, bonds, params.box, sg)
     system = system_from_types(xyz, types, bonds, read_prm(prm_path))
-    return system, params_from_key(key, **overrides)
+    system.n_symm = len(types) // n_asu
+    system.n_asu = n_asu
+    return system, params
+
+
+def unit_cell(xyz, types, bonds, box, sg: str):
+    """The P1 unit cell of an asymmetric unit: every symmetry mate's atoms (types and bonds
+    repeated with the atom offset of the mate).  The crystal energy per asymmetric unit is
+    the cell's energy over the number of mates, and the asymmetric unit's gradient is the
+    first mate's rows of the cell's gradient (the mates are images of one another)."""
+    n = len(types)
+    ops = SPACE_GROUPS[sg]
+    cell_xyz = expand_coordinates(xyz, box, sg)
+    cell_types = np.concatenate([np.asarray(types)] * len(ops))
+    b = np.asarray(bonds, dtype=np.int64).reshape(-1, 2)
+    cell_bonds = np.concatenate([b + m * n for m in range(len(ops))])
+    return cell_xyz, cell_types, cell_bonds

@@ -391,10 +391,16 @@ def replicate(system: AmoebaSystem, edge, reps=(2, 2, 2)) -> AmoebaSystem:
     indices offset per copy (the expansion C/ReplicatesCrystal.java:172-202 describes).
     Copy m = (k * reps[1] + j) * reps[0] + i holds atoms m*n .. m*n + n - 1."""
     edge = np.broadcast_to(np.asarray(edge, dtype=np.float64), (3,))
-    n = system.n_atoms
     copies = [(i, j, k) for k in range(reps[2]) for j in range(reps[1]) for i in range(reps[0])]
-    nc = len(copies)
     xyz = np.concatenate([system.xyz + np.array(c) * edge for c in copies])
+    return tile_system(system, xyz, len(copies))
+
+
+def tile_system(system: AmoebaSystem, xyz: np.ndarray, nc: int) -> AmoebaSystem:
+    """``nc`` copies of a system with the given coordinates ([nc * n, 3], copy after copy):
+    per-atom parameters repeated, connectivity and frame indices offset per copy.  Local
+    frame multipoles need no change (each copy's frames follow its own atoms)."""
+    n = system.n_atoms
     tile = lambda a: np.concatenate([a] * nc)  # noqa: E731
     axis = np.concatenate([np.where(system.axis >= 0, system.axis + m * n, -1) for m in range(nc)]).astype(np.int32)
     red_parent = np.concatenate([system.red_parent + m * n for m in range(nc)]).astype(np.int32)

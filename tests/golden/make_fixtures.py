@@ -30,10 +30,11 @@ import numpy as np
 HERE = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, os.path.dirname(os.path.dirname(HERE)))
 
-from forcefieldx_b200.ffxio import read_key, read_prm, read_xyz, system_from_types  # noqa: E402
+from forcefieldx_b200.ffxio import read_key, read_prm, read_xyz, space_group, system_from_types  # noqa: E402
 from forcefieldx_b200.system import pme_grid_dim  # noqa: E402
 
 PRM = "modules/potential/src/main/java/ffx/potential/parameters/ff/AMOEBA_BIO_2009"
+PRM_PROTEIN = "modules/potential/src/main/java/ffx/potential/parameters/ff/AMOEBA_PROTEIN_2004"
 RES = "modules/potential/src/test/resources"
 ENERGY_TEST = "modules/potential/src/test/java/ffx/potential/commands/EnergyTest.java"
 
@@ -70,7 +71,7 @@ def build(ref_root, name, xyz_file, key_file, prm):
                 ewald_alpha=float(key["ewald-alpha"][0]), pme_order=int(key.get("pme-order", ["5"])[0]),
                 pme_grid=grid, polar_eps=float(key.get("polar-eps", ["1e-6"])[0]))
     return dict(keys=keys, golden=golden_from_energy_test(os.path.join(ref_root, ENERGY_TEST), xyz_file),
-                n_atoms=n, ip11_symmetric=bool(sym),
+                n_atoms=n, ip11_symmetric=bool(sym), space_group=space_group(key),
                 frames={str(f): int((system.frame == f).sum()) for f in range(6)})
 
 
@@ -105,6 +106,11 @@ def main():
                                      ("ubiquitin", "ubiquitin.xyz", "ubiquitin.key")):
         out[name] = build(ref_root, name, xyz_file, key_file, prm)
         print(name, json.dumps(out[name]))
+    # SNARE in P212121 (EnergyTest.java:70-104): the asymmetric unit; tests expand it to
+    # the P1 cell of its four mates (forcefieldx_b200.ffxio.expand_system).
+    prm_protein = read_prm(os.path.join(ref_root, PRM_PROTEIN))
+    out["snare"] = build(ref_root, "snare", "1n7s.P212121.xyz", "1n7s.P212121.key", prm_protein)
+    print("snare", json.dumps(out["snare"]))
     out["numerics"] = numerics_known_answers(ref_root)
     print("numerics", len(out["numerics"]["erf"]), "erf cases,", len(out["numerics"]["bspline"]), "bspline cases")
     with open(os.path.join(HERE, "fixtures.json"), "w") as f:

@@ -5,6 +5,8 @@
    same oracle energy.
 2. The reference's own DHFR inputs (XYZ, key, AMOEBA_BIO_2009), where present, resolve to
    the committed golden system (tests/golden/dhfr_system.npz) exactly.
+3. Its SNARE asymmetric unit in P212121, expanded by the four symmetry operators, is the
+   reference's own P1 file of the same crystal (1n7s.P1.xyz) up to lattice translations.
 """
 import os
 
@@ -78,3 +80,20 @@ def test_dhfr_reference_inputs_resolve_to_golden_system():
         assert np.array_equal(np.asarray(getattr(got, f)), np.asarray(getattr(want, f))), f
     assert [list(v) for v in got.ip11] == [list(v) for v in want.ip11]
     assert p.ewald_cutoff == 6.7 and p.ewald_alpha == 0.57
+
+
+@pytest.mark.skipif(not os.path.isdir(REFERENCE), reason="reference source tree not present")
+def test_p212121_expansion_is_the_reference_p1_cell():
+    """The P212121 asymmetric unit expanded by the four symmetry operators gives the atoms
+    of the reference's own P1 file (1n7s.P1.xyz), mate after mate, up to lattice
+    translations of whole atoms."""
+    from forcefieldx_b200.ffxio import expand_coordinates, read_key
+    res = os.path.join(REFERENCE, "modules/potential/src/test/resources")
+    xyz, types, _ = read_xyz(os.path.join(res, "1n7s.P212121.xyz"))
+    key = read_key(os.path.join(res, "1n7s.P212121.key"))
+    box = np.array([float(key["a-axis"][0]), float(key["b-axis"][0]), float(key["c-axis"][0])])
+    cell = expand_coordinates(xyz, box, "P212121")
+    ref, rtypes, _ = read_xyz(os.path.join(res, "1n7s.P1.xyz"))
+    d = (cell - ref) / box
+    assert np.abs(d - np.round(d)).max() < 1e-6
+    assert list(rtypes) == list(types) * 4

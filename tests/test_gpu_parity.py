@@ -62,15 +62,18 @@ def test_water_648_buffered_list_beyond_half_box():
     compare(s, p)
 
 
-@pytest.mark.parametrize("name", ["ubiquitin", "dhfr"])
+@pytest.mark.parametrize("name", ["ubiquitin", "dhfr", "snare"])
 def test_reference_golden(name, fixtures):
+    """DHFR and ubiquitin in P1; SNARE in P212121 as the P1 cell of its four mates, whose
+    energy per asymmetric unit is the reference's P212121 golden."""
     s, p = golden_system(name, fixtures)
     terms, counts, _, _ = compare(s, p)
     gold = fixtures[name]["golden"]
-    assert abs(terms[0] - gold["vdw"]) < gold["tolerance"]
-    assert abs(terms[1] - gold["permanent"]) < gold["tolerance"]
-    assert abs(terms[2] - gold["polarization"]) < gold["tolerance"]
-    assert counts[0] == gold["n_vdw"] and counts[1] == gold["n_permanent"]
+    m = s.n_symm
+    assert abs(terms[0] / m - gold["vdw"]) < gold["tolerance"]
+    assert abs(terms[1] / m - gold["permanent"]) < gold["tolerance"]
+    assert abs(terms[2] / m - gold["polarization"]) < gold["tolerance"]
+    assert counts[0] == m * gold["n_vdw"] and counts[1] == m * gold["n_permanent"]
 
 
 def test_water_24k():
@@ -173,3 +176,19 @@ def test_graph_replay_reports_scf_errors():
             with pytest.raises(EnergyException) as ei:
                 ffe.energy(s.xyz)
             assert ei.value.status == 4         # SCF_MAXITER, decided on the device
+
+
+def test_crystal_energy_p212121(fixtures):
+    """CrystalEnergy on the SNARE asymmetric unit: energy per asymmetric unit and its
+    gradient, against the oracle's P1 cell of the four mates."""
+    from forcefieldx_b200.energy import CrystalEnergy
+    from forcefieldx_b200.system import AmoebaSystem
+    from tests.common import GOLDEN
+    import os
+    asu = AmoebaSystem.load_npz(os.path.join(GOLDEN, "snare_system.npz"))
+    cell, p = golden_system("snare", fixtures)
+    ref = ob.energy(cell, p)
+    with CrystalEnergy(asu, p, "P212121") as ce:
+        e, g = ce.energy_and_gradient(asu.xyz)
+    assert abs(e - ref["terms"][9] / 4) < 1e-8 * abs(ref["terms"][9] / 4)
+    assert float(np.sqrt(np.mean((g - ref["grad"][:asu.n_atoms]) ** 2))) < 1e-6

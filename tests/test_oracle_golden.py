@@ -2,8 +2,8 @@
 
 EnergyTest.java (modules/potential/src/test/java/ffx/potential/commands/EnergyTest.java)
 asserts per-term energies to 1e-2 kcal/mol and exact interaction counts for DHFR
-(:147-182) and ubiquitin (:363-398); tests/golden/make_fixtures.py resolved the
-same inputs into tests/golden/*_system.npz.
+(:147-182), ubiquitin (:363-398) and SNARE in P212121 (:70-104, AMOEBA_PROTEIN_2004);
+tests/golden/make_fixtures.py resolved the same inputs into tests/golden/*_system.npz.
 """
 import pytest
 
@@ -11,16 +11,18 @@ from oracle import binding as ob
 from tests.common import golden_system
 
 
-@pytest.mark.parametrize("name", ["ubiquitin", "dhfr"])
+@pytest.mark.parametrize("name", ["ubiquitin", "dhfr", "snare"])
 def test_oracle_matches_reference_golden(name, fixtures):
+    """SNARE (EnergyTest.java:70-104) is the P212121 asymmetric unit, evaluated as the P1
+    cell of its four mates: energies and counts per asymmetric unit."""
     system, params = golden_system(name, fixtures)
     g = fixtures[name]["golden"]
     tol = g["tolerance"]
     r = ob.energy(system, params, gradient=False)
     assert r["status"] == 0
-    t, c = r["terms"], r["counts"]
+    t, c = r["terms"] / system.n_symm, r["counts"]
     assert abs(t[0] - g["vdw"]) < tol
     assert abs(t[1] - g["permanent"]) < tol
     assert abs(t[2] - g["polarization"]) < tol
-    assert c[0] == g["n_vdw"]
-    assert c[1] == g["n_permanent"]
+    assert c[0] == system.n_symm * g["n_vdw"]
+    assert c[1] == system.n_symm * g["n_permanent"]
