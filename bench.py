@@ -377,6 +377,39 @@ def run_reference(args):
     }))
 
 
+def run_lambda(args):
+    """Electrostatic + vdW lambda evaluations of the 24k box (a 30-atom soft subset, OST:
+    three evaluations per call plus the vacuum sub-system), timed on the device per call
+    through the public API with host buffers: one JSON line per precision form."""
+    import torch
+    from forcefieldx_b200.energy import ForceFieldEnergy
+    from forcefieldx_b200.system import Alchemy
+    torch.cuda.set_device(0)
+    system = build_system()
+    n = system.n_atoms
+    soft = np.zeros(n, dtype=np.int32)
+    soft[:30] = 1
+    alch = Alchemy(soft=soft, molecule=np.arange(n) // 3, elec=True)
+    out = {"workload": WORKLOAD + "; elec-lambdaterm on 30 soft atoms (10 waters)", "lambda": {}}
+    for name, prec in (("mixed", PRECISION_MIXED), ("fp64", PRECISION_FP64)):
+        with ForceFieldEnergy(system, build_params(prec)) as ffe:
+            ffe.set_alchemy(alch)
+            res = {}
+            for lam in args.lambda_values:
+                ffe.set_lambda(lam)
+                for _ in range(args.warmup):
+                    ffe.energy_and_gradient(system.xyz)
+                t0 = time.perf_counter()
+                for _ in range(args.steps):
+                    e, _ = ffe.energy_and_gradient(system.xyz)
+                dt = (time.perf_counter() - t0) / args.steps
+                d1, _, _ = ffe.get_dEdL()
+                res[str(lam)] = {"evals_per_s": 1.0 / dt, "ms_per_eval": 1e3 * dt, "energy": e, "dEdL": d1,
+                                 "pcg_iterations": int(ffe.count("scf_iter"))}
+            out["lambda"][name] = res
+    print(json.dumps(out))
+
+
 def run_accuracy(args):
     """Mixed form vs FP64 on frames of a 300 K trajectory of the 24k box.
 
@@ -455,12 +488,17 @@ def main():
     ap.add_argument("--batch-systems", type=int, default=512,
                     help="also time a batch of this many small systems (0: skip)")
     ap.add_argument("--batch-steps", type=int, default=5)
+    ap.add_argument("--lambda-values", type=float, nargs="*", default=None,
+                    help="instead of the headline, time electrostatic lambda evaluations at these lambdas")
     ap.add_argument("--accuracy-frames", type=int, default=0,
                     help="instead of timing, report the mixed form's error on this many trajectory frames")
     ap.add_argument("--accuracy-equil", type=int, default=200, help="equilibration steps before the first frame")
     args = ap.parse_args()
     if args.accuracy_frames > 0:
         run_accuracy(args)
+        return
+    if args.lambda_values:
+        run_lambda(args)
         return
     if args.warmup < 3 and args.impl == "mine":
         args.warmup = 3
