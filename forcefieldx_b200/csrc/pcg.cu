@@ -390,10 +390,36 @@ __global__ void k_pcg_reset(PcgState *st) {
 template <typename T>
 __global__ void __launch_bounds__(kVecThreads) k_pcg_update(
     int n, const double *__restrict__ vec, const double *__restrict__ vecP, const double *__restrict__ p,
-    const double *__restrict__ pP, double *r, double *rP, double *uD, double *uP, const double *__restrict__ tot,
+    const double *__restrict__ pP, double *r, double *rP, double *uD, double *uP, double *tot,
     double *partE, unsigned *counter, PcgState *st, int max_iter, double polar_eps, const int *flags,
-    cudaGraphConditionalHandle cond, int use_cond, const double *__restrict__ polar, T *recP, int n_eps) {
-  const double pap = tot[T_PAP], papP = tot[T_PAPP], rz = tot[T_RZ], rzP = tot[T_RZP];
+    cudaGraphConditionalHandle cond, int use_cond, const double *__restrict__ polar, T *recP, int n_eps,
+    const double *__restrict__ partC, int rowsC) {
+  // p.Ap and r.z of both systems: every block sums the combine's partial rows itself, in
+  // one fixed order (so every block holds the same values), instead of a separate totals
+  // launch on the critical path; block 0 keeps them for the next beta.
+  __shared__ double tsum[4][kVecThreads / 32];
+  __shared__ double tv[4];
+  {
+    double s4[4] = {0.0, 0.0, 0.0, 0.0};
+    for (int b = threadIdx.x; b < rowsC; b += blockDim.x)
+#pragma unroll
+      for (int q = 0; q < 4; q++) s4[q] += partC[b * 8 + q];
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+#pragma unroll
+    for (int q = 0; q < 4; q++) {
+      const double w = warp_sum(s4[q]);
+      if (lane == 0) tsum[q][wid] = w;
+    }
+    __syncthreads();
+    if (threadIdx.x < 4) {
+      double t = 0.0;
+      for (int w = 0; w < (int)(blockDim.x >> 5); w++) t += tsum[threadIdx.x][w];
+      tv[threadIdx.x] = t;
+      if (blockIdx.x == 0) tot[T_PAP + threadIdx.x] = t;
+    }
+    __syncthreads();
+  }
+  const double pap = tv[0], papP = tv[1], rz = tv[2], rzP = tv[3];
   const double alpha0 = (pap != 0.0) ? rz / pap : rz;
   const double alpha1 = (papP != 0.0) ? rzP / papP : rzP;
   double v[2] = {0.0, 0.0};
@@ -518,6 +544,12 @@ int pcg_partial_rows(int n) {
 }
 static double *part_region(const Handle &h, int k) { return h.d_part2 + (size_t)k * h.part_rows * 8; }
 
+// beta = r.z_new / r.z_old from the preconditioner's partial rows (the totals kernel).
+static void beta_totals(Handle &h, cudaStream_t st) {
+  k_pcg_totals<2, true><<<1, 1024, 0, st>>>(part_region(h, 1), field_blocks(h.n), h.d_scalars, T_RZN);
+  FFX_LAUNCHED(h);
+}
+
 template <typename T>
 static void pair_field_launch(Handle &h, cudaStream_t st) {
   k_pair_field<T><<<field_blocks(h.n), kFieldThreads, 0, st>>>(
@@ -538,11 +570,6 @@ static void combine(Handle &h, const double *vD, const double *vP, bool first, d
       vP, aewald3_of(h), h.d_polar, h.d_udirD, h.d_udirP, h.d_p, h.d_pP, h.d_tp, first ? 1 : 0, h.d_r, h.d_rP, outD,
       outP, reinterpret_cast<T *>(h.d_recP), part_region(h, 0), h.d_counter + K_FIELD, h.d_scalars);
   FFX_LAUNCHED(h);
-  if (MODE == 2) {
-    k_pcg_totals<4, false><<<1, 1024, 0, h.stream>>>(part_region(h, 0), nblocks((int64_t)h.n * 32, 256), h.d_scalars,
-                                                   T_PAP);
-    FFX_LAUNCHED(h);
-  }
 }
 
 // The full field of (vD, vP), whose source record is in d_recF: the pair field on the
@@ -575,10 +602,9 @@ static void precond(Handle &h) {
       h.prm.precond_scale, h.d_zpre, h.d_zpreP, h.d_p, h.d_pP, reinterpret_cast<T *>(h.d_recF), part_region(h, 1),
       h.d_counter + K_PRECOND, h.d_scalars);
   FFX_LAUNCHED(h);
-  if (!INIT) {
-    k_pcg_totals<2, true><<<1, 1024, 0, h.stream>>>(part_region(h, 1), field_blocks(h.n), h.d_scalars, T_RZN);
-    FFX_LAUNCHED(h);
-  }
+  // On the main stream: on the low-priority side stream the one-block totals wait for the
+  // spread to drain and hold back the pair field behind them (measured slower).
+  if (!INIT) beta_totals(h, h.stream);
 }
 
 template <bool INIT>
@@ -591,7 +617,8 @@ static void update(Handle &h, cudaGraphConditionalHandle cond, int use_cond) {
   k_pcg_update<T><<<vec_blocks(h.n), kVecThreads, 0, h.stream>>>(
       h.n, h.d_vec, h.d_vecP, h.d_p, h.d_pP, h.d_r, h.d_rP, h.d_uD, h.d_uP, h.d_scalars, part_region(h, 2),
       h.d_counter + K_UPDATE, h.d_pcg, h.prm.max_scf_iter, h.prm.polar_eps, h.d_flags, cond, use_cond, h.d_polar,
-      reinterpret_cast<T *>(h.d_recP), h.eps_atoms > 0 ? h.eps_atoms : h.n);
+      reinterpret_cast<T *>(h.d_recP), h.eps_atoms > 0 ? h.eps_atoms : h.n, part_region(h, 0),
+      nblocks((int64_t)h.n * 32, 256));
   FFX_LAUNCHED(h);
 }
 
