@@ -409,6 +409,11 @@ struct Handle {
   bool use_graphs = true;
   bool want_grad = true;                            // gradient requested by the current call
   cudaStream_t side = nullptr;                      // captures the PCG while-node body
+  // Captured evaluations run the vdW term (independent of electrostatics) on its own
+  // low-priority stream beside the permanent field and the PCG, joined before the gradient.
+  bool capturing = false;
+  cudaStream_t vdw_stream = nullptr;
+  cudaEvent_t ev_vdw_fork = nullptr, ev_vdw_join = nullptr;
   cudaGraphExec_t graph_exec[2] = {nullptr, nullptr};
   int64_t graph_launches[2] = {0, 0};               // kernels outside the PCG body
   int64_t graph_body_launches = 0;
@@ -434,7 +439,7 @@ constexpr int kEnergyRows = 11;
 // ---- kernels / launchers (defined in the .cu files)
 void launch_set_coordinates(Handle &h, const double *d_xyz);
 void launch_neighbor_list(Handle &h, bool force);
-void launch_vdw(Handle &h, bool grad);
+void launch_vdw(Handle &h, bool grad, cudaStream_t st);
 void launch_rotate(Handle &h);
 void launch_bsplines(Handle &h);
 void launch_spread_permanent(Handle &h);

@@ -204,8 +204,11 @@ static int create_impl(const ffxg_system *s, const ffxg_params *p, Handle &h) {
   CK(cudaStreamCreateWithPriority(&h.side, cudaStreamNonBlocking, prio_high));
   CK(cudaStreamCreateWithPriority(&h.aux, cudaStreamNonBlocking, prio_low));
   CK(cudaStreamCreateWithPriority(&h.aux_side, cudaStreamNonBlocking, prio_low));
+  CK(cudaStreamCreateWithPriority(&h.vdw_stream, cudaStreamNonBlocking, prio_low));
   CK(cudaEventCreateWithFlags(&h.ev_fork, cudaEventDisableTiming));
   CK(cudaEventCreateWithFlags(&h.ev_join, cudaEventDisableTiming));
+  CK(cudaEventCreateWithFlags(&h.ev_vdw_fork, cudaEventDisableTiming));
+  CK(cudaEventCreateWithFlags(&h.ev_vdw_join, cudaEventDisableTiming));
 
   h.box.a = p->box[0]; h.box.b = p->box[1]; h.box.c = p->box[2];
   h.box.A00 = 1.0 / h.box.a; h.box.A11 = 1.0 / h.box.b; h.box.A22 = 1.0 / h.box.c;
@@ -447,8 +450,11 @@ static void free_all(Handle &h) {
   if (h.side) cudaStreamDestroy(h.side);
   if (h.aux) cudaStreamDestroy(h.aux);
   if (h.aux_side) cudaStreamDestroy(h.aux_side);
+  if (h.vdw_stream) cudaStreamDestroy(h.vdw_stream);
   if (h.ev_fork) cudaEventDestroy(h.ev_fork);
   if (h.ev_join) cudaEventDestroy(h.ev_join);
+  if (h.ev_vdw_fork) cudaEventDestroy(h.ev_vdw_fork);
+  if (h.ev_vdw_join) cudaEventDestroy(h.ev_vdw_join);
   if (h.stream) cudaStreamDestroy(h.stream);
 }
 
@@ -462,9 +468,18 @@ static void emit_front(Handle &h, const double *d_xyz) {
   launch_set_coordinates(h, d_xyz);
   launch_neighbor_list(h, false);
   timer_end(h, tk);
-  tk = timer_begin(h, FFXG_STAGE_VDW);
-  launch_vdw(h, h.want_grad);
-  timer_end(h, tk);
+  if (h.capturing && !h.vacuum) {
+    // A branch of the graph: vdW depends on the list alone, and only the gradient
+    // assembly and the sums read it (emit_back joins it there).
+    cudaEventRecord(h.ev_vdw_fork, h.stream);
+    cudaStreamWaitEvent(h.vdw_stream, h.ev_vdw_fork, 0);
+    launch_vdw(h, h.want_grad, h.vdw_stream);
+    cudaEventRecord(h.ev_vdw_join, h.vdw_stream);
+  } else {
+    tk = timer_begin(h, FFXG_STAGE_VDW);
+    launch_vdw(h, h.want_grad, h.stream);
+    timer_end(h, tk);
+  }
   tk = timer_begin(h, FFXG_STAGE_MULTIPOLES);
   launch_rotate(h);
   launch_bsplines(h);
@@ -499,6 +514,7 @@ static void emit_back(Handle &h, double *d_grad_xyz) {
   tk = timer_begin(h, FFXG_STAGE_RECIP_ENERGY);
   launch_recip_energy(h, h.want_grad);
   timer_end(h, tk);
+  if (h.capturing && !h.vacuum) cudaStreamWaitEvent(h.stream, h.ev_vdw_join, 0);
   tk = timer_begin(h, FFXG_STAGE_GRADIENT);
   if (h.want_grad) {
     launch_torque(h);
@@ -628,6 +644,7 @@ namespace ffx {
 int eval_capture_body(Handle &h, const double *d_xyz, double *d_grad) {
   const int key = h.want_grad ? 1 : 0;
   const int64_t before = h.launches;
+  h.capturing = true;
   emit_front(h, d_xyz);
   int st = FFXG_OK;
   if (h.prm.polarization != FFXG_POLAR_NONE) {
@@ -637,6 +654,7 @@ int eval_capture_body(Handle &h, const double *d_xyz, double *d_grad) {
     emit_no_polarization(h);
   }
   emit_back(h, d_grad);
+  h.capturing = false;
   cudaMemcpyAsync(h.h_pcg, h.d_pcg, sizeof(PcgState), cudaMemcpyDeviceToHost, h.stream);
   h.graph_launches[key] = h.launches - before - h.graph_body_launches;
   return st;

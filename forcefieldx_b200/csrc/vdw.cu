@@ -197,7 +197,7 @@ __global__ void k_vdw_distribute(int n, const double *__restrict__ gred, const i
 }
 
 
-void launch_vdw(Handle &h, bool grad) {
+void launch_vdw(Handle &h, bool grad, cudaStream_t st) {
   if (h.vacuum) return;   // a vacuum sub-system carries electrostatics only
   VdwForm vf{};
   const double off = h.prm.vdw_cutoff, cut = h.prm.vdw_taper * h.prm.vdw_cutoff;
@@ -218,18 +218,18 @@ void launch_vdw(Handle &h, bool grad) {
   vf.iwidth = 1.0 / (off - cut);
   auto kern = h.alch.active ? (h.mixed ? k_vdw<float, true> : k_vdw<double, true>)
                             : (h.mixed ? k_vdw<float, false> : k_vdw<double, false>);
-  kern<<<nblocks((int64_t)h.n * 32, 256), 256, 0, h.stream>>>(
+  kern<<<nblocks((int64_t)h.n * 32, 256), 256, 0, st>>>(
       h.n, h.d_rx, h.d_ry, h.d_rz, h.box, h.d_vtype, h.ntypes, h.d_vrad, h.d_veps, h.d_nbr, h.d_nbr_cnt, h.cap_nbr,
       h.d_nbr_sh, h.d_excl_ptr, h.d_excl_k, h.d_excl_code, h.d_excl_lo, h.d_excl_hi, vf, h.scales, grad ? 1 : 0, h.d_eatom, h.d_catom,
       h.d_gred, h.d_soft, h.d_mol, h.alch, h.d_eatom + 7 * (size_t)h.n, h.d_eatom + 8 * (size_t)h.n, h.d_lgred);
   FFX_LAUNCHED(h);
   if (grad) {
     // Rows 3-5 of d_gred hold the distributed per-atom vdW gradient.
-    k_vdw_distribute<<<nblocks(h.n, 256), 256, 0, h.stream>>>(h.n, h.d_gred, h.d_redp, h.d_redf, h.d_red_ptr,
+    k_vdw_distribute<<<nblocks(h.n, 256), 256, 0, st>>>(h.n, h.d_gred, h.d_redp, h.d_redf, h.d_red_ptr,
                                                                h.d_red_child, h.d_gred + 3 * (size_t)h.n);
     FFX_LAUNCHED(h);
     if (h.alch.active) {   // dU/dX dL rows 3-5 of d_lgred, distributed the same way
-      k_vdw_distribute<<<nblocks(h.n, 256), 256, 0, h.stream>>>(h.n, h.d_lgred, h.d_redp, h.d_redf, h.d_red_ptr,
+      k_vdw_distribute<<<nblocks(h.n, 256), 256, 0, st>>>(h.n, h.d_lgred, h.d_redp, h.d_redf, h.d_red_ptr,
                                                                  h.d_red_child, h.d_lgred + 3 * (size_t)h.n);
       FFX_LAUNCHED(h);
     }
