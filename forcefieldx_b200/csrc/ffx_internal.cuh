@@ -164,6 +164,42 @@ __device__ __forceinline__ void get_rec(const T *__restrict__ rec, int k, T *v) 
   }
 }
 
+// Per-atom gather records of the real-space energy and field kernels, kRecStride values
+// of the pair type per atom: 0-9 the global-frame multipole (quadrupole divided by 3),
+// 10 the Thole damping factor, 11 the Thole parameter, 12-15 zero, 16-18 u_D, 19-21 u_P,
+// 22-23 zero.  A pair reads its partner's row as a few aligned 16-byte loads from 2-3
+// (FP32) or 4-6 (FP64) sectors instead of one sector per structure-of-arrays column.
+constexpr int kRecStride = 24;
+constexpr int kRecInduced = 16;
+
+// M entries of atom k's record from entry OFF (both multiples of four values or two).
+template <int OFF, int M>
+__device__ __forceinline__ void load_rec(const float *__restrict__ rec, int k, float *v) {
+  static_assert(OFF % 4 == 0 && M % 4 == 0, "float records load as float4");
+  const float4 *q = reinterpret_cast<const float4 *>(rec + (size_t)k * kRecStride + OFF);
+#pragma unroll
+  for (int j = 0; j < M / 4; j++) {
+    const float4 t = __ldg(q + j);
+    v[4 * j] = t.x; v[4 * j + 1] = t.y; v[4 * j + 2] = t.z; v[4 * j + 3] = t.w;
+  }
+}
+template <int OFF, int M>
+__device__ __forceinline__ void load_rec(const double *__restrict__ rec, int k, double *v) {
+  static_assert(OFF % 2 == 0 && M % 2 == 0, "double records load as double2");
+  const double2 *q = reinterpret_cast<const double2 *>(rec + (size_t)k * kRecStride + OFF);
+#pragma unroll
+  for (int j = 0; j < M / 2; j++) {
+    const double2 t = __ldg(q + j);
+    v[2 * j] = t.x; v[2 * j + 1] = t.y;
+  }
+}
+
+// Position of atom k from the packed (x, y), (z, 0) pairs: one 32-byte sector.
+__device__ __forceinline__ void load_pos(const double2 *__restrict__ pos, int k, double &x, double &y, double &z) {
+  const double2 a = __ldg(pos + 2 * (size_t)k), b = __ldg(pos + 2 * (size_t)k + 1);
+  x = a.x; y = a.y; z = b.x;
+}
+
 // One cached pair of the dipole-field lists: the minimum-image displacement r = x_k - x_i
 // and the coefficients A (scalar part) and B (dyadic part) of the field -A u + B (u.r) r.
 // Plain form: FP64, 40 bytes; mixed form: FP32, 20 bytes.  Stored as a 32- or 16-byte
@@ -332,6 +368,8 @@ struct Handle {
   // the dipoles whose field is taken (u, then p), d_recP holds alpha r.
   double2 *d_pos = nullptr;
   void *d_recF = nullptr, *d_recP = nullptr;
+  void *d_erec = nullptr;                     // [n][kRecStride] real-space gather records
+  double2 *d_rpos = nullptr;                  // [n] (rx, ry), (rz, vdW type bits): vdW gather record
   double *d_tpair = nullptr;                  // [6][n] pair field of the current source
   double *d_tp = nullptr;                     // [6][n] field of the PCG direction p
   cudaStream_t aux = nullptr;                 // runs the pair field beside spread + FFT

@@ -325,7 +325,9 @@ static int create_impl(const ffxg_system *s, const ffxg_params *p, Handle &h) {
   CK(dalloc(&h.d_uD, 3 * N)); CK(dalloc(&h.d_uP, 3 * N)); CK(dalloc(&h.d_udirD, 3 * N)); CK(dalloc(&h.d_udirP, 3 * N));
   CK(dalloc(&h.d_r, 3 * N)); CK(dalloc(&h.d_rP, 3 * N)); CK(dalloc(&h.d_zpre, 3 * N)); CK(dalloc(&h.d_zpreP, 3 * N));
   CK(dalloc(&h.d_p, 3 * N)); CK(dalloc(&h.d_pP, 3 * N));
-  CK(dalloc(&h.d_pos, 2 * N));
+  CK(dalloc(&h.d_pos, 2 * N)); CK(dalloc(&h.d_rpos, 2 * N));
+  CK(cudaMalloc(&h.d_erec, (size_t)kRecStride * N * sizeof(double)));
+  CK(cudaMemset(h.d_erec, 0, (size_t)kRecStride * N * sizeof(double)));
   CK(dalloc(&h.d_tpair, 6 * N)); CK(dalloc(&h.d_tp, 6 * N));
   CK(cudaMalloc(&h.d_recF, 8 * N * sizeof(double)));
   CK(cudaMalloc(&h.d_recP, 8 * N * sizeof(double))); CK(dalloc(&h.d_vec, 3 * N)); CK(dalloc(&h.d_vecP, 3 * N));
@@ -436,7 +438,7 @@ static void free_all(Handle &h) {
                   h.d_uP, h.d_udirD, h.d_udirP, h.d_r, h.d_rP, h.d_zpre, h.d_zpreP, h.d_p, h.d_pP, h.d_vec, h.d_vecP,
                   h.d_partials, h.d_scalars, h.d_grid, h.d_influence, h.d_twiddle, h.d_gridf, h.d_influencef, h.d_twiddlef, h.d_grad, h.d_torque, h.d_gred,
                   h.d_eatom, h.d_catom, h.d_result, h.d_cresult, h.d_flags, h.d_xyz_in, h.d_grad_out,
-                  h.d_coefE, h.d_coefP, h.d_coefEB, h.d_coefPB, h.d_part2, h.d_counter, h.d_pos, h.d_recF, h.d_recP, h.d_tpair, h.d_tp, h.d_soft, h.d_mol, h.d_lgred, h.d_mass, h.d_mdx, h.d_mdv, h.d_mda, h.d_mdxp, h.d_mdg, h.d_mdke, h.d_settle, h.d_aspc, h.d_aspc_state, h.d_nbr_sh, h.d_ewl_sh, h.d_lg, h.d_lt, h.d_acc, h.d_polar_env, h.d_lig, h.d_rot};
+                  h.d_coefE, h.d_coefP, h.d_coefEB, h.d_coefPB, h.d_part2, h.d_counter, h.d_pos, h.d_rpos, h.d_erec, h.d_recF, h.d_recP, h.d_tpair, h.d_tp, h.d_soft, h.d_mol, h.d_lgred, h.d_mass, h.d_mdx, h.d_mdv, h.d_mda, h.d_mdxp, h.d_mdg, h.d_mdke, h.d_settle, h.d_aspc, h.d_aspc_state, h.d_nbr_sh, h.d_ewl_sh, h.d_lg, h.d_lt, h.d_acc, h.d_polar_env, h.d_lig, h.d_rot};
   for (void *q : ptrs)
     if (q) cudaFree(q);
   if (h.h_scalars) cudaFreeHost(h.h_scalars);

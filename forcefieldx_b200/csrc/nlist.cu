@@ -35,7 +35,8 @@ __global__ void k_reduce_coordinates(int n, const double *__restrict__ x, const 
                                      const double *__restrict__ z, const int *__restrict__ redp,
                                      const double *__restrict__ redf, double *rx, double *ry, double *rz,
                                      const double *__restrict__ refx, const double *__restrict__ refy,
-                                     const double *__restrict__ refz, double half_buffer2, int *flags) {
+                                     const double *__restrict__ refz, double half_buffer2, int *flags,
+                                     const int *__restrict__ vtype, double2 *rpos) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
   const int p = redp[i];
@@ -49,6 +50,8 @@ __global__ void k_reduce_coordinates(int n, const double *__restrict__ x, const 
     vz = __dadd_rn(__dmul_rn(a, __dsub_rn(zi, pz)), pz);
   }
   rx[i] = vx; ry[i] = vy; rz[i] = vz;
+  rpos[2 * i] = make_double2(vx, vy);
+  rpos[2 * i + 1] = make_double2(vz, __longlong_as_double((long long)vtype[i]));
   const double dx = vx - refx[i], dy = vy - refy[i], dz = vz - refz[i];
   const double d2 = dx * dx + dy * dy + dz * dz;
   if (!(d2 <= half_buffer2)) atomicOr(flags, FLAG_REBUILD);
@@ -312,7 +315,7 @@ void launch_set_coordinates(Handle &h, const double *d_xyz) {
   const double hb = 0.5 * h.prm.list_buffer;
   k_reduce_coordinates<<<nblocks(n, 256), 256, 0, h.stream>>>(n, h.d_x, h.d_y, h.d_z, h.d_redp, h.d_redf, h.d_rx,
                                                                h.d_ry, h.d_rz, h.d_refx, h.d_refy, h.d_refz,
-                                                               hb * hb, h.d_flags);
+                                                               hb * hb, h.d_flags, h.d_vtype, h.d_rpos);
   FFX_LAUNCHED(h);
 }
 

@@ -15,6 +15,8 @@
 // exclusion list; the masks are symmetric, so the i-side lookup reproduces the
 // reference's applyMask(i) (PermanentFieldRegion.java:231-258,
 // RealSpaceEnergyRegion.java:307-342).
+#include <cmath>
+
 #include "ffx_internal.cuh"
 
 namespace ffx {
@@ -52,15 +54,15 @@ struct Excl {
 // so the field of any dipole set is -A u_k + B (u_k . r) r; entries inside the
 // preconditioner cutoff also store the Ewald-free pair (pme/PCGSolver.java:1300-1331).
 template <typename R>
-__global__ void __launch_bounds__(128) k_realspace_field(
+__global__ void __launch_bounds__(128, sizeof(R) == 4 ? 8 : 1) k_realspace_field(
     int n, const double *__restrict__ x, const double *__restrict__ y, const double *__restrict__ z, Box bx,
     const double *__restrict__ gm, const double *__restrict__ ipdamp, const double *__restrict__ thole,
     const int *__restrict__ nbr, const int *__restrict__ nbr_cnt, int cap, const int *__restrict__ nbr_sh,
-    double off2, double pcut, int *ewl, int *ewl_cnt, int capE, int *ewl_sh, int *prl, int *prl_cnt, int capP,
+    double off2, double pcut2, int *ewl, int *ewl_cnt, int capE, int *ewl_sh, int *prl, int *prl_cnt, int capP,
     PairRec<R> *coefE, R *coefEB,
-    PairRec<R> *coefP, R *coefPB, Excl ex, EwaldCoef ec, ScaleTables c_scales, const double *__restrict__ cphi,
+    PairRec<R> *coefP, R *coefPB, Excl ex, EwaldCoef ec, const __grid_constant__ ScaleTables c_scales, const double *__restrict__ cphi,
     const double *__restrict__ polar, int direct, double *fieldD, double *fieldP, double *uD, double *uP,
-    double *udD, double *udP, R *recF, int *flags) {
+    double *udD, double *udP, R *recF, int *flags, const double2 *__restrict__ pos, const R *__restrict__ rec) {
   using V2 = typename Vec2<R>::type;
   const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const int lane = threadIdx.x & 31;
@@ -79,10 +81,12 @@ __global__ void __launch_bounds__(128) k_realspace_field(
       int k = -1;
       if (a < cnt) {
         k = row[a];
-        double dx = __dsub_rn(x[k], xi), dy = __dsub_rn(y[k], yi), dz = __dsub_rn(z[k], zi);
+        double xk, yk, zk;
+        load_pos(pos, k, xk, yk, zk);
+        double dx = __dsub_rn(xk, xi), dy = __dsub_rn(yk, yi), dz = __dsub_rn(zk, zi);
         const double r2 = pair_image(dx, dy, dz, bx, nbr_sh, (size_t)i * cap + a, 1.0);
         ew = r2 <= off2;
-        pr = ew && (sqrt(r2) < pcut);
+        pr = ew && (r2 <= pcut2);   // sqrt(r2) < pcut, exactly (pcut2 from below_sqrt)
       }
       const unsigned me = __ballot_sync(0xffffffffu, ew);
       const unsigned mp = __ballot_sync(0xffffffffu, pr);
@@ -123,13 +127,15 @@ __global__ void __launch_bounds__(128) k_realspace_field(
     if (act) {
       const int k = row[a];
       const size_t ent = (size_t)i * capE + a;
-      double xd = __dsub_rn(x[k], xi), yd = __dsub_rn(y[k], yi), zd = __dsub_rn(z[k], zi);
+      double xk, yk, zk;
+      load_pos(pos, k, xk, yk, zk);
+      R mk[12];
+      load_rec<0, 12>(rec, k, mk);
+      double xd = __dsub_rn(xk, xi), yd = __dsub_rn(yk, yi), zd = __dsub_rn(zk, zi);
       const double r2d = pair_image(xd, yd, zd, bx, ewl_sh, ent, 1.0);
       const R xr = (R)xd, yr = (R)yd, zr = (R)zd, r2 = (R)r2d;
-      const R ck = gm[t000 * n + k], dkx = gm[t100 * n + k], dky = gm[t010 * n + k], dkz = gm[t001 * n + k];
-      const R qkxx = gm[t200 * n + k] * (R(1.0) / R(3.0)), qkyy = gm[t020 * n + k] * (R(1.0) / R(3.0));
-      const R qkzz = gm[t002 * n + k] * (R(1.0) / R(3.0)), qkxy = gm[t110 * n + k] * (R(1.0) / R(3.0));
-      const R qkxz = gm[t101 * n + k] * (R(1.0) / R(3.0)), qkyz = gm[t011 * n + k] * (R(1.0) / R(3.0));
+      const R ck = mk[t000], dkx = mk[t100], dky = mk[t010], dkz = mk[t001];
+      const R qkxx = mk[t200], qkyy = mk[t020], qkzz = mk[t002], qkxy = mk[t110], qkxz = mk[t101], qkyz = mk[t011];
       const R r = m_sqrt(r2);
       const R ralpha = aewald * r;
       const R exp2a = m_exp(-ralpha * ralpha);
@@ -139,8 +145,8 @@ __global__ void __launch_bounds__(128) k_realspace_field(
       const R bn2 = (R(3.0) * bn1 + an1 * exp2a) * rr2;
       const R bn3 = (R(5.0) * bn2 + an2 * exp2a) * rr2;
       R scale3 = R(1.0), scale5 = R(1.0), scale7 = R(1.0);
-      R damp = pdi * ipdamp[k];
-      const R pgamma = m_min(pti, thole[k]);
+      R damp = pdi * mk[10];
+      const R pgamma = m_min(pti, mk[11]);
       const R rdamp = r * damp;
       damp = -pgamma * rdamp * rdamp * rdamp;
       if (damp > -R(50.0)) {
@@ -182,7 +188,7 @@ __global__ void __launch_bounds__(128) k_realspace_field(
         store_pair(coefE, (size_t)i * capE + a, xr, yr, zr, bn1 - urr3);
         coefEB[(size_t)i * capE + a] = bn2 - urr5;
       }
-      pr = sqrt(r2d) < pcut;   // the same test, in FP64, that selected the preconditioner row
+      pr = r2d <= pcut2;   // the same test, in FP64, that selected the preconditioner row
       if (pr) {
         const R b1 = rr1 * rr2, b2 = R(3.0) * b1 * rr2;   // Ewald off: bn0 = 1/r
         pA = b1 - urr3;
@@ -233,9 +239,10 @@ __global__ void __launch_bounds__(128) k_real_energy(
     int n, const double *__restrict__ x, const double *__restrict__ y, const double *__restrict__ z, Box bx,
     const double *__restrict__ gm, const double *__restrict__ uD, const double *__restrict__ uP,
     const double *__restrict__ ipdamp, const double *__restrict__ thole, const int *__restrict__ ewl,
-    const int *__restrict__ ewl_cnt, int capE, const int *__restrict__ ewl_sh, Excl ex, EwaldCoef ec, ScaleTables c_scales, int polarization, int gradient,
+    const int *__restrict__ ewl_cnt, int capE, const int *__restrict__ ewl_sh, Excl ex, EwaldCoef ec, const __grid_constant__ ScaleTables c_scales, int polarization, int gradient,
     double *eatom_perm, double *eatom_pol, long long *catom, double *grad, double *torque,
-    const int *__restrict__ soft, ElecStep st, double *edl, double *ed2l, double *lgrad, double *ltorque) {
+    const int *__restrict__ soft, ElecStep st, double *edl, double *ed2l, double *lgrad, double *ltorque,
+    const double2 *__restrict__ pos, const R *__restrict__ rec) {
   const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const int lane = threadIdx.x & 31;
   if (warp >= n) return;
@@ -265,15 +272,18 @@ __global__ void __launch_bounds__(128) k_real_energy(
   for (int a = lane; a < cnt; a += 32) {
     const int k = row[a];
     const size_t ent = (size_t)i * capE + a;
-    double xd = __dsub_rn(x[k], xi), yd = __dsub_rn(y[k], yi), zd = __dsub_rn(z[k], zi);
+    double xk, yk, zk;
+    load_pos(pos, k, xk, yk, zk);
+    R mk[12], uk[8];
+    load_rec<0, 12>(rec, k, mk);
+    load_rec<kRecInduced, 8>(rec, k, uk);
+    double xd = __dsub_rn(xk, xi), yd = __dsub_rn(yk, yi), zd = __dsub_rn(zk, zi);
     const double r2d = pair_image(xd, yd, zd, bx, ewl_sh, ent, 1.0);
     const R xr = (R)xd, yr = (R)yd, zr = (R)zd, r2 = (R)r2d;
-    const R ck = gm[t000 * n + k], dkx = gm[t100 * n + k], dky = gm[t010 * n + k], dkz = gm[t001 * n + k];
-    const R qkxx = gm[t200 * n + k] * (R(1.0) / R(3.0)), qkyy = gm[t020 * n + k] * (R(1.0) / R(3.0));
-    const R qkzz = gm[t002 * n + k] * (R(1.0) / R(3.0)), qkxy = gm[t110 * n + k] * (R(1.0) / R(3.0));
-    const R qkxz = gm[t101 * n + k] * (R(1.0) / R(3.0)), qkyz = gm[t011 * n + k] * (R(1.0) / R(3.0));
-    const R ukx = uD[k], uky = uD[n + k], ukz = uD[2 * n + k];
-    const R pkx = uP[k], pky = uP[n + k], pkz = uP[2 * n + k];
+    const R ck = mk[t000], dkx = mk[t100], dky = mk[t010], dkz = mk[t001];
+    const R qkxx = mk[t200], qkyy = mk[t020], qkzz = mk[t002], qkxy = mk[t110], qkxz = mk[t101], qkyz = mk[t011];
+    const R ukx = uk[0], uky = uk[1], ukz = uk[2];
+    const R pkx = uk[3], pky = uk[4], pkz = uk[5];
     const unsigned code = pair_primary(ewl_sh, ent) ? excl_code(i, k, ex.ptr, ex.k, ex.code, ex.lo, ex.hi) : 0u;
     const R scale = c_scales.m[code & 7u];
     const R scalep = c_scales.p[(code >> 3) & 7u];
@@ -300,8 +310,8 @@ __global__ void __launch_bounds__(128) k_real_energy(
     R scale3 = R(1.0), scale5 = R(1.0), scale7 = R(1.0);
     R ddsc3x = 0, ddsc3y = 0, ddsc3z = 0, ddsc5x = 0, ddsc5y = 0, ddsc5z = 0, ddsc7x = 0, ddsc7y = 0, ddsc7z = 0;
     (void)an5;
-    R damp = pdi * ipdamp[k];
-    const R tho = m_min(pti, thole[k]);
+    R damp = pdi * mk[10];
+    const R tho = m_min(pti, mk[11]);
     const R rdamp = r * damp;
     damp = -tho * rdamp * rdamp * rdamp;
     if (damp > -R(50.0)) {
@@ -689,18 +699,63 @@ static Excl excl(const Handle &h) {
 }
 
 
+// Gather records (kRecStride layout): multipole part from the global-frame multipoles and
+// the Thole parameters, induced part from u_D and u_P.  The quadrupole is divided by 3 in
+// the pair kernels' own expression.
+template <typename R>
+__global__ void k_pack_mpole(int n, const double *__restrict__ gm, const double *__restrict__ ipdamp,
+                             const double *__restrict__ thole, R *rec) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  R v[16];
+#pragma unroll
+  for (int j = 0; j < 4; j++) v[j] = (R)gm[(size_t)j * n + i];
+#pragma unroll
+  for (int j = 4; j < 10; j++) v[j] = (R)(gm[(size_t)j * n + i] * (R(1.0) / R(3.0)));
+  v[10] = (R)ipdamp[i];
+  v[11] = (R)thole[i];
+  v[12] = v[13] = v[14] = v[15] = R(0);
+  R *o = rec + (size_t)i * kRecStride;
+#pragma unroll
+  for (int j = 0; j < 16; j++) o[j] = v[j];
+}
+
+template <typename R>
+__global__ void k_pack_induced(int n, const double *__restrict__ uD, const double *__restrict__ uP, R *rec) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  R *o = rec + (size_t)i * kRecStride + kRecInduced;
+  o[0] = (R)uD[i]; o[1] = (R)uD[n + i]; o[2] = (R)uD[2 * (size_t)n + i];
+  o[3] = (R)uP[i]; o[4] = (R)uP[n + i]; o[5] = (R)uP[2 * (size_t)n + i];
+  o[6] = o[7] = R(0);
+}
+
+// The largest double t with sqrt(t) < c.  sqrt is correctly rounded, hence monotone, so
+// the preconditioner-cutoff test sqrt(r2) < c is exactly r2 <= t.
+static double below_sqrt(double c) {
+  if (!(c > 0.0)) return -1.0;
+  double t = c * c;
+  while (std::sqrt(t) >= c) t = std::nextafter(t, 0.0);
+  while (std::sqrt(std::nextafter(t, INFINITY)) < c) t = std::nextafter(t, INFINITY);
+  return t;
+}
+
 template <typename R>
 static void realspace_field(Handle &h) {
   using V2 = typename Vec2<R>::type;
   const double off2 = h.vacuum ? INFINITY : h.prm.ewald_cutoff * h.prm.ewald_cutoff;
+  k_pack_mpole<R><<<nblocks(h.n, 256), 256, 0, h.stream>>>(h.n, h.d_gm, h.d_ipdamp, h.d_thole,
+                                                            reinterpret_cast<R *>(h.d_erec));
+  FFX_LAUNCHED(h);
   k_realspace_field<R><<<nblocks((int64_t)h.n * 32, 128), 128, 0, h.stream>>>(
       h.n, h.d_x, h.d_y, h.d_z, h.box, h.d_gm, h.d_ipdamp, h.d_thole, h.d_nbr, h.d_nbr_cnt, h.cap_nbr,
-      h.d_nbr_sh, off2, h.prm.precond_cutoff, h.d_ewl, h.d_ewl_cnt, h.cap_ewl, h.d_ewl_sh, h.d_prl, h.d_prl_cnt,
+      h.d_nbr_sh, off2, below_sqrt(h.prm.precond_cutoff), h.d_ewl, h.d_ewl_cnt, h.cap_ewl, h.d_ewl_sh, h.d_prl, h.d_prl_cnt,
       h.cap_prl,
       reinterpret_cast<PairRec<R> *>(h.d_coefE), reinterpret_cast<R *>(h.d_coefEB),
       reinterpret_cast<PairRec<R> *>(h.d_coefP), reinterpret_cast<R *>(h.d_coefPB), excl(h),
       ewald_coef(h, ewald_alpha_of(h)), h.scales, h.d_cphi, h.d_polar, h.prm.polarization != FFXG_POLAR_NONE ? 1 : 0,
-      h.d_fieldD, h.d_fieldP, h.d_uD, h.d_uP, h.d_udirD, h.d_udirP, reinterpret_cast<R *>(h.d_recF), h.d_flags);
+      h.d_fieldD, h.d_fieldP, h.d_uD, h.d_uP, h.d_udirD, h.d_udirP, reinterpret_cast<R *>(h.d_recF), h.d_flags,
+      h.d_pos, reinterpret_cast<const R *>(h.d_erec));
   FFX_LAUNCHED(h);
 }
 
@@ -716,11 +771,14 @@ void launch_realspace_field(Handle &h) {
 template <typename R>
 static void real_energy(Handle &h, bool grad) {
   auto kern = h.step.lam ? k_real_energy<R, true> : k_real_energy<R, false>;
+  k_pack_induced<R><<<nblocks(h.n, 256), 256, 0, h.stream>>>(h.n, h.d_uD, h.d_uP, reinterpret_cast<R *>(h.d_erec));
+  FFX_LAUNCHED(h);
   kern<<<nblocks((int64_t)h.n * 32, 128), 128, 0, h.stream>>>(
       h.n, h.d_x, h.d_y, h.d_z, h.box, h.d_gm, h.d_uD, h.d_uP, h.d_ipdamp, h.d_thole, h.d_ewl, h.d_ewl_cnt,
       h.cap_ewl, h.d_ewl_sh, excl(h), ewald_coef(h, ewald_alpha_of(h)), h.scales, h.prm.polarization, grad ? 1 : 0,
       h.d_eatom + 1 * (size_t)h.n, h.d_eatom + 2 * (size_t)h.n, h.d_catom + (size_t)h.n, h.d_grad, h.d_torque,
-      h.d_soft, h.step, h.d_eatom + 9 * (size_t)h.n, h.d_eatom + 10 * (size_t)h.n, h.d_lg, h.d_lt);
+      h.d_soft, h.step, h.d_eatom + 9 * (size_t)h.n, h.d_eatom + 10 * (size_t)h.n, h.d_lg, h.d_lt, h.d_pos,
+      reinterpret_cast<const R *>(h.d_erec));
   FFX_LAUNCHED(h);
 }
 
@@ -779,7 +837,7 @@ __global__ void __launch_bounds__(128) k_param_real(
     const double *__restrict__ gm, const double *__restrict__ uD, const double *__restrict__ uP,
     const double *__restrict__ ipdamp, const double *__restrict__ thole, const int *__restrict__ ewl,
     const int *__restrict__ ewl_cnt, int capE, const int *__restrict__ ewl_sh, Excl ex, EwaldCoef ec,
-    ScaleTables c_scales, int pol, double *phi) {
+    const __grid_constant__ ScaleTables c_scales, int pol, double *phi) {
   const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const int lane = threadIdx.x & 31;
   if (warp >= n) return;

@@ -4,7 +4,8 @@
 // (VanDerWaalsForm.java:313-334; delta 0.07, gamma 0.12), the multiplicative taper
 // from vdw-taper * cutoff to the cutoff (MultiplicativeSwitch.java:84-124, 234-236) and
 // the 1-2/1-3/1-4 masks (VanDerWaals.applyMask, :412-428).  A warp owns atom i and
-// gathers over the buffered list in both directions: the force on i's reduced site
+// gathers over the buffered list in both directions (a partner's reduced position and
+// type from one 32-byte record): the force on i's reduced site
 // accumulates in registers; k_vdw_distribute then splits every reduced-site force
 // between the hydrogen and its heavy atom (VanDerWaals.java:1786-1797) as a gather.
 #include "ffx_internal.cuh"
@@ -38,9 +39,10 @@ __global__ void __launch_bounds__(256) k_vdw(int n, const double *__restrict__ r
                                              const int *__restrict__ eptr,
                                              const int *__restrict__ ek, const unsigned *__restrict__ ecode,
                                              const int *__restrict__ elo, const int *__restrict__ ehi, VdwForm vf,
-                                             ScaleTables c_vscales, int gradient, double *eatom, long long *catom, double *gred,
+                                             const __grid_constant__ ScaleTables c_vscales, int gradient, double *eatom, long long *catom, double *gred,
                                              const int *__restrict__ soft, const int *__restrict__ mol, AlchConst al,
-                                             double *edl, double *ed2l, double *lgred) {
+                                             double *edl, double *ed2l, double *lgred,
+                                             const double2 *__restrict__ rpos) {
   const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const int lane = threadIdx.x & 31;
   if (warp >= n) return;
@@ -60,9 +62,10 @@ __global__ void __launch_bounds__(256) k_vdw(int n, const double *__restrict__ r
   for (int a = lane; a < m; a += 32) {
     const int k = row[a];
     const size_t ent = (size_t)i * cap + a;
-    double dxd = __dsub_rn(xi, rx[k]), dyd = __dsub_rn(yi, ry[k]), dzd = __dsub_rn(zi, rz[k]);
+    const double2 pa = __ldg(rpos + 2 * (size_t)k), pb = __ldg(rpos + 2 * (size_t)k + 1);
+    double dxd = __dsub_rn(xi, pa.x), dyd = __dsub_rn(yi, pa.y), dzd = __dsub_rn(zi, pb.x);
     const double r2d = pair_image(dxd, dyd, dzd, bx, nbr_sh, ent, -1.0);
-    const int tk = vtype[k];
+    const int tk = (int)__double_as_longlong(pb.y);
     const R irv = vrad[ti * ntypes + tk];
     if (!(r2d <= vf.off2) || !(irv > R(0.0))) continue;
     const unsigned code = pair_primary(nbr_sh, ent) ? vexcl_code(i, k, eptr, ek, ecode, elo, ehi) : 0u;
@@ -221,7 +224,8 @@ void launch_vdw(Handle &h, bool grad, cudaStream_t st) {
   kern<<<nblocks((int64_t)h.n * 32, 256), 256, 0, st>>>(
       h.n, h.d_rx, h.d_ry, h.d_rz, h.box, h.d_vtype, h.ntypes, h.d_vrad, h.d_veps, h.d_nbr, h.d_nbr_cnt, h.cap_nbr,
       h.d_nbr_sh, h.d_excl_ptr, h.d_excl_k, h.d_excl_code, h.d_excl_lo, h.d_excl_hi, vf, h.scales, grad ? 1 : 0, h.d_eatom, h.d_catom,
-      h.d_gred, h.d_soft, h.d_mol, h.alch, h.d_eatom + 7 * (size_t)h.n, h.d_eatom + 8 * (size_t)h.n, h.d_lgred);
+      h.d_gred, h.d_soft, h.d_mol, h.alch, h.d_eatom + 7 * (size_t)h.n, h.d_eatom + 8 * (size_t)h.n, h.d_lgred,
+      h.d_rpos);
   FFX_LAUNCHED(h);
   if (grad) {
     // Rows 3-5 of d_gred hold the distributed per-atom vdW gradient.
