@@ -27,25 +27,37 @@
 
 namespace ffx {
 
-constexpr int kFieldThreads = 128;               // 4 warps; each warp takes one atom at a time
-constexpr int kFieldBlocks = 148 * 8;            // fixed grid (grid-stride over atoms)
+constexpr int kFieldThreads = 128;               // blocks of the pair-field kernels
 constexpr int kVecThreads = 256;
 constexpr int kVecBlocks = 148 * 2;
-// Grids of the grid-stride kernels: the fixed sizes above for large systems, fewer blocks
-// for small ones (a 96-atom box needs 24 warps-per-atom blocks, not 1,184), so the kernels
-// of many small systems can share the device (batches).
-static int field_blocks(int n) { return std::min(kFieldBlocks, std::max(1, (n + 3) / 4)); }
+// Lane groups of the pair-field kernels: G lanes per atom (a warp takes 32 / G atoms), a
+// grid that gives every group one atom.  The short preconditioner rows (~40 pairs at
+// 4.5 A) take 8 lanes, the Ewald rows (~140 pairs at 7 A) 16.  Grids follow the system
+// size, so the kernels of many small systems can share the device (batches).
+constexpr int kPrecondGroup = 8;
+constexpr int kEwaldGroup = 16;
+static int group_blocks(int n, int G) { return std::max(1, (n + kFieldThreads / G - 1) / (kFieldThreads / G)); }
+// The vector kernels stride over atoms with a fixed grid for large systems.
 static int vec_blocks(int n) { return std::min(kVecBlocks, std::max(1, (n + kVecThreads - 1) / kVecThreads)); }
+// The combine takes one atom per warp; its partial rows are one per block.
+static int combine_blocks(int n) { return nblocks((int64_t)n * 32, 256); }
 // Totals of the PCG scalars in Handle::d_scalars.
 enum { T_PAP = 0, T_PAPP, T_RZ, T_RZP, T_RZN, T_RZNP, T_BETA, T_BETAP };
 // Counters (each returns to 0 after use) in Handle::d_counter.
 enum { K_UPDATE = 0, K_FIELD, K_PRECOND };
 
-// Fixed-order total of column c over nb rows by one warp (lane l sums l, l+32, ...).
+// Fixed-order total of column c over nb rows by one warp (lane l sums l, l+32, ...; four
+// rows' loads in flight at a time).
 __device__ __forceinline__ double warp_total(const double *__restrict__ part, int nb, int c) {
   const int lane = threadIdx.x & 31;
   double s = 0.0;
-  for (int b = lane; b < nb; b += 32) s += part[b * 8 + c];
+  for (int b0 = lane; b0 < nb; b0 += 128) {
+    double v[4];
+#pragma unroll
+    for (int u = 0; u < 4; u++) v[u] = (b0 + 32 * u < nb) ? part[(b0 + 32 * u) * 8 + c] : 0.0;
+#pragma unroll
+    for (int u = 0; u < 4; u++) s += v[u];
+  }
   return warp_sum(s);
 }
 
@@ -148,25 +160,26 @@ __device__ __forceinline__ void field_term(T xr, T yr, T zr, T A, T B, const T *
   acc[3] += -A * s[3] + pkr * xr; acc[4] += -A * s[4] + pkr * yr; acc[5] += -A * s[5] + pkr * zr;
 }
 
-// Lane partials of the dipole field at atom i from the cached pair row: the displacement
-// and A, B of each pair stream in coalesced; only the neighbour's source record is
-// gathered.  T is double (plain form) or float (mixed form).  Each lane handles NU entries
-// (a, a + 32, ...) together so that all their loads are in flight at once (4 for the long
-// Ewald rows in the FP32 form, 2 otherwise); the summation order stays a, a + 32, a + 64, ...
-template <typename T, int NU>
-__device__ __forceinline__ void pair_field(int i, const int *__restrict__ lst, const int *__restrict__ lst_cnt, int cap,
-                                           const PairRec<T> *__restrict__ pr, const T *__restrict__ pb,
+// Lane partials of the dipole field at atom i from the cached pair row, taken by the G
+// lanes (sub = 0 .. G-1) of one aligned lane group: the displacement and A, B of each pair
+// stream in coalesced; only the neighbour's source record is gathered.  T is double
+// (plain form) or float (mixed form).  Each lane handles NU entries (a, a + G, ...)
+// together so that all their loads are in flight at once; the summation order stays a,
+// a + G, a + 2G, ...  i < 0 marks an idle group (no atom left), which still takes part in
+// the group's shuffles.
+template <typename T, int NU, int G>
+__device__ __forceinline__ void pair_field(int i, int sub, const int *__restrict__ lst, const int *__restrict__ lst_cnt,
+                                           int cap, const PairRec<T> *__restrict__ pr, const T *__restrict__ pb,
                                            const T *__restrict__ rec, T *acc) {
-  const int lane = threadIdx.x & 31;
-  const int cnt = min(lst_cnt[i], cap);
-  const size_t e0 = (size_t)i * cap;
+  const int cnt = (i < 0) ? 0 : min(lst_cnt[i], cap);
+  const size_t e0 = (size_t)(i < 0 ? 0 : i) * cap;
   const int *row = lst + e0;
-  for (int a = lane; a < cnt; a += 32 * NU) {
+  for (int a = sub; a < cnt; a += G * NU) {
     int ix[NU], kk[NU];
     T xx[NU], yy[NU], zz[NU], AA[NU], BB[NU], ss[NU][6];
 #pragma unroll
     for (int u = 0; u < NU; u++) {
-      ix[u] = (a + 32 * u < cnt) ? a + 32 * u : a;
+      ix[u] = (a + G * u < cnt) ? a + G * u : a;
       kk[u] = row[ix[u]];
     }
 #pragma unroll
@@ -177,8 +190,16 @@ __device__ __forceinline__ void pair_field(int i, const int *__restrict__ lst, c
     }
 #pragma unroll
     for (int u = 0; u < NU; u++)
-      if (a + 32 * u < cnt) field_term(xx[u], yy[u], zz[u], AA[u], BB[u], ss[u], acc);
+      if (a + G * u < cnt) field_term(xx[u], yy[u], zz[u], AA[u], BB[u], ss[u], acc);
   }
+}
+
+// Sum over the G lanes of an aligned lane group (every lane of the warp takes part).
+template <int G>
+__device__ __forceinline__ double group_sum(double v) {
+#pragma unroll
+  for (int o = G / 2; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  return v;
 }
 
 // Fractional-to-Cartesian transform of the potential gradient (rows and columns 1-3 of
@@ -224,22 +245,26 @@ __device__ __forceinline__ void mesh_field(int i, int n, const int *__restrict__
 }
 
 // Real-space pair field of the source records `rec` (u, then z) at every atom, into
-// out[6][n] (D xyz, CR xyz).
-template <typename T>
+// out[6][n] (D xyz, CR xyz).  A group of G lanes takes one atom; the groups of a warp take
+// consecutive atoms and stride over the system together.
+template <typename T, int G>
 __global__ void __launch_bounds__(kFieldThreads) k_pair_field(int n, const int *__restrict__ ewl,
                                                               const int *__restrict__ ewl_cnt, int capE,
                                                               const PairRec<T> *__restrict__ coefE,
                                                               const T *__restrict__ coefEB,
                                                               const T *__restrict__ rec, double *out) {
-  const int lane = threadIdx.x & 31;
-  const int wstride = gridDim.x * (blockDim.x >> 5);
-  for (int i = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5); i < n; i += wstride) {
+  constexpr int GPW = 32 / G;
+  const int lane = threadIdx.x & 31, sub = lane & (G - 1), gi = lane / G;
+  const int astride = gridDim.x * (blockDim.x >> 5) * GPW;
+  for (int i0 = (blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5)) * GPW; i0 < n; i0 += astride) {
+    const int i = i0 + gi;
+    const bool live = i < n;
     T a6[6] = {0, 0, 0, 0, 0, 0};
-    pair_field<T, 2>(i, ewl, ewl_cnt, capE, coefE, coefEB, rec, a6);
+    pair_field<T, 2, G>(live ? i : -1, sub, ewl, ewl_cnt, capE, coefE, coefEB, rec, a6);
     double f[6];
 #pragma unroll
-    for (int q = 0; q < 6; q++) f[q] = warp_sum((double)a6[q]);
-    if (lane == 0) {
+    for (int q = 0; q < 6; q++) f[q] = group_sum<G>((double)a6[q]);
+    if (live && sub == 0) {
 #pragma unroll
       for (int q = 0; q < 6; q++) out[(size_t)q * n + i] = f[q];
     }
@@ -258,7 +283,7 @@ __global__ void __launch_bounds__(kFieldThreads) k_pair_field(int n, const int *
 template <int MODE, typename T>
 __global__ void __launch_bounds__(256) k_pcg_combine(
     int n, const int *__restrict__ igrid, const T *__restrict__ spl, const typename Vec2<T>::type *__restrict__ mesh,
-    int nfx, int nfy, int nfz, FieldXform xf, const double *__restrict__ tpair, const double *__restrict__ vD,
+    int nfx, int nfy, int nfz, const __grid_constant__ FieldXform xf, const double *__restrict__ tpair, const double *__restrict__ vD,
     const double *__restrict__ vP, double aewald3, const double *__restrict__ polar,
     const double *__restrict__ udirD, const double *__restrict__ udirP, double *p, double *pP, double *tp,
     int first, const double *__restrict__ r, const double *__restrict__ rP, double *outD, double *outP, T *recP,
@@ -304,8 +329,11 @@ __global__ void __launch_bounds__(256) k_pcg_combine(
         pp[j] = pv;
         const double vv = ok ? pv * ip - t : 0.0;
         (set ? outP : outD)[j] = vv;
-        acc[set] = pv * vv;
-        acc[2 + set] = (set ? rP : r)[j] * vj;
+        const double pav = pv * vv, rzv = (set ? rP : r)[j] * vj;
+        acc[0] = set ? 0.0 : pav;
+        acc[1] = set ? pav : 0.0;
+        acc[2] = set ? 0.0 : rzv;
+        acc[3] = set ? rzv : 0.0;
       }
     }
     if (MODE == 1) {
@@ -328,45 +356,48 @@ __global__ void __launch_bounds__(256) k_pcg_combine(
 // and z's source record for the next field.  INIT also sets p = z; otherwise r . z_new
 // is finished into d_scalars and the last block forms beta = r.z_new / r.z_old
 // (UpdateConjugateLoop, Fletcher-Reeves; a zero r.z_old counts as 1).
-template <bool INIT, typename T>
+template <bool INIT, typename T, int G>
 __global__ void __launch_bounds__(kFieldThreads) k_pcg_precond(
     int n, const int *__restrict__ prl, const int *__restrict__ prl_cnt, int capP,
     const PairRec<T> *__restrict__ coefP, const T *__restrict__ coefPB, const T *__restrict__ recP,
     const double *__restrict__ polar, const double *__restrict__ r, const double *__restrict__ rP, double s,
     double *zz, double *zP, double *p, double *pP, T *recF, double *part, unsigned *counter, double *tot) {
-  const int lane = threadIdx.x & 31;
-  const int wstride = gridDim.x * (blockDim.x >> 5);
+  static_assert(G >= 8, "lanes 0-5 of a group finish the six components");
+  constexpr int GPW = 32 / G;
+  const int lane = threadIdx.x & 31, sub = lane & (G - 1), gi = lane / G, g0 = lane & ~(G - 1);
+  const int astride = gridDim.x * (blockDim.x >> 5) * GPW;
   double acc[2] = {0, 0};
-  for (int i = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5); i < n; i += wstride) {
+  for (int i0 = (blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5)) * GPW; i0 < n; i0 += astride) {
+    const int i = i0 + gi;
+    const bool live = i < n;
     T a6[6] = {0, 0, 0, 0, 0, 0};
-    pair_field<T, 2>(i, prl, prl_cnt, capP, coefP, coefPB, recP, a6);
+    pair_field<T, 2, G>(live ? i : -1, sub, prl, prl_cnt, capP, coefP, coefPB, recP, a6);
     double f[6];
 #pragma unroll
-    for (int q = 0; q < 6; q++) f[q] = warp_sum((double)a6[q]);
+    for (int q = 0; q < 6; q++) f[q] = group_sum<G>((double)a6[q]);
     double mine = f[0];
 #pragma unroll
     for (int q = 1; q < 6; q++)
-      if (lane == q) mine = f[q];
+      if (sub == q) mine = f[q];
     double zv = 0.0;
-    if (lane < 6) {
-      const int d = lane % 3, set = lane / 3;
+    if (live && sub < 6) {
+      const int d = sub % 3, set = sub / 3;
       const size_t j = (size_t)d * n + i;
       const double rj = (set ? rP : r)[j];
       zv = polar[i] * (mine + s * rj);
       (set ? zP : zz)[j] = zv;
       if (INIT) (set ? pP : p)[j] = zv;
-      acc[set] += rj * zv;
+      if (set) acc[1] += rj * zv;
+      else acc[0] += rj * zv;
     }
     double w[6];
 #pragma unroll
-    for (int q = 0; q < 6; q++) w[q] = __shfl_sync(0xffffffffu, zv, q);
-    if (lane == 0) put_rec(recF, i, w[0], w[1], w[2], w[3], w[4], w[5]);
+    for (int q = 0; q < 6; q++) w[q] = __shfl_sync(0xffffffffu, zv, g0 + q);
+    if (live && sub == 0) put_rec(recF, i, w[0], w[1], w[2], w[3], w[4], w[5]);
   }
   if (!INIT) {
 #pragma unroll
-    for (int q = 0; q < 2; q++)
-#pragma unroll
-      for (int o = 4; o > 0; o >>= 1) acc[q] += __shfl_xor_sync(0xffffffffu, acc[q], o);
+    for (int q = 0; q < 2; q++) acc[q] = group_sum<32>(acc[q]);
     block_store_lane0<2>(acc, part);
   }
 }
@@ -400,10 +431,22 @@ __global__ void __launch_bounds__(kVecThreads) k_pcg_update(
   __shared__ double tsum[4][kVecThreads / 32];
   __shared__ double tv[4];
   {
+    // Rows b, b + blockDim, ... per thread, eight rows' loads in flight at a time.
     double s4[4] = {0.0, 0.0, 0.0, 0.0};
-    for (int b = threadIdx.x; b < rowsC; b += blockDim.x)
+    constexpr int U = 8;
+    for (int b0 = threadIdx.x; b0 < rowsC; b0 += U * blockDim.x) {
+      double v[U][4];
 #pragma unroll
-      for (int q = 0; q < 4; q++) s4[q] += partC[b * 8 + q];
+      for (int u = 0; u < U; u++) {
+        const int b = b0 + u * blockDim.x;
+#pragma unroll
+        for (int q = 0; q < 4; q++) v[u][q] = (b < rowsC) ? partC[b * 8 + q] : 0.0;
+      }
+#pragma unroll
+      for (int u = 0; u < U; u++)
+#pragma unroll
+        for (int q = 0; q < 4; q++) s4[q] += v[u][q];
+    }
     const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
 #pragma unroll
     for (int q = 0; q < 4; q++) {
@@ -539,20 +582,20 @@ static double aewald3_of(const Handle &h) {
 // Partial-sum regions of d_part2 (combine, preconditioner, update): one row of 8 per
 // block of the largest grid that writes them.
 int pcg_partial_rows(int n) {
-  const int per_atom = nblocks((int64_t)n * 32, 256);   // k_pcg_combine
-  return std::max(std::max(kFieldBlocks, kVecBlocks), per_atom);
+  return std::max(std::max(kVecBlocks, combine_blocks(n)), group_blocks(n, kPrecondGroup));
 }
 static double *part_region(const Handle &h, int k) { return h.d_part2 + (size_t)k * h.part_rows * 8; }
 
 // beta = r.z_new / r.z_old from the preconditioner's partial rows (the totals kernel).
 static void beta_totals(Handle &h, cudaStream_t st) {
-  k_pcg_totals<2, true><<<1, 1024, 0, st>>>(part_region(h, 1), field_blocks(h.n), h.d_scalars, T_RZN);
+  k_pcg_totals<2, true><<<1, 1024, 0, st>>>(part_region(h, 1), group_blocks(h.n, kPrecondGroup), h.d_scalars,
+                                            T_RZN);
   FFX_LAUNCHED(h);
 }
 
 template <typename T>
 static void pair_field_launch(Handle &h, cudaStream_t st) {
-  k_pair_field<T><<<field_blocks(h.n), kFieldThreads, 0, st>>>(
+  k_pair_field<T, kEwaldGroup><<<group_blocks(h.n, kEwaldGroup), kFieldThreads, 0, st>>>(
       h.n, h.d_ewl, h.d_ewl_cnt, h.cap_ewl, reinterpret_cast<const PairRec<T> *>(h.d_coefE),
       reinterpret_cast<const T *>(h.d_coefEB), reinterpret_cast<const T *>(h.d_recF), h.d_tpair);
   FFX_LAUNCHED(h);
@@ -565,7 +608,7 @@ static void combine(Handle &h, const double *vD, const double *vP, bool first, d
   for (int a = 0; a < 3; a++)
     for (int b = 0; b < 3; b++) xf.m[a][b] = h.pc.tfm[1 + a][1 + b];
   const V2 *mesh = reinterpret_cast<const V2 *>(h.mixed ? (const void *)h.d_gridf : (const void *)h.d_grid);
-  k_pcg_combine<MODE, T><<<nblocks((int64_t)h.n * 32, 256), 256, 0, h.stream>>>(
+  k_pcg_combine<MODE, T><<<combine_blocks(h.n), 256, 0, h.stream>>>(
       h.n, h.d_igrid, reinterpret_cast<const T *>(h.d_spl), mesh, h.nfft[0], h.nfft[1], h.nfft[2], xf, h.d_tpair, vD,
       vP, aewald3_of(h), h.d_polar, h.d_udirD, h.d_udirP, h.d_p, h.d_pP, h.d_tp, first ? 1 : 0, h.d_r, h.d_rP, outD,
       outP, reinterpret_cast<T *>(h.d_recP), part_region(h, 0), h.d_counter + K_FIELD, h.d_scalars);
@@ -596,7 +639,7 @@ static void field_of(Handle &h, const double *vD, const double *vP, bool first, 
 
 template <bool INIT, typename T>
 static void precond(Handle &h) {
-  k_pcg_precond<INIT, T><<<field_blocks(h.n), kFieldThreads, 0, h.stream>>>(
+  k_pcg_precond<INIT, T, kPrecondGroup><<<group_blocks(h.n, kPrecondGroup), kFieldThreads, 0, h.stream>>>(
       h.n, h.d_prl, h.d_prl_cnt, h.cap_prl, reinterpret_cast<const PairRec<T> *>(h.d_coefP),
       reinterpret_cast<const T *>(h.d_coefPB), reinterpret_cast<const T *>(h.d_recP), h.d_polar, h.d_r, h.d_rP,
       h.prm.precond_scale, h.d_zpre, h.d_zpreP, h.d_p, h.d_pP, reinterpret_cast<T *>(h.d_recF), part_region(h, 1),
@@ -618,7 +661,7 @@ static void update(Handle &h, cudaGraphConditionalHandle cond, int use_cond) {
       h.n, h.d_vec, h.d_vecP, h.d_p, h.d_pP, h.d_r, h.d_rP, h.d_uD, h.d_uP, h.d_scalars, part_region(h, 2),
       h.d_counter + K_UPDATE, h.d_pcg, h.prm.max_scf_iter, h.prm.polar_eps, h.d_flags, cond, use_cond, h.d_polar,
       reinterpret_cast<T *>(h.d_recP), h.eps_atoms > 0 ? h.eps_atoms : h.n, part_region(h, 0),
-      nblocks((int64_t)h.n * 32, 256));
+      combine_blocks(h.n));
   FFX_LAUNCHED(h);
 }
 

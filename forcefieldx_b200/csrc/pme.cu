@@ -201,25 +201,30 @@ __device__ __forceinline__ int jmod(int a, int m) {
   return r < 0 ? r + m : r;
 }
 
-// Mesh accumulation: FP64 atomics into the complex double mesh in both forms.  The
-// mixed form first rounds each FP32 contribution to a multiple of 2^-32; sums of such
-// values are exact in FP64 (below 2^21 in magnitude), so the accumulated mesh has the
-// same bits whatever order the atoms arrive in.  The first FFT pass reads the double
-// mesh and continues in FP32.
+// Mesh accumulation with FP64 atomics.  FP64 form: into the complex double mesh that the
+// FFT transforms in place.  Mixed form: into two planes of doubles (real parts, then
+// imaginary parts, ng points each), so that a warp's row of five support points touches
+// two 32-byte sectors instead of three; each FP32 contribution is first rounded to a
+// multiple of 2^-32, so sums of such values are exact in FP64 (below 2^21 in magnitude)
+// and the accumulated mesh has the same bits whatever order the atoms arrive in.  The
+// first FFT pass reads the planes and continues in FP32.
 __device__ __forceinline__ double mesh_quantize(float v) {
   return rint((double)v * 4294967296.0) * 2.3283064365386962890625e-10;
 }
-__device__ __forceinline__ void mesh_add(double2 *grid, size_t idx, double re) { atomicAdd(&grid[idx].x, re); }
-__device__ __forceinline__ void mesh_add(double2 *grid, size_t idx, float re) {
-  atomicAdd(&grid[idx].x, mesh_quantize(re));
+__device__ __forceinline__ void mesh_add(double2 *grid, size_t, size_t idx, double re) {
+  atomicAdd(&grid[idx].x, re);
 }
-__device__ __forceinline__ void mesh_add(double2 *grid, size_t idx, double re, double im) {
+__device__ __forceinline__ void mesh_add(double2 *grid, size_t, size_t idx, float re) {
+  atomicAdd(reinterpret_cast<double *>(grid) + idx, mesh_quantize(re));
+}
+__device__ __forceinline__ void mesh_add(double2 *grid, size_t, size_t idx, double re, double im) {
   atomicAdd(&grid[idx].x, re);
   atomicAdd(&grid[idx].y, im);
 }
-__device__ __forceinline__ void mesh_add(double2 *grid, size_t idx, float re, float im) {
-  atomicAdd(&grid[idx].x, mesh_quantize(re));
-  atomicAdd(&grid[idx].y, mesh_quantize(im));
+__device__ __forceinline__ void mesh_add(double2 *grid, size_t ng, size_t idx, float re, float im) {
+  double *plane = reinterpret_cast<double *>(grid);
+  atomicAdd(plane + idx, mesh_quantize(re));
+  atomicAdd(plane + ng + idx, mesh_quantize(im));
 }
 
 // Wrap a support index (within one period of the mesh) into [0, m).
@@ -235,6 +240,7 @@ __global__ void k_spread_permanent(int n, const double *__restrict__ fm, const S
   const int lane = threadIdx.x & 31;
   if (warp >= n || lane >= 25) return;
   const int i = warp;
+  const size_t ng = (size_t)nfx * nfy * nfz;
   const S *s = spl + (size_t)i * 3 * kOrder * 4;
   const S *sx = s, *sy = s + kOrder * 4, *sz = s + 2 * kOrder * 4;
   const int a1 = lane % 5, a2 = lane / 5;
@@ -257,7 +263,7 @@ __global__ void k_spread_permanent(int n, const double *__restrict__ fm, const S
     const S term2 = f[t200] * v0 * u0;
     const S val = fma(x0, term0, fma(x1, term1, x2 * term2));
     const int kk = wrap1(k0 + a3, nfz);
-    mesh_add(grid, (size_t)kk * nfy * nfx + row, val);
+    mesh_add(grid, ng, (size_t)kk * nfy * nfx + row, val);
   }
 }
 
@@ -269,6 +275,7 @@ __global__ void k_spread_induced(int n, const double *__restrict__ ud, const dou
   const int lane = threadIdx.x & 31;
   if (warp >= n || lane >= 25) return;
   const int i = warp;
+  const size_t ng = (size_t)nfx * nfy * nfz;
   const S *s = spl + (size_t)i * 3 * kOrder * 4;
   const S *sx = s, *sy = s + kOrder * 4, *sz = s + 2 * kOrder * 4;
   const int a1 = lane % 5, a2 = lane / 5;
@@ -294,7 +301,7 @@ __global__ void k_spread_induced(int n, const double *__restrict__ ud, const dou
     const S re = fma(v0, Ad, v1 * Bd);
     const S im = fma(v0, Ap, v1 * Bp);
     const int kk = wrap1(k0 + a3, nfz);
-    mesh_add(grid, (size_t)kk * nfy * nfx + row, re, im);
+    mesh_add(grid, ng, (size_t)kk * nfy * nfx + row, re, im);
   }
 }
 
@@ -376,13 +383,13 @@ __device__ __forceinline__ void fft_butterfly(const typename Vec2<S>::type *in, 
   for (int q = 0; q < R; q++) out[(idxD + q * Ns) * L + l] = y[q];
 }
 
-// FROMD (mixed form, first pass only): the input is the double accumulation mesh `src`,
-// converted to FP32 on load.
+// FROMD (mixed form, first pass only): the input is the double accumulation mesh `src`
+// (real plane, then imaginary plane at src + src_ng), converted to FP32 on load.
 template <bool FUSE_G, typename S, bool FROMD>
 __global__ void __launch_bounds__(256) k_fft_axis(typename Vec2<S>::type *grid, FftAxis ax, int sign,
                                                   const typename Vec2<S>::type *__restrict__ tw,
                                                   const S *__restrict__ G, int gnx, int gny,
-                                                  const double2 *__restrict__ src) {
+                                                  const double *__restrict__ src, size_t src_ng) {
   using V2 = typename Vec2<S>::type;
   // Shared layout is element-major, line-minor: buf[j * L + l].  Consecutive threads
   // take consecutive lines, so butterflies are bank-conflict free and the Y and Z
@@ -398,7 +405,7 @@ __global__ void __launch_bounds__(256) k_fft_axis(typename Vec2<S>::type *grid, 
     const int l = contiguous ? t / len : t % L, j = contiguous ? t % len : t / L;
     const size_t g = base + (size_t)l * ax.line_step + (size_t)j * ax.stride;
     if (FROMD) {
-      const double2 q = src[g];
+      const double2 q = make_double2(src[g], src[src_ng + g]);
       buf0[j * L + l] = mk2<S>((S)q.x, (S)q.y);
     } else {
       buf0[j * L + l] = grid[g];
@@ -482,7 +489,7 @@ template <int LEN, int L, bool FUSE_G, typename S, bool FROMD>
 __global__ void __launch_bounds__(256) k_fft_fixed(typename Vec2<S>::type *grid, FftAxis ax, int sign,
                                                    const typename Vec2<S>::type *__restrict__ twg,
                                                    const S *__restrict__ G, int gnx, int gny,
-                                                   const double2 *__restrict__ src) {
+                                                   const double *__restrict__ src, size_t src_ng) {
   using V2 = typename Vec2<S>::type;
   __shared__ V2 buf[2][LEN * L];
   __shared__ V2 tw[LEN];
@@ -494,7 +501,7 @@ __global__ void __launch_bounds__(256) k_fft_fixed(typename Vec2<S>::type *grid,
     const int l = contiguous ? t / LEN : t % L, j = contiguous ? t % LEN : t / L;
     const size_t g = base + (size_t)l * ax.line_step + (size_t)j * ax.stride;
     if (FROMD) {
-      const double2 q = src[g];
+      const double2 q = make_double2(src[g], src[src_ng + g]);
       buf[0][j * L + l] = mk2<S>((S)q.x, (S)q.y);
     } else {
       buf[0][j * L + l] = grid[g];
@@ -869,6 +876,9 @@ static void fft_convolution(Handle &h, typename Vec2<S>::type *grid, const typen
                             const S *influence) {
   const int nfx = h.nfft[0], nfy = h.nfft[1], nfz = h.nfft[2];
   const int maxn = std::max(nfx, std::max(nfy, nfz));
+  // The mixed form's accumulation mesh: real plane, then imaginary plane.
+  const double *plane = reinterpret_cast<const double *>(h.d_grid);
+  const size_t ng = (size_t)nfx * nfy * nfz;
   auto run = [&](int d, int sign, bool fuse, bool fromd) {
     const FftAxis &a = h.axes[d];
     const int outer = (d == 0) ? nfz : ((d == 1) ? nfz : nfy);
@@ -878,22 +888,24 @@ static void fft_convolution(Handle &h, typename Vec2<S>::type *grid, const typen
     if (a.len == 64 && a.L == 16) {
       if (fuse)
         k_fft_fixed<64, 16, true, S, false><<<blocks, 256, 0, h.stream>>>(grid, a, sign, tw, influence, nfx, nfy,
-                                                                          nullptr);
+                                                                          nullptr, 0);
       else if (fromd)
         k_fft_fixed<64, 16, false, S, true><<<blocks, 256, 0, h.stream>>>(grid, a, sign, tw, nullptr, nfx, nfy,
-                                                                          h.d_grid);
+                                                                          plane, ng);
       else
         k_fft_fixed<64, 16, false, S, false><<<blocks, 256, 0, h.stream>>>(grid, a, sign, tw, nullptr, nfx, nfy,
-                                                                           nullptr);
+                                                                           nullptr, 0);
       FFX_LAUNCHED(h);
       return;
     }
     if (fuse)
-      k_fft_axis<true, S, false><<<blocks, 256, smem, h.stream>>>(grid, a, sign, tw, influence, nfx, nfy, nullptr);
+      k_fft_axis<true, S, false><<<blocks, 256, smem, h.stream>>>(grid, a, sign, tw, influence, nfx, nfy, nullptr,
+                                                                  0);
     else if (fromd)
-      k_fft_axis<false, S, true><<<blocks, 256, smem, h.stream>>>(grid, a, sign, tw, nullptr, nfx, nfy, h.d_grid);
+      k_fft_axis<false, S, true><<<blocks, 256, smem, h.stream>>>(grid, a, sign, tw, nullptr, nfx, nfy, plane, ng);
     else
-      k_fft_axis<false, S, false><<<blocks, 256, smem, h.stream>>>(grid, a, sign, tw, nullptr, nfx, nfy, nullptr);
+      k_fft_axis<false, S, false><<<blocks, 256, smem, h.stream>>>(grid, a, sign, tw, nullptr, nfx, nfy, nullptr,
+                                                                   0);
     FFX_LAUNCHED(h);
   };
   const bool fromd = (sizeof(S) == 4);   // mixed: the first pass reads the double mesh
@@ -1278,10 +1290,10 @@ extern "C" int ffxg_pme_recip_permanent_noalloc(const double *d_xyz, const doubl
     const size_t smem = 2 * (size_t)ax.len * ax.L * sizeof(double2);
     if (pass == 2)
       k_fft_axis<true, double, false><<<ax.groups_inner * outer, 256, smem, st>>>(
-          grid, ax, sign, s->twiddle + d * kNaMaxDim, s->influence, nf[0], nf[1], nullptr);
+          grid, ax, sign, s->twiddle + d * kNaMaxDim, s->influence, nf[0], nf[1], nullptr, 0);
     else
       k_fft_axis<false, double, false><<<ax.groups_inner * outer, 256, smem, st>>>(
-          grid, ax, sign, s->twiddle + d * kNaMaxDim, nullptr, nf[0], nf[1], nullptr);
+          grid, ax, sign, s->twiddle + d * kNaMaxDim, nullptr, nf[0], nf[1], nullptr, 0);
   }
   const int nb = nblocks(n_atoms, kNaThreads);
   k_na_phi<<<nb, kNaThreads, 0, st>>>(n_atoms, d_xyz, d_mpole, nf[0], nf[1], nf[2], pc, d_phi, s);
