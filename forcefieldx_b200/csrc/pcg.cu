@@ -15,11 +15,12 @@
 // T z: T p = T z + beta T p_old, with T p_old kept from the previous iteration.  T z is
 // available as soon as the preconditioner has produced z, and its real-space part
 // (k_pair_field) runs on a second stream beside the spread and FFT convolution of z,
-// which leave most SMs idle.  One iteration: k_pcg_precond (z, r . z, beta), {spread z,
-// FFT} || k_pair_field, k_pcg_combine (mesh field of z, self term, T p, p, A p and its
-// dot products), k_pcg_update (r, u, norms; its last block applies the reference's
-// stopping rules on the device).  Vectors are FP64 [3][n]; every dot product is a
-// fixed-order sum of per-block partials (k_pcg_totals, or k_pcg_update's last block).
+// which leave most SMs idle.  One iteration: k_pcg_precond (z, r . z partials), {spread
+// z, FFT} || k_pair_field (and beta), k_pcg_combine (mesh field of z, self term, T p, p,
+// A p and its dot products), k_pcg_update (r, u, norms; its last block applies the
+// reference's stopping rules on the device).  Vectors are FP64 [3][n]; every dot product is a
+// fixed-order sum of per-block partials (by one block of the pair field, every block of
+// k_pcg_update, or k_pcg_update's last block).
 #include <algorithm>
 #include <cmath>
 
@@ -98,7 +99,7 @@ __device__ __forceinline__ bool block_partials(const double *v, double *part, un
 }
 
 // Block sum of NV values already reduced to lane 0 of each warp, stored as
-// part[blockIdx.x][0 .. NV) (no atomics; k_pcg_totals finishes the sum).
+// part[blockIdx.x][0 .. NV) (no atomics; beta_block or k_pcg_update finishes the sum).
 template <int NV>
 __device__ __forceinline__ void block_store_lane0(const double *v, double *part) {
   __shared__ double sh[NV][32];
@@ -115,39 +116,40 @@ __device__ __forceinline__ void block_store_lane0(const double *v, double *part)
   }
 }
 
-// Fixed-order totals of the first NV columns of nrows partial rows into tot[t0 ..], by
-// one block of 1024 threads (thread t sums rows t, t + 1024, ...; the per-thread sums are
-// added in thread order by a fixed warp tree).
-// BETA: then beta = r.z_new / r.z_old for both systems (a zero r.z_old counts as 1).
-template <int NV, bool BETA>
-__global__ void __launch_bounds__(1024) k_pcg_totals(const double *__restrict__ part, int nrows, double *tot, int t0) {
-  __shared__ double sh[NV][32];
-  double s[NV];
+// beta = r.z_new / r.z_old for both systems (a zero r.z_old counts as 1) from the
+// preconditioner's partial rows, by one whole block: thread t sums rows t, t + blockDim,
+// ... (eight rows' loads in flight), then a fixed warp tree and the warps in order.  The
+// new r.z totals go to tot[T_RZN], tot[T_RZNP].
+__device__ void beta_block(const double *__restrict__ part, int nrows, double *tot) {
+  __shared__ double sh[2][32];
+  double s0 = 0.0, s1 = 0.0;
+  constexpr int U = 8;
+  for (int b0 = threadIdx.x; b0 < nrows; b0 += U * blockDim.x) {
+    double v[U][2];
 #pragma unroll
-  for (int q = 0; q < NV; q++) s[q] = 0.0;
-  for (int b = threadIdx.x; b < nrows; b += 1024)
+    for (int u = 0; u < U; u++) {
+      const int b = b0 + u * blockDim.x;
+      v[u][0] = (b < nrows) ? part[b * 8] : 0.0;
+      v[u][1] = (b < nrows) ? part[b * 8 + 1] : 0.0;
+    }
 #pragma unroll
-    for (int q = 0; q < NV; q++) s[q] += part[b * 8 + q];
-  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
-#pragma unroll
-  for (int q = 0; q < NV; q++) {
-    const double w = warp_sum(s[q]);
-    if (lane == 0) sh[q][wid] = w;
+    for (int u = 0; u < U; u++) { s0 += v[u][0]; s1 += v[u][1]; }
   }
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = blockDim.x >> 5;
+  s0 = warp_sum(s0);
+  s1 = warp_sum(s1);
+  if (lane == 0) { sh[0][wid] = s0; sh[1][wid] = s1; }
   __syncthreads();
-  if (wid == 0) {
-#pragma unroll
-    for (int q = 0; q < NV; q++) {
-      const double t = warp_sum(sh[q][lane]);
-      if (lane == 0) tot[t0 + q] = t;
-    }
-    if (BETA && lane == 0) {
-      double old = tot[T_RZ], oldP = tot[T_RZP];
-      if (old == 0.0) old = 1.0;
-      if (oldP == 0.0) oldP = 1.0;
-      tot[T_BETA] = tot[T_RZN] / old;
-      tot[T_BETAP] = tot[T_RZNP] / oldP;
-    }
+  if (threadIdx.x == 0) {
+    double t0 = 0.0, t1 = 0.0;
+    for (int w = 0; w < nw; w++) { t0 += sh[0][w]; t1 += sh[1][w]; }
+    tot[T_RZN] = t0;
+    tot[T_RZNP] = t1;
+    double old = tot[T_RZ], oldP = tot[T_RZP];
+    if (old == 0.0) old = 1.0;
+    if (oldP == 0.0) oldP = 1.0;
+    tot[T_BETA] = t0 / old;
+    tot[T_BETAP] = t1 / oldP;
   }
 }
 
@@ -252,7 +254,12 @@ __global__ void __launch_bounds__(kFieldThreads) k_pair_field(int n, const int *
                                                               const int *__restrict__ ewl_cnt, int capE,
                                                               const PairRec<T> *__restrict__ coefE,
                                                               const T *__restrict__ coefEB,
-                                                              const T *__restrict__ rec, double *out) {
+                                                              const T *__restrict__ rec, double *out,
+                                                              const double *__restrict__ beta_part, int beta_rows,
+                                                              double *tot) {
+  // Block 0 first forms beta from the preconditioner's partial rows (the combine, after
+  // the join, reads it): no separate totals launch on the solver's chain.
+  if (beta_part && blockIdx.x == 0) beta_block(beta_part, beta_rows, tot);
   constexpr int GPW = 32 / G;
   const int lane = threadIdx.x & 31, sub = lane & (G - 1), gi = lane / G;
   const int astride = gridDim.x * (blockDim.x >> 5) * GPW;
@@ -468,20 +475,32 @@ __global__ void __launch_bounds__(kVecThreads) k_pcg_update(
   double v[2] = {0.0, 0.0};
   const int stride = gridDim.x * blockDim.x;
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) {
-    double nr[6];
+    // Every load first (one memory round trip), then the arithmetic, then the stores.
+    double r0[3], r1[3], v0[3], v1[3], p0[3], p1[3], u0[3], u1[3];
+#pragma unroll
     for (int d = 0; d < 3; d++) {
       const size_t j = (size_t)d * n + i;
-      const double rr = r[j] - alpha0 * vec[j];
-      const double rp = rP[j] - alpha1 * vecP[j];
-      r[j] = rr; rP[j] = rp;
-      uD[j] += alpha0 * p[j];
-      uP[j] += alpha1 * pP[j];
+      r0[d] = r[j]; r1[d] = rP[j]; v0[d] = vec[j]; v1[d] = vecP[j];
+      p0[d] = p[j]; p1[d] = pP[j]; u0[d] = uD[j]; u1[d] = uP[j];
+    }
+    const double a = polar[i];
+    double nr[6];
+#pragma unroll
+    for (int d = 0; d < 3; d++) {
+      const double rr = r0[d] - alpha0 * v0[d];
+      const double rp = r1[d] - alpha1 * v1[d];
       v[0] += rr * rr;
       v[1] += rp * rp;
       nr[d] = rr;
       nr[3 + d] = rp;
+      u0[d] += alpha0 * p0[d];
+      u1[d] += alpha1 * p1[d];
     }
-    const double a = polar[i];
+#pragma unroll
+    for (int d = 0; d < 3; d++) {
+      const size_t j = (size_t)d * n + i;
+      r[j] = nr[d]; rP[j] = nr[3 + d]; uD[j] = u0[d]; uP[j] = u1[d];
+    }
     put_rec(recP, i, a * nr[0], a * nr[1], a * nr[2], a * nr[3], a * nr[4], a * nr[5]);
   }
   __shared__ double norms[2];
@@ -586,18 +605,12 @@ int pcg_partial_rows(int n) {
 }
 static double *part_region(const Handle &h, int k) { return h.d_part2 + (size_t)k * h.part_rows * 8; }
 
-// beta = r.z_new / r.z_old from the preconditioner's partial rows (the totals kernel).
-static void beta_totals(Handle &h, cudaStream_t st) {
-  k_pcg_totals<2, true><<<1, 1024, 0, st>>>(part_region(h, 1), group_blocks(h.n, kPrecondGroup), h.d_scalars,
-                                            T_RZN);
-  FFX_LAUNCHED(h);
-}
-
 template <typename T>
-static void pair_field_launch(Handle &h, cudaStream_t st) {
+static void pair_field_launch(Handle &h, cudaStream_t st, bool beta) {
   k_pair_field<T, kEwaldGroup><<<group_blocks(h.n, kEwaldGroup), kFieldThreads, 0, st>>>(
       h.n, h.d_ewl, h.d_ewl_cnt, h.cap_ewl, reinterpret_cast<const PairRec<T> *>(h.d_coefE),
-      reinterpret_cast<const T *>(h.d_coefEB), reinterpret_cast<const T *>(h.d_recF), h.d_tpair);
+      reinterpret_cast<const T *>(h.d_coefEB), reinterpret_cast<const T *>(h.d_recF), h.d_tpair,
+      beta ? part_region(h, 1) : nullptr, group_blocks(h.n, kPrecondGroup), h.d_scalars);
   FFX_LAUNCHED(h);
 }
 
@@ -623,7 +636,9 @@ static void field_of(Handle &h, const double *vD, const double *vP, bool first, 
   cudaEventRecord(h.ev_fork, h.stream);
   cudaStreamWaitEvent(ax, h.ev_fork, 0);
   int tk = timer_begin_on(h, FFXG_STAGE_IND_FIELD, ax);
-  if (h.mixed) pair_field_launch<float>(h, ax); else pair_field_launch<double>(h, ax);
+  // After a non-initial preconditioner step the pair field also forms beta.
+  const bool beta = (MODE == 2) && !first;
+  if (h.mixed) pair_field_launch<float>(h, ax, beta); else pair_field_launch<double>(h, ax, beta);
   timer_end_on(h, tk, ax);
   cudaEventRecord(h.ev_join, ax);
   tk = timer_begin(h, FFXG_STAGE_IND_RECIP);
@@ -645,9 +660,6 @@ static void precond(Handle &h) {
       h.prm.precond_scale, h.d_zpre, h.d_zpreP, h.d_p, h.d_pP, reinterpret_cast<T *>(h.d_recF), part_region(h, 1),
       h.d_counter + K_PRECOND, h.d_scalars);
   FFX_LAUNCHED(h);
-  // On the main stream: on the low-priority side stream the one-block totals wait for the
-  // spread to drain and hold back the pair field behind them (measured slower).
-  if (!INIT) beta_totals(h, h.stream);
 }
 
 template <bool INIT>
