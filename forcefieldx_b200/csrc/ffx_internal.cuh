@@ -390,6 +390,8 @@ struct Handle {
   float2 *d_gridf = nullptr;
   float *d_influencef = nullptr;
   float2 *d_twiddlef = nullptr;
+  // The mixed form's accumulation mesh as two planes of doubles (real, imaginary).
+  double *d_grid_planes() const { return reinterpret_cast<double *>(d_grid); }
   PmeConst pc{};
   FftAxis axes[3]{};
 

@@ -344,6 +344,7 @@ static int create_impl(const ffxg_system *s, const ffxg_params *p, Handle &h) {
   const int nfx = p->pme_grid[0], nfy = p->pme_grid[1], nfz = p->pme_grid[2];
   const size_t ng = (size_t)nfx * nfy * nfz;
   CK(dalloc(&h.d_grid, ng)); CK(dalloc(&h.d_influence, ng));
+  CK(cudaMemset(h.d_grid, 0, ng * sizeof(double2)));   // the mixed form keeps it clear between uses
   CK(dalloc(&h.d_twiddle, 3 * (size_t)std::max(nfx, std::max(nfy, nfz))));
   if (h.mixed) {
     CK(dalloc(&h.d_gridf, ng));

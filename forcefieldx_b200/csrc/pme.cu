@@ -15,7 +15,11 @@
 #include <cmath>
 #include <cstring>
 
+#include <cooperative_groups.h>
+
 #include "ffx_internal.cuh"
+
+namespace cg = cooperative_groups;
 
 namespace ffx {
 
@@ -384,12 +388,13 @@ __device__ __forceinline__ void fft_butterfly(const typename Vec2<S>::type *in, 
 }
 
 // FROMD (mixed form, first pass only): the input is the double accumulation mesh `src`
-// (real plane, then imaginary plane at src + src_ng), converted to FP32 on load.
+// (real plane, then imaginary plane at src + src_ng), converted to FP32 on load and
+// cleared behind the read, so that the next spread starts from zero without a memset.
 template <bool FUSE_G, typename S, bool FROMD>
 __global__ void __launch_bounds__(256) k_fft_axis(typename Vec2<S>::type *grid, FftAxis ax, int sign,
                                                   const typename Vec2<S>::type *__restrict__ tw,
                                                   const S *__restrict__ G, int gnx, int gny,
-                                                  const double *__restrict__ src, size_t src_ng) {
+                                                  double *src, size_t src_ng) {
   using V2 = typename Vec2<S>::type;
   // Shared layout is element-major, line-minor: buf[j * L + l].  Consecutive threads
   // take consecutive lines, so butterflies are bank-conflict free and the Y and Z
@@ -406,6 +411,8 @@ __global__ void __launch_bounds__(256) k_fft_axis(typename Vec2<S>::type *grid, 
     const size_t g = base + (size_t)l * ax.line_step + (size_t)j * ax.stride;
     if (FROMD) {
       const double2 q = make_double2(src[g], src[src_ng + g]);
+      src[g] = 0.0;
+      src[src_ng + g] = 0.0;
       buf0[j * L + l] = mk2<S>((S)q.x, (S)q.y);
     } else {
       buf0[j * L + l] = grid[g];
@@ -467,7 +474,9 @@ __host__ __device__ constexpr int plan_radix(int len, int st) {
   return 0;
 }
 
-template <int LEN, int ST, int NS, int L, typename S>
+// LS: the element stride of the shared layout (L, or L + 1 to spread a line's elements
+// over the banks when lines are loaded along their elements).
+template <int LEN, int ST, int NS, int L, typename S, int LS = L>
 __device__ __forceinline__ void fixed_stages(typename Vec2<S>::type *&in, typename Vec2<S>::type *&out,
                                              const typename Vec2<S>::type *tw, int sg) {
   constexpr int R = plan_radix(LEN, ST);
@@ -475,13 +484,105 @@ __device__ __forceinline__ void fixed_stages(typename Vec2<S>::type *&in, typena
     constexpr int NB = LEN / R;
     for (int t = threadIdx.x; t < NB * L; t += 256) {
       const int l = t % L, j = t / L;
-      fft_butterfly<R, S>(in, out, j, l, L, NB, NS, LEN, sg, tw);
+      fft_butterfly<R, S>(in, out, j, l, LS, NB, NS, LEN, sg, tw);
     }
     __syncthreads();
     typename Vec2<S>::type *tmp = in;
     in = out;
     out = tmp;
-    fixed_stages<LEN, ST + 1, NS * R, L, S>(in, out, tw, sg);
+    fixed_stages<LEN, ST + 1, NS * R, L, S, LS>(in, out, tw, sg);
+  }
+}
+
+// Two-dimensional FFT of the 64 x 64 (x, y) planes of an FP32 mesh by a cluster of four
+// CTAs per z plane.  Forward: CTA c transforms rows y in [16c, 16c + 16) along x, the
+// cluster synchronises, and CTA c gathers columns x in [16c, 16c + 16) of every row from
+// the four CTAs' shared memory and transforms them along y.  Inverse: the same with the
+// axes swapped (y first, then x).  Two mesh passes become one launch, and the exchange
+// between them stays on chip.  FROMD (forward only): the input is the planar double
+// accumulation mesh (real plane, imaginary plane at + src_ng), which is cleared behind
+// the read so that the next spread starts from zero.
+template <bool INVERSE, bool FROMD>
+__global__ void __cluster_dims__(4, 1, 1) __launch_bounds__(256)
+    k_fft_plane64(float2 *grid, int sign, const float2 *__restrict__ twg, double *src, size_t src_ng) {
+  constexpr int LEN = 64, L = 16, LS = L + 1, NP = LEN * L, NB = LEN * LS, PER = NP / 256;
+  __shared__ float2 buf[3][NB];
+  __shared__ float2 tw[LEN];
+  cg::cluster_group cluster = cg::this_cluster();
+  const int c = (int)cluster.block_rank();
+  const size_t plane = (size_t)(blockIdx.x >> 2) * LEN * LEN;
+  for (int t = threadIdx.x; t < LEN; t += 256) tw[t] = twg[t];
+  // Phase A lines: rows [16c, 16c + 16) along x (forward) or columns (inverse), stored
+  // element-major, line-minor with stride LS: a[j * LS + l].  All loads of a thread are
+  // issued before any store.
+  {
+    float2 v[PER];
+    size_t g[PER];
+    int at[PER];
+#pragma unroll
+    for (int u = 0; u < PER; u++) {
+      const int t = threadIdx.x + 256 * u;
+      int j, l;
+      if (!INVERSE) {   // row l = t / 64, element x = t % 64 (coalesced rows)
+        l = t / LEN; j = t % LEN;
+        g[u] = plane + (size_t)(16 * c + l) * LEN + j;
+      } else {          // column x = 16c + t % 16, element y = t / 16
+        l = t % L; j = t / L;
+        g[u] = plane + (size_t)j * LEN + 16 * c + l;
+      }
+      at[u] = j * LS + l;
+      v[u] = FROMD ? make_float2((float)src[g[u]], (float)src[src_ng + g[u]]) : grid[g[u]];
+    }
+#pragma unroll
+    for (int u = 0; u < PER; u++) {
+      if (FROMD) {
+        src[g[u]] = 0.0;
+        src[src_ng + g[u]] = 0.0;
+      }
+      buf[0][at[u]] = v[u];
+    }
+  }
+  __syncthreads();
+  float2 *in = buf[0], *out = buf[1];
+  fixed_stages<LEN, 0, 1, L, float, LS>(in, out, tw, sign);
+  // The first phase's result sits at the same offset in every CTA of the cluster.
+  const int res = (int)((in - &buf[0][0]) / NB);
+  const int spare = (res == 0) ? 1 : 0;
+  cluster.sync();
+  // Phase B lines: the other axis, gathered from the four CTAs into buf[2].  Forward:
+  // element y = j of column x = 16c + l lives in CTA y / 16 as its row y % 16, element x.
+  // Inverse: element x = j of row y = 16c + l lives in CTA x / 16 as its column x % 16,
+  // element y.  Both sit at [(16c + l) * LS + j % 16] of the owner.
+  {
+    float2 v[PER];
+#pragma unroll
+    for (int u = 0; u < PER; u++) {
+      const int t = threadIdx.x + 256 * u;
+      const int l = t % L, j = t / L;
+      const float2 *peer = cluster.map_shared_rank(&buf[res][0], j >> 4);
+      v[u] = peer[(16 * c + l) * LS + (j & 15)];
+    }
+#pragma unroll
+    for (int u = 0; u < PER; u++) {
+      const int t = threadIdx.x + 256 * u;
+      buf[2][(t / L) * LS + t % L] = v[u];
+    }
+  }
+  cluster.sync();   // every peer has read this CTA's phase-A result
+  in = buf[2];
+  out = buf[spare];
+  fixed_stages<LEN, 0, 1, L, float, LS>(in, out, tw, sign);
+  for (int t = threadIdx.x; t < NP; t += 256) {
+    size_t g;
+    int j, l;
+    if (!INVERSE) {   // column x = 16c + t % 16, element y = t / 16
+      l = t % L; j = t / L;
+      g = plane + (size_t)j * LEN + 16 * c + l;
+    } else {          // row y = 16c + t / 64, element x = t % 64
+      l = t / LEN; j = t % LEN;
+      g = plane + (size_t)(16 * c + l) * LEN + j;
+    }
+    grid[g] = in[j * LS + l];
   }
 }
 
@@ -489,7 +590,7 @@ template <int LEN, int L, bool FUSE_G, typename S, bool FROMD>
 __global__ void __launch_bounds__(256) k_fft_fixed(typename Vec2<S>::type *grid, FftAxis ax, int sign,
                                                    const typename Vec2<S>::type *__restrict__ twg,
                                                    const S *__restrict__ G, int gnx, int gny,
-                                                   const double *__restrict__ src, size_t src_ng) {
+                                                   double *src, size_t src_ng) {
   using V2 = typename Vec2<S>::type;
   __shared__ V2 buf[2][LEN * L];
   __shared__ V2 tw[LEN];
@@ -502,6 +603,8 @@ __global__ void __launch_bounds__(256) k_fft_fixed(typename Vec2<S>::type *grid,
     const size_t g = base + (size_t)l * ax.line_step + (size_t)j * ax.stride;
     if (FROMD) {
       const double2 q = make_double2(src[g], src[src_ng + g]);
+      src[g] = 0.0;
+      src[src_ng + g] = 0.0;
       buf[0][j * L + l] = mk2<S>((S)q.x, (S)q.y);
     } else {
       buf[0][j * L + l] = grid[g];
@@ -843,12 +946,13 @@ void launch_bsplines(Handle &h) {
 
 static size_t grid_points(const Handle &h) { return (size_t)h.nfft[0] * h.nfft[1] * h.nfft[2]; }
 
-// Both forms accumulate into the double mesh d_grid (cleared first); the mixed form's
-// FFT continues in the FP32 mesh d_gridf.
+// Both forms accumulate into the double mesh d_grid; the FP64 form clears it first, the
+// mixed form keeps it clear between uses (its first FFT pass zeroes what it reads) and
+// continues in the FP32 mesh d_gridf.
 void launch_spread_permanent(Handle &h) {
   if (h.vacuum) return;   // no reciprocal space: the mesh and potentials stay zero
   const int nb = nblocks((int64_t)h.n * 32, 256);
-  cudaMemsetAsync(h.d_grid, 0, grid_points(h) * sizeof(double2), h.stream);
+  if (!h.mixed) cudaMemsetAsync(h.d_grid, 0, grid_points(h) * sizeof(double2), h.stream);
   if (h.mixed)
     k_spread_permanent<float><<<nb, 256, 0, h.stream>>>(h.n, h.d_fm, reinterpret_cast<const float *>(h.d_spl),
                                                         h.d_igrid, h.nfft[0], h.nfft[1], h.nfft[2], h.d_grid);
@@ -861,7 +965,7 @@ void launch_spread_permanent(Handle &h) {
 void launch_spread_induced(Handle &h, const double *ud, const double *up) {
   if (h.vacuum) return;   // no reciprocal space: the mesh and potentials stay zero
   const int nb = nblocks((int64_t)h.n * 32, 256);
-  cudaMemsetAsync(h.d_grid, 0, grid_points(h) * sizeof(double2), h.stream);
+  if (!h.mixed) cudaMemsetAsync(h.d_grid, 0, grid_points(h) * sizeof(double2), h.stream);
   if (h.mixed)
     k_spread_induced<float><<<nb, 256, 0, h.stream>>>(h.n, ud, up, reinterpret_cast<const float *>(h.d_spl), h.d_igrid,
                                                       h.nfft[0], h.nfft[1], h.nfft[2], h.d_grid, h.pc);
@@ -877,7 +981,7 @@ static void fft_convolution(Handle &h, typename Vec2<S>::type *grid, const typen
   const int nfx = h.nfft[0], nfy = h.nfft[1], nfz = h.nfft[2];
   const int maxn = std::max(nfx, std::max(nfy, nfz));
   // The mixed form's accumulation mesh: real plane, then imaginary plane.
-  const double *plane = reinterpret_cast<const double *>(h.d_grid);
+  double *plane = h.d_grid_planes();
   const size_t ng = (size_t)nfx * nfy * nfz;
   auto run = [&](int d, int sign, bool fuse, bool fromd) {
     const FftAxis &a = h.axes[d];
@@ -909,6 +1013,17 @@ static void fft_convolution(Handle &h, typename Vec2<S>::type *grid, const typen
     FFX_LAUNCHED(h);
   };
   const bool fromd = (sizeof(S) == 4);   // mixed: the first pass reads the double mesh
+  if (sizeof(S) == 4 && nfx == 64 && nfy == 64 && h.axes[2].len == 64 && h.axes[2].L == 16) {
+    // Mixed form on 64 x 64 planes: xy, z (with the influence function), yx.
+    float2 *gf = reinterpret_cast<float2 *>(grid);
+    const float2 *tw = reinterpret_cast<const float2 *>(twiddle);
+    k_fft_plane64<false, true><<<nfz * 4, 256, 0, h.stream>>>(gf, -1, tw, h.d_grid_planes(), ng);
+    FFX_LAUNCHED(h);
+    run(2, -1, true, false);
+    k_fft_plane64<true, false><<<nfz * 4, 256, 0, h.stream>>>(gf, +1, tw, nullptr, 0);
+    FFX_LAUNCHED(h);
+    return;
+  }
   run(0, -1, false, fromd);
   run(1, -1, false, false);
   run(2, -1, true, false);
