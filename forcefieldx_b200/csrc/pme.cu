@@ -630,101 +630,103 @@ __global__ void __launch_bounds__(256) k_fft_fixed(typename Vec2<S>::type *grid,
 }
 
 // ---------------------------------------------------------------------------
-// Potential and derivatives at each atom (20 fractional terms -> Cartesian).
+// Sum over the 32 lanes of v[0 .. 32): after a halving butterfly (16 + 8 + 4 + 2 + 1
+// shuffles instead of five per value) lane l holds the total of entry l.  Fixed order.
+template <typename S>
+__device__ __forceinline__ S lane_totals32(S (&v)[32]) {
+  const int lane = threadIdx.x & 31;
+#pragma unroll
+  for (int s = 16; s >= 1; s >>= 1) {
+    const bool upper = (lane & s) != 0;
+#pragma unroll
+    for (int k = 0; k < s; k++) {
+      const S send = upper ? v[k] : v[k + s];
+      const S keep = upper ? v[k + s] : v[k];
+      v[k] = keep + __shfl_xor_sync(0xffffffffu, send, s);
+    }
+  }
+  return v[0];
+}
+
+// Potential and its derivatives at each atom from the mesh (real or imaginary part), one
+// warp per atom: lane l < 25 owns the (x, y) support column (l % 5, l / 5) and walks the
+// five z layers, then the lanes' partial sums are totalled with lane_totals32 (lane t
+// holds term t).  The reference's order of terms (ReciprocalSpace.java:2506-2775).
 template <int NT, typename S>
-__device__ __forceinline__ void interp(int i, int n, const S *__restrict__ spl, const int *__restrict__ igrid,
-                                       const typename Vec2<S>::type *__restrict__ grid, int nfx, int nfy, int nfz,
-                                       bool imag, S *tuv) {
-  const S *s = spl + (size_t)i * 3 * kOrder * 4;
-  const S *sx = s, *sy = s + kOrder * 4, *sz = s + 2 * kOrder * 4;
-  const int i0 = igrid[i], j0 = igrid[n + i], k0 = igrid[2 * n + i];
+__device__ __forceinline__ S phi_terms_warp(int i, int n, const S *__restrict__ spl, const int *__restrict__ igrid,
+                                            const typename Vec2<S>::type *__restrict__ grid, int nfx, int nfy,
+                                            int nfz, bool imag) {
+  const int lane = threadIdx.x & 31;
+  S v[32];
 #pragma unroll
-  for (int t = 0; t < NT; t++) tuv[t] = S(0);
-  for (int a3 = 0; a3 < kOrder; a3++) {
-    const int kk = jmod(k0 + 1 + a3, nfz);
-    S tu00 = 0, tu10 = 0, tu01 = 0, tu20 = 0, tu11 = 0, tu02 = 0, tu30 = 0, tu21 = 0, tu12 = 0, tu03 = 0;
-    for (int a2 = 0; a2 < kOrder; a2++) {
-      const int jj = jmod(j0 + 1 + a2, nfy);
-      S t0 = 0, t1 = 0, t2 = 0, t3 = 0;
+  for (int t = 0; t < 32; t++) v[t] = S(0);
+  if (lane < 25) {
+    const S *sp = spl + (size_t)i * 3 * kOrder * 4;
+    const S *sx = sp + (lane % 5) * 4, *sy = sp + kOrder * 4 + (lane / 5) * 4, *sz = sp + 2 * kOrder * 4;
+    const int ii = wrap1(igrid[i] + 1 + lane % 5, nfx), jj = wrap1(igrid[n + i] + 1 + lane / 5, nfy);
+    const int k0 = igrid[2 * n + i] + 1;
+    const S x0 = sx[0], x1 = sx[1], x2 = sx[2], x3 = sx[3];
+    const S y0 = sy[0], y1 = sy[1], y2 = sy[2], y3 = sy[3];
+    const S a00 = x0 * y0, a10 = x1 * y0, a01 = x0 * y1, a20 = x2 * y0, a02 = x0 * y2, a11 = x1 * y1;
+    const S a30 = x3 * y0, a03 = x0 * y3, a21 = x2 * y1, a12 = x1 * y2;
+    const auto *col = grid + (size_t)jj * nfx + ii;
 #pragma unroll
-      for (int a1 = 0; a1 < kOrder; a1++) {
-        const int ii = jmod(i0 + 1 + a1, nfx);
-        const auto gv = grid[((size_t)kk * nfy + jj) * nfx + ii];
-        const S tq = imag ? gv.y : gv.x;
-        t0 = fma(tq, sx[a1 * 4], t0);
-        t1 = fma(tq, sx[a1 * 4 + 1], t1);
-        if (NT > 4) {
-          t2 = fma(tq, sx[a1 * 4 + 2], t2);
-          t3 = fma(tq, sx[a1 * 4 + 3], t3);
-        }
-      }
-      const S u0 = sy[a2 * 4], u1 = sy[a2 * 4 + 1], u2 = sy[a2 * 4 + 2], u3 = sy[a2 * 4 + 3];
-      tu00 = fma(t0, u0, tu00); tu10 = fma(t1, u0, tu10); tu01 = fma(t0, u1, tu01);
+    for (int a3 = 0; a3 < kOrder; a3++) {
+      const auto gv = col[(size_t)wrap1(k0 + a3, nfz) * nfy * nfx];
+      const S q = imag ? gv.y : gv.x;
+      const S q0 = q * sz[a3 * 4], q1 = q * sz[a3 * 4 + 1];
+      v[t000] = fma(a00, q0, v[t000]); v[t100] = fma(a10, q0, v[t100]);
+      v[t010] = fma(a01, q0, v[t010]); v[t001] = fma(a00, q1, v[t001]);
       if (NT > 4) {
-        tu20 = fma(t2, u0, tu20); tu11 = fma(t1, u1, tu11); tu02 = fma(t0, u2, tu02);
-        tu30 = fma(t3, u0, tu30); tu21 = fma(t2, u1, tu21); tu12 = fma(t1, u2, tu12); tu03 = fma(t0, u3, tu03);
+        const S q2 = q * sz[a3 * 4 + 2], q3 = q * sz[a3 * 4 + 3];
+        v[t200] = fma(a20, q0, v[t200]); v[t020] = fma(a02, q0, v[t020]);
+        v[t002] = fma(a00, q2, v[t002]); v[t110] = fma(a11, q0, v[t110]);
+        v[t101] = fma(a10, q1, v[t101]); v[t011] = fma(a01, q1, v[t011]);
+        v[t300] = fma(a30, q0, v[t300]); v[t030] = fma(a03, q0, v[t030]);
+        v[t003] = fma(a00, q3, v[t003]); v[t210] = fma(a21, q0, v[t210]);
+        v[t201] = fma(a20, q1, v[t201]); v[t120] = fma(a12, q0, v[t120]);
+        v[t021] = fma(a02, q1, v[t021]); v[t102] = fma(a10, q2, v[t102]);
+        v[t012] = fma(a01, q2, v[t012]); v[t111] = fma(a11, q1, v[t111]);
       }
     }
-    const S v0 = sz[a3 * 4], v1 = sz[a3 * 4 + 1], v2 = sz[a3 * 4 + 2], v3 = sz[a3 * 4 + 3];
-    tuv[t000] = fma(tu00, v0, tuv[t000]); tuv[t100] = fma(tu10, v0, tuv[t100]);
-    tuv[t010] = fma(tu01, v0, tuv[t010]); tuv[t001] = fma(tu00, v1, tuv[t001]);
-    if (NT > 4) {
-      tuv[t200] = fma(tu20, v0, tuv[t200]); tuv[t020] = fma(tu02, v0, tuv[t020]);
-      tuv[t002] = fma(tu00, v2, tuv[t002]); tuv[t110] = fma(tu11, v0, tuv[t110]);
-      tuv[t101] = fma(tu10, v1, tuv[t101]); tuv[t011] = fma(tu01, v1, tuv[t011]);
-      tuv[t300] = fma(tu30, v0, tuv[t300]); tuv[t030] = fma(tu03, v0, tuv[t030]);
-      tuv[t003] = fma(tu00, v3, tuv[t003]); tuv[t210] = fma(tu21, v0, tuv[t210]);
-      tuv[t201] = fma(tu20, v1, tuv[t201]); tuv[t120] = fma(tu12, v0, tuv[t120]);
-      tuv[t021] = fma(tu02, v1, tuv[t021]); tuv[t102] = fma(tu10, v2, tuv[t102]);
-      tuv[t012] = fma(tu01, v2, tuv[t012]); tuv[t111] = fma(tu11, v1, tuv[t111]);
-    }
   }
+  return lane_totals32<S>(v);
 }
 
-template <int NT>
-__device__ __forceinline__ void store_phi(int i, int n, const double *tuv, double *fphi, double *cphi,
-                                          const PmeConst &pc) {
-  if (fphi) {
+// fphi (fractional terms, lane t < NT writes term t) and cphi (Cartesian: lane j < 10
+// transforms the terms it gathers from the lanes that hold them).
+template <int NT, typename S>
+__device__ __forceinline__ void store_phi_warp(int i, int n, S term, double *fphi, double *cphi, const PmeConst &pc) {
+  const int lane = threadIdx.x & 31;
+  const double tv = (double)term;
+  if (fphi && lane < NT) fphi[(size_t)lane * n + i] = tv;
+  double g[10];
 #pragma unroll
-    for (int t = 0; t < NT; t++) fphi[t * n + i] = tuv[t];
+  for (int k = 0; k < 10; k++) g[k] = __shfl_sync(0xffffffffu, tv, k);
+  double c = 0.0;
+  if (lane == 0) {
+    c = pc.tfm[0][0] * g[0];
+  } else if (lane < 4) {
+#pragma unroll
+    for (int k = 1; k < 4; k++) c = fma(pc.tfm[lane][k], g[k], c);
+  } else if (lane < 10 && NT > 4) {
+#pragma unroll
+    for (int k = 4; k < 10; k++) c = fma(pc.tfm[lane][k], g[k], c);
   }
-  cphi[i] = pc.tfm[0][0] * tuv[0];
-#pragma unroll
-  for (int j = 1; j < 4; j++) {
-    double s = 0.0;
-#pragma unroll
-    for (int k = 1; k < 4; k++) s = fma(pc.tfm[j][k], tuv[k], s);
-    cphi[j * n + i] = s;
-  }
-  if (NT > 4) {
-#pragma unroll
-    for (int j = 4; j < 10; j++) {
-      double s = 0.0;
-#pragma unroll
-      for (int k = 4; k < 10; k++) s = fma(pc.tfm[j][k], tuv[k], s);
-      cphi[j * n + i] = s;
-    }
-  }
+  if (lane < (NT > 4 ? 10 : 4)) cphi[(size_t)lane * n + i] = c;
 }
 
 template <int NT, typename S>
-__global__ void k_phi(int n, const S *__restrict__ spl, const int *__restrict__ igrid,
-                      const typename Vec2<S>::type *__restrict__ grid, int nfx, int nfy, int nfz, double *fphiR,
-                      double *cphiR, double *fphiI, double *cphiI, PmeConst pc) {
-  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+__global__ void __launch_bounds__(256) k_phi(int n, const S *__restrict__ spl, const int *__restrict__ igrid,
+                                             const typename Vec2<S>::type *__restrict__ grid, int nfx, int nfy,
+                                             int nfz, double *fphiR, double *cphiR, double *fphiI, double *cphiI,
+                                             const __grid_constant__ PmeConst pc) {
+  const int i = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   if (i >= n) return;
-  S tuv[NT];
-  double td[NT];
-  interp<NT, S>(i, n, spl, igrid, grid, nfx, nfy, nfz, false, tuv);
-#pragma unroll
-  for (int t = 0; t < NT; t++) td[t] = (double)tuv[t];
-  store_phi<NT>(i, n, td, fphiR, cphiR, pc);
-  if (cphiI) {
-    interp<NT, S>(i, n, spl, igrid, grid, nfx, nfy, nfz, true, tuv);
-#pragma unroll
-    for (int t = 0; t < NT; t++) td[t] = (double)tuv[t];
-    store_phi<NT>(i, n, td, fphiI, cphiI, pc);
-  }
+  store_phi_warp<NT, S>(i, n, phi_terms_warp<NT, S>(i, n, spl, igrid, grid, nfx, nfy, nfz, false), fphiR, cphiR, pc);
+  if (cphiI)
+    store_phi_warp<NT, S>(i, n, phi_terms_warp<NT, S>(i, n, spl, igrid, grid, nfx, nfy, nfz, true), fphiI, cphiI,
+                          pc);
 }
 
 // ---------------------------------------------------------------------------
@@ -1044,11 +1046,13 @@ static void phi(Handle &h, int which) {
   const S *spl = reinterpret_cast<const S *>(h.d_spl);
   const auto *grid = reinterpret_cast<const typename Vec2<S>::type *>(h.mixed ? (void *)h.d_gridf : (void *)h.d_grid);
   if (which == 0)
-    k_phi<20, S><<<nblocks(h.n, 128), 128, 0, h.stream>>>(h.n, spl, h.d_igrid, grid, h.nfft[0], h.nfft[1], h.nfft[2],
-                                                         h.d_fphi, h.d_cphi, nullptr, nullptr, h.pc);
+    k_phi<20, S><<<nblocks((int64_t)h.n * 32, 256), 256, 0, h.stream>>>(h.n, spl, h.d_igrid, grid, h.nfft[0],
+                                                                        h.nfft[1], h.nfft[2], h.d_fphi, h.d_cphi,
+                                                                        nullptr, nullptr, h.pc);
   else
-    k_phi<20, S><<<nblocks(h.n, 128), 128, 0, h.stream>>>(h.n, spl, h.d_igrid, grid, h.nfft[0], h.nfft[1], h.nfft[2],
-                                                         h.d_fphiI, h.d_cphiI, h.d_fphiP, h.d_cphiP, h.pc);
+    k_phi<20, S><<<nblocks((int64_t)h.n * 32, 256), 256, 0, h.stream>>>(h.n, spl, h.d_igrid, grid, h.nfft[0],
+                                                                        h.nfft[1], h.nfft[2], h.d_fphiI, h.d_cphiI,
+                                                                        h.d_fphiP, h.d_cphiP, h.pc);
   FFX_LAUNCHED(h);
 }
 

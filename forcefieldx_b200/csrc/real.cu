@@ -235,7 +235,7 @@ __global__ void __launch_bounds__(128, sizeof(R) == 4 ? 8 : 1) k_realspace_field
 // permanent part, the polarization part is scaled by polScale, and dU/dL, d2U/dL2, the
 // lambda gradient and torque are gathered (written to edl/ed2l/lgrad/ltorque).
 template <typename R, bool LAM>
-__global__ void __launch_bounds__(128) k_real_energy(
+__global__ void __launch_bounds__(128, sizeof(R) == 4 ? 4 : 1) k_real_energy(
     int n, const double *__restrict__ x, const double *__restrict__ y, const double *__restrict__ z, Box bx,
     const double *__restrict__ gm, const double *__restrict__ uD, const double *__restrict__ uP,
     const double *__restrict__ ipdamp, const double *__restrict__ thole, const int *__restrict__ ewl,
