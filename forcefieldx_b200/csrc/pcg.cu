@@ -33,9 +33,10 @@ constexpr int kVecThreads = 256;
 constexpr int kVecBlocks = 148 * 2;
 // Lane groups of the pair-field kernels: G lanes per atom (a warp takes 32 / G atoms), a
 // grid that gives every group one atom.  The short preconditioner rows (~40 pairs at
-// 4.5 A) take 8 lanes, the Ewald rows (~140 pairs at 7 A) 16.  Grids follow the system
+// 4.5 A) take 4 lanes with four gathers in flight each, the Ewald rows (~140 pairs at
+// 7 A) 16 lanes with two (measured best of 4/8 and 8/16/32).  Grids follow the system
 // size, so the kernels of many small systems can share the device (batches).
-constexpr int kPrecondGroup = 8;
+constexpr int kPrecondGroup = 4;
 constexpr int kEwaldGroup = 16;
 static int group_blocks(int n, int G) { return std::max(1, (n + kFieldThreads / G - 1) / (kFieldThreads / G)); }
 // The vector kernels stride over atoms with a fixed grid for large systems.
@@ -369,8 +370,8 @@ __global__ void __launch_bounds__(kFieldThreads) k_pcg_precond(
     const PairRec<T> *__restrict__ coefP, const T *__restrict__ coefPB, const T *__restrict__ recP,
     const double *__restrict__ polar, const double *__restrict__ r, const double *__restrict__ rP, double s,
     double *zz, double *zP, double *p, double *pP, T *recF, double *part, unsigned *counter, double *tot) {
-  static_assert(G >= 8, "lanes 0-5 of a group finish the six components");
   constexpr int GPW = 32 / G;
+  constexpr int QPL = (6 + G - 1) / G;   // components finished per lane: q = sub, sub + G, ...
   const int lane = threadIdx.x & 31, sub = lane & (G - 1), gi = lane / G, g0 = lane & ~(G - 1);
   const int astride = gridDim.x * (blockDim.x >> 5) * GPW;
   double acc[2] = {0, 0};
@@ -378,28 +379,34 @@ __global__ void __launch_bounds__(kFieldThreads) k_pcg_precond(
     const int i = i0 + gi;
     const bool live = i < n;
     T a6[6] = {0, 0, 0, 0, 0, 0};
-    pair_field<T, 2, G>(live ? i : -1, sub, prl, prl_cnt, capP, coefP, coefPB, recP, a6);
+    pair_field<T, 4, G>(live ? i : -1, sub, prl, prl_cnt, capP, coefP, coefPB, recP, a6);
     double f[6];
 #pragma unroll
     for (int q = 0; q < 6; q++) f[q] = group_sum<G>((double)a6[q]);
-    double mine = f[0];
+    double zq[QPL];
 #pragma unroll
-    for (int q = 1; q < 6; q++)
-      if (sub == q) mine = f[q];
-    double zv = 0.0;
-    if (live && sub < 6) {
-      const int d = sub % 3, set = sub / 3;
-      const size_t j = (size_t)d * n + i;
-      const double rj = (set ? rP : r)[j];
-      zv = polar[i] * (mine + s * rj);
-      (set ? zP : zz)[j] = zv;
-      if (INIT) (set ? pP : p)[j] = zv;
-      if (set) acc[1] += rj * zv;
-      else acc[0] += rj * zv;
+    for (int u = 0; u < QPL; u++) {
+      const int q = sub + u * G;
+      double mine = f[0];
+#pragma unroll
+      for (int c = 1; c < 6; c++)
+        if (q == c) mine = f[c];
+      zq[u] = 0.0;
+      if (live && q < 6) {
+        const int d = q % 3, set = q / 3;
+        const size_t j = (size_t)d * n + i;
+        const double rj = (set ? rP : r)[j];
+        const double zv = polar[i] * (mine + s * rj);
+        zq[u] = zv;
+        (set ? zP : zz)[j] = zv;
+        if (INIT) (set ? pP : p)[j] = zv;
+        if (set) acc[1] += rj * zv;
+        else acc[0] += rj * zv;
+      }
     }
     double w[6];
 #pragma unroll
-    for (int q = 0; q < 6; q++) w[q] = __shfl_sync(0xffffffffu, zv, g0 + q);
+    for (int q = 0; q < 6; q++) w[q] = __shfl_sync(0xffffffffu, zq[q / G], g0 + q % G);
     if (live && sub == 0) put_rec(recF, i, w[0], w[1], w[2], w[3], w[4], w[5]);
   }
   if (!INIT) {
