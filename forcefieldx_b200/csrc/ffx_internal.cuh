@@ -454,6 +454,11 @@ struct Handle {
   bool capturing = false;
   cudaStream_t vdw_stream = nullptr;
   cudaEvent_t ev_vdw_fork = nullptr, ev_vdw_join = nullptr;
+  // ... and the reciprocal-space chains (permanent: beside the real-space field; final
+  // induced: beside the real-space energy) on a second high-priority stream.
+  cudaStream_t recip_stream = nullptr;
+  cudaEvent_t ev_recip_fork = nullptr, ev_recip_join = nullptr;
+  bool recip_forked = false;
   cudaGraphExec_t graph_exec[2] = {nullptr, nullptr};
   int64_t graph_launches[2] = {0, 0};               // kernels outside the PCG body
   int64_t graph_body_launches = 0;
@@ -488,6 +493,7 @@ void launch_fft_convolution(Handle &h);
 void launch_phi_permanent(Handle &h);
 void launch_phi_induced(Handle &h);
 void launch_realspace_field(Handle &h);
+void launch_direct_dipoles(Handle &h);
 int run_pcg(Handle &h, bool capture);
 // Evaluation entry points shared by the single-system ABI and batches (handle.cu).
 int evaluate(Handle &h, const double *d_xyz, double *d_grad_xyz, bool grad, double *terms, int64_t *counts);

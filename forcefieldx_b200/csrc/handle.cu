@@ -209,6 +209,9 @@ static int create_impl(const ffxg_system *s, const ffxg_params *p, Handle &h) {
   CK(cudaEventCreateWithFlags(&h.ev_join, cudaEventDisableTiming));
   CK(cudaEventCreateWithFlags(&h.ev_vdw_fork, cudaEventDisableTiming));
   CK(cudaEventCreateWithFlags(&h.ev_vdw_join, cudaEventDisableTiming));
+  CK(cudaStreamCreateWithPriority(&h.recip_stream, cudaStreamNonBlocking, prio_high));
+  CK(cudaEventCreateWithFlags(&h.ev_recip_fork, cudaEventDisableTiming));
+  CK(cudaEventCreateWithFlags(&h.ev_recip_join, cudaEventDisableTiming));
 
   h.box.a = p->box[0]; h.box.b = p->box[1]; h.box.c = p->box[2];
   h.box.A00 = 1.0 / h.box.a; h.box.A11 = 1.0 / h.box.b; h.box.A22 = 1.0 / h.box.c;
@@ -458,8 +461,15 @@ static void free_all(Handle &h) {
   if (h.ev_join) cudaEventDestroy(h.ev_join);
   if (h.ev_vdw_fork) cudaEventDestroy(h.ev_vdw_fork);
   if (h.ev_vdw_join) cudaEventDestroy(h.ev_vdw_join);
+  if (h.recip_stream) cudaStreamDestroy(h.recip_stream);
+  if (h.ev_recip_fork) cudaEventDestroy(h.ev_recip_fork);
+  if (h.ev_recip_join) cudaEventDestroy(h.ev_recip_join);
   if (h.stream) cudaStreamDestroy(h.stream);
 }
+
+// Captured evaluations of systems with a reciprocal space run the reciprocal chains as
+// graph branches.
+static bool branch_recip(const Handle &h) { return h.capturing && !h.vacuum; }
 
 // ---------------------------------------------------------------------------
 // Evaluation.  emit_front (coordinates .. permanent field) and emit_back (energies,
@@ -485,19 +495,53 @@ static void emit_front(Handle &h, const double *d_xyz) {
   }
   tk = timer_begin(h, FFXG_STAGE_MULTIPOLES);
   launch_rotate(h);
-  launch_bsplines(h);
+  if (!branch_recip(h)) launch_bsplines(h);
   timer_end(h, tk);
-  tk = timer_begin(h, FFXG_STAGE_PERM_RECIP);
-  launch_spread_permanent(h);
-  launch_fft_convolution(h);
-  launch_phi_permanent(h);
-  timer_end(h, tk);
+  if (branch_recip(h)) {
+    // The permanent reciprocal chain needs only the global multipoles: a graph branch on
+    // the second high-priority stream beside the real-space field, joined before the
+    // direct dipoles.
+    cudaEventRecord(h.ev_recip_fork, h.stream);
+    cudaStreamWaitEvent(h.recip_stream, h.ev_recip_fork, 0);
+    cudaStream_t main = h.stream;
+    h.stream = h.recip_stream;
+    launch_bsplines(h);
+    launch_spread_permanent(h);
+    launch_fft_convolution(h);
+    launch_phi_permanent(h);
+    cudaEventRecord(h.ev_recip_join, h.recip_stream);
+    h.stream = main;
+  } else {
+    tk = timer_begin(h, FFXG_STAGE_PERM_RECIP);
+    launch_spread_permanent(h);
+    launch_fft_convolution(h);
+    launch_phi_permanent(h);
+    timer_end(h, tk);
+  }
   tk = timer_begin(h, FFXG_STAGE_PERM_FIELD);
-  launch_realspace_field(h);   // sub-lists, permanent field, pair coefficients, direct dipoles
+  launch_realspace_field(h);   // sub-lists, permanent real-space field, pair coefficients
+  if (branch_recip(h)) cudaStreamWaitEvent(h.stream, h.ev_recip_join, 0);
+  launch_direct_dipoles(h);
   timer_end(h, tk);
 }
 
+// The reciprocal potential of the converged dipoles.  In a captured evaluation it is a
+// branch beside the real-space energy (which needs only the dipoles), joined in emit_back
+// before the reciprocal energy.
 static void emit_final_induced(Handle &h) {
+  if (branch_recip(h)) {
+    cudaEventRecord(h.ev_recip_fork, h.stream);
+    cudaStreamWaitEvent(h.recip_stream, h.ev_recip_fork, 0);
+    cudaStream_t main = h.stream;
+    h.stream = h.recip_stream;
+    launch_spread_induced(h, h.d_uD, h.d_uP);
+    launch_fft_convolution(h);
+    launch_phi_induced(h);
+    cudaEventRecord(h.ev_recip_join, h.recip_stream);
+    h.stream = main;
+    h.recip_forked = true;
+    return;
+  }
   const int tk = timer_begin(h, FFXG_STAGE_IND_RECIP);
   launch_spread_induced(h, h.d_uD, h.d_uP);
   launch_fft_convolution(h);
@@ -514,6 +558,10 @@ static void emit_back(Handle &h, double *d_grad_xyz) {
   int tk = timer_begin(h, FFXG_STAGE_REAL_ENERGY);
   launch_real_energy(h, h.want_grad);
   timer_end(h, tk);
+  if (h.recip_forked) {
+    cudaStreamWaitEvent(h.stream, h.ev_recip_join, 0);
+    h.recip_forked = false;
+  }
   tk = timer_begin(h, FFXG_STAGE_RECIP_ENERGY);
   launch_recip_energy(h, h.want_grad);
   timer_end(h, tk);
@@ -817,6 +865,7 @@ static int evaluate_elec(Handle &h, const double *d_xyz, double *d_grad_xyz, dou
       launch_fft_convolution(h);
       launch_phi_permanent(h);
       launch_realspace_field(h);
+      launch_direct_dipoles(h);
       h.scf_iter = 0;
       if (anyPol && h.step.doPol) {
         if (mutual) st = run_pcg(h, false);

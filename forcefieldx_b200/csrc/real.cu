@@ -1,7 +1,7 @@
 // real.cu -- real-space Ewald pair kernels (warp per atom, gather over the full list).
 //
 //  k_permanent_field   PermanentRealSpaceFieldLoop (pme/PermanentFieldRegion.java:595-815)
-//  k_direct            DirectLoop (pme/DirectRegion.java:170-243)
+//  k_direct_dipoles    DirectLoop (pme/DirectRegion.java:170-243)
 //  k_induced_field     InducedDipoleFieldRegion (pme/InducedDipoleFieldRegion.java:308-470) plus the
 //                      self and reciprocal terms of InducedDipoleFieldReduceRegion (:159-207)
 //  k_precond_field     InducedPreconditionerFieldLoop (pme/PCGSolver.java:1254-1400), Ewald off
@@ -44,8 +44,7 @@ struct Excl {
 };
 
 
-// Real-space lists, permanent field, cached pair coefficients and direct dipoles in one
-// pass (PermanentRealSpaceFieldLoop, pme/PermanentFieldRegion.java:595-815, which also
+// Real-space lists, permanent real-space field and cached pair coefficients in one pass (PermanentRealSpaceFieldLoop, pme/PermanentFieldRegion.java:595-815, which also
 // derives the Ewald and preconditioner lists; DirectLoop, pme/DirectRegion.java:170-243).
 // Phase 1 compacts the buffered row into the Ewald row (r2 <= off2) and the
 // preconditioner row (r < pcut).  Phase 2 walks the Ewald row: it accumulates the D and
@@ -60,9 +59,8 @@ __global__ void __launch_bounds__(128, sizeof(R) == 4 ? 8 : 1) k_realspace_field
     const int *__restrict__ nbr, const int *__restrict__ nbr_cnt, int cap, const int *__restrict__ nbr_sh,
     double off2, double pcut2, int *ewl, int *ewl_cnt, int capE, int *ewl_sh, int *prl, int *prl_cnt, int capP,
     PairRec<R> *coefE, R *coefEB,
-    PairRec<R> *coefP, R *coefPB, Excl ex, EwaldCoef ec, const __grid_constant__ ScaleTables c_scales, const double *__restrict__ cphi,
-    const double *__restrict__ polar, int direct, double *fieldD, double *fieldP, double *uD, double *uP,
-    double *udD, double *udP, R *recF, int *flags, const double2 *__restrict__ pos, const R *__restrict__ rec) {
+    PairRec<R> *coefP, R *coefPB, Excl ex, EwaldCoef ec, const __grid_constant__ ScaleTables c_scales,
+    double *fieldD, double *fieldP, int *flags, const double2 *__restrict__ pos, const R *__restrict__ rec) {
   using V2 = typename Vec2<R>::type;
   const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const int lane = threadIdx.x & 31;
@@ -209,24 +207,39 @@ __global__ void __launch_bounds__(128, sizeof(R) == 4 ? 8 : 1) k_realspace_field
   double Fx = warp_sum((double)fx), Fy = warp_sum((double)fy), Fz = warp_sum((double)fz);
   double Px = warp_sum((double)px), Py = warp_sum((double)py), Pz = warp_sum((double)pz);
   if (lane == 0) {
-    if (direct) {
-      const double a = polar[i];
-      const double f0 = ec.aewald3 * gm[t100 * n + i] - cphi[1 * n + i];
-      const double f1 = ec.aewald3 * gm[t010 * n + i] - cphi[2 * n + i];
-      const double f2 = ec.aewald3 * gm[t001 * n + i] - cphi[3 * n + i];
-      Fx += f0; Fy += f1; Fz += f2;
-      Px += f0; Py += f1; Pz += f2;
-      uD[i] = a * Fx; uD[n + i] = a * Fy; uD[2 * n + i] = a * Fz;
-      uP[i] = a * Px; uP[n + i] = a * Py; uP[2 * n + i] = a * Pz;
-      udD[i] = a * Fx; udD[n + i] = a * Fy; udD[2 * n + i] = a * Fz;
-      udP[i] = a * Px; udP[n + i] = a * Py; udP[2 * n + i] = a * Pz;
-      put_rec(recF, i, a * Fx, a * Fy, a * Fz, a * Px, a * Py, a * Pz);
-    }
     fieldD[i] = Fx; fieldD[n + i] = Fy; fieldD[2 * n + i] = Fz;
     fieldP[i] = Px; fieldP[n + i] = Py; fieldP[2 * n + i] = Pz;
   }
 }
 
+
+// Direct dipoles of both sets, u = alpha (E_real + E_self + E_recip), from the real-space
+// fields, the Ewald self field of the dipole and the reciprocal potential gradient
+// (DirectLoop, pme/DirectRegion.java:170-243), and their source record for the first PCG
+// field; the field rows are completed in place.  Separate from k_realspace_field so that
+// the permanent reciprocal chain can run beside it.
+template <typename R>
+__global__ void k_direct_dipoles(int n, const double *__restrict__ gm, const double *__restrict__ cphi,
+                                 const double *__restrict__ polar, double aewald3, double *fieldD, double *fieldP,
+                                 double *uD, double *uP, double *udD, double *udP, R *recF) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const double a = polar[i];
+  double d[3], q[3];
+#pragma unroll
+  for (int c = 0; c < 3; c++) {
+    const size_t j = (size_t)c * n + i;
+    const double f = aewald3 * gm[(size_t)(1 + c) * n + i] - cphi[(size_t)(1 + c) * n + i];
+    const double fd = fieldD[j] + f, fp = fieldP[j] + f;
+    fieldD[j] = fd;
+    fieldP[j] = fp;
+    d[c] = a * fd;
+    q[c] = a * fp;
+    uD[j] = d[c]; udD[j] = d[c];
+    uP[j] = q[c]; udP[j] = q[c];
+  }
+  put_rec(recF, i, d[0], d[1], d[2], q[0], q[1], q[2]);
+}
 
 // ---------------------------------------------------------------------------
 // Permanent and polarization real-space energy, i-side force and torque.
@@ -753,10 +766,22 @@ static void realspace_field(Handle &h) {
       h.cap_prl,
       reinterpret_cast<PairRec<R> *>(h.d_coefE), reinterpret_cast<R *>(h.d_coefEB),
       reinterpret_cast<PairRec<R> *>(h.d_coefP), reinterpret_cast<R *>(h.d_coefPB), excl(h),
-      ewald_coef(h, ewald_alpha_of(h)), h.scales, h.d_cphi, h.d_polar, h.prm.polarization != FFXG_POLAR_NONE ? 1 : 0,
-      h.d_fieldD, h.d_fieldP, h.d_uD, h.d_uP, h.d_udirD, h.d_udirP, reinterpret_cast<R *>(h.d_recF), h.d_flags,
-      h.d_pos, reinterpret_cast<const R *>(h.d_erec));
+      ewald_coef(h, ewald_alpha_of(h)), h.scales, h.d_fieldD, h.d_fieldP, h.d_flags, h.d_pos,
+      reinterpret_cast<const R *>(h.d_erec));
   FFX_LAUNCHED(h);
+}
+
+template <typename R>
+static void direct_dipoles(Handle &h) {
+  k_direct_dipoles<R><<<nblocks(h.n, 256), 256, 0, h.stream>>>(
+      h.n, h.d_gm, h.d_cphi, h.d_polar, ewald_coef(h, ewald_alpha_of(h)).aewald3, h.d_fieldD, h.d_fieldP, h.d_uD,
+      h.d_uP, h.d_udirD, h.d_udirP, reinterpret_cast<R *>(h.d_recF));
+  FFX_LAUNCHED(h);
+}
+
+void launch_direct_dipoles(Handle &h) {
+  if (h.prm.polarization == FFXG_POLAR_NONE) return;
+  if (h.mixed) direct_dipoles<float>(h); else direct_dipoles<double>(h);
 }
 
 void launch_realspace_field(Handle &h) {
