@@ -179,7 +179,7 @@ __device__ __forceinline__ void nrm3(double *v) {
 }
 
 // Cartesian force on frame slot `slot` (0 = z, 1 = x, 2 = y, 3 = the atom) from atom i's torque.
-__device__ void torque_slot(int i, int slot, int n, const double *__restrict__ x, const double *__restrict__ y,
+__device__ __forceinline__ void torque_slot(int i, int slot, int n, const double *__restrict__ x, const double *__restrict__ y,
                             const double *__restrict__ z, const int *__restrict__ frame, const int *__restrict__ axis,
                             const double *trq, double *out) {
   out[0] = out[1] = out[2] = 0.0;
@@ -261,6 +261,7 @@ __device__ void torque_slot(int i, int slot, int n, const double *__restrict__ x
     const double *va[3] = {vZ, vX, vY};
     const double ra[3] = {rZ, rX, rY};
     const double cs[3] = {cosZSum, cosXSum, cosYSum};
+#pragma unroll
     for (int q = 0; q < 3; q++) {
       // q = 0: r = x + y about z; q = 1: r = z + y about x; q = 2: r = z + x about y
       const double *a1 = (q == 0) ? vX : vZ;
@@ -281,7 +282,10 @@ __device__ void torque_slot(int i, int slot, int n, const double *__restrict__ x
       }
     }
   }
-  out[0] = g[slot][0]; out[1] = g[slot][1]; out[2] = g[slot][2];
+  // Select the slot with compares so that g stays in registers (a runtime index would put
+  // it in local memory).
+#pragma unroll
+  for (int j = 0; j < 3; j++) out[j] = (slot == 0) ? g[0][j] : (slot == 1) ? g[1][j] : (slot == 2) ? g[2][j] : g[3][j];
 }
 
 __global__ void k_torque_gather(int n, const double *__restrict__ x, const double *__restrict__ y,
@@ -347,17 +351,24 @@ __global__ void k_sum_partial(int n, const double *__restrict__ eatom, const lon
   }
 }
 
+// Row t of the totals by warp t: lane l sums blocks l, l + 32, ..., then a fixed shuffle
+// tree (the same order on every call).
 __global__ void k_sum_final(int nb, const double *__restrict__ pe, const long long *__restrict__ pc, double *out,
                             long long *cout) {
-  if (threadIdx.x < kNE) {
+  const int lane = threadIdx.x & 31, row = threadIdx.x >> 5;
+  if (row < kNE) {
     double s = 0.0;
-    for (int b = 0; b < nb; b++) s += pe[b * kNE + threadIdx.x];
-    out[threadIdx.x] = s;
-  } else if (threadIdx.x < kNE + kNC) {
-    const int t = threadIdx.x - kNE;
+    for (int b = lane; b < nb; b += 32) s += pe[b * kNE + row];
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+    if (lane == 0) out[row] = s;
+  } else if (row < kNE + kNC) {
+    const int t = row - kNE;
     long long s = 0;
-    for (int b = 0; b < nb; b++) s += pc[b * kNC + t];
-    cout[t] = s;
+    for (int b = lane; b < nb; b += 32) s += pc[b * kNC + t];
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+    if (lane == 0) cout[t] = s;
   }
 }
 
@@ -475,7 +486,7 @@ void launch_reduce_results(Handle &h) {
   long long *pc = reinterpret_cast<long long *>(h.d_partials + kSumBlocks * kNE);
   const int nb = std::min(kSumBlocks, std::max(1, (h.n + 255) / 256));   // fewer blocks for small systems
   k_sum_partial<<<nb, 256, 0, h.stream>>>(h.n, h.d_eatom, h.d_catom, pe, pc);
-  k_sum_final<<<1, 32, 0, h.stream>>>(nb, pe, pc, h.d_result, h.d_cresult);
+  k_sum_final<<<1, 32 * (kNE + kNC), 0, h.stream>>>(nb, pe, pc, h.d_result, h.d_cresult);
   h.launches += 2;
 }
 
