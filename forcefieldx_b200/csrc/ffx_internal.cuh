@@ -448,6 +448,7 @@ struct Handle {
   // Graph execution: the whole evaluation captured once per gradient mode and replayed.
   bool use_graphs = true;
   bool want_grad = true;                            // gradient requested by the current call
+  bool grad_to_pin = false, grad_pinned = false;    // host-gradient call: D2H queued before the sync
   cudaStream_t side = nullptr;                      // captures the PCG while-node body
   // Captured evaluations run the vdW term (independent of electrostatics) on its own
   // low-priority stream beside the permanent field and the PCG, joined before the gradient.
@@ -487,6 +488,9 @@ void launch_neighbor_list(Handle &h, bool force);
 void launch_vdw(Handle &h, bool grad, cudaStream_t st);
 void launch_rotate(Handle &h);
 void launch_bsplines(Handle &h);
+// Copies m doubles into dst (the pinned staging buffer) and tests them for Inf/NaN in the
+// same pass (exponent bits all ones); false if any is not finite.
+bool copy_finite(double *dst, const double *src, size_t m);
 void launch_spread_permanent(Handle &h);
 void launch_spread_induced(Handle &h, const double *ud, const double *up);
 void launch_fft_convolution(Handle &h);

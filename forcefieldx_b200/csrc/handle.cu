@@ -467,6 +467,19 @@ static void free_all(Handle &h) {
   if (h.stream) cudaStreamDestroy(h.stream);
 }
 
+namespace ffx {
+bool copy_finite(double *dst, const double *src, size_t m) {
+  uint64_t bad = 0;
+  for (size_t j = 0; j < m; j++) {
+    uint64_t u;
+    std::memcpy(&u, src + j, sizeof(u));
+    std::memcpy(dst + j, &u, sizeof(u));
+    bad |= (uint64_t)((u & 0x7ff0000000000000ull) == 0x7ff0000000000000ull);
+  }
+  return bad == 0;
+}
+}  // namespace ffx
+
 // Captured evaluations of systems with a reciprocal space run the reciprocal chains as
 // graph branches.
 static bool branch_recip(const Handle &h) { return h.capturing && !h.vacuum; }
@@ -641,6 +654,14 @@ static int grow_lists(Handle &h, int f) {
 
 static constexpr int kOverflow = FLAG_NBR_OVERFLOW | FLAG_EWALD_OVERFLOW | FLAG_PRECOND_OVERFLOW;
 
+// ffxg_energy with a host gradient: the device-to-host copy into the pinned buffer is
+// queued before the evaluation's own synchronisation, so the call waits once.
+static void copy_grad_to_pinned(Handle &h, const double *d_grad) {
+  if (!h.grad_to_pin || !h.want_grad) return;
+  cudaMemcpyAsync(h.h_grad_pin, d_grad, 3 * (size_t)h.n * sizeof(double), cudaMemcpyDeviceToHost, h.stream);
+  h.grad_pinned = true;
+}
+
 // Direct execution: one host check of the list and coordinate flags before the solver,
 // the solver's stopping test read back per iteration.  Grows list capacities and repeats
 // on overflow.
@@ -676,6 +697,7 @@ static int evaluate_direct(Handle &h, const double *d_xyz, double *d_grad_xyz, d
     }
     if (st != FFXG_OK) { h.err = scf_message(st); return st; }
     emit_back(h, d_grad_xyz);
+    copy_grad_to_pinned(h, d_grad_xyz);
     if (cudaStreamSynchronize(h.stream) != cudaSuccess) {
       h.err = std::string("CUDA error: ") + cudaGetErrorString(cudaGetLastError());
       return FFXG_ERR_CUDA;
@@ -751,6 +773,7 @@ static int evaluate_graph(Handle &h, const double *d_xyz, double *d_grad_xyz, do
   }
   if (h.want_grad && d_grad_xyz != h.d_grad_out)
     cudaMemcpyAsync(d_grad_xyz, h.d_grad_out, 3 * (size_t)h.n * sizeof(double), cudaMemcpyDeviceToDevice, h.stream);
+  copy_grad_to_pinned(h, d_grad_xyz);
   if (cudaStreamSynchronize(h.stream) != cudaSuccess) {
     h.err = std::string("CUDA error: ") + cudaGetErrorString(cudaGetLastError());
     return FFXG_ERR_CUDA;
@@ -1001,9 +1024,7 @@ const char *ffxg_last_error(const ffxg_handle *hh) { return hh ? hh->h.err.c_str
 int ffxg_set_coordinates(ffxg_handle *hh, const double *xyz) {
   if (!hh || !xyz) return FFXG_ERR_BAD_ARG;
   Handle &h = hh->h;
-  for (size_t j = 0; j < 3 * (size_t)h.n; j++)
-    if (!std::isfinite(xyz[j])) { h.err = "non-finite coordinates"; return FFXG_ERR_NONFINITE; }
-  std::memcpy(h.h_xyz_pin, xyz, 3 * (size_t)h.n * sizeof(double));
+  if (!copy_finite(h.h_xyz_pin, xyz, 3 * (size_t)h.n)) { h.err = "non-finite coordinates"; return FFXG_ERR_NONFINITE; }
   CK(cudaMemcpyAsync(h.d_xyz_in, h.h_xyz_pin, 3 * (size_t)h.n * sizeof(double), cudaMemcpyHostToDevice, h.stream));
   return FFXG_OK;
 }
@@ -1011,11 +1032,17 @@ int ffxg_set_coordinates(ffxg_handle *hh, const double *xyz) {
 int ffxg_energy(ffxg_handle *hh, int want_grad, double *terms, double *grad, int64_t *counts) {
   if (!hh) return FFXG_ERR_BAD_ARG;
   Handle &h = hh->h;
+  h.grad_to_pin = want_grad && grad;
+  h.grad_pinned = false;
   const int st = evaluate(h, h.d_xyz_in, h.d_grad_out, want_grad != 0, terms, counts);
+  h.grad_to_pin = false;
   if (st != FFXG_OK) return st;
   if (want_grad && grad) {
-    CK(cudaMemcpyAsync(h.h_grad_pin, h.d_grad_out, 3 * (size_t)h.n * sizeof(double), cudaMemcpyDeviceToHost, h.stream));
-    CK(cudaStreamSynchronize(h.stream));
+    if (!h.grad_pinned) {   // paths that synchronise more than once copy afterwards
+      CK(cudaMemcpyAsync(h.h_grad_pin, h.d_grad_out, 3 * (size_t)h.n * sizeof(double), cudaMemcpyDeviceToHost,
+                         h.stream));
+      CK(cudaStreamSynchronize(h.stream));
+    }
     std::memcpy(grad, h.h_grad_pin, 3 * (size_t)h.n * sizeof(double));
   }
   return FFXG_OK;
