@@ -460,8 +460,10 @@ struct Handle {
   cudaStream_t recip_stream = nullptr;
   cudaEvent_t ev_recip_fork = nullptr, ev_recip_join = nullptr;
   bool recip_forked = false;
-  cudaGraphExec_t graph_exec[2] = {nullptr, nullptr};
-  int64_t graph_launches[2] = {0, 0};               // kernels outside the PCG body
+  // Per call kind: energy only, gradient on the device, gradient to the host (the graph
+  // then ends with the gradient's device-to-host copy beside the energy sums).
+  cudaGraphExec_t graph_exec[3] = {nullptr, nullptr, nullptr};
+  int64_t graph_launches[3] = {0, 0, 0};            // kernels outside the PCG body
   int64_t graph_body_launches = 0;
   double e_charge_correction = 0.0;
   // Stage timers (PMETimings counterpart).

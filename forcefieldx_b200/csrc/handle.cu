@@ -583,6 +583,15 @@ static void emit_back(Handle &h, double *d_grad_xyz) {
   if (h.want_grad) {
     launch_torque(h);
     launch_assemble(h, d_grad_xyz);
+    if (h.capturing && h.grad_to_pin && !h.vacuum) {
+      // Host-gradient graphs: the copy to the pinned buffer runs beside the energy sums.
+      cudaEventRecord(h.ev_recip_fork, h.stream);
+      cudaStreamWaitEvent(h.recip_stream, h.ev_recip_fork, 0);
+      cudaMemcpyAsync(h.h_grad_pin, d_grad_xyz, 3 * (size_t)h.n * sizeof(double), cudaMemcpyDeviceToHost,
+                      h.recip_stream);
+      cudaEventRecord(h.ev_recip_join, h.recip_stream);
+      h.recip_forked = true;
+    }
   }
   if (h.step.lam) {   // electrostatic lambda gradient into the dU/dX dL rows (after the vdW part)
     if (h.vacuum) cudaMemsetAsync(h.d_lgred + 3 * (size_t)h.n, 0, 3 * (size_t)h.n * sizeof(double), h.stream);
@@ -593,6 +602,10 @@ static void emit_back(Handle &h, double *d_grad_xyz) {
   cudaMemcpyAsync(h.h_scalars, h.d_result, kEnergyRows * sizeof(double), cudaMemcpyDeviceToHost, h.stream);
   cudaMemcpyAsync(h.h_flags + 2, h.d_cresult, 2 * sizeof(long long), cudaMemcpyDeviceToHost, h.stream);
   cudaMemcpyAsync(h.h_flags, h.d_flags, sizeof(int), cudaMemcpyDeviceToHost, h.stream);
+  if (h.recip_forked) {
+    cudaStreamWaitEvent(h.stream, h.ev_recip_join, 0);
+    h.recip_forked = false;
+  }
 }
 
 static const char *scf_message(int st) {
@@ -653,6 +666,8 @@ static int grow_lists(Handle &h, int f) {
 }
 
 static constexpr int kOverflow = FLAG_NBR_OVERFLOW | FLAG_EWALD_OVERFLOW | FLAG_PRECOND_OVERFLOW;
+
+static int graph_key(const Handle &h) { return h.want_grad ? (h.grad_to_pin ? 2 : 1) : 0; }
 
 // ffxg_energy with a host gradient: the device-to-host copy into the pinned buffer is
 // queued before the evaluation's own synchronisation, so the call waits once.
@@ -715,7 +730,7 @@ namespace ffx {
 // of a batch capture): inputs from d_xyz, gradient into d_grad, and the pinned copies of
 // scalars, flags and solver state that eval_after_graph reads.
 int eval_capture_body(Handle &h, const double *d_xyz, double *d_grad) {
-  const int key = h.want_grad ? 1 : 0;
+  const int key = graph_key(h);
   const int64_t before = h.launches;
   h.capturing = true;
   emit_front(h, d_xyz);
@@ -737,7 +752,7 @@ int eval_capture_body(Handle &h, const double *d_xyz, double *d_grad) {
 
 // Capture the whole evaluation (internal coordinate and gradient buffers) as one graph.
 static int capture_graph(Handle &h) {
-  const int key = h.want_grad ? 1 : 0;
+  const int key = graph_key(h);
   if (cudaStreamBeginCapture(h.stream, cudaStreamCaptureModeThreadLocal) != cudaSuccess) return FFXG_ERR_CUDA;
   const int st = eval_capture_body(h, h.d_xyz_in, h.d_grad_out);
   cudaGraph_t graph = nullptr;
@@ -760,7 +775,7 @@ static int capture_graph(Handle &h) {
 // Graph execution: one launch, one synchronisation.  Returns -1 when the evaluation must
 // be repeated directly (list overflow, or the graph could not be built).
 static int evaluate_graph(Handle &h, const double *d_xyz, double *d_grad_xyz, double *terms, int64_t *counts) {
-  const int key = h.want_grad ? 1 : 0;
+  const int key = graph_key(h);
   if (!h.graph_exec[key] && capture_graph(h) != FFXG_OK) {
     h.use_graphs = false;   // fall back to direct launches for this handle
     return -1;
@@ -773,7 +788,8 @@ static int evaluate_graph(Handle &h, const double *d_xyz, double *d_grad_xyz, do
   }
   if (h.want_grad && d_grad_xyz != h.d_grad_out)
     cudaMemcpyAsync(d_grad_xyz, h.d_grad_out, 3 * (size_t)h.n * sizeof(double), cudaMemcpyDeviceToDevice, h.stream);
-  copy_grad_to_pinned(h, d_grad_xyz);
+  if (key == 2) h.grad_pinned = true;   // the graph ends with the copy
+  else copy_grad_to_pinned(h, d_grad_xyz);
   if (cudaStreamSynchronize(h.stream) != cudaSuccess) {
     h.err = std::string("CUDA error: ") + cudaGetErrorString(cudaGetLastError());
     return FFXG_ERR_CUDA;
@@ -787,7 +803,7 @@ namespace ffx {
 // Returns -1 when a list overflowed: capacities grew, the handle's graphs are gone, and the
 // evaluation must be repeated directly.
 int eval_after_graph(Handle &h, double *terms, int64_t *counts) {
-  const int key = h.want_grad ? 1 : 0;
+  const int key = graph_key(h);
   const int f = h.h_flags[0];
   if (f & kOverflow) {
     if (int a = grow_lists(h, f)) return a;   // also drops the graphs
