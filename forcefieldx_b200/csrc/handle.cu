@@ -205,6 +205,7 @@ static int create_impl(const ffxg_system *s, const ffxg_params *p, Handle &h) {
   CK(cudaStreamCreateWithPriority(&h.aux, cudaStreamNonBlocking, prio_low));
   CK(cudaStreamCreateWithPriority(&h.aux_side, cudaStreamNonBlocking, prio_low));
   CK(cudaStreamCreateWithPriority(&h.vdw_stream, cudaStreamNonBlocking, prio_low));
+  h.num_sms = prop.multiProcessorCount;
   CK(cudaEventCreateWithFlags(&h.ev_fork, cudaEventDisableTiming));
   CK(cudaEventCreateWithFlags(&h.ev_join, cudaEventDisableTiming));
   CK(cudaEventCreateWithFlags(&h.ev_vdw_fork, cudaEventDisableTiming));
