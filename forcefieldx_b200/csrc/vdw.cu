@@ -4,10 +4,11 @@
 // (VanDerWaalsForm.java:313-334; delta 0.07, gamma 0.12), the multiplicative taper
 // from vdw-taper * cutoff to the cutoff (MultiplicativeSwitch.java:84-124, 234-236) and
 // the 1-2/1-3/1-4 masks (VanDerWaals.applyMask, :412-428).  A warp owns an atom i and
-// gathers over the buffered list in both directions (a partner's reduced position and
-// type from one 32-byte record): the force on i's reduced site
-// accumulates in registers; k_vdw_distribute then splits every reduced-site force
-// between the hydrogen and its heavy atom (VanDerWaals.java:1786-1797) as a gather.
+// scans its buffered row in both directions (a partner's reduced position and type from
+// one 32-byte record); entries inside the cutoff go to a per-warp queue in shared memory
+// and are evaluated 32 at a time.  The force on i's reduced site accumulates in
+// registers; k_vdw_distribute then splits every reduced-site force between the hydrogen
+// and its heavy atom (VanDerWaals.java:1786-1797) as a gather.
 #include <algorithm>
 
 #include "ffx_internal.cuh"
