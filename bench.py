@@ -104,6 +104,11 @@ class ClockSampler:
 
 
 # ---------------------------------------------------------------------------
+# DRAM bytes (read + write) of one k_pair_field<float> launch on this workload, from an ncu
+# capture with caches flushed before the launch (profiles/pcg_kernels_water24k_mixed.md).
+PAIR_FIELD_TRAFFIC = 90.9e6
+
+
 def algorithmic_traffic(stage: str, n: int, pairs_half: int, vdw_list_full: int, mixed: bool) -> float:
     """Compulsory HBM bytes of one launch of a stage's dominant kernel: every input read
     once, every output written once."""
@@ -221,10 +226,12 @@ def measure(args, precision, system, dist, world, local):
         "stages_ms_per_step": {k: v["ms_total"] / args.steps for k, v in per_stage.items()},
         "stages_note": "direct launches with per-stage events (the timed steps replay one CUDA graph)",
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
-                     "frac": achieved / peak, "traffic": None, "kernel_stage": dom,
+                     "frac": achieved / peak,
+                     "traffic": PAIR_FIELD_TRAFFIC if (mixed and dom == "ind_field") else None,
+                     "kernel_stage": dom,
                      "algorithmic_bytes_per_launch": traffic_alg, "avg_launch_ms": avg_ms,
                      "peak_source": peak_src,
-                     "note": "stage timed with direct launches; the pair kernels are bound by gather latency, not HBM (profiles/pcg_kernels_water24k_mixed.md)"},
+                     "note": "stage timed with direct launches, the kernel alone on its stream; the pair kernels are bound by gather latency, not HBM (profiles/pcg_kernels_water24k_mixed.md)"},
     }
 
 

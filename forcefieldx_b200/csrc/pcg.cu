@@ -639,7 +639,9 @@ static void combine(Handle &h, const double *vD, const double *vP, bool first, d
 // auxiliary stream, concurrently with spread + FFT on the main stream, then the combine.
 template <int MODE>
 static void field_of(Handle &h, const double *vD, const double *vP, bool first, double *outD, double *outP) {
-  cudaStream_t ax = (h.stream == h.side) ? h.aux_side : h.aux;
+  // Stage timing (direct launches, ffxg_set_timing) keeps the pair field on the main
+  // stream, so that its events time the kernel alone rather than its overlap.
+  cudaStream_t ax = h.timing ? h.stream : ((h.stream == h.side) ? h.aux_side : h.aux);
   cudaEventRecord(h.ev_fork, h.stream);
   cudaStreamWaitEvent(ax, h.ev_fork, 0);
   int tk = timer_begin_on(h, FFXG_STAGE_IND_FIELD, ax);
