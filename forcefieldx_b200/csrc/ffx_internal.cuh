@@ -34,7 +34,16 @@ enum : int {
   FLAG_NONFINITE = 8,
   FLAG_REBUILD = 16,
   FLAG_IMAGE_RANGE = 32,   // a multi-image shift beyond the 10-bit packing (|n| > 511)
+  FLAG_NEAR_INVALID = 64,  // a hydrogen's reduction offset exceeds the near list's margin
 };
+
+// The near list: at every rebuild of the buffered list the cell builder also keeps the
+// pairs within ewald-cutoff + buffer + 2 kNearDelta on the reduced coordinates, where
+// kNearDelta bounds |x - x_reduced| of every atom.  Any pair within the Ewald cutoff at
+// a later evaluation (real coordinates) is in it, so the Ewald sub-list scans that row
+// instead of the full one; an atom whose reduction offset exceeds kNearDelta makes that
+// evaluation scan the full row (FLAG_NEAR_INVALID).
+constexpr double kNearDelta = 0.25;
 
 // Exclusion codes: bits 0-2 mpole class, 3-5 polar class, 6 same polarization group,
 // 7-8 vdW class.
@@ -333,6 +342,9 @@ struct Handle {
   int *d_cell_cnt = nullptr, *d_cell_start = nullptr, *d_cell_atoms = nullptr, *d_atom_cell = nullptr;
   int cap_nbr = 0, cap_ewl = 0, cap_prl = 0;
   int *d_nbr = nullptr, *d_nbr_cnt = nullptr;
+  bool near_list = false;                     // minimum-image cell lists with a near list
+  int cap_nbl = 0;
+  int *d_nbl = nullptr, *d_nbl_cnt = nullptr;
   int *d_ewl = nullptr, *d_ewl_cnt = nullptr;
   int *d_prl = nullptr, *d_prl_cnt = nullptr;
   // Multi-image lists: on when an edge is at most twice an interaction cutoff (or forced

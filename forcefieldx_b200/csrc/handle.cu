@@ -80,6 +80,8 @@ static void drop_graphs(Handle &h) {
 static int alloc_lists(Handle &h) {
   drop_graphs(h);   // the captured kernels hold the old list pointers
   if (h.d_nbr) cudaFree(h.d_nbr);
+  if (h.d_nbl) cudaFree(h.d_nbl);
+  h.d_nbl = nullptr;
   if (h.d_ewl) cudaFree(h.d_ewl);
   if (h.d_prl) cudaFree(h.d_prl);
   if (h.d_coefE) cudaFree(h.d_coefE);
@@ -93,6 +95,7 @@ static int alloc_lists(Handle &h) {
   h.d_coefE = h.d_coefP = nullptr;
   h.d_coefEB = h.d_coefPB = nullptr;
   CK(dalloc(&h.d_nbr, (size_t)h.n * h.cap_nbr));
+  if (h.near_list) CK(dalloc(&h.d_nbl, (size_t)h.n * h.cap_nbl));
   CK(dalloc(&h.d_ewl, (size_t)h.n * h.cap_ewl));
   CK(dalloc(&h.d_prl, (size_t)h.n * h.cap_prl));
   CK(dalloc(&h.d_coefE, (size_t)h.n * h.cap_ewl));
@@ -109,6 +112,10 @@ static int alloc_lists(Handle &h) {
 
 static int round32(double v) { return ((int)std::ceil(v) + 31) / 32 * 32; }
 
+static double near_radius(const Handle &h) {
+  return h.prm.ewald_cutoff + h.prm.list_buffer + 2.0 * kNearDelta;
+}
+
 // Multi-image mode and the shift range of its list builder: |n_d - n0_d| <=
 // floor(rlist / L_d + 1/2), n0 the minimum-image shift, covers every image within rlist.
 static void configure_images(Handle &h) {
@@ -120,6 +127,7 @@ static void configure_images(Handle &h) {
     if (p->box[d] <= 2.0 * rcut) h.images = true;
     h.img_range[d] = (int)std::floor(rlist / p->box[d] + 0.5);
   }
+  h.near_list = !h.images && !h.vacuum && near_radius(h) < rlist;
 }
 
 // Host copy of the inputs (sub-systems are built from it).
@@ -297,6 +305,7 @@ static int create_impl(const ffxg_system *s, const ffxg_params *p, Handle &h) {
   const double PI = 3.14159265358979323846;
   auto sphere = [&](double r) { return 4.0 / 3.0 * PI * r * r * r * rho; };
   h.cap_nbr = round32(1.3 * sphere(rlist) + 64);
+  h.cap_nbl = round32(1.3 * sphere(std::min(near_radius(h), rlist)) + 64);
   h.cap_ewl = round32(1.3 * sphere(p->ewald_cutoff) + 32);
   h.cap_prl = round32(1.3 * sphere(p->precond_cutoff) + 32);
   for (int d = 0; d < 3; d++) h.ncell[d] = std::max(1, (int)std::floor(p->box[d] / (rlist * 0.5)));
@@ -319,6 +328,7 @@ static int create_impl(const ffxg_system *s, const ffxg_params *p, Handle &h) {
   CK(dalloc(&h.d_cell_cnt, 2 * (size_t)ncells)); CK(dalloc(&h.d_cell_start, (size_t)ncells + 1));
   CK(dalloc(&h.d_cell_atoms, N)); CK(dalloc(&h.d_atom_cell, N));
   CK(dalloc(&h.d_nbr_cnt, N)); CK(dalloc(&h.d_ewl_cnt, N)); CK(dalloc(&h.d_prl_cnt, N));
+  CK(dalloc(&h.d_nbl_cnt, N));
   if (int st = alloc_lists(h)) return st;
   CK(dalloc(&h.d_gm, 10 * N)); CK(dalloc(&h.d_fm, 10 * N)); CK(dalloc(&h.d_rot, 9 * N));
   CK(dalloc(&h.d_spl, N * 3 * kOrder * 4)); CK(dalloc(&h.d_igrid, 3 * N));
@@ -438,7 +448,7 @@ static void free_all(Handle &h) {
                   h.d_vrad, h.d_veps, h.d_excl_ptr, h.d_excl_k, h.d_excl_code, h.d_excl_lo, h.d_excl_hi, h.d_tq_ptr,
                   h.d_tq_ent, h.d_red_ptr, h.d_red_child, h.d_x, h.d_y, h.d_z, h.d_rx, h.d_ry, h.d_rz, h.d_refx,
                   h.d_refy, h.d_refz, h.d_cell_cnt, h.d_cell_start, h.d_cell_atoms, h.d_atom_cell, h.d_nbr,
-                  h.d_nbr_cnt, h.d_ewl, h.d_ewl_cnt, h.d_prl, h.d_prl_cnt, h.d_gm, h.d_fm, h.d_spl, h.d_igrid,
+                  h.d_nbr_cnt, h.d_nbl, h.d_nbl_cnt, h.d_ewl, h.d_ewl_cnt, h.d_prl, h.d_prl_cnt, h.d_gm, h.d_fm, h.d_spl, h.d_igrid,
                   h.d_cphi, h.d_fphi, h.d_cphiI, h.d_fphiI, h.d_cphiP, h.d_fphiP, h.d_fieldD, h.d_fieldP, h.d_uD,
                   h.d_uP, h.d_udirD, h.d_udirP, h.d_r, h.d_rP, h.d_zpre, h.d_zpreP, h.d_p, h.d_pP, h.d_vec, h.d_vecP,
                   h.d_partials, h.d_scalars, h.d_grid, h.d_influence, h.d_twiddle, h.d_gridf, h.d_influencef, h.d_twiddlef, h.d_grad, h.d_torque, h.d_gred,
@@ -660,7 +670,10 @@ static int finish(Handle &h, bool rebuilt, double *terms, int64_t *counts) {
 }
 
 static int grow_lists(Handle &h, int f) {
-  if (f & FLAG_NBR_OVERFLOW) h.cap_nbr = round32(h.cap_nbr * 1.5);
+  if (f & FLAG_NBR_OVERFLOW) {   // the buffered row or the near row
+    h.cap_nbr = round32(h.cap_nbr * 1.5);
+    h.cap_nbl = round32(h.cap_nbl * 1.5);
+  }
   if (f & FLAG_EWALD_OVERFLOW) h.cap_ewl = round32(h.cap_ewl * 1.5);
   if (f & FLAG_PRECOND_OVERFLOW) h.cap_prl = round32(h.cap_prl * 1.5);
   return alloc_lists(h);
@@ -1284,6 +1297,7 @@ static int build_vacuum(Handle &h, const std::vector<int> &soft, const std::vect
   int st = create_impl(&sub, &prm, *v);
   if (st != FFXG_OK) { h.err = "vacuum sub-system: " + v->err; free_all(*v); delete v; return st; }
   v->vacuum = true;
+  v->near_list = false;
   v->use_graphs = false;
   v->eps_atoms = h.n;
   v->images = true;

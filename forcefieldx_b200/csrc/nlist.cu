@@ -55,6 +55,8 @@ __global__ void k_reduce_coordinates(int n, const double *__restrict__ x, const 
   const double dx = vx - refx[i], dy = vy - refy[i], dz = vz - refz[i];
   const double d2 = dx * dx + dy * dy + dz * dz;
   if (!(d2 <= half_buffer2)) atomicOr(flags, FLAG_REBUILD);
+  const double ox = xi - vx, oy = yi - vy, oz = zi - vz;
+  if (!(ox * ox + oy * oy + oz * oz <= kNearDelta * kNearDelta)) atomicOr(flags, FLAG_NEAR_INVALID);
   if (!isfinite(vx) || !isfinite(vy) || !isfinite(vz)) atomicOr(flags, FLAG_NONFINITE);
 }
 
@@ -146,7 +148,7 @@ __global__ void k_verlet(int n, const double *__restrict__ rx, const double *__r
                          const double *__restrict__ rz, Box bx, CellOffsets co,
                          const int *__restrict__ atom_cell, const int *__restrict__ start,
                          const int *__restrict__ cell_atoms, double rl2, int cap, int *nbr, int *nbr_cnt,
-                         int *flags) {
+                         int *flags, double rn2, int capN, int *nbl, int *nbl_cnt) {
   if (!(*flags & FLAG_REBUILD)) return;
   const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const int lane = threadIdx.x & 31;
@@ -156,8 +158,9 @@ __global__ void k_verlet(int n, const double *__restrict__ rx, const double *__r
   const int c = atom_cell[i];
   const int ncx = co.n[0], ncy = co.n[1], ncz = co.n[2];
   const int cx = c % ncx, cy = (c / ncx) % ncy, cz = c / (ncx * ncy);
-  int count = 0;
+  int count = 0, countN = 0;
   int *row = nbr + (size_t)i * cap;
+  int *rowN = nbl ? nbl + (size_t)i * capN : nullptr;
   for (int oz = 0; oz < 5; oz++) {
     const int dz = co.off[2][oz];
     if (dz == 0x7fff) break;
@@ -174,7 +177,7 @@ __global__ void k_verlet(int n, const double *__restrict__ rx, const double *__r
         const int s = start[cell], e = start[cell + 1];
         for (int base = s; base < e; base += 32) {
           const int a = base + lane;
-          bool pass = false;
+          bool pass = false, near = false;
           int k = -1;
           if (a < e) {
             k = cell_atoms[a];
@@ -182,14 +185,24 @@ __global__ void k_verlet(int n, const double *__restrict__ rx, const double *__r
               double ddx = __dsub_rn(xi, rx[k]), ddy = __dsub_rn(yi, ry[k]), ddz = __dsub_rn(zi, rz[k]);
               const double d2 = image_exact(ddx, ddy, ddz, bx);
               pass = d2 <= rl2;
+              near = d2 <= rn2;
             }
           }
+          const unsigned lt = (1u << lane) - 1u;
           const unsigned m = __ballot_sync(0xffffffffu, pass);
           if (pass) {
-            const int pos = count + __popc(m & ((1u << lane) - 1u));
+            const int pos = count + __popc(m & lt);
             if (pos < cap) row[pos] = k;
           }
           count += __popc(m);
+          if (rowN) {
+            const unsigned mn = __ballot_sync(0xffffffffu, near);
+            if (near) {
+              const int pos = countN + __popc(mn & lt);
+              if (pos < capN) rowN[pos] = k;
+            }
+            countN += __popc(mn);
+          }
         }
       }
     }
@@ -197,6 +210,10 @@ __global__ void k_verlet(int n, const double *__restrict__ rx, const double *__r
   if (lane == 0) {
     nbr_cnt[i] = count;
     if (count > cap) atomicOr(flags, FLAG_NBR_OVERFLOW);
+    if (rowN) {
+      nbl_cnt[i] = countN;
+      if (countN > capN) atomicOr(flags, FLAG_NBR_OVERFLOW);
+    }
   }
 }
 
@@ -341,6 +358,7 @@ void launch_neighbor_list(Handle &h, bool force) {
     cudaStreamSynchronize(h.stream);
   }
   const double rl = fmax(h.prm.vdw_cutoff, h.prm.ewald_cutoff) + h.prm.list_buffer;
+  const double rn = h.prm.ewald_cutoff + h.prm.list_buffer + 2.0 * kNearDelta;
   if (h.vacuum) {
     k_vacuum_pairs<<<nblocks((int64_t)n * 32, 256), 256, 0, h.stream>>>(n, h.d_mol, h.alch.inter, h.alch.intra,
                                                                         h.cap_nbr, h.d_nbr, h.d_nbr_sh, h.d_nbr_cnt,
@@ -369,7 +387,8 @@ void launch_neighbor_list(Handle &h, bool force) {
   k_cell_sort<<<nblocks(ncells, 128), 128, 0, h.stream>>>(ncells, h.d_cell_start, h.d_cell_atoms, h.d_flags);
   k_verlet<<<nblocks((int64_t)n * 32, 256), 256, 0, h.stream>>>(
       n, h.d_rx, h.d_ry, h.d_rz, h.box, cell_offsets(h.ncell), h.d_atom_cell, h.d_cell_start, h.d_cell_atoms,
-      rl * rl, h.cap_nbr, h.d_nbr, h.d_nbr_cnt, h.d_flags);
+      rl * rl, h.cap_nbr, h.d_nbr, h.d_nbr_cnt, h.d_flags, rn * rn, h.cap_nbl, h.near_list ? h.d_nbl : nullptr,
+      h.d_nbl_cnt);
   k_list_done<<<nblocks(n, 256), 256, 0, h.stream>>>(n, h.d_refx, h.d_refy, h.d_refz, h.d_rx, h.d_ry, h.d_rz,
                                                       h.d_flags);
   h.launches += 6;

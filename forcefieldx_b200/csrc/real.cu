@@ -60,7 +60,8 @@ __global__ void __launch_bounds__(128, sizeof(R) == 4 ? 8 : 1) k_realspace_field
     double off2, double pcut2, int *ewl, int *ewl_cnt, int capE, int *ewl_sh, int *prl, int *prl_cnt, int capP,
     PairRec<R> *coefE, R *coefEB,
     PairRec<R> *coefP, R *coefPB, Excl ex, EwaldCoef ec, const __grid_constant__ ScaleTables c_scales,
-    double *fieldD, double *fieldP, int *flags, const double2 *__restrict__ pos, const R *__restrict__ rec) {
+    double *fieldD, double *fieldP, int *flags, const double2 *__restrict__ pos, const R *__restrict__ rec,
+    const int *__restrict__ nbl, const int *__restrict__ nbl_cnt, int capN) {
   using V2 = typename Vec2<R>::type;
   const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const int lane = threadIdx.x & 31;
@@ -68,10 +69,12 @@ __global__ void __launch_bounds__(128, sizeof(R) == 4 ? 8 : 1) k_realspace_field
   const int i = warp;
   const unsigned lt = (1u << lane) - 1u;
   const double xi = x[i], yi = y[i], zi = z[i];
-  // ---- phase 1: sub-lists
+  // ---- phase 1: sub-lists, from the near row when the near list is valid (every Ewald
+  // pair of this evaluation is in it), else from the buffered row
   {
-    const int cnt = min(nbr_cnt[i], cap);
-    const int *row = nbr + (size_t)i * cap;
+    const bool nearrow = nbl && !(*flags & FLAG_NEAR_INVALID);
+    const int cnt = nearrow ? min(nbl_cnt[i], capN) : min(nbr_cnt[i], cap);
+    const int *row = nearrow ? nbl + (size_t)i * capN : nbr + (size_t)i * cap;
     int ce = 0, cp = 0;
     for (int base = 0; base < cnt; base += 32) {
       const int a = base + lane;
@@ -767,7 +770,7 @@ static void realspace_field(Handle &h) {
       reinterpret_cast<PairRec<R> *>(h.d_coefE), reinterpret_cast<R *>(h.d_coefEB),
       reinterpret_cast<PairRec<R> *>(h.d_coefP), reinterpret_cast<R *>(h.d_coefPB), excl(h),
       ewald_coef(h, ewald_alpha_of(h)), h.scales, h.d_fieldD, h.d_fieldP, h.d_flags, h.d_pos,
-      reinterpret_cast<const R *>(h.d_erec));
+      reinterpret_cast<const R *>(h.d_erec), h.near_list ? h.d_nbl : nullptr, h.d_nbl_cnt, h.cap_nbl);
   FFX_LAUNCHED(h);
 }
 
