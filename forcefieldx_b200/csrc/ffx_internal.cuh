@@ -465,6 +465,7 @@ struct Handle {
   // Captured evaluations run the vdW term (independent of electrostatics) on its own
   // low-priority stream beside the permanent field and the PCG, joined before the gradient.
   bool capturing = false;
+  bool batch_branch = false;                        // captured as one branch of a batch graph
   int num_sms = 148;
   cudaStream_t vdw_stream = nullptr;
   cudaEvent_t ev_vdw_fork = nullptr, ev_vdw_join = nullptr;
