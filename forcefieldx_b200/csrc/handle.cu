@@ -506,9 +506,10 @@ static void emit_front(Handle &h, const double *d_xyz) {
   launch_set_coordinates(h, d_xyz);
   launch_neighbor_list(h, false);
   timer_end(h, tk);
-  if (h.capturing && !h.vacuum) {
+  if (h.capturing && !h.vacuum && !h.batch_branch) {
     // A branch of the graph: vdW depends on the list alone, and only the gradient
-    // assembly and the sums read it (emit_back joins it there).
+    // assembly and the sums read it (emit_back joins it there).  Inside a batch graph the
+    // systems are the branches, and vdW stays in line (measured 16% more systems/s).
     cudaEventRecord(h.ev_vdw_fork, h.stream);
     cudaStreamWaitEvent(h.vdw_stream, h.ev_vdw_fork, 0);
     launch_vdw(h, h.want_grad, h.vdw_stream);
@@ -590,7 +591,7 @@ static void emit_back(Handle &h, double *d_grad_xyz) {
   tk = timer_begin(h, FFXG_STAGE_RECIP_ENERGY);
   launch_recip_energy(h, h.want_grad);
   timer_end(h, tk);
-  if (h.capturing && !h.vacuum) cudaStreamWaitEvent(h.stream, h.ev_vdw_join, 0);
+  if (h.capturing && !h.vacuum && !h.batch_branch) cudaStreamWaitEvent(h.stream, h.ev_vdw_join, 0);
   tk = timer_begin(h, FFXG_STAGE_GRADIENT);
   if (h.want_grad) {
     launch_torque(h);
