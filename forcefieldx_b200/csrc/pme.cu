@@ -792,7 +792,7 @@ static std::vector<double> bsmod_host(int nfft, int order, const std::vector<dou
 
 static FftAxis make_axis(int axis, const int nf[3]) {
   FftAxis a{};
-  const int nx = nf[0], ny = nf[1], nz = nf[2];
+  const int nx = nf[0], ny = nf[1];
   a.len = nf[axis];
   int m = a.len;
   a.nradix = 0;
