@@ -250,8 +250,11 @@ __global__ void k_direct_dipoles(int n, const double *__restrict__ gm, const dou
 // 2153-2176): pairs with a soft atom take r^2 + beta and the scale permScale in the
 // permanent part, the polarization part is scaled by polScale, and dU/dL, d2U/dL2, the
 // lambda gradient and torque are gathered (written to edl/ed2l/lgrad/ltorque).
-template <typename R, bool LAM>
-__global__ void __launch_bounds__(128, sizeof(R) == 4 ? 4 : 1) k_real_energy(
+#ifndef FFX_REAL_ENERGY_MIN_BLOCKS
+#define FFX_REAL_ENERGY_MIN_BLOCKS 4   // FP32 form: resident 128-thread blocks per SM
+#endif
+template <typename R, bool LAM, bool DIRECT>
+__global__ void __launch_bounds__(128, sizeof(R) == 4 ? FFX_REAL_ENERGY_MIN_BLOCKS : 1) k_real_energy(
     int n, const double *__restrict__ x, const double *__restrict__ y, const double *__restrict__ z, Box bx,
     const double *__restrict__ gm, const double *__restrict__ uD, const double *__restrict__ uP,
     const double *__restrict__ ipdamp, const double *__restrict__ thole, const int *__restrict__ ewl,
@@ -637,7 +640,7 @@ __global__ void __launch_bounds__(128, sizeof(R) == 4 ? 4 : 1) k_real_energy(
       ftm2ix = ftm2ix - fridmpx - findmpx;
       ftm2iy = ftm2iy - fridmpy - findmpy;
       ftm2iz = ftm2iz - fridmpz - findmpz;
-      if (polarization == FFXG_POLAR_DIRECT) {
+      if (DIRECT) {   // the direct-polarization terms (compiled out of the mutual form)
         const R gfd = R(0.5) * (bn2 * scip2 - bn3 * (scip3 * sci4 + sci3 * scip4));
         const R gfdr = R(0.5) * (rr5 * scip2 * usc3 - rr7 * (scip3 * sci4 + sci3 * scip4) * usc5);
         ftm2ix = ftm2ix - gfd * xr - R(0.5) * bn2 * (sci4 * pix + scip4 * uix + sci3 * pkx + scip3 * ukx);
@@ -798,7 +801,9 @@ void launch_realspace_field(Handle &h) {
 
 template <typename R>
 static void real_energy(Handle &h, bool grad) {
-  auto kern = h.step.lam ? k_real_energy<R, true> : k_real_energy<R, false>;
+  const bool direct = h.prm.polarization == FFXG_POLAR_DIRECT;
+  auto kern = h.step.lam ? (direct ? k_real_energy<R, true, true> : k_real_energy<R, true, false>)
+                         : (direct ? k_real_energy<R, false, true> : k_real_energy<R, false, false>);
   k_pack_induced<R><<<nblocks(h.n, 256), 256, 0, h.stream>>>(h.n, h.d_uD, h.d_uP, reinterpret_cast<R *>(h.d_erec));
   FFX_LAUNCHED(h);
   kern<<<nblocks((int64_t)h.n * 32, 128), 128, 0, h.stream>>>(
