@@ -250,6 +250,19 @@ __global__ void k_direct_dipoles(int n, const double *__restrict__ gm, const dou
 // 2153-2176): pairs with a soft atom take r^2 + beta and the scale permScale in the
 // permanent part, the polarization part is scaled by polScale, and dU/dL, d2U/dL2, the
 // lambda gradient and torque are gathered (written to edl/ed2l/lgrad/ltorque).
+// Adds (vx, vy, vz) to row-major [3][n] v at atom k.  FP64 form: FP64 atomics.  FP32 form:
+// each value is rounded to a multiple of 2^-32 first, so the sums are exact in FP64 (below
+// 2^21 in magnitude) and independent of the order of the atomics.
+template <typename R>
+__device__ __forceinline__ void real_acc(double *v, int k, double vx, double vy, double vz, int n) {
+  if constexpr (sizeof(R) == 4) {
+    vx = rint(vx * 4294967296.0) * 2.3283064365386962890625e-10;
+    vy = rint(vy * 4294967296.0) * 2.3283064365386962890625e-10;
+    vz = rint(vz * 4294967296.0) * 2.3283064365386962890625e-10;
+  }
+  atomicAdd(v + k, vx); atomicAdd(v + n + k, vy); atomicAdd(v + 2 * (size_t)n + k, vz);
+}
+
 #ifndef FFX_REAL_ENERGY_MIN_BLOCKS
 #define FFX_REAL_ENERGY_MIN_BLOCKS 4   // FP32 form: resident 128-thread blocks per SM
 #endif
@@ -262,6 +275,8 @@ __global__ void __launch_bounds__(128, sizeof(R) == 4 ? FFX_REAL_ENERGY_MIN_BLOC
     double *eatom_perm, double *eatom_pol, long long *catom, double *grad, double *torque,
     const int *__restrict__ soft, ElecStep st, double *edl, double *ed2l, double *lgrad, double *ltorque,
     const double2 *__restrict__ pos, const R *__restrict__ rec) {
+  constexpr bool HALF = !LAM && !DIRECT;   // the softcore and direct forms walk the full rows
+  __shared__ int qbuf[HALF ? 4 : 1][64];
   const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const int lane = threadIdx.x & 31;
   if (warp >= n) return;
@@ -288,7 +303,11 @@ __global__ void __launch_bounds__(128, sizeof(R) == 4 ? FFX_REAL_ENERGY_MIN_BLOC
   const int soft_i = LAM ? soft[i] : 0;
   const int cnt = min(ewl_cnt[i], capE);
   const int *row = ewl + (size_t)i * capE;
-  for (int a = lane; a < cnt; a += 32) {
+  // One pair of the Ewald row (entry a).  The full form (HALF false) takes every entry and
+  // keeps only atom i's share; the half form takes each pair once (pair_counted) and adds
+  // atom k's force and torque (RealSpaceEnergyRegion.java:1457-1460, 2157-2160) with
+  // atomics into grad and torque, zeroed by k_pack_induced.
+  auto pair = [&](int a) {
     const int k = row[a];
     const size_t ent = (size_t)i * capE + a;
     double xk, yk, zk;
@@ -396,7 +415,7 @@ __global__ void __launch_bounds__(128, sizeof(R) == 4 ? FFX_REAL_ENERGY_MIN_BLOC
       const R ereal = gl0 * bn0 + (gl1 + gl6) * bn1 + (gl2 + gl7 + gl8) * bn2 + (gl3 + gl5) * bn3 + gl4 * bn4;
       const R efix = scale1 * (gl0 * rr1 + (gl1 + gl6) * rr3 + (gl2 + gl7 + gl8) * rr5 + (gl3 + gl5) * rr7 + gl4 * rr9);
       const R e = ereal - efix;
-      if (e != R(0.0)) { eP += R(0.5) * (LAM ? l2 * e : e); if (pair_counted(i, k, ewl_sh, ent)) cnt_pairs++; }
+      if (e != R(0.0)) { eP += (HALF ? R(1.0) : R(0.5)) * (LAM ? l2 * e : e); if (pair_counted(i, k, ewl_sh, ent)) cnt_pairs++; }
       if (gr) {
         const R gf1 = bn1 * gl0 + bn2 * (gl1 + gl6) + bn3 * (gl2 + gl7 + gl8) + bn4 * (gl3 + gl5) + bn5 * gl4;
         const R gf2 = -ck * bn1 + sc4 * bn2 - sc6 * bn3;
@@ -438,6 +457,10 @@ __global__ void __launch_bounds__(128, sizeof(R) == 4 ? FFX_REAL_ENERGY_MIN_BLOC
         const R pre = LAM ? electric * l2 : electric;
         gx += pre * ftm2x; gy += pre * ftm2y; gz += pre * ftm2z;
         tx += pre * ttm2x; ty += pre * ttm2y; tz += pre * ttm2z;
+        if constexpr (HALF) {
+          real_acc<R>(grad, k, -pre * ftm2x, -pre * ftm2y, -pre * ftm2z, n);
+          real_acc<R>(torque, k, pre * ttm3x, pre * ttm3y, pre * ttm3z, n);
+        }
         if (LAM && spair) {   // d[dlPow * ereal]/dX (:1465-1475)
           const R pf = electric * (R)(st.dEdLSign * st.dlPowPerm);
           lgx += pf * ftm2x; lgy += pf * ftm2y; lgz += pf * ftm2z;
@@ -496,7 +519,7 @@ __global__ void __launch_bounds__(128, sizeof(R) == 4 ? FFX_REAL_ENERGY_MIN_BLOC
         ltx += pf * qx; lty += pf * qy; ltz += pf * qz;
       }
     }
-    if (!doPol) continue;
+    if (!doPol) return;
     // ---- polarizationPair
     {
       const R dsc3 = R(1.0) - scale3 * scaled, dsc5 = R(1.0) - scale5 * scaled, dsc7 = R(1.0) - scale7 * scaled;
@@ -558,12 +581,12 @@ __global__ void __launch_bounds__(128, sizeof(R) == 4 ? FFX_REAL_ENERGY_MIN_BLOC
       const R ereal = (gli1 + gli6) * bn1 + (gli2 + gli7) * bn2 + gli3 * bn3;
       const R efix = (gli1 + gli6) * rr3 * psc3 + (gli2 + gli7) * rr5 * psc5 + gli3 * rr7 * psc7;
       const R epol = R(0.25) * (ereal - efix);
-      eI += LAM ? (R)st.polScale * epol : epol;
+      eI += HALF ? R(2.0) * epol : (LAM ? (R)st.polScale * epol : epol);
       if (LAM) {
         dl += st.dEdLSign * st.dlPowPol * (double)epol;
         d2l += st.dEdLSign * st.d2lPowPol * (double)epol;
       }
-      if (!gr) continue;
+      if (!gr) return;
       const bool dorli = (psc3 != R(0.0) || dsc3 != R(0.0) || usc3 != R(0.0));
       const R gfi1 = R(0.5) * bn2 * (gli1 + glip1 + gli6 + glip6) + R(0.5) * bn2 * scip2 +
                           R(0.5) * bn3 * (gli2 + glip2 + gli7 + glip7) - R(0.5) * bn3 * (sci3 * scip4 + scip3 * sci4) +
@@ -659,6 +682,10 @@ __global__ void __launch_bounds__(128, sizeof(R) == 4 ? FFX_REAL_ENERGY_MIN_BLOC
       const R sc = LAM ? electric * (R)st.polScale : electric;
       gx += sc * ftm2ix; gy += sc * ftm2iy; gz += sc * ftm2iz;
       tx += sc * ttm2ix; ty += sc * ttm2iy; tz += sc * ttm2iz;
+      if constexpr (HALF) {
+        real_acc<R>(grad, k, -sc * ftm2ix, -sc * ftm2iy, -sc * ftm2iz, n);
+        real_acc<R>(torque, k, sc * ttm3ix, sc * ttm3iy, sc * ttm3iz, n);
+      }
       if (LAM) {   // RealSpaceEnergyRegion.java:2163-2174
         const R sl = electric * (R)(st.dEdLSign * st.dlPowPol);
         lgx += sl * ftm2ix; lgy += sl * ftm2iy; lgz += sl * ftm2iz;
@@ -666,6 +693,33 @@ __global__ void __launch_bounds__(128, sizeof(R) == 4 ? FFX_REAL_ENERGY_MIN_BLOC
       }
     }
 
+  };
+  if constexpr (HALF) {
+    // Counted entries are queued in shared memory and evaluated 32 at a time, so the
+    // pair arithmetic runs on full warps although half of each row is skipped.
+    // One call site of the pair body: fill to 32 or the end of the row, evaluate, shift.
+    int *q = qbuf[threadIdx.x >> 5];
+    int qn = 0, base = 0;   // warp-uniform; qn < 64 after every fill
+    while (true) {
+      while (qn < 32 && base < cnt) {
+        const int a = base + lane;
+        const bool take = a < cnt && pair_counted(i, row[a], ewl_sh, (size_t)i * capE + a);
+        const unsigned bal = __ballot_sync(0xffffffffu, take);
+        if (take) q[qn + __popc(bal & ((1u << lane) - 1u))] = a;
+        qn += __popc(bal);
+        base += 32;
+      }
+      __syncwarp();
+      if (qn == 0) break;
+      if (lane < qn) pair(q[lane]);
+      __syncwarp();
+      const int rest = qn > 32 ? qn - 32 : 0;
+      if (lane < rest) q[lane] = q[lane + 32];
+      __syncwarp();
+      qn = rest;
+    }
+  } else {
+    for (int a = lane; a < cnt; a += 32) pair(a);
   }
   eP = warp_sum(eP); eI = warp_sum(eI);
   const double Gx = warp_sum((double)gx), Gy = warp_sum((double)gy), Gz = warp_sum((double)gz);
@@ -683,8 +737,13 @@ __global__ void __launch_bounds__(128, sizeof(R) == 4 ? FFX_REAL_ENERGY_MIN_BLOC
     eatom_pol[i] = eI * ec.electric;
     catom[i] = cnt_pairs;
     if (gr) {
-      grad[i] = Gx; grad[n + i] = Gy; grad[2 * n + i] = Gz;
-      torque[i] = Tx; torque[n + i] = Ty; torque[2 * n + i] = Tz;
+      if constexpr (HALF) {
+        real_acc<R>(grad, i, Gx, Gy, Gz, n);
+        real_acc<R>(torque, i, Tx, Ty, Tz, n);
+      } else {
+        grad[i] = Gx; grad[n + i] = Gy; grad[2 * n + i] = Gz;
+        torque[i] = Tx; torque[n + i] = Ty; torque[2 * n + i] = Tz;
+      }
     }
     if (LAM) {
       edl[i] = L[0] * ec.electric;
@@ -740,9 +799,14 @@ __global__ void k_pack_mpole(int n, const double *__restrict__ gm, const double 
 }
 
 template <typename R>
-__global__ void k_pack_induced(int n, const double *__restrict__ uD, const double *__restrict__ uP, R *rec) {
+__global__ void k_pack_induced(int n, const double *__restrict__ uD, const double *__restrict__ uP, R *rec,
+                               double *grad, double *torque) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
+  if (grad) {   // the half-row real-space energy adds into these
+    grad[i] = grad[n + i] = grad[2 * (size_t)n + i] = 0.0;
+    torque[i] = torque[n + i] = torque[2 * (size_t)n + i] = 0.0;
+  }
   R *o = rec + (size_t)i * kRecStride + kRecInduced;
   o[0] = (R)uD[i]; o[1] = (R)uD[n + i]; o[2] = (R)uD[2 * (size_t)n + i];
   o[3] = (R)uP[i]; o[4] = (R)uP[n + i]; o[5] = (R)uP[2 * (size_t)n + i];
@@ -804,7 +868,9 @@ static void real_energy(Handle &h, bool grad) {
   const bool direct = h.prm.polarization == FFXG_POLAR_DIRECT;
   auto kern = h.step.lam ? (direct ? k_real_energy<R, true, true> : k_real_energy<R, true, false>)
                          : (direct ? k_real_energy<R, false, true> : k_real_energy<R, false, false>);
-  k_pack_induced<R><<<nblocks(h.n, 256), 256, 0, h.stream>>>(h.n, h.d_uD, h.d_uP, reinterpret_cast<R *>(h.d_erec));
+  const bool half = !h.step.lam && !direct;   // k_real_energy's HALF form
+  k_pack_induced<R><<<nblocks(h.n, 256), 256, 0, h.stream>>>(h.n, h.d_uD, h.d_uP, reinterpret_cast<R *>(h.d_erec),
+                                                             half && grad ? h.d_grad : nullptr, h.d_torque);
   FFX_LAUNCHED(h);
   kern<<<nblocks((int64_t)h.n * 32, 128), 128, 0, h.stream>>>(
       h.n, h.d_x, h.d_y, h.d_z, h.box, h.d_gm, h.d_uD, h.d_uP, h.d_ipdamp, h.d_thole, h.d_ewl, h.d_ewl_cnt,
