@@ -9,10 +9,11 @@ _I = ctypes.POINTER(ctypes.c_int32)
 _L = ctypes.POINTER(ctypes.c_int64)
 
 N_TERMS = 10
-N_COUNTS = 5
+N_COUNTS = 6
 
 STATUS_NAMES = {0: "OK", 1: "BAD_ARG", 2: "CUDA", 3: "SCF_DIVERGED", 4: "SCF_MAXITER",
-                5: "NONFINITE", 6: "CAPACITY"}
+                5: "NONFINITE", 6: "CAPACITY", 7: "RANGE"}
+STATUS_RANGE = 7
 
 
 class FfxgSystem(ctypes.Structure):
@@ -76,11 +77,14 @@ PROTOTYPES = {
     "ffxg_destroy": (None, [ctypes.c_void_p]),
     "ffxg_last_error": (ctypes.c_char_p, [ctypes.c_void_p]),
     "ffxg_set_coordinates": (ctypes.c_int, [ctypes.c_void_p, _D]),
+    "ffxg_set_box": (ctypes.c_int, [ctypes.c_void_p, _D, _I]),
+    "ffxg_update_parameters": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(FfxgSystem)]),
     "ffxg_energy": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, _D, _D, _L]),
     "ffxg_energy_and_gradient": (ctypes.c_int, [ctypes.c_void_p, _D, _D, _D, _L]),
     "ffxg_energy_device": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, _D, _L]),
     "ffxg_get_induced_dipoles": (ctypes.c_int, [ctypes.c_void_p, _D, _D]),
     "ffxg_get_global_multipoles": (ctypes.c_int, [ctypes.c_void_p, _D]),
+    "ffxg_get_permanent_potential": (ctypes.c_int, [ctypes.c_void_p, _D]),
     "ffxg_get_neighbor_pairs": (ctypes.c_int, [ctypes.c_void_p, _I, _L]),
     "ffxg_get_neighbor_images": (ctypes.c_int, [ctypes.c_void_p, _I, _L]),
     "ffxg_set_image_mode": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int]),

@@ -207,6 +207,7 @@ int ffxg_batch_energy(ffxg_batch *b, const double *xyz, int want_grad, double *t
     for (size_t s = 0; s < S; s++) {
       Handle &h = handle_of(b->sys[s]);
       h.want_grad = want_grad != 0;
+      h.growths = 0;
       const int r = eval_after_graph(h, terms + s * FFXG_N_TERMS, counts ? counts + s * FFXG_N_COUNTS : nullptr);
       if (r == -1) {           // a list grew: the batch graph holds the old buffers
         redo[s] = 1;
@@ -221,6 +222,7 @@ int ffxg_batch_energy(ffxg_batch *b, const double *xyz, int want_grad, double *t
   for (size_t s = 0; s < S; s++) {
     if (!redo[s]) continue;
     Handle &h = handle_of(b->sys[s]);
+    if (!graph) h.growths = 0;   // a graph replay counted its regrowth already
     st[s] = evaluate(h, b->d_xyz + 3 * b->off[s], b->d_grad + 3 * b->off[s], want_grad != 0,
                      terms + s * FFXG_N_TERMS, counts ? counts + s * FFXG_N_COUNTS : nullptr);
   }

@@ -35,7 +35,17 @@ enum : int {
   FLAG_REBUILD = 16,
   FLAG_IMAGE_RANGE = 32,   // a multi-image shift beyond the 10-bit packing (|n| > 511)
   FLAG_NEAR_INVALID = 64,  // a hydrogen's reduction offset exceeds the near list's margin
+  FLAG_QUANT_RANGE = 128,  // mixed form: a fixed-point (2^-32) value reached kQuantLimit
 };
+
+// The mixed form accumulates forces, torques and the PME mesh as FP64 sums of values
+// rounded to multiples of 2^-32: such sums are exact, hence independent of the order of
+// the atomics, while every partial sum stays below 2^21 in magnitude.  A contribution or
+// an accumulated value of kQuantLimit = 2^20 or more raises FLAG_QUANT_RANGE, and the
+// evaluation returns FFXG_ERR_RANGE: its results are complete and FP64-accurate, but no
+// longer guaranteed to repeat bit for bit.
+constexpr double kQuantLimit = 1048576.0;
+__device__ __forceinline__ bool quant_out(double v) { return fabs(v) >= kQuantLimit; }
 
 // The near list: at every rebuild of the buffered list the cell builder also keeps the
 // pairs within ewald-cutoff + buffer + 2 kNearDelta on the reduced coordinates, where
@@ -339,6 +349,7 @@ struct Handle {
   double *d_refx = nullptr, *d_refy = nullptr, *d_refz = nullptr;  // list reference coords
   bool list_valid = false;
   int ncell[3] = {0, 0, 0};
+  int cell_cap = 0;                           // cells the cell-list arrays hold
   int *d_cell_cnt = nullptr, *d_cell_start = nullptr, *d_cell_atoms = nullptr, *d_atom_cell = nullptr;
   int cap_nbr = 0, cap_ewl = 0, cap_prl = 0;
   int *d_nbr = nullptr, *d_nbr_cnt = nullptr;
@@ -440,6 +451,7 @@ struct Handle {
   double e_corr_env = 0.0;
   Handle *vac = nullptr;
   std::vector<int> lig;
+  std::vector<int> soft_host, mol_host;             // the last ffxg_set_alchemy's atoms
   int *d_lig = nullptr;
   bool vacuum = false;                              // this handle is a vacuum sub-system
   int eps_atoms = 0;                                // atom count of the PCG residual norm (0: n);
@@ -488,6 +500,7 @@ struct Handle {
   double stage_ms[16] = {0};
   int64_t stage_calls[16] = {0};
   int64_t list_builds = 0;
+  int64_t growths = 0;             // list capacity regrowths during the current call
 };
 
 // Ewald coefficient of the evaluation: 0 for a vacuum sub-system (no screening).
@@ -535,7 +548,7 @@ void launch_zero_soft_multipoles(Handle &h);
 void launch_assemble(Handle &h, double *d_grad_xyz);
 void launch_reduce_results(Handle &h);
 int param_gradients(Handle &h, double *dEdM, double *dEdA);
-void setup_pme(Handle &h);
+int setup_pme(Handle &h);   // FFXG_OK or a status (h.err set)
 
 inline int nblocks(int64_t n, int t) { return (int)((n + t - 1) / t); }
 

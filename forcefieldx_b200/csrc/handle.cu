@@ -112,6 +112,50 @@ static int alloc_lists(Handle &h) {
 
 static int round32(double v) { return ((int)std::ceil(v) + 31) / 32 * 32; }
 
+// The orthorhombic cell of Crystal (a, b, c; A = 1 / edges; volume).
+static void set_cell(Handle &h, const double box[3]) {
+  for (int d = 0; d < 3; d++) h.prm.box[d] = box[d];
+  h.box.a = box[0]; h.box.b = box[1]; h.box.c = box[2];
+  h.box.A00 = 1.0 / h.box.a; h.box.A11 = 1.0 / h.box.b; h.box.A22 = 1.0 / h.box.c;
+  h.box.Ai00 = h.box.a; h.box.Ai11 = h.box.b; h.box.Ai22 = h.box.c;
+  h.box.volume = h.box.a * h.box.b * h.box.c;
+}
+
+// Cells of the list builder: edges of at least half the buffered cutoff.
+static void set_cell_grid(Handle &h) {
+  const double rlist = std::max(h.prm.vdw_cutoff, h.prm.ewald_cutoff) + h.prm.list_buffer;
+  for (int d = 0; d < 3; d++) h.ncell[d] = std::max(1, (int)std::floor(h.prm.box[d] / (rlist * 0.5)));
+}
+
+// Charge correction of a charged cell, -1/2 electric pi q^2 / (V alpha^2)
+// (ReciprocalEnergyRegion.java:229-255), for total charge q.
+static double charge_correction(const Handle &h, double q) {
+  const double PI = 3.14159265358979323846;
+  return (q != 0.0) ? -0.5 * h.prm.electric * PI * (q * q) / (h.box.volume * h.prm.ewald_alpha * h.prm.ewald_alpha)
+                    : 0.0;
+}
+
+// The PME mesh of h.prm.pme_grid, its influence function and twiddles (any earlier mesh
+// is released first).
+static int alloc_mesh(Handle &h) {
+  for (void *q : {(void *)h.d_grid, (void *)h.d_influence, (void *)h.d_twiddle, (void *)h.d_gridf,
+                  (void *)h.d_influencef, (void *)h.d_twiddlef})
+    if (q) cudaFree(q);
+  h.d_grid = nullptr; h.d_influence = nullptr; h.d_twiddle = nullptr;
+  h.d_gridf = nullptr; h.d_influencef = nullptr; h.d_twiddlef = nullptr;
+  const int nfx = h.prm.pme_grid[0], nfy = h.prm.pme_grid[1], nfz = h.prm.pme_grid[2];
+  const size_t ng = (size_t)nfx * nfy * nfz;
+  CK(dalloc(&h.d_grid, ng)); CK(dalloc(&h.d_influence, ng));
+  CK(cudaMemset(h.d_grid, 0, ng * sizeof(double2)));   // the mixed form keeps it clear between uses
+  CK(dalloc(&h.d_twiddle, 3 * (size_t)std::max(nfx, std::max(nfy, nfz))));
+  if (h.mixed) {
+    CK(dalloc(&h.d_gridf, ng));
+    CK(dalloc(&h.d_influencef, ng));
+    CK(dalloc(&h.d_twiddlef, 3 * (size_t)std::max(nfx, std::max(nfy, nfz))));
+  }
+  return FFXG_OK;
+}
+
 static double near_radius(const Handle &h) {
   return h.prm.ewald_cutoff + h.prm.list_buffer + 2.0 * kNearDelta;
 }
@@ -222,10 +266,7 @@ static int create_impl(const ffxg_system *s, const ffxg_params *p, Handle &h) {
   CK(cudaEventCreateWithFlags(&h.ev_recip_fork, cudaEventDisableTiming));
   CK(cudaEventCreateWithFlags(&h.ev_recip_join, cudaEventDisableTiming));
 
-  h.box.a = p->box[0]; h.box.b = p->box[1]; h.box.c = p->box[2];
-  h.box.A00 = 1.0 / h.box.a; h.box.A11 = 1.0 / h.box.b; h.box.A22 = 1.0 / h.box.c;
-  h.box.Ai00 = h.box.a; h.box.Ai11 = h.box.b; h.box.Ai22 = h.box.c;
-  h.box.volume = h.box.a * h.box.b * h.box.c;
+  set_cell(h, p->box);
 
   // ---- validate topology indices
   for (int i = 0; i < n; i++) {
@@ -308,8 +349,9 @@ static int create_impl(const ffxg_system *s, const ffxg_params *p, Handle &h) {
   h.cap_nbl = round32(1.3 * sphere(std::min(near_radius(h), rlist)) + 64);
   h.cap_ewl = round32(1.3 * sphere(p->ewald_cutoff) + 32);
   h.cap_prl = round32(1.3 * sphere(p->precond_cutoff) + 32);
-  for (int d = 0; d < 3; d++) h.ncell[d] = std::max(1, (int)std::floor(p->box[d] / (rlist * 0.5)));
+  set_cell_grid(h);
   const int ncells = h.ncell[0] * h.ncell[1] * h.ncell[2];
+  h.cell_cap = ncells;
 
   // ---- allocations
   const size_t N = n;
@@ -355,16 +397,7 @@ static int create_impl(const ffxg_system *s, const ffxg_params *p, Handle &h) {
   CK(cudaMallocHost((void **)&h.h_scalars, 16 * sizeof(double)));
   CK(cudaMalloc((void **)&h.d_pcg, sizeof(PcgState)));
   CK(cudaMallocHost((void **)&h.h_pcg, sizeof(PcgState)));
-  const int nfx = p->pme_grid[0], nfy = p->pme_grid[1], nfz = p->pme_grid[2];
-  const size_t ng = (size_t)nfx * nfy * nfz;
-  CK(dalloc(&h.d_grid, ng)); CK(dalloc(&h.d_influence, ng));
-  CK(cudaMemset(h.d_grid, 0, ng * sizeof(double2)));   // the mixed form keeps it clear between uses
-  CK(dalloc(&h.d_twiddle, 3 * (size_t)std::max(nfx, std::max(nfy, nfz))));
-  if (h.mixed) {
-    CK(dalloc(&h.d_gridf, ng));
-    CK(dalloc(&h.d_influencef, ng));
-    CK(dalloc(&h.d_twiddlef, 3 * (size_t)std::max(nfx, std::max(nfy, nfz))));
-  }
+  if (int st = alloc_mesh(h)) return st;
   CK(dalloc(&h.d_grad, 3 * N)); CK(dalloc(&h.d_torque, 3 * N)); CK(dalloc(&h.d_gred, 6 * N));
   CK(dalloc(&h.d_eatom, (size_t)kEnergyRows * N)); CK(dalloc(&h.d_catom, 2 * N));
   CK(cudaMemset(h.d_eatom, 0, (size_t)kEnergyRows * N * sizeof(double)));
@@ -420,9 +453,9 @@ static int create_impl(const ffxg_system *s, const ffxg_params *p, Handle &h) {
   {
     double q = 0.0;
     for (int i = 0; i < n; i++) q += s->multipole[10 * (size_t)i];
-    h.e_charge_correction = (q != 0.0) ? -0.5 * p->electric * PI * (q * q) / (h.box.volume * p->ewald_alpha * p->ewald_alpha) : 0.0;
+    h.e_charge_correction = charge_correction(h, q);
   }
-  setup_pme(h);
+  if (const int st = setup_pme(h)) return st;
   CK(cudaGetLastError());
   // Coordinates.
   std::memcpy(h.h_xyz_pin, s->xyz, 3 * N * sizeof(double));
@@ -664,14 +697,20 @@ static int finish(Handle &h, bool rebuilt, double *terms, int64_t *counts) {
     counts[FFXG_COUNT_SCF_ITER] = h.scf_iter;
     counts[FFXG_COUNT_LIST_BUILDS] = rebuilt ? 1 : 0;
     counts[FFXG_COUNT_LIST_PAIRS] = -1;
+    counts[FFXG_COUNT_LIST_GROWTHS] = h.growths;
   }
   if (h.h_flags[0] & FLAG_NONFINITE) { h.err = "non-finite energy, torque or gradient"; return FFXG_ERR_NONFINITE; }
   for (int t = 0; t < 7; t++)
     if (!std::isfinite(res[t])) { h.err = "non-finite energy"; return FFXG_ERR_NONFINITE; }
+  if (h.h_flags[0] & FLAG_QUANT_RANGE) {
+    h.err = "a fixed-point force, torque or mesh sum reached 2^20: results are valid but not bitwise reproducible";
+    return FFXG_ERR_RANGE;
+  }
   return FFXG_OK;
 }
 
 static int grow_lists(Handle &h, int f) {
+  h.growths++;
   if (f & FLAG_NBR_OVERFLOW) {   // the buffered row or the near row
     h.cap_nbr = round32(h.cap_nbr * 1.5);
     h.cap_nbl = round32(h.cap_nbl * 1.5);
@@ -1009,8 +1048,8 @@ static int evaluate_elec(Handle &h, const double *d_xyz, double *d_grad_xyz, dou
   return FFXG_ERR_CAPACITY;
 }
 
-namespace ffx {
-int evaluate(Handle &h, const double *d_xyz, double *d_grad_xyz, bool grad, double *terms, int64_t *counts) {
+static int evaluate_any(Handle &h, const double *d_xyz, double *d_grad_xyz, bool grad, double *terms,
+                        int64_t *counts) {
   if (h.elec.on && h.alch.active && !h.vacuum) {
     h.launches = 0;
     return evaluate_elec(h, d_xyz, d_grad_xyz, terms, counts);
@@ -1023,6 +1062,21 @@ int evaluate(Handle &h, const double *d_xyz, double *d_grad_xyz, bool grad, doub
     h.launches = 0;
   }
   return evaluate_direct(h, d_xyz, d_grad_xyz, terms, counts);
+}
+
+namespace ffx {
+// A launch that the runtime refuses (a bad configuration, too much shared memory) leaves
+// no trace in the stream, only in the thread's last-error state: an evaluation that began
+// with that state clear and ends with an error reports it instead of a partial result.
+// An error the caller left pending is neither cleared nor taken for this call's.
+int evaluate(Handle &h, const double *d_xyz, double *d_grad_xyz, bool grad, double *terms, int64_t *counts) {
+  const bool clear = cudaPeekAtLastError() == cudaSuccess;
+  const int st = evaluate_any(h, d_xyz, d_grad_xyz, grad, terms, counts);
+  if (clear && cudaPeekAtLastError() != cudaSuccess) {
+    h.err = std::string("CUDA launch error: ") + cudaGetErrorString(cudaGetLastError());
+    return FFXG_ERR_CUDA;
+  }
+  return st;
 }
 
 Handle &handle_of(ffxg_handle *hh) { return hh->h; }
@@ -1061,14 +1115,130 @@ int ffxg_set_coordinates(ffxg_handle *hh, const double *xyz) {
   return FFXG_OK;
 }
 
+static int setup_elec(Handle &h, const std::vector<int> &soft, const std::vector<int> &mol);
+
+// Crystal change (ForceFieldEnergy.setCrystal, ForceFieldEnergy.java:2650-2666, which passes
+// it to VanDerWaals, ParticleMeshEwald.setCrystal :1262-1283 and ReciprocalSpace.setCrystal
+// :750-761 / initConvolution :909-1000).
+int ffxg_set_box(ffxg_handle *hh, const double box[3], const int32_t pme_grid[3]) {
+  if (!hh || !box) return FFXG_ERR_BAD_ARG;
+  Handle &h = hh->h;
+  if (h.vacuum) { h.err = "a vacuum sub-system has no cell"; return FFXG_ERR_BAD_ARG; }
+  for (int d = 0; d < 3; d++) {
+    if (!(box[d] > 0.0) || !std::isfinite(box[d])) { h.err = "box edges must be positive"; return FFXG_ERR_BAD_ARG; }
+    if (pme_grid && !fft_supported(pme_grid[d])) {
+      h.err = "PME grid dimensions must be >= 5 and factor into 2, 3, 5 and 7";
+      return FFXG_ERR_BAD_ARG;
+    }
+  }
+  CK(cudaStreamSynchronize(h.stream));   // nothing in flight reads the old tables
+  const bool images_before = h.images, near_before = h.near_list;
+  set_cell(h, box);
+  configure_images(h);
+  set_cell_grid(h);
+  const int ncells = h.ncell[0] * h.ncell[1] * h.ncell[2];
+  if (ncells > h.cell_cap) {
+    cudaFree(h.d_cell_cnt);
+    cudaFree(h.d_cell_start);
+    h.d_cell_cnt = h.d_cell_start = nullptr;
+    CK(dalloc(&h.d_cell_cnt, 2 * (size_t)ncells));
+    CK(dalloc(&h.d_cell_start, (size_t)ncells + 1));
+    h.cell_cap = ncells;
+  }
+  if (pme_grid && (pme_grid[0] != h.prm.pme_grid[0] || pme_grid[1] != h.prm.pme_grid[1] ||
+                   pme_grid[2] != h.prm.pme_grid[2])) {
+    for (int d = 0; d < 3; d++) h.prm.pme_grid[d] = pme_grid[d];
+    if (int st = alloc_mesh(h)) return st;
+  }
+  if (int st = setup_pme(h)) return st;
+  double q = 0.0, qenv = 0.0;
+  for (int i = 0; i < h.n; i++) {
+    const double qi = h.sys.multipole[10 * (size_t)i];
+    q += qi;
+    if (!h.soft_host.empty() && !h.soft_host[i]) qenv += qi;
+  }
+  h.e_charge_correction = charge_correction(h, q);
+  if (h.elec.on) h.e_corr_env = charge_correction(h, qenv);
+  if (h.images != images_before || h.near_list != near_before) {
+    if (int st = alloc_lists(h)) return st;   // also drops the graphs and invalidates the list
+  } else {
+    drop_graphs(h);          // captured launches hold the cell and the PME transforms by value
+    h.list_valid = false;    // the next evaluation rebuilds the list
+  }
+  CK(cudaGetLastError());
+  return FFXG_OK;
+}
+
+// New parameter values for the same atoms and topology (OpenMMEnergy.updateParameters,
+// OpenMMEnergy.java:623-631, over ForceFieldEnergy's parameter arrays): local multipoles,
+// polarizabilities, Thole and damping, hydrogen reduction factors and the vdW pair tables.
+// Uploaded in place: no allocation and no new capture while the sizes stay the same.
+int ffxg_update_parameters(ffxg_handle *hh, const ffxg_system *s) {
+  if (!hh || !s) return FFXG_ERR_BAD_ARG;
+  Handle &h = hh->h;
+  const int n = h.n;
+  if (s->n_atoms != n || s->n_vdw_types != h.ntypes) {
+    h.err = "update_parameters: the atom and vdW type counts must not change";
+    return FFXG_ERR_BAD_ARG;
+  }
+  if (!s->multipole || !s->polarizability || !s->thole || !s->pdamp || !s->red_factor || !s->vdw_inv_rmin ||
+      !s->vdw_eps) {
+    h.err = "update_parameters: null parameter array";
+    return FFXG_ERR_BAD_ARG;
+  }
+  for (int i = 0; i < n; i++) {
+    const double *m = s->multipole + 10 * (size_t)i;
+    bool ok = std::isfinite(s->polarizability[i]) && s->polarizability[i] >= 0.0 && std::isfinite(s->thole[i]) &&
+              std::isfinite(s->pdamp[i]) && std::isfinite(s->red_factor[i]);
+    for (int t = 0; t < 10; t++) ok = ok && std::isfinite(m[t]);
+    if (!ok) { h.err = "update_parameters: non-finite or negative parameter"; return FFXG_ERR_BAD_ARG; }
+  }
+  CK(cudaStreamSynchronize(h.stream));
+  const size_t N = n;
+  SystemCopy &c = h.sys;
+  c.multipole.assign(s->multipole, s->multipole + 10 * N);
+  c.polarizability.assign(s->polarizability, s->polarizability + N);
+  c.thole.assign(s->thole, s->thole + N);
+  c.pdamp.assign(s->pdamp, s->pdamp + N);
+  c.red_factor.assign(s->red_factor, s->red_factor + N);
+  const size_t t2 = (size_t)h.ntypes * h.ntypes;
+  c.vdw_inv_rmin.assign(s->vdw_inv_rmin, s->vdw_inv_rmin + t2);
+  c.vdw_eps.assign(s->vdw_eps, s->vdw_eps + t2);
+  std::vector<double> lmp(10 * N), ipd(N);
+  for (size_t i = 0; i < N; i++) {
+    for (int t = 0; t < 10; t++) lmp[t * N + i] = s->multipole[10 * i + t];
+    ipd[i] = (s->pdamp[i] > 0.0) ? 1.0 / s->pdamp[i] : INFINITY;   // ParticleMeshEwald.java:1401-1406
+  }
+  // With electrostatic lambda on, d_polar_all holds the full set and d_polar_env the set
+  // without the soft atoms.
+  double *d_pol = h.d_polar_all ? h.d_polar_all : h.d_polar;
+  CK(cudaMemcpy(h.d_lmp, lmp.data(), 10 * N * sizeof(double), cudaMemcpyHostToDevice));
+  CK(cudaMemcpy(d_pol, s->polarizability, N * sizeof(double), cudaMemcpyHostToDevice));
+  CK(cudaMemcpy(h.d_thole, s->thole, N * sizeof(double), cudaMemcpyHostToDevice));
+  CK(cudaMemcpy(h.d_ipdamp, ipd.data(), N * sizeof(double), cudaMemcpyHostToDevice));
+  CK(cudaMemcpy(h.d_redf, s->red_factor, N * sizeof(double), cudaMemcpyHostToDevice));
+  CK(cudaMemcpy(h.d_vrad, s->vdw_inv_rmin, t2 * sizeof(double), cudaMemcpyHostToDevice));
+  CK(cudaMemcpy(h.d_veps, s->vdw_eps, t2 * sizeof(double), cudaMemcpyHostToDevice));
+  double q = 0.0;
+  for (size_t i = 0; i < N; i++) q += s->multipole[10 * i];
+  h.e_charge_correction = charge_correction(h, q);
+  if (h.elec.on && h.alch.active) {
+    // The soft-free polarizabilities, the soft-free charge correction and the vacuum
+    // sub-system follow the new values.
+    if (int st = setup_elec(h, h.soft_host, h.mol_host)) return st;
+  }
+  return FFXG_OK;
+}
+
 int ffxg_energy(ffxg_handle *hh, int want_grad, double *terms, double *grad, int64_t *counts) {
   if (!hh) return FFXG_ERR_BAD_ARG;
   Handle &h = hh->h;
   h.grad_to_pin = want_grad && grad;
   h.grad_pinned = false;
+  h.growths = 0;
   const int st = evaluate(h, h.d_xyz_in, h.d_grad_out, want_grad != 0, terms, counts);
   h.grad_to_pin = false;
-  if (st != FFXG_OK) return st;
+  if (st != FFXG_OK && st != FFXG_ERR_RANGE) return st;   // RANGE: every output is complete
   if (want_grad && grad) {
     if (!h.grad_pinned) {   // paths that synchronise more than once copy afterwards
       CK(cudaMemcpyAsync(h.h_grad_pin, h.d_grad_out, 3 * (size_t)h.n * sizeof(double), cudaMemcpyDeviceToHost,
@@ -1077,7 +1247,7 @@ int ffxg_energy(ffxg_handle *hh, int want_grad, double *terms, double *grad, int
     }
     std::memcpy(grad, h.h_grad_pin, 3 * (size_t)h.n * sizeof(double));
   }
-  return FFXG_OK;
+  return st;
 }
 
 int ffxg_energy_and_gradient(ffxg_handle *hh, const double *xyz, double *terms, double *grad, int64_t *counts) {
@@ -1088,6 +1258,7 @@ int ffxg_energy_and_gradient(ffxg_handle *hh, const double *xyz, double *terms, 
 int ffxg_energy_device(ffxg_handle *hh, const double *d_xyz, double *d_grad, double *terms, int64_t *counts) {
   if (!hh || !d_xyz) return FFXG_ERR_BAD_ARG;
   Handle &h = hh->h;
+  h.growths = 0;
   return evaluate(h, d_xyz, d_grad ? d_grad : h.d_grad_out, d_grad != nullptr, terms, counts);
 }
 
@@ -1103,6 +1274,18 @@ int ffxg_get_induced_dipoles(ffxg_handle *hh, double *u, double *u_cr) {
       if (u) u[3 * i + d] = a[d * N + i];
       if (u_cr) u_cr[3 * i + d] = b[d * N + i];
     }
+  return FFXG_OK;
+}
+
+int ffxg_get_permanent_potential(ffxg_handle *hh, double *phi) {
+  if (!hh || !phi) return FFXG_ERR_BAD_ARG;
+  Handle &h = hh->h;
+  if (!h.list_valid) { h.err = "no evaluation yet: call ffxg_energy first"; return FFXG_ERR_BAD_ARG; }
+  const size_t N = h.n;
+  std::vector<double> a(20 * N);
+  CK(cudaMemcpy(a.data(), h.d_cphi, 20 * N * sizeof(double), cudaMemcpyDeviceToHost));
+  for (size_t i = 0; i < N; i++)
+    for (int t = 0; t < 20; t++) phi[20 * i + t] = a[t * N + i];
   return FFXG_OK;
 }
 
@@ -1350,9 +1533,7 @@ static int setup_elec(Handle &h, const std::vector<int> &soft, const std::vector
   }
   CK(cudaMemcpy(h.d_polar_env, pe.data(), N * sizeof(double), cudaMemcpyHostToDevice));
   // ReciprocalEnergyRegion.java:228-238 for the atoms in use.
-  h.e_corr_env = 0.0;
-  if (q != 0.0) h.e_corr_env = -0.5 * h.prm.electric * 3.14159265358979323846 * q * q /
-                               (h.box.volume * h.prm.ewald_alpha * h.prm.ewald_alpha);
+  h.e_corr_env = charge_correction(h, q);
   return build_vacuum(h, soft, mol);
 }
 
@@ -1393,6 +1574,8 @@ int ffxg_set_alchemy(ffxg_handle *hh, const ffxg_alchemy *a) {
     soft[i] = a->soft[i] != 0;
     mol[i] = a->molecule ? a->molecule[i] : (int)i;
   }
+  h.soft_host = soft;
+  h.mol_host = mol;
   CK(cudaMemcpy(h.d_soft, soft.data(), N * sizeof(int), cudaMemcpyHostToDevice));
   CK(cudaMemcpy(h.d_mol, mol.data(), N * sizeof(int), cudaMemcpyHostToDevice));
   h.alch_alpha = a->vdw_lambda_alpha;
@@ -1465,6 +1648,7 @@ int ffxg_set_scf_predictor(ffxg_handle *hh, int predictor) {
 }
 
 static int md_force(Handle &h, const double *d_xyz, double *d_grad, double *terms) {
+  h.growths = 0;
   return evaluate(h, d_xyz, d_grad, true, terms, nullptr);
 }
 

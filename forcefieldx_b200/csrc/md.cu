@@ -238,9 +238,16 @@ int md_run(Handle &h, double dt, int steps, double *xyz, double *vel, double *ep
   cudaMemcpyAsync(h.d_mdx, xyz, N3 * sizeof(double), cudaMemcpyHostToDevice, h.stream);
   cudaMemcpyAsync(h.d_mdv, vel, N3 * sizeof(double), cudaMemcpyHostToDevice, h.stream);
   double terms[FFXG_N_TERMS];
+  // FFXG_ERR_RANGE (the mixed form's fixed-point sums out of their exact range) leaves
+  // complete forces: the run goes on and reports it at the end.
+  bool range = false;
+  auto fatal = [&](int st) {
+    if (st == FFXG_ERR_RANGE) { range = true; return false; }
+    return st != FFXG_OK;
+  };
   // Accelerations of the starting configuration.
   int st = force(h, h.d_mdx, h.d_mdg, terms);
-  if (st != FFXG_OK) return st;
+  if (fatal(st)) return st;
   k_md_accel<<<nb, 256, 0, h.stream>>>(n, h.d_mass, h.d_mdg, h.d_mda);
   for (int s = 0; s < steps; s++) {
     k_md_pre<<<nb, 256, 0, h.stream>>>(n, dt, h.d_mass, h.d_mdx, h.d_mdv, h.d_mda, h.d_mdxp);
@@ -250,7 +257,7 @@ int md_run(Handle &h, double dt, int steps, double *xyz, double *vel, double *ep
       k_md_velocity_from_step<<<nb, 256, 0, h.stream>>>(n, dt, h.d_mass, h.d_mdx, h.d_mdxp, h.d_mdv);
     }
     st = force(h, h.d_mdx, h.d_mdg, terms);
-    if (st != FFXG_OK) return st;
+    if (fatal(st)) return st;
     k_md_post<<<nb, 256, 0, h.stream>>>(n, dt, h.d_mass, h.d_mdg, h.d_mdv, h.d_mda);
     if (h.n_settle > 0)
       k_settle_velocities<<<nw, 128, 0, h.stream>>>(h.n_settle, h.d_settle, h.d_mass, h.d_mdx, h.d_mdv);
@@ -267,7 +274,7 @@ int md_run(Handle &h, double dt, int steps, double *xyz, double *vel, double *ep
   if (cudaStreamSynchronize(h.stream) != cudaSuccess) return FFXG_ERR_CUDA;
   std::memcpy(xyz, h.h_xyz_pin, N3 * sizeof(double));
   std::memcpy(vel, h.h_grad_pin, N3 * sizeof(double));
-  return FFXG_OK;
+  return range ? FFXG_ERR_RANGE : FFXG_OK;
 }
 
 }  // namespace ffx

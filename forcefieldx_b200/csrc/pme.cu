@@ -14,6 +14,8 @@
 #include <atomic>
 #include <cmath>
 #include <cstring>
+#include <map>
+#include <mutex>
 
 #include <cooperative_groups.h>
 
@@ -215,17 +217,21 @@ __device__ __forceinline__ int jmod(int a, int m) {
 __device__ __forceinline__ double mesh_quantize(float v) {
   return rint((double)v * 4294967296.0) * 2.3283064365386962890625e-10;
 }
-__device__ __forceinline__ void mesh_add(double2 *grid, size_t, size_t idx, double re) {
+// A mixed-form contribution of kQuantLimit or more raises FLAG_QUANT_RANGE (the first FFT
+// pass checks the accumulated values as it reads them).
+__device__ __forceinline__ void mesh_add(double2 *grid, size_t, size_t idx, double re, int *) {
   atomicAdd(&grid[idx].x, re);
 }
-__device__ __forceinline__ void mesh_add(double2 *grid, size_t, size_t idx, float re) {
+__device__ __forceinline__ void mesh_add(double2 *grid, size_t, size_t idx, float re, int *flags) {
+  if (quant_out(re)) atomicOr(flags, FLAG_QUANT_RANGE);
   atomicAdd(reinterpret_cast<double *>(grid) + idx, mesh_quantize(re));
 }
-__device__ __forceinline__ void mesh_add(double2 *grid, size_t, size_t idx, double re, double im) {
+__device__ __forceinline__ void mesh_add(double2 *grid, size_t, size_t idx, double re, double im, int *) {
   atomicAdd(&grid[idx].x, re);
   atomicAdd(&grid[idx].y, im);
 }
-__device__ __forceinline__ void mesh_add(double2 *grid, size_t ng, size_t idx, float re, float im) {
+__device__ __forceinline__ void mesh_add(double2 *grid, size_t ng, size_t idx, float re, float im, int *flags) {
+  if (quant_out(re) || quant_out(im)) atomicOr(flags, FLAG_QUANT_RANGE);
   double *plane = reinterpret_cast<double *>(grid);
   atomicAdd(plane + idx, mesh_quantize(re));
   atomicAdd(plane + ng + idx, mesh_quantize(im));
@@ -239,7 +245,8 @@ __device__ __forceinline__ int wrap1(int v, int m) { return v < 0 ? v + m : (v >
 // the atomic add (no integer division in the loop).
 template <typename S>
 __global__ void k_spread_permanent(int n, const double *__restrict__ fm, const S *__restrict__ spl,
-                                   const int *__restrict__ igrid, int nfx, int nfy, int nfz, double2 *grid) {
+                                   const int *__restrict__ igrid, int nfx, int nfy, int nfz, double2 *grid,
+                                   int *flags) {
   const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const int lane = threadIdx.x & 31;
   if (warp >= n || lane >= 25) return;
@@ -267,14 +274,14 @@ __global__ void k_spread_permanent(int n, const double *__restrict__ fm, const S
     const S term2 = f[t200] * v0 * u0;
     const S val = fma(x0, term0, fma(x1, term1, x2 * term2));
     const int kk = wrap1(k0 + a3, nfz);
-    mesh_add(grid, ng, (size_t)kk * nfy * nfx + row, val);
+    mesh_add(grid, ng, (size_t)kk * nfy * nfx + row, val, flags);
   }
 }
 
 template <typename S>
 __global__ void k_spread_induced(int n, const double *__restrict__ ud, const double *__restrict__ up,
                                  const S *__restrict__ spl, const int *__restrict__ igrid, int nfx, int nfy,
-                                 int nfz, double2 *grid, PmeConst pc) {
+                                 int nfz, double2 *grid, PmeConst pc, int *flags) {
   const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const int lane = threadIdx.x & 31;
   if (warp >= n || lane >= 25) return;
@@ -305,7 +312,7 @@ __global__ void k_spread_induced(int n, const double *__restrict__ ud, const dou
     const S re = fma(v0, Ad, v1 * Bd);
     const S im = fma(v0, Ap, v1 * Bp);
     const int kk = wrap1(k0 + a3, nfz);
-    mesh_add(grid, ng, (size_t)kk * nfy * nfx + row, re, im);
+    mesh_add(grid, ng, (size_t)kk * nfy * nfx + row, re, im, flags);
   }
 }
 
@@ -394,7 +401,7 @@ template <bool FUSE_G, typename S, bool FROMD>
 __global__ void __launch_bounds__(256) k_fft_axis(typename Vec2<S>::type *grid, FftAxis ax, int sign,
                                                   const typename Vec2<S>::type *__restrict__ tw,
                                                   const S *__restrict__ G, int gnx, int gny,
-                                                  double *src, size_t src_ng) {
+                                                  double *src, size_t src_ng, int *flags) {
   using V2 = typename Vec2<S>::type;
   // Shared layout is element-major, line-minor: buf[j * L + l].  Consecutive threads
   // take consecutive lines, so butterflies are bank-conflict free and the Y and Z
@@ -411,6 +418,7 @@ __global__ void __launch_bounds__(256) k_fft_axis(typename Vec2<S>::type *grid, 
     const size_t g = base + (size_t)l * ax.line_step + (size_t)j * ax.stride;
     if (FROMD) {
       const double2 q = make_double2(src[g], src[src_ng + g]);
+      if (quant_out(q.x) || quant_out(q.y)) atomicOr(flags, FLAG_QUANT_RANGE);
       src[g] = 0.0;
       src[src_ng + g] = 0.0;
       buf0[j * L + l] = mk2<S>((S)q.x, (S)q.y);
@@ -504,7 +512,7 @@ __device__ __forceinline__ void fixed_stages(typename Vec2<S>::type *&in, typena
 // the read so that the next spread starts from zero.
 template <bool INVERSE, bool FROMD>
 __global__ void __cluster_dims__(4, 1, 1) __launch_bounds__(256)
-    k_fft_plane64(float2 *grid, int sign, const float2 *__restrict__ twg, double *src, size_t src_ng) {
+    k_fft_plane64(float2 *grid, int sign, const float2 *__restrict__ twg, double *src, size_t src_ng, int *flags) {
   constexpr int LEN = 64, L = 16, LS = L + 1, NP = LEN * L, NB = LEN * LS, PER = NP / 256;
   __shared__ float2 buf[3][NB];
   __shared__ float2 tw[LEN];
@@ -531,7 +539,13 @@ __global__ void __cluster_dims__(4, 1, 1) __launch_bounds__(256)
         g[u] = plane + (size_t)j * LEN + 16 * c + l;
       }
       at[u] = j * LS + l;
-      v[u] = FROMD ? make_float2((float)src[g[u]], (float)src[src_ng + g[u]]) : grid[g[u]];
+      if (FROMD) {
+        const double re = src[g[u]], im = src[src_ng + g[u]];
+        if (quant_out(re) || quant_out(im)) atomicOr(flags, FLAG_QUANT_RANGE);
+        v[u] = make_float2((float)re, (float)im);
+      } else {
+        v[u] = grid[g[u]];
+      }
     }
 #pragma unroll
     for (int u = 0; u < PER; u++) {
@@ -590,7 +604,7 @@ template <int LEN, int L, bool FUSE_G, typename S, bool FROMD>
 __global__ void __launch_bounds__(256) k_fft_fixed(typename Vec2<S>::type *grid, FftAxis ax, int sign,
                                                    const typename Vec2<S>::type *__restrict__ twg,
                                                    const S *__restrict__ G, int gnx, int gny,
-                                                   double *src, size_t src_ng) {
+                                                   double *src, size_t src_ng, int *flags) {
   using V2 = typename Vec2<S>::type;
   __shared__ V2 buf[2][LEN * L];
   __shared__ V2 tw[LEN];
@@ -603,6 +617,7 @@ __global__ void __launch_bounds__(256) k_fft_fixed(typename Vec2<S>::type *grid,
     const size_t g = base + (size_t)l * ax.line_step + (size_t)j * ax.stride;
     if (FROMD) {
       const double2 q = make_double2(src[g], src[src_ng + g]);
+      if (quant_out(q.x) || quant_out(q.y)) atomicOr(flags, FLAG_QUANT_RANGE);
       src[g] = 0.0;
       src[src_ng + g] = 0.0;
       buf[0][j * L + l] = mk2<S>((S)q.x, (S)q.y);
@@ -820,7 +835,35 @@ static FftAxis make_axis(int axis, const int nf[3]) {
 }
 
 
-void setup_pme(Handle &h) {
+// The dynamic shared-memory limit of the generic FFT kernels is an attribute of each kernel
+// on a device, shared by every handle in the process.  It only ever grows: a handle raises
+// it to the largest line batch of its three axes, so a handle created later (with smaller
+// axes, or its largest axis in another position) never lowers a limit on which an earlier
+// handle's launches rely.
+static std::mutex g_fft_smem_mu;
+static std::map<int, int> g_fft_smem;   // device -> current attribute value (bytes)
+
+static cudaError_t raise_fft_smem(int device, int need) {
+  std::lock_guard<std::mutex> lock(g_fft_smem_mu);
+  int &cur = g_fft_smem[device];
+  if (need <= cur) return cudaSuccess;
+  const cudaError_t e[5] = {
+      cudaFuncSetAttribute(k_fft_axis<false, double, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, need),
+      cudaFuncSetAttribute(k_fft_axis<true, double, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, need),
+      cudaFuncSetAttribute(k_fft_axis<false, float, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, need),
+      cudaFuncSetAttribute(k_fft_axis<false, float, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, need),
+      cudaFuncSetAttribute(k_fft_axis<true, float, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, need)};
+  for (cudaError_t q : e)
+    if (q != cudaSuccess) return q;
+  cur = need;
+  return cudaSuccess;
+}
+
+// Dynamic shared memory of one generic FFT pass over axis a (both sizes of the mesh type
+// fit in the FP64 figure).
+static size_t fft_axis_smem(const FftAxis &a) { return 2 * (size_t)a.len * a.L * sizeof(double2); }
+
+int setup_pme(Handle &h) {
   const int nfx = h.prm.pme_grid[0], nfy = h.prm.pme_grid[1], nfz = h.prm.pme_grid[2];
   h.nfft[0] = nfx; h.nfft[1] = nfy; h.nfft[2] = nfz;
   const int nf[3] = {nfx, nfy, nfz};
@@ -918,14 +961,18 @@ void setup_pme(Handle &h) {
     cudaMemcpy(h.d_twiddlef, twf.data(), twf.size() * sizeof(float2), cudaMemcpyHostToDevice);
   }
   for (int d = 0; d < 3; d++) h.axes[d] = make_axis(d, nf);
-  for (int d = 0; d < 3; d++) {
-    const int smem = (int)std::max<size_t>(2 * (size_t)h.axes[d].len * h.axes[d].L * sizeof(double2), 48 * 1024);
-    cudaFuncSetAttribute(k_fft_axis<false, double, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
-    cudaFuncSetAttribute(k_fft_axis<true, double, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
-    cudaFuncSetAttribute(k_fft_axis<false, float, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
-    cudaFuncSetAttribute(k_fft_axis<false, float, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
-    cudaFuncSetAttribute(k_fft_axis<true, float, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+  size_t smem = 48 * 1024;
+  for (int d = 0; d < 3; d++) smem = std::max(smem, fft_axis_smem(h.axes[d]));
+  if (smem > 227 * 1024) {
+    h.err = "PME grid dimension too long for the shared-memory FFT";
+    return FFXG_ERR_BAD_ARG;
   }
+  const cudaError_t e = raise_fft_smem(h.device, (int)smem);
+  if (e != cudaSuccess) {
+    h.err = std::string("FFT shared-memory attribute: ") + cudaGetErrorString(e);
+    return FFXG_ERR_CUDA;
+  }
+  return FFXG_OK;
 }
 
 // ---------------------------------------------------------------------------
@@ -957,10 +1004,11 @@ void launch_spread_permanent(Handle &h) {
   if (!h.mixed) cudaMemsetAsync(h.d_grid, 0, grid_points(h) * sizeof(double2), h.stream);
   if (h.mixed)
     k_spread_permanent<float><<<nb, 256, 0, h.stream>>>(h.n, h.d_fm, reinterpret_cast<const float *>(h.d_spl),
-                                                        h.d_igrid, h.nfft[0], h.nfft[1], h.nfft[2], h.d_grid);
+                                                        h.d_igrid, h.nfft[0], h.nfft[1], h.nfft[2], h.d_grid,
+                                                        h.d_flags);
   else
     k_spread_permanent<double><<<nb, 256, 0, h.stream>>>(h.n, h.d_fm, h.d_spl, h.d_igrid, h.nfft[0], h.nfft[1],
-                                                         h.nfft[2], h.d_grid);
+                                                         h.nfft[2], h.d_grid, h.d_flags);
   FFX_LAUNCHED(h);
 }
 
@@ -970,10 +1018,10 @@ void launch_spread_induced(Handle &h, const double *ud, const double *up) {
   if (!h.mixed) cudaMemsetAsync(h.d_grid, 0, grid_points(h) * sizeof(double2), h.stream);
   if (h.mixed)
     k_spread_induced<float><<<nb, 256, 0, h.stream>>>(h.n, ud, up, reinterpret_cast<const float *>(h.d_spl), h.d_igrid,
-                                                      h.nfft[0], h.nfft[1], h.nfft[2], h.d_grid, h.pc);
+                                                      h.nfft[0], h.nfft[1], h.nfft[2], h.d_grid, h.pc, h.d_flags);
   else
     k_spread_induced<double><<<nb, 256, 0, h.stream>>>(h.n, ud, up, h.d_spl, h.d_igrid, h.nfft[0], h.nfft[1],
-                                                       h.nfft[2], h.d_grid, h.pc);
+                                                       h.nfft[2], h.d_grid, h.pc, h.d_flags);
   FFX_LAUNCHED(h);
 }
 
@@ -994,24 +1042,25 @@ static void fft_convolution(Handle &h, typename Vec2<S>::type *grid, const typen
     if (a.len == 64 && a.L == 16) {
       if (fuse)
         k_fft_fixed<64, 16, true, S, false><<<blocks, 256, 0, h.stream>>>(grid, a, sign, tw, influence, nfx, nfy,
-                                                                          nullptr, 0);
+                                                                          nullptr, 0, h.d_flags);
       else if (fromd)
         k_fft_fixed<64, 16, false, S, true><<<blocks, 256, 0, h.stream>>>(grid, a, sign, tw, nullptr, nfx, nfy,
-                                                                          plane, ng);
+                                                                          plane, ng, h.d_flags);
       else
         k_fft_fixed<64, 16, false, S, false><<<blocks, 256, 0, h.stream>>>(grid, a, sign, tw, nullptr, nfx, nfy,
-                                                                           nullptr, 0);
+                                                                           nullptr, 0, h.d_flags);
       FFX_LAUNCHED(h);
       return;
     }
     if (fuse)
       k_fft_axis<true, S, false><<<blocks, 256, smem, h.stream>>>(grid, a, sign, tw, influence, nfx, nfy, nullptr,
-                                                                  0);
+                                                                  0, h.d_flags);
     else if (fromd)
-      k_fft_axis<false, S, true><<<blocks, 256, smem, h.stream>>>(grid, a, sign, tw, nullptr, nfx, nfy, plane, ng);
+      k_fft_axis<false, S, true><<<blocks, 256, smem, h.stream>>>(grid, a, sign, tw, nullptr, nfx, nfy, plane, ng,
+                                                                  h.d_flags);
     else
       k_fft_axis<false, S, false><<<blocks, 256, smem, h.stream>>>(grid, a, sign, tw, nullptr, nfx, nfy, nullptr,
-                                                                   0);
+                                                                   0, h.d_flags);
     FFX_LAUNCHED(h);
   };
   const bool fromd = (sizeof(S) == 4);   // mixed: the first pass reads the double mesh
@@ -1019,10 +1068,10 @@ static void fft_convolution(Handle &h, typename Vec2<S>::type *grid, const typen
     // Mixed form on 64 x 64 planes: xy, z (with the influence function), yx.
     float2 *gf = reinterpret_cast<float2 *>(grid);
     const float2 *tw = reinterpret_cast<const float2 *>(twiddle);
-    k_fft_plane64<false, true><<<nfz * 4, 256, 0, h.stream>>>(gf, -1, tw, h.d_grid_planes(), ng);
+    k_fft_plane64<false, true><<<nfz * 4, 256, 0, h.stream>>>(gf, -1, tw, h.d_grid_planes(), ng, h.d_flags);
     FFX_LAUNCHED(h);
     run(2, -1, true, false);
-    k_fft_plane64<true, false><<<nfz * 4, 256, 0, h.stream>>>(gf, +1, tw, nullptr, 0);
+    k_fft_plane64<true, false><<<nfz * 4, 256, 0, h.stream>>>(gf, +1, tw, nullptr, 0, h.d_flags);
     FFX_LAUNCHED(h);
     return;
   }
@@ -1395,29 +1444,49 @@ extern "C" int ffxg_pme_recip_permanent_noalloc(const double *d_xyz, const doubl
   for (int i = 0; i < 3; i++)
     for (int j = 0; j < 3; j++) pc.recip[i][j] = A[i][j];
   const int npts = nf[0] * nf[1] * nf[2];
-  k_na_tables<<<3, kNaMaxDim, 0, st>>>(nf[0], nf[1], nf[2], s);
-  k_na_influence<<<nblocks(npts, 256), 256, 0, st>>>(nf[0], nf[1], nf[2], A[0][0], A[1][1], A[2][2], ewald_alpha,
-                                                       box[0] * box[1] * box[2], s);
-  k_na_spread<<<nblocks(n_atoms, kNaThreads / 32), kNaThreads, 0, st>>>(n_atoms, d_xyz, d_mpole, nf[0], nf[1], nf[2],
-                                                                        pc, s);
+  // Each launch reports its own error (cudaLaunchKernelEx returns it), so an error the
+  // caller left pending is neither taken for this call's nor cleared by it.
+  auto launch = [&](auto kernel, int blocks, int threads, size_t smem, auto... args) {
+    cudaLaunchConfig_t c{};
+    c.gridDim = dim3(blocks);
+    c.blockDim = dim3(threads);
+    c.dynamicSmemBytes = smem;
+    c.stream = st;
+    return cudaLaunchKernelEx(&c, kernel, args...);
+  };
+  if (launch(k_na_tables, 3, kNaMaxDim, 0, nf[0], nf[1], nf[2], s) != cudaSuccess) return FFXG_ERR_CUDA;
+  if (launch(k_na_influence, nblocks(npts, 256), 256, 0, nf[0], nf[1], nf[2], A[0][0], A[1][1], A[2][2], ewald_alpha,
+             box[0] * box[1] * box[2], s) != cudaSuccess)
+    return FFXG_ERR_CUDA;
+  if (launch(k_na_spread, nblocks(n_atoms, kNaThreads / 32), kNaThreads, 0, (int)n_atoms, d_xyz, d_mpole, nf[0], nf[1],
+             nf[2], pc, s) != cudaSuccess)
+    return FFXG_ERR_CUDA;
   double2 *grid = s->grid;
+  const double *no_influence = nullptr;
+  double *no_plane = nullptr;
+  int *no_flags = nullptr;   // only the mixed form's first pass reads it
   for (int pass = 0; pass < 5; pass++) {
     const int d = (pass < 2) ? pass : (pass == 2 ? 2 : 4 - pass);
     const int sign = (pass < 3) ? -1 : +1;
     const FftAxis ax = make_axis(d, nf);
     const int outer = (d == 2) ? nf[1] : nf[2];
-    const size_t smem = 2 * (size_t)ax.len * ax.L * sizeof(double2);
-    if (pass == 2)
-      k_fft_axis<true, double, false><<<ax.groups_inner * outer, 256, smem, st>>>(
-          grid, ax, sign, s->twiddle + d * kNaMaxDim, s->influence, nf[0], nf[1], nullptr, 0);
-    else
-      k_fft_axis<false, double, false><<<ax.groups_inner * outer, 256, smem, st>>>(
-          grid, ax, sign, s->twiddle + d * kNaMaxDim, nullptr, nf[0], nf[1], nullptr, 0);
+    const size_t smem = fft_axis_smem(ax);   // <= 32 KB at kNaMaxDim: no attribute needed
+    const cudaError_t e =
+        (pass == 2) ? launch(k_fft_axis<true, double, false>, ax.groups_inner * outer, 256, smem, grid, ax, sign,
+                             (const double2 *)(s->twiddle + d * kNaMaxDim), (const double *)s->influence, nf[0], nf[1],
+                             no_plane, (size_t)0, no_flags)
+                    : launch(k_fft_axis<false, double, false>, ax.groups_inner * outer, 256, smem, grid, ax, sign,
+                             (const double2 *)(s->twiddle + d * kNaMaxDim), no_influence, nf[0], nf[1], no_plane,
+                             (size_t)0, no_flags);
+    if (e != cudaSuccess) return FFXG_ERR_CUDA;
   }
   const int nb = nblocks(n_atoms, kNaThreads);
-  k_na_phi<<<nb, kNaThreads, 0, st>>>(n_atoms, d_xyz, d_mpole, nf[0], nf[1], nf[2], pc, d_phi, s);
-  k_na_energy<<<1, 32, 0, st>>>(nb, electric, s, d_energy);
-  return cudaGetLastError() == cudaSuccess ? FFXG_OK : FFXG_ERR_CUDA;
+  if (launch(k_na_phi, nb, kNaThreads, 0, (int)n_atoms, d_xyz, d_mpole, nf[0], nf[1], nf[2], pc, d_phi, s) !=
+      cudaSuccess)
+    return FFXG_ERR_CUDA;
+  if (launch(k_na_energy, 1, 32, 0, nb, electric, (const NoAllocScratch *)s, d_energy) != cudaSuccess)
+    return FFXG_ERR_CUDA;
+  return FFXG_OK;
 }
 
 }  // namespace ffx

@@ -253,9 +253,12 @@ __global__ void k_direct_dipoles(int n, const double *__restrict__ gm, const dou
 // Adds (vx, vy, vz) to row-major [3][n] v at atom k.  FP64 form: FP64 atomics.  FP32 form:
 // each value is rounded to a multiple of 2^-32 first, so the sums are exact in FP64 (below
 // 2^21 in magnitude) and independent of the order of the atomics.
+// A contribution of kQuantLimit or more raises FLAG_QUANT_RANGE (the accumulated values are
+// checked where the gradient is assembled).
 template <typename R>
-__device__ __forceinline__ void real_acc(double *v, int k, double vx, double vy, double vz, int n) {
+__device__ __forceinline__ void real_acc(double *v, int k, double vx, double vy, double vz, int n, int *flags) {
   if constexpr (sizeof(R) == 4) {
+    if (quant_out(vx) || quant_out(vy) || quant_out(vz)) atomicOr(flags, FLAG_QUANT_RANGE);
     vx = rint(vx * 4294967296.0) * 2.3283064365386962890625e-10;
     vy = rint(vy * 4294967296.0) * 2.3283064365386962890625e-10;
     vz = rint(vz * 4294967296.0) * 2.3283064365386962890625e-10;
@@ -274,7 +277,7 @@ __global__ void __launch_bounds__(128, sizeof(R) == 4 ? FFX_REAL_ENERGY_MIN_BLOC
     const int *__restrict__ ewl_cnt, int capE, const int *__restrict__ ewl_sh, Excl ex, EwaldCoef ec, const __grid_constant__ ScaleTables c_scales, int polarization, int gradient,
     double *eatom_perm, double *eatom_pol, long long *catom, double *grad, double *torque,
     const int *__restrict__ soft, ElecStep st, double *edl, double *ed2l, double *lgrad, double *ltorque,
-    const double2 *__restrict__ pos, const R *__restrict__ rec) {
+    const double2 *__restrict__ pos, const R *__restrict__ rec, int *flags) {
   constexpr bool HALF = !LAM && !DIRECT;   // the softcore and direct forms walk the full rows
   __shared__ int qbuf[HALF ? 4 : 1][64];
   const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
@@ -458,8 +461,8 @@ __global__ void __launch_bounds__(128, sizeof(R) == 4 ? FFX_REAL_ENERGY_MIN_BLOC
         gx += pre * ftm2x; gy += pre * ftm2y; gz += pre * ftm2z;
         tx += pre * ttm2x; ty += pre * ttm2y; tz += pre * ttm2z;
         if constexpr (HALF) {
-          real_acc<R>(grad, k, -pre * ftm2x, -pre * ftm2y, -pre * ftm2z, n);
-          real_acc<R>(torque, k, pre * ttm3x, pre * ttm3y, pre * ttm3z, n);
+          real_acc<R>(grad, k, -pre * ftm2x, -pre * ftm2y, -pre * ftm2z, n, flags);
+          real_acc<R>(torque, k, pre * ttm3x, pre * ttm3y, pre * ttm3z, n, flags);
         }
         if (LAM && spair) {   // d[dlPow * ereal]/dX (:1465-1475)
           const R pf = electric * (R)(st.dEdLSign * st.dlPowPerm);
@@ -683,8 +686,8 @@ __global__ void __launch_bounds__(128, sizeof(R) == 4 ? FFX_REAL_ENERGY_MIN_BLOC
       gx += sc * ftm2ix; gy += sc * ftm2iy; gz += sc * ftm2iz;
       tx += sc * ttm2ix; ty += sc * ttm2iy; tz += sc * ttm2iz;
       if constexpr (HALF) {
-        real_acc<R>(grad, k, -sc * ftm2ix, -sc * ftm2iy, -sc * ftm2iz, n);
-        real_acc<R>(torque, k, sc * ttm3ix, sc * ttm3iy, sc * ttm3iz, n);
+        real_acc<R>(grad, k, -sc * ftm2ix, -sc * ftm2iy, -sc * ftm2iz, n, flags);
+        real_acc<R>(torque, k, sc * ttm3ix, sc * ttm3iy, sc * ttm3iz, n, flags);
       }
       if (LAM) {   // RealSpaceEnergyRegion.java:2163-2174
         const R sl = electric * (R)(st.dEdLSign * st.dlPowPol);
@@ -738,8 +741,8 @@ __global__ void __launch_bounds__(128, sizeof(R) == 4 ? FFX_REAL_ENERGY_MIN_BLOC
     catom[i] = cnt_pairs;
     if (gr) {
       if constexpr (HALF) {
-        real_acc<R>(grad, i, Gx, Gy, Gz, n);
-        real_acc<R>(torque, i, Tx, Ty, Tz, n);
+        real_acc<R>(grad, i, Gx, Gy, Gz, n, flags);
+        real_acc<R>(torque, i, Tx, Ty, Tz, n, flags);
       } else {
         grad[i] = Gx; grad[n + i] = Gy; grad[2 * n + i] = Gz;
         torque[i] = Tx; torque[n + i] = Ty; torque[2 * n + i] = Tz;
@@ -877,7 +880,7 @@ static void real_energy(Handle &h, bool grad) {
       h.cap_ewl, h.d_ewl_sh, excl(h), ewald_coef(h, ewald_alpha_of(h)), h.scales, h.prm.polarization, grad ? 1 : 0,
       h.d_eatom + 1 * (size_t)h.n, h.d_eatom + 2 * (size_t)h.n, h.d_catom + (size_t)h.n, h.d_grad, h.d_torque,
       h.d_soft, h.step, h.d_eatom + 9 * (size_t)h.n, h.d_eatom + 10 * (size_t)h.n, h.d_lg, h.d_lt, h.d_pos,
-      reinterpret_cast<const R *>(h.d_erec));
+      reinterpret_cast<const R *>(h.d_erec), h.d_flags);
   FFX_LAUNCHED(h);
 }
 

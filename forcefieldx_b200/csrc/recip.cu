@@ -292,7 +292,7 @@ __global__ void k_torque_gather(int n, const double *__restrict__ x, const doubl
                                 const double *__restrict__ z, const int *__restrict__ frame,
                                 const int *__restrict__ axis, const double *__restrict__ torque,
                                 const int *__restrict__ tq_ptr, const int *__restrict__ tq_ent, double *gtq,
-                                int *flags) {
+                                int *flags, int quant) {
   const int j = blockIdx.x * blockDim.x + threadIdx.x;
   if (j >= n) return;
   double s0 = 0, s1 = 0, s2 = 0;
@@ -300,6 +300,9 @@ __global__ void k_torque_gather(int n, const double *__restrict__ x, const doubl
     const int ent = tq_ent[e];
     const int i = ent >> 2, slot = ent & 3;
     const double trq[3] = {torque[i], torque[n + i], torque[2 * n + i]};
+    // The mixed form's accumulated torques (fixed-point sums) must stay in their exact range.
+    if (quant && slot == 3 && (quant_out(trq[0]) || quant_out(trq[1]) || quant_out(trq[2])))
+      atomicOr(flags, FLAG_QUANT_RANGE);
     double g[3];
     torque_slot(i, slot, n, x, y, z, frame, axis, trq, g);
     s0 += g[0]; s1 += g[1]; s2 += g[2];
@@ -309,11 +312,13 @@ __global__ void k_torque_gather(int n, const double *__restrict__ x, const doubl
 }
 
 __global__ void k_assemble(int n, const double *__restrict__ grad, const double *__restrict__ gtq,
-                           const double *__restrict__ gvdw, double *out, int *flags) {
+                           const double *__restrict__ gvdw, double *out, int *flags, int quant) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
   for (int d = 0; d < 3; d++) {
-    const double v = grad[d * n + i] + gtq[d * n + i] + gvdw[d * n + i];
+    const double ge = grad[d * n + i];
+    if (quant && quant_out(ge)) atomicOr(flags, FLAG_QUANT_RANGE);   // mixed form: fixed-point sums
+    const double v = ge + gtq[d * n + i] + gvdw[d * n + i];
     if (!isfinite(v)) atomicOr(flags, FLAG_NONFINITE);
     out[3 * i + d] = v;
   }
@@ -398,13 +403,14 @@ void launch_torque(Handle &h) { launch_torque_of(h, h.d_torque, h.d_vec); }
 // Torque -> Cartesian gradient of `torque` into out[3][n] (written, not added).
 void launch_torque_of(Handle &h, const double *torque, double *out) {
   k_torque_gather<<<nblocks(h.n, 128), 128, 0, h.stream>>>(h.n, h.d_x, h.d_y, h.d_z, h.d_frame, h.d_axis, torque,
-                                                            h.d_tq_ptr, h.d_tq_ent, out, h.d_flags);
+                                                            h.d_tq_ptr, h.d_tq_ent, out, h.d_flags,
+                                                            h.mixed && torque == h.d_torque ? 1 : 0);
   FFX_LAUNCHED(h);
 }
 
 void launch_assemble(Handle &h, double *d_grad_xyz) {
   k_assemble<<<nblocks(h.n, 256), 256, 0, h.stream>>>(h.n, h.d_grad, h.d_vec, h.d_gred + 3 * (size_t)h.n, d_grad_xyz,
-                                                       h.d_flags);
+                                                       h.d_flags, h.mixed ? 1 : 0);
   FFX_LAUNCHED(h);
 }
 

@@ -9,6 +9,8 @@ this class                     reference
 energy(x)                      ForceFieldEnergy.energy(double[])            :1806-1830
 energy_and_gradient(x, g)      ForceFieldEnergy.energyAndGradient(x, g)     :1843-1890
 set_coordinates(x)             ForceFieldEnergy.setCoordinates             :2629
+set_crystal(box, grid)         ForceFieldEnergy.setCrystal                  :2650-2666
+update_parameters(system)      OpenMMEnergy.updateParameters (openmm/OpenMMEnergy.java:623)
 get_permanent_multipole_energy getPermanentMultipoleEnergy                  :2294
 get_polarization_energy        getPolarizationEnergy                        :2322
 get_vdw_energy                 getVanDerWaalsEnergy
@@ -23,6 +25,8 @@ RealSpaceEnergyRegion.java:384-391.
 from __future__ import annotations
 
 import ctypes
+import dataclasses
+import warnings
 from typing import Optional
 
 import numpy as np
@@ -78,7 +82,12 @@ class ForceFieldEnergy:
 
     # ------------------------------------------------------------------
     def _check(self, st: int):
-        if st != 0:
+        """Nonzero status -> EnergyException, except RANGE (the mixed form's fixed-point sums
+        left their exact range: outputs complete, not bitwise reproducible), which warns."""
+        self.last_status = st
+        if st == cabi.STATUS_RANGE:
+            warnings.warn(self.lib.ffxg_last_error(self._h).decode(), RuntimeWarning, stacklevel=3)
+        elif st != 0:
             raise EnergyException(st, self.lib.ffxg_last_error(self._h).decode())
 
     def close(self):
@@ -103,6 +112,21 @@ class ForceFieldEnergy:
     def set_coordinates(self, x) -> None:
         self._x = np.ascontiguousarray(np.asarray(x, dtype=np.float64).reshape(self.n, 3))
         self._check(self.lib.ffxg_set_coordinates(self._h, _dp(self._x)))
+
+    def set_crystal(self, box, pme_grid=None) -> None:
+        """New orthorhombic cell edges (and optionally PME mesh dimensions; None keeps the mesh)."""
+        b = np.ascontiguousarray(np.broadcast_to(np.asarray(box, dtype=np.float64), (3,)))
+        g = None if pme_grid is None else np.ascontiguousarray(pme_grid, dtype=np.int32)
+        self._check(self.lib.ffxg_set_box(self._h, _dp(b), g.ctypes.data_as(cabi._I) if g is not None else None))
+        grid = tuple(self.params.grid()) if g is None else tuple(int(v) for v in g)
+        self.params = dataclasses.replace(self.params, box=tuple(float(v) for v in b), pme_grid=grid)
+
+    def update_parameters(self, system: AmoebaSystem) -> None:
+        """New multipole, polarization, damping, reduction and vdW-table values for the same
+        atoms and topology (in place on the device)."""
+        s, keep = system.c_struct(cabi)
+        self._check(self.lib.ffxg_update_parameters(self._h, ctypes.byref(s)))
+        self.system = system
 
     def energy(self, x=None) -> float:
         if x is not None:
@@ -160,6 +184,13 @@ class ForceFieldEnergy:
         m = np.zeros((self.n, 10))
         self._check(self.lib.ffxg_get_global_multipoles(self._h, _dp(m)))
         return m
+
+    def get_permanent_potential(self):
+        """ParticleMeshEwald.cartesianMultipolePhi: the permanent multipoles' reciprocal-space
+        potential and its derivatives at each atom, [n, 20]."""
+        phi = np.zeros((self.n, 20))
+        self._check(self.lib.ffxg_get_permanent_potential(self._h, _dp(phi)))
+        return phi
 
     def neighbor_pairs(self) -> np.ndarray:
         cnt = ctypes.c_int64(0)

@@ -33,7 +33,7 @@ PRECISION_FP64, PRECISION_MIXED = range(2)
 
 TERM_NAMES = ["vdw", "permanent", "polarization", "perm_real", "perm_self", "perm_recip",
               "pol_real", "pol_self", "pol_recip", "total"]
-COUNT_NAMES = ["vdw", "permanent", "scf_iter", "list_builds", "list_pairs"]
+COUNT_NAMES = ["vdw", "permanent", "scf_iter", "list_builds", "list_pairs", "list_growths"]
 
 
 def csr_from_lists(lists: Sequence[Sequence[int]]):

@@ -41,7 +41,11 @@ typedef enum {
   FFXG_ERR_SCF_DIVERGED = 3,  /* PCG residual grew (PCGSolver.java:547-559) */
   FFXG_ERR_SCF_MAXITER = 4,   /* PCG hit the iteration cap (PCGSolver.java:563-568) */
   FFXG_ERR_NONFINITE = 5,     /* NaN/Inf energy, torque or gradient */
-  FFXG_ERR_CAPACITY = 6       /* neighbour capacity exceeded even after regrowth */
+  FFXG_ERR_CAPACITY = 6,      /* neighbour capacity exceeded even after regrowth */
+  FFXG_ERR_RANGE = 7          /* mixed form only: a fixed-point (2^-32) force, torque or mesh
+                                 sum reached 2^20 in magnitude.  Every output is written and
+                                 accurate to FP64 rounding, but no longer guaranteed to repeat
+                                 bit for bit; callers may treat it as a warning. */
 } ffxg_status;
 
 /* Local multipole frame definitions (MultipoleType.MultipoleFrameDefinition). */
@@ -86,8 +90,13 @@ enum {
   FFXG_COUNT_PERMANENT = 1,    /* ParticleMeshEwald.getInteractions (ParticleMeshEwald.java:1014) */
   FFXG_COUNT_SCF_ITER = 2,     /* completed PCG cycles (PCGSolver.scfByPCG return value) */
   FFXG_COUNT_LIST_BUILDS = 3,  /* neighbour-list rebuilds performed during this call */
-  FFXG_COUNT_LIST_PAIRS = 4,   /* unordered pairs in the buffered neighbour list */
-  FFXG_N_COUNTS = 5
+  FFXG_COUNT_LIST_PAIRS = 4,   /* unordered pairs in the buffered neighbour list (the CPU
+                                  oracle fills it; the library writes -1 and returns the pair
+                                  set through ffxg_get_neighbor_pairs) */
+  FFXG_COUNT_LIST_GROWTHS = 5, /* list capacity regrowths during this call: a row overflowed
+                                  its capacity, the rows grew by half and the evaluation was
+                                  repeated (the result is that of the repeat) */
+  FFXG_N_COUNTS = 6
 };
 
 /* Resolved per-atom topology and parameters.  This is exactly the data that
@@ -157,6 +166,26 @@ const char *ffxg_last_error(const ffxg_handle *h);
  * (ForceFieldEnergy.java:2629). */
 int ffxg_set_coordinates(ffxg_handle *h, const double *xyz);
 
+/* New orthorhombic cell edges box[3] (A), and, when pme_grid is not NULL, new PME mesh
+ * dimensions (NULL keeps the mesh, as a pme-grid key does in the reference):
+ * ForceFieldEnergy.setCrystal (ForceFieldEnergy.java:2650-2666), which passes the crystal to
+ * ParticleMeshEwald.setCrystal (ParticleMeshEwald.java:1262-1283) and
+ * ReciprocalSpace.setCrystal / initConvolution (ReciprocalSpace.java:750-761, 909-1000); the
+ * FFM binding's override is OpenMMEnergy.setCrystal's counterpart (OpenMMEnergy.java:585).
+ * Rebuilds the PME tables and the charge correction; the next evaluation rebuilds the
+ * neighbour list and captures its graph anew.  A barostat or lattice move needs no new
+ * handle. */
+int ffxg_set_box(ffxg_handle *h, const double box[3], const int32_t pme_grid[3]);
+
+/* New parameter values for the same atoms, topology and vdW types: sys->multipole,
+ * polarizability, thole, pdamp, red_factor, vdw_inv_rmin and vdw_eps are read (the other
+ * fields are ignored; n_atoms and n_vdw_types must equal the handle's).  The counterpart
+ * of OpenMMEnergy.updateParameters (OpenMMEnergy.java:623-631) for this library: a
+ * parameter-fitting loop (ffxg_param_grad) updates values in place, with no allocation
+ * and no new graph capture (with electrostatic lambda on, the soft atoms' vacuum
+ * sub-system is rebuilt). */
+int ffxg_update_parameters(ffxg_handle *h, const ffxg_system *sys);
+
 /* Energy (and optionally gradient) at the current coordinates.
  * ForceFieldEnergy.energy(gradient, print) (ForceFieldEnergy.java:1638-1800) for the
  * vdW + PME terms.  terms[FFXG_N_TERMS] (kcal/mol), grad[n][3] (kcal/mol/A, may be
@@ -181,6 +210,14 @@ int ffxg_get_induced_dipoles(ffxg_handle *h, double *u, double *u_cr);
 
 /* Global-frame multipoles from the last energy call ([n][10]). */
 int ffxg_get_global_multipoles(ffxg_handle *h, double *mpole);
+
+/* Cartesian reciprocal-space potential of the permanent multipoles and its first to third
+ * derivatives from the last energy call, [n][20] in the tensor order t000, t100, t010,
+ * t001, t200, t020, t002, t110, t101, t011, t300, t030, t003, t210, t201, t120, t021,
+ * t102, t012, t111: ParticleMeshEwald.cartesianMultipolePhi (ParticleMeshEwald.java:438),
+ * filled by ReciprocalSpace.computePermanentPhi (PermanentPhiLoop, ReciprocalSpace.java:
+ * 2295-2454). */
+int ffxg_get_permanent_potential(ffxg_handle *h, double *phi);
 
 /* Pair set of the buffered neighbour list (NeighborList.java:905-1115) as
  * unordered (i, k) with i < k.  With pairs == NULL only *n_pairs is written. */

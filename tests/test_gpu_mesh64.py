@@ -32,6 +32,21 @@ def test_fp64_mesh64_against_oracle():
     compare(s, water_params(EDGE, pme_grid=(64, 64, 64)), check_pairs=False)
 
 
+def test_fp64_repeat_agrees_to_rounding():
+    """The FP64 form adds the mesh and the real-space k-side force and torque with FP64
+    atomics in arrival order, so repeated calls agree to rounding, not bit for bit (the
+    mixed form's quantised sums do repeat exactly)."""
+    from forcefieldx_b200.energy import ForceFieldEnergy
+    s = _box(45)
+    with ForceFieldEnergy(s, water_params(EDGE, pme_grid=(64, 64, 64))) as ffe:
+        e1, g1 = ffe.energy_and_gradient(s.xyz)
+        t1 = ffe.terms.copy()
+        e2, g2 = ffe.energy_and_gradient(s.xyz)
+        t2 = ffe.terms.copy()
+    assert np.max(np.abs(t1 - t2) / np.maximum(np.abs(t1), 1.0)) < 1e-12
+    assert np.max(np.abs(g1 - g2)) < 1e-9
+
+
 def test_mixed_mesh64_against_oracle_and_repeatable():
     s = _box(43)
     compare_mixed(s, water_params(EDGE, pme_grid=(64, 64, 64), precision=PRECISION_MIXED))

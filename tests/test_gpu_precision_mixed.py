@@ -27,6 +27,7 @@ def compare_mixed(system, params, xyz=None):
     assert ref["status"] == 0
     with ForceFieldEnergy(system, params) as ffe:
         e, g = ffe.energy_and_gradient(x)
+        assert ffe.last_status == 0                  # no fixed-point sum left its exact range
         terms, counts = ffe.terms.copy(), ffe.counts.copy()
         u, _ = ffe.get_induced_dipoles()
         e2, g2 = ffe.energy_and_gradient(x)
