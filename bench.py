@@ -104,25 +104,31 @@ class ClockSampler:
 
 
 # ---------------------------------------------------------------------------
-# DRAM bytes (read + write) of one k_pair_field<float> launch on this workload, from an ncu
-# capture with caches flushed before the launch (profiles/pcg_kernels_water24k_mixed.md).
-PAIR_FIELD_TRAFFIC = 90.9e6
+# Algorithmic work of one launch of a stage's dominant kernel, frozen in BASELINE.md: the
+# compulsory HBM bytes of a pass (every per-atom input read once, every output written
+# once; neighbour lists are derived data and not counted) and the FLOPs of the pair
+# arithmetic, per undirected pair.
+BYTES_PER_ATOM = {"ind_field": 150.0, "precond": 150.0, "real_energy": 240.0, "vdw": 80.0}
+FLOPS_PER_PAIR = {"ind_field": 110.0, "precond": 110.0, "real_energy": 900.0, "vdw": 70.0}
 
 
-def algorithmic_traffic(stage: str, n: int, pairs_half: int, vdw_list_full: int, mixed: bool) -> float:
-    """Compulsory HBM bytes of one launch of a stage's dominant kernel: every input read
-    once, every output written once."""
-    full = 2 * pairs_half
-    if stage == "ind_field":      # k_pair_field: per directed pair index 4 B + displacement and A
-        # (16 B mixed, 32 B FP64) + B (4 B / 8 B); per atom one source record (32 B / 64 B) and
-        # the six-component output (48 B)
-        per_pair = 24.0 if mixed else 44.0
-        return per_pair * full + n * ((32 if mixed else 64) + 48)
-    if stage == "real_energy":    # list + x,y,z,gm(10),u,p,ipdamp,thole in; e(2),count,grad,torque out
-        return 4.0 * full + n * (4 + 8 * (3 + 10 + 6 + 2) + 8 * 2 + 8 + 8 * 6)
-    if stage == "vdw":
-        return 4.0 * vdw_list_full + n * (4 + 8 * 3 + 4 + 8 + 8 + 8 * 3)
-    return float("nan")
+def algorithmic_work(stage: str, n: int, pairs_half: int, vdw_pairs: int):
+    """(compulsory bytes, FLOPs) of one launch of the stage's dominant kernel."""
+    pairs = vdw_pairs if stage == "vdw" else pairs_half
+    return BYTES_PER_ATOM[stage] * n, FLOPS_PER_PAIR[stage] * pairs
+
+
+def fma_peak_tflops(fp64: bool):
+    """FMA-pipe throughput of this GPU measured by libffxpeak.so (best of five launches)."""
+    import ctypes
+    path = os.path.join(ROOT, "forcefieldx_b200", "libffxpeak.so")
+    lib = ctypes.CDLL(path)
+    lib.ffxpeak_fma_tflops.restype = ctypes.c_int
+    lib.ffxpeak_fma_tflops.argtypes = [ctypes.c_int, ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_double)]
+    tf = ctypes.c_double(0.0)
+    if lib.ffxpeak_fma_tflops(1 if fp64 else 0, ctypes.byref(tf), None) != 0:
+        raise RuntimeError("FMA peak microkernel failed")
+    return tf.value
 
 
 def measure(args, precision, system, dist, world, local):
@@ -187,7 +193,9 @@ def measure(args, precision, system, dist, world, local):
         t_max = float(t.item())
     value = world * args.steps / (t_max / 1000.0)
 
-    # Dominant stage and its roofline (algorithmic bytes / measured average launch time).
+    # Dominant pair stage and its roofline: compulsory bytes and algorithmic FLOPs of one
+    # launch over the stage's measured average launch time (the kernel alone on the stream),
+    # against the measured HBM copy bandwidth and the measured FMA-pipe throughput.
     kernel_stages = ["vdw", "ind_field", "real_energy"]
     per_stage = {cabi.STAGE_NAMES[i]: {"ms_total": float(stage_ms[i]), "launches": int(stage_n[i])}
                  for i in range(12)}
@@ -197,8 +205,10 @@ def measure(args, precision, system, dist, world, local):
     peak, peak_src = 6650.0, "fallback"
     if os.path.exists(peaks_path):
         peak, peak_src = float(json.load(open(peaks_path))["hbm_gbs"]), "measured"
-    traffic_alg = algorithmic_traffic(dom, n, pairs_half, 2 * ffe.count("vdw"), mixed)
-    achieved = traffic_alg / (avg_ms * 1e-3) / 1e9
+    bytes_alg, flops_alg = algorithmic_work(dom, n, pairs_half, ffe.count("vdw"))
+    achieved = bytes_alg / (avg_ms * 1e-3) / 1e9
+    fp_peak = fma_peak_tflops(fp64=not mixed)
+    fp_achieved = flops_alg / (avg_ms * 1e-3) / 1e12
 
     # End to end through the public API with host buffers (H2D coordinates, D2H gradient).
     x_host = np.ascontiguousarray(system.xyz)
@@ -226,13 +236,54 @@ def measure(args, precision, system, dist, world, local):
         "stages_ms_per_step": {k: v["ms_total"] / args.steps for k, v in per_stage.items()},
         "stages_note": "direct launches with per-stage events (the timed steps replay one CUDA graph)",
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
-                     "frac": achieved / peak,
-                     "traffic": PAIR_FIELD_TRAFFIC if (mixed and dom == "ind_field") else None,
-                     "kernel_stage": dom,
-                     "algorithmic_bytes_per_launch": traffic_alg, "avg_launch_ms": avg_ms,
-                     "peak_source": peak_src,
-                     "note": "stage timed with direct launches, the kernel alone on its stream; the pair kernels are bound by gather latency, not HBM (profiles/pcg_kernels_water24k_mixed.md)"},
+                     "frac": achieved / peak, "traffic": None,
+                     "kernel_stage": dom, "algorithmic_bytes_per_launch": bytes_alg,
+                     "bytes_rule": f"{BYTES_PER_ATOM[dom]:.0f} B per atom per pass (compulsory HBM bytes)",
+                     "avg_launch_ms": avg_ms, "peak_source": peak_src,
+                     "fp_pipe": {"achieved": fp_achieved, "peak": fp_peak, "unit": "TFLOP/s",
+                                 "frac": fp_achieved / fp_peak, "pipe": "FP64 FMA" if not mixed else "FP32 FMA",
+                                 "flops_per_launch": flops_alg,
+                                 "flops_rule": f"{FLOPS_PER_PAIR[dom]:.0f} FLOPs per undirected pair",
+                                 "peak_source": "measured: FMA microkernel (libffxpeak.so) in this run"},
+                     "note": "the stage's kernel timed alone on its stream with CUDA events (direct launches); "
+                             "traffic: DRAM bytes come from separate ncu captures, not from this run"},
     }
+
+
+def measure_md(args, system, dist, world):
+    """Config 2's dynamics: ``--md-steps`` velocity-Verlet steps of 2 fs with SETTLE rigid
+    waters on the device (ffxg_md_run: positions and velocities stay on the GPU, every step
+    replays the evaluation graph, the neighbour list is rebuilt whenever an atom has moved
+    more than half the buffer), mixed form, velocities drawn at 300 K.  Timed on the host
+    clock around the one call, host copies included; ns/day is measured, not extrapolated."""
+    import math
+    import torch
+    from forcefieldx_b200.energy import ForceFieldEnergy
+    n = system.n_atoms
+    kcal, kb = 418.4, 0.0019872041
+    mass = np.where(np.arange(n) % 3 == 0, 15.999, 1.008)
+    roh, theta = 0.9572, math.radians(104.52)
+    rng = np.random.default_rng(300)
+    vel = rng.normal(size=(n, 3)) * np.sqrt(kb * 300.0 * kcal / mass)[:, None]
+    with ForceFieldEnergy(system, build_params(PRECISION_MIXED)) as ffe:
+        ffe.md_setup(mass, np.arange(n).reshape(-1, 3), roh, 2.0 * roh * math.sin(theta / 2.0))
+        x, v, _, _ = ffe.md_run(system.xyz, vel, 0.002, 20)          # warm-up: graphs captured
+        if dist:
+            dist.barrier()
+        builds0 = ffe.list_builds()
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        x, v, _, _ = ffe.md_run(x, v, 0.002, args.md_steps)
+        dt = time.perf_counter() - t0
+        builds = ffe.list_builds() - builds0
+        if dist:
+            t = torch.tensor([dt], dtype=torch.float64, device="cuda")
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            dt = float(t.item())
+    return {"steps": args.md_steps, "dt_fs": 2.0, "precision": "mixed", "seconds": dt,
+            "ns_per_day": world * args.md_steps * 2e-6 / dt * 86400.0, "steps_per_s": world * args.md_steps / dt,
+            "list_builds": int(builds),
+            "method": "ffxg_md_run: velocity Verlet + SETTLE on the device, 300 K start, host clock around the call"}
 
 
 def run_mine(args):
@@ -256,6 +307,10 @@ def run_mine(args):
     head_name = order[-1]
     head = runs[head_name]
 
+    md = None
+    if args.md_steps > 0:
+        md = measure_md(args, system, dist, world)
+
     batch = None
     if args.batch_systems > 0:
         try:
@@ -275,7 +330,7 @@ def run_mine(args):
         "config": {"workload": WORKLOAD, "atoms": n, "precision": head_name,
                    "pcg_iterations": head["pcg_iterations"], "energy_kcal_mol": head["terms"][9],
                    "parallelism": f"replicas x{world}", "l2": "flushed between steps (256 MB write, untimed)",
-                   "ns_per_day_2fs": head["value"] / world * 2e-6 * 86400},
+                   "ns_per_day_2fs_from_evals": head["value"] / world * 2e-6 * 86400},
         "roofline": head["roofline"],
         "stages_ms_per_step": head["stages_ms_per_step"],
         "e2e": head["e2e"], "gpu_launches": head["launches"], "clocks": head["clocks"],
@@ -291,6 +346,8 @@ def run_mine(args):
         result["mixed_energy_error_vs_fp64_gpu"] = {
             "total_rel": abs(head["terms"][9] - f["terms"][9]) / abs(f["terms"][9]),
             "terms_abs": [abs(a - b) for a, b in zip(head["terms"], ref_terms)]}
+    if md:
+        result["md"] = md
     if batch:
         result["batch"] = batch
     if cpu:
@@ -495,6 +552,8 @@ def main():
     ap.add_argument("--batch-systems", type=int, default=512,
                     help="also time a batch of this many small systems (0: skip)")
     ap.add_argument("--batch-steps", type=int, default=5)
+    ap.add_argument("--md-steps", type=int, default=1000,
+                    help="also time this many 2 fs MD steps on the device (0: skip)")
     ap.add_argument("--lambda-values", type=float, nargs="*", default=None,
                     help="instead of the headline, time electrostatic lambda evaluations at these lambdas")
     ap.add_argument("--accuracy-frames", type=int, default=0,

@@ -1,4 +1,6 @@
-"""Build libffxcuda.so in-tree with nvcc for sm_100a (no JIT cache, no torch extension)."""
+"""Build libffxcuda.so (the energy library) and libffxpeak.so (FMA-throughput microkernels
+for the benchmark's pipe fractions) in-tree with nvcc for sm_100a (no JIT cache, no torch
+extension)."""
 from __future__ import annotations
 
 import os
@@ -8,6 +10,8 @@ import sys
 HERE = os.path.dirname(os.path.abspath(__file__))
 SOURCES = ["handle.cu", "nlist.cu", "pme.cu", "real.cu", "vdw.cu", "recip.cu", "pcg.cu", "md.cu", "batch.cu"]
 LIB = os.path.join(HERE, "libffxcuda.so")
+PEAK_SRC = "peak.cu"
+PEAK_LIB = os.path.join(HERE, "libffxpeak.so")
 NVCC_FLAGS = ["-gencode", "arch=compute_100a,code=sm_100a", "-O3", "-lineinfo", "-std=c++17",
               "-Xcompiler", "-fPIC", "-shared", "-diag-suppress", "177"]
 
@@ -29,6 +33,12 @@ def stale() -> bool:
 
 
 def build(force: bool = False, verbose: bool = False) -> str:
+    peak_src = os.path.join(HERE, "csrc", PEAK_SRC)
+    if force or not os.path.exists(PEAK_LIB) or os.path.getmtime(PEAK_LIB) < os.path.getmtime(peak_src):
+        cmd = [nvcc()] + NVCC_FLAGS + ["-o", PEAK_LIB, peak_src]
+        if verbose:
+            print(" ".join(cmd), file=sys.stderr)
+        subprocess.run(cmd, check=True)
     if not force and not stale():
         return LIB
     cmd = [nvcc()] + NVCC_FLAGS + ["-o", LIB] + [os.path.join(HERE, "csrc", s) for s in SOURCES]

@@ -105,6 +105,7 @@ PROTOTYPES = {
     "ffxg_md_run": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_double, ctypes.c_int32, _D, _D, _D, _D]),
     "ffxg_set_scf_predictor": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int]),
     "ffxg_stream": (ctypes.c_void_p, [ctypes.c_void_p]),
+    "ffxg_list_builds": (ctypes.c_int64, [ctypes.c_void_p]),
     "ffxg_last_launch_count": (ctypes.c_int64, [ctypes.c_void_p]),
     "ffxg_set_timing": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int]),
     "ffxg_set_graph_mode": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int]),

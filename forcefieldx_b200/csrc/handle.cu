@@ -1664,6 +1664,8 @@ int ffxg_md_run(ffxg_handle *hh, double dt, int32_t n_steps, double *xyz, double
 
 void *ffxg_stream(ffxg_handle *hh) { return hh ? (void *)hh->h.stream : nullptr; }
 
+int64_t ffxg_list_builds(const ffxg_handle *hh) { return hh ? hh->h.list_builds : -1; }
+
 int64_t ffxg_last_launch_count(const ffxg_handle *hh) { return hh ? hh->h.launches : 0; }
 
 int ffxg_set_graph_mode(ffxg_handle *hh, int on) {

@@ -281,6 +281,10 @@ class ForceFieldEnergy:
     def launch_count(self) -> int:
         return int(self.lib.ffxg_last_launch_count(self._h))
 
+    def list_builds(self) -> int:
+        """Neighbour-list builds since the handle was created."""
+        return int(self.lib.ffxg_list_builds(self._h))
+
 
 class CrystalEnergy:
     """Energy and gradient of an asymmetric unit in a space group with an orthorhombic cell,

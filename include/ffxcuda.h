@@ -369,6 +369,11 @@ int ffxg_set_scf_predictor(ffxg_handle *h, int predictor);
 /* The CUDA stream (cudaStream_t) the handle launches on, for event timing. */
 void *ffxg_stream(ffxg_handle *h);
 
+/* Neighbour-list builds since the handle was created (every evaluation and MD step that
+ * found an atom moved more than half the list buffer, as NeighborList's motion check
+ * decides, NeighborList.java:777-799), for MD statistics. */
+int64_t ffxg_list_builds(const ffxg_handle *h);
+
 /* Device count of kernel launches issued by the last energy call. */
 int64_t ffxg_last_launch_count(const ffxg_handle *h);
 

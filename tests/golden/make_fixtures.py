@@ -99,7 +99,9 @@ def numerics_known_answers(ref_root):
 
 
 def main():
-    ref_root = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
+    ref_root = sys.argv[1] if len(sys.argv) > 1 else os.environ.get("FFX_REFERENCE_ROOT", "")
+    if not ref_root or not os.path.isdir(ref_root):
+        sys.exit("usage: make_fixtures.py <reference checkout> (or set FFX_REFERENCE_ROOT)")
     prm = read_prm(os.path.join(ref_root, PRM))
     out = {}
     for name, xyz_file, key_file in (("dhfr", "dhfr.xyz", "dhfr.key"),
