@@ -47,6 +47,7 @@ class FfxgParams(ctypes.Structure):
         ("intra14", ctypes.c_double), ("d11", ctypes.c_double),
         ("v12", ctypes.c_double), ("v13", ctypes.c_double), ("v14", ctypes.c_double),
         ("precision", ctypes.c_int32),
+        ("angles", ctypes.c_double * 3),
     ]
 
 

@@ -62,11 +62,17 @@ static cudaError_t dalloc(T **p, size_t count) {
   return cudaMalloc((void **)p, std::max<size_t>(count, 1) * sizeof(T));
 }
 
+// Any mesh length of at least the B-spline order: radices 2, 3, 4, 5, 7 have their own
+// butterflies and larger prime factors the general pass (Complex.java:173-330, 371-383).
+// A length has at most 12 factors (4096 = 4^6 needs 6).
 static bool fft_supported(int n) {
-  if (n < kOrder) return false;
-  for (int f : {2, 3, 5, 7})
-    while (n % f == 0) n /= f;
-  return n == 1;
+  if (n < kOrder || n > 4096) return false;
+  int m = n, count = 0;
+  for (int f : {4, 2, 3, 5, 7})
+    while (m % f == 0) { m /= f; count++; }
+  for (int f = 11; m > 1; f += 2)
+    while (m % f == 0) { m /= f; count++; }
+  return count <= 12;
 }
 
 __global__ void k_set_flags(int *flags, int v) { *flags = v; }
@@ -218,7 +224,7 @@ static int create_impl(const ffxg_system *s, const ffxg_params *p, Handle &h) {
   for (int d = 0; d < 3; d++) {
     if (!(p->box[d] > 0.0)) { h.err = "box edges must be positive"; return FFXG_ERR_BAD_ARG; }
     if (!fft_supported(p->pme_grid[d])) {
-      h.err = "PME grid dimensions must be >= 5 and factor into 2, 3, 5 and 7";
+      h.err = "PME grid dimensions must lie in [5, 4096]";
       return FFXG_ERR_BAD_ARG;
     }
   }
@@ -1127,7 +1133,7 @@ int ffxg_set_box(ffxg_handle *hh, const double box[3], const int32_t pme_grid[3]
   for (int d = 0; d < 3; d++) {
     if (!(box[d] > 0.0) || !std::isfinite(box[d])) { h.err = "box edges must be positive"; return FFXG_ERR_BAD_ARG; }
     if (pme_grid && !fft_supported(pme_grid[d])) {
-      h.err = "PME grid dimensions must be >= 5 and factor into 2, 3, 5 and 7";
+      h.err = "PME grid dimensions must lie in [5, 4096]";
       return FFXG_ERR_BAD_ARG;
     }
   }

@@ -394,6 +394,37 @@ __device__ __forceinline__ void fft_butterfly(const typename Vec2<S>::type *in, 
   for (int q = 0; q < R; q++) out[(idxD + q * Ns) * L + l] = y[q];
 }
 
+// Radix-R pass for any R known only at run time (prime factors above 7, as the general
+// pass of Complex.java:173-330 handles them): each output q of the length-R DFT is summed
+// from the R twiddled inputs read from shared memory, O(R^2) per butterfly.
+template <typename S>
+__device__ __forceinline__ void fft_butterfly_any(int R, const typename Vec2<S>::type *in,
+                                                  typename Vec2<S>::type *out, int j, int l, int L, int nb, int Ns,
+                                                  int len, int sg, const typename Vec2<S>::type *__restrict__ tw) {
+  using V2 = typename Vec2<S>::type;
+  const int k = j % Ns;
+  const int tstep = len / (Ns * R);
+  const int wstep = len / R;
+  const int idxD = (j / Ns) * Ns * R + k;
+  for (int q = 0; q < R; q++) {
+    V2 acc = in[j * L + l];
+    for (int r = 1; r < R; r++) {
+      V2 a = in[(j + r * nb) * L + l];
+      if (k > 0) {
+        V2 w = tw[r * k * tstep];
+        if (sg > 0) w.y = -w.y;
+        a = cmul(a, w);
+      }
+      V2 w = tw[((r * q) % R) * wstep];
+      if (sg > 0) w.y = -w.y;
+      a = cmul(a, w);
+      acc.x += a.x;
+      acc.y += a.y;
+    }
+    out[(idxD + q * Ns) * L + l] = acc;
+  }
+}
+
 // FROMD (mixed form, first pass only): the input is the double accumulation mesh `src`
 // (real plane, then imaginary plane at src + src_ng), converted to FP32 on load and
 // cleared behind the read, so that the next spread starts from zero without a memset.
@@ -442,7 +473,8 @@ __global__ void __launch_bounds__(256) k_fft_axis(typename Vec2<S>::type *grid, 
           case 2: fft_butterfly<2, S>(in, out, j, l, L, nb, Ns, len, sg, tw); break;
           case 3: fft_butterfly<3, S>(in, out, j, l, L, nb, Ns, len, sg, tw); break;
           case 5: fft_butterfly<5, S>(in, out, j, l, L, nb, Ns, len, sg, tw); break;
-          default: fft_butterfly<7, S>(in, out, j, l, L, nb, Ns, len, sg, tw); break;
+          case 7: fft_butterfly<7, S>(in, out, j, l, L, nb, Ns, len, sg, tw); break;
+          default: fft_butterfly_any<S>(R, in, out, j, l, L, nb, Ns, len, sg, tw); break;
         }
       }
       __syncthreads();
@@ -813,6 +845,9 @@ static FftAxis make_axis(int axis, const int nf[3]) {
   a.nradix = 0;
   for (int f : {4, 2, 3, 5, 7}) {
     while (m % f == 0) { a.radix[a.nradix++] = f; m /= f; }
+  }
+  for (int f = 11; m > 1 && a.nradix < 12; f += 2) {   // remaining primes: the general pass
+    while (m % f == 0 && a.nradix < 12) { a.radix[a.nradix++] = f; m /= f; }
   }
   // Lines of a CTA: consecutive along the fastest index that is not the transform axis.
   const int inner = (axis == 0) ? ny : nx;
@@ -1379,12 +1414,7 @@ __global__ void k_na_energy(int nb, double electric, const NoAllocScratch *s, do
   }
 }
 
-static bool na_dim_ok(int n) {
-  if (n < kOrder) return false;
-  for (int f : {2, 3, 5, 7})
-    while (n % f == 0) n /= f;
-  return n == 1;
-}
+static bool na_dim_ok(int n) { return n >= kOrder; }   // any length: the general radix pass
 
 extern "C" int ffxg_pme_recip_permanent_noalloc(const double *d_xyz, const double *d_mpole, int32_t n_atoms,
                                                 const double box[3], const int32_t pme_grid[3], double ewald_alpha,

@@ -26,6 +26,7 @@ per asymmetric unit.
 """
 from __future__ import annotations
 
+import math
 import os
 import re
 from typing import Dict, List, Optional, Tuple
@@ -239,16 +240,29 @@ def write_xyz(path, xyz, types, bonds, names=None, title="") -> None:
             f.write(f"{a + 1:6d}  {name:<3s}{xyz[a, 0]:12.6f}{xyz[a, 1]:12.6f}{xyz[a, 2]:12.6f}{int(types[a]):6d}{links}\n")
 
 
-# Symmetry operators (fractional: x' = R x + t) of the space groups whose unit cell is
-# orthorhombic, the only cells the library takes; standard settings of the International
-# Tables, in the order Force Field X lists them for its P1 expansion of P212121
-# (the reference's 1n7s.P212121 / 1n7s.P1 test pair).
+# Symmetry operators (fractional: x' = R x + t), standard settings of the International
+# Tables, in the order Force Field X's SpaceGroupDefinitions lists them
+# (crystal/SpaceGroupDefinitions.java: P-1 :116-126, P21 :146-156, P21/c :312-328,
+# C2/c :329-349, Pbca :1270-1287; the P212121 order follows the reference's
+# 1n7s.P212121 / 1n7s.P1 test pair).
 def _op(r, t):
     return (np.array(r, dtype=np.float64), np.array(t, dtype=np.float64))
 
 
+_I, _INV = np.eye(3), -np.eye(3)
+_M2Y, _MY = np.diag([-1.0, 1.0, -1.0]), np.diag([1.0, -1.0, 1.0])   # 2-fold along b; mirror normal to b
+
 SPACE_GROUPS = {
     "P1": [_op(np.eye(3), (0, 0, 0))],
+    "P-1": [_op(_I, (0, 0, 0)), _op(_INV, (0, 0, 0))],
+    "P21": [_op(_I, (0, 0, 0)), _op(_M2Y, (0, 0.5, 0))],
+    "P21/C": [_op(_I, (0, 0, 0)), _op(_INV, (0, 0, 0)), _op(_M2Y, (0, 0.5, 0.5)), _op(_MY, (0, 0.5, 0.5))],
+    "C2/C": [_op(_I, (0, 0, 0)), _op(_M2Y, (0, 0, 0.5)), _op(_INV, (0, 0, 0)), _op(_MY, (0, 0, 0.5)),
+             _op(_I, (0.5, 0.5, 0)), _op(_M2Y, (0.5, 0.5, 0.5)), _op(_INV, (0.5, 0.5, 0)), _op(_MY, (0.5, 0.5, 0.5))],
+    "PBCA": [_op(_I, (0, 0, 0)), _op(np.diag([-1.0, -1.0, 1.0]), (0.5, 0, 0.5)),
+             _op(np.diag([-1.0, 1.0, -1.0]), (0, 0.5, 0.5)), _op(np.diag([1.0, -1.0, -1.0]), (0.5, 0.5, 0)),
+             _op(_INV, (0, 0, 0)), _op(np.diag([1.0, 1.0, -1.0]), (0.5, 0, 0.5)),
+             _op(np.diag([1.0, -1.0, 1.0]), (0, 0.5, 0.5)), _op(np.diag([-1.0, 1.0, 1.0]), (0.5, 0.5, 0))],
     "P222": [_op(np.eye(3), (0, 0, 0)), _op(np.diag([-1, -1, 1]), (0, 0, 0)),
              _op(np.diag([-1, 1, -1]), (0, 0, 0)), _op(np.diag([1, -1, -1]), (0, 0, 0))],
     "P2221": [_op(np.eye(3), (0, 0, 0)), _op(np.diag([-1, -1, 1]), (0, 0, 0.5)),
@@ -263,23 +277,48 @@ SPACE_GROUPS = {
 def space_group(key: Dict[str, List[str]]) -> str:
     sg = key.get("spacegroup", ["P1"])[0].upper().replace(" ", "")
     if sg not in SPACE_GROUPS:
-        raise ValueError(f"space group {sg}: supported are {sorted(SPACE_GROUPS)} (orthorhombic cells)")
+        raise ValueError(f"space group {sg}: supported are {sorted(SPACE_GROUPS)}")
     return sg
 
 
-def expand_coordinates(xyz, box, sg: str) -> np.ndarray:
+def cell_matrices(box, angles=(90.0, 90.0, 90.0)):
+    """(A^-1, A) of Crystal.updateCrystal (C/Crystal.java:1428-1548): the rows of A^-1 are
+    the lattice vectors, x_frac = x A, x = x_frac A^-1; orthorhombic, monoclinic and
+    general branches as the library and the oracle build them."""
+    a, b, c = (float(v) for v in box)
+    al, be, ga = (float(v) if float(v) > 0 else 90.0 for v in angles)
+    if al == 90.0 and be == 90.0 and ga == 90.0:
+        return np.diag([a, b, c]), np.diag([1.0 / a, 1.0 / b, 1.0 / c])
+    deg = 0.017453292519943295
+    if al == 90.0 and ga == 90.0:
+        cos_a, sin_b, cos_b, sin_g, cos_g = 0.0, math.sin(be * deg), math.cos(be * deg), 1.0, 0.0
+        beta_term, gamma_term = 0.0, sin_b
+    else:
+        cos_a, sin_b, cos_b = math.cos(al * deg), math.sin(be * deg), math.cos(be * deg)
+        sin_g, cos_g = math.sin(ga * deg), math.cos(ga * deg)
+        beta_term = (cos_a - cos_b * cos_g) / sin_g
+        gamma_term = math.sqrt(sin_b * sin_b - beta_term * beta_term)
+    ai = np.array([[a, 0.0, 0.0], [b * cos_g, b * sin_g, 0.0], [c * cos_b, c * beta_term, c * gamma_term]])
+    return ai, np.linalg.inv(ai)
+
+
+def expand_coordinates(xyz, box, sg: str, angles=(90.0, 90.0, 90.0)) -> np.ndarray:
     """Coordinates of the unit cell's symmetry mates of an asymmetric unit, mate after mate
     (x_frac' = R x_frac + t; no wrapping, the energy is periodic)."""
     xyz = np.asarray(xyz, dtype=np.float64).reshape(-1, 3)
     box = np.asarray(box, dtype=np.float64)
-    frac = xyz / box
-    return np.concatenate([((frac @ R.T) + t) * box for R, t in SPACE_GROUPS[sg]])
+    ai, a = cell_matrices(box, angles)
+    if np.count_nonzero(ai - np.diag(np.diag(ai))) == 0:
+        frac = xyz / box
+        return np.concatenate([((frac @ R.T) + t) * box for R, t in SPACE_GROUPS[sg]])
+    frac = xyz @ a
+    return np.concatenate([((frac @ R.T) + t) @ ai for R, t in SPACE_GROUPS[sg]])
 
 
-def expand_system(system: AmoebaSystem, box, sg: str) -> AmoebaSystem:
+def expand_system(system: AmoebaSystem, box, sg: str, angles=(90.0, 90.0, 90.0)) -> AmoebaSystem:
     """A resolved asymmetric-unit system expanded to the P1 cell of its symmetry mates
     (attributes n_symm, n_asu set)."""
-    cell = tile_system(system, expand_coordinates(system.xyz, box, sg), len(SPACE_GROUPS[sg]))
+    cell = tile_system(system, expand_coordinates(system.xyz, box, sg, angles), len(SPACE_GROUPS[sg]))
     cell.n_symm = len(SPACE_GROUPS[sg])
     cell.n_asu = system.n_atoms
     return cell
@@ -288,12 +327,10 @@ def expand_system(system: AmoebaSystem, box, sg: str) -> AmoebaSystem:
 def params_from_key(key: Dict[str, List[str]], **overrides) -> AmoebaParams:
     """AmoebaParams from a key file's keywords (ForceFieldEnergy / PME defaults otherwise)."""
     space_group(key)
-    for ang in ("alpha", "beta", "gamma"):
-        if ang in key and abs(float(key[ang][0]) - 90.0) > 1e-9:
-            raise ValueError("only orthorhombic boxes are supported")
     a = float(key["a-axis"][0])
     box = [a, float(key.get("b-axis", [a])[0]), float(key.get("c-axis", [a])[0])]
-    kw = dict(box=box)
+    angles = tuple(float(key.get(ang, ["90.0"])[0]) for ang in ("alpha", "beta", "gamma"))
+    kw = dict(box=box, angles=angles)
     for name, field, conv in (("vdw-cutoff", "vdw_cutoff", float), ("ewald-cutoff", "ewald_cutoff", float),
                               ("ewald-alpha", "ewald_alpha", float), ("pme-order", "pme_order", int),
                               ("polar-eps", "polar_eps", float), ("pme-mesh-density", "pme_mesh_density", float)):
@@ -364,21 +401,21 @@ def load_system(xyz_path: str, key_path: str, prm_path: Optional[str] = None, ex
     sg = space_group(key)
     n_asu = len(types)
     if expand_symmetry and sg != "P1":
-        xyz, types, bonds = unit_cell(xyz, types, bonds, params.box, sg)
+        xyz, types, bonds = unit_cell(xyz, types, bonds, params.box, sg, params.angles)
     system = system_from_types(xyz, types, bonds, read_prm(prm_path))
     system.n_symm = len(types) // n_asu
     system.n_asu = n_asu
     return system, params
 
 
-def unit_cell(xyz, types, bonds, box, sg: str):
+def unit_cell(xyz, types, bonds, box, sg: str, angles=(90.0, 90.0, 90.0)):
     """The P1 unit cell of an asymmetric unit: every symmetry mate's atoms (types and bonds
     repeated with the atom offset of the mate).  The crystal energy per asymmetric unit is
     the cell's energy over the number of mates, and the asymmetric unit's gradient is the
     first mate's rows of the cell's gradient (the mates are images of one another)."""
     n = len(types)
     ops = SPACE_GROUPS[sg]
-    cell_xyz = expand_coordinates(xyz, box, sg)
+    cell_xyz = expand_coordinates(xyz, box, sg, angles)
     cell_types = np.concatenate([np.asarray(types)] * len(ops))
     b = np.asarray(bonds, dtype=np.int64).reshape(-1, 2)
     cell_bonds = np.concatenate([b + m * n for m in range(len(ops))])

@@ -144,6 +144,7 @@ class AmoebaParams:
     v13: float = 0.0
     v14: float = 1.0
     precision: int = PRECISION_FP64
+    angles: Sequence[float] = (90.0, 90.0, 90.0)   # alpha, beta, gamma (degrees)
 
     def grid(self):
         if self.pme_grid is not None:
@@ -274,6 +275,8 @@ def params_struct(params: AmoebaParams, lib_types):
     p.max_scf_iter = int(params.max_scf_iter)
     p.polarization = int(params.polarization)
     p.precision = int(params.precision)
+    for i in range(3):
+        p.angles[i] = float(params.angles[i])
     return p
 
 

@@ -128,13 +128,14 @@ typedef struct {
 } ffxg_system;
 
 typedef struct {
-  double box[3];                 /* orthorhombic cell edges a, b, c (A) */
+  double box[3];                 /* cell edges a, b, c (A); angles below */
   double vdw_cutoff;             /* A (vdw-cutoff) */
   double vdw_taper;              /* fraction of the cutoff where the taper starts (vdw-taper, 0.9) */
   double ewald_cutoff;           /* A (ewald-cutoff) */
   double ewald_alpha;            /* 1/A (ewald-alpha) */
   double list_buffer;            /* A (list-buffer, 2.0) */
-  int32_t pme_grid[3];           /* PME mesh dimensions */
+  int32_t pme_grid[3];           /* PME mesh dimensions, 5 .. 4096 each (any factors: radices 2-7 have
+                                    their own butterflies, larger primes a general pass) */
   int32_t pme_order;             /* B-spline order (5) */
   double polar_eps;              /* PCG convergence, Debye RMS (polar-eps) */
   int32_t max_scf_iter;          /* PCG iteration cap (1000 in the reference) */
@@ -148,6 +149,12 @@ typedef struct {
   double d11;                    /* direct-11-scale */
   double v12, v13, v14;          /* vdw-1n-scale */
   int32_t precision;             /* ffxg_precision */
+  double angles[3];              /* cell angles alpha, beta, gamma (degrees; 0 reads as 90).  With box
+                                    (a, b, c) they give the cell of Crystal.updateCrystal
+                                    (C/Crystal.java:1428-1548): orthorhombic, monoclinic (only beta
+                                    differs from 90) or general.  The pair lists need every
+                                    interaction cutoff below half of each perpendicular width, or
+                                    take lists of every lattice image. */
 } ffxg_params;
 
 /* Build a handle: validate the system, upload topology and parameters, pick a
@@ -427,7 +434,7 @@ int ffxg_set_graph_mode(ffxg_handle *h, int on);
  *
  * All intermediates live in one fixed array of about 6.3 MB that each device
  * holds from the first call until the process exits.  Limits: n_atoms <= 32768 and
- * every mesh dimension <= 64 (factors 2, 3, 5, 7); beyond them the call returns
+ * every mesh dimension <= 64 (and >= 5, any factors); beyond them the call returns
  * FFXG_ERR_CAPACITY without launching anything.  The first call on a device looks
  * up the array's device address (cudaGetSymbolAddress) with that device current;
  * make that first call before any stream capture.  Every call on a device shares

@@ -46,6 +46,8 @@ struct Cell {
   double A00, A10, A20, A11, A21, A22;        // A = (A^-1)^-1, columns = reciprocal vectors
   double Ai00, Ai10, Ai20, Ai11, Ai21, Ai22;  // A^-1 rows = lattice vectors
   double A[3][3];
+  bool ortho = true;                          // all angles 90: A and A^-1 diagonal
+  double width[3];                            // perpendicular widths 1 / |a*_d|
 };
 
 inline double jsignum(double v) { return v > 0.0 ? 1.0 : (v < 0.0 ? -1.0 : v); }
@@ -63,16 +65,85 @@ inline double image(double &x, double &y, double &z, const Cell &c) {
   return x * x + y * y + z * z;
 }
 
-Cell make_cell(const double box[3]) {
+// Crystal.updateCrystal (C/Crystal.java:1428-1548): the lattice vectors a = (a, 0, 0),
+// b = (b cos g, b sin g, 0), c = (c cos b, c beta_term, c gamma_term) as the rows of A^-1,
+// A its inverse (lower triangular, so inverted in closed form here) and the volume, by the
+// orthorhombic, monoclinic (only beta differs from 90) and general branches.  Angles of 0
+// read as 90.
+Cell make_cell(const double box[3], const double angles[3]) {
   Cell c{};
   c.a = box[0]; c.b = box[1]; c.c = box[2];
-  c.volume = c.a * c.b * c.c;  // Crystal.java (orthorhombic branch)
-  c.Ai00 = c.a; c.Ai10 = 0.0; c.Ai20 = 0.0; c.Ai11 = c.b; c.Ai21 = 0.0; c.Ai22 = c.c;
-  // LU inverse of a diagonal matrix is the elementwise reciprocal.
-  c.A00 = 1.0 / c.a; c.A10 = 0.0; c.A20 = 0.0; c.A11 = 1.0 / c.b; c.A21 = 0.0; c.A22 = 1.0 / c.c;
+  double ang[3];
+  for (int d = 0; d < 3; d++) ang[d] = (angles && angles[d] > 0.0) ? angles[d] : 90.0;
   std::memset(c.A, 0, sizeof(c.A));
-  c.A[0][0] = c.A00; c.A[1][1] = c.A11; c.A[2][2] = c.A22;
+  if (ang[0] == 90.0 && ang[1] == 90.0 && ang[2] == 90.0) {
+    c.volume = c.a * c.b * c.c;  // Crystal.java (orthorhombic branch)
+    c.Ai00 = c.a; c.Ai10 = 0.0; c.Ai20 = 0.0; c.Ai11 = c.b; c.Ai21 = 0.0; c.Ai22 = c.c;
+    // LU inverse of a diagonal matrix is the elementwise reciprocal.
+    c.A00 = 1.0 / c.a; c.A10 = 0.0; c.A20 = 0.0; c.A11 = 1.0 / c.b; c.A21 = 0.0; c.A22 = 1.0 / c.c;
+    c.A[0][0] = c.A00; c.A[1][1] = c.A11; c.A[2][2] = c.A22;
+    c.ortho = true;
+    c.width[0] = c.a; c.width[1] = c.b; c.width[2] = c.c;
+    return c;
+  }
+  const double deg = 0.017453292519943295;   // Math.toRadians
+  double cos_alpha, sin_beta, cos_beta, sin_gamma, cos_gamma, beta_term, gamma_term;
+  if (ang[0] == 90.0 && ang[2] == 90.0) {    // monoclinic
+    cos_alpha = 0.0;
+    sin_beta = std::sin(ang[1] * deg);
+    cos_beta = std::cos(ang[1] * deg);
+    sin_gamma = 1.0;
+    cos_gamma = 0.0;
+    beta_term = 0.0;
+    gamma_term = sin_beta;
+    c.volume = sin_beta * c.a * c.b * c.c;
+  } else {                                   // triclinic, hexagonal, trigonal
+    cos_alpha = std::cos(ang[0] * deg);
+    sin_beta = std::sin(ang[1] * deg);
+    cos_beta = std::cos(ang[1] * deg);
+    sin_gamma = std::sin(ang[2] * deg);
+    cos_gamma = std::cos(ang[2] * deg);
+    beta_term = (cos_alpha - cos_beta * cos_gamma) / sin_gamma;
+    gamma_term = std::sqrt(sin_beta * sin_beta - beta_term * beta_term);
+    c.volume = sin_gamma * gamma_term * c.a * c.b * c.c;
+  }
+  c.Ai00 = c.a;
+  c.Ai10 = c.b * cos_gamma; c.Ai11 = c.b * sin_gamma;
+  c.Ai20 = c.c * cos_beta; c.Ai21 = c.c * beta_term; c.Ai22 = c.c * gamma_term;
+  c.A00 = 1.0 / c.Ai00;
+  c.A11 = 1.0 / c.Ai11;
+  c.A22 = 1.0 / c.Ai22;
+  c.A10 = -c.Ai10 / (c.Ai00 * c.Ai11);
+  c.A21 = -c.Ai21 / (c.Ai11 * c.Ai22);
+  c.A20 = (c.Ai10 * c.Ai21 - c.Ai11 * c.Ai20) / (c.Ai00 * c.Ai11 * c.Ai22);
+  c.A[0][0] = c.A00; c.A[1][0] = c.A10; c.A[1][1] = c.A11;
+  c.A[2][0] = c.A20; c.A[2][1] = c.A21; c.A[2][2] = c.A22;
+  c.ortho = false;
+  c.width[0] = 1.0 / std::sqrt(c.A00 * c.A00 + c.A10 * c.A10 + c.A20 * c.A20);
+  c.width[1] = 1.0 / std::sqrt(c.A11 * c.A11 + c.A21 * c.A21);
+  c.width[2] = 1.0 / std::fabs(c.A22);
   return c;
+}
+
+// Fractional coordinates x A (Crystal.toFractionalCoordinates order).
+inline void to_frac(double x, double y, double z, const Cell &c, double &fx, double &fy, double &fz) {
+  if (c.ortho) { fx = x * c.A00; fy = y * c.A11; fz = z * c.A22; return; }
+  fx = x * c.A00 + y * c.A10 + z * c.A20;
+  fy = y * c.A11 + z * c.A21;
+  fz = z * c.A22;
+}
+
+// The lattice translation n A^-1 added to a displacement (multi-image lists).
+inline void add_shift(double &dx, double &dy, double &dz, int nx, int ny, int nz, double sign, const Cell &c) {
+  if (c.ortho) {
+    dx += sign * ((double)nx * c.a);
+    dy += sign * ((double)ny * c.b);
+    dz += sign * ((double)nz * c.c);
+    return;
+  }
+  dx += sign * ((double)nx * c.Ai00 + (double)ny * c.Ai10 + (double)nz * c.Ai20);
+  dy += sign * ((double)ny * c.Ai11 + (double)nz * c.Ai21);
+  dz += sign * ((double)nz * c.Ai22);
 }
 
 // ---------------------------------------------------------------------------
@@ -336,9 +407,7 @@ struct Oracle {
               double sign = 1.0) const {
     if (!multi_image) return image(dx, dy, dz, cell);
     const int c = sh[i][e];
-    dx += sign * ((double)((c & 1023) - 512) * cell.a);
-    dy += sign * ((double)(((c >> 10) & 1023) - 512) * cell.b);
-    dz += sign * ((double)(((c >> 20) & 1023) - 512) * cell.c);
+    add_shift(dx, dy, dz, (c & 1023) - 512, ((c >> 10) & 1023) - 512, ((c >> 20) & 1023) - 512, sign, cell);
     return dx * dx + dy * dy + dz * dz;
   }
   // Whether entry e of atom i is the pair's minimum image (masks apply only there).
@@ -363,7 +432,7 @@ struct Oracle {
   void setup(const ffxg_system *s, const ffxg_params *prm, const double *xyz) {
     n = s->n_atoms;
     p = *prm;
-    cell = make_cell(p.box);
+    cell = make_cell(p.box, p.angles);
     x.resize(n); y.resize(n); z.resize(n);
     for (int i = 0; i < n; i++) { x[i] = xyz[3 * i]; y[i] = xyz[3 * i + 1]; z[i] = xyz[3 * i + 2]; }
     lmp.assign(s->multipole, s->multipole + 10 * (size_t)n);
@@ -406,7 +475,7 @@ struct Oracle {
     const double maxcut = std::max(std::max(p.vdw_cutoff, p.ewald_cutoff), p.precond_cutoff);
     multi_image = g_force_images != 0;
     for (int d = 0; d < 3; d++)
-      if (p.box[d] <= 2.0 * maxcut) multi_image = true;
+      if (cell.width[d] <= 2.0 * maxcut) multi_image = true;
     setup_recip();
   }
 
@@ -431,34 +500,56 @@ struct Oracle {
 
   // Multi-image list: every image k + n L (k >= i; n > 0 in (z, y, x) lexicographic order
   // for k == i) within the buffered cutoff.  n runs over n0 + m, n0 the minimum-image
-  // shift of the raw difference and |m_d| <= floor(rlist / L_d + 1/2), which covers every
-  // image inside rlist.  Brute force over atom pairs: boxes this small hold few atoms.
+  // shift of the raw difference and |m_d| <= floor(rlist / w_d + 1/2) (w_d the
+  // perpendicular width), which covers every image inside rlist.  Brute force over atom
+  // pairs: boxes this small hold few atoms.
+  //
+  // The primary image of a pair (the one the bonded masks apply to) is the reference's
+  // iSymm = 0 pair: the minimum image in its replicate supercell of l x m x n unit cells,
+  // the smallest counts whose interfacial radii (half the perpendicular widths) reach the
+  // buffered cutoff (ReplicatesCrystal.replicatesCrystalFactory, C/ReplicatesCrystal.java:
+  // 172-202).  For the covalent partners of a whole molecule that is the molecule's own
+  // geometry even when the unit cell is narrower than the molecule.
   void build_list_images(const std::vector<double> &rx, const std::vector<double> &ry,
                          const std::vector<double> &rz, double rlist) {
     const double rl2 = rlist * rlist;
-    const int R[3] = {(int)std::floor(rlist / cell.a + 0.5), (int)std::floor(rlist / cell.b + 0.5),
-                      (int)std::floor(rlist / cell.c + 0.5)};
+    const int R[3] = {(int)std::floor(rlist / cell.width[0] + 0.5), (int)std::floor(rlist / cell.width[1] + 0.5),
+                      (int)std::floor(rlist / cell.width[2] + 0.5)};
+    int rep[3];
+    double sbox[3];
+    for (int d = 0; d < 3; d++) {
+      rep[d] = 1;
+      while (cell.width[d] / 2.0 * rep[d] < rlist) rep[d]++;
+    }
+    sbox[0] = cell.a * rep[0]; sbox[1] = cell.b * rep[1]; sbox[2] = cell.c * rep[2];
+    const Cell super = make_cell(sbox, p.angles);
     nlist.assign(n, {});
     nsh.assign(n, {});
 #pragma omp parallel for schedule(dynamic, 16)
     for (int i = 0; i < n; i++) {
       for (int k = i; k < n; k++) {
         const double dx = rx[k] - rx[i], dy = ry[k] - ry[i], dz = rz[k] - rz[i];
-        const double fx = dx * cell.A00, fy = dy * cell.A11, fz = dz * cell.A22;
+        double fx, fy, fz;
+        to_frac(dx, dy, dz, cell, fx, fy, fz);
         const int n0x = (int)(std::floor(std::fabs(fx) + 0.5) * jsignum(-fx));
         const int n0y = (int)(std::floor(std::fabs(fy) + 0.5) * jsignum(-fy));
         const int n0z = (int)(std::floor(std::fabs(fz) + 0.5) * jsignum(-fz));
+        double sx, sy, sz;
+        to_frac(dx, dy, dz, super, sx, sy, sz);
+        const int px = rep[0] * (int)(std::floor(std::fabs(sx) + 0.5) * jsignum(-sx));
+        const int py = rep[1] * (int)(std::floor(std::fabs(sy) + 0.5) * jsignum(-sy));
+        const int pz = rep[2] * (int)(std::floor(std::fabs(sz) + 0.5) * jsignum(-sz));
         for (int mz = -R[2]; mz <= R[2]; mz++)
           for (int my = -R[1]; my <= R[1]; my++)
             for (int mx = -R[0]; mx <= R[0]; mx++) {
               const int nx = n0x + mx, ny = n0y + my, nz = n0z + mz;
               if (k == i && !(nz > 0 || (nz == 0 && (ny > 0 || (ny == 0 && nx > 0))))) continue;
-              const double ex = dx + (double)nx * cell.a, ey = dy + (double)ny * cell.b,
-                           ez = dz + (double)nz * cell.c;
+              double ex = dx, ey = dy, ez = dz;
+              add_shift(ex, ey, ez, nx, ny, nz, 1.0, cell);
               const double d2 = ex * ex + ey * ey + ez * ez;
               if (d2 <= rl2) {
                 nlist[i].push_back(k);
-                nsh[i].push_back(pack_shift(nx, ny, nz, mx == 0 && my == 0 && mz == 0));
+                nsh[i].push_back(pack_shift(nx, ny, nz, nx == px && ny == py && nz == pz));
               }
             }
       }
@@ -475,12 +566,13 @@ struct Oracle {
       return;
     }
     // Cells at least rlist/2 wide; search +-2 cells (nEdge = 2, NeighborList.java:1296-1345).
-    const int nca = std::max(1, (int)std::floor(cell.a / (rlist * 0.5)));
-    const int ncb = std::max(1, (int)std::floor(cell.b / (rlist * 0.5)));
-    const int ncc = std::max(1, (int)std::floor(cell.c / (rlist * 0.5)));
+    const int nca = std::max(1, (int)std::floor(cell.width[0] / (rlist * 0.5)));
+    const int ncb = std::max(1, (int)std::floor(cell.width[1] / (rlist * 0.5)));
+    const int ncc = std::max(1, (int)std::floor(cell.width[2] / (rlist * 0.5)));
     std::vector<std::vector<int>> cells((size_t)nca * ncb * ncc);
     auto cidx = [&](int i, int &ca, int &cb, int &cc) {
-      double fx = rx[i] * cell.A00, fy = ry[i] * cell.A11, fz = rz[i] * cell.A22;
+      double fx, fy, fz;
+      to_frac(rx[i], ry[i], rz[i], cell, fx, fy, fz);
       fx -= std::floor(fx); fy -= std::floor(fy); fz -= std::floor(fz);
       ca = std::min(nca - 1, (int)(fx * nca));
       cb = std::min(ncb - 1, (int)(fy * ncb));

@@ -75,6 +75,33 @@ def build(ref_root, name, xyz_file, key_file, prm):
                 frames={str(f): int((system.frame == f).sum()) for f in range(6)})
 
 
+def build_crystal(ref_root, name):
+    """A small-molecule crystal of EnergyTest (its .xyz asymmetric unit, .properties keys and
+    the .patch parameter file they name): cell edges and angles, space group, cutoffs; the
+    Ewald coefficient is the key's or the reference's default 0.545 (EwaldParameters.java:70),
+    the PME mesh ReciprocalSpace.initConvolution's on the unit cell (ReciprocalSpace.java:
+    909-975)."""
+    res = os.path.join(ref_root, RES)
+    key = read_key(os.path.join(res, f"{name}.properties"))
+    prm = read_prm(os.path.join(res, key["parameters"][0]))
+    xyz, types, bonds = read_xyz(os.path.join(res, f"{name}.xyz"))
+    system = system_from_types(xyz, types, bonds, prm)
+    system.save_npz(os.path.join(HERE, f"{name}_system.npz"))
+    box = [float(key["a-axis"][0]), float(key.get("b-axis", key["a-axis"])[0]),
+           float(key.get("c-axis", key["a-axis"])[0])]
+    angles = [float(key.get(a, ["90.0"])[0]) for a in ("alpha", "beta", "gamma")]
+    density = float(key.get("pme-mesh-density", ["1.2"])[0])
+    keys = dict(box=box, angles=angles, vdw_cutoff=float(key["vdw-cutoff"][0]),
+                ewald_cutoff=float(key["ewald-cutoff"][0]),
+                ewald_alpha=float(key.get("ewald-alpha", ["0.545"])[0]), pme_order=5,
+                pme_grid=[pme_grid_dim(b, density) for b in box],
+                polar_eps=float(key.get("polar-eps", ["1e-6"])[0]))
+    return dict(keys=keys, golden=golden_from_energy_test(os.path.join(ref_root, ENERGY_TEST), f"{name}.xyz"),
+                n_atoms=system.n_atoms, space_group=space_group(key))
+
+
+CRYSTALS = ("methylparaben", "paracetamol", "phenacetin", "ethylparaben", "acetanilide")
+
 ERF_TEST = "modules/numerics/src/test/java/ffx/numerics/special/ErfTest.java"
 BSPLINE_TEST = "modules/numerics/src/test/java/ffx/numerics/spline/UniformBSplineTest.java"
 
@@ -113,6 +140,10 @@ def main():
     prm_protein = read_prm(os.path.join(ref_root, PRM_PROTEIN))
     out["snare"] = build(ref_root, "snare", "1n7s.P212121.xyz", "1n7s.P212121.key", prm_protein)
     print("snare", json.dumps(out["snare"]))
+    # Small-molecule crystals in P21/c (monoclinic cells) and Pbca (EnergyTest.java:437-616).
+    for name in CRYSTALS:
+        out[name] = build_crystal(ref_root, name)
+        print(name, json.dumps(out[name]))
     out["numerics"] = numerics_known_answers(ref_root)
     print("numerics", len(out["numerics"]["erf"]), "erf cases,", len(out["numerics"]["bspline"]), "bspline cases")
     with open(os.path.join(HERE, "fixtures.json"), "w") as f:

@@ -140,7 +140,7 @@ def test_bad_boundary_arguments():
             ffe.set_crystal(-1.0)
         assert ei.value.status == 1
         with pytest.raises(EnergyException) as ei:
-            ffe.set_crystal(12.4, (22, 16, 16))
+            ffe.set_crystal(12.4, (4, 16, 16))           # a mesh shorter than the B-spline order
         assert ei.value.status == 1
         w = water_box(5, 15.5, seed=2)
         with pytest.raises(EnergyException) as ei:

@@ -135,10 +135,29 @@ def test_error_status_codes():
         with pytest.raises(EnergyException) as ei:
             ffe.energy(x)
         assert ei.value.status == 5                                       # NONFINITE
-    p = water_params(18.643, vdw_cutoff=7.0, ewald_cutoff=7.0, pme_grid=(20, 20, 22))
+    p = water_params(18.643, vdw_cutoff=7.0, ewald_cutoff=7.0, pme_grid=(20, 20, 4))
     with pytest.raises(EnergyException) as ei:
-        ForceFieldEnergy(s, p)                                            # 22 = 2 * 11: radix 11 unsupported
+        ForceFieldEnergy(s, p)                                            # a mesh shorter than the B-spline order
     assert ei.value.status == 1
+
+
+@pytest.mark.parametrize("precision", [0, 1])
+def test_mesh_with_prime_factors_above_seven(precision):
+    """Mesh lengths 22 = 2 x 11, 26 = 2 x 13 and 33 = 3 x 11 take the general radix pass, as
+    the reference's Complex transforms any length (Complex.java:173-330)."""
+    s = water_box(6, 18.643, seed=61)
+    p = water_params(18.643, vdw_cutoff=7.0, ewald_cutoff=7.0, pme_grid=(22, 26, 33), precision=precision)
+    if precision == 0:
+        compare(s, p, check_pairs=False)
+        return
+    # Mixed form: this box's total cancels to ~50 kcal/mol, so the terms are held to 1e-5 of
+    # the largest term's magnitude, the gradient to the mixed bar's 1e-3 RMS.
+    ref = ob.energy(s, p)
+    with ForceFieldEnergy(s, p) as ffe:
+        e, g = ffe.energy_and_gradient(s.xyz)
+        terms = ffe.terms.copy()
+    assert np.abs(terms - ref["terms"]).max() < 1e-5 * np.abs(ref["terms"]).max(), (terms, ref["terms"])
+    assert float(np.sqrt(np.mean((g - ref["grad"]) ** 2))) < 1e-3
 
 
 @pytest.mark.parametrize("precision", [0, 1])

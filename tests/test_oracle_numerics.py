@@ -31,7 +31,9 @@ def test_fft_round_trip(shape):
     assert np.max(np.abs(back - data)) < 1e-14
 
 
-def test_fft_matches_numpy():
+@pytest.mark.parametrize("shape", [(20, 21, 28), (33, 26, 22), (13, 17, 11)])
+def test_fft_matches_numpy(shape):
+    """Including lengths with prime factors above 7 (the general pass)."""
     rng = np.random.default_rng(8)
-    data = rng.random((20, 21, 28)) + 1j * rng.random((20, 21, 28))
+    data = rng.random(shape) + 1j * rng.random(shape)
     assert np.allclose(ob.fft3d(data, -1), np.fft.fftn(data), atol=1e-11)

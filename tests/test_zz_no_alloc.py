@@ -80,6 +80,10 @@ def test_no_alloc_odd_mesh():
     _check(7, 21.7, (45, 27, 35), 37, False)
 
 
+def test_no_alloc_mesh_with_prime_factors_above_seven():
+    _check(7, 21.7, (22, 26, 33), 39, False)     # 2 x 11, 2 x 13, 3 x 11: the general radix pass
+
+
 def test_no_alloc_non_cubic_mesh_at_the_limit_on_a_user_stream():
     _check(21, 65.184, (64, 48, 60), 41, True)     # 9,261 waters: 27,783 atoms
 
@@ -92,4 +96,4 @@ def test_no_alloc_rejects_sizes_beyond_its_maximum():
     ptr = d.data_ptr()
     assert _call(lib, ptr, ptr, 40000, (40.0, 40.0, 40.0), (32, 32, 32), 0.545, 332.0637133, 0, ptr) == 6
     assert _call(lib, ptr, ptr, 100, (40.0, 40.0, 40.0), (80, 32, 32), 0.545, 332.0637133, 0, ptr) == 6
-    assert _call(lib, ptr, ptr, 100, (40.0, 40.0, 40.0), (22, 32, 32), 0.545, 332.0637133, 0, ptr) == 1
+    assert _call(lib, ptr, ptr, 100, (40.0, 40.0, 40.0), (4, 32, 32), 0.545, 332.0637133, 0, ptr) == 1
