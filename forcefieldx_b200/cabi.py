@@ -78,7 +78,7 @@ PROTOTYPES = {
     "ffxg_destroy": (None, [ctypes.c_void_p]),
     "ffxg_last_error": (ctypes.c_char_p, [ctypes.c_void_p]),
     "ffxg_set_coordinates": (ctypes.c_int, [ctypes.c_void_p, _D]),
-    "ffxg_set_box": (ctypes.c_int, [ctypes.c_void_p, _D, _I]),
+    "ffxg_set_box": (ctypes.c_int, [ctypes.c_void_p, _D, _D, _I]),
     "ffxg_update_parameters": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(FfxgSystem)]),
     "ffxg_energy": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, _D, _D, _L]),
     "ffxg_energy_and_gradient": (ctypes.c_int, [ctypes.c_void_p, _D, _D, _D, _L]),

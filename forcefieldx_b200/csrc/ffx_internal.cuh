@@ -64,30 +64,73 @@ struct ScaleTables {
   double v[4];   // 1, v12, v13, v14
 };
 
-// Cell / Crystal description for the device (orthorhombic; the general
-// fractional round trip of Crystal.image is kept term by term).
+// Cell / Crystal description for the device: the rows of A^-1 are the lattice vectors
+// (a, 0, 0), (b cos g, b sin g, 0), (c cos b, c beta_term, c gamma_term) and A their inverse
+// (Crystal.updateCrystal, C/Crystal.java:1428-1548).  tric == 0 (every angle 90) keeps the
+// diagonal arithmetic of the orthorhombic cell; otherwise Crystal.image's general
+// fractional round trip is kept term by term.
 struct Box {
   double a, b, c;
-  double A00, A11, A22;    // 1/a, 1/b, 1/c
-  double Ai00, Ai11, Ai22; // a, b, c
+  double A00, A11, A22;    // 1/a, 1/b, 1/c when orthorhombic
+  double Ai00, Ai11, Ai22; // a, b, c when orthorhombic
   double volume;
+  double A10, A20, A21;    // off-diagonal terms of A (lower triangular)
+  double Ai10, Ai20, Ai21; // off-diagonal terms of A^-1 (lower triangular)
+  int tric;
 };
 
 // Minimum image exactly as Crystal.image (Crystal.java:1069-1083): no FMA
 // contraction, Java signum semantics, same operation order.
 __device__ __forceinline__ double jsignum(double v) { return v > 0.0 ? 1.0 : (v < 0.0 ? -1.0 : v); }
 
+// Fractional coordinates x A in Crystal.image's operation order.
+__device__ __forceinline__ void to_frac(double x, double y, double z, const Box &bx, double &xf, double &yf,
+                                        double &zf) {
+  if (!bx.tric) {
+    xf = __dmul_rn(x, bx.A00);
+    yf = __dmul_rn(y, bx.A11);
+    zf = __dmul_rn(z, bx.A22);
+    return;
+  }
+  xf = __dadd_rn(__dadd_rn(__dmul_rn(x, bx.A00), __dmul_rn(y, bx.A10)), __dmul_rn(z, bx.A20));
+  yf = __dadd_rn(__dmul_rn(y, bx.A11), __dmul_rn(z, bx.A21));
+  zf = __dmul_rn(z, bx.A22);
+}
+
 __device__ __forceinline__ double image_exact(double &x, double &y, double &z, const Box &bx) {
-  double xf = __dmul_rn(x, bx.A00);
-  double yf = __dmul_rn(y, bx.A11);
-  double zf = __dmul_rn(z, bx.A22);
+  double xf, yf, zf;
+  to_frac(x, y, z, bx, xf, yf, zf);
   xf = __dadd_rn(__dmul_rn(floor(__dadd_rn(fabs(xf), 0.5)), jsignum(-xf)), xf);
   yf = __dadd_rn(__dmul_rn(floor(__dadd_rn(fabs(yf), 0.5)), jsignum(-yf)), yf);
   zf = __dadd_rn(__dmul_rn(floor(__dadd_rn(fabs(zf), 0.5)), jsignum(-zf)), zf);
-  x = __dmul_rn(xf, bx.Ai00);
-  y = __dmul_rn(yf, bx.Ai11);
-  z = __dmul_rn(zf, bx.Ai22);
+  if (!bx.tric) {
+    x = __dmul_rn(xf, bx.Ai00);
+    y = __dmul_rn(yf, bx.Ai11);
+    z = __dmul_rn(zf, bx.Ai22);
+  } else {
+    x = __dadd_rn(__dadd_rn(__dmul_rn(xf, bx.Ai00), __dmul_rn(yf, bx.Ai10)), __dmul_rn(zf, bx.Ai20));
+    y = __dadd_rn(__dmul_rn(yf, bx.Ai11), __dmul_rn(zf, bx.Ai21));
+    z = __dmul_rn(zf, bx.Ai22);
+  }
   return __dadd_rn(__dadd_rn(__dmul_rn(x, x), __dmul_rn(y, y)), __dmul_rn(z, z));
+}
+
+// The lattice translation sign * (n A^-1) added to a displacement, in the oracle's order.
+__device__ __forceinline__ void add_shift(double &x, double &y, double &z, int nx, int ny, int nz, double sign,
+                                          const Box &bx) {
+  if (!bx.tric) {
+    x = __dadd_rn(x, sign * __dmul_rn((double)nx, bx.Ai00));
+    y = __dadd_rn(y, sign * __dmul_rn((double)ny, bx.Ai11));
+    z = __dadd_rn(z, sign * __dmul_rn((double)nz, bx.Ai22));
+    return;
+  }
+  const double sx = __dadd_rn(__dadd_rn(__dmul_rn((double)nx, bx.Ai00), __dmul_rn((double)ny, bx.Ai10)),
+                              __dmul_rn((double)nz, bx.Ai20));
+  const double sy = __dadd_rn(__dmul_rn((double)ny, bx.Ai11), __dmul_rn((double)nz, bx.Ai21));
+  const double sz = __dmul_rn((double)nz, bx.Ai22);
+  x = __dadd_rn(x, sign * sx);
+  y = __dadd_rn(y, sign * sy);
+  z = __dadd_rn(z, sign * sz);
 }
 
 // Multi-image lists (boxes at most twice an interaction cutoff; the reference's
@@ -105,9 +148,7 @@ __device__ __forceinline__ double pair_image(double &x, double &y, double &z, co
                                              const int *__restrict__ sh, size_t e, double sign) {
   if (sh == nullptr) return image_exact(x, y, z, bx);
   const int c = sh[e];
-  x = __dadd_rn(x, sign * __dmul_rn((double)((c & 1023) - 512), bx.Ai00));
-  y = __dadd_rn(y, sign * __dmul_rn((double)(((c >> 10) & 1023) - 512), bx.Ai11));
-  z = __dadd_rn(z, sign * __dmul_rn((double)(((c >> 20) & 1023) - 512), bx.Ai22));
+  add_shift(x, y, z, (c & 1023) - 512, ((c >> 10) & 1023) - 512, ((c >> 20) & 1023) - 512, sign, bx);
   return __dadd_rn(__dadd_rn(__dmul_rn(x, x), __dmul_rn(y, y)), __dmul_rn(z, z));
 }
 
@@ -364,6 +405,9 @@ struct Handle {
   bool images = false;
   int image_mode = 0;                                // FFXG_IMAGES_AUTO / FFXG_IMAGES_ALL
   int img_range[3] = {0, 0, 0};                      // |n - n0| bound per axis of the builder
+  int img_rep[3] = {1, 1, 1};                        // replicate supercell whose minimum image is primary
+  Box img_super{};                                   // that supercell
+  double width[3] = {0, 0, 0};                       // perpendicular widths of the cell
   int *d_nbr_sh = nullptr, *d_ewl_sh = nullptr;
   // Cached dipole-field pairs of the Ewald and preconditioner rows (PairRec + B), sized
   // for the FP64 records; the mixed form uses the leading half.

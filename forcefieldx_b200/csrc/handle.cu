@@ -118,19 +118,70 @@ static int alloc_lists(Handle &h) {
 
 static int round32(double v) { return ((int)std::ceil(v) + 31) / 32 * 32; }
 
-// The orthorhombic cell of Crystal (a, b, c; A = 1 / edges; volume).
-static void set_cell(Handle &h, const double box[3]) {
-  for (int d = 0; d < 3; d++) h.prm.box[d] = box[d];
-  h.box.a = box[0]; h.box.b = box[1]; h.box.c = box[2];
-  h.box.A00 = 1.0 / h.box.a; h.box.A11 = 1.0 / h.box.b; h.box.A22 = 1.0 / h.box.c;
-  h.box.Ai00 = h.box.a; h.box.Ai11 = h.box.b; h.box.Ai22 = h.box.c;
-  h.box.volume = h.box.a * h.box.b * h.box.c;
+// Crystal.updateCrystal (C/Crystal.java:1428-1548): lattice vectors as the rows of A^-1,
+// A their inverse (lower triangular: closed form), the volume and the perpendicular widths
+// 1 / |a*_d|, by the orthorhombic, monoclinic (only beta differs from 90) and general
+// branches.  Angles of 0 read as 90.
+static Box make_box(const double box[3], const double angles[3], double width[3]) {
+  Box b{};
+  b.a = box[0]; b.b = box[1]; b.c = box[2];
+  double ang[3];
+  for (int d = 0; d < 3; d++) ang[d] = (angles[d] > 0.0) ? angles[d] : 90.0;
+  if (ang[0] == 90.0 && ang[1] == 90.0 && ang[2] == 90.0) {
+    b.A00 = 1.0 / b.a; b.A11 = 1.0 / b.b; b.A22 = 1.0 / b.c;
+    b.Ai00 = b.a; b.Ai11 = b.b; b.Ai22 = b.c;
+    b.volume = b.a * b.b * b.c;
+    b.tric = 0;
+    width[0] = b.a; width[1] = b.b; width[2] = b.c;
+    return b;
+  }
+  const double deg = 0.017453292519943295;   // Math.toRadians
+  double cos_alpha, sin_beta, cos_beta, sin_gamma, cos_gamma, beta_term, gamma_term;
+  if (ang[0] == 90.0 && ang[2] == 90.0) {
+    cos_alpha = 0.0; sin_beta = std::sin(ang[1] * deg); cos_beta = std::cos(ang[1] * deg);
+    sin_gamma = 1.0; cos_gamma = 0.0; beta_term = 0.0; gamma_term = sin_beta;
+    b.volume = sin_beta * b.a * b.b * b.c;
+  } else {
+    cos_alpha = std::cos(ang[0] * deg); sin_beta = std::sin(ang[1] * deg); cos_beta = std::cos(ang[1] * deg);
+    sin_gamma = std::sin(ang[2] * deg); cos_gamma = std::cos(ang[2] * deg);
+    beta_term = (cos_alpha - cos_beta * cos_gamma) / sin_gamma;
+    gamma_term = std::sqrt(sin_beta * sin_beta - beta_term * beta_term);
+    b.volume = sin_gamma * gamma_term * b.a * b.b * b.c;
+  }
+  b.Ai00 = b.a;
+  b.Ai10 = b.b * cos_gamma; b.Ai11 = b.b * sin_gamma;
+  b.Ai20 = b.c * cos_beta; b.Ai21 = b.c * beta_term; b.Ai22 = b.c * gamma_term;
+  b.A00 = 1.0 / b.Ai00; b.A11 = 1.0 / b.Ai11; b.A22 = 1.0 / b.Ai22;
+  b.A10 = -b.Ai10 / (b.Ai00 * b.Ai11);
+  b.A21 = -b.Ai21 / (b.Ai11 * b.Ai22);
+  b.A20 = (b.Ai10 * b.Ai21 - b.Ai11 * b.Ai20) / (b.Ai00 * b.Ai11 * b.Ai22);
+  b.tric = 1;
+  width[0] = 1.0 / std::sqrt(b.A00 * b.A00 + b.A10 * b.A10 + b.A20 * b.A20);
+  width[1] = 1.0 / std::sqrt(b.A11 * b.A11 + b.A21 * b.A21);
+  width[2] = 1.0 / std::fabs(b.A22);
+  return b;
 }
 
-// Cells of the list builder: edges of at least half the buffered cutoff.
+static bool angles_ok(const double angles[3]) {
+  for (int d = 0; d < 3; d++) {
+    const double v = angles[d] > 0.0 ? angles[d] : 90.0;
+    if (!(v > 0.0 && v < 180.0)) return false;
+  }
+  return true;
+}
+
+static void set_cell(Handle &h, const double box[3], const double angles[3]) {
+  for (int d = 0; d < 3; d++) {
+    h.prm.box[d] = box[d];
+    h.prm.angles[d] = angles[d];
+  }
+  h.box = make_box(box, angles, h.width);
+}
+
+// Cells of the list builder: fractional slabs at least half the buffered cutoff wide.
 static void set_cell_grid(Handle &h) {
   const double rlist = std::max(h.prm.vdw_cutoff, h.prm.ewald_cutoff) + h.prm.list_buffer;
-  for (int d = 0; d < 3; d++) h.ncell[d] = std::max(1, (int)std::floor(h.prm.box[d] / (rlist * 0.5)));
+  for (int d = 0; d < 3; d++) h.ncell[d] = std::max(1, (int)std::floor(h.width[d] / (rlist * 0.5)));
 }
 
 // Charge correction of a charged cell, -1/2 electric pi q^2 / (V alpha^2)
@@ -167,16 +218,25 @@ static double near_radius(const Handle &h) {
 }
 
 // Multi-image mode and the shift range of its list builder: |n_d - n0_d| <=
-// floor(rlist / L_d + 1/2), n0 the minimum-image shift, covers every image within rlist.
+// floor(rlist / w_d + 1/2), n0 the minimum-image shift and w_d the perpendicular width,
+// covers every image within rlist.  The primary image of a pair (the one the bonded masks
+// apply to) is the minimum image in the replicate supercell of the reference
+// (ReplicatesCrystal.replicatesCrystalFactory, C/ReplicatesCrystal.java:172-202: the
+// smallest counts whose interfacial radii, half the widths, reach rlist).
 static void configure_images(Handle &h) {
   const ffxg_params *p = &h.prm;
   const double rcut = std::max(std::max(p->vdw_cutoff, p->ewald_cutoff), p->precond_cutoff);
   const double rlist = std::max(p->vdw_cutoff, p->ewald_cutoff) + p->list_buffer;
   h.images = h.image_mode == FFXG_IMAGES_ALL;
+  double sbox[3], sw[3];
   for (int d = 0; d < 3; d++) {
-    if (p->box[d] <= 2.0 * rcut) h.images = true;
-    h.img_range[d] = (int)std::floor(rlist / p->box[d] + 0.5);
+    if (h.width[d] <= 2.0 * rcut) h.images = true;
+    h.img_range[d] = (int)std::floor(rlist / h.width[d] + 0.5);
+    h.img_rep[d] = 1;
+    while (h.width[d] / 2.0 * h.img_rep[d] < rlist) h.img_rep[d]++;
+    sbox[d] = p->box[d] * h.img_rep[d];
   }
+  h.img_super = make_box(sbox, p->angles, sw);
   h.near_list = !h.images && !h.vacuum && near_radius(h) < rlist;
 }
 
@@ -221,6 +281,7 @@ static int create_impl(const ffxg_system *s, const ffxg_params *p, Handle &h) {
   }
   copy_system(s, h.sys);
   if (p->pme_order != kOrder) { h.err = "only pme-order 5 is supported"; return FFXG_ERR_BAD_ARG; }
+  if (!angles_ok(p->angles)) { h.err = "cell angles must lie in (0, 180) degrees"; return FFXG_ERR_BAD_ARG; }
   for (int d = 0; d < 3; d++) {
     if (!(p->box[d] > 0.0)) { h.err = "box edges must be positive"; return FFXG_ERR_BAD_ARG; }
     if (!fft_supported(p->pme_grid[d])) {
@@ -228,6 +289,8 @@ static int create_impl(const ffxg_system *s, const ffxg_params *p, Handle &h) {
       return FFXG_ERR_BAD_ARG;
     }
   }
+  set_cell(h, p->box, p->angles);
+  if (!(h.box.volume > 0.0)) { h.err = "the cell angles give no volume"; return FFXG_ERR_BAD_ARG; }
   // ReplicatesCrystal (C/ReplicatesCrystal.java:172-202) switches to a supercell of
   // replicate cells when an edge is shorter than twice the buffered list cutoff.  While
   // every interaction cutoff stays below half of each edge, each pair has exactly one
@@ -272,7 +335,6 @@ static int create_impl(const ffxg_system *s, const ffxg_params *p, Handle &h) {
   CK(cudaEventCreateWithFlags(&h.ev_recip_fork, cudaEventDisableTiming));
   CK(cudaEventCreateWithFlags(&h.ev_recip_join, cudaEventDisableTiming));
 
-  set_cell(h, p->box);
 
   // ---- validate topology indices
   for (int i = 0; i < n; i++) {
@@ -1126,10 +1188,13 @@ static int setup_elec(Handle &h, const std::vector<int> &soft, const std::vector
 // Crystal change (ForceFieldEnergy.setCrystal, ForceFieldEnergy.java:2650-2666, which passes
 // it to VanDerWaals, ParticleMeshEwald.setCrystal :1262-1283 and ReciprocalSpace.setCrystal
 // :750-761 / initConvolution :909-1000).
-int ffxg_set_box(ffxg_handle *hh, const double box[3], const int32_t pme_grid[3]) {
+int ffxg_set_box(ffxg_handle *hh, const double box[3], const double angles[3], const int32_t pme_grid[3]) {
   if (!hh || !box) return FFXG_ERR_BAD_ARG;
   Handle &h = hh->h;
   if (h.vacuum) { h.err = "a vacuum sub-system has no cell"; return FFXG_ERR_BAD_ARG; }
+  const double right[3] = {90.0, 90.0, 90.0};
+  if (!angles) angles = right;
+  if (!angles_ok(angles)) { h.err = "cell angles must lie in (0, 180) degrees"; return FFXG_ERR_BAD_ARG; }
   for (int d = 0; d < 3; d++) {
     if (!(box[d] > 0.0) || !std::isfinite(box[d])) { h.err = "box edges must be positive"; return FFXG_ERR_BAD_ARG; }
     if (pme_grid && !fft_supported(pme_grid[d])) {
@@ -1139,7 +1204,16 @@ int ffxg_set_box(ffxg_handle *hh, const double box[3], const int32_t pme_grid[3]
   }
   CK(cudaStreamSynchronize(h.stream));   // nothing in flight reads the old tables
   const bool images_before = h.images, near_before = h.near_list;
-  set_cell(h, box);
+  const Box keep_box = h.box;
+  double keep_prm[6], keep_w[3];
+  for (int d = 0; d < 3; d++) { keep_prm[d] = h.prm.box[d]; keep_prm[3 + d] = h.prm.angles[d]; keep_w[d] = h.width[d]; }
+  set_cell(h, box, angles);
+  if (!(h.box.volume > 0.0)) {
+    h.box = keep_box;
+    for (int d = 0; d < 3; d++) { h.prm.box[d] = keep_prm[d]; h.prm.angles[d] = keep_prm[3 + d]; h.width[d] = keep_w[d]; }
+    h.err = "the cell angles give no volume";
+    return FFXG_ERR_BAD_ARG;
+  }
   configure_images(h);
   set_cell_grid(h);
   const int ncells = h.ncell[0] * h.ncell[1] * h.ncell[2];

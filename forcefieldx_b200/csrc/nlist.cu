@@ -60,8 +60,8 @@ __global__ void k_reduce_coordinates(int n, const double *__restrict__ x, const 
   if (!isfinite(vx) || !isfinite(vy) || !isfinite(vz)) atomicOr(flags, FLAG_NONFINITE);
 }
 
-__device__ __forceinline__ int cell_of(double v, double inv, int nc) {
-  double f = v * inv;
+// Cell index along one axis of a fractional coordinate f (wrapped into [0, 1)).
+__device__ __forceinline__ int cell_of(double f, int nc) {
   f = f - floor(f);
   int c = (int)(f * nc);
   return c < 0 ? 0 : (c >= nc ? nc - 1 : c);
@@ -73,7 +73,9 @@ __global__ void k_cell_count(int n, const double *__restrict__ rx, const double 
   if (!(*flags & FLAG_REBUILD)) return;
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
-  const int cx = cell_of(rx[i], bx.A00, ncx), cy = cell_of(ry[i], bx.A11, ncy), cz = cell_of(rz[i], bx.A22, ncz);
+  double fx, fy, fz;
+  to_frac(rx[i], ry[i], rz[i], bx, fx, fy, fz);
+  const int cx = cell_of(fx, ncx), cy = cell_of(fy, ncy), cz = cell_of(fz, ncz);
   const int c = (cz * ncy + cy) * ncx + cx;
   atom_cell[i] = c;
   atomicAdd(&cell_cnt[c], 1);
@@ -223,7 +225,8 @@ __global__ void k_verlet(int n, const double *__restrict__ rx, const double *__r
 // packed shift; the order (k chunk, then m) is fixed, so lists are reproducible.
 __global__ void k_verlet_images(int n, const double *__restrict__ rx, const double *__restrict__ ry,
                                 const double *__restrict__ rz, Box bx, int R0, int R1, int R2, double rl2,
-                                int cap, int *nbr, int *nbr_sh, int *nbr_cnt, int *flags) {
+                                int cap, int *nbr, int *nbr_sh, int *nbr_cnt, int *flags, Box super, int P0,
+                                int P1, int P2) {
   if (!(*flags & FLAG_REBUILD)) return;
   const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const int lane = threadIdx.x & 31;
@@ -237,19 +240,26 @@ __global__ void k_verlet_images(int n, const double *__restrict__ rx, const doub
     const int k = base + lane;
     const bool valid = k < n;
     double dx = 0.0, dy = 0.0, dz = 0.0;
-    int n0x = 0, n0y = 0, n0z = 0;
+    int n0x = 0, n0y = 0, n0z = 0, px = 0, py = 0, pz = 0;
     bool ok = valid;
     if (valid) {
       dx = __dsub_rn(rx[k], xi); dy = __dsub_rn(ry[k], yi); dz = __dsub_rn(rz[k], zi);
-      const double fx = __dmul_rn(dx, bx.A00), fy = __dmul_rn(dy, bx.A11), fz = __dmul_rn(dz, bx.A22);
+      double fx, fy, fz, sx, sy, sz;
+      to_frac(dx, dy, dz, bx, fx, fy, fz);
       const double gx = floor(__dadd_rn(fabs(fx), 0.5)) * jsignum(-fx);
       const double gy = floor(__dadd_rn(fabs(fy), 0.5)) * jsignum(-fy);
       const double gz = floor(__dadd_rn(fabs(fz), 0.5)) * jsignum(-fz);
+      // The primary image: the minimum image in the replicate supercell (P0 x P1 x P2 cells).
+      to_frac(dx, dy, dz, super, sx, sy, sz);
+      const double hx = floor(__dadd_rn(fabs(sx), 0.5)) * jsignum(-sx);
+      const double hy = floor(__dadd_rn(fabs(sy), 0.5)) * jsignum(-sy);
+      const double hz = floor(__dadd_rn(fabs(sz), 0.5)) * jsignum(-sz);
       if (fabs(gx) + R0 > 511.0 || fabs(gy) + R1 > 511.0 || fabs(gz) + R2 > 511.0) {
         atomicOr(flags, FLAG_IMAGE_RANGE);
         ok = false;
       } else {
         n0x = (int)gx; n0y = (int)gy; n0z = (int)gz;
+        px = P0 * (int)hx; py = P1 * (int)hy; pz = P2 * (int)hz;
       }
     }
     for (int mz = -R2; mz <= R2; mz++)
@@ -258,9 +268,8 @@ __global__ void k_verlet_images(int n, const double *__restrict__ rx, const doub
           const int nx = n0x + mx, ny = n0y + my, nz = n0z + mz;
           bool pass = false;
           if (ok && !(k == i && nx == 0 && ny == 0 && nz == 0)) {
-            const double ex = __dadd_rn(dx, __dmul_rn((double)nx, bx.Ai00));
-            const double ey = __dadd_rn(dy, __dmul_rn((double)ny, bx.Ai11));
-            const double ez = __dadd_rn(dz, __dmul_rn((double)nz, bx.Ai22));
+            double ex = dx, ey = dy, ez = dz;
+            add_shift(ex, ey, ez, nx, ny, nz, 1.0, bx);
             const double d2 = __dadd_rn(__dadd_rn(__dmul_rn(ex, ex), __dmul_rn(ey, ey)), __dmul_rn(ez, ez));
             pass = d2 <= rl2;
           }
@@ -269,7 +278,7 @@ __global__ void k_verlet_images(int n, const double *__restrict__ rx, const doub
             const int pos = count + __popc(m & ((1u << lane) - 1u));
             if (pos < cap) {
               row[pos] = k;
-              rsh[pos] = pack_shift(nx, ny, nz, mx == 0 && my == 0 && mz == 0);
+              rsh[pos] = pack_shift(nx, ny, nz, nx == px && ny == py && nz == pz);
             }
           }
           count += __popc(m);
@@ -371,7 +380,7 @@ void launch_neighbor_list(Handle &h, bool force) {
   if (h.images) {
     k_verlet_images<<<nblocks((int64_t)n * 32, 256), 256, 0, h.stream>>>(
         n, h.d_rx, h.d_ry, h.d_rz, h.box, h.img_range[0], h.img_range[1], h.img_range[2], rl * rl, h.cap_nbr,
-        h.d_nbr, h.d_nbr_sh, h.d_nbr_cnt, h.d_flags);
+        h.d_nbr, h.d_nbr_sh, h.d_nbr_cnt, h.d_flags, h.img_super, h.img_rep[0], h.img_rep[1], h.img_rep[2]);
     k_list_done<<<nblocks(n, 256), 256, 0, h.stream>>>(n, h.d_refx, h.d_refy, h.d_refz, h.d_rx, h.d_ry, h.d_rz,
                                                         h.d_flags);
     h.launches += 2;

@@ -902,7 +902,8 @@ int setup_pme(Handle &h) {
   const int nfx = h.prm.pme_grid[0], nfy = h.prm.pme_grid[1], nfz = h.prm.pme_grid[2];
   h.nfft[0] = nfx; h.nfft[1] = nfy; h.nfft[2] = nfz;
   const int nf[3] = {nfx, nfy, nfz};
-  const double A[3][3] = {{h.box.A00, 0, 0}, {0, h.box.A11, 0}, {0, 0, h.box.A22}};
+  // Crystal.A: lower triangular (zero off the diagonal for an orthorhombic cell).
+  const double A[3][3] = {{h.box.A00, 0, 0}, {h.box.A10, h.box.A11, 0}, {h.box.A20, h.box.A21, h.box.A22}};
   static const int qi1[6] = {0, 1, 2, 0, 0, 1};
   static const int qi2[6] = {0, 1, 2, 1, 2, 2};
   double a[3][3];

@@ -113,13 +113,17 @@ class ForceFieldEnergy:
         self._x = np.ascontiguousarray(np.asarray(x, dtype=np.float64).reshape(self.n, 3))
         self._check(self.lib.ffxg_set_coordinates(self._h, _dp(self._x)))
 
-    def set_crystal(self, box, pme_grid=None) -> None:
-        """New orthorhombic cell edges (and optionally PME mesh dimensions; None keeps the mesh)."""
+    def set_crystal(self, box, pme_grid=None, angles=None) -> None:
+        """A new cell: edges, optionally angles (alpha, beta, gamma; None: 90) and PME mesh
+        dimensions (None keeps the mesh)."""
         b = np.ascontiguousarray(np.broadcast_to(np.asarray(box, dtype=np.float64), (3,)))
+        ang = np.ascontiguousarray(angles if angles is not None else (90.0, 90.0, 90.0), dtype=np.float64)
         g = None if pme_grid is None else np.ascontiguousarray(pme_grid, dtype=np.int32)
-        self._check(self.lib.ffxg_set_box(self._h, _dp(b), g.ctypes.data_as(cabi._I) if g is not None else None))
+        self._check(self.lib.ffxg_set_box(self._h, _dp(b), _dp(ang),
+                                          g.ctypes.data_as(cabi._I) if g is not None else None))
         grid = tuple(self.params.grid()) if g is None else tuple(int(v) for v in g)
-        self.params = dataclasses.replace(self.params, box=tuple(float(v) for v in b), pme_grid=grid)
+        self.params = dataclasses.replace(self.params, box=tuple(float(v) for v in b), pme_grid=grid,
+                                          angles=tuple(float(v) for v in ang))
 
     def update_parameters(self, system: AmoebaSystem) -> None:
         """New multipole, polarization, damping, reduction and vdW-table values for the same

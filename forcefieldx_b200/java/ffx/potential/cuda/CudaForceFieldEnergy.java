@@ -49,12 +49,12 @@ public class CudaForceFieldEnergy extends ForceFieldEnergy {
   private final int nAtoms;
   private final boolean gpuLambda;
   private MemorySegment handle = MemorySegment.NULL;
-  private final MemorySegment xyz, grad, terms, counts, dEdL, d2EdL2, lambdaGrad, box3, systemStruct;
+  private final MemorySegment xyz, grad, terms, counts, dEdL, d2EdL2, lambdaGrad, box3, angles3, systemStruct;
   private STATE termState = STATE.BOTH;
 
   /**
-   * @param molecularAssembly the system (every atom active; one asymmetric unit in P1 or an
-   *                          orthorhombic cell).
+   * @param molecularAssembly the system (every atom active) in P1: a crystal's space-group mates
+   *                          are expanded into the P1 cell first.
    * @param nThreads          threads of the parent's bonded terms.
    */
   public CudaForceFieldEnergy(MolecularAssembly molecularAssembly, int nThreads) {
@@ -62,8 +62,8 @@ public class CudaForceFieldEnergy extends ForceFieldEnergy {
     atoms = molecularAssembly.getAtomArray();
     nAtoms = atoms.length;
     Crystal crystal = getCrystal();
-    if (crystal.spaceGroup.getNumberOfSymOps() > 1 || !orthorhombic(crystal)) {
-      throw new EnergyException(" libffxcuda takes an orthorhombic P1 cell (expand space groups first)");
+    if (crystal.spaceGroup.getNumberOfSymOps() > 1) {
+      throw new EnergyException(" libffxcuda takes a P1 cell (expand the space group's mates first)");
     }
     ForceField ff = molecularAssembly.getForceField();
     xyz = arena.allocate(JAVA_DOUBLE, 3L * nAtoms);
@@ -74,6 +74,7 @@ public class CudaForceFieldEnergy extends ForceFieldEnergy {
     dEdL = arena.allocate(JAVA_DOUBLE);
     d2EdL2 = arena.allocate(JAVA_DOUBLE);
     box3 = arena.allocate(JAVA_DOUBLE, 3);
+    angles3 = arena.allocate(JAVA_DOUBLE, 3);
     systemStruct = arena.allocate(FfxCuda.SYSTEM);
     fillSystem(systemStruct);
     MemorySegment params = arena.allocate(FfxCuda.PARAMS);
@@ -174,13 +175,14 @@ public class CudaForceFieldEnergy extends ForceFieldEnergy {
   @Override
   public void setCrystal(Crystal crystal) {
     super.setCrystal(crystal);
-    if (!orthorhombic(crystal)) {
-      throw new EnergyException(" libffxcuda takes an orthorhombic cell");
-    }
-    box3.setAtIndex(JAVA_DOUBLE, 0, crystal.a);
-    box3.setAtIndex(JAVA_DOUBLE, 1, crystal.b);
-    box3.setAtIndex(JAVA_DOUBLE, 2, crystal.c);
-    check(call(() -> (int) FfxCuda.SET_BOX.invokeExact(handle, box3, MemorySegment.NULL)));
+    Crystal unit = crystal.getUnitCell();
+    box3.setAtIndex(JAVA_DOUBLE, 0, unit.a);
+    box3.setAtIndex(JAVA_DOUBLE, 1, unit.b);
+    box3.setAtIndex(JAVA_DOUBLE, 2, unit.c);
+    angles3.setAtIndex(JAVA_DOUBLE, 0, unit.alpha);
+    angles3.setAtIndex(JAVA_DOUBLE, 1, unit.beta);
+    angles3.setAtIndex(JAVA_DOUBLE, 2, unit.gamma);
+    check(call(() -> (int) FfxCuda.SET_BOX.invokeExact(handle, box3, angles3, MemorySegment.NULL)));
   }
 
   @Override
@@ -309,10 +311,6 @@ public class CudaForceFieldEnergy extends ForceFieldEnergy {
     } catch (Throwable t) {
       throw new EnergyException(" libffxcuda call failed: " + t);
     }
-  }
-
-  private static boolean orthorhombic(Crystal c) {
-    return c.alpha == 90.0 && c.beta == 90.0 && c.gamma == 90.0;
   }
 
   // ---------------------------------------------------------------------------------------
@@ -445,10 +443,15 @@ public class CudaForceFieldEnergy extends ForceFieldEnergy {
   }
 
   private void fillParams(MemorySegment p, ForceField ff, Crystal crystal) {
+    Crystal unit = crystal.getUnitCell();
     MemorySegment boxSeg = p.asSlice(0, 24);
-    boxSeg.setAtIndex(JAVA_DOUBLE, 0, crystal.a);
-    boxSeg.setAtIndex(JAVA_DOUBLE, 1, crystal.b);
-    boxSeg.setAtIndex(JAVA_DOUBLE, 2, crystal.c);
+    boxSeg.setAtIndex(JAVA_DOUBLE, 0, unit.a);
+    boxSeg.setAtIndex(JAVA_DOUBLE, 1, unit.b);
+    boxSeg.setAtIndex(JAVA_DOUBLE, 2, unit.c);
+    MemorySegment angSeg = p.asSlice(232, 24);
+    angSeg.setAtIndex(JAVA_DOUBLE, 0, unit.alpha);
+    angSeg.setAtIndex(JAVA_DOUBLE, 1, unit.beta);
+    angSeg.setAtIndex(JAVA_DOUBLE, 2, unit.gamma);
     ParticleMeshEwald pme = getPmeNode();
     param("vdw_cutoff").set(p, 0L, ff.getDouble("VDW_CUTOFF", 12.0));
     param("vdw_taper").set(p, 0L, ff.getDouble("VDW_TAPER", 0.9));

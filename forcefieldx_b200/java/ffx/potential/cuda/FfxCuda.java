@@ -62,7 +62,7 @@ public final class FfxCuda {
       ADDRESS.withName("mask15_ptr"), ADDRESS.withName("mask15_idx"),
       ADDRESS.withName("ip11_ptr"), ADDRESS.withName("ip11_idx"));
 
-  /** ffxg_params, 232 bytes. */
+  /** ffxg_params, 256 bytes. */
   public static final StructLayout PARAMS = MemoryLayout.structLayout(
       MemoryLayout.sequenceLayout(3, JAVA_DOUBLE).withName("box"),
       JAVA_DOUBLE.withName("vdw_cutoff"), JAVA_DOUBLE.withName("vdw_taper"),
@@ -78,7 +78,8 @@ public final class FfxCuda {
       JAVA_DOUBLE.withName("p15"),
       JAVA_DOUBLE.withName("intra14"), JAVA_DOUBLE.withName("d11"),
       JAVA_DOUBLE.withName("v12"), JAVA_DOUBLE.withName("v13"), JAVA_DOUBLE.withName("v14"),
-      JAVA_INT.withName("precision"), MemoryLayout.paddingLayout(4));
+      JAVA_INT.withName("precision"), MemoryLayout.paddingLayout(4),
+      MemoryLayout.sequenceLayout(3, JAVA_DOUBLE).withName("angles"));
 
   /** ffxg_alchemy, 112 bytes. */
   public static final StructLayout ALCHEMY = MemoryLayout.structLayout(
@@ -103,9 +104,9 @@ public final class FfxCuda {
   // int ffxg_set_coordinates(ffxg_handle*, const double* xyz)
   public static final MethodHandle SET_COORDINATES = fn("ffxg_set_coordinates",
       FunctionDescriptor.of(JAVA_INT, ADDRESS, ADDRESS));
-  // int ffxg_set_box(ffxg_handle*, const double box[3], const int32_t pme_grid[3])
+  // int ffxg_set_box(ffxg_handle*, const double box[3], const double angles[3], const int32_t pme_grid[3])
   public static final MethodHandle SET_BOX = fn("ffxg_set_box",
-      FunctionDescriptor.of(JAVA_INT, ADDRESS, ADDRESS, ADDRESS));
+      FunctionDescriptor.of(JAVA_INT, ADDRESS, ADDRESS, ADDRESS, ADDRESS));
   // int ffxg_update_parameters(ffxg_handle*, const ffxg_system*)
   public static final MethodHandle UPDATE_PARAMETERS = fn("ffxg_update_parameters",
       FunctionDescriptor.of(JAVA_INT, ADDRESS, ADDRESS));

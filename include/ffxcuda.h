@@ -173,8 +173,9 @@ const char *ffxg_last_error(const ffxg_handle *h);
  * (ForceFieldEnergy.java:2629). */
 int ffxg_set_coordinates(ffxg_handle *h, const double *xyz);
 
-/* New orthorhombic cell edges box[3] (A), and, when pme_grid is not NULL, new PME mesh
- * dimensions (NULL keeps the mesh, as a pme-grid key does in the reference):
+/* A new cell: edges box[3] (A), angles[3] (alpha, beta, gamma in degrees; NULL: 90) and,
+ * when pme_grid is not NULL, new PME mesh dimensions (NULL keeps the mesh, as a pme-grid
+ * key does in the reference):
  * ForceFieldEnergy.setCrystal (ForceFieldEnergy.java:2650-2666), which passes the crystal to
  * ParticleMeshEwald.setCrystal (ParticleMeshEwald.java:1262-1283) and
  * ReciprocalSpace.setCrystal / initConvolution (ReciprocalSpace.java:750-761, 909-1000); the
@@ -182,7 +183,7 @@ int ffxg_set_coordinates(ffxg_handle *h, const double *xyz);
  * Rebuilds the PME tables and the charge correction; the next evaluation rebuilds the
  * neighbour list and captures its graph anew.  A barostat or lattice move needs no new
  * handle. */
-int ffxg_set_box(ffxg_handle *h, const double box[3], const int32_t pme_grid[3]);
+int ffxg_set_box(ffxg_handle *h, const double box[3], const double angles[3], const int32_t pme_grid[3]);
 
 /* New parameter values for the same atoms, topology and vdW types: sys->multipole,
  * polarizability, thole, pdamp, red_factor, vdw_inv_rmin and vdw_eps are read (the other
