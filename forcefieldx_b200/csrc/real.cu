@@ -414,49 +414,32 @@ __global__ void __launch_bounds__(128, sizeof(R) == 4 ? FFX_REAL_ENERGY_MIN_BLOC
       const R gl0 = ci * ck, gl1 = ck * sc3 - ci * sc4, gl2 = ci * sc6 + ck * sc5 - sc3 * sc4;
       const R gl3 = sc3 * sc6 - sc4 * sc5, gl4 = sc5 * sc6, gl5 = -R(4.0) * sc9, gl6 = sc2;
       const R gl7 = R(2.0) * (sc7 - sc8), gl8 = R(2.0) * sc10;
+      // The masked part (scale1 = 1 - scale of the Ewald-free tensor) enters every energy,
+      // force and torque expression linearly in the radial factors, so the combined factors
+      // b_k = bn_k - scale1 rr_(2k+1) give ereal - efix and the corrected forces and torques
+      // in one contraction (the reference evaluates the masked correction as a second pass).
       const R scale1 = R(1.0) - scale;
-      const R ereal = gl0 * bn0 + (gl1 + gl6) * bn1 + (gl2 + gl7 + gl8) * bn2 + (gl3 + gl5) * bn3 + gl4 * bn4;
-      const R efix = scale1 * (gl0 * rr1 + (gl1 + gl6) * rr3 + (gl2 + gl7 + gl8) * rr5 + (gl3 + gl5) * rr7 + gl4 * rr9);
-      const R e = ereal - efix;
+      const R b0 = bn0 - scale1 * rr1, b1 = bn1 - scale1 * rr3, b2 = bn2 - scale1 * rr5;
+      const R b3 = bn3 - scale1 * rr7, b4 = bn4 - scale1 * rr9, b5 = bn5 - scale1 * rr11;
+      const R e = gl0 * b0 + (gl1 + gl6) * b1 + (gl2 + gl7 + gl8) * b2 + (gl3 + gl5) * b3 + gl4 * b4;
       if (e != R(0.0)) { eP += (HALF ? R(1.0) : R(0.5)) * (LAM ? l2 * e : e); if (pair_counted(i, k, ewl_sh, ent)) cnt_pairs++; }
       if (gr) {
-        const R gf1 = bn1 * gl0 + bn2 * (gl1 + gl6) + bn3 * (gl2 + gl7 + gl8) + bn4 * (gl3 + gl5) + bn5 * gl4;
-        const R gf2 = -ck * bn1 + sc4 * bn2 - sc6 * bn3;
-        const R gf3 = ci * bn1 + sc3 * bn2 + sc5 * bn3;
-        const R gf4 = R(2.0) * bn2;
-        const R gf5 = R(2.0) * (-ck * bn2 + sc4 * bn3 - sc6 * bn4);
-        const R gf6 = R(2.0) * (-ci * bn2 - sc3 * bn3 - sc5 * bn4);
-        const R gf7 = R(4.0) * bn3;
-        R ftm2x = gf1 * xr + gf2 * dix + gf3 * dkx + gf4 * (qkdix - qidkx) + gf5 * qirx + gf6 * qkrx + gf7 * (qiqkrx + qkqirx);
-        R ftm2y = gf1 * yr + gf2 * diy + gf3 * dky + gf4 * (qkdiy - qidky) + gf5 * qiry + gf6 * qkry + gf7 * (qiqkry + qkqiry);
-        R ftm2z = gf1 * zr + gf2 * diz + gf3 * dkz + gf4 * (qkdiz - qidkz) + gf5 * qirz + gf6 * qkrz + gf7 * (qiqkrz + qkqirz);
-        R ttm2x = -bn1 * dixdkx + gf2 * dixrx + gf4 * (dixqkrx + dkxqirx + rxqidkx - R(2.0) * qixqkx) - gf5 * rxqirx - gf7 * (rxqikrx + qkrxqirx);
-        R ttm2y = -bn1 * dixdky + gf2 * dixry + gf4 * (dixqkry + dkxqiry + rxqidky - R(2.0) * qixqky) - gf5 * rxqiry - gf7 * (rxqikry + qkrxqiry);
-        R ttm2z = -bn1 * dixdkz + gf2 * dixrz + gf4 * (dixqkrz + dkxqirz + rxqidkz - R(2.0) * qixqkz) - gf5 * rxqirz - gf7 * (rxqikrz + qkrxqirz);
-        R ttm3x = bn1 * dixdkx + gf3 * dkxrx - gf4 * (dixqkrx + dkxqirx + rxqkdix - R(2.0) * qixqkx) - gf6 * rxqkrx - gf7 * (rxqkirx - qkrxqirx);
-        R ttm3y = bn1 * dixdky + gf3 * dkxry - gf4 * (dixqkry + dkxqiry + rxqkdiy - R(2.0) * qixqky) - gf6 * rxqkry - gf7 * (rxqkiry - qkrxqiry);
-        R ttm3z = bn1 * dixdkz + gf3 * dkxrz - gf4 * (dixqkrz + dkxqirz + rxqkdiz - R(2.0) * qixqkz) - gf6 * rxqkrz - gf7 * (rxqkirz - qkrxqirz);
-        if (scale1 != R(0.0)) {
-          const R gfr1 = rr3 * gl0 + rr5 * (gl1 + gl6) + rr7 * (gl2 + gl7 + gl8) + rr9 * (gl3 + gl5) + rr11 * gl4;
-          const R gfr2 = -ck * rr3 + sc4 * rr5 - sc6 * rr7;
-          const R gfr3 = ci * rr3 + sc3 * rr5 + sc5 * rr7;
-          const R gfr4 = R(2.0) * rr5;
-          const R gfr5 = R(2.0) * (-ck * rr5 + sc4 * rr7 - sc6 * rr9);
-          const R gfr6 = R(2.0) * (-ci * rr5 - sc3 * rr7 - sc5 * rr9);
-          const R gfr7 = R(4.0) * rr7;
-          const R ftm2rx = gfr1 * xr + gfr2 * dix + gfr3 * dkx + gfr4 * (qkdix - qidkx) + gfr5 * qirx + gfr6 * qkrx + gfr7 * (qiqkrx + qkqirx);
-          const R ftm2ry = gfr1 * yr + gfr2 * diy + gfr3 * dky + gfr4 * (qkdiy - qidky) + gfr5 * qiry + gfr6 * qkry + gfr7 * (qiqkry + qkqiry);
-          const R ftm2rz = gfr1 * zr + gfr2 * diz + gfr3 * dkz + gfr4 * (qkdiz - qidkz) + gfr5 * qirz + gfr6 * qkrz + gfr7 * (qiqkrz + qkqirz);
-          const R ttm2rx = -rr3 * dixdkx + gfr2 * dixrx + gfr4 * (dixqkrx + dkxqirx + rxqidkx - R(2.0) * qixqkx) - gfr5 * rxqirx - gfr7 * (rxqikrx + qkrxqirx);
-          const R ttm2ry = -rr3 * dixdky + gfr2 * dixry + gfr4 * (dixqkry + dkxqiry + rxqidky - R(2.0) * qixqky) - gfr5 * rxqiry - gfr7 * (rxqikry + qkrxqiry);
-          const R ttm2rz = -rr3 * dixdkz + gfr2 * dixrz + gfr4 * (dixqkrz + dkxqirz + rxqidkz - R(2.0) * qixqkz) - gfr5 * rxqirz - gfr7 * (rxqikrz + qkrxqirz);
-          const R ttm3rx = rr3 * dixdkx + gfr3 * dkxrx - gfr4 * (dixqkrx + dkxqirx + rxqkdix - R(2.0) * qixqkx) - gfr6 * rxqkrx - gfr7 * (rxqkirx - qkrxqirx);
-          const R ttm3ry = rr3 * dixdky + gfr3 * dkxry - gfr4 * (dixqkry + dkxqiry + rxqkdiy - R(2.0) * qixqky) - gfr6 * rxqkry - gfr7 * (rxqkiry - qkrxqiry);
-          const R ttm3rz = rr3 * dixdkz + gfr3 * dkxrz - gfr4 * (dixqkrz + dkxqirz + rxqkdiz - R(2.0) * qixqkz) - gfr6 * rxqkrz - gfr7 * (rxqkirz - qkrxqirz);
-          ftm2x -= scale1 * ftm2rx; ftm2y -= scale1 * ftm2ry; ftm2z -= scale1 * ftm2rz;
-          ttm2x -= scale1 * ttm2rx; ttm2y -= scale1 * ttm2ry; ttm2z -= scale1 * ttm2rz;
-          ttm3x -= scale1 * ttm3rx; ttm3y -= scale1 * ttm3ry; ttm3z -= scale1 * ttm3rz;
-        }
+        const R gf1 = b1 * gl0 + b2 * (gl1 + gl6) + b3 * (gl2 + gl7 + gl8) + b4 * (gl3 + gl5) + b5 * gl4;
+        const R gf2 = -ck * b1 + sc4 * b2 - sc6 * b3;
+        const R gf3 = ci * b1 + sc3 * b2 + sc5 * b3;
+        const R gf4 = R(2.0) * b2;
+        const R gf5 = R(2.0) * (-ck * b2 + sc4 * b3 - sc6 * b4);
+        const R gf6 = R(2.0) * (-ci * b2 - sc3 * b3 - sc5 * b4);
+        const R gf7 = R(4.0) * b3;
+        const R ftm2x = gf1 * xr + gf2 * dix + gf3 * dkx + gf4 * (qkdix - qidkx) + gf5 * qirx + gf6 * qkrx + gf7 * (qiqkrx + qkqirx);
+        const R ftm2y = gf1 * yr + gf2 * diy + gf3 * dky + gf4 * (qkdiy - qidky) + gf5 * qiry + gf6 * qkry + gf7 * (qiqkry + qkqiry);
+        const R ftm2z = gf1 * zr + gf2 * diz + gf3 * dkz + gf4 * (qkdiz - qidkz) + gf5 * qirz + gf6 * qkrz + gf7 * (qiqkrz + qkqirz);
+        const R ttm2x = -b1 * dixdkx + gf2 * dixrx + gf4 * (dixqkrx + dkxqirx + rxqidkx - R(2.0) * qixqkx) - gf5 * rxqirx - gf7 * (rxqikrx + qkrxqirx);
+        const R ttm2y = -b1 * dixdky + gf2 * dixry + gf4 * (dixqkry + dkxqiry + rxqidky - R(2.0) * qixqky) - gf5 * rxqiry - gf7 * (rxqikry + qkrxqiry);
+        const R ttm2z = -b1 * dixdkz + gf2 * dixrz + gf4 * (dixqkrz + dkxqirz + rxqidkz - R(2.0) * qixqkz) - gf5 * rxqirz - gf7 * (rxqikrz + qkrxqirz);
+        const R ttm3x = b1 * dixdkx + gf3 * dkxrx - gf4 * (dixqkrx + dkxqirx + rxqkdix - R(2.0) * qixqkx) - gf6 * rxqkrx - gf7 * (rxqkirx - qkrxqirx);
+        const R ttm3y = b1 * dixdky + gf3 * dkxry - gf4 * (dixqkry + dkxqiry + rxqkdiy - R(2.0) * qixqky) - gf6 * rxqkry - gf7 * (rxqkiry - qkrxqiry);
+        const R ttm3z = b1 * dixdkz + gf3 * dkxrz - gf4 * (dixqkrz + dkxqirz + rxqkdiz - R(2.0) * qixqkz) - gf6 * rxqkrz - gf7 * (rxqkirz - qkrxqirz);
         const R pre = LAM ? electric * l2 : electric;
         gx += pre * ftm2x; gy += pre * ftm2y; gz += pre * ftm2z;
         tx += pre * ttm2x; ty += pre * ttm2y; tz += pre * ttm2z;
@@ -475,48 +458,29 @@ __global__ void __launch_bounds__(128, sizeof(R) == 4 ? FFX_REAL_ENERGY_MIN_BLOC
         // term, every radial order one higher (:1477-1690).  Half weight per direction.
         const R bn6 = (R(11.0) * bn5 + an5 * exp2a) * rr2;
         const R rr13 = R(11.0) * rr11 * rr2;
-        const R dRealdL = gl0 * bn1 + (gl1 + gl6) * bn2 + (gl2 + gl7 + gl8) * bn3 + (gl3 + gl5) * bn4 + gl4 * bn5;
-        const R d2RealdL2 = gl0 * bn2 + (gl1 + gl6) * bn3 + (gl2 + gl7 + gl8) * bn4 + (gl3 + gl5) * bn5 + gl4 * bn6;
-        R dFixdL = gl0 * rr3 + (gl1 + gl6) * rr5 + (gl2 + gl7 + gl8) * rr7 + (gl3 + gl5) * rr9 + gl4 * rr11;
-        R d2FixdL2 = gl0 * rr5 + (gl1 + gl6) * rr7 + (gl2 + gl7 + gl8) * rr9 + (gl3 + gl5) * rr11 + gl4 * rr13;
-        dFixdL *= scale1;
-        d2FixdL2 *= scale1;
+        const R b6 = bn6 - scale1 * rr13;
+        // ereal - efix = e and the radial derivatives of both through the combined factors
+        // (one radial order higher per derivative).
+        const R dEdL1 = gl0 * b1 + (gl1 + gl6) * b2 + (gl2 + gl7 + gl8) * b3 + (gl3 + gl5) * b4 + gl4 * b5;
+        const R dEdL2 = gl0 * b2 + (gl1 + gl6) * b3 + (gl2 + gl7 + gl8) * b4 + (gl3 + gl5) * b5 + gl4 * b6;
         const double sg = st.dEdLSign, dP = st.dlPowPerm, d2P = st.d2lPowPerm, dA = st.dlAlpha, d2A = st.d2lAlpha;
         const double L2 = (double)l2;
-        dl += 0.5 * (sg * dP * (double)ereal + L2 * dA * (double)dRealdL);
-        d2l += 0.5 * (sg * (d2P * (double)ereal + 2.0 * dP * dA * (double)dRealdL) + L2 * d2A * (double)dRealdL +
-                      L2 * dA * dA * (double)d2RealdL2);
-        dl -= 0.5 * (sg * dP * (double)efix + L2 * dA * (double)dFixdL);
-        d2l -= 0.5 * (sg * (d2P * (double)efix + 2.0 * dP * dA * (double)dFixdL) + L2 * d2A * (double)dFixdL +
-                      L2 * dA * dA * (double)d2FixdL2);
-        const R gf1 = bn2 * gl0 + bn3 * (gl1 + gl6) + bn4 * (gl2 + gl7 + gl8) + bn5 * (gl3 + gl5) + bn6 * gl4;
-        const R gf2 = -ck * bn2 + sc4 * bn3 - sc6 * bn4;
-        const R gf3 = ci * bn2 + sc3 * bn3 + sc5 * bn4;
-        const R gf4 = R(2.0) * bn3;
-        const R gf5 = R(2.0) * (-ck * bn3 + sc4 * bn4 - sc6 * bn5);
-        const R gf6 = R(2.0) * (-ci * bn3 - sc3 * bn4 - sc5 * bn5);
-        const R gf7 = R(4.0) * bn4;
-        R fx = gf1 * xr + gf2 * dix + gf3 * dkx + gf4 * (qkdix - qidkx) + gf5 * qirx + gf6 * qkrx + gf7 * (qiqkrx + qkqirx);
-        R fy = gf1 * yr + gf2 * diy + gf3 * dky + gf4 * (qkdiy - qidky) + gf5 * qiry + gf6 * qkry + gf7 * (qiqkry + qkqiry);
-        R fz = gf1 * zr + gf2 * diz + gf3 * dkz + gf4 * (qkdiz - qidkz) + gf5 * qirz + gf6 * qkrz + gf7 * (qiqkrz + qkqirz);
-        R qx = -bn2 * dixdkx + gf2 * dixrx + gf4 * (dixqkrx + dkxqirx + rxqidkx - R(2.0) * qixqkx) - gf5 * rxqirx - gf7 * (rxqikrx + qkrxqirx);
-        R qy = -bn2 * dixdky + gf2 * dixry + gf4 * (dixqkry + dkxqiry + rxqidky - R(2.0) * qixqky) - gf5 * rxqiry - gf7 * (rxqikry + qkrxqiry);
-        R qz = -bn2 * dixdkz + gf2 * dixrz + gf4 * (dixqkrz + dkxqirz + rxqidkz - R(2.0) * qixqkz) - gf5 * rxqirz - gf7 * (rxqikrz + qkrxqirz);
-        if (scale1 != R(0.0)) {
-          const R gfr1 = rr5 * gl0 + rr7 * (gl1 + gl6) + rr9 * (gl2 + gl7 + gl8) + rr11 * (gl3 + gl5) + rr13 * gl4;
-          const R gfr2 = -ck * rr5 + sc4 * rr7 - sc6 * rr9;
-          const R gfr3 = ci * rr5 + sc3 * rr7 + sc5 * rr9;
-          const R gfr4 = R(2.0) * rr7;
-          const R gfr5 = R(2.0) * (-ck * rr7 + sc4 * rr9 - sc6 * rr11);
-          const R gfr6 = R(2.0) * (-ci * rr7 - sc3 * rr9 - sc5 * rr11);
-          const R gfr7 = R(4.0) * rr9;
-          fx -= scale1 * (gfr1 * xr + gfr2 * dix + gfr3 * dkx + gfr4 * (qkdix - qidkx) + gfr5 * qirx + gfr6 * qkrx + gfr7 * (qiqkrx + qkqirx));
-          fy -= scale1 * (gfr1 * yr + gfr2 * diy + gfr3 * dky + gfr4 * (qkdiy - qidky) + gfr5 * qiry + gfr6 * qkry + gfr7 * (qiqkry + qkqiry));
-          fz -= scale1 * (gfr1 * zr + gfr2 * diz + gfr3 * dkz + gfr4 * (qkdiz - qidkz) + gfr5 * qirz + gfr6 * qkrz + gfr7 * (qiqkrz + qkqirz));
-          qx -= scale1 * (-rr5 * dixdkx + gfr2 * dixrx + gfr4 * (dixqkrx + dkxqirx + rxqidkx - R(2.0) * qixqkx) - gfr5 * rxqirx - gfr7 * (rxqikrx + qkrxqirx));
-          qy -= scale1 * (-rr5 * dixdky + gfr2 * dixry + gfr4 * (dixqkry + dkxqiry + rxqidky - R(2.0) * qixqky) - gfr5 * rxqiry - gfr7 * (rxqikry + qkrxqiry));
-          qz -= scale1 * (-rr5 * dixdkz + gfr2 * dixrz + gfr4 * (dixqkrz + dkxqirz + rxqidkz - R(2.0) * qixqkz) - gfr5 * rxqirz - gfr7 * (rxqikrz + qkrxqirz));
-        }
+        dl += 0.5 * (sg * dP * (double)e + L2 * dA * (double)dEdL1);
+        d2l += 0.5 * (sg * (d2P * (double)e + 2.0 * dP * dA * (double)dEdL1) + L2 * d2A * (double)dEdL1 +
+                      L2 * dA * dA * (double)dEdL2);
+        const R gf1 = b2 * gl0 + b3 * (gl1 + gl6) + b4 * (gl2 + gl7 + gl8) + b5 * (gl3 + gl5) + b6 * gl4;
+        const R gf2 = -ck * b2 + sc4 * b3 - sc6 * b4;
+        const R gf3 = ci * b2 + sc3 * b3 + sc5 * b4;
+        const R gf4 = R(2.0) * b3;
+        const R gf5 = R(2.0) * (-ck * b3 + sc4 * b4 - sc6 * b5);
+        const R gf6 = R(2.0) * (-ci * b3 - sc3 * b4 - sc5 * b5);
+        const R gf7 = R(4.0) * b4;
+        const R fx = gf1 * xr + gf2 * dix + gf3 * dkx + gf4 * (qkdix - qidkx) + gf5 * qirx + gf6 * qkrx + gf7 * (qiqkrx + qkqirx);
+        const R fy = gf1 * yr + gf2 * diy + gf3 * dky + gf4 * (qkdiy - qidky) + gf5 * qiry + gf6 * qkry + gf7 * (qiqkry + qkqiry);
+        const R fz = gf1 * zr + gf2 * diz + gf3 * dkz + gf4 * (qkdiz - qidkz) + gf5 * qirz + gf6 * qkrz + gf7 * (qiqkrz + qkqirz);
+        const R qx = -b2 * dixdkx + gf2 * dixrx + gf4 * (dixqkrx + dkxqirx + rxqidkx - R(2.0) * qixqkx) - gf5 * rxqirx - gf7 * (rxqikrx + qkrxqirx);
+        const R qy = -b2 * dixdky + gf2 * dixry + gf4 * (dixqkry + dkxqiry + rxqidky - R(2.0) * qixqky) - gf5 * rxqiry - gf7 * (rxqikry + qkrxqiry);
+        const R qz = -b2 * dixdkz + gf2 * dixrz + gf4 * (dixqkrz + dkxqirz + rxqidkz - R(2.0) * qixqkz) - gf5 * rxqirz - gf7 * (rxqikrz + qkrxqirz);
         const R pf = electric * l2 * (R)st.dlAlpha;
         lgx += pf * fx; lgy += pf * fy; lgz += pf * fz;
         ltx += pf * qx; lty += pf * qy; ltz += pf * qz;
@@ -581,77 +545,51 @@ __global__ void __launch_bounds__(128, sizeof(R) == 4 ? FFX_REAL_ENERGY_MIN_BLOC
       const R gli6 = sci1, gli7 = R(2.0) * (sci7 - sci8);
       const R glip1 = ck * scip3 - ci * scip4, glip2 = -sc3 * scip4 - scip3 * sc4, glip3 = scip3 * sc6 - scip4 * sc5;
       const R glip6 = scip1, glip7 = R(2.0) * (scip7 - scip8);
-      const R ereal = (gli1 + gli6) * bn1 + (gli2 + gli7) * bn2 + gli3 * bn3;
-      const R efix = (gli1 + gli6) * rr3 * psc3 + (gli2 + gli7) * rr5 * psc5 + gli3 * rr7 * psc7;
-      const R epol = R(0.25) * (ereal - efix);
+      // As for the permanent pair, the Thole-damped masked parts (p-, d- and u-scaled rr
+      // terms) are linear in the radial factors: P, D and U below are bn_k minus the rr
+      // term of each scale family, Pa..Dc the same one radial order higher, and every
+      // energy, force and torque takes one contraction with them.
+      const R P1 = bn1 - rr3 * psc3, P2 = bn2 - rr5 * psc5, P3 = bn3 - rr7 * psc7;
+      const R epol = R(0.25) * ((gli1 + gli6) * P1 + (gli2 + gli7) * P2 + gli3 * P3);
       eI += HALF ? R(2.0) * epol : (LAM ? (R)st.polScale * epol : epol);
       if (LAM) {
         dl += st.dEdLSign * st.dlPowPol * (double)epol;
         d2l += st.dEdLSign * st.d2lPowPol * (double)epol;
       }
       if (!gr) return;
-      const bool dorli = (psc3 != R(0.0) || dsc3 != R(0.0) || usc3 != R(0.0));
-      const R gfi1 = R(0.5) * bn2 * (gli1 + glip1 + gli6 + glip6) + R(0.5) * bn2 * scip2 +
-                          R(0.5) * bn3 * (gli2 + glip2 + gli7 + glip7) - R(0.5) * bn3 * (sci3 * scip4 + scip3 * sci4) +
-                          R(0.5) * bn4 * (gli3 + glip3);
-      const R gfi2 = -ck * bn1 + sc4 * bn2 - sc6 * bn3;
-      const R gfi3 = ci * bn1 + sc3 * bn2 + sc5 * bn3;
-      const R gfi4 = R(2.0) * bn2;
-      const R gfi5 = bn3 * (sci4 + scip4);
-      const R gfi6 = -bn3 * (sci3 + scip3);
-      R ftm2ix = gfi1 * xr + R(0.5) * (gfi2 * (uix + pix) + bn2 * (sci4 * pix + scip4 * uix) + gfi3 * (ukx + pkx) +
-                                         bn2 * (sci3 * pkx + scip3 * ukx) + (sci4 + scip4) * bn2 * dix +
-                                         (sci3 + scip3) * bn2 * dkx + gfi4 * (qkuix + qkuipx - qiukx - qiukpx)) +
-                      gfi5 * qirx + gfi6 * qkrx;
-      R ftm2iy = gfi1 * yr + R(0.5) * (gfi2 * (uiy + piy) + bn2 * (sci4 * piy + scip4 * uiy) + gfi3 * (uky + pky) +
-                                         bn2 * (sci3 * pky + scip3 * uky) + (sci4 + scip4) * bn2 * diy +
-                                         (sci3 + scip3) * bn2 * dky + gfi4 * (qkuiy + qkuipy - qiuky - qiukpy)) +
-                      gfi5 * qiry + gfi6 * qkry;
-      R ftm2iz = gfi1 * zr + R(0.5) * (gfi2 * (uiz + piz) + bn2 * (sci4 * piz + scip4 * uiz) + gfi3 * (ukz + pkz) +
-                                         bn2 * (sci3 * pkz + scip3 * ukz) + (sci4 + scip4) * bn2 * diz +
-                                         (sci3 + scip3) * bn2 * dkz + gfi4 * (qkuiz + qkuipz - qiukz - qiukpz)) +
-                      gfi5 * qirz + gfi6 * qkrz;
-      const R gti2 = R(0.5) * bn2 * (sci4 + scip4), gti3 = R(0.5) * bn2 * (sci3 + scip3);
-      const R gti4 = gfi4, gti5 = gfi5, gti6 = gfi6;
-      R ttm2ix = -R(0.5) * bn1 * (dixukx + dixukpx) + gti2 * dixrx - gti5 * rxqirx + R(0.5) * gti4 * (ukxqirx + rxqiukx + ukxqirpx + rxqiukpx);
-      R ttm2iy = -R(0.5) * bn1 * (dixuky + dixukpy) + gti2 * dixry - gti5 * rxqiry + R(0.5) * gti4 * (ukxqiry + rxqiuky + ukxqirpy + rxqiukpy);
-      R ttm2iz = -R(0.5) * bn1 * (dixukz + dixukpz) + gti2 * dixrz - gti5 * rxqirz + R(0.5) * gti4 * (ukxqirz + rxqiukz + ukxqirpz + rxqiukpz);
-      R ttm3ix = -R(0.5) * bn1 * (dkxuix + dkxuipx) + gti3 * dkxrx - gti6 * rxqkrx - R(0.5) * gti4 * (uixqkrx + rxqkuix + uixqkrpx + rxqkuipx);
-      R ttm3iy = -R(0.5) * bn1 * (dkxuiy + dkxuipy) + gti3 * dkxry - gti6 * rxqkry - R(0.5) * gti4 * (uixqkry + rxqkuiy + uixqkrpy + rxqkuipy);
-      R ttm3iz = -R(0.5) * bn1 * (dkxuiz + dkxuipz) + gti3 * dkxrz - gti6 * rxqkrz - R(0.5) * gti4 * (uixqkrz + rxqkuiz + uixqkrpz + rxqkuipz);
-      R ftm2rix = 0, ftm2riy = 0, ftm2riz = 0, ttm2rix = 0, ttm2riy = 0, ttm2riz = 0, ttm3rix = 0, ttm3riy = 0, ttm3riz = 0;
-      if (dorli) {
-        const R gfri1 = R(0.5) * rr5 * ((gli1 + gli6) * psc3 + (glip1 + glip6) * dsc3 + scip2 * usc3) +
-                             R(0.5) * rr7 * ((gli7 + gli2) * psc5 + (glip7 + glip2) * dsc5 - (sci3 * scip4 + scip3 * sci4) * usc5) +
-                             R(0.5) * rr9 * (gli3 * psc7 + glip3 * dsc7);
-        const R gfri4 = R(2.0) * rr5;
-        const R gfri5 = rr7 * (sci4 * psc7 + scip4 * dsc7);
-        const R gfri6 = -rr7 * (sci3 * psc7 + scip3 * dsc7);
-        ftm2rix = gfri1 * xr + R(0.5) * (-rr3 * ck * (uix * psc3 + pix * dsc3) + rr5 * sc4 * (uix * psc5 + pix * dsc5) - rr7 * sc6 * (uix * psc7 + pix * dsc7)) +
-                  (rr3 * ci * (ukx * psc3 + pkx * dsc3) + rr5 * sc3 * (ukx * psc5 + pkx * dsc5) + rr7 * sc5 * (ukx * psc7 + pkx * dsc7)) * R(0.5) +
-                  rr5 * usc5 * (sci4 * pix + scip4 * uix + sci3 * pkx + scip3 * ukx) * R(0.5) +
-                  R(0.5) * (sci4 * psc5 + scip4 * dsc5) * rr5 * dix + R(0.5) * (sci3 * psc5 + scip3 * dsc5) * rr5 * dkx +
-                  R(0.5) * gfri4 * ((qkuix - qiukx) * psc5 + (qkuipx - qiukpx) * dsc5) + gfri5 * qirx + gfri6 * qkrx;
-        ftm2riy = gfri1 * yr + R(0.5) * (-rr3 * ck * (uiy * psc3 + piy * dsc3) + rr5 * sc4 * (uiy * psc5 + piy * dsc5) - rr7 * sc6 * (uiy * psc7 + piy * dsc7)) +
-                  (rr3 * ci * (uky * psc3 + pky * dsc3) + rr5 * sc3 * (uky * psc5 + pky * dsc5) + rr7 * sc5 * (uky * psc7 + pky * dsc7)) * R(0.5) +
-                  rr5 * usc5 * (sci4 * piy + scip4 * uiy + sci3 * pky + scip3 * uky) * R(0.5) +
-                  R(0.5) * (sci4 * psc5 + scip4 * dsc5) * rr5 * diy + R(0.5) * (sci3 * psc5 + scip3 * dsc5) * rr5 * dky +
-                  R(0.5) * gfri4 * ((qkuiy - qiuky) * psc5 + (qkuipy - qiukpy) * dsc5) + gfri5 * qiry + gfri6 * qkry;
-        ftm2riz = gfri1 * zr + R(0.5) * (-rr3 * ck * (uiz * psc3 + piz * dsc3) + rr5 * sc4 * (uiz * psc5 + piz * dsc5) - rr7 * sc6 * (uiz * psc7 + piz * dsc7)) +
-                  (rr3 * ci * (ukz * psc3 + pkz * dsc3) + rr5 * sc3 * (ukz * psc5 + pkz * dsc5) + rr7 * sc5 * (ukz * psc7 + pkz * dsc7)) * R(0.5) +
-                  rr5 * usc5 * (sci4 * piz + scip4 * uiz + sci3 * pkz + scip3 * ukz) * R(0.5) +
-                  R(0.5) * (sci4 * psc5 + scip4 * dsc5) * rr5 * diz + R(0.5) * (sci3 * psc5 + scip3 * dsc5) * rr5 * dkz +
-                  R(0.5) * gfri4 * ((qkuiz - qiukz) * psc5 + (qkuipz - qiukpz) * dsc5) + gfri5 * qirz + gfri6 * qkrz;
-        const R gtri2 = R(0.5) * rr5 * (sci4 * psc5 + scip4 * dsc5);
-        const R gtri3 = R(0.5) * rr5 * (sci3 * psc5 + scip3 * dsc5);
-        const R gtri4 = gfri4, gtri5 = gfri5, gtri6 = gfri6;
-        ttm2rix = -rr3 * (dixukx * psc3 + dixukpx * dsc3) * R(0.5) + gtri2 * dixrx - gtri5 * rxqirx + gtri4 * ((ukxqirx + rxqiukx) * psc5 + (ukxqirpx + rxqiukpx) * dsc5) * R(0.5);
-        ttm2riy = -rr3 * (dixuky * psc3 + dixukpy * dsc3) * R(0.5) + gtri2 * dixry - gtri5 * rxqiry + gtri4 * ((ukxqiry + rxqiuky) * psc5 + (ukxqirpy + rxqiukpy) * dsc5) * R(0.5);
-        ttm2riz = -rr3 * (dixukz * psc3 + dixukpz * dsc3) * R(0.5) + gtri2 * dixrz - gtri5 * rxqirz + gtri4 * ((ukxqirz + rxqiukz) * psc5 + (ukxqirpz + rxqiukpz) * dsc5) * R(0.5);
-        ttm3rix = -rr3 * (dkxuix * psc3 + dkxuipx * dsc3) * R(0.5) + gtri3 * dkxrx - gtri6 * rxqkrx - gtri4 * ((uixqkrx + rxqkuix) * psc5 + (uixqkrpx + rxqkuipx) * dsc5) * R(0.5);
-        ttm3riy = -rr3 * (dkxuiy * psc3 + dkxuipy * dsc3) * R(0.5) + gtri3 * dkxry - gtri6 * rxqkry - gtri4 * ((uixqkry + rxqkuiy) * psc5 + (uixqkrpy + rxqkuipy) * dsc5) * R(0.5);
-        ttm3riz = -rr3 * (dkxuiz * psc3 + dkxuipz * dsc3) * R(0.5) + gtri3 * dkxrz - gtri6 * rxqkrz - gtri4 * ((uixqkrz + rxqkuiz) * psc5 + (uixqkrpz + rxqkuipz) * dsc5) * R(0.5);
-      }
+      const R D1 = bn1 - rr3 * dsc3, D2 = bn2 - rr5 * dsc5, D3 = bn3 - rr7 * dsc7;
+      const R U2 = bn2 - rr5 * usc5;
+      const R Pa = bn2 - rr5 * psc3, Da = bn2 - rr5 * dsc3, Ua = bn2 - rr5 * usc3;
+      const R Pb = bn3 - rr7 * psc5, Db = bn3 - rr7 * dsc5, Ub = bn3 - rr7 * usc5;
+      const R Pc = bn4 - rr9 * psc7, Dc = bn4 - rr9 * dsc7;
+      const R sci34 = sci3 * scip4 + scip3 * sci4;
+      const R gfi1 = R(0.5) * ((gli1 + gli6) * Pa + (glip1 + glip6) * Da + scip2 * Ua + (gli2 + gli7) * Pb +
+                               (glip2 + glip7) * Db - sci34 * Ub + gli3 * Pc + glip3 * Dc);
+      const R fu = -ck * P1 + sc4 * P2 - sc6 * P3, fp = -ck * D1 + sc4 * D2 - sc6 * D3;
+      const R ku = ci * P1 + sc3 * P2 + sc5 * P3, kp = ci * D1 + sc3 * D2 + sc5 * D3;
+      const R di2 = sci4 * P2 + scip4 * D2, dk2 = sci3 * P2 + scip3 * D2;
+      const R qi3 = sci4 * P3 + scip4 * D3, qk3 = sci3 * P3 + scip3 * D3;
+      R ftm2ix = gfi1 * xr + R(0.5) * (uix * fu + pix * fp + ukx * ku + pkx * kp) +
+                 R(0.5) * U2 * (sci4 * pix + scip4 * uix + sci3 * pkx + scip3 * ukx) + R(0.5) * (dix * di2 + dkx * dk2) +
+                 (qkuix - qiukx) * P2 + (qkuipx - qiukpx) * D2 + qirx * qi3 - qkrx * qk3;
+      R ftm2iy = gfi1 * yr + R(0.5) * (uiy * fu + piy * fp + uky * ku + pky * kp) +
+                 R(0.5) * U2 * (sci4 * piy + scip4 * uiy + sci3 * pky + scip3 * uky) + R(0.5) * (diy * di2 + dky * dk2) +
+                 (qkuiy - qiuky) * P2 + (qkuipy - qiukpy) * D2 + qiry * qi3 - qkry * qk3;
+      R ftm2iz = gfi1 * zr + R(0.5) * (uiz * fu + piz * fp + ukz * ku + pkz * kp) +
+                 R(0.5) * U2 * (sci4 * piz + scip4 * uiz + sci3 * pkz + scip3 * ukz) + R(0.5) * (diz * di2 + dkz * dk2) +
+                 (qkuiz - qiukz) * P2 + (qkuipz - qiukpz) * D2 + qirz * qi3 - qkrz * qk3;
+      const R ttm2ix = -R(0.5) * (dixukx * P1 + dixukpx * D1) + R(0.5) * dixrx * di2 - rxqirx * qi3 +
+                       (ukxqirx + rxqiukx) * P2 + (ukxqirpx + rxqiukpx) * D2;
+      const R ttm2iy = -R(0.5) * (dixuky * P1 + dixukpy * D1) + R(0.5) * dixry * di2 - rxqiry * qi3 +
+                       (ukxqiry + rxqiuky) * P2 + (ukxqirpy + rxqiukpy) * D2;
+      const R ttm2iz = -R(0.5) * (dixukz * P1 + dixukpz * D1) + R(0.5) * dixrz * di2 - rxqirz * qi3 +
+                       (ukxqirz + rxqiukz) * P2 + (ukxqirpz + rxqiukpz) * D2;
+      const R ttm3ix = -R(0.5) * (dkxuix * P1 + dkxuipx * D1) + R(0.5) * dkxrx * dk2 + rxqkrx * qk3 -
+                       (uixqkrx + rxqkuix) * P2 - (uixqkrpx + rxqkuipx) * D2;
+      const R ttm3iy = -R(0.5) * (dkxuiy * P1 + dkxuipy * D1) + R(0.5) * dkxry * dk2 + rxqkry * qk3 -
+                       (uixqkry + rxqkuiy) * P2 - (uixqkrpy + rxqkuipy) * D2;
+      const R ttm3iz = -R(0.5) * (dkxuiz * P1 + dkxuipz * D1) + R(0.5) * dkxrz * dk2 + rxqkrz * qk3 -
+                       (uixqkrz + rxqkuiz) * P2 - (uixqkrpz + rxqkuipz) * D2;
       R temp3 = R(0.5) * rr3 * ((gli1 + gli6) * scalep + (glip1 + glip6) * scaled);
       R temp5 = R(0.5) * rr5 * ((gli2 + gli7) * scalep + (glip2 + glip7) * scaled);
       const R temp7 = R(0.5) * rr7 * (gli3 * scalep + glip3 * scaled);
@@ -667,21 +605,11 @@ __global__ void __launch_bounds__(128, sizeof(R) == 4 ? FFX_REAL_ENERGY_MIN_BLOC
       ftm2iy = ftm2iy - fridmpy - findmpy;
       ftm2iz = ftm2iz - fridmpz - findmpz;
       if (DIRECT) {   // the direct-polarization terms (compiled out of the mutual form)
-        const R gfd = R(0.5) * (bn2 * scip2 - bn3 * (scip3 * sci4 + sci3 * scip4));
-        const R gfdr = R(0.5) * (rr5 * scip2 * usc3 - rr7 * (scip3 * sci4 + sci3 * scip4) * usc5);
-        ftm2ix = ftm2ix - gfd * xr - R(0.5) * bn2 * (sci4 * pix + scip4 * uix + sci3 * pkx + scip3 * ukx);
-        ftm2iy = ftm2iy - gfd * yr - R(0.5) * bn2 * (sci4 * piy + scip4 * uiy + sci3 * pky + scip3 * uky);
-        ftm2iz = ftm2iz - gfd * zr - R(0.5) * bn2 * (sci4 * piz + scip4 * uiz + sci3 * pkz + scip3 * ukz);
-        const R fdirx = gfdr * xr + R(0.5) * usc5 * rr5 * (sci4 * pix + scip4 * uix + sci3 * pkx + scip3 * ukx);
-        const R fdiry = gfdr * yr + R(0.5) * usc5 * rr5 * (sci4 * piy + scip4 * uiy + sci3 * pky + scip3 * uky);
-        const R fdirz = gfdr * zr + R(0.5) * usc5 * rr5 * (sci4 * piz + scip4 * uiz + sci3 * pkz + scip3 * ukz);
-        ftm2ix = ftm2ix + fdirx + findmpx;
-        ftm2iy = ftm2iy + fdiry + findmpy;
-        ftm2iz = ftm2iz + fdirz + findmpz;
+        const R gfd = R(0.5) * (scip2 * Ua - sci34 * Ub);
+        ftm2ix = ftm2ix - gfd * xr - R(0.5) * U2 * (sci4 * pix + scip4 * uix + sci3 * pkx + scip3 * ukx) + findmpx;
+        ftm2iy = ftm2iy - gfd * yr - R(0.5) * U2 * (sci4 * piy + scip4 * uiy + sci3 * pky + scip3 * uky) + findmpy;
+        ftm2iz = ftm2iz - gfd * zr - R(0.5) * U2 * (sci4 * piz + scip4 * uiz + sci3 * pkz + scip3 * ukz) + findmpz;
       }
-      ftm2ix -= ftm2rix; ftm2iy -= ftm2riy; ftm2iz -= ftm2riz;
-      ttm2ix -= ttm2rix; ttm2iy -= ttm2riy; ttm2iz -= ttm2riz;
-      ttm3ix -= ttm3rix; ttm3iy -= ttm3riy; ttm3iz -= ttm3riz;
       const R sc = LAM ? electric * (R)st.polScale : electric;
       gx += sc * ftm2ix; gy += sc * ftm2iy; gz += sc * ftm2iz;
       tx += sc * ttm2ix; ty += sc * ttm2iy; tz += sc * ttm2iz;

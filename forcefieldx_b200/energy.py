@@ -291,7 +291,7 @@ class ForceFieldEnergy:
 
 
 class CrystalEnergy:
-    """Energy and gradient of an asymmetric unit in a space group with an orthorhombic cell,
+    """Energy and gradient of an asymmetric unit in a space group (any cell: params.angles),
     evaluated as the P1 unit cell of its symmetry mates (forcefieldx_b200.ffxio): the
     reference sums the asymmetric unit's interactions with its mates
     (ParticleMeshEwald / NeighborList symmetry loops); the cell of mates has the same
@@ -299,11 +299,12 @@ class CrystalEnergy:
 
     def __init__(self, asu_system: AmoebaSystem, params: AmoebaParams, space_group: str):
         from .ffxio import SPACE_GROUPS, expand_system
-        self.space_group = space_group
+        self.space_group = space_group.upper().replace(" ", "")
         self.n_asu = asu_system.n_atoms
-        self.n_symm = len(SPACE_GROUPS[space_group])
+        self.n_symm = len(SPACE_GROUPS[self.space_group])
         self.box = params.box
-        self.cell = expand_system(asu_system, params.box, space_group)
+        self.angles = tuple(params.angles)
+        self.cell = expand_system(asu_system, params.box, self.space_group, self.angles)
         self.ffe = ForceFieldEnergy(self.cell, params)
 
     def close(self):
@@ -318,7 +319,7 @@ class CrystalEnergy:
     def energy_and_gradient(self, x_asu=None):
         """(energy per asymmetric unit, gradient [n_asu, 3]) at the asymmetric unit's coordinates."""
         from .ffxio import expand_coordinates
-        x = None if x_asu is None else expand_coordinates(x_asu, self.box, self.space_group)
+        x = None if x_asu is None else expand_coordinates(x_asu, self.box, self.space_group, self.angles)
         e, g = self.ffe.energy_and_gradient(x)
         return e / self.n_symm, g[:self.n_asu].copy()
 
