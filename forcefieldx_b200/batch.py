@@ -22,7 +22,8 @@ from . import cabi
 from .energy import EnergyException, ForceFieldEnergy, library
 from .system import PRECISION_MIXED, AmoebaParams, AmoebaSystem, params_struct, small_water_box, water_params
 
-BATCH_GRAPH, BATCH_LOOP = 0, 1
+BATCH_GRAPH, BATCH_LOOP, BATCH_BRANCHES = 0, 1, 2
+_MODES = {"graph": BATCH_GRAPH, "loop": BATCH_LOOP, "branches": BATCH_BRANCHES}
 
 
 def smooth235(n: int) -> int:
@@ -111,15 +112,24 @@ class BatchEnergy:
     def __exit__(self, *a):
         self.close()
 
-    def set_mode(self, loop: bool) -> None:
-        """One CUDA graph for the batch (default) or a loop of single-system launches."""
-        st = self.lib.ffxg_batch_set_mode(self._b, BATCH_LOOP if loop else BATCH_GRAPH)
+    def set_mode(self, mode) -> None:
+        """"graph" (default: one CUDA graph, stage by stage), "branches" (one graph of
+        per-system branches) or "loop" (single-system launches one after another).  A bool
+        selects "loop" (True) or "graph" (False)."""
+        if isinstance(mode, bool):
+            mode = "loop" if mode else "graph"
+        st = self.lib.ffxg_batch_set_mode(self._b, _MODES[mode])
         if st != 0:
             raise EnergyException(st, self.lib.ffxg_batch_last_error(self._b).decode())
 
     @property
     def graph_builds(self) -> int:
         return int(self.lib.ffxg_batch_graph_builds(self._b))
+
+    def stages(self, gradient: bool = True) -> int:
+        """Stages (one launch each for all systems) of the stage-by-stage graph; 0 when the
+        batch runs as branches or has not been evaluated yet."""
+        return int(self.lib.ffxg_batch_stages(self._b, 1 if gradient else 0))
 
     def system_energy(self, i: int) -> ForceFieldEnergy:
         """A non-owning ForceFieldEnergy on system i's handle (induced dipoles, lambda ...)."""

@@ -19,6 +19,7 @@
 #include <vector>
 
 #include "../../include/ffxcuda.h"
+#include "launch.cuh"
 
 namespace ffx {
 
@@ -184,6 +185,15 @@ __device__ __forceinline__ double m_erfc(double v) { return erfc(v); }
 __device__ __forceinline__ float m_erfc(float v) { return erfcf(v); }
 __device__ __forceinline__ double m_min(double a, double b) { return fmin(a, b); }
 __device__ __forceinline__ float m_min(float a, float b) { return fminf(a, b); }
+// Products, sums and fused multiply-adds whose rounding is fixed in the source: the
+// compiler neither fuses nor splits them, so every instance of a kernel body (one system
+// or a batch, launch.cuh) rounds alike.
+__device__ __forceinline__ float xmul(float a, float b) { return __fmul_rn(a, b); }
+__device__ __forceinline__ double xmul(double a, double b) { return __dmul_rn(a, b); }
+__device__ __forceinline__ float xadd(float a, float b) { return __fadd_rn(a, b); }
+__device__ __forceinline__ double xadd(double a, double b) { return __dadd_rn(a, b); }
+__device__ __forceinline__ float xfma(float a, float b, float c) { return __fmaf_rn(a, b, c); }
+__device__ __forceinline__ double xfma(double a, double b, double c) { return __fma_rn(a, b, c); }
 
 template <typename T>
 __device__ __forceinline__ T warp_sum(T v) {
@@ -214,12 +224,12 @@ template <typename T>
 __device__ __forceinline__ void get_rec(const T *__restrict__ rec, int k, T *v) {
   const T *q = rec + 8 * (size_t)k;
   if constexpr (sizeof(T) == 8) {
-    const double2 a = reinterpret_cast<const double2 *>(q)[0], b = reinterpret_cast<const double2 *>(q)[1],
-                  c = reinterpret_cast<const double2 *>(q)[2];
+    const double2 a = __ldg(reinterpret_cast<const double2 *>(q)), b = __ldg(reinterpret_cast<const double2 *>(q) + 1),
+                  c = __ldg(reinterpret_cast<const double2 *>(q) + 2);
     v[0] = a.x; v[1] = a.y; v[2] = b.x; v[3] = b.y; v[4] = c.x; v[5] = c.y;
   } else {
-    const float4 a = reinterpret_cast<const float4 *>(q)[0];
-    const float2 b = reinterpret_cast<const float2 *>(q)[2];
+    const float4 a = __ldg(reinterpret_cast<const float4 *>(q));
+    const float2 b = __ldg(reinterpret_cast<const float2 *>(q) + 2);
     v[0] = a.x; v[1] = a.y; v[2] = a.z; v[3] = a.w; v[4] = b.x; v[5] = b.y;
   }
 }
@@ -277,12 +287,12 @@ __device__ __forceinline__ void store_pair(PairRec<float> *p, size_t e, float x,
 }
 __device__ __forceinline__ void load_pair(const PairRec<double> *__restrict__ p, size_t e, double &x, double &y,
                                           double &z, double &a) {
-  const double2 u = p[e].xy, v = p[e].za;
+  const double2 u = __ldg(&p[e].xy), v = __ldg(&p[e].za);
   x = u.x; y = u.y; z = v.x; a = v.y;
 }
 __device__ __forceinline__ void load_pair(const PairRec<float> *__restrict__ p, size_t e, float &x, float &y,
                                           float &z, float &a) {
-  const float4 u = p[e].v;
+  const float4 u = __ldg(&p[e].v);
   x = u.x; y = u.y; z = u.z; a = u.w;
 }
 
@@ -367,6 +377,8 @@ struct Handle {
   cudaStream_t stream = nullptr;
   std::string err;
   int64_t launches = 0;
+  Recorder *rec = nullptr;            // set while a batch records this system's launches
+  unsigned char *d_stage = nullptr;   // while recording: this system's slot of the batch's result staging
 
   // ---- static per-atom parameters (device)
   double *d_lmp = nullptr;        // [10][n] local multipoles

@@ -75,7 +75,38 @@ static bool fft_supported(int n) {
   return count <= 12;
 }
 
-__global__ void k_set_flags(int *flags, int v) { *flags = v; }
+__device__ __forceinline__ void k_set_flags(VGrid, int *flags, int v) { *flags = v; }
+
+// m doubles cleared.
+__device__ __forceinline__ void k_zero(VGrid vg, size_t m, double *p) {
+  for (size_t j = (size_t)vg.bid * blockDim.x + threadIdx.x; j < m; j += (size_t)vg.nblk * blockDim.x) p[j] = 0.0;
+}
+
+// words 4-byte words copied (a result into a batch's staging buffer).
+__device__ __forceinline__ void k_copy_words(VGrid, const unsigned *src, unsigned *dst, int words) {
+  for (int j = threadIdx.x; j < words; j += blockDim.x) dst[j] = src[j];
+}
+
+static void zero_doubles(Handle &h, double *p, size_t m) {
+  launch_on<k_zero, 0, 0>(h.rec, (int)std::min<size_t>(nblocks((int64_t)m, 256), 2 * (size_t)h.num_sms), 256, 0,
+                          h.stream, m, p);
+  FFX_LAUNCHED(h);
+}
+
+// A result read back to the host: queued on the handle's stream, or, while a batch records
+// the evaluation, copied on the device into the system's slot of the batch's staging
+// buffer (the batch reads every slot back with one copy and hands each system its bytes).
+static void copy_result(Handle &h, void *host, const void *dev, size_t bytes) {
+  if (h.rec) {
+    const size_t off = h.rec->stage_bytes;
+    launch_on<k_copy_words, 0, 0>(h.rec, 1, 32, 0, h.stream, (const unsigned *)dev,
+                                  (unsigned *)(h.d_stage + off), (int)(bytes / 4));
+    h.rec->copies.push_back(Recorder::Copy{dev, off, host, bytes});
+    h.rec->stage_bytes += (bytes + 15) & ~(size_t)15;
+    return;
+  }
+  cudaMemcpyAsync(host, dev, bytes, cudaMemcpyDeviceToHost, h.stream);
+}
 
 static void drop_graphs(Handle &h) {
   for (cudaGraphExec_t &g : h.graph_exec)
@@ -602,7 +633,7 @@ static bool branch_recip(const Handle &h) { return h.capturing && !h.vacuum && !
 // torques, gradient, reductions) are shared by the direct path and the captured graph.
 static void emit_front(Handle &h, const double *d_xyz) {
   int tk = timer_begin(h, FFXG_STAGE_LISTS);
-  k_set_flags<<<1, 1, 0, h.stream>>>(h.d_flags, h.list_valid ? 0 : FLAG_REBUILD);
+  launch_on<k_set_flags, 0, 0>(h.rec, 1, 1, 0, h.stream, h.d_flags, h.list_valid ? 0 : FLAG_REBUILD);
   FFX_LAUNCHED(h);
   launch_set_coordinates(h, d_xyz);
   launch_neighbor_list(h, false);
@@ -677,8 +708,8 @@ static void emit_final_induced(Handle &h) {
 }
 
 static void emit_no_polarization(Handle &h) {
-  cudaMemsetAsync(h.d_uD, 0, 3 * (size_t)h.n * sizeof(double), h.stream);
-  cudaMemsetAsync(h.d_uP, 0, 3 * (size_t)h.n * sizeof(double), h.stream);
+  zero_doubles(h, h.d_uD, 3 * (size_t)h.n);
+  zero_doubles(h, h.d_uP, 3 * (size_t)h.n);
 }
 
 static void emit_back(Handle &h, double *d_grad_xyz) {
@@ -708,14 +739,14 @@ static void emit_back(Handle &h, double *d_grad_xyz) {
     }
   }
   if (h.step.lam) {   // electrostatic lambda gradient into the dU/dX dL rows (after the vdW part)
-    if (h.vacuum) cudaMemsetAsync(h.d_lgred + 3 * (size_t)h.n, 0, 3 * (size_t)h.n * sizeof(double), h.stream);
+    if (h.vacuum) zero_doubles(h, h.d_lgred + 3 * (size_t)h.n, 3 * (size_t)h.n);
     launch_lambda_grad_add(h, h.d_lgred + 3 * (size_t)h.n);
   }
   launch_reduce_results(h);
   timer_end(h, tk);
-  cudaMemcpyAsync(h.h_scalars, h.d_result, kEnergyRows * sizeof(double), cudaMemcpyDeviceToHost, h.stream);
-  cudaMemcpyAsync(h.h_flags + 2, h.d_cresult, 2 * sizeof(long long), cudaMemcpyDeviceToHost, h.stream);
-  cudaMemcpyAsync(h.h_flags, h.d_flags, sizeof(int), cudaMemcpyDeviceToHost, h.stream);
+  copy_result(h, h.h_scalars, h.d_result, kEnergyRows * sizeof(double));
+  copy_result(h, h.h_flags + 2, h.d_cresult, 2 * sizeof(long long));
+  copy_result(h, h.h_flags, h.d_flags, sizeof(int));
   if (h.recip_forked) {
     cudaStreamWaitEvent(h.stream, h.ev_recip_join, 0);
     h.recip_forked = false;
@@ -866,7 +897,7 @@ int eval_capture_body(Handle &h, const double *d_xyz, double *d_grad) {
   }
   emit_back(h, d_grad);
   h.capturing = false;
-  cudaMemcpyAsync(h.h_pcg, h.d_pcg, sizeof(PcgState), cudaMemcpyDeviceToHost, h.stream);
+  copy_result(h, h.h_pcg, h.d_pcg, sizeof(PcgState));
   h.graph_launches[key] = h.launches - before - h.graph_body_launches;
   return st;
 }

@@ -18,10 +18,10 @@ struct CellOffsets {
 
 // Interleaved [n][3] -> SoA, plus reduced coordinates r = a*(x - x_p) + x_p evaluated
 // without contraction like Java (VanDerWaals.java:1521-1527).
-__global__ void k_set_coordinates(int n, const double *__restrict__ xyz, const int *__restrict__ redp,
+__device__ __forceinline__ void k_set_coordinates(VGrid vg, int n, const double *__restrict__ xyz, const int *__restrict__ redp,
                                   const double *__restrict__ redf, double *x, double *y, double *z,
                                   double *rx, double *ry, double *rz, double2 *pos) {
-  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  const int i = vg.bid * blockDim.x + threadIdx.x;
   if (i >= n) return;
   const double a = xyz[3 * i], b = xyz[3 * i + 1], c = xyz[3 * i + 2];
   x[i] = a;
@@ -31,13 +31,13 @@ __global__ void k_set_coordinates(int n, const double *__restrict__ xyz, const i
   pos[2 * i + 1] = make_double2(c, 0.0);
 }
 
-__global__ void k_reduce_coordinates(int n, const double *__restrict__ x, const double *__restrict__ y,
+__device__ __forceinline__ void k_reduce_coordinates(VGrid vg, int n, const double *__restrict__ x, const double *__restrict__ y,
                                      const double *__restrict__ z, const int *__restrict__ redp,
                                      const double *__restrict__ redf, double *rx, double *ry, double *rz,
                                      const double *__restrict__ refx, const double *__restrict__ refy,
                                      const double *__restrict__ refz, double half_buffer2, int *flags,
                                      const int *__restrict__ vtype, double2 *rpos) {
-  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  const int i = vg.bid * blockDim.x + threadIdx.x;
   if (i >= n) return;
   const int p = redp[i];
   const double a = redf[i];
@@ -67,11 +67,11 @@ __device__ __forceinline__ int cell_of(double f, int nc) {
   return c < 0 ? 0 : (c >= nc ? nc - 1 : c);
 }
 
-__global__ void k_cell_count(int n, const double *__restrict__ rx, const double *__restrict__ ry,
-                             const double *__restrict__ rz, Box bx, int ncx, int ncy, int ncz,
+__device__ __forceinline__ void k_cell_count(VGrid vg, int n, const double *__restrict__ rx, const double *__restrict__ ry,
+                             const double *__restrict__ rz, const Box &bx, int ncx, int ncy, int ncz,
                              int *cell_cnt, int *atom_cell, const int *flags) {
   if (!(*flags & FLAG_REBUILD)) return;
-  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  const int i = vg.bid * blockDim.x + threadIdx.x;
   if (i >= n) return;
   double fx, fy, fz;
   to_frac(rx[i], ry[i], rz[i], bx, fx, fy, fz);
@@ -82,7 +82,7 @@ __global__ void k_cell_count(int n, const double *__restrict__ rx, const double 
 }
 
 // Exclusive scan of the cell counts in one CTA (cells <= a few 1e5).
-__global__ void k_cell_scan(int ncells, const int *__restrict__ cnt, int *start, const int *flags) {
+__device__ __forceinline__ void k_cell_scan(VGrid vg, int ncells, const int *__restrict__ cnt, int *start, const int *flags) {
   if (!(*flags & FLAG_REBUILD)) return;
   __shared__ int warp_tot[32];
   __shared__ int carry;
@@ -121,19 +121,19 @@ __global__ void k_cell_scan(int ncells, const int *__restrict__ cnt, int *start,
 
 // Deterministic placement: an atom's slot is the number of lower-indexed atoms in
 // its cell (cells hold tens of atoms; the scan over the cell is short).
-__global__ void k_cell_fill(int n, const int *__restrict__ atom_cell, const int *__restrict__ start,
+__device__ __forceinline__ void k_cell_fill(VGrid vg, int n, const int *__restrict__ atom_cell, const int *__restrict__ start,
                             int *cell_atoms, int *cell_cursor, const int *flags) {
   if (!(*flags & FLAG_REBUILD)) return;
-  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  const int i = vg.bid * blockDim.x + threadIdx.x;
   if (i >= n) return;
   const int c = atom_cell[i];
   const int slot = atomicAdd(&cell_cursor[c], 1);
   cell_atoms[start[c] + slot] = i;
 }
 
-__global__ void k_cell_sort(int ncells, const int *__restrict__ start, int *cell_atoms, const int *flags) {
+__device__ __forceinline__ void k_cell_sort(VGrid vg, int ncells, const int *__restrict__ start, int *cell_atoms, const int *flags) {
   if (!(*flags & FLAG_REBUILD)) return;
-  const int c = blockIdx.x * blockDim.x + threadIdx.x;
+  const int c = vg.bid * blockDim.x + threadIdx.x;
   if (c >= ncells) return;
   const int s = start[c], e = start[c + 1];
   for (int a = s + 1; a < e; a++) {
@@ -146,13 +146,13 @@ __global__ void k_cell_sort(int ncells, const int *__restrict__ start, int *cell
 
 // One warp per atom i: every atom k != i of the neighbouring cells with
 // image d2 <= rl2 on reduced coordinates (NeighborList.atomCellPairs, :1026-1115).
-__global__ void k_verlet(int n, const double *__restrict__ rx, const double *__restrict__ ry,
-                         const double *__restrict__ rz, Box bx, CellOffsets co,
+__device__ __forceinline__ void k_verlet(VGrid vg, int n, const double *__restrict__ rx, const double *__restrict__ ry,
+                         const double *__restrict__ rz, const Box &bx, const CellOffsets &co,
                          const int *__restrict__ atom_cell, const int *__restrict__ start,
                          const int *__restrict__ cell_atoms, double rl2, int cap, int *nbr, int *nbr_cnt,
                          int *flags, double rn2, int capN, int *nbl, int *nbl_cnt) {
   if (!(*flags & FLAG_REBUILD)) return;
-  const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const int warp = (vg.bid * blockDim.x + threadIdx.x) >> 5;
   const int lane = threadIdx.x & 31;
   if (warp >= n) return;
   const int i = warp;
@@ -223,12 +223,12 @@ __global__ void k_verlet(int n, const double *__restrict__ rx, const double *__r
 // n = n0 + m (n0 the minimum-image shift of the reduced-coordinate difference, |m_d| <=
 // R_d) with |x_k + n L - x_i|^2 <= rl2, except k == i at n = 0.  Entries keep k and the
 // packed shift; the order (k chunk, then m) is fixed, so lists are reproducible.
-__global__ void k_verlet_images(int n, const double *__restrict__ rx, const double *__restrict__ ry,
-                                const double *__restrict__ rz, Box bx, int R0, int R1, int R2, double rl2,
-                                int cap, int *nbr, int *nbr_sh, int *nbr_cnt, int *flags, Box super, int P0,
+__device__ __forceinline__ void k_verlet_images(VGrid vg, int n, const double *__restrict__ rx, const double *__restrict__ ry,
+                                const double *__restrict__ rz, const Box &bx, int R0, int R1, int R2, double rl2,
+                                int cap, int *nbr, int *nbr_sh, int *nbr_cnt, int *flags, const Box &super, int P0,
                                 int P1, int P2) {
   if (!(*flags & FLAG_REBUILD)) return;
-  const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const int warp = (vg.bid * blockDim.x + threadIdx.x) >> 5;
   const int lane = threadIdx.x & 31;
   if (warp >= n) return;
   const int i = warp;
@@ -293,10 +293,10 @@ __global__ void k_verlet_images(int n, const double *__restrict__ rx, const doub
 // Vacuum sub-system: every pair (k != i), no images, the shift field zero and marked
 // minimum image; pairs dropped by the vapor softcore options (intermolecular: different
 // molecules; intramolecular: the same molecule; PermanentFieldRegion.java:665-670).
-__global__ void k_vacuum_pairs(int n, const int *__restrict__ mol, int inter, int intra, int cap, int *nbr,
+__device__ __forceinline__ void k_vacuum_pairs(VGrid vg, int n, const int *__restrict__ mol, int inter, int intra, int cap, int *nbr,
                                int *nbr_sh, int *nbr_cnt, int *flags) {
   if (!(*flags & FLAG_REBUILD)) return;
-  const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const int warp = (vg.bid * blockDim.x + threadIdx.x) >> 5;
   const int lane = threadIdx.x & 31;
   if (warp >= n) return;
   const int i = warp;
@@ -324,24 +324,32 @@ __global__ void k_vacuum_pairs(int n, const int *__restrict__ mol, int inter, in
   }
 }
 
-__global__ void k_list_done(int n, double *refx, double *refy, double *refz, const double *__restrict__ rx,
+__device__ __forceinline__ void k_list_done(VGrid vg, int n, double *refx, double *refy, double *refz, const double *__restrict__ rx,
                             const double *__restrict__ ry, const double *__restrict__ rz, const int *flags) {
   if (!(*flags & FLAG_REBUILD)) return;
-  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  const int i = vg.bid * blockDim.x + threadIdx.x;
   if (i >= n) return;
   refx[i] = rx[i]; refy[i] = ry[i]; refz[i] = rz[i];
+}
+
+// Cell counts and cursors cleared before a rebuild.
+__device__ __forceinline__ void k_cell_clear(VGrid vg, int m, int *cnt, const int *flags) {
+  if (!(*flags & FLAG_REBUILD)) return;
+  for (int j = vg.bid * blockDim.x + threadIdx.x; j < m; j += vg.nblk * blockDim.x) cnt[j] = 0;
 }
 
 // ---------------------------------------------------------------------------
 void launch_set_coordinates(Handle &h, const double *d_xyz) {
   const int n = h.n;
-  k_set_coordinates<<<nblocks(n, 256), 256, 0, h.stream>>>(n, d_xyz, h.d_redp, h.d_redf, h.d_x, h.d_y, h.d_z,
-                                                            h.d_rx, h.d_ry, h.d_rz, h.d_pos);
+  launch_on<k_set_coordinates, 0, 0>(h.rec, nblocks(n, 256), 256, 0, h.stream, n, d_xyz, (const int *)h.d_redp,
+                                     (const double *)h.d_redf, h.d_x, h.d_y, h.d_z, h.d_rx, h.d_ry, h.d_rz, h.d_pos);
   FFX_LAUNCHED(h);
   const double hb = 0.5 * h.prm.list_buffer;
-  k_reduce_coordinates<<<nblocks(n, 256), 256, 0, h.stream>>>(n, h.d_x, h.d_y, h.d_z, h.d_redp, h.d_redf, h.d_rx,
-                                                               h.d_ry, h.d_rz, h.d_refx, h.d_refy, h.d_refz,
-                                                               hb * hb, h.d_flags, h.d_vtype, h.d_rpos);
+  launch_on<k_reduce_coordinates, 0, 0>(h.rec, nblocks(n, 256), 256, 0, h.stream, n, (const double *)h.d_x,
+                                        (const double *)h.d_y, (const double *)h.d_z, (const int *)h.d_redp,
+                                        (const double *)h.d_redf, h.d_rx, h.d_ry, h.d_rz, (const double *)h.d_refx,
+                                        (const double *)h.d_refy, (const double *)h.d_refz, hb * hb, h.d_flags,
+                                        (const int *)h.d_vtype, h.d_rpos);
   FFX_LAUNCHED(h);
 }
 
@@ -368,39 +376,44 @@ void launch_neighbor_list(Handle &h, bool force) {
   }
   const double rl = fmax(h.prm.vdw_cutoff, h.prm.ewald_cutoff) + h.prm.list_buffer;
   const double rn = h.prm.ewald_cutoff + h.prm.list_buffer + 2.0 * kNearDelta;
+  const int warps = nblocks((int64_t)n * 32, 256);
+  const double *rx = h.d_rx, *ry = h.d_ry, *rz = h.d_rz;
+  const int *flags = h.d_flags;
   if (h.vacuum) {
-    k_vacuum_pairs<<<nblocks((int64_t)n * 32, 256), 256, 0, h.stream>>>(n, h.d_mol, h.alch.inter, h.alch.intra,
-                                                                        h.cap_nbr, h.d_nbr, h.d_nbr_sh, h.d_nbr_cnt,
-                                                                        h.d_flags);
-    k_list_done<<<nblocks(n, 256), 256, 0, h.stream>>>(n, h.d_refx, h.d_refy, h.d_refz, h.d_rx, h.d_ry, h.d_rz,
-                                                        h.d_flags);
+    launch_on<k_vacuum_pairs, 0, 0>(h.rec, warps, 256, 0, h.stream, n, (const int *)h.d_mol, h.alch.inter,
+                                    h.alch.intra, h.cap_nbr, h.d_nbr, h.d_nbr_sh, h.d_nbr_cnt, h.d_flags);
+    launch_on<k_list_done, 0, 0>(h.rec, nblocks(n, 256), 256, 0, h.stream, n, h.d_refx, h.d_refy, h.d_refz, rx, ry,
+                                 rz, flags);
     h.launches += 2;
     return;
   }
   if (h.images) {
-    k_verlet_images<<<nblocks((int64_t)n * 32, 256), 256, 0, h.stream>>>(
-        n, h.d_rx, h.d_ry, h.d_rz, h.box, h.img_range[0], h.img_range[1], h.img_range[2], rl * rl, h.cap_nbr,
-        h.d_nbr, h.d_nbr_sh, h.d_nbr_cnt, h.d_flags, h.img_super, h.img_rep[0], h.img_rep[1], h.img_rep[2]);
-    k_list_done<<<nblocks(n, 256), 256, 0, h.stream>>>(n, h.d_refx, h.d_refy, h.d_refz, h.d_rx, h.d_ry, h.d_rz,
-                                                        h.d_flags);
+    launch_on<k_verlet_images, 0, 0>(h.rec, warps, 256, 0, h.stream, n, rx, ry, rz, h.box, h.img_range[0],
+                                     h.img_range[1], h.img_range[2], rl * rl, h.cap_nbr, h.d_nbr, h.d_nbr_sh,
+                                     h.d_nbr_cnt, h.d_flags, h.img_super, h.img_rep[0], h.img_rep[1], h.img_rep[2]);
+    launch_on<k_list_done, 0, 0>(h.rec, nblocks(n, 256), 256, 0, h.stream, n, h.d_refx, h.d_refy, h.d_refz, rx, ry,
+                                 rz, flags);
     h.launches += 2;
     return;
   }
   const int ncells = h.ncell[0] * h.ncell[1] * h.ncell[2];
-  cudaMemsetAsync(h.d_cell_cnt, 0, sizeof(int) * (size_t)ncells * 2, h.stream);  // counts and cursors
-  k_cell_count<<<nblocks(n, 256), 256, 0, h.stream>>>(n, h.d_rx, h.d_ry, h.d_rz, h.box, h.ncell[0], h.ncell[1],
-                                                       h.ncell[2], h.d_cell_cnt, h.d_atom_cell, h.d_flags);
-  k_cell_scan<<<1, 1024, 0, h.stream>>>(ncells, h.d_cell_cnt, h.d_cell_start, h.d_flags);
-  k_cell_fill<<<nblocks(n, 256), 256, 0, h.stream>>>(n, h.d_atom_cell, h.d_cell_start, h.d_cell_atoms,
-                                                      h.d_cell_cnt + ncells, h.d_flags);
-  k_cell_sort<<<nblocks(ncells, 128), 128, 0, h.stream>>>(ncells, h.d_cell_start, h.d_cell_atoms, h.d_flags);
-  k_verlet<<<nblocks((int64_t)n * 32, 256), 256, 0, h.stream>>>(
-      n, h.d_rx, h.d_ry, h.d_rz, h.box, cell_offsets(h.ncell), h.d_atom_cell, h.d_cell_start, h.d_cell_atoms,
-      rl * rl, h.cap_nbr, h.d_nbr, h.d_nbr_cnt, h.d_flags, rn * rn, h.cap_nbl, h.near_list ? h.d_nbl : nullptr,
-      h.d_nbl_cnt);
-  k_list_done<<<nblocks(n, 256), 256, 0, h.stream>>>(n, h.d_refx, h.d_refy, h.d_refz, h.d_rx, h.d_ry, h.d_rz,
-                                                      h.d_flags);
-  h.launches += 6;
+  launch_on<k_cell_clear, 0, 0>(h.rec, nblocks(2 * ncells, 256), 256, 0, h.stream, 2 * ncells, h.d_cell_cnt,
+                                flags);   // counts and cursors
+  launch_on<k_cell_count, 0, 0>(h.rec, nblocks(n, 256), 256, 0, h.stream, n, rx, ry, rz, h.box, h.ncell[0],
+                                h.ncell[1], h.ncell[2], h.d_cell_cnt, h.d_atom_cell, flags);
+  launch_on<k_cell_scan, 0, 0>(h.rec, 1, 1024, 0, h.stream, ncells, (const int *)h.d_cell_cnt, h.d_cell_start,
+                               flags);
+  launch_on<k_cell_fill, 0, 0>(h.rec, nblocks(n, 256), 256, 0, h.stream, n, (const int *)h.d_atom_cell,
+                               (const int *)h.d_cell_start, h.d_cell_atoms, h.d_cell_cnt + ncells, flags);
+  launch_on<k_cell_sort, 0, 0>(h.rec, nblocks(ncells, 128), 128, 0, h.stream, ncells, (const int *)h.d_cell_start,
+                               h.d_cell_atoms, flags);
+  launch_on<k_verlet, 0, 0>(h.rec, warps, 256, 0, h.stream, n, rx, ry, rz, h.box, cell_offsets(h.ncell),
+                            (const int *)h.d_atom_cell, (const int *)h.d_cell_start, (const int *)h.d_cell_atoms,
+                            rl * rl, h.cap_nbr, h.d_nbr, h.d_nbr_cnt, h.d_flags, rn * rn, h.cap_nbl,
+                            h.near_list ? h.d_nbl : (int *)nullptr, h.d_nbl_cnt);
+  launch_on<k_list_done, 0, 0>(h.rec, nblocks(n, 256), 256, 0, h.stream, n, h.d_refx, h.d_refy, h.d_refz, rx, ry, rz,
+                               flags);
+  h.launches += 7;
 }
 
 }  // namespace ffx

@@ -63,11 +63,11 @@ __device__ __forceinline__ double warp_total(const double *__restrict__ part, in
   return warp_sum(s);
 }
 
-// Block sum of NV per-thread values into part[blockIdx.x][0 .. NV); the last block to
+// Block sum of NV per-thread values into part[vg.bid][0 .. NV); the last block to
 // finish sums all rows in block order into tot[t0 .. t0 + NV) and re-arms the counter.
 // Returns true in the last block (all threads).
 template <int NV>
-__device__ __forceinline__ bool block_partials(const double *v, double *part, unsigned *counter, double *tot,
+__device__ __forceinline__ bool block_partials(VGrid vg, const double *v, double *part, unsigned *counter, double *tot,
                                                int t0) {
   __shared__ double sh[NV][32];
   __shared__ bool last;
@@ -81,17 +81,17 @@ __device__ __forceinline__ bool block_partials(const double *v, double *part, un
   if (threadIdx.x < NV) {
     double s = 0.0;
     for (int w = 0; w < nw; w++) s += sh[threadIdx.x][w];
-    part[blockIdx.x * 8 + threadIdx.x] = s;
+    part[vg.bid * 8 + threadIdx.x] = s;
   }
   __threadfence();
   __syncthreads();
-  if (threadIdx.x == 0) last = (atomicAdd(counter, 1u) == gridDim.x - 1);
+  if (threadIdx.x == 0) last = (atomicAdd(counter, 1u) == vg.nblk - 1);
   __syncthreads();
   if (last && threadIdx.x < 32) {
     __threadfence();
 #pragma unroll
     for (int q = 0; q < NV; q++) {
-      const double t = warp_total(part, gridDim.x, q);
+      const double t = warp_total(part, vg.nblk, q);
       if (threadIdx.x == 0) tot[t0 + q] = t;
     }
     if (threadIdx.x == 0) *counter = 0u;
@@ -100,9 +100,9 @@ __device__ __forceinline__ bool block_partials(const double *v, double *part, un
 }
 
 // Block sum of NV values already reduced to lane 0 of each warp, stored as
-// part[blockIdx.x][0 .. NV) (no atomics; beta_block or k_pcg_update finishes the sum).
+// part[vg.bid][0 .. NV) (no atomics; beta_block or k_pcg_update finishes the sum).
 template <int NV>
-__device__ __forceinline__ void block_store_lane0(const double *v, double *part) {
+__device__ __forceinline__ void block_store_lane0(VGrid vg, const double *v, double *part) {
   __shared__ double sh[NV][32];
   const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = blockDim.x >> 5;
   if (lane == 0) {
@@ -113,7 +113,7 @@ __device__ __forceinline__ void block_store_lane0(const double *v, double *part)
   if (threadIdx.x < NV) {
     double s = 0.0;
     for (int w = 0; w < nw; w++) s += sh[threadIdx.x][w];
-    part[blockIdx.x * 8 + threadIdx.x] = s;
+    part[vg.bid * 8 + threadIdx.x] = s;
   }
 }
 
@@ -183,12 +183,12 @@ __device__ __forceinline__ void pair_field(int i, int sub, const int *__restrict
 #pragma unroll
     for (int u = 0; u < NU; u++) {
       ix[u] = (a + G * u < cnt) ? a + G * u : a;
-      kk[u] = row[ix[u]];
+      kk[u] = __ldg(row + ix[u]);
     }
 #pragma unroll
     for (int u = 0; u < NU; u++) {
       load_pair(pr, e0 + ix[u], xx[u], yy[u], zz[u], AA[u]);
-      BB[u] = pb[e0 + ix[u]];
+      BB[u] = __ldg(pb + e0 + ix[u]);
       get_rec(rec, kk[u], ss[u]);
     }
 #pragma unroll
@@ -251,7 +251,7 @@ __device__ __forceinline__ void mesh_field(int i, int n, const int *__restrict__
 // out[6][n] (D xyz, CR xyz).  A group of G lanes takes one atom; the groups of a warp take
 // consecutive atoms and stride over the system together.
 template <typename T, int G>
-__global__ void __launch_bounds__(kFieldThreads) k_pair_field(int n, const int *__restrict__ ewl,
+__device__ __forceinline__ void k_pair_field(VGrid vg, int n, const int *__restrict__ ewl,
                                                               const int *__restrict__ ewl_cnt, int capE,
                                                               const PairRec<T> *__restrict__ coefE,
                                                               const T *__restrict__ coefEB,
@@ -260,11 +260,11 @@ __global__ void __launch_bounds__(kFieldThreads) k_pair_field(int n, const int *
                                                               double *tot) {
   // Block 0 first forms beta from the preconditioner's partial rows (the combine, after
   // the join, reads it): no separate totals launch on the solver's chain.
-  if (beta_part && blockIdx.x == 0) beta_block(beta_part, beta_rows, tot);
+  if (beta_part && vg.bid == 0) beta_block(beta_part, beta_rows, tot);
   constexpr int GPW = 32 / G;
   const int lane = threadIdx.x & 31, sub = lane & (G - 1), gi = lane / G;
-  const int astride = gridDim.x * (blockDim.x >> 5) * GPW;
-  for (int i0 = (blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5)) * GPW; i0 < n; i0 += astride) {
+  const int astride = vg.nblk * (blockDim.x >> 5) * GPW;
+  for (int i0 = (vg.bid * (blockDim.x >> 5) + (threadIdx.x >> 5)) * GPW; i0 < n; i0 += astride) {
     const int i = i0 + gi;
     const bool live = i < n;
     T a6[6] = {0, 0, 0, 0, 0, 0};
@@ -289,15 +289,15 @@ __global__ void __launch_bounds__(kFieldThreads) k_pair_field(int n, const int *
 // One warp per atom: all lanes interpolate the mesh, then lane q < 6 finishes component
 // q (D x, y, z, CR x, y, z).
 template <int MODE, typename T>
-__global__ void __launch_bounds__(256) k_pcg_combine(
+__device__ __forceinline__ void k_pcg_combine(VGrid vg, 
     int n, const int *__restrict__ igrid, const T *__restrict__ spl, const typename Vec2<T>::type *__restrict__ mesh,
-    int nfx, int nfy, int nfz, const __grid_constant__ FieldXform xf, const double *__restrict__ tpair, const double *__restrict__ vD,
+    int nfx, int nfy, int nfz, const FieldXform &xf, const double *__restrict__ tpair, const double *__restrict__ vD,
     const double *__restrict__ vP, double aewald3, const double *__restrict__ polar,
     const double *__restrict__ udirD, const double *__restrict__ udirP, double *p, double *pP, double *tp,
     int first, const double *__restrict__ r, const double *__restrict__ rP, double *outD, double *outP, T *recP,
     double *part, unsigned *counter, double *tot) {
   const int lane = threadIdx.x & 31;
-  const int i = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const int i = (vg.bid * blockDim.x + threadIdx.x) >> 5;
   double acc[4] = {0, 0, 0, 0};
   if (i < n) {
     T a6[6] = {0, 0, 0, 0, 0, 0};
@@ -356,7 +356,7 @@ __global__ void __launch_bounds__(256) k_pcg_combine(
     for (int q = 0; q < 4; q++)
 #pragma unroll
       for (int o = 4; o > 0; o >>= 1) acc[q] += __shfl_xor_sync(0xffffffffu, acc[q], o);
-    block_store_lane0<4>(acc, part);
+    block_store_lane0<4>(vg, acc, part);
   }
 }
 
@@ -365,7 +365,7 @@ __global__ void __launch_bounds__(256) k_pcg_combine(
 // is finished into d_scalars and the last block forms beta = r.z_new / r.z_old
 // (UpdateConjugateLoop, Fletcher-Reeves; a zero r.z_old counts as 1).
 template <bool INIT, typename T, int G>
-__global__ void __launch_bounds__(kFieldThreads) k_pcg_precond(
+__device__ __forceinline__ void k_pcg_precond(VGrid vg, 
     int n, const int *__restrict__ prl, const int *__restrict__ prl_cnt, int capP,
     const PairRec<T> *__restrict__ coefP, const T *__restrict__ coefPB, const T *__restrict__ recP,
     const double *__restrict__ polar, const double *__restrict__ r, const double *__restrict__ rP, double s,
@@ -373,9 +373,9 @@ __global__ void __launch_bounds__(kFieldThreads) k_pcg_precond(
   constexpr int GPW = 32 / G;
   constexpr int QPL = (6 + G - 1) / G;   // components finished per lane: q = sub, sub + G, ...
   const int lane = threadIdx.x & 31, sub = lane & (G - 1), gi = lane / G, g0 = lane & ~(G - 1);
-  const int astride = gridDim.x * (blockDim.x >> 5) * GPW;
+  const int astride = vg.nblk * (blockDim.x >> 5) * GPW;
   double acc[2] = {0, 0};
-  for (int i0 = (blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5)) * GPW; i0 < n; i0 += astride) {
+  for (int i0 = (vg.bid * (blockDim.x >> 5) + (threadIdx.x >> 5)) * GPW; i0 < n; i0 += astride) {
     const int i = i0 + gi;
     const bool live = i < n;
     T a6[6] = {0, 0, 0, 0, 0, 0};
@@ -412,7 +412,7 @@ __global__ void __launch_bounds__(kFieldThreads) k_pcg_precond(
   if (!INIT) {
 #pragma unroll
     for (int q = 0; q < 2; q++) acc[q] = group_sum<32>(acc[q]);
-    block_store_lane0<2>(acc, part);
+    block_store_lane0<2>(vg, acc, part);
   }
 }
 
@@ -421,7 +421,7 @@ __global__ void __launch_bounds__(kFieldThreads) k_pcg_precond(
 // is not finite) or the iteration limit is reached, stop converged when eps < polar-eps.
 // A list overflow seen earlier in the evaluation also stops the loop (the host repeats
 // the evaluation with larger lists).
-__global__ void k_pcg_reset(PcgState *st) {
+__device__ __forceinline__ void k_pcg_reset(VGrid vg, PcgState *st) {
   st->eps = 100.0;
   st->iter = 0;
   st->status = FFXG_OK;
@@ -433,7 +433,7 @@ __global__ void k_pcg_reset(PcgState *st) {
 // rules to PcgState, re-arms the counter and, inside a captured graph, sets the
 // condition of the PCG while node.
 template <typename T>
-__global__ void __launch_bounds__(kVecThreads) k_pcg_update(
+__device__ __forceinline__ void k_pcg_update(VGrid vg, 
     int n, const double *__restrict__ vec, const double *__restrict__ vecP, const double *__restrict__ p,
     const double *__restrict__ pP, double *r, double *rP, double *uD, double *uP, double *tot,
     double *partE, unsigned *counter, PcgState *st, int max_iter, double polar_eps, const int *flags,
@@ -472,7 +472,7 @@ __global__ void __launch_bounds__(kVecThreads) k_pcg_update(
       double t = 0.0;
       for (int w = 0; w < (int)(blockDim.x >> 5); w++) t += tsum[threadIdx.x][w];
       tv[threadIdx.x] = t;
-      if (blockIdx.x == 0) tot[T_PAP + threadIdx.x] = t;
+      if (vg.bid == 0) tot[T_PAP + threadIdx.x] = t;
     }
     __syncthreads();
   }
@@ -480,8 +480,8 @@ __global__ void __launch_bounds__(kVecThreads) k_pcg_update(
   const double alpha0 = (pap != 0.0) ? rz / pap : rz;
   const double alpha1 = (papP != 0.0) ? rzP / papP : rzP;
   double v[2] = {0.0, 0.0};
-  const int stride = gridDim.x * blockDim.x;
-  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) {
+  const int stride = vg.nblk * blockDim.x;
+  for (int i = vg.bid * blockDim.x + threadIdx.x; i < n; i += stride) {
     // Every load first (one memory round trip), then the arithmetic, then the stores.
     double r0[3], r1[3], v0[3], v1[3], p0[3], p1[3], u0[3], u1[3];
 #pragma unroll
@@ -511,7 +511,7 @@ __global__ void __launch_bounds__(kVecThreads) k_pcg_update(
     put_rec(recP, i, a * nr[0], a * nr[1], a * nr[2], a * nr[3], a * nr[4], a * nr[5]);
   }
   __shared__ double norms[2];
-  if (block_partials<2>(v, partE, counter, norms, 0) && threadIdx.x == 0) {
+  if (block_partials<2>(vg, v, partE, counter, norms, 0) && threadIdx.x == 0) {
     const double e0 = norms[0], e1 = norms[1];
     const double m = (e0 < e1) ? e1 : e0;
     const double eps = kElecAngToDebye * sqrt(m / (double)n_eps);
@@ -542,10 +542,10 @@ __global__ void __launch_bounds__(kVecThreads) k_pcg_update(
 // ring[6][6][n] holds u - u_dir (D xyz, CR xyz) of the last six converged solves; state[0]
 // is the slot of the most recent one and state[1] how many are stored.  With six stored,
 // the solve starts from u = u_dir + sum_k c_k ring[(state[0] + k) % 6].
-__global__ void k_aspc_predict(int n, const double *__restrict__ ring, const int *__restrict__ state,
+__device__ __forceinline__ void k_aspc_predict(VGrid vg, int n, const double *__restrict__ ring, const int *__restrict__ state,
                                const double *__restrict__ udD, const double *__restrict__ udP, double *uD, double *uP,
                                void *recF, int mixed) {
-  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  const int i = vg.bid * blockDim.x + threadIdx.x;
   if (i >= n || state[1] < 6) return;
   const double c[6] = {22.0 / 7.0, -55.0 / 14.0, 55.0 / 21.0, -22.0 / 21.0, 5.0 / 21.0, -1.0 / 42.0};
   double u[6];
@@ -565,10 +565,10 @@ __global__ void k_aspc_predict(int n, const double *__restrict__ ring, const int
 
 // Store u - u_dir of a converged solve in the slot before state[0] (k_aspc_commit then
 // advances the state); nothing is stored after a failed solve or a list overflow.
-__global__ void k_aspc_save(int n, double *ring, const int *__restrict__ state, const double *__restrict__ uD,
+__device__ __forceinline__ void k_aspc_save(VGrid vg, int n, double *ring, const int *__restrict__ state, const double *__restrict__ uD,
                             const double *__restrict__ uP, const double *__restrict__ udD,
                             const double *__restrict__ udP, const PcgState *__restrict__ st, const int *flags) {
-  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  const int i = vg.bid * blockDim.x + threadIdx.x;
   if (i >= n || st->status != FFXG_OK) return;
   if (*flags & (FLAG_NBR_OVERFLOW | FLAG_EWALD_OVERFLOW | FLAG_PRECOND_OVERFLOW | FLAG_NONFINITE)) return;
   const int slot = (state[0] + 5) % 6;
@@ -578,7 +578,7 @@ __global__ void k_aspc_save(int n, double *ring, const int *__restrict__ state, 
   }
 }
 
-__global__ void k_aspc_commit(int *state, const PcgState *__restrict__ st, const int *flags) {
+__device__ __forceinline__ void k_aspc_commit(VGrid vg, int *state, const PcgState *__restrict__ st, const int *flags) {
   if (st->status != FFXG_OK) return;
   if (*flags & (FLAG_NBR_OVERFLOW | FLAG_EWALD_OVERFLOW | FLAG_PRECOND_OVERFLOW | FLAG_NONFINITE)) return;
   state[0] = (state[0] + 5) % 6;
@@ -587,16 +587,20 @@ __global__ void k_aspc_commit(int *state, const PcgState *__restrict__ st, const
 
 static void aspc_predict(Handle &h) {
   if (h.scf_predictor != FFXG_PREDICTOR_ASPC) return;
-  k_aspc_predict<<<nblocks(h.n, 256), 256, 0, h.stream>>>(h.n, h.d_aspc, h.d_aspc_state, h.d_udirD, h.d_udirP, h.d_uD,
-                                                           h.d_uP, h.d_recF, h.mixed ? 1 : 0);
+  launch_on<k_aspc_predict, 0, 0>(h.rec, nblocks(h.n, 256), 256, 0, h.stream, h.n, (const double *)h.d_aspc,
+                                   (const int *)h.d_aspc_state, (const double *)h.d_udirD,
+                                   (const double *)h.d_udirP, h.d_uD, h.d_uP, (void *)h.d_recF, h.mixed ? 1 : 0);
   FFX_LAUNCHED(h);
 }
 
 static void aspc_save(Handle &h) {
   if (h.scf_predictor != FFXG_PREDICTOR_ASPC) return;
-  k_aspc_save<<<nblocks(h.n, 256), 256, 0, h.stream>>>(h.n, h.d_aspc, h.d_aspc_state, h.d_uD, h.d_uP, h.d_udirD,
-                                                        h.d_udirP, h.d_pcg, h.d_flags);
-  k_aspc_commit<<<1, 1, 0, h.stream>>>(h.d_aspc_state, h.d_pcg, h.d_flags);
+  launch_on<k_aspc_save, 0, 0>(h.rec, nblocks(h.n, 256), 256, 0, h.stream, h.n, h.d_aspc,
+                                (const int *)h.d_aspc_state, (const double *)h.d_uD, (const double *)h.d_uP,
+                                (const double *)h.d_udirD, (const double *)h.d_udirP, (const PcgState *)h.d_pcg,
+                                (const int *)h.d_flags);
+  launch_on<k_aspc_commit, 0, 0>(h.rec, 1, 1, 0, h.stream, h.d_aspc_state, (const PcgState *)h.d_pcg,
+                                  (const int *)h.d_flags);
   h.launches += 2;
 }
 
@@ -614,10 +618,11 @@ static double *part_region(const Handle &h, int k) { return h.d_part2 + (size_t)
 
 template <typename T>
 static void pair_field_launch(Handle &h, cudaStream_t st, bool beta) {
-  k_pair_field<T, kEwaldGroup><<<group_blocks(h.n, kEwaldGroup), kFieldThreads, 0, st>>>(
-      h.n, h.d_ewl, h.d_ewl_cnt, h.cap_ewl, reinterpret_cast<const PairRec<T> *>(h.d_coefE),
+  launch_on<k_pair_field<T, kEwaldGroup>, kFieldThreads, 0>(
+      h.rec, group_blocks(h.n, kEwaldGroup), kFieldThreads, 0, st, h.n, (const int *)h.d_ewl,
+      (const int *)h.d_ewl_cnt, h.cap_ewl, reinterpret_cast<const PairRec<T> *>(h.d_coefE),
       reinterpret_cast<const T *>(h.d_coefEB), reinterpret_cast<const T *>(h.d_recF), h.d_tpair,
-      beta ? part_region(h, 1) : nullptr, group_blocks(h.n, kPrecondGroup), h.d_scalars);
+      (const double *)(beta ? part_region(h, 1) : nullptr), group_blocks(h.n, kPrecondGroup), h.d_scalars);
   FFX_LAUNCHED(h);
 }
 
@@ -628,10 +633,12 @@ static void combine(Handle &h, const double *vD, const double *vP, bool first, d
   for (int a = 0; a < 3; a++)
     for (int b = 0; b < 3; b++) xf.m[a][b] = h.pc.tfm[1 + a][1 + b];
   const V2 *mesh = reinterpret_cast<const V2 *>(h.mixed ? (const void *)h.d_gridf : (const void *)h.d_grid);
-  k_pcg_combine<MODE, T><<<combine_blocks(h.n), 256, 0, h.stream>>>(
-      h.n, h.d_igrid, reinterpret_cast<const T *>(h.d_spl), mesh, h.nfft[0], h.nfft[1], h.nfft[2], xf, h.d_tpair, vD,
-      vP, aewald3_of(h), h.d_polar, h.d_udirD, h.d_udirP, h.d_p, h.d_pP, h.d_tp, first ? 1 : 0, h.d_r, h.d_rP, outD,
-      outP, reinterpret_cast<T *>(h.d_recP), part_region(h, 0), h.d_counter + K_FIELD, h.d_scalars);
+  launch_on<k_pcg_combine<MODE, T>, 256, 0>(
+      h.rec, combine_blocks(h.n), 256, 0, h.stream, h.n, (const int *)h.d_igrid, reinterpret_cast<const T *>(h.d_spl),
+      mesh, h.nfft[0], h.nfft[1], h.nfft[2], xf, (const double *)h.d_tpair, vD, vP, aewald3_of(h),
+      (const double *)h.d_polar, (const double *)h.d_udirD, (const double *)h.d_udirP, h.d_p, h.d_pP, h.d_tp,
+      first ? 1 : 0, (const double *)h.d_r, (const double *)h.d_rP, outD, outP, reinterpret_cast<T *>(h.d_recP),
+      part_region(h, 0), h.d_counter + K_FIELD, h.d_scalars);
   FFX_LAUNCHED(h);
 }
 
@@ -641,20 +648,23 @@ template <int MODE>
 static void field_of(Handle &h, const double *vD, const double *vP, bool first, double *outD, double *outP) {
   // Stage timing (direct launches, ffxg_set_timing) keeps the pair field on the main
   // stream, so that its events time the kernel alone rather than its overlap.
-  cudaStream_t ax = h.timing ? h.stream : ((h.stream == h.side) ? h.aux_side : h.aux);
-  cudaEventRecord(h.ev_fork, h.stream);
-  cudaStreamWaitEvent(ax, h.ev_fork, 0);
+  // A recording batch orders its stages itself: no fork.
+  cudaStream_t ax = (h.timing || h.rec) ? h.stream : ((h.stream == h.side) ? h.aux_side : h.aux);
+  if (!h.rec) {
+    cudaEventRecord(h.ev_fork, h.stream);
+    cudaStreamWaitEvent(ax, h.ev_fork, 0);
+  }
   int tk = timer_begin_on(h, FFXG_STAGE_IND_FIELD, ax);
   // After a non-initial preconditioner step the pair field also forms beta.
   const bool beta = (MODE == 2) && !first;
   if (h.mixed) pair_field_launch<float>(h, ax, beta); else pair_field_launch<double>(h, ax, beta);
   timer_end_on(h, tk, ax);
-  cudaEventRecord(h.ev_join, ax);
+  if (!h.rec) cudaEventRecord(h.ev_join, ax);
   tk = timer_begin(h, FFXG_STAGE_IND_RECIP);
   launch_spread_induced(h, vD, vP);
   launch_fft_convolution(h);
   timer_end(h, tk);
-  cudaStreamWaitEvent(h.stream, h.ev_join, 0);
+  if (!h.rec) cudaStreamWaitEvent(h.stream, h.ev_join, 0);
   tk = timer_begin(h, FFXG_STAGE_PCG_VECTOR);
   if (h.mixed) combine<MODE, float>(h, vD, vP, first, outD, outP);
   else combine<MODE, double>(h, vD, vP, first, outD, outP);
@@ -663,11 +673,12 @@ static void field_of(Handle &h, const double *vD, const double *vP, bool first, 
 
 template <bool INIT, typename T>
 static void precond(Handle &h) {
-  k_pcg_precond<INIT, T, kPrecondGroup><<<group_blocks(h.n, kPrecondGroup), kFieldThreads, 0, h.stream>>>(
-      h.n, h.d_prl, h.d_prl_cnt, h.cap_prl, reinterpret_cast<const PairRec<T> *>(h.d_coefP),
-      reinterpret_cast<const T *>(h.d_coefPB), reinterpret_cast<const T *>(h.d_recP), h.d_polar, h.d_r, h.d_rP,
-      h.prm.precond_scale, h.d_zpre, h.d_zpreP, h.d_p, h.d_pP, reinterpret_cast<T *>(h.d_recF), part_region(h, 1),
-      h.d_counter + K_PRECOND, h.d_scalars);
+  launch_on<k_pcg_precond<INIT, T, kPrecondGroup>, kFieldThreads, 0>(
+      h.rec, group_blocks(h.n, kPrecondGroup), kFieldThreads, 0, h.stream, h.n, (const int *)h.d_prl,
+      (const int *)h.d_prl_cnt, h.cap_prl, reinterpret_cast<const PairRec<T> *>(h.d_coefP),
+      reinterpret_cast<const T *>(h.d_coefPB), reinterpret_cast<const T *>(h.d_recP), (const double *)h.d_polar,
+      (const double *)h.d_r, (const double *)h.d_rP, h.prm.precond_scale, h.d_zpre, h.d_zpreP, h.d_p, h.d_pP,
+      reinterpret_cast<T *>(h.d_recF), part_region(h, 1), h.d_counter + K_PRECOND, h.d_scalars);
   FFX_LAUNCHED(h);
 }
 
@@ -678,11 +689,12 @@ static void launch_precond(Handle &h) {
 
 template <typename T>
 static void update(Handle &h, cudaGraphConditionalHandle cond, int use_cond) {
-  k_pcg_update<T><<<vec_blocks(h.n), kVecThreads, 0, h.stream>>>(
-      h.n, h.d_vec, h.d_vecP, h.d_p, h.d_pP, h.d_r, h.d_rP, h.d_uD, h.d_uP, h.d_scalars, part_region(h, 2),
-      h.d_counter + K_UPDATE, h.d_pcg, h.prm.max_scf_iter, h.prm.polar_eps, h.d_flags, cond, use_cond, h.d_polar,
-      reinterpret_cast<T *>(h.d_recP), h.eps_atoms > 0 ? h.eps_atoms : h.n, part_region(h, 0),
-      combine_blocks(h.n));
+  launch_on<k_pcg_update<T>, kVecThreads, 0>(
+      h.rec, vec_blocks(h.n), kVecThreads, 0, h.stream, h.n, (const double *)h.d_vec, (const double *)h.d_vecP,
+      (const double *)h.d_p, (const double *)h.d_pP, h.d_r, h.d_rP, h.d_uD, h.d_uP, h.d_scalars, part_region(h, 2),
+      h.d_counter + K_UPDATE, h.d_pcg, h.prm.max_scf_iter, h.prm.polar_eps, (const int *)h.d_flags, cond, use_cond,
+      (const double *)h.d_polar, reinterpret_cast<T *>(h.d_recP), h.eps_atoms > 0 ? h.eps_atoms : h.n,
+      (const double *)part_region(h, 0), combine_blocks(h.n));
   FFX_LAUNCHED(h);
 }
 
@@ -706,7 +718,7 @@ static void pcg_precond(Handle &h) {
 // step) the update kernel re-arms on the device, so the loop runs with no host round
 // trip.  Either way the loop ends by max_scf_iter at the latest.
 int run_pcg(Handle &h, bool capture) {
-  k_pcg_reset<<<1, 1, 0, h.stream>>>(h.d_pcg);
+  launch_on<k_pcg_reset, 0, 0>(h.rec, 1, 1, 0, h.stream, h.d_pcg);
   FFX_LAUNCHED(h);
   aspc_predict(h);
   // Field of the direct dipoles (u == u_dir at entry) gives the initial residual.
@@ -714,6 +726,20 @@ int run_pcg(Handle &h, bool capture) {
   int tk = timer_begin(h, FFXG_STAGE_PRECOND);
   launch_precond<true>(h);
   timer_end(h, tk);
+  if (h.rec) {
+    // A batch records the solve: the first step in line, then the loop body, which the
+    // batch runs as one conditional WHILE node for all its systems (k_many skips the
+    // systems whose solve has stopped).
+    pcg_step(h, true, 0, 0);
+    h.rec->phase = 1;
+    const int64_t before = h.launches;
+    pcg_precond(h);
+    pcg_step(h, false, 0, 0);
+    h.graph_body_launches = h.launches - before;
+    h.rec->phase = 2;
+    aspc_save(h);
+    return FFXG_OK;
+  }
   if (!capture) {
     bool first = true;
     while (true) {

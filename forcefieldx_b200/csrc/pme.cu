@@ -35,10 +35,10 @@ __device__ __forceinline__ void d_norm(double *v) {
   v[0] /= l; v[1] /= l; v[2] /= l;
 }
 
-__global__ void k_rotate(int n, const double *__restrict__ x, const double *__restrict__ y,
+__device__ __forceinline__ void k_rotate(VGrid vg, int n, const double *__restrict__ x, const double *__restrict__ y,
                          const double *__restrict__ z, const int *__restrict__ frame, const int *__restrict__ axis,
                          const double *__restrict__ lmp, double *gm, double *rot) {
-  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  const int i = vg.bid * blockDim.x + threadIdx.x;
   if (i >= n) return;
   double R[3][3] = {{1, 0, 0}, {0, 1, 0}, {0, 0, 1}};
   const int fr = frame[i];
@@ -162,10 +162,10 @@ __device__ __forceinline__ void bspline5(S x, S *out /* [5][4] */) {
 }
 
 template <typename S>
-__global__ void k_bsplines(int n, const double *__restrict__ x, const double *__restrict__ y,
+__device__ __forceinline__ void k_bsplines(VGrid vg, int n, const double *__restrict__ x, const double *__restrict__ y,
                            const double *__restrict__ z, const double *__restrict__ gm, int nfx, int nfy, int nfz,
-                           S *spl, int *igrid, double *fm, PmeConst pc) {
-  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+                           S *spl, int *igrid, double *fm, const PmeConst &pc) {
+  const int i = vg.bid * blockDim.x + threadIdx.x;
   if (i >= n) return;
   const double xi = x[i], yi = y[i], zi = z[i];
   const int nf[3] = {nfx, nfy, nfz};
@@ -244,10 +244,10 @@ __device__ __forceinline__ int wrap1(int v, int m) { return v < 0 ? v + m : (v >
 // support and walks the five z layers, so the per-point work is the B-spline product and
 // the atomic add (no integer division in the loop).
 template <typename S>
-__global__ void k_spread_permanent(int n, const double *__restrict__ fm, const S *__restrict__ spl,
+__device__ __forceinline__ void k_spread_permanent(VGrid vg, int n, const double *__restrict__ fm, const S *__restrict__ spl,
                                    const int *__restrict__ igrid, int nfx, int nfy, int nfz, double2 *grid,
                                    int *flags) {
-  const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const int warp = (vg.bid * blockDim.x + threadIdx.x) >> 5;
   const int lane = threadIdx.x & 31;
   if (warp >= n || lane >= 25) return;
   const int i = warp;
@@ -279,10 +279,10 @@ __global__ void k_spread_permanent(int n, const double *__restrict__ fm, const S
 }
 
 template <typename S>
-__global__ void k_spread_induced(int n, const double *__restrict__ ud, const double *__restrict__ up,
+__device__ __forceinline__ void k_spread_induced(VGrid vg, int n, const double *__restrict__ ud, const double *__restrict__ up,
                                  const S *__restrict__ spl, const int *__restrict__ igrid, int nfx, int nfy,
-                                 int nfz, double2 *grid, PmeConst pc, int *flags) {
-  const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+                                 int nfz, double2 *grid, const PmeConst &pc, int *flags) {
+  const int warp = (vg.bid * blockDim.x + threadIdx.x) >> 5;
   const int lane = threadIdx.x & 31;
   if (warp >= n || lane >= 25) return;
   const int i = warp;
@@ -332,7 +332,15 @@ __device__ __forceinline__ V2 cmul(V2 a, V2 b) {
 // Radix-R Stockham butterfly for one (line, j) pair.  R is a compile-time constant so
 // the R values stay in registers; the small DFTs of R = 2, 3, 4 use their closed
 // forms, R = 5 and 7 use the twiddle table.
-template <int R, typename S>
+// The twiddle table tw is in global memory (GTW: read through the read-only path) or in
+// shared memory (the fixed-length kernels).
+template <typename V2, bool GTW>
+__device__ __forceinline__ V2 tw_at(const V2 *tw, int i) {
+  if constexpr (GTW) return __ldg(tw + i);
+  else return tw[i];
+}
+
+template <int R, typename S, bool GTW = false>
 __device__ __forceinline__ void fft_butterfly(const typename Vec2<S>::type *in, typename Vec2<S>::type *out, int j,
                                               int l, int L, int nb, int Ns, int len, int sg,
                                               const typename Vec2<S>::type *__restrict__ tw) {
@@ -344,7 +352,7 @@ __device__ __forceinline__ void fft_butterfly(const typename Vec2<S>::type *in, 
   for (int r = 0; r < R; r++) {
     V2 a = in[(j + r * nb) * L + l];
     if (r > 0 && k > 0) {
-      V2 w = tw[r * k * tstep];
+      V2 w = tw_at<V2, GTW>(tw, r * k * tstep);
       if (sg > 0) w.y = -w.y;
       a = cmul(a, w);
     }
@@ -382,7 +390,7 @@ __device__ __forceinline__ void fft_butterfly(const typename Vec2<S>::type *in, 
       V2 acc = v[0];
 #pragma unroll
       for (int r = 1; r < R; r++) {
-        V2 w = tw[((r * q) % R) * wstep];
+        V2 w = tw_at<V2, GTW>(tw, ((r * q) % R) * wstep);
         if (sg > 0) w.y = -w.y;
         const V2 m = cmul(v[r], w);
         acc.x += m.x; acc.y += m.y;
@@ -397,7 +405,7 @@ __device__ __forceinline__ void fft_butterfly(const typename Vec2<S>::type *in, 
 // Radix-R pass for any R known only at run time (prime factors above 7, as the general
 // pass of Complex.java:173-330 handles them): each output q of the length-R DFT is summed
 // from the R twiddled inputs read from shared memory, O(R^2) per butterfly.
-template <typename S>
+template <typename S, bool GTW = false>
 __device__ __forceinline__ void fft_butterfly_any(int R, const typename Vec2<S>::type *in,
                                                   typename Vec2<S>::type *out, int j, int l, int L, int nb, int Ns,
                                                   int len, int sg, const typename Vec2<S>::type *__restrict__ tw) {
@@ -411,11 +419,11 @@ __device__ __forceinline__ void fft_butterfly_any(int R, const typename Vec2<S>:
     for (int r = 1; r < R; r++) {
       V2 a = in[(j + r * nb) * L + l];
       if (k > 0) {
-        V2 w = tw[r * k * tstep];
+        V2 w = tw_at<V2, GTW>(tw, r * k * tstep);
         if (sg > 0) w.y = -w.y;
         a = cmul(a, w);
       }
-      V2 w = tw[((r * q) % R) * wstep];
+      V2 w = tw_at<V2, GTW>(tw, ((r * q) % R) * wstep);
       if (sg > 0) w.y = -w.y;
       a = cmul(a, w);
       acc.x += a.x;
@@ -429,7 +437,7 @@ __device__ __forceinline__ void fft_butterfly_any(int R, const typename Vec2<S>:
 // (real plane, then imaginary plane at src + src_ng), converted to FP32 on load and
 // cleared behind the read, so that the next spread starts from zero without a memset.
 template <bool FUSE_G, typename S, bool FROMD>
-__global__ void __launch_bounds__(256) k_fft_axis(typename Vec2<S>::type *grid, FftAxis ax, int sign,
+__device__ __forceinline__ void k_fft_axis(VGrid vg, typename Vec2<S>::type *grid, const FftAxis &ax, int sign,
                                                   const typename Vec2<S>::type *__restrict__ tw,
                                                   const S *__restrict__ G, int gnx, int gny,
                                                   double *src, size_t src_ng, int *flags) {
@@ -441,7 +449,7 @@ __global__ void __launch_bounds__(256) k_fft_axis(typename Vec2<S>::type *grid, 
   V2 *sm = reinterpret_cast<V2 *>(sm_raw);
   const int len = ax.len, L = ax.L;
   V2 *buf0 = sm, *buf1 = sm + (size_t)len * L;
-  const int gi = blockIdx.x % ax.groups_inner, go = blockIdx.x / ax.groups_inner;
+  const int gi = vg.bid % ax.groups_inner, go = vg.bid / ax.groups_inner;
   const size_t base = (size_t)gi * ax.group_step_inner + (size_t)go * ax.group_step_outer;
   const bool contiguous = (ax.stride == 1);
   for (int t = threadIdx.x; t < len * L; t += blockDim.x) {
@@ -469,12 +477,12 @@ __global__ void __launch_bounds__(256) k_fft_axis(typename Vec2<S>::type *grid, 
       for (int t = threadIdx.x; t < nb * L; t += blockDim.x) {
         const int l = t % L, j = t / L;
         switch (R) {
-          case 4: fft_butterfly<4, S>(in, out, j, l, L, nb, Ns, len, sg, tw); break;
-          case 2: fft_butterfly<2, S>(in, out, j, l, L, nb, Ns, len, sg, tw); break;
-          case 3: fft_butterfly<3, S>(in, out, j, l, L, nb, Ns, len, sg, tw); break;
-          case 5: fft_butterfly<5, S>(in, out, j, l, L, nb, Ns, len, sg, tw); break;
-          case 7: fft_butterfly<7, S>(in, out, j, l, L, nb, Ns, len, sg, tw); break;
-          default: fft_butterfly_any<S>(R, in, out, j, l, L, nb, Ns, len, sg, tw); break;
+          case 4: fft_butterfly<4, S, true>(in, out, j, l, L, nb, Ns, len, sg, tw); break;
+          case 2: fft_butterfly<2, S, true>(in, out, j, l, L, nb, Ns, len, sg, tw); break;
+          case 3: fft_butterfly<3, S, true>(in, out, j, l, L, nb, Ns, len, sg, tw); break;
+          case 5: fft_butterfly<5, S, true>(in, out, j, l, L, nb, Ns, len, sg, tw); break;
+          case 7: fft_butterfly<7, S, true>(in, out, j, l, L, nb, Ns, len, sg, tw); break;
+          default: fft_butterfly_any<S, true>(R, in, out, j, l, L, nb, Ns, len, sg, tw); break;
         }
       }
       __syncthreads();
@@ -485,7 +493,7 @@ __global__ void __launch_bounds__(256) k_fft_axis(typename Vec2<S>::type *grid, 
       // Influence function: lines run along z at fixed (x, y) = base + l (line_step 1).
       for (int t = threadIdx.x; t < len * L; t += blockDim.x) {
         const int l = t % L, j = t / L;
-        const S g = G[(size_t)j * gnx * gny + base + (size_t)l * ax.line_step];
+        const S g = __ldg(G + (size_t)j * gnx * gny + base + (size_t)l * ax.line_step);
         in[j * L + l].x *= g;
         in[j * L + l].y *= g;
       }
@@ -633,7 +641,7 @@ __global__ void __cluster_dims__(4, 1, 1) __launch_bounds__(256)
 }
 
 template <int LEN, int L, bool FUSE_G, typename S, bool FROMD>
-__global__ void __launch_bounds__(256) k_fft_fixed(typename Vec2<S>::type *grid, FftAxis ax, int sign,
+__device__ __forceinline__ void k_fft_fixed(VGrid vg, typename Vec2<S>::type *grid, const FftAxis &ax, int sign,
                                                    const typename Vec2<S>::type *__restrict__ twg,
                                                    const S *__restrict__ G, int gnx, int gny,
                                                    double *src, size_t src_ng, int *flags) {
@@ -641,7 +649,7 @@ __global__ void __launch_bounds__(256) k_fft_fixed(typename Vec2<S>::type *grid,
   __shared__ V2 buf[2][LEN * L];
   __shared__ V2 tw[LEN];
   for (int t = threadIdx.x; t < LEN; t += 256) tw[t] = twg[t];
-  const int gi = blockIdx.x % ax.groups_inner, go = blockIdx.x / ax.groups_inner;
+  const int gi = vg.bid % ax.groups_inner, go = vg.bid / ax.groups_inner;
   const size_t base = (size_t)gi * ax.group_step_inner + (size_t)go * ax.group_step_outer;
   const bool contiguous = (ax.stride == 1);
   for (int t = threadIdx.x; t < LEN * L; t += 256) {
@@ -764,11 +772,11 @@ __device__ __forceinline__ void store_phi_warp(int i, int n, S term, double *fph
 }
 
 template <int NT, typename S>
-__global__ void __launch_bounds__(256) k_phi(int n, const S *__restrict__ spl, const int *__restrict__ igrid,
+__device__ __forceinline__ void k_phi(VGrid vg, int n, const S *__restrict__ spl, const int *__restrict__ igrid,
                                              const typename Vec2<S>::type *__restrict__ grid, int nfx, int nfy,
                                              int nfz, double *fphiR, double *cphiR, double *fphiI, double *cphiI,
-                                             const __grid_constant__ PmeConst pc) {
-  const int i = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+                                             const PmeConst &pc) {
+  const int i = (vg.bid * blockDim.x + threadIdx.x) >> 5;
   if (i >= n) return;
   store_phi_warp<NT, S>(i, n, phi_terms_warp<NT, S>(i, n, spl, igrid, grid, nfx, nfy, nfz, false), fphiR, cphiR, pc);
   if (cphiI)
@@ -878,16 +886,36 @@ static FftAxis make_axis(int axis, const int nf[3]) {
 static std::mutex g_fft_smem_mu;
 static std::map<int, int> g_fft_smem;   // device -> current attribute value (bytes)
 
+// The generic FFT pass as launched by fft_convolution, with its argument types fixed so
+// that the instances whose shared-memory limit raise_fft_smem sets are the ones launched.
+template <bool FUSE, typename S, bool FROMD>
+struct FftAxisPass {
+  using V = typename Vec2<S>::type;
+  static void launch(Handle &h, int blocks, size_t smem, V *grid, FftAxis a, int sign, const V *tw, const S *infl,
+                     int nfx, int nfy, double *plane, size_t ng) {
+    launch_on<k_fft_axis<FUSE, S, FROMD>, 256, 0>(h.rec, blocks, 256, smem, h.stream, grid, a, sign, tw, infl, nfx,
+                                                  nfy, plane, ng, h.d_flags);
+  }
+  static cudaError_t raise(int need) {
+    const cudaError_t e1 = cudaFuncSetAttribute(
+        one_fn<k_fft_axis<FUSE, S, FROMD>, 256, 0, V *, FftAxis, int, const V *, const S *, int, int, double *, size_t,
+               int *>(),
+        cudaFuncAttributeMaxDynamicSharedMemorySize, need);
+    const cudaError_t e2 = cudaFuncSetAttribute(
+        many_fn<k_fft_axis<FUSE, S, FROMD>, 256, 0, V *, FftAxis, int, const V *, const S *, int, int, double *, size_t,
+                int *>(),
+        cudaFuncAttributeMaxDynamicSharedMemorySize, need);
+    return e1 != cudaSuccess ? e1 : e2;
+  }
+};
+
 static cudaError_t raise_fft_smem(int device, int need) {
   std::lock_guard<std::mutex> lock(g_fft_smem_mu);
   int &cur = g_fft_smem[device];
   if (need <= cur) return cudaSuccess;
-  const cudaError_t e[5] = {
-      cudaFuncSetAttribute(k_fft_axis<false, double, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, need),
-      cudaFuncSetAttribute(k_fft_axis<true, double, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, need),
-      cudaFuncSetAttribute(k_fft_axis<false, float, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, need),
-      cudaFuncSetAttribute(k_fft_axis<false, float, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, need),
-      cudaFuncSetAttribute(k_fft_axis<true, float, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, need)};
+  const cudaError_t e[5] = {FftAxisPass<false, double, false>::raise(need), FftAxisPass<true, double, false>::raise(need),
+                            FftAxisPass<false, float, false>::raise(need), FftAxisPass<false, float, true>::raise(need),
+                            FftAxisPass<true, float, false>::raise(need)};
   for (cudaError_t q : e)
     if (q != cudaSuccess) return q;
   cur = need;
@@ -1013,23 +1041,38 @@ int setup_pme(Handle &h) {
 
 // ---------------------------------------------------------------------------
 void launch_rotate(Handle &h) {
-  k_rotate<<<nblocks(h.n, 128), 128, 0, h.stream>>>(h.n, h.d_x, h.d_y, h.d_z, h.d_frame, h.d_axis, h.d_lmp, h.d_gm,
-                                                     h.d_rot);
+  launch_on<k_rotate, 0, 0>(h.rec, nblocks(h.n, 128), 128, 0, h.stream, h.n, (const double *)h.d_x,
+                            (const double *)h.d_y, (const double *)h.d_z, (const int *)h.d_frame,
+                            (const int *)h.d_axis, (const double *)h.d_lmp, h.d_gm, h.d_rot);
   FFX_LAUNCHED(h);
 }
 
 void launch_bsplines(Handle &h) {
   if (h.mixed)
-    k_bsplines<float><<<nblocks(h.n, 128), 128, 0, h.stream>>>(h.n, h.d_x, h.d_y, h.d_z, h.d_gm, h.nfft[0], h.nfft[1],
-                                                              h.nfft[2], reinterpret_cast<float *>(h.d_spl), h.d_igrid,
-                                                              h.d_fm, h.pc);
+    launch_on<k_bsplines<float>, 0, 0>(h.rec, nblocks(h.n, 128), 128, 0, h.stream, h.n, (const double *)h.d_x,
+                                       (const double *)h.d_y, (const double *)h.d_z, (const double *)h.d_gm,
+                                       h.nfft[0], h.nfft[1], h.nfft[2], reinterpret_cast<float *>(h.d_spl),
+                                       h.d_igrid, h.d_fm, h.pc);
   else
-    k_bsplines<double><<<nblocks(h.n, 128), 128, 0, h.stream>>>(h.n, h.d_x, h.d_y, h.d_z, h.d_gm, h.nfft[0], h.nfft[1],
-                                                               h.nfft[2], h.d_spl, h.d_igrid, h.d_fm, h.pc);
+    launch_on<k_bsplines<double>, 0, 0>(h.rec, nblocks(h.n, 128), 128, 0, h.stream, h.n, (const double *)h.d_x,
+                                        (const double *)h.d_y, (const double *)h.d_z, (const double *)h.d_gm,
+                                        h.nfft[0], h.nfft[1], h.nfft[2], h.d_spl, h.d_igrid, h.d_fm, h.pc);
   FFX_LAUNCHED(h);
 }
 
 static size_t grid_points(const Handle &h) { return (size_t)h.nfft[0] * h.nfft[1] * h.nfft[2]; }
+
+// The FP64 mesh cleared before a spread.
+__device__ __forceinline__ void k_clear_mesh(VGrid vg, size_t m, double2 *grid) {
+  for (size_t j = (size_t)vg.bid * blockDim.x + threadIdx.x; j < m; j += (size_t)vg.nblk * blockDim.x)
+    grid[j] = make_double2(0.0, 0.0);
+}
+static void clear_mesh(Handle &h) {
+  const size_t m = grid_points(h);
+  launch_on<k_clear_mesh, 0, 0>(h.rec, (int)std::min<size_t>(nblocks((int64_t)m, 256), 4 * (size_t)h.num_sms), 256, 0,
+                                h.stream, m, h.d_grid);
+  FFX_LAUNCHED(h);
+}
 
 // Both forms accumulate into the double mesh d_grid; the FP64 form clears it first, the
 // mixed form keeps it clear between uses (its first FFT pass zeroes what it reads) and
@@ -1037,33 +1080,37 @@ static size_t grid_points(const Handle &h) { return (size_t)h.nfft[0] * h.nfft[1
 void launch_spread_permanent(Handle &h) {
   if (h.vacuum) return;   // no reciprocal space: the mesh and potentials stay zero
   const int nb = nblocks((int64_t)h.n * 32, 256);
-  if (!h.mixed) cudaMemsetAsync(h.d_grid, 0, grid_points(h) * sizeof(double2), h.stream);
+  if (!h.mixed) clear_mesh(h);
   if (h.mixed)
-    k_spread_permanent<float><<<nb, 256, 0, h.stream>>>(h.n, h.d_fm, reinterpret_cast<const float *>(h.d_spl),
-                                                        h.d_igrid, h.nfft[0], h.nfft[1], h.nfft[2], h.d_grid,
-                                                        h.d_flags);
+    launch_on<k_spread_permanent<float>, 0, 0>(h.rec, nb, 256, 0, h.stream, h.n, (const double *)h.d_fm,
+                                               reinterpret_cast<const float *>(h.d_spl), (const int *)h.d_igrid,
+                                               h.nfft[0], h.nfft[1], h.nfft[2], h.d_grid, h.d_flags);
   else
-    k_spread_permanent<double><<<nb, 256, 0, h.stream>>>(h.n, h.d_fm, h.d_spl, h.d_igrid, h.nfft[0], h.nfft[1],
-                                                         h.nfft[2], h.d_grid, h.d_flags);
+    launch_on<k_spread_permanent<double>, 0, 0>(h.rec, nb, 256, 0, h.stream, h.n, (const double *)h.d_fm,
+                                                (const double *)h.d_spl, (const int *)h.d_igrid, h.nfft[0],
+                                                h.nfft[1], h.nfft[2], h.d_grid, h.d_flags);
   FFX_LAUNCHED(h);
 }
 
 void launch_spread_induced(Handle &h, const double *ud, const double *up) {
   if (h.vacuum) return;   // no reciprocal space: the mesh and potentials stay zero
   const int nb = nblocks((int64_t)h.n * 32, 256);
-  if (!h.mixed) cudaMemsetAsync(h.d_grid, 0, grid_points(h) * sizeof(double2), h.stream);
+  if (!h.mixed) clear_mesh(h);
   if (h.mixed)
-    k_spread_induced<float><<<nb, 256, 0, h.stream>>>(h.n, ud, up, reinterpret_cast<const float *>(h.d_spl), h.d_igrid,
-                                                      h.nfft[0], h.nfft[1], h.nfft[2], h.d_grid, h.pc, h.d_flags);
+    launch_on<k_spread_induced<float>, 0, 0>(h.rec, nb, 256, 0, h.stream, h.n, ud, up,
+                                             reinterpret_cast<const float *>(h.d_spl), (const int *)h.d_igrid,
+                                             h.nfft[0], h.nfft[1], h.nfft[2], h.d_grid, h.pc, h.d_flags);
   else
-    k_spread_induced<double><<<nb, 256, 0, h.stream>>>(h.n, ud, up, h.d_spl, h.d_igrid, h.nfft[0], h.nfft[1],
-                                                       h.nfft[2], h.d_grid, h.pc, h.d_flags);
+    launch_on<k_spread_induced<double>, 0, 0>(h.rec, nb, 256, 0, h.stream, h.n, ud, up, (const double *)h.d_spl,
+                                              (const int *)h.d_igrid, h.nfft[0], h.nfft[1], h.nfft[2], h.d_grid,
+                                              h.pc, h.d_flags);
   FFX_LAUNCHED(h);
 }
 
 template <typename S>
 static void fft_convolution(Handle &h, typename Vec2<S>::type *grid, const typename Vec2<S>::type *twiddle,
                             const S *influence) {
+  using V = typename Vec2<S>::type;
   const int nfx = h.nfft[0], nfy = h.nfft[1], nfz = h.nfft[2];
   const int maxn = std::max(nfx, std::max(nfy, nfz));
   // The mixed form's accumulation mesh: real plane, then imaginary plane.
@@ -1073,35 +1120,36 @@ static void fft_convolution(Handle &h, typename Vec2<S>::type *grid, const typen
     const FftAxis &a = h.axes[d];
     const int outer = (d == 0) ? nfz : ((d == 1) ? nfz : nfy);
     const int blocks = a.groups_inner * outer;
-    const size_t smem = 2 * (size_t)a.len * a.L * sizeof(typename Vec2<S>::type);
-    const auto *tw = twiddle + (size_t)d * maxn;
+    const size_t smem = 2 * (size_t)a.len * a.L * sizeof(V);
+    const V *tw = twiddle + (size_t)d * maxn;
+    const S *none = nullptr;
     if (a.len == 64 && a.L == 16) {
       if (fuse)
-        k_fft_fixed<64, 16, true, S, false><<<blocks, 256, 0, h.stream>>>(grid, a, sign, tw, influence, nfx, nfy,
-                                                                          nullptr, 0, h.d_flags);
+        launch_on<k_fft_fixed<64, 16, true, S, false>, 256, 0>(h.rec, blocks, 256, 0, h.stream, grid, a, sign, tw,
+                                                               influence, nfx, nfy, (double *)nullptr, (size_t)0,
+                                                               h.d_flags);
       else if (fromd)
-        k_fft_fixed<64, 16, false, S, true><<<blocks, 256, 0, h.stream>>>(grid, a, sign, tw, nullptr, nfx, nfy,
-                                                                          plane, ng, h.d_flags);
+        launch_on<k_fft_fixed<64, 16, false, S, true>, 256, 0>(h.rec, blocks, 256, 0, h.stream, grid, a, sign, tw,
+                                                               none, nfx, nfy, plane, ng, h.d_flags);
       else
-        k_fft_fixed<64, 16, false, S, false><<<blocks, 256, 0, h.stream>>>(grid, a, sign, tw, nullptr, nfx, nfy,
-                                                                           nullptr, 0, h.d_flags);
+        launch_on<k_fft_fixed<64, 16, false, S, false>, 256, 0>(h.rec, blocks, 256, 0, h.stream, grid, a, sign, tw,
+                                                                none, nfx, nfy, (double *)nullptr, (size_t)0,
+                                                                h.d_flags);
       FFX_LAUNCHED(h);
       return;
     }
     if (fuse)
-      k_fft_axis<true, S, false><<<blocks, 256, smem, h.stream>>>(grid, a, sign, tw, influence, nfx, nfy, nullptr,
-                                                                  0, h.d_flags);
+      FftAxisPass<true, S, false>::launch(h, blocks, smem, grid, a, sign, tw, influence, nfx, nfy, nullptr, 0);
     else if (fromd)
-      k_fft_axis<false, S, true><<<blocks, 256, smem, h.stream>>>(grid, a, sign, tw, nullptr, nfx, nfy, plane, ng,
-                                                                  h.d_flags);
+      FftAxisPass<false, S, true>::launch(h, blocks, smem, grid, a, sign, tw, none, nfx, nfy, plane, ng);
     else
-      k_fft_axis<false, S, false><<<blocks, 256, smem, h.stream>>>(grid, a, sign, tw, nullptr, nfx, nfy, nullptr,
-                                                                   0, h.d_flags);
+      FftAxisPass<false, S, false>::launch(h, blocks, smem, grid, a, sign, tw, none, nfx, nfy, nullptr, 0);
     FFX_LAUNCHED(h);
   };
   const bool fromd = (sizeof(S) == 4);   // mixed: the first pass reads the double mesh
-  if (sizeof(S) == 4 && nfx == 64 && nfy == 64 && h.axes[2].len == 64 && h.axes[2].L == 16) {
-    // Mixed form on 64 x 64 planes: xy, z (with the influence function), yx.
+  if (sizeof(S) == 4 && nfx == 64 && nfy == 64 && h.axes[2].len == 64 && h.axes[2].L == 16 && !h.rec) {
+    // Mixed form on 64 x 64 planes: xy, z (with the influence function), yx.  (A recorded
+    // batch takes the per-axis passes instead: a cluster launch cannot span systems.)
     float2 *gf = reinterpret_cast<float2 *>(grid);
     const float2 *tw = reinterpret_cast<const float2 *>(twiddle);
     k_fft_plane64<false, true><<<nfz * 4, 256, 0, h.stream>>>(gf, -1, tw, h.d_grid_planes(), ng, h.d_flags);
@@ -1130,14 +1178,14 @@ template <typename S>
 static void phi(Handle &h, int which) {
   const S *spl = reinterpret_cast<const S *>(h.d_spl);
   const auto *grid = reinterpret_cast<const typename Vec2<S>::type *>(h.mixed ? (void *)h.d_gridf : (void *)h.d_grid);
+  const int nb = nblocks((int64_t)h.n * 32, 256);
   if (which == 0)
-    k_phi<20, S><<<nblocks((int64_t)h.n * 32, 256), 256, 0, h.stream>>>(h.n, spl, h.d_igrid, grid, h.nfft[0],
-                                                                        h.nfft[1], h.nfft[2], h.d_fphi, h.d_cphi,
-                                                                        nullptr, nullptr, h.pc);
+    launch_on<k_phi<20, S>, 256, 0>(h.rec, nb, 256, 0, h.stream, h.n, spl, (const int *)h.d_igrid, grid, h.nfft[0],
+                                    h.nfft[1], h.nfft[2], h.d_fphi, h.d_cphi, (double *)nullptr, (double *)nullptr,
+                                    h.pc);
   else
-    k_phi<20, S><<<nblocks((int64_t)h.n * 32, 256), 256, 0, h.stream>>>(h.n, spl, h.d_igrid, grid, h.nfft[0],
-                                                                        h.nfft[1], h.nfft[2], h.d_fphiI, h.d_cphiI,
-                                                                        h.d_fphiP, h.d_cphiP, h.pc);
+    launch_on<k_phi<20, S>, 256, 0>(h.rec, nb, 256, 0, h.stream, h.n, spl, (const int *)h.d_igrid, grid, h.nfft[0],
+                                    h.nfft[1], h.nfft[2], h.d_fphiI, h.d_cphiI, h.d_fphiP, h.d_cphiP, h.pc);
   FFX_LAUNCHED(h);
 }
 
@@ -1502,13 +1550,17 @@ extern "C" int ffxg_pme_recip_permanent_noalloc(const double *d_xyz, const doubl
     const FftAxis ax = make_axis(d, nf);
     const int outer = (d == 2) ? nf[1] : nf[2];
     const size_t smem = fft_axis_smem(ax);   // <= 32 KB at kNaMaxDim: no attribute needed
-    const cudaError_t e =
-        (pass == 2) ? launch(k_fft_axis<true, double, false>, ax.groups_inner * outer, 256, smem, grid, ax, sign,
-                             (const double2 *)(s->twiddle + d * kNaMaxDim), (const double *)s->influence, nf[0], nf[1],
-                             no_plane, (size_t)0, no_flags)
-                    : launch(k_fft_axis<false, double, false>, ax.groups_inner * outer, 256, smem, grid, ax, sign,
-                             (const double2 *)(s->twiddle + d * kNaMaxDim), no_influence, nf[0], nf[1], no_plane,
-                             (size_t)0, no_flags);
+    using OneFft = void (*)(double2 *, FftAxis, int, const double2 *, const double *, int, int, double *, size_t,
+                            int *);
+    const OneFft f =
+        (pass == 2) ? (OneFft)one_fn<k_fft_axis<true, double, false>, 256, 0, double2 *, FftAxis, int, const double2 *,
+                                     const double *, int, int, double *, size_t, int *>()
+                    : (OneFft)one_fn<k_fft_axis<false, double, false>, 256, 0, double2 *, FftAxis, int,
+                                     const double2 *, const double *, int, int, double *, size_t, int *>();
+    const cudaError_t e = launch(f, ax.groups_inner * outer, 256, smem, grid, ax, sign,
+                                 (const double2 *)(s->twiddle + d * kNaMaxDim),
+                                 pass == 2 ? (const double *)s->influence : no_influence, nf[0], nf[1], no_plane,
+                                 (size_t)0, no_flags);
     if (e != cudaSuccess) return FFXG_ERR_CUDA;
   }
   const int nb = nblocks(n_atoms, kNaThreads);

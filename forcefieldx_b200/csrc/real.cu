@@ -53,17 +53,17 @@ struct Excl {
 // so the field of any dipole set is -A u_k + B (u_k . r) r; entries inside the
 // preconditioner cutoff also store the Ewald-free pair (pme/PCGSolver.java:1300-1331).
 template <typename R>
-__global__ void __launch_bounds__(128, sizeof(R) == 4 ? 8 : 1) k_realspace_field(
-    int n, const double *__restrict__ x, const double *__restrict__ y, const double *__restrict__ z, Box bx,
+__device__ __forceinline__ void k_realspace_field(VGrid vg, 
+    int n, const double *__restrict__ x, const double *__restrict__ y, const double *__restrict__ z, const Box &bx,
     const double *__restrict__ gm, const double *__restrict__ ipdamp, const double *__restrict__ thole,
     const int *__restrict__ nbr, const int *__restrict__ nbr_cnt, int cap, const int *__restrict__ nbr_sh,
     double off2, double pcut2, int *ewl, int *ewl_cnt, int capE, int *ewl_sh, int *prl, int *prl_cnt, int capP,
     PairRec<R> *coefE, R *coefEB,
-    PairRec<R> *coefP, R *coefPB, Excl ex, EwaldCoef ec, const __grid_constant__ ScaleTables c_scales,
+    PairRec<R> *coefP, R *coefPB, const Excl &ex, const EwaldCoef &ec, const ScaleTables &c_scales,
     double *fieldD, double *fieldP, int *flags, const double2 *__restrict__ pos, const R *__restrict__ rec,
     const int *__restrict__ nbl, const int *__restrict__ nbl_cnt, int capN) {
   using V2 = typename Vec2<R>::type;
-  const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const int warp = (vg.bid * blockDim.x + threadIdx.x) >> 5;
   const int lane = threadIdx.x & 31;
   if (warp >= n) return;
   const int i = warp;
@@ -222,10 +222,10 @@ __global__ void __launch_bounds__(128, sizeof(R) == 4 ? 8 : 1) k_realspace_field
 // field; the field rows are completed in place.  Separate from k_realspace_field so that
 // the permanent reciprocal chain can run beside it.
 template <typename R>
-__global__ void k_direct_dipoles(int n, const double *__restrict__ gm, const double *__restrict__ cphi,
+__device__ __forceinline__ void k_direct_dipoles(VGrid vg, int n, const double *__restrict__ gm, const double *__restrict__ cphi,
                                  const double *__restrict__ polar, double aewald3, double *fieldD, double *fieldP,
                                  double *uD, double *uP, double *udD, double *udP, R *recF) {
-  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  const int i = vg.bid * blockDim.x + threadIdx.x;
   if (i >= n) return;
   const double a = polar[i];
   double d[3], q[3];
@@ -270,17 +270,17 @@ __device__ __forceinline__ void real_acc(double *v, int k, double vx, double vy,
 #define FFX_REAL_ENERGY_MIN_BLOCKS 4   // FP32 form: resident 128-thread blocks per SM
 #endif
 template <typename R, bool LAM, bool DIRECT>
-__global__ void __launch_bounds__(128, sizeof(R) == 4 ? FFX_REAL_ENERGY_MIN_BLOCKS : 1) k_real_energy(
-    int n, const double *__restrict__ x, const double *__restrict__ y, const double *__restrict__ z, Box bx,
+__device__ __forceinline__ void k_real_energy(VGrid vg, 
+    int n, const double *__restrict__ x, const double *__restrict__ y, const double *__restrict__ z, const Box &bx,
     const double *__restrict__ gm, const double *__restrict__ uD, const double *__restrict__ uP,
     const double *__restrict__ ipdamp, const double *__restrict__ thole, const int *__restrict__ ewl,
-    const int *__restrict__ ewl_cnt, int capE, const int *__restrict__ ewl_sh, Excl ex, EwaldCoef ec, const __grid_constant__ ScaleTables c_scales, int polarization, int gradient,
+    const int *__restrict__ ewl_cnt, int capE, const int *__restrict__ ewl_sh, const Excl &ex, const EwaldCoef &ec, const ScaleTables &c_scales, int polarization, int gradient,
     double *eatom_perm, double *eatom_pol, long long *catom, double *grad, double *torque,
-    const int *__restrict__ soft, ElecStep st, double *edl, double *ed2l, double *lgrad, double *ltorque,
+    const int *__restrict__ soft, const ElecStep &st, double *edl, double *ed2l, double *lgrad, double *ltorque,
     const double2 *__restrict__ pos, const R *__restrict__ rec, int *flags) {
   constexpr bool HALF = !LAM && !DIRECT;   // the softcore and direct forms walk the full rows
   __shared__ int qbuf[HALF ? 4 : 1][64];
-  const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const int warp = (vg.bid * blockDim.x + threadIdx.x) >> 5;
   const int lane = threadIdx.x & 31;
   if (warp >= n) return;
   const int i = warp;
@@ -712,9 +712,9 @@ static Excl excl(const Handle &h) {
 // the Thole parameters, induced part from u_D and u_P.  The quadrupole is divided by 3 in
 // the pair kernels' own expression.
 template <typename R>
-__global__ void k_pack_mpole(int n, const double *__restrict__ gm, const double *__restrict__ ipdamp,
+__device__ __forceinline__ void k_pack_mpole(VGrid vg, int n, const double *__restrict__ gm, const double *__restrict__ ipdamp,
                              const double *__restrict__ thole, R *rec) {
-  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  const int i = vg.bid * blockDim.x + threadIdx.x;
   if (i >= n) return;
   R v[16];
 #pragma unroll
@@ -730,9 +730,9 @@ __global__ void k_pack_mpole(int n, const double *__restrict__ gm, const double 
 }
 
 template <typename R>
-__global__ void k_pack_induced(int n, const double *__restrict__ uD, const double *__restrict__ uP, R *rec,
+__device__ __forceinline__ void k_pack_induced(VGrid vg, int n, const double *__restrict__ uD, const double *__restrict__ uP, R *rec,
                                double *grad, double *torque) {
-  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  const int i = vg.bid * blockDim.x + threadIdx.x;
   if (i >= n) return;
   if (grad) {   // the half-row real-space energy adds into these
     grad[i] = grad[n + i] = grad[2 * (size_t)n + i] = 0.0;
@@ -758,25 +758,29 @@ template <typename R>
 static void realspace_field(Handle &h) {
   using V2 = typename Vec2<R>::type;
   const double off2 = h.vacuum ? INFINITY : h.prm.ewald_cutoff * h.prm.ewald_cutoff;
-  k_pack_mpole<R><<<nblocks(h.n, 256), 256, 0, h.stream>>>(h.n, h.d_gm, h.d_ipdamp, h.d_thole,
-                                                            reinterpret_cast<R *>(h.d_erec));
+  launch_on<k_pack_mpole<R>, 0, 0>(h.rec, nblocks(h.n, 256), 256, 0, h.stream, h.n, (const double *)h.d_gm,
+                                   (const double *)h.d_ipdamp, (const double *)h.d_thole,
+                                   reinterpret_cast<R *>(h.d_erec));
   FFX_LAUNCHED(h);
-  k_realspace_field<R><<<nblocks((int64_t)h.n * 32, 128), 128, 0, h.stream>>>(
-      h.n, h.d_x, h.d_y, h.d_z, h.box, h.d_gm, h.d_ipdamp, h.d_thole, h.d_nbr, h.d_nbr_cnt, h.cap_nbr,
-      h.d_nbr_sh, off2, below_sqrt(h.prm.precond_cutoff), h.d_ewl, h.d_ewl_cnt, h.cap_ewl, h.d_ewl_sh, h.d_prl, h.d_prl_cnt,
-      h.cap_prl,
+  launch_on<k_realspace_field<R>, 128, sizeof(R) == 4 ? 8 : 1>(
+      h.rec, nblocks((int64_t)h.n * 32, 128), 128, 0, h.stream, h.n, (const double *)h.d_x, (const double *)h.d_y,
+      (const double *)h.d_z, h.box, (const double *)h.d_gm, (const double *)h.d_ipdamp, (const double *)h.d_thole,
+      (const int *)h.d_nbr, (const int *)h.d_nbr_cnt, h.cap_nbr, (const int *)h.d_nbr_sh, off2,
+      below_sqrt(h.prm.precond_cutoff), h.d_ewl, h.d_ewl_cnt, h.cap_ewl, h.d_ewl_sh, h.d_prl, h.d_prl_cnt, h.cap_prl,
       reinterpret_cast<PairRec<R> *>(h.d_coefE), reinterpret_cast<R *>(h.d_coefEB),
       reinterpret_cast<PairRec<R> *>(h.d_coefP), reinterpret_cast<R *>(h.d_coefPB), excl(h),
-      ewald_coef(h, ewald_alpha_of(h)), h.scales, h.d_fieldD, h.d_fieldP, h.d_flags, h.d_pos,
-      reinterpret_cast<const R *>(h.d_erec), h.near_list ? h.d_nbl : nullptr, h.d_nbl_cnt, h.cap_nbl);
+      ewald_coef(h, ewald_alpha_of(h)), h.scales, h.d_fieldD, h.d_fieldP, h.d_flags, (const double2 *)h.d_pos,
+      reinterpret_cast<const R *>(h.d_erec), (const int *)(h.near_list ? h.d_nbl : nullptr), (const int *)h.d_nbl_cnt,
+      h.cap_nbl);
   FFX_LAUNCHED(h);
 }
 
 template <typename R>
 static void direct_dipoles(Handle &h) {
-  k_direct_dipoles<R><<<nblocks(h.n, 256), 256, 0, h.stream>>>(
-      h.n, h.d_gm, h.d_cphi, h.d_polar, ewald_coef(h, ewald_alpha_of(h)).aewald3, h.d_fieldD, h.d_fieldP, h.d_uD,
-      h.d_uP, h.d_udirD, h.d_udirP, reinterpret_cast<R *>(h.d_recF));
+  launch_on<k_direct_dipoles<R>, 0, 0>(h.rec, nblocks(h.n, 256), 256, 0, h.stream, h.n, (const double *)h.d_gm,
+                                       (const double *)h.d_cphi, (const double *)h.d_polar,
+                                       ewald_coef(h, ewald_alpha_of(h)).aewald3, h.d_fieldD, h.d_fieldP, h.d_uD,
+                                       h.d_uP, h.d_udirD, h.d_udirP, reinterpret_cast<R *>(h.d_recF));
   FFX_LAUNCHED(h);
 }
 
@@ -797,18 +801,28 @@ void launch_realspace_field(Handle &h) {
 template <typename R>
 static void real_energy(Handle &h, bool grad) {
   const bool direct = h.prm.polarization == FFXG_POLAR_DIRECT;
-  auto kern = h.step.lam ? (direct ? k_real_energy<R, true, true> : k_real_energy<R, true, false>)
-                         : (direct ? k_real_energy<R, false, true> : k_real_energy<R, false, false>);
   const bool half = !h.step.lam && !direct;   // k_real_energy's HALF form
-  k_pack_induced<R><<<nblocks(h.n, 256), 256, 0, h.stream>>>(h.n, h.d_uD, h.d_uP, reinterpret_cast<R *>(h.d_erec),
-                                                             half && grad ? h.d_grad : nullptr, h.d_torque);
+  launch_on<k_pack_induced<R>, 0, 0>(h.rec, nblocks(h.n, 256), 256, 0, h.stream, h.n, (const double *)h.d_uD,
+                                     (const double *)h.d_uP, reinterpret_cast<R *>(h.d_erec),
+                                     half && grad ? h.d_grad : (double *)nullptr, h.d_torque);
   FFX_LAUNCHED(h);
-  kern<<<nblocks((int64_t)h.n * 32, 128), 128, 0, h.stream>>>(
-      h.n, h.d_x, h.d_y, h.d_z, h.box, h.d_gm, h.d_uD, h.d_uP, h.d_ipdamp, h.d_thole, h.d_ewl, h.d_ewl_cnt,
-      h.cap_ewl, h.d_ewl_sh, excl(h), ewald_coef(h, ewald_alpha_of(h)), h.scales, h.prm.polarization, grad ? 1 : 0,
-      h.d_eatom + 1 * (size_t)h.n, h.d_eatom + 2 * (size_t)h.n, h.d_catom + (size_t)h.n, h.d_grad, h.d_torque,
-      h.d_soft, h.step, h.d_eatom + 9 * (size_t)h.n, h.d_eatom + 10 * (size_t)h.n, h.d_lg, h.d_lt, h.d_pos,
-      reinterpret_cast<const R *>(h.d_erec), h.d_flags);
+  auto go = [&](auto body) {
+    launch_on<decltype(body)::value, 128, sizeof(R) == 4 ? FFX_REAL_ENERGY_MIN_BLOCKS : 1>(
+        h.rec, nblocks((int64_t)h.n * 32, 128), 128, 0, h.stream, h.n, (const double *)h.d_x, (const double *)h.d_y,
+        (const double *)h.d_z, h.box, (const double *)h.d_gm, (const double *)h.d_uD, (const double *)h.d_uP,
+        (const double *)h.d_ipdamp, (const double *)h.d_thole, (const int *)h.d_ewl, (const int *)h.d_ewl_cnt,
+        h.cap_ewl, (const int *)h.d_ewl_sh, excl(h), ewald_coef(h, ewald_alpha_of(h)), h.scales, h.prm.polarization,
+        grad ? 1 : 0, h.d_eatom + 1 * (size_t)h.n, h.d_eatom + 2 * (size_t)h.n, h.d_catom + (size_t)h.n, h.d_grad,
+        h.d_torque, (const int *)h.d_soft, h.step, h.d_eatom + 9 * (size_t)h.n, h.d_eatom + 10 * (size_t)h.n, h.d_lg,
+        h.d_lt, (const double2 *)h.d_pos, reinterpret_cast<const R *>(h.d_erec), h.d_flags);
+  };
+  if (h.step.lam) {
+    if (direct) go(BodyOf<k_real_energy<R, true, true>>{});
+    else go(BodyOf<k_real_energy<R, true, false>>{});
+  } else {
+    if (direct) go(BodyOf<k_real_energy<R, false, true>>{});
+    else go(BodyOf<k_real_energy<R, false, false>>{});
+  }
   FFX_LAUNCHED(h);
 }
 

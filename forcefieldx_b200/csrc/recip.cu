@@ -23,14 +23,14 @@ struct RecipCoef {
   int polarization;
 };
 
-__global__ void k_recip_energy(int n, const double *__restrict__ gm, const double *__restrict__ fm,
+__device__ __forceinline__ void k_recip_energy(VGrid vg, int n, const double *__restrict__ gm, const double *__restrict__ fm,
                                const double *__restrict__ cphi, const double *__restrict__ fphi,
                                const double *__restrict__ uD, const double *__restrict__ uP,
                                const double *__restrict__ cphiI, const double *__restrict__ cphiP,
-                               const double *__restrict__ fphiI, const double *__restrict__ fphiP, RecipCoef rc,
-                               PmeConst pc, int gradient, double *eatom, double *grad, double *torque, ElecStep st,
+                               const double *__restrict__ fphiI, const double *__restrict__ fphiP, const RecipCoef &rc,
+                               const PmeConst &pc, int gradient, double *eatom, double *grad, double *torque, const ElecStep &st,
                                double *lgrad, double *ltorque) {
-  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  const int i = vg.bid * blockDim.x + threadIdx.x;
   if (i >= n) return;
   double mp[10], f[10];
 #pragma unroll
@@ -288,12 +288,12 @@ __device__ __forceinline__ void torque_slot(int i, int slot, int n, const double
   for (int j = 0; j < 3; j++) out[j] = (slot == 0) ? g[0][j] : (slot == 1) ? g[1][j] : (slot == 2) ? g[2][j] : g[3][j];
 }
 
-__global__ void k_torque_gather(int n, const double *__restrict__ x, const double *__restrict__ y,
+__device__ __forceinline__ void k_torque_gather(VGrid vg, int n, const double *__restrict__ x, const double *__restrict__ y,
                                 const double *__restrict__ z, const int *__restrict__ frame,
                                 const int *__restrict__ axis, const double *__restrict__ torque,
                                 const int *__restrict__ tq_ptr, const int *__restrict__ tq_ent, double *gtq,
                                 int *flags, int quant) {
-  const int j = blockIdx.x * blockDim.x + threadIdx.x;
+  const int j = vg.bid * blockDim.x + threadIdx.x;
   if (j >= n) return;
   double s0 = 0, s1 = 0, s2 = 0;
   for (int e = tq_ptr[j]; e < tq_ptr[j + 1]; e++) {
@@ -311,9 +311,9 @@ __global__ void k_torque_gather(int n, const double *__restrict__ x, const doubl
   gtq[j] = s0; gtq[n + j] = s1; gtq[2 * n + j] = s2;
 }
 
-__global__ void k_assemble(int n, const double *__restrict__ grad, const double *__restrict__ gtq,
+__device__ __forceinline__ void k_assemble(VGrid vg, int n, const double *__restrict__ grad, const double *__restrict__ gtq,
                            const double *__restrict__ gvdw, double *out, int *flags, int quant) {
-  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  const int i = vg.bid * blockDim.x + threadIdx.x;
   if (i >= n) return;
   for (int d = 0; d < 3; d++) {
     const double ge = grad[d * n + i];
@@ -328,12 +328,12 @@ __global__ void k_assemble(int n, const double *__restrict__ grad, const double 
 constexpr int kSumBlocks = 148;
 constexpr int kNE = kEnergyRows, kNC = 2;   // energy rows (kEnergyRows), count rows
 
-__global__ void k_sum_partial(int n, const double *__restrict__ eatom, const long long *__restrict__ catom,
+__device__ __forceinline__ void k_sum_partial(VGrid vg, int n, const double *__restrict__ eatom, const long long *__restrict__ catom,
                               double *pe, long long *pc) {
   __shared__ double se[kNE][256];
   __shared__ long long sc[kNC][256];
-  const int chunk = (n + gridDim.x - 1) / gridDim.x;
-  const int s = blockIdx.x * chunk, e = min(n, s + chunk);
+  const int chunk = (n + vg.nblk - 1) / vg.nblk;
+  const int s = vg.bid * chunk, e = min(n, s + chunk);
   double acc[kNE] = {0};
   long long cc[kNC] = {0};
   for (int i = s + threadIdx.x; i < e; i += blockDim.x) {
@@ -351,14 +351,14 @@ __global__ void k_sum_partial(int n, const double *__restrict__ eatom, const lon
     __syncthreads();
   }
   if (threadIdx.x == 0) {
-    for (int t = 0; t < kNE; t++) pe[blockIdx.x * kNE + t] = se[t][0];
-    for (int t = 0; t < kNC; t++) pc[blockIdx.x * kNC + t] = sc[t][0];
+    for (int t = 0; t < kNE; t++) pe[vg.bid * kNE + t] = se[t][0];
+    for (int t = 0; t < kNC; t++) pc[vg.bid * kNC + t] = sc[t][0];
   }
 }
 
 // Row t of the totals by warp t: lane l sums blocks l, l + 32, ..., then a fixed shuffle
 // tree (the same order on every call).
-__global__ void k_sum_final(int nb, const double *__restrict__ pe, const long long *__restrict__ pc, double *out,
+__device__ __forceinline__ void k_sum_final(VGrid vg, int nb, const double *__restrict__ pe, const long long *__restrict__ pc, double *out,
                             long long *cout) {
   const int lane = threadIdx.x & 31, row = threadIdx.x >> 5;
   if (row < kNE) {
@@ -391,10 +391,12 @@ void launch_recip_energy(Handle &h, bool grad) {
   rc.nf[0] = h.nfft[0]; rc.nf[1] = h.nfft[1]; rc.nf[2] = h.nfft[2];
   rc.polarization = h.step.doPol ? h.prm.polarization : FFXG_POLAR_NONE;
   if (h.vacuum) return;   // no reciprocal space and no Ewald self terms (alpha 0)
-  k_recip_energy<<<nblocks(h.n, 128), 128, 0, h.stream>>>(h.n, h.d_gm, h.d_fm, h.d_cphi, h.d_fphi, h.d_uD, h.d_uP,
-                                                           h.d_cphiI, h.d_cphiP, h.d_fphiI, h.d_fphiP, rc, h.pc,
-                                                           (grad || h.step.lam) ? 1 : 0, h.d_eatom, h.d_grad, h.d_torque,
-                                                           h.step, h.d_lg, h.d_lt);
+  launch_on<k_recip_energy, 0, 0>(h.rec, nblocks(h.n, 128), 128, 0, h.stream, h.n, (const double *)h.d_gm,
+                                   (const double *)h.d_fm, (const double *)h.d_cphi, (const double *)h.d_fphi,
+                                   (const double *)h.d_uD, (const double *)h.d_uP, (const double *)h.d_cphiI,
+                                   (const double *)h.d_cphiP, (const double *)h.d_fphiI, (const double *)h.d_fphiP, rc,
+                                   h.pc, (grad || h.step.lam) ? 1 : 0, h.d_eatom, h.d_grad, h.d_torque, h.step, h.d_lg,
+                                   h.d_lt);
   FFX_LAUNCHED(h);
 }
 
@@ -402,15 +404,17 @@ void launch_torque(Handle &h) { launch_torque_of(h, h.d_torque, h.d_vec); }
 
 // Torque -> Cartesian gradient of `torque` into out[3][n] (written, not added).
 void launch_torque_of(Handle &h, const double *torque, double *out) {
-  k_torque_gather<<<nblocks(h.n, 128), 128, 0, h.stream>>>(h.n, h.d_x, h.d_y, h.d_z, h.d_frame, h.d_axis, torque,
-                                                            h.d_tq_ptr, h.d_tq_ent, out, h.d_flags,
-                                                            h.mixed && torque == h.d_torque ? 1 : 0);
+  launch_on<k_torque_gather, 0, 0>(h.rec, nblocks(h.n, 128), 128, 0, h.stream, h.n, (const double *)h.d_x,
+                                    (const double *)h.d_y, (const double *)h.d_z, (const int *)h.d_frame,
+                                    (const int *)h.d_axis, torque, (const int *)h.d_tq_ptr, (const int *)h.d_tq_ent,
+                                    out, h.d_flags, h.mixed && torque == h.d_torque ? 1 : 0);
   FFX_LAUNCHED(h);
 }
 
 void launch_assemble(Handle &h, double *d_grad_xyz) {
-  k_assemble<<<nblocks(h.n, 256), 256, 0, h.stream>>>(h.n, h.d_grad, h.d_vec, h.d_gred + 3 * (size_t)h.n, d_grad_xyz,
-                                                       h.d_flags, h.mixed ? 1 : 0);
+  launch_on<k_assemble, 0, 0>(h.rec, nblocks(h.n, 256), 256, 0, h.stream, h.n, (const double *)h.d_grad,
+                              (const double *)h.d_vec, (const double *)(h.d_gred + 3 * (size_t)h.n), d_grad_xyz,
+                              h.d_flags, h.mixed ? 1 : 0);
   FFX_LAUNCHED(h);
 }
 
@@ -419,10 +423,10 @@ void launch_assemble(Handle &h, double *d_grad_xyz) {
 // torque, [6,14) energy rows 1-6, 9, 10, [14,17) lambda gradient, [17,20) lambda torque.
 __device__ __constant__ int kAccRows[8] = {1, 2, 3, 4, 5, 6, 9, 10};
 
-__global__ void k_elec_accumulate(int n, int first, const double *__restrict__ grad, const double *__restrict__ torque,
+__device__ __forceinline__ void k_elec_accumulate(VGrid vg, int n, int first, const double *__restrict__ grad, const double *__restrict__ torque,
                                   const double *__restrict__ eatom, const double *__restrict__ lg,
                                   const double *__restrict__ lt, double *acc) {
-  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  const int i = vg.bid * blockDim.x + threadIdx.x;
   if (i >= n) return;
   double v[20];
   for (int d = 0; d < 3; d++) {
@@ -435,9 +439,9 @@ __global__ void k_elec_accumulate(int n, int first, const double *__restrict__ g
   for (int r = 0; r < 20; r++) acc[(size_t)r * n + i] = first ? v[r] : acc[(size_t)r * n + i] + v[r];
 }
 
-__global__ void k_elec_restore(int n, const double *__restrict__ acc, double *grad, double *torque, double *eatom,
+__device__ __forceinline__ void k_elec_restore(VGrid vg, int n, const double *__restrict__ acc, double *grad, double *torque, double *eatom,
                                double *lg, double *lt) {
-  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  const int i = vg.bid * blockDim.x + threadIdx.x;
   if (i >= n) return;
   for (int d = 0; d < 3; d++) {
     grad[d * n + i] = acc[(size_t)d * n + i];
@@ -449,41 +453,44 @@ __global__ void k_elec_restore(int n, const double *__restrict__ acc, double *gr
 }
 
 // out[3][n] += lg + the torque-derived part of the lambda gradient.
-__global__ void k_lambda_grad_add(int n, const double *__restrict__ lg, const double *__restrict__ lgtq, double *out) {
-  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+__device__ __forceinline__ void k_lambda_grad_add(VGrid vg, int n, const double *__restrict__ lg, const double *__restrict__ lgtq, double *out) {
+  const int i = vg.bid * blockDim.x + threadIdx.x;
   if (i >= n) return;
   for (int d = 0; d < 3; d++) out[d * n + i] += lg[d * n + i] + lgtq[d * n + i];
 }
 
 // Zero the global and fractional multipoles of the soft atoms (the condensed step without
 // them: an atom with no multipoles and no polarizability takes no part).
-__global__ void k_zero_soft_multipoles(int n, const int *__restrict__ soft, double *gm, double *fm) {
-  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+__device__ __forceinline__ void k_zero_soft_multipoles(VGrid vg, int n, const int *__restrict__ soft, double *gm, double *fm) {
+  const int i = vg.bid * blockDim.x + threadIdx.x;
   if (i >= n || !soft[i]) return;
   for (int t = 0; t < 10; t++) { gm[(size_t)t * n + i] = 0.0; fm[(size_t)t * n + i] = 0.0; }
 }
 
 void launch_elec_accumulate(Handle &h, bool first) {
-  k_elec_accumulate<<<nblocks(h.n, 256), 256, 0, h.stream>>>(h.n, first ? 1 : 0, h.d_grad, h.d_torque, h.d_eatom,
-                                                              h.d_lg, h.d_lt, h.d_acc);
+  launch_on<k_elec_accumulate, 0, 0>(h.rec, nblocks(h.n, 256), 256, 0, h.stream, h.n, first ? 1 : 0,
+                                     (const double *)h.d_grad, (const double *)h.d_torque, (const double *)h.d_eatom,
+                                     (const double *)h.d_lg, (const double *)h.d_lt, h.d_acc);
   FFX_LAUNCHED(h);
 }
 
 void launch_elec_restore(Handle &h) {
-  k_elec_restore<<<nblocks(h.n, 256), 256, 0, h.stream>>>(h.n, h.d_acc, h.d_grad, h.d_torque, h.d_eatom, h.d_lg,
-                                                           h.d_lt);
+  launch_on<k_elec_restore, 0, 0>(h.rec, nblocks(h.n, 256), 256, 0, h.stream, h.n, (const double *)h.d_acc, h.d_grad,
+                                  h.d_torque, h.d_eatom, h.d_lg, h.d_lt);
   FFX_LAUNCHED(h);
 }
 
 void launch_lambda_grad_add(Handle &h, double *out) {
   // The torque-derived part goes through d_vec's scratch rows, like launch_torque.
   launch_torque_of(h, h.d_lt, h.d_vec);
-  k_lambda_grad_add<<<nblocks(h.n, 256), 256, 0, h.stream>>>(h.n, h.d_lg, h.d_vec, out);
+  launch_on<k_lambda_grad_add, 0, 0>(h.rec, nblocks(h.n, 256), 256, 0, h.stream, h.n, (const double *)h.d_lg,
+                                     (const double *)h.d_vec, out);
   FFX_LAUNCHED(h);
 }
 
 void launch_zero_soft_multipoles(Handle &h) {
-  k_zero_soft_multipoles<<<nblocks(h.n, 256), 256, 0, h.stream>>>(h.n, h.d_soft, h.d_gm, h.d_fm);
+  launch_on<k_zero_soft_multipoles, 0, 0>(h.rec, nblocks(h.n, 256), 256, 0, h.stream, h.n, (const int *)h.d_soft,
+                                          h.d_gm, h.d_fm);
   FFX_LAUNCHED(h);
 }
 
@@ -491,8 +498,10 @@ void launch_reduce_results(Handle &h) {
   double *pe = h.d_partials;
   long long *pc = reinterpret_cast<long long *>(h.d_partials + kSumBlocks * kNE);
   const int nb = std::min(kSumBlocks, std::max(1, (h.n + 255) / 256));   // fewer blocks for small systems
-  k_sum_partial<<<nb, 256, 0, h.stream>>>(h.n, h.d_eatom, h.d_catom, pe, pc);
-  k_sum_final<<<1, 32 * (kNE + kNC), 0, h.stream>>>(nb, pe, pc, h.d_result, h.d_cresult);
+  launch_on<k_sum_partial, 0, 0>(h.rec, nb, 256, 0, h.stream, h.n, (const double *)h.d_eatom,
+                                 (const long long *)h.d_catom, pe, pc);
+  launch_on<k_sum_final, 0, 0>(h.rec, 1, 32 * (kNE + kNC), 0, h.stream, nb, (const double *)pe,
+                               (const long long *)pc, h.d_result, h.d_cresult);
   h.launches += 2;
 }
 

@@ -34,23 +34,23 @@ __device__ __forceinline__ unsigned vexcl_code(int i, int k, const int *__restri
 
 // ALCH: the softcore variant (launched only while soft atoms are set).
 template <typename R, bool ALCH>
-__global__ void __launch_bounds__(256) k_vdw(int n, const double *__restrict__ rx, const double *__restrict__ ry,
-                                             const double *__restrict__ rz, Box bx, const int *__restrict__ vtype,
+__device__ __forceinline__ void k_vdw(VGrid vg, int n, const double *__restrict__ rx, const double *__restrict__ ry,
+                                             const double *__restrict__ rz, const Box &bx, const int *__restrict__ vtype,
                                              int ntypes, const double *__restrict__ vrad,
                                              const double *__restrict__ veps, const int *__restrict__ nbr,
                                              const int *__restrict__ nbr_cnt, int cap, const int *__restrict__ nbr_sh,
                                              const int *__restrict__ eptr,
                                              const int *__restrict__ ek, const unsigned *__restrict__ ecode,
-                                             const int *__restrict__ elo, const int *__restrict__ ehi, VdwForm vf,
-                                             const __grid_constant__ ScaleTables c_vscales, int gradient, double *eatom, long long *catom, double *gred,
-                                             const int *__restrict__ soft, const int *__restrict__ mol, AlchConst al,
+                                             const int *__restrict__ elo, const int *__restrict__ ehi, const VdwForm &vf,
+                                             const ScaleTables &c_vscales, int gradient, double *eatom, long long *catom, double *gred,
+                                             const int *__restrict__ soft, const int *__restrict__ mol, const AlchConst &al,
                                              double *edl, double *ed2l, double *lgred,
                                              const double2 *__restrict__ rpos) {
   struct Queue { R x[64], y[64], z[64], r[64], m[64]; int k[64], t[64], f[64]; };
   __shared__ Queue qbuf[8];
-  const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const int warp = (vg.bid * blockDim.x + threadIdx.x) >> 5;
   const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
-  const int nwarps = (gridDim.x * blockDim.x) >> 5;
+  const int nwarps = (vg.nblk * blockDim.x) >> 5;
   for (int i = warp; i < n; i += nwarps) {
     const double xi = rx[i], yi = ry[i], zi = rz[i];
     const int ti = vtype[i];
@@ -85,49 +85,55 @@ __global__ void __launch_bounds__(256) k_vdw(int n, const double *__restrict__ r
             else if (al.intra && same) spair = true;
           }
         }
+        // The energy and gradient arithmetic with its roundings fixed (xmul / xadd / xfma),
+        // so that a system's vdW term is the same bits alone and in a batch.
         const R alpha = spair ? (R)al.sc1 : R(0);
         const R lambda5 = spair ? (R)al.sc2 : R(1);
-        const R ev = mask * veps[ti * ntypes + tk];
-        const R eps_lambda = ev * lambda5;
-        const R rho = r * irv;
-        const R rho2 = rho * rho;
-        const R rhoDisp1 = rho2 * rho2 * rho2;
-        const R rhoDisp = rhoDisp1 * rho;
-        const R rd = rho + delta, rd2 = rd * rd;
-        const R rhoDelta1 = rd2 * rd2 * rd2;
-        const R rhoDelta = rhoDelta1 * rd;
-        const R t1d = R(1.0) / (alpha + rhoDelta);
-        const R t2d = R(1.0) / (alpha + rhoDisp + gamma);
-        const R t1 = t1n * t1d;
-        const R t2a = gamma1 * t2d;
-        const R t2 = t2a - R(2.0);
-        const R eik = eps_lambda * t1 * t2;
+        const R ev = xmul(mask, veps[ti * ntypes + tk]);
+        const R eps_lambda = xmul(ev, lambda5);
+        const R rho = xmul(r, irv);
+        const R rho2 = xmul(rho, rho);
+        const R rhoDisp1 = xmul(xmul(rho2, rho2), rho2);
+        const R rhoDisp = xmul(rhoDisp1, rho);
+        const R rd = xadd(rho, delta), rd2 = xmul(rd, rd);
+        const R rhoDelta1 = xmul(xmul(rd2, rd2), rd2);
+        const R rhoDelta = xmul(rhoDelta1, rd);
+        const R t1d = R(1.0) / xadd(alpha, rhoDelta);
+        const R t2d = R(1.0) / xadd(xadd(alpha, rhoDisp), gamma);
+        const R t1 = xmul(t1n, t1d);
+        const R t2a = xmul(gamma1, t2d);
+        const R t2 = xadd(t2a, R(-2.0));
+        const R eik = xmul(xmul(eps_lambda, t1), t2);
         R taper = R(1.0), dtaper = R(0.0);
         if (tap) {
           if (sizeof(R) == 8) {
-            const R r3 = r2 * r, r4 = r2 * r2, r5 = r2 * r3;
-            taper = c5 * r5 + c4 * r4 + c3 * r3 + c2 * r2 + c1 * r + c0;
-            dtaper = R(5.0) * c5 * r4 + R(4.0) * c4 * r3 + R(3.0) * c3 * r2 + R(2.0) * c2 * r + c1;
+            // The polynomial summed left to right, as the reference sums its terms.
+            const R r3 = xmul(r2, r), r4 = xmul(r2, r2), r5 = xmul(r2, r3);
+            taper = xadd(xfma(c1, r, xfma(c2, r2, xfma(c3, r3, xfma(c4, r4, xmul(c5, r5))))), c0);
+            dtaper = xadd(xfma(R(2.0) * c2, r, xfma(R(3.0) * c3, r2, xfma(R(4.0) * c4, r3, xmul(R(5.0) * c5, r4)))),
+                          c1);
           } else {
             // The same quintic in t = (r - cut) / (off - cut): 1 - 10 t^3 + 15 t^4 - 6 t^5.
             // The power form above cancels ~1e6-sized terms and is unusable in FP32.
-            const R t = (r - cut) * iwidth, t2 = t * t;
-            taper = R(1) + t2 * t * (R(-10) + t * (R(15) - R(6) * t));
-            dtaper = t2 * (R(-30) + t * (R(60) - R(30) * t)) * iwidth;
+            const R t = xmul(xadd(r, -cut), iwidth), t2 = xmul(t, t);
+            taper = xfma(xmul(t2, t), xfma(t, xfma(R(-6), t, R(15)), R(-10)), R(1));
+            dtaper = xmul(xmul(t2, xfma(t, xfma(R(-30), t, R(60)), R(-30))), iwidth);
           }
         }
-        e += R(0.5) * eik * taper;
+        e += xmul(xmul(R(0.5), eik), taper);
         if (counted) cnt++;
         if (gradient || (ALCH && spair)) {
-          const R dt1d_dr = R(7.0) * rhoDelta1 * irv;
-          const R dt2d_dr = R(7.0) * rhoDisp1 * irv;
-          const R dt1_dr = t1 * dt1d_dr * t1d;
-          const R dt2_dr = t2a * dt2d_dr * t2d;
-          const R dedr = -eps_lambda * (dt1_dr * t2 + t1 * dt2_dr);
+          const R dt1d_dr = xmul(xmul(R(7.0), rhoDelta1), irv);
+          const R dt2d_dr = xmul(xmul(R(7.0), rhoDisp1), irv);
+          const R dt1_dr = xmul(xmul(t1, dt1d_dr), t1d);
+          const R dt2_dr = xmul(xmul(t2a, dt2d_dr), t2d);
+          const R dedr = -xmul(eps_lambda, xfma(dt1_dr, t2, xmul(t1, dt2_dr)));
           const R ir = R(1.0) / r;
           if (gradient) {
-            const R dsw = eik * dtaper + dedr * taper;
-            gx += dsw * dx * ir; gy += dsw * dy * ir; gz += dsw * dz * ir;
+            const R dsw = xfma(eik, dtaper, xmul(dedr, taper));
+            gx = xfma(xmul(dsw, dx), ir, gx);
+            gy = xfma(xmul(dsw, dy), ir, gy);
+            gz = xfma(xmul(dsw, dz), ir, gz);
           }
           if (ALCH && spair) {
             // dU/dL, d2U/dL2 and dU/dX dL of the softcore pair (VanDerWaals.java:1842-1880); each
@@ -227,10 +233,10 @@ __global__ void __launch_bounds__(256) k_vdw(int n, const double *__restrict__ r
 
 // g[j] = red_j * G[j] (reduced hydrogen) or G[j] (heavy / unreduced) + sum over the
 // hydrogens c reduced toward j of (1 - red_c) * G[c].
-__global__ void k_vdw_distribute(int n, const double *__restrict__ gred, const int *__restrict__ redp,
+__device__ __forceinline__ void k_vdw_distribute(VGrid vg, int n, const double *__restrict__ gred, const int *__restrict__ redp,
                                  const double *__restrict__ redf, const int *__restrict__ cptr,
                                  const int *__restrict__ child, double *gvdw) {
-  const int j = blockIdx.x * blockDim.x + threadIdx.x;
+  const int j = vg.bid * blockDim.x + threadIdx.x;
   if (j >= n) return;
   const double w = (redp[j] != j) ? redf[j] : 1.0 - redf[j];
   double s0 = w * gred[j], s1 = w * gred[n + j], s2 = w * gred[2 * n + j];
@@ -262,27 +268,39 @@ void launch_vdw(Handle &h, bool grad, cudaStream_t st) {
   vf.c5 = -6.0 / den;
   vf.cut = cut;
   vf.iwidth = 1.0 / (off - cut);
-  auto kern = h.alch.active ? (h.mixed ? k_vdw<float, true> : k_vdw<double, true>)
-                            : (h.mixed ? k_vdw<float, false> : k_vdw<double, false>);
   // In a captured evaluation vdW is a low-priority branch beside the solver: at most four
   // blocks per SM, warps striding over atoms, leave the solver's kernels most of every SM
   // (measured 1% faster than a full grid, which takes issue slots from the solver).
   const int full = nblocks((int64_t)h.n * 32, 256);
   const int blocks = h.capturing ? std::min(full, 4 * h.num_sms) : full;
-  kern<<<blocks, 256, 0, st>>>(
-      h.n, h.d_rx, h.d_ry, h.d_rz, h.box, h.d_vtype, h.ntypes, h.d_vrad, h.d_veps, h.d_nbr, h.d_nbr_cnt, h.cap_nbr,
-      h.d_nbr_sh, h.d_excl_ptr, h.d_excl_k, h.d_excl_code, h.d_excl_lo, h.d_excl_hi, vf, h.scales, grad ? 1 : 0, h.d_eatom, h.d_catom,
-      h.d_gred, h.d_soft, h.d_mol, h.alch, h.d_eatom + 7 * (size_t)h.n, h.d_eatom + 8 * (size_t)h.n, h.d_lgred,
-      h.d_rpos);
+  auto go = [&](auto body) {
+    launch_on<decltype(body)::value, 256, 0>(
+        h.rec, blocks, 256, 0, st, h.n, (const double *)h.d_rx, (const double *)h.d_ry, (const double *)h.d_rz,
+        h.box, (const int *)h.d_vtype, h.ntypes, (const double *)h.d_vrad, (const double *)h.d_veps,
+        (const int *)h.d_nbr, (const int *)h.d_nbr_cnt, h.cap_nbr, (const int *)h.d_nbr_sh,
+        (const int *)h.d_excl_ptr, (const int *)h.d_excl_k, (const unsigned *)h.d_excl_code,
+        (const int *)h.d_excl_lo, (const int *)h.d_excl_hi, vf, h.scales, grad ? 1 : 0, h.d_eatom, h.d_catom,
+        h.d_gred, (const int *)h.d_soft, (const int *)h.d_mol, h.alch, h.d_eatom + 7 * (size_t)h.n,
+        h.d_eatom + 8 * (size_t)h.n, h.d_lgred, (const double2 *)h.d_rpos);
+  };
+  if (h.alch.active) {
+    if (h.mixed) go(BodyOf<k_vdw<float, true>>{});
+    else go(BodyOf<k_vdw<double, true>>{});
+  } else {
+    if (h.mixed) go(BodyOf<k_vdw<float, false>>{});
+    else go(BodyOf<k_vdw<double, false>>{});
+  }
   FFX_LAUNCHED(h);
   if (grad) {
     // Rows 3-5 of d_gred hold the distributed per-atom vdW gradient.
-    k_vdw_distribute<<<nblocks(h.n, 256), 256, 0, st>>>(h.n, h.d_gred, h.d_redp, h.d_redf, h.d_red_ptr,
-                                                               h.d_red_child, h.d_gred + 3 * (size_t)h.n);
+    launch_on<k_vdw_distribute, 0, 0>(h.rec, nblocks(h.n, 256), 256, 0, st, h.n, (const double *)h.d_gred,
+                                      (const int *)h.d_redp, (const double *)h.d_redf, (const int *)h.d_red_ptr,
+                                      (const int *)h.d_red_child, h.d_gred + 3 * (size_t)h.n);
     FFX_LAUNCHED(h);
     if (h.alch.active) {   // dU/dX dL rows 3-5 of d_lgred, distributed the same way
-      k_vdw_distribute<<<nblocks(h.n, 256), 256, 0, st>>>(h.n, h.d_lgred, h.d_redp, h.d_redf, h.d_red_ptr,
-                                                                 h.d_red_child, h.d_lgred + 3 * (size_t)h.n);
+      launch_on<k_vdw_distribute, 0, 0>(h.rec, nblocks(h.n, 256), 256, 0, st, h.n, (const double *)h.d_lgred,
+                                      (const int *)h.d_redp, (const double *)h.d_redf, (const int *)h.d_red_ptr,
+                                      (const int *)h.d_red_child, h.d_lgred + 3 * (size_t)h.n);
       FFX_LAUNCHED(h);
     }
   }

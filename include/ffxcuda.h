@@ -260,17 +260,23 @@ int ffxg_set_image_mode(ffxg_handle *h, int mode);
  * Many small periodic systems of uneven size (conformer, rotamer or lambda-window
  * energies) evaluated together.  The reference evaluates such sets one ForceFieldEnergy
  * at a time (ForceFieldEnergy.energyAndGradient, P/ForceFieldEnergy.java:1843-1890, in a
- * caller's loop); here each system keeps its own handle and one batch evaluation replays
- * every system's captured evaluation as a branch of one CUDA graph (GRAPH mode, one
- * launch), or loops over single-system launches (LOOP mode, for comparison).  Results are
- * those of the single-system path bit for bit.
+ * caller's loop); here each system keeps its own handle, and one batch evaluation is one
+ * CUDA graph launch.  GRAPH mode runs the batch stage by stage: each kernel of the
+ * evaluation is one launch for all systems (each system a contiguous range of the grid's
+ * blocks, with its own arguments), and the solver loop is one device-side loop that skips
+ * the systems already converged.  BRANCHES mode replays every system's own captured
+ * evaluation as a branch of one graph (GRAPH falls back to it when the systems'
+ * evaluations cannot be merged into common stages); LOOP mode loops over single-system
+ * launches, for comparison.  Results are those of the single-system path (bit for bit in
+ * the mixed form, except a 64 x 64 mixed-form mesh, whose FFT a stage-by-stage batch
+ * takes by its per-axis passes).
  *   systems[n_systems], params[n_systems]: as for ffxg_create, one per system.
  *   xyz, grad: all systems' coordinates / gradients concatenated in system order
  *     ([total atoms][3]; xyz may be NULL to reuse the last coordinates).
  *   terms[n_systems][FFXG_N_TERMS]; counts[n_systems][FFXG_N_COUNTS] and
  *   status[n_systems] may be NULL.  Returns the first nonzero status, if any. */
 typedef struct ffxg_batch ffxg_batch;
-enum { FFXG_BATCH_GRAPH = 0, FFXG_BATCH_LOOP = 1 };
+enum { FFXG_BATCH_GRAPH = 0, FFXG_BATCH_LOOP = 1, FFXG_BATCH_BRANCHES = 2 };
 int ffxg_batch_create(int32_t n_systems, const ffxg_system *systems, const ffxg_params *params, ffxg_batch **out);
 int ffxg_batch_energy(ffxg_batch *b, const double *xyz, int want_grad, double *terms, double *grad, int64_t *counts,
                       int32_t *status);
@@ -282,6 +288,9 @@ ffxg_handle *ffxg_batch_system(ffxg_batch *b, int32_t i);
 /* How many times the batch graph was captured (a new capture follows list growth or a
  * change of a system's lambda or modes). */
 int64_t ffxg_batch_graph_builds(const ffxg_batch *b);
+/* Stages of the batch's stage-by-stage graph for want_grad (0 when the batch has none:
+ * not built yet, or BRANCHES / LOOP). */
+int32_t ffxg_batch_stages(const ffxg_batch *b, int want_grad);
 const char *ffxg_batch_last_error(const ffxg_batch *b);
 void ffxg_batch_destroy(ffxg_batch *b);
 

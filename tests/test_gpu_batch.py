@@ -2,9 +2,11 @@
 
 1. Every system of a batch (multi-image and minimum-image boxes, 96-1,200 atoms, odd and
    even PME grids) gives the energy terms and gradient of its own single-system handle,
-   in GRAPH mode (one launch) and in LOOP mode, on first and repeated calls and after the
+   in GRAPH mode (stage by stage: one launch per kernel for all systems), BRANCHES mode
+   (one graph branch per system) and LOOP mode, on first and repeated calls and after the
    coordinates move: bit for bit in the mixed form, to rounding (1e-11) in the plain FP64
-   form, whose mesh atomics add in arrival order.
+   form, whose mesh atomics add in arrival order.  A batch that mixes the two forms and a
+   softcore system (different kernel instances in the same stages) does the same.
 2. The plain FP64 batch against the oracle at the parity bar (1e-8 relative per term,
    1e-6 gradient RMS).
 3. A lambda change on one system's handle makes the batch recapture its graph.
@@ -39,20 +41,52 @@ def test_batch_matches_single_system_handles(precision):
     moved = [s.xyz + rng.normal(scale=0.05, size=s.xyz.shape) for s in systems]
     hist = [_single(s, p, [s.xyz, s.xyz, x]) for s, p, x in zip(systems, params, moved)]
     with BatchEnergy(systems, params) as b:
-        for loop in (False, True, False):
-            b.set_mode(loop)
+        for mode in ("graph", "loop", "branches", "graph"):
+            b.set_mode(mode)
             for k, xs in enumerate(([s.xyz for s in systems], moved, moved)):
                 e, grads = b.energy_and_gradient(xs)
                 for j in range(len(systems)):
-                    ref = hist[j][1 if k == 0 else 2]
-                    if precision == PRECISION_MIXED:     # deterministic form: bit for bit
-                        assert np.array_equal(b.terms[j], ref[0]), (loop, k, j, b.terms[j], ref[0])
-                        assert np.array_equal(grads[j], ref[1]), (loop, k, j)
-                    else:   # FP64 mesh atomics add in arrival order: rounding-level differences
-                        rel = np.abs(b.terms[j] - ref[0]) / np.maximum(np.abs(ref[0]), 1.0)
-                        assert rel.max() < 1e-11, (loop, k, j, rel)
-                        assert np.abs(grads[j] - ref[1]).max() < 1e-9
+                    _same(precision, b.terms[j], grads[j], hist[j][1 if k == 0 else 2], (mode, k, j))
+            if mode == "graph":
+                assert b.stages() > 50
         assert b.graph_builds >= 1
+
+
+def _same(precision, terms, grad, ref, tag):
+    if precision == PRECISION_MIXED:     # deterministic form: bit for bit
+        assert np.array_equal(terms, ref[0]), (tag, terms, ref[0])
+        assert np.array_equal(grad, ref[1]), tag
+    else:   # FP64 mesh atomics add in arrival order: rounding-level differences
+        rel = np.abs(terms - ref[0]) / np.maximum(np.abs(ref[0]), 1.0)
+        assert rel.max() < 1e-11, (tag, rel)
+        assert np.abs(grad - ref[1]).max() < 1e-9, tag
+
+
+def test_staged_batch_of_mixed_forms_and_a_softcore_system():
+    w = batch_workload(n_systems=6, seed=41, n_min=96, n_max=900, precision=PRECISION_MIXED)
+    systems = [s for s, _ in w]
+    params = [p if j % 2 else type(p)(**{**p.__dict__, "precision": PRECISION_FP64}) for j, (_, p) in enumerate(w)]
+    soft = np.zeros(systems[1].n_atoms, dtype=np.int32)
+    soft[:6] = 1
+    alch = Alchemy(soft=soft, molecule=np.arange(systems[1].n_atoms) // 3)
+    hist = []
+    for j, (s, p) in enumerate(zip(systems, params)):
+        with ForceFieldEnergy(s, p) as f:
+            if j == 1:
+                f.set_alchemy(alch)
+                f.set_lambda(0.6)
+            f.energy_and_gradient(s.xyz)
+            e, g = f.energy_and_gradient(s.xyz)
+            hist.append((f.terms.copy(), g.copy()))
+    with BatchEnergy(systems, params) as b:
+        sf = b.system_energy(1)
+        sf.set_alchemy(alch)
+        sf.set_lambda(0.6)
+        for _ in range(3):
+            e, grads = b.energy_and_gradient()
+            for j in range(len(systems)):
+                _same(params[j].precision, b.terms[j], grads[j], hist[j], j)
+        assert b.stages() > 50
 
 
 def test_batch_fp64_against_oracle():
