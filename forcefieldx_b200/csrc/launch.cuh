@@ -161,11 +161,14 @@ inline const void *many_fn() {
   else return (const void *)k_many<BODY, MAXT, MINB, A...>;
 }
 
-template <auto BODY, int MAXT, int MINB, typename... A>
+// MB: the batch instance's minimum resident blocks (0: the single-system bounds).  A
+// batch kernel reads its arguments from memory, not from the parameter bank, and keeps
+// them in registers; MB caps the registers where that would cost occupancy.
+template <auto BODY, int MAXT, int MINB, int MB = MINB, typename... A>
 inline void launch_on(Recorder *rec, int grid, int block, size_t smem, cudaStream_t st, const A &...a) {
   if (rec) {
     RecLaunch r;
-    r.fn = many_fn<BODY, MAXT, MINB, A...>();
+    r.fn = many_fn<BODY, MAXT, MB, A...>();
     r.grid = grid;
     r.block = block;
     r.smem = smem;

@@ -618,7 +618,7 @@ static double *part_region(const Handle &h, int k) { return h.d_part2 + (size_t)
 
 template <typename T>
 static void pair_field_launch(Handle &h, cudaStream_t st, bool beta) {
-  launch_on<k_pair_field<T, kEwaldGroup>, kFieldThreads, 0>(
+  launch_on<k_pair_field<T, kEwaldGroup>, kFieldThreads, 0, sizeof(T) == 4 ? 10 : 0>(
       h.rec, group_blocks(h.n, kEwaldGroup), kFieldThreads, 0, st, h.n, (const int *)h.d_ewl,
       (const int *)h.d_ewl_cnt, h.cap_ewl, reinterpret_cast<const PairRec<T> *>(h.d_coefE),
       reinterpret_cast<const T *>(h.d_coefEB), reinterpret_cast<const T *>(h.d_recF), h.d_tpair,
@@ -633,7 +633,7 @@ static void combine(Handle &h, const double *vD, const double *vP, bool first, d
   for (int a = 0; a < 3; a++)
     for (int b = 0; b < 3; b++) xf.m[a][b] = h.pc.tfm[1 + a][1 + b];
   const V2 *mesh = reinterpret_cast<const V2 *>(h.mixed ? (const void *)h.d_gridf : (const void *)h.d_grid);
-  launch_on<k_pcg_combine<MODE, T>, 256, 0>(
+  launch_on<k_pcg_combine<MODE, T>, 256, 0, 4>(
       h.rec, combine_blocks(h.n), 256, 0, h.stream, h.n, (const int *)h.d_igrid, reinterpret_cast<const T *>(h.d_spl),
       mesh, h.nfft[0], h.nfft[1], h.nfft[2], xf, (const double *)h.d_tpair, vD, vP, aewald3_of(h),
       (const double *)h.d_polar, (const double *)h.d_udirD, (const double *)h.d_udirP, h.d_p, h.d_pP, h.d_tp,
@@ -673,7 +673,7 @@ static void field_of(Handle &h, const double *vD, const double *vP, bool first, 
 
 template <bool INIT, typename T>
 static void precond(Handle &h) {
-  launch_on<k_pcg_precond<INIT, T, kPrecondGroup>, kFieldThreads, 0>(
+  launch_on<k_pcg_precond<INIT, T, kPrecondGroup>, kFieldThreads, sizeof(T) == 8 ? 7 : 0, sizeof(T) == 4 ? 5 : 0>(
       h.rec, group_blocks(h.n, kPrecondGroup), kFieldThreads, 0, h.stream, h.n, (const int *)h.d_prl,
       (const int *)h.d_prl_cnt, h.cap_prl, reinterpret_cast<const PairRec<T> *>(h.d_coefP),
       reinterpret_cast<const T *>(h.d_coefPB), reinterpret_cast<const T *>(h.d_recP), (const double *)h.d_polar,
@@ -689,7 +689,7 @@ static void launch_precond(Handle &h) {
 
 template <typename T>
 static void update(Handle &h, cudaGraphConditionalHandle cond, int use_cond) {
-  launch_on<k_pcg_update<T>, kVecThreads, 0>(
+  launch_on<k_pcg_update<T>, kVecThreads, 0, 3>(
       h.rec, vec_blocks(h.n), kVecThreads, 0, h.stream, h.n, (const double *)h.d_vec, (const double *)h.d_vecP,
       (const double *)h.d_p, (const double *)h.d_pP, h.d_r, h.d_rP, h.d_uD, h.d_uP, h.d_scalars, part_region(h, 2),
       h.d_counter + K_UPDATE, h.d_pcg, h.prm.max_scf_iter, h.prm.polar_eps, (const int *)h.d_flags, cond, use_cond,

@@ -857,10 +857,13 @@ static FftAxis make_axis(int axis, const int nf[3]) {
   for (int f = 11; m > 1 && a.nradix < 12; f += 2) {   // remaining primes: the general pass
     while (m % f == 0 && a.nradix < 12) { a.radix[a.nradix++] = f; m /= f; }
   }
-  // Lines of a CTA: consecutive along the fastest index that is not the transform axis.
+  // Lines of a CTA: consecutive along the fastest index that is not the transform axis;
+  // up to 1,024 elements for short lines (a whole plane of a small mesh per CTA, so that
+  // the 256 threads have work in every stage), else 16 lines.  Length 64 keeps 16: the
+  // fixed-length kernel takes exactly that shape.
   const int inner = (axis == 0) ? ny : nx;
   int L = 1;
-  const int cap = std::max(1, std::min(16, 4096 / a.len));
+  const int cap = (a.len == 64) ? 16 : std::max(1, std::max(std::min(16, 4096 / a.len), std::min(64, 1024 / a.len)));
   for (int d = 1; d <= cap; d++)
     if (inner % d == 0) L = d;
   a.L = L;
@@ -1180,11 +1183,11 @@ static void phi(Handle &h, int which) {
   const auto *grid = reinterpret_cast<const typename Vec2<S>::type *>(h.mixed ? (void *)h.d_gridf : (void *)h.d_grid);
   const int nb = nblocks((int64_t)h.n * 32, 256);
   if (which == 0)
-    launch_on<k_phi<20, S>, 256, 0>(h.rec, nb, 256, 0, h.stream, h.n, spl, (const int *)h.d_igrid, grid, h.nfft[0],
+    launch_on<k_phi<20, S>, 256, 0, sizeof(S) == 4 ? 6 : 3>(h.rec, nb, 256, 0, h.stream, h.n, spl, (const int *)h.d_igrid, grid, h.nfft[0],
                                     h.nfft[1], h.nfft[2], h.d_fphi, h.d_cphi, (double *)nullptr, (double *)nullptr,
                                     h.pc);
   else
-    launch_on<k_phi<20, S>, 256, 0>(h.rec, nb, 256, 0, h.stream, h.n, spl, (const int *)h.d_igrid, grid, h.nfft[0],
+    launch_on<k_phi<20, S>, 256, 0, sizeof(S) == 4 ? 6 : 3>(h.rec, nb, 256, 0, h.stream, h.n, spl, (const int *)h.d_igrid, grid, h.nfft[0],
                                     h.nfft[1], h.nfft[2], h.d_fphiI, h.d_cphiI, h.d_fphiP, h.d_cphiP, h.pc);
   FFX_LAUNCHED(h);
 }

@@ -249,6 +249,19 @@ __device__ __forceinline__ void k_vdw_distribute(VGrid vg, int n, const double *
 }
 
 
+// One vdW launch.  The batch instance is held to four resident blocks of 256 threads in
+// the FP32 form (64 registers, as the single-system instance uses).
+template <typename R, bool ALCH>
+static void vdw_launch(Handle &h, bool grad, cudaStream_t st, const VdwForm &vf, int blocks) {
+  launch_on<k_vdw<R, ALCH>, 256, 0, sizeof(R) == 4 ? 4 : 0>(
+      h.rec, blocks, 256, 0, st, h.n, (const double *)h.d_rx, (const double *)h.d_ry, (const double *)h.d_rz, h.box,
+      (const int *)h.d_vtype, h.ntypes, (const double *)h.d_vrad, (const double *)h.d_veps, (const int *)h.d_nbr,
+      (const int *)h.d_nbr_cnt, h.cap_nbr, (const int *)h.d_nbr_sh, (const int *)h.d_excl_ptr,
+      (const int *)h.d_excl_k, (const unsigned *)h.d_excl_code, (const int *)h.d_excl_lo, (const int *)h.d_excl_hi,
+      vf, h.scales, grad ? 1 : 0, h.d_eatom, h.d_catom, h.d_gred, (const int *)h.d_soft, (const int *)h.d_mol, h.alch,
+      h.d_eatom + 7 * (size_t)h.n, h.d_eatom + 8 * (size_t)h.n, h.d_lgred, (const double2 *)h.d_rpos);
+}
+
 void launch_vdw(Handle &h, bool grad, cudaStream_t st) {
   if (h.vacuum) return;   // a vacuum sub-system carries electrostatics only
   VdwForm vf{};
@@ -273,22 +286,12 @@ void launch_vdw(Handle &h, bool grad, cudaStream_t st) {
   // (measured 1% faster than a full grid, which takes issue slots from the solver).
   const int full = nblocks((int64_t)h.n * 32, 256);
   const int blocks = h.capturing ? std::min(full, 4 * h.num_sms) : full;
-  auto go = [&](auto body) {
-    launch_on<decltype(body)::value, 256, 0>(
-        h.rec, blocks, 256, 0, st, h.n, (const double *)h.d_rx, (const double *)h.d_ry, (const double *)h.d_rz,
-        h.box, (const int *)h.d_vtype, h.ntypes, (const double *)h.d_vrad, (const double *)h.d_veps,
-        (const int *)h.d_nbr, (const int *)h.d_nbr_cnt, h.cap_nbr, (const int *)h.d_nbr_sh,
-        (const int *)h.d_excl_ptr, (const int *)h.d_excl_k, (const unsigned *)h.d_excl_code,
-        (const int *)h.d_excl_lo, (const int *)h.d_excl_hi, vf, h.scales, grad ? 1 : 0, h.d_eatom, h.d_catom,
-        h.d_gred, (const int *)h.d_soft, (const int *)h.d_mol, h.alch, h.d_eatom + 7 * (size_t)h.n,
-        h.d_eatom + 8 * (size_t)h.n, h.d_lgred, (const double2 *)h.d_rpos);
-  };
   if (h.alch.active) {
-    if (h.mixed) go(BodyOf<k_vdw<float, true>>{});
-    else go(BodyOf<k_vdw<double, true>>{});
+    if (h.mixed) vdw_launch<float, true>(h, grad, st, vf, blocks);
+    else vdw_launch<double, true>(h, grad, st, vf, blocks);
   } else {
-    if (h.mixed) go(BodyOf<k_vdw<float, false>>{});
-    else go(BodyOf<k_vdw<double, false>>{});
+    if (h.mixed) vdw_launch<float, false>(h, grad, st, vf, blocks);
+    else vdw_launch<double, false>(h, grad, st, vf, blocks);
   }
   FFX_LAUNCHED(h);
   if (grad) {
