@@ -28,6 +28,9 @@ import time
 
 ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
+# Hardware work queues per process (read when CUDA starts): a batch in BRANCHES mode runs
+# one graph branch per system, and more queues let more of them run at once.
+os.environ.setdefault("CUDA_DEVICE_MAX_CONNECTIONS", "32")
 
 import numpy as np  # noqa: E402
 
@@ -364,8 +367,9 @@ def measure_batch(args, dist, world, rank):
     multiples of 3, 29.915 A^3 per molecule, PME grid per system at <= 1.2 A rounded up to
     2,3,5-smooth), mixed precision, energy + gradient of all of them per step through
     BatchEnergy (host coordinates in, host gradients out).  Systems are split over ranks by
-    the longest-processing-time rule; one all-reduce gathers the per-system energies.  Both
-    the one-graph batch and the loop of single-system launches are timed."""
+    the longest-processing-time rule; one all-reduce gathers the per-system energies.  The
+    stage-by-stage graph (the default, with its autotuned number of groups), the graph of
+    per-system branches and the loop of single-system launches are timed."""
     import torch
     from forcefieldx_b200.batch import BatchEnergy, batch_workload, partition_lpt, torch_all_reduce
     nsys = args.batch_systems
@@ -376,8 +380,8 @@ def measure_batch(args, dist, world, rank):
     out = {"systems": nsys, "atoms": int(sum(s.n_atoms for s, _ in w)), "steps": args.batch_steps,
            "metric": "energy+gradient systems/s (e2e: host coordinates in, host gradients out)"}
     with BatchEnergy([w[j][0] for j in mine], [w[j][1] for j in mine]) as b:
-        for mode in ("graph", "loop"):
-            b.set_mode(mode == "loop")
+        for mode in ("graph", "branches", "loop"):
+            b.set_mode(mode)
             for _ in range(3):
                 b.energy_and_gradient()
             if dist:
@@ -391,6 +395,10 @@ def measure_batch(args, dist, world, rank):
                 dist.all_reduce(t, op=dist.ReduceOp.MAX)
                 dt = float(t.item())
             out[mode] = {"systems_per_s": nsys * args.batch_steps / dt, "ms_per_batch": 1e3 * dt / args.batch_steps}
+            if mode == "graph":
+                groups, times = b.tuning()
+                out[mode]["stages"] = b.stages()
+                out[mode]["tuning"] = {"groups": groups, "device_ms_per_batch_by_groups": times}
         table = np.zeros(nsys)
         table[mine] = b.terms[:, 9]
         table = reduce_sum(table)

@@ -126,6 +126,21 @@ class BatchEnergy:
     def graph_builds(self) -> int:
         return int(self.lib.ffxg_batch_graph_builds(self._b))
 
+    def tuning(self):
+        """(chosen number of groups, {groups: ms per batch} of the candidates timed) of the
+        stage-by-stage graph's autotuning; (0, {}) before the first build."""
+        import ctypes
+        cand = (ctypes.c_int32 * 4)()
+        ms = (ctypes.c_double * 4)()
+        chosen = int(self.lib.ffxg_batch_tuning(self._b, cand, ms))
+        return chosen, {int(cand[k]): float(ms[k]) for k in range(4) if cand[k] > 0}
+
+    def set_groups(self, groups: int) -> None:
+        """Fix the number of concurrent groups of the stage-by-stage graph (0: autotune)."""
+        st = self.lib.ffxg_batch_set_groups(self._b, int(groups))
+        if st != 0:
+            raise EnergyException(st, "bad number of groups")
+
     def stages(self, gradient: bool = True) -> int:
         """Stages (one launch each for all systems) of the stage-by-stage graph; 0 when the
         batch runs as branches or has not been evaluated yet."""

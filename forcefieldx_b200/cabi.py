@@ -98,6 +98,8 @@ PROTOTYPES = {
     "ffxg_batch_system": (ctypes.c_void_p, [ctypes.c_void_p, ctypes.c_int32]),
     "ffxg_batch_graph_builds": (ctypes.c_int64, [ctypes.c_void_p]),
     "ffxg_batch_stages": (ctypes.c_int32, [ctypes.c_void_p, ctypes.c_int]),
+    "ffxg_batch_tuning": (ctypes.c_int32, [ctypes.c_void_p, ctypes.POINTER(ctypes.c_int32), _D]),
+    "ffxg_batch_set_groups": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int32]),
     "ffxg_batch_last_error": (ctypes.c_char_p, [ctypes.c_void_p]),
     "ffxg_batch_destroy": (None, [ctypes.c_void_p]),
     "ffxg_set_alchemy": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(FfxgAlchemy)]),

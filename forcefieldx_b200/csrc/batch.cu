@@ -81,6 +81,12 @@ struct ffxg_batch {
   unsigned char *d_stage = nullptr, *h_stage = nullptr;
   std::vector<std::vector<Recorder::Copy>> copies[2];
   int n_stages[2] = {0, 0};
+  std::vector<cudaStream_t> group_streams;        // one per concurrent group of systems
+  // Autotuning of the number of groups: the choice (0 until the first staged build) and
+  // the candidates' measured milliseconds per batch.
+  int tuned_groups = 0;
+  int tune_groups[4] = {0, 0, 0, 0};
+  float tune_ms[4] = {0, 0, 0, 0};
 };
 
 static std::string g_batch_create_error;
@@ -109,6 +115,8 @@ static void batch_free(ffxg_batch &b) {
   if (b.ev_join) cudaEventDestroy(b.ev_join);
   if (b.stream) cudaStreamDestroy(b.stream);
   if (b.side) cudaStreamDestroy(b.side);
+  for (cudaStream_t st : b.group_streams) cudaStreamDestroy(st);
+  b.group_streams.clear();
 }
 
 // The systems' recordings merged into stages, phase by phase: a stage is (phase, kernel
@@ -117,13 +125,14 @@ static void batch_free(ffxg_batch &b) {
 // earliest recorded position first).  Systems share no data, so any such order is
 // correct for each of them.  False when one stage's block size differs between systems
 // or the orders cannot be reconciled.
-static bool merge_recordings(const std::vector<Recorder> &rec, std::vector<Stage> &out, std::string &why) {
+static bool merge_recordings(const std::vector<Recorder> &rec, const std::vector<int> &group, std::vector<Stage> &out,
+                             std::string &why) {
   out.clear();
   for (int phase = 0; phase < 3; phase++) {
     std::map<std::tuple<const void *, int>, int> id;
     std::vector<Stage> nodes;
     std::vector<std::set<int>> succ;
-    for (size_t s = 0; s < rec.size(); s++) {
+    for (int s : group) {
       std::map<const void *, int> ordinal;
       int prev = -1, pos = 0;
       for (const RecLaunch &L : rec[s].seq) {
@@ -193,12 +202,10 @@ static void launch_stage(const Stage &st, const unsigned char *tab, cudaStream_t
   cudaLaunchKernel(st.fn, dim3(st.blocks), dim3(st.block), args, st.smem, stream);
 }
 
-// Record every system's evaluation, merge the recordings into stages and capture the
-// stage-by-stage graph (exec[key]).  Returns FFXG_OK, or a status with b.err set; the
-// caller then falls back to the branch graph.
-static int staged_capture(ffxg_batch &b, int key) {
+// Record every system's evaluation (rec[s]: its launches, phases and result copies).
+static int record_all(ffxg_batch &b, int key, std::vector<Recorder> &rec) {
   const size_t S = b.sys.size();
-  std::vector<Recorder> rec(S);
+  rec.assign(S, Recorder{});
   for (size_t s = 0; s < S; s++) {
     Handle &h = handle_of(b.sys[s]);
     h.want_grad = key != 0;
@@ -232,43 +239,85 @@ static int staged_capture(ffxg_batch &b, int key) {
       return FFXG_ERR_CUDA;
     }
   }
-  std::vector<Stage> stages;
-  if (!merge_recordings(rec, stages, b.err)) return FFXG_ERR_CUDA;
+  return FFXG_OK;
+}
 
+// The systems split into `groups` groups of near-equal atom count (longest first, each to
+// the lightest group), each group in system order.
+static std::vector<std::vector<int>> split_groups(const ffxg_batch &b, int groups) {
+  const int S = (int)b.sys.size();
+  groups = std::max(1, std::min(groups, S));
+  std::vector<int> order(S);
+  for (int s = 0; s < S; s++) order[s] = s;
+  std::stable_sort(order.begin(), order.end(), [&](int x, int y) {
+    return b.off[x + 1] - b.off[x] > b.off[y + 1] - b.off[y];
+  });
+  std::vector<std::vector<int>> out(groups);
+  std::vector<int64_t> load(groups, 0);
+  for (int s : order) {
+    const int g = (int)(std::min_element(load.begin(), load.end()) - load.begin());
+    out[g].push_back(s);
+    load[g] += b.off[s + 1] - b.off[s];
+  }
+  for (auto &g : out) std::sort(g.begin(), g.end());
+  return out;
+}
+
+// The stage-by-stage graph of the recordings with the systems in `groups` groups: each
+// group is one branch of the graph (its stages, its own solver loop), so the groups' kernels
+// overlap on the device.  On success *exec and *tab hold the graph and its argument tables.
+static int build_staged(ffxg_batch &b, const std::vector<Recorder> &rec, int groups, cudaGraphExec_t *exec_out,
+                        unsigned char **tab_out, int *n_stages) {
+  const std::vector<std::vector<int>> part = split_groups(b, groups);
+  const int G = (int)part.size();
+  std::vector<std::vector<Stage>> stages(G);
+  *n_stages = 0;
+  for (int g = 0; g < G; g++) {
+    if (!merge_recordings(rec, part[g], stages[g], b.err)) return FFXG_ERR_CUDA;
+    *n_stages += (int)stages[g].size();
+  }
   // Argument tables: per stage the block prefix, the packed arguments and (loop stages)
-  // each system's solver flag; then the flags of every system in the loop.
+  // each system's solver flag; then per group the flags of its systems in the loop.
   size_t bytes = 0;
-  for (Stage &st : stages) {
-    const size_t ns = st.sys.size();
-    st.off_pre = bytes = align_up(bytes, 16);
-    bytes += (ns + 1) * sizeof(int);
-    st.off_pack = bytes = align_up(bytes, 16);
-    bytes += ns * st.pack_size;
-    st.off_cont = bytes = align_up(bytes, 16);
-    if (st.phase == 1) bytes += ns * sizeof(const int *);
-  }
-  std::vector<unsigned char> tab(std::max<size_t>(bytes, 16), 0);
-  std::set<int> in_loop;
-  for (Stage &st : stages) {
-    const size_t ns = st.sys.size();
-    int *pre = reinterpret_cast<int *>(tab.data() + st.off_pre);
-    pre[0] = 0;
-    for (size_t j = 0; j < ns; j++) {
-      pre[j + 1] = pre[j] + st.grid[j];
-      std::memcpy(tab.data() + st.off_pack + j * st.pack_size, st.pack[j], st.pack_size);
-      if (st.phase == 1) {
-        const int *c = &handle_of(b.sys[st.sys[j]]).d_pcg->cont;
-        std::memcpy(tab.data() + st.off_cont + j * sizeof(const int *), &c, sizeof(c));
-        in_loop.insert(st.sys[j]);
-      }
+  for (auto &sg : stages)
+    for (Stage &st : sg) {
+      const size_t ns = st.sys.size();
+      st.off_pre = bytes = align_up(bytes, 16);
+      bytes += (ns + 1) * sizeof(int);
+      st.off_pack = bytes = align_up(bytes, 16);
+      bytes += ns * st.pack_size;
+      st.off_cont = bytes = align_up(bytes, 16);
+      if (st.phase == 1) bytes += ns * sizeof(const int *);
     }
-    st.blocks = pre[ns];
+  std::vector<unsigned char> tab(std::max<size_t>(bytes, 16), 0);
+  std::vector<size_t> off_loop(G);
+  std::vector<int> n_loop(G, 0);
+  for (int g = 0; g < G; g++) {
+    std::set<int> in_loop;
+    for (Stage &st : stages[g]) {
+      const size_t ns = st.sys.size();
+      int *pre = reinterpret_cast<int *>(tab.data() + st.off_pre);
+      pre[0] = 0;
+      for (size_t j = 0; j < ns; j++) {
+        pre[j + 1] = pre[j] + st.grid[j];
+        std::memcpy(tab.data() + st.off_pack + j * st.pack_size, st.pack[j], st.pack_size);
+        if (st.phase == 1) {
+          const int *c = &handle_of(b.sys[st.sys[j]]).d_pcg->cont;
+          std::memcpy(tab.data() + st.off_cont + j * sizeof(const int *), &c, sizeof(c));
+          in_loop.insert(st.sys[j]);
+        }
+      }
+      st.blocks = pre[ns];
+    }
+    off_loop[g] = align_up(tab.size(), 16);
+    tab.resize(off_loop[g] + std::max<size_t>(1, in_loop.size()) * sizeof(const int *));
+    size_t j = 0;
+    for (int sidx : in_loop) {
+      const int *c = &handle_of(b.sys[sidx]).d_pcg->cont;
+      std::memcpy(tab.data() + off_loop[g] + (j++) * sizeof(const int *), &c, sizeof(c));
+    }
+    n_loop[g] = (int)in_loop.size();
   }
-  std::vector<const int *> loop_cont;
-  for (int sidx : in_loop) loop_cont.push_back(&handle_of(b.sys[sidx]).d_pcg->cont);
-  const size_t off_loop = align_up(tab.size(), 16);
-  tab.resize(off_loop + std::max<size_t>(1, loop_cont.size()) * sizeof(const int *));
-  if (!loop_cont.empty()) std::memcpy(tab.data() + off_loop, loop_cont.data(), loop_cont.size() * sizeof(const int *));
   unsigned char *d_tab = nullptr;
   if (cudaMalloc(&d_tab, tab.size()) != cudaSuccess ||
       cudaMemcpy(d_tab, tab.data(), tab.size(), cudaMemcpyHostToDevice) != cudaSuccess) {
@@ -277,53 +326,69 @@ static int staged_capture(ffxg_batch &b, int key) {
     b.err = "batch stage tables: could not be uploaded";
     return FFXG_ERR_CUDA;
   }
-  const int *const *d_loop = reinterpret_cast<const int *const *>(d_tab + off_loop);
-  const int n_loop = (int)loop_cont.size();
+  for (int g = (int)b.group_streams.size(); g < G; g++) {
+    cudaStream_t st = nullptr;
+    if (cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking) != cudaSuccess) {
+      cudaGetLastError();
+      cudaFree(d_tab);
+      b.err = "batch streams could not be created";
+      return FFXG_ERR_CUDA;
+    }
+    b.group_streams.push_back(st);
+  }
 
-  // The graph: phase 0, the loop (a WHILE node whose body is phase 1 and the loop test),
-  // phase 2, then the results read back in one copy.
+  // One branch per group: phase 0, the loop (a WHILE node whose body is phase 1 and the
+  // loop test), phase 2; after the join the results are read back in one copy.
   cudaGraph_t graph = nullptr;
   bool ok = cudaStreamBeginCapture(b.stream, cudaStreamCaptureModeThreadLocal) == cudaSuccess;
   if (ok) {
-    for (const Stage &st : stages)
-      if (st.phase == 0) launch_stage(st, d_tab, b.stream);
-    if (n_loop > 0) {
-      cudaStreamCaptureStatus cs;
-      cudaGraph_t g = nullptr;
-      const cudaGraphNode_t *deps = nullptr;
-      size_t ndeps = 0;
-      cudaGraphConditionalHandle cond{};
-      ok = cudaStreamGetCaptureInfo(b.stream, &cs, nullptr, &g, &deps, &ndeps) == cudaSuccess &&
-           cudaGraphConditionalHandleCreate(&cond, g, 0, cudaGraphCondAssignDefault) == cudaSuccess;
-      if (ok) {
-        k_batch_cond<<<1, 32, 0, b.stream>>>(d_loop, n_loop, cond);
-        ok = cudaStreamGetCaptureInfo(b.stream, &cs, nullptr, &g, &deps, &ndeps) == cudaSuccess;
-      }
-      cudaGraphNodeParams cp = {};
-      cudaGraphNode_t node;
-      if (ok) {
-        cp.type = cudaGraphNodeTypeConditional;
-        cp.conditional.handle = cond;
-        cp.conditional.type = cudaGraphCondTypeWhile;
-        cp.conditional.size = 1;
-        ok = cudaGraphAddNode(&node, g, deps, ndeps, &cp) == cudaSuccess &&
-             cudaStreamUpdateCaptureDependencies(b.stream, &node, 1, cudaStreamSetCaptureDependencies) == cudaSuccess;
-      }
-      if (ok) {
-        cudaGraph_t body = cp.conditional.phGraph_out[0];
-        ok = cudaStreamBeginCaptureToGraph(b.side, body, nullptr, nullptr, 0, cudaStreamCaptureModeRelaxed) ==
-             cudaSuccess;
+    cudaEventRecord(b.ev_fork, b.stream);
+    for (int g = 0; g < G && ok; g++) {
+      cudaStream_t gs = b.group_streams[g];
+      ok = cudaStreamWaitEvent(gs, b.ev_fork, 0) == cudaSuccess;
+      for (const Stage &st : stages[g])
+        if (st.phase == 0) launch_stage(st, d_tab, gs);
+      if (ok && n_loop[g] > 0) {
+        const int *const *d_loop = reinterpret_cast<const int *const *>(d_tab + off_loop[g]);
+        cudaStreamCaptureStatus cs;
+        cudaGraph_t cg = nullptr;
+        const cudaGraphNode_t *deps = nullptr;
+        size_t ndeps = 0;
+        cudaGraphConditionalHandle cond{};
+        ok = cudaStreamGetCaptureInfo(gs, &cs, nullptr, &cg, &deps, &ndeps) == cudaSuccess &&
+             cudaGraphConditionalHandleCreate(&cond, cg, 0, cudaGraphCondAssignDefault) == cudaSuccess;
         if (ok) {
-          for (const Stage &st : stages)
-            if (st.phase == 1) launch_stage(st, d_tab, b.side);
-          k_batch_cond<<<1, 32, 0, b.side>>>(d_loop, n_loop, cond);
-          ok = cudaStreamEndCapture(b.side, &body) == cudaSuccess;
+          k_batch_cond<<<1, 32, 0, gs>>>(d_loop, n_loop[g], cond);
+          ok = cudaStreamGetCaptureInfo(gs, &cs, nullptr, &cg, &deps, &ndeps) == cudaSuccess;
+        }
+        cudaGraphNodeParams cp = {};
+        cudaGraphNode_t node;
+        if (ok) {
+          cp.type = cudaGraphNodeTypeConditional;
+          cp.conditional.handle = cond;
+          cp.conditional.type = cudaGraphCondTypeWhile;
+          cp.conditional.size = 1;
+          ok = cudaGraphAddNode(&node, cg, deps, ndeps, &cp) == cudaSuccess &&
+               cudaStreamUpdateCaptureDependencies(gs, &node, 1, cudaStreamSetCaptureDependencies) == cudaSuccess;
+        }
+        if (ok) {
+          cudaGraph_t body = cp.conditional.phGraph_out[0];
+          ok = cudaStreamBeginCaptureToGraph(b.side, body, nullptr, nullptr, 0, cudaStreamCaptureModeRelaxed) ==
+               cudaSuccess;
+          if (ok) {
+            for (const Stage &st : stages[g])
+              if (st.phase == 1) launch_stage(st, d_tab, b.side);
+            k_batch_cond<<<1, 32, 0, b.side>>>(d_loop, n_loop[g], cond);
+            ok = cudaStreamEndCapture(b.side, &body) == cudaSuccess;
+          }
         }
       }
+      for (const Stage &st : stages[g])
+        if (st.phase == 2) launch_stage(st, d_tab, gs);
+      cudaEventRecord(b.ev_join, gs);
+      cudaStreamWaitEvent(b.stream, b.ev_join, 0);
     }
-    for (const Stage &st : stages)
-      if (st.phase == 2) launch_stage(st, d_tab, b.stream);
-    cudaMemcpyAsync(b.h_stage, b.d_stage, S * kStageSlot, cudaMemcpyDeviceToHost, b.stream);
+    cudaMemcpyAsync(b.h_stage, b.d_stage, b.sys.size() * kStageSlot, cudaMemcpyDeviceToHost, b.stream);
     const bool ended = cudaStreamEndCapture(b.stream, &graph) == cudaSuccess;
     ok = ok && ended;
   }
@@ -337,12 +402,88 @@ static int staged_capture(ffxg_batch &b, int key) {
     b.err = "the stage-by-stage batch graph could not be built";
     return FFXG_ERR_CUDA;
   }
-  b.exec[key] = exec;
-  b.d_tab[key] = d_tab;
+  *exec_out = exec;
+  *tab_out = d_tab;
+  return FFXG_OK;
+}
+
+// The stage-by-stage graph for key.  The number of groups (concurrent branches) is the
+// batch's autotuned choice: on the first build each candidate (1, 2, 4, 8 groups, at
+// most one per system) is built and timed over two replays after one, and the fastest
+// kept; ffxg_batch_tuning reports the choice and the times.  A batch whose systems use
+// the ASPC predictor (whose history every evaluation advances) is not timed: it takes
+// four groups.
+static int staged_capture(ffxg_batch &b, int key) {
+  std::vector<Recorder> rec;
+  if (int st = record_all(b, key, rec)) return st;
+  bool aspc = false;
+  for (ffxg_handle *hh : b.sys) aspc = aspc || handle_of(hh).scf_predictor == FFXG_PREDICTOR_ASPC;
+  std::vector<int> cand;
+  if (b.tuned_groups > 0) cand = {b.tuned_groups};
+  else if (aspc) cand = {4};
+  else
+    for (int g : {1, 2, 4, 8})
+      if (g == 1 || g <= (int)b.sys.size()) cand.push_back(g);
+  cudaGraphExec_t best = nullptr;
+  unsigned char *best_tab = nullptr;
+  int best_groups = 0, best_stages = 0;
+  float best_ms = 1e30f;
+  cudaEvent_t e0 = nullptr, e1 = nullptr;
+  const bool timing = cand.size() > 1;
+  if (timing) {
+    cudaEventCreate(&e0);
+    cudaEventCreate(&e1);
+  }
+  for (int g : cand) {
+    cudaGraphExec_t ex = nullptr;
+    unsigned char *tb = nullptr;
+    int ns = 0;
+    if (build_staged(b, rec, g, &ex, &tb, &ns) != FFXG_OK) continue;
+    float ms = 0.f;
+    if (timing) {
+      bool ok = cudaGraphLaunch(ex, b.stream) == cudaSuccess;
+      ok = ok && cudaEventRecord(e0, b.stream) == cudaSuccess;
+      for (int r = 0; r < 2 && ok; r++) ok = cudaGraphLaunch(ex, b.stream) == cudaSuccess;
+      ok = ok && cudaEventRecord(e1, b.stream) == cudaSuccess && cudaEventSynchronize(e1) == cudaSuccess;
+      if (!ok || cudaEventElapsedTime(&ms, e0, e1) != cudaSuccess) {
+        cudaGetLastError();
+        cudaGraphExecDestroy(ex);
+        cudaFree(tb);
+        continue;
+      }
+      ms *= 0.5f;
+      for (size_t k = 0; k < 4; k++)
+        if (b.tune_groups[k] == g || b.tune_groups[k] == 0) {
+          b.tune_groups[k] = g;
+          b.tune_ms[k] = ms;
+          break;
+        }
+    }
+    if (!best || ms < best_ms) {
+      if (best) {
+        cudaGraphExecDestroy(best);
+        cudaFree(best_tab);
+      }
+      best = ex;
+      best_tab = tb;
+      best_ms = ms;
+      best_groups = g;
+      best_stages = ns;
+    } else {
+      cudaGraphExecDestroy(ex);
+      cudaFree(tb);
+    }
+  }
+  if (e0) cudaEventDestroy(e0);
+  if (e1) cudaEventDestroy(e1);
+  if (!best) return FFXG_ERR_CUDA;
+  b.tuned_groups = best_groups;
+  b.exec[key] = best;
+  b.d_tab[key] = best_tab;
   b.staged[key] = true;
-  b.n_stages[key] = (int)stages.size();
-  b.copies[key].resize(S);
-  for (size_t s = 0; s < S; s++) b.copies[key][s] = rec[s].copies;
+  b.n_stages[key] = best_stages;
+  b.copies[key].resize(rec.size());
+  for (size_t s = 0; s < rec.size(); s++) b.copies[key][s] = rec[s].copies;
   b.gen.clear();
   for (ffxg_handle *hh : b.sys) b.gen.push_back(handle_of(hh).graph_gen);
   b.graph_builds++;
@@ -485,6 +626,23 @@ int32_t ffxg_batch_stages(const ffxg_batch *b, int want_grad) {
   if (!b) return -1;
   const int key = want_grad ? 1 : 0;
   return b->staged[key] ? b->n_stages[key] : 0;
+}
+
+int32_t ffxg_batch_tuning(const ffxg_batch *b, int32_t *candidates, double *ms) {
+  if (!b) return -1;
+  for (int k = 0; k < 4; k++) {
+    if (candidates) candidates[k] = b->tune_groups[k];
+    if (ms) ms[k] = b->tune_ms[k];
+  }
+  return b->tuned_groups;
+}
+
+int ffxg_batch_set_groups(ffxg_batch *b, int32_t groups) {
+  if (!b || groups < 0 || groups > 64) return FFXG_ERR_BAD_ARG;
+  if (groups != b->tuned_groups) batch_drop_graphs(*b);
+  b->tuned_groups = groups;
+  for (int k = 0; k < 4; k++) { b->tune_groups[k] = 0; b->tune_ms[k] = 0.f; }
+  return FFXG_OK;
 }
 
 int ffxg_batch_energy(ffxg_batch *b, const double *xyz, int want_grad, double *terms, double *grad, int64_t *counts,

@@ -291,6 +291,16 @@ int64_t ffxg_batch_graph_builds(const ffxg_batch *b);
 /* Stages of the batch's stage-by-stage graph for want_grad (0 when the batch has none:
  * not built yet, or BRANCHES / LOOP). */
 int32_t ffxg_batch_stages(const ffxg_batch *b, int want_grad);
+/* GRAPH mode runs the systems in groups of near-equal atom count, each group a branch of
+ * the graph with its own stages and solver loop, so that the groups' kernels overlap.  The
+ * number of groups is autotuned when the graph is first built: 1, 2, 4 and 8 groups are
+ * built and timed on the device, and the fastest is kept (a batch with the ASPC predictor
+ * takes 4 untimed).  ffxg_batch_tuning returns the chosen number (0 before the first
+ * build) and fills candidates[4] / ms[4] (each may be NULL) with the candidates timed and
+ * their milliseconds per batch; ffxg_batch_set_groups fixes the number instead (0: tune
+ * again) and drops the built graphs. */
+int32_t ffxg_batch_tuning(const ffxg_batch *b, int32_t *candidates, double *ms);
+int ffxg_batch_set_groups(ffxg_batch *b, int32_t groups);
 const char *ffxg_batch_last_error(const ffxg_batch *b);
 void ffxg_batch_destroy(ffxg_batch *b);
 

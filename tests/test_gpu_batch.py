@@ -49,7 +49,15 @@ def test_batch_matches_single_system_handles(precision):
                     _same(precision, b.terms[j], grads[j], hist[j][1 if k == 0 else 2], (mode, k, j))
             if mode == "graph":
                 assert b.stages() > 50
+                chosen, times = b.tuning()
+                assert chosen in (1, 2, 4, 8) and chosen in times and min(times, key=times.get) == chosen
         assert b.graph_builds >= 1
+        for groups in (3, 1):     # a fixed number of groups: the same results
+            b.set_groups(groups)
+            e, grads = b.energy_and_gradient(moved)
+            for j in range(len(systems)):
+                _same(precision, b.terms[j], grads[j], hist[j][2], ("groups", groups, j))
+            assert b.tuning()[0] == groups
 
 
 def _same(precision, terms, grad, ref, tag):
