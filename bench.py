@@ -28,9 +28,6 @@ import time
 
 ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
-# Hardware work queues per process (read when CUDA starts): a batch in BRANCHES mode runs
-# one graph branch per system, and more queues let more of them run at once.
-os.environ.setdefault("CUDA_DEVICE_MAX_CONNECTIONS", "32")
 
 import numpy as np  # noqa: E402
 
