@@ -250,12 +250,14 @@ def measure(args, precision, system, dist, world, local):
     }
 
 
-def measure_md(args, system, dist, world):
+def measure_md(args, system, dist, world, aspc=False):
     """Config 2's dynamics: ``--md-steps`` velocity-Verlet steps of 2 fs with SETTLE rigid
     waters on the device (ffxg_md_run: positions and velocities stay on the GPU, every step
     replays the evaluation graph, the neighbour list is rebuilt whenever an atom has moved
     more than half the buffer), mixed form, velocities drawn at 300 K.  Timed on the host
-    clock around the one call, host copies included; ns/day is measured, not extrapolated."""
+    clock around the one call, host copies included; ns/day is measured, not extrapolated.
+    aspc: with the `scf-predictor ASPC` key (the solve starts from the extrapolation of the
+    last six solutions; the reference's default, and the headline's, is no predictor)."""
     import math
     import torch
     from forcefieldx_b200.energy import ForceFieldEnergy
@@ -267,6 +269,8 @@ def measure_md(args, system, dist, world):
     vel = rng.normal(size=(n, 3)) * np.sqrt(kb * 300.0 * kcal / mass)[:, None]
     with ForceFieldEnergy(system, build_params(PRECISION_MIXED)) as ffe:
         ffe.md_setup(mass, np.arange(n).reshape(-1, 3), roh, 2.0 * roh * math.sin(theta / 2.0))
+        if aspc:
+            ffe.set_scf_predictor(True)
         x, v, _, _ = ffe.md_run(system.xyz, vel, 0.002, 20)          # warm-up: graphs captured
         if dist:
             dist.barrier()
@@ -282,7 +286,7 @@ def measure_md(args, system, dist, world):
             dt = float(t.item())
     return {"steps": args.md_steps, "dt_fs": 2.0, "precision": "mixed", "seconds": dt,
             "ns_per_day": world * args.md_steps * 2e-6 / dt * 86400.0, "steps_per_s": world * args.md_steps / dt,
-            "list_builds": int(builds),
+            "list_builds": int(builds), "scf_predictor": "ASPC" if aspc else "none",
             "method": "ffxg_md_run: velocity Verlet + SETTLE on the device, 300 K start, host clock around the call"}
 
 
@@ -310,6 +314,7 @@ def run_mine(args):
     md = None
     if args.md_steps > 0:
         md = measure_md(args, system, dist, world)
+        md["with_aspc_predictor"] = measure_md(args, system, dist, world, aspc=True)
 
     batch = None
     if args.batch_systems > 0:

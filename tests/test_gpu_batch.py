@@ -130,3 +130,25 @@ def test_lambda_change_recaptures_batch_graph():
         ref = ob.energy(s0, params[0], alchemy=a, lam=0.5)
         assert abs(e1[0] - ref["terms"][9]) < 1e-8 * abs(ref["terms"][9])
         assert np.all(np.abs(e1[1:] - e0[1:]) < 1e-11 * np.abs(e0[1:]))   # the other systems unchanged
+
+
+@pytest.mark.parametrize("precision", [PRECISION_MIXED, PRECISION_FP64])
+def test_staged_batch_of_the_reference_crystals(precision, fixtures):
+    """The five small-molecule crystals (P1 cells of their mates, monoclinic and
+    orthorhombic, every lattice image listed) as one stage-by-stage batch against their
+    own handles."""
+    from tests.common import CRYSTALS, golden_system
+    pairs = [golden_system(name, fixtures, precision=precision) for name in CRYSTALS]
+    systems, params = [s for s, _ in pairs], [p for _, p in pairs]
+    hist = []
+    for s, p in pairs:
+        with ForceFieldEnergy(s, p) as f:
+            f.energy_and_gradient(s.xyz)
+            e, g = f.energy_and_gradient(s.xyz)
+            hist.append((f.terms.copy(), g.copy()))
+    with BatchEnergy(systems, params) as b:
+        for _ in range(3):
+            e, grads = b.energy_and_gradient()
+            for j in range(len(systems)):
+                _same(precision, b.terms[j], grads[j], hist[j], CRYSTALS[j])
+        assert b.stages() > 50
