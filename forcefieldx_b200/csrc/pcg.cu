@@ -42,7 +42,10 @@ static int group_blocks(int n, int G) { return std::max(1, (n + kFieldThreads / 
 // The vector kernels stride over atoms with a fixed grid for large systems.
 static int vec_blocks(int n) { return std::min(kVecBlocks, std::max(1, (n + kVecThreads - 1) / kVecThreads)); }
 // The combine takes one atom per warp; its partial rows are one per block.
-static int combine_blocks(int n) { return nblocks((int64_t)n * 32, 256); }
+// The combine takes kCombineGroup lanes per atom (32 / kCombineGroup atoms per warp);
+// its partial rows are one per block.
+constexpr int kCombineGroup = 8;
+static int combine_blocks(int n) { return nblocks((int64_t)n * kCombineGroup, 256); }
 // Totals of the PCG scalars in Handle::d_scalars.
 enum { T_PAP = 0, T_PAPP, T_RZ, T_RZP, T_RZN, T_RZNP, T_BETA, T_BETAP };
 // Counters (each returns to 0 after use) in Handle::d_counter.
@@ -247,6 +250,47 @@ __device__ __forceinline__ void mesh_field(int i, int n, const int *__restrict__
   for (int q = 0; q < 6; q++) acc[q] += g[q];
 }
 
+// The same for a group of G lanes per atom (sub = 0 .. G-1): lane sub takes the (x, y)
+// support points sub, sub + G, ... of the 25, each with its five z layers, so that every
+// lane has several gathers in flight.  i < 0: an idle group (no loads, zero partials).
+template <typename T, int G>
+__device__ __forceinline__ void mesh_field_group(int i, int sub, int n, const int *__restrict__ igrid,
+                                                 const T *__restrict__ spl,
+                                                 const typename Vec2<T>::type *__restrict__ mesh, int nfx, int nfy,
+                                                 int nfz, T *acc) {
+  if (i < 0) return;
+  const T *sp = spl + (size_t)i * 3 * kOrder * 4;
+  const T *sx = sp, *sy = sp + kOrder * 4, *sz = sp + 2 * kOrder * 4;
+  const int i0 = igrid[i] + 1, j0 = igrid[n + i] + 1, k0 = igrid[2 * n + i] + 1;
+  T g[6] = {0, 0, 0, 0, 0, 0};
+#pragma unroll
+  for (int t = 0; t < (25 + G - 1) / G; t++) {
+    const int pt = sub + G * t;
+    if (pt < 25) {
+      const int a1 = pt % 5, a2 = pt / 5;
+      int ii = i0 + a1, jj = j0 + a2;
+      ii += (ii < 0) ? nfx : ((ii >= nfx) ? -nfx : 0);
+      jj += (jj < 0) ? nfy : ((jj >= nfy) ? -nfy : 0);
+      const T x0 = sx[a1 * 4], x1 = sx[a1 * 4 + 1];
+      const T y0 = sy[a2 * 4], y1 = sy[a2 * 4 + 1];
+      const T w10 = x1 * y0, w01 = x0 * y1, w00 = x0 * y0;
+      const auto *col = mesh + (size_t)jj * nfx + ii;
+#pragma unroll
+      for (int a3 = 0; a3 < 5; a3++) {
+        int kk = k0 + a3;
+        kk += (kk < 0) ? nfz : ((kk >= nfz) ? -nfz : 0);
+        const auto m = col[(size_t)kk * nfy * nfx];
+        const T z0 = sz[a3 * 4], z1 = sz[a3 * 4 + 1];
+        const T wx = w10 * z0, wy = w01 * z0, wz = w00 * z1;
+        g[0] = fma(m.x, wx, g[0]); g[1] = fma(m.x, wy, g[1]); g[2] = fma(m.x, wz, g[2]);
+        g[3] = fma(m.y, wx, g[3]); g[4] = fma(m.y, wy, g[4]); g[5] = fma(m.y, wz, g[5]);
+      }
+    }
+  }
+#pragma unroll
+  for (int q = 0; q < 6; q++) acc[q] += g[q];
+}
+
 // Real-space pair field of the source records `rec` (u, then z) at every atom, into
 // out[6][n] (D xyz, CR xyz).  A group of G lanes takes one atom; the groups of a warp take
 // consecutive atoms and stride over the system together.
@@ -286,8 +330,8 @@ __device__ __forceinline__ void k_pair_field(VGrid vg, int n, const int *__restr
 // MODE 2: v = z.  T p = E(z) + beta T p_old and p = z + beta p_old (first: T p = E(z),
 //         p = z); vec = p / alpha - T p; p . vec and r . z finished into d_scalars
 //         (UpdateApLoop).
-// One warp per atom: all lanes interpolate the mesh, then lane q < 6 finishes component
-// q (D x, y, z, CR x, y, z).
+// kCombineGroup lanes per atom: the group interpolates the mesh, then its lane q < 6
+// finishes component q (D x, y, z, CR x, y, z).
 template <int MODE, typename T>
 __device__ __forceinline__ void k_pcg_combine(VGrid vg, 
     int n, const int *__restrict__ igrid, const T *__restrict__ spl, const typename Vec2<T>::type *__restrict__ mesh,
@@ -296,66 +340,70 @@ __device__ __forceinline__ void k_pcg_combine(VGrid vg,
     const double *__restrict__ udirD, const double *__restrict__ udirP, double *p, double *pP, double *tp,
     int first, const double *__restrict__ r, const double *__restrict__ rP, double *outD, double *outP, T *recP,
     double *part, unsigned *counter, double *tot) {
-  const int lane = threadIdx.x & 31;
-  const int i = (vg.bid * blockDim.x + threadIdx.x) >> 5;
+  constexpr int G = kCombineGroup;
+  const int lane = threadIdx.x & 31, sub = lane & (G - 1), g0 = lane & ~(G - 1);
+  const int i = (vg.bid * blockDim.x + threadIdx.x) / G;
+  const bool live = i < n;
   double acc[4] = {0, 0, 0, 0};
-  if (i < n) {
-    T a6[6] = {0, 0, 0, 0, 0, 0};
-    mesh_field(i, n, igrid, spl, mesh, nfx, nfy, nfz, a6);
-    T g[6];
+  T a6[6] = {0, 0, 0, 0, 0, 0};
+  mesh_field_group<T, G>(live ? i : -1, sub, n, igrid, spl, mesh, nfx, nfy, nfz, a6);
+  T g[6];
 #pragma unroll
-    for (int q = 0; q < 6; q++) g[q] = warp_sum(a6[q]);
-    // Lane q < 6 takes Cartesian field component q: -(xf . gradient) of its set.
-    const int d = lane % 3, set = lane / 3;
-    const double *row = xf.m[lane < 6 ? d : 0];
-    const double mine = (lane < 6) ? -(row[0] * (double)(set ? g[3] : g[0]) + row[1] * (double)(set ? g[4] : g[1]) +
-                                       row[2] * (double)(set ? g[5] : g[2]))
-                                   : 0.0;
-    double rec_v = 0.0;
-    if (lane < 6) {
-      const size_t j = (size_t)d * n + i, jt = (size_t)lane * n + i;
-      const double *v = set ? vP : vD;
-      const double vj = v[j];
-      const double e = mine + tpair[jt] + aewald3 * vj;
-      const double a = polar[i];
-      const bool ok = a > 0.0;
-      const double ip = ok ? 1.0 / a : 0.0;
-      if (MODE == 1) {
-        const double *ud = set ? udirP : udirD;
-        const double rv = ok ? (ud[j] - vj) * ip + e : 0.0;
-        (set ? outP : outD)[j] = rv;
-        rec_v = a * rv;
-      } else {
-        const double b = first ? 0.0 : tot[set ? T_BETAP : T_BETA];
-        double *pp = set ? pP : p;
-        double t = e, pv = vj;
-        if (!first) {
-          t += b * tp[jt];
-          pv += b * pp[j];
-        }
-        tp[jt] = t;
-        pp[j] = pv;
-        const double vv = ok ? pv * ip - t : 0.0;
-        (set ? outP : outD)[j] = vv;
-        const double pav = pv * vv, rzv = (set ? rP : r)[j] * vj;
-        acc[0] = set ? 0.0 : pav;
-        acc[1] = set ? pav : 0.0;
-        acc[2] = set ? 0.0 : rzv;
-        acc[3] = set ? rzv : 0.0;
-      }
-    }
+  for (int q = 0; q < 6; q++) {
+    T v = a6[q];
+#pragma unroll
+    for (int o = G / 2; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    g[q] = v;
+  }
+  double rec_v = 0.0;
+  if (live && sub < 6) {
+    // Lane sub takes Cartesian field component sub: -(xf . gradient) of its set.
+    const int d = sub % 3, set = sub / 3;
+    const double *row = xf.m[d];
+    const double mine = -(row[0] * (double)(set ? g[3] : g[0]) + row[1] * (double)(set ? g[4] : g[1]) +
+                          row[2] * (double)(set ? g[5] : g[2]));
+    const size_t j = (size_t)d * n + i, jt = (size_t)sub * n + i;
+    const double *v = set ? vP : vD;
+    const double vj = v[j];
+    const double e = mine + tpair[jt] + aewald3 * vj;
+    const double a = polar[i];
+    const bool ok = a > 0.0;
+    const double ip = ok ? 1.0 / a : 0.0;
     if (MODE == 1) {
-      double w[6];
-#pragma unroll
-      for (int q = 0; q < 6; q++) w[q] = __shfl_sync(0xffffffffu, rec_v, q);
-      if (lane == 0) put_rec(recP, i, w[0], w[1], w[2], w[3], w[4], w[5]);
+      const double *ud = set ? udirP : udirD;
+      const double rv = ok ? (ud[j] - vj) * ip + e : 0.0;
+      (set ? outP : outD)[j] = rv;
+      rec_v = a * rv;
+    } else {
+      const double b = first ? 0.0 : tot[set ? T_BETAP : T_BETA];
+      double *pp = set ? pP : p;
+      double t = e, pv = vj;
+      if (!first) {
+        t += b * tp[jt];
+        pv += b * pp[j];
+      }
+      tp[jt] = t;
+      pp[j] = pv;
+      const double vv = ok ? pv * ip - t : 0.0;
+      (set ? outP : outD)[j] = vv;
+      const double pav = pv * vv, rzv = (set ? rP : r)[j] * vj;
+      acc[0] = set ? 0.0 : pav;
+      acc[1] = set ? pav : 0.0;
+      acc[2] = set ? 0.0 : rzv;
+      acc[3] = set ? rzv : 0.0;
     }
+  }
+  if (MODE == 1) {
+    double w[6];
+#pragma unroll
+    for (int q = 0; q < 6; q++) w[q] = __shfl_sync(0xffffffffu, rec_v, g0 + q);
+    if (live && sub == 0) put_rec(recP, i, w[0], w[1], w[2], w[3], w[4], w[5]);
   }
   if (MODE == 2) {
 #pragma unroll
     for (int q = 0; q < 4; q++)
 #pragma unroll
-      for (int o = 4; o > 0; o >>= 1) acc[q] += __shfl_xor_sync(0xffffffffu, acc[q], o);
+      for (int o = 16; o > 0; o >>= 1) acc[q] += __shfl_xor_sync(0xffffffffu, acc[q], o);
     block_store_lane0<4>(vg, acc, part);
   }
 }
@@ -633,7 +681,7 @@ static void combine(Handle &h, const double *vD, const double *vP, bool first, d
   for (int a = 0; a < 3; a++)
     for (int b = 0; b < 3; b++) xf.m[a][b] = h.pc.tfm[1 + a][1 + b];
   const V2 *mesh = reinterpret_cast<const V2 *>(h.mixed ? (const void *)h.d_gridf : (const void *)h.d_grid);
-  launch_on<k_pcg_combine<MODE, T>, 256, 0, 4>(
+  launch_on<k_pcg_combine<MODE, T>, 256, 0, 3>(
       h.rec, combine_blocks(h.n), 256, 0, h.stream, h.n, (const int *)h.d_igrid, reinterpret_cast<const T *>(h.d_spl),
       mesh, h.nfft[0], h.nfft[1], h.nfft[2], xf, (const double *)h.d_tpair, vD, vP, aewald3_of(h),
       (const double *)h.d_polar, (const double *)h.d_udirD, (const double *)h.d_udirP, h.d_p, h.d_pP, h.d_tp,
