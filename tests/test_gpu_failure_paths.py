@@ -10,6 +10,8 @@
   throws it (PCGSolver.java:547-559).
 * The mixed form's fixed-point range: a close contact drives real-space forces above
   2^20 kcal/mol/A; the call completes and returns FFXG_ERR_RANGE.
+* List regrowth inside a batch graph (stage by stage and as branches): the overflowing
+  system is repeated directly and the batch graph rebuilt on the grown lists.
 * The FFT's shared-memory limit is process-wide: a mesh whose longest axis comes first
   needs more than 48 KB per line batch, and creating a handle with smaller axes later
   must not take that limit away from the first handle.
@@ -137,3 +139,31 @@ def test_fft_limit_survives_later_handles(fixtures, graph):
     assert rel.max() < E_REL, (terms, ref["terms"])
     assert np.max(np.abs(terms - first) / np.maximum(np.abs(first), 1.0)) < 1e-11
     assert float(np.sqrt(np.mean((g - ref["grad"]) ** 2))) < G_RMS
+
+
+@pytest.mark.parametrize("mode", ["graph", "branches"])
+def test_list_overflow_inside_a_batch_graph(mode):
+    """One system of a batch meets a configuration at twice its density while the batch
+    replays its graph: the system's rows overflow, the batch drops its graph, grows that
+    system's lists and repeats it directly, and every system's result is the oracle's; the
+    next call rebuilds the batch graph on the grown lists."""
+    from forcefieldx_b200.batch import BatchEnergy
+    dilute, compact = _dilute_and_compact(seed=23)
+    other = water_box(6, 18.643, seed=29)
+    p24 = water_params(24.0, pme_grid=(24, 24, 24), precision=PRECISION_FP64)
+    p18 = water_params(18.643, pme_grid=(20, 20, 20), precision=PRECISION_FP64)
+    with BatchEnergy([dilute, other], [p24, p18]) as b:
+        b.set_mode(mode)
+        for _ in range(2):                          # lists built, then the batch graph
+            b.energy_and_gradient([dilute.xyz, other.xyz])
+        builds = b.graph_builds
+        for call in range(2):
+            e, grads = b.energy_and_gradient([compact, other.xyz])
+            for j, (s, p, x) in enumerate([(dilute, p24, compact), (other, p18, other.xyz)]):
+                ref = ob.energy(s, p, xyz=x)
+                rel = np.abs(b.terms[j] - ref["terms"]) / np.maximum(np.abs(ref["terms"]), 1.0)
+                assert rel.max() < E_REL, (mode, call, j, b.terms[j], ref["terms"])
+                assert float(np.sqrt(np.mean((grads[j] - ref["grad"]) ** 2))) < G_RMS
+            if call == 0:
+                assert b.counts[0][5] >= 1           # the dense system's lists grew
+        assert b.graph_builds > builds               # rebuilt on the grown lists
