@@ -202,6 +202,20 @@ __device__ __forceinline__ T warp_sum(T v) {
   return v;
 }
 
+// One 32-byte read-only global load: a single 256-bit access on sm_100 (one pass through
+// the L1 for a gathered record instead of two or three).  p must be 32-byte aligned and
+// point to global memory.
+__device__ __forceinline__ void ldg_32b(const float *p, float *v) {
+  asm("ld.global.nc.v8.f32 {%0, %1, %2, %3, %4, %5, %6, %7}, [%8];"
+      : "=f"(v[0]), "=f"(v[1]), "=f"(v[2]), "=f"(v[3]), "=f"(v[4]), "=f"(v[5]), "=f"(v[6]), "=f"(v[7])
+      : "l"(__cvta_generic_to_global(p)));
+}
+__device__ __forceinline__ void ldg_32b(const double *p, double *v) {
+  asm("ld.global.nc.v4.f64 {%0, %1, %2, %3}, [%4];"
+      : "=d"(v[0]), "=d"(v[1]), "=d"(v[2]), "=d"(v[3])
+      : "l"(__cvta_generic_to_global(p)));
+}
+
 // Packed per-atom source records for the field gathers: T[8] per atom = (D xyz, CR xyz,
 // pad), T = double (plain form) or float (mixed form), so a neighbour costs one 64- or
 // 32-byte record instead of six scattered loads.  Positions are packed as double2
@@ -228,9 +242,10 @@ __device__ __forceinline__ void get_rec(const T *__restrict__ rec, int k, T *v) 
                   c = __ldg(reinterpret_cast<const double2 *>(q) + 2);
     v[0] = a.x; v[1] = a.y; v[2] = b.x; v[3] = b.y; v[4] = c.x; v[5] = c.y;
   } else {
-    const float4 a = __ldg(reinterpret_cast<const float4 *>(q));
-    const float2 b = __ldg(reinterpret_cast<const float2 *>(q) + 2);
-    v[0] = a.x; v[1] = a.y; v[2] = a.z; v[3] = a.w; v[4] = b.x; v[5] = b.y;
+    float a[8];
+    ldg_32b(q, a);
+#pragma unroll
+    for (int c = 0; c < 6; c++) v[c] = a[c];
   }
 }
 
@@ -245,12 +260,13 @@ constexpr int kRecInduced = 16;
 // M entries of atom k's record from entry OFF (both multiples of four values or two).
 template <int OFF, int M>
 __device__ __forceinline__ void load_rec(const float *__restrict__ rec, int k, float *v) {
-  static_assert(OFF % 4 == 0 && M % 4 == 0, "float records load as float4");
-  const float4 *q = reinterpret_cast<const float4 *>(rec + (size_t)k * kRecStride + OFF);
+  static_assert(OFF % 8 == 0 && M % 4 == 0, "float records load as 32 bytes, then 16");
+  const float *q = rec + (size_t)k * kRecStride + OFF;
 #pragma unroll
-  for (int j = 0; j < M / 4; j++) {
-    const float4 t = __ldg(q + j);
-    v[4 * j] = t.x; v[4 * j + 1] = t.y; v[4 * j + 2] = t.z; v[4 * j + 3] = t.w;
+  for (int j = 0; j < M / 8; j++) ldg_32b(q + 8 * j, v + 8 * j);
+  if constexpr (M % 8 == 4) {
+    const float4 t = __ldg(reinterpret_cast<const float4 *>(q + M - 4));
+    v[M - 4] = t.x; v[M - 3] = t.y; v[M - 2] = t.z; v[M - 1] = t.w;
   }
 }
 template <int OFF, int M>
@@ -266,8 +282,9 @@ __device__ __forceinline__ void load_rec(const double *__restrict__ rec, int k, 
 
 // Position of atom k from the packed (x, y), (z, 0) pairs: one 32-byte sector.
 __device__ __forceinline__ void load_pos(const double2 *__restrict__ pos, int k, double &x, double &y, double &z) {
-  const double2 a = __ldg(pos + 2 * (size_t)k), b = __ldg(pos + 2 * (size_t)k + 1);
-  x = a.x; y = a.y; z = b.x;
+  double t[4];
+  ldg_32b(reinterpret_cast<const double *>(pos + 2 * (size_t)k), t);
+  x = t[0]; y = t[1]; z = t[2];
 }
 
 // One cached pair of the dipole-field lists: the minimum-image displacement r = x_k - x_i

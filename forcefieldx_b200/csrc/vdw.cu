@@ -175,10 +175,11 @@ __device__ __forceinline__ void k_vdw(VGrid vg, int n, const double *__restrict_
       if (a < m) {
         k = row[a];
         const size_t ent = (size_t)i * cap + a;
-        const double2 pa = __ldg(rpos + 2 * (size_t)k), pb = __ldg(rpos + 2 * (size_t)k + 1);
-        double dxd = __dsub_rn(xi, pa.x), dyd = __dsub_rn(yi, pa.y), dzd = __dsub_rn(zi, pb.x);
+        double pk[4];
+        ldg_32b(reinterpret_cast<const double *>(rpos + 2 * (size_t)k), pk);
+        double dxd = __dsub_rn(xi, pk[0]), dyd = __dsub_rn(yi, pk[1]), dzd = __dsub_rn(zi, pk[2]);
         const double r2d = pair_image(dxd, dyd, dzd, bx, nbr_sh, ent, -1.0);
-        tk = (int)__double_as_longlong(pb.y);
+        tk = (int)__double_as_longlong(pk[3]);
         const R irv = vrad[ti * ntypes + tk];
         if (r2d <= vf.off2 && irv > R(0.0)) {
           const unsigned code = pair_primary(nbr_sh, ent) ? vexcl_code(i, k, eptr, ek, ecode, elo, ehi) : 0u;
