@@ -290,7 +290,8 @@ __device__ __forceinline__ void load_pos(const double2 *__restrict__ pos, int k,
 // One cached pair of the dipole-field lists: the minimum-image displacement r = x_k - x_i
 // and the coefficients A (scalar part) and B (dyadic part) of the field -A u + B (u.r) r.
 // Plain form: FP64, 40 bytes; mixed form: FP32, 20 bytes.  Stored as a 32- or 16-byte
-// record (x, y, z, A) plus B in a parallel array, both read as coalesced streams.
+// record (x, y, z, A) plus B in a parallel array of 8-byte slots (store_pair_b), both read
+// as coalesced streams.
 template <typename T> struct PairRec;
 template <> struct alignas(32) PairRec<double> { double2 xy, za; };
 template <> struct alignas(16) PairRec<float> { float4 v; };
@@ -311,6 +312,25 @@ __device__ __forceinline__ void load_pair(const PairRec<float> *__restrict__ p, 
                                           float &z, float &a) {
   const float4 u = __ldg(&p[e].v);
   x = u.x; y = u.y; z = u.z; a = u.w;
+}
+
+// The dyadic coefficient B of cached pair e and its partner k.  Plain form: B in its own
+// FP64 array, k from the list row.  Mixed form: (k, B) packed in the same 8-byte slot, so
+// one load brings both (the list row is still written for the other pair kernels).
+__device__ __forceinline__ void store_pair_b(double *pb, size_t e, int, double b) { pb[e] = b; }
+__device__ __forceinline__ void store_pair_b(float *pb, size_t e, int k, float b) {
+  reinterpret_cast<int2 *>(pb)[e] = make_int2(k, __float_as_int(b));
+}
+__device__ __forceinline__ void load_pair_b(const double *__restrict__ pb, const int *__restrict__ lst, size_t e,
+                                            int &k, double &b) {
+  k = __ldg(lst + e);
+  b = __ldg(pb + e);
+}
+__device__ __forceinline__ void load_pair_b(const float *__restrict__ pb, const int *__restrict__, size_t e, int &k,
+                                            float &b) {
+  const int2 t = __ldg(reinterpret_cast<const int2 *>(pb) + e);
+  k = t.x;
+  b = __int_as_float(t.y);
 }
 
 // PME transforms of one handle (passed to kernels by value).

@@ -179,19 +179,17 @@ __device__ __forceinline__ void pair_field(int i, int sub, const int *__restrict
                                            const T *__restrict__ rec, T *acc) {
   const int cnt = (i < 0) ? 0 : min(lst_cnt[i], cap);
   const size_t e0 = (size_t)(i < 0 ? 0 : i) * cap;
-  const int *row = lst + e0;
   for (int a = sub; a < cnt; a += G * NU) {
     int ix[NU], kk[NU];
     T xx[NU], yy[NU], zz[NU], AA[NU], BB[NU], ss[NU][6];
 #pragma unroll
     for (int u = 0; u < NU; u++) {
       ix[u] = (a + G * u < cnt) ? a + G * u : a;
-      kk[u] = __ldg(row + ix[u]);
+      load_pair_b(pb, lst, e0 + ix[u], kk[u], BB[u]);
     }
 #pragma unroll
     for (int u = 0; u < NU; u++) {
       load_pair(pr, e0 + ix[u], xx[u], yy[u], zz[u], AA[u]);
-      BB[u] = __ldg(pb + e0 + ix[u]);
       get_rec(rec, kk[u], ss[u]);
     }
 #pragma unroll
@@ -721,7 +719,7 @@ static void field_of(Handle &h, const double *vD, const double *vP, bool first, 
 
 template <bool INIT, typename T>
 static void precond(Handle &h) {
-  launch_on<k_pcg_precond<INIT, T, kPrecondGroup>, kFieldThreads, sizeof(T) == 8 ? 7 : 0, sizeof(T) == 4 ? 5 : 0>(
+  launch_on<k_pcg_precond<INIT, T, kPrecondGroup>, kFieldThreads, 7, sizeof(T) == 4 ? 5 : 0>(
       h.rec, group_blocks(h.n, kPrecondGroup), kFieldThreads, 0, h.stream, h.n, (const int *)h.d_prl,
       (const int *)h.d_prl_cnt, h.cap_prl, reinterpret_cast<const PairRec<T> *>(h.d_coefP),
       reinterpret_cast<const T *>(h.d_coefPB), reinterpret_cast<const T *>(h.d_recP), (const double *)h.d_polar,

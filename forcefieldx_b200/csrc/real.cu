@@ -125,6 +125,7 @@ __device__ __forceinline__ void k_realspace_field(VGrid vg,
     const bool act = a < cnt;
     bool pr = false;
     R pA = R(0), pB = R(0), px_ = R(0), py_ = R(0), pz_ = R(0);
+    int pk = 0;
     if (act) {
       const int k = row[a];
       const size_t ent = (size_t)i * capE + a;
@@ -187,13 +188,14 @@ __device__ __forceinline__ void k_realspace_field(VGrid vg,
       const R urr3 = (R(1.0) - scale3) * rr3, urr5 = (R(1.0) - scale5) * rr5;
       if (a < capE) {
         store_pair(coefE, (size_t)i * capE + a, xr, yr, zr, bn1 - urr3);
-        coefEB[(size_t)i * capE + a] = bn2 - urr5;
+        store_pair_b(coefEB, (size_t)i * capE + a, k, bn2 - urr5);
       }
       pr = r2d <= pcut2;   // the same test, in FP64, that selected the preconditioner row
       if (pr) {
         const R b1 = rr1 * rr2, b2 = R(3.0) * b1 * rr2;   // Ewald off: bn0 = 1/r
         pA = b1 - urr3;
         pB = b2 - urr5;
+        pk = k;
         px_ = xr; py_ = yr; pz_ = zr;
       }
     }
@@ -202,7 +204,7 @@ __device__ __forceinline__ void k_realspace_field(VGrid vg,
       const int pos = cp + __popc(mp & lt);
       if (pos < capP) {
         store_pair(coefP, (size_t)i * capP + pos, px_, py_, pz_, pA);
-        coefPB[(size_t)i * capP + pos] = pB;
+        store_pair_b(coefPB, (size_t)i * capP + pos, pk, pB);
       }
     }
     cp += __popc(mp);
