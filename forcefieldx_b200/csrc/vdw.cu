@@ -282,11 +282,15 @@ void launch_vdw(Handle &h, bool grad, cudaStream_t st) {
   vf.c5 = -6.0 / den;
   vf.cut = cut;
   vf.iwidth = 1.0 / (off - cut);
-  // In a captured evaluation vdW is a low-priority branch beside the solver: at most four
-  // blocks per SM, warps striding over atoms, leave the solver's kernels most of every SM
-  // (measured 1% faster than a full grid, which takes issue slots from the solver).
+  // In a captured evaluation vdW is a low-priority branch beside the permanent field and
+  // the solver: one block of eight warps per SM, warps striding over atoms.  Its blocks
+  // stay resident until the term is done, so a wider branch holds the registers the
+  // other kernels need: at four blocks per SM (the whole register file) the permanent
+  // field and reciprocal chain waited ~140 us for it on the 24k box; at one block per SM
+  // it runs in the solver's idle issue slots (657-668 -> 696 evals/s; 128-thread blocks
+  // or two per SM measured slower).
   const int full = nblocks((int64_t)h.n * 32, 256);
-  const int blocks = h.capturing ? std::min(full, 4 * h.num_sms) : full;
+  const int blocks = h.capturing ? std::min(full, h.num_sms) : full;
   if (h.alch.active) {
     if (h.mixed) vdw_launch<float, true>(h, grad, st, vf, blocks);
     else vdw_launch<double, true>(h, grad, st, vf, blocks);
