@@ -69,6 +69,7 @@ struct ffxg_batch {
   int mode = FFXG_BATCH_GRAPH;
   double *d_xyz = nullptr, *d_grad = nullptr;    // [total][3] on the device
   double *h_xyz = nullptr, *h_grad = nullptr;    // pinned mirrors
+  bool xyz_valid = true;   // h_xyz holds accepted coordinates (false after a rejected copy)
   cudaStream_t stream = nullptr, side = nullptr;
   cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
   cudaGraphExec_t exec[2] = {nullptr, nullptr};  // by want_grad
@@ -650,10 +651,17 @@ int ffxg_batch_energy(ffxg_batch *b, const double *xyz, int want_grad, double *t
   if (!b || !terms || (want_grad && !grad)) return FFXG_ERR_BAD_ARG;
   const size_t S = b->sys.size();
   const size_t m = 3 * (size_t)b->off.back();
+  // Checked while copied (one pass, several host threads); a rejected copy leaves no
+  // coordinates to reuse.
   if (xyz) {
-    for (size_t j = 0; j < m; j++)
-      if (!std::isfinite(xyz[j])) { b->err = "non-finite coordinates"; return FFXG_ERR_NONFINITE; }
-    std::memcpy(b->h_xyz, xyz, m * sizeof(double));
+    b->xyz_valid = copy_finite_parallel(b->h_xyz, xyz, m);
+    if (!b->xyz_valid) {
+      b->err = "non-finite coordinates";
+      return FFXG_ERR_NONFINITE;
+    }
+  } else if (!b->xyz_valid) {
+    b->err = "no coordinates to reuse: the last ones were rejected";
+    return FFXG_ERR_BAD_ARG;
   }
   auto fail_cuda = [&]() {
     b->err = std::string("CUDA error: ") + cudaGetErrorString(cudaGetLastError());
@@ -702,7 +710,7 @@ int ffxg_batch_energy(ffxg_batch *b, const double *xyz, int want_grad, double *t
     if (cudaMemcpyAsync(b->h_grad, b->d_grad, m * sizeof(double), cudaMemcpyDeviceToHost, b->stream) != cudaSuccess)
       return fail_cuda();
     if (cudaStreamSynchronize(b->stream) != cudaSuccess) return fail_cuda();
-    std::memcpy(grad, b->h_grad, m * sizeof(double));
+    copy_parallel(grad, b->h_grad, m);
   }
   int first = FFXG_OK;
   for (size_t s = 0; s < S; s++) {

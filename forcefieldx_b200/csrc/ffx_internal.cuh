@@ -613,6 +613,8 @@ void launch_bsplines(Handle &h);
 // Copies m doubles into dst (the pinned staging buffer) and tests them for Inf/NaN in the
 // same pass (exponent bits all ones); false if any is not finite.
 bool copy_finite(double *dst, const double *src, size_t m);
+bool copy_finite_parallel(double *dst, const double *src, size_t m);
+void copy_parallel(double *dst, const double *src, size_t m);
 void launch_spread_permanent(Handle &h);
 void launch_spread_induced(Handle &h, const double *ud, const double *up);
 void launch_fft_convolution(Handle &h);

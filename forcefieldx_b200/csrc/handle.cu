@@ -12,6 +12,7 @@
 #include <cstring>
 #include <map>
 #include <string>
+#include <thread>
 #include <vector>
 
 #include "ffx_internal.cuh"
@@ -620,6 +621,40 @@ bool copy_finite(double *dst, const double *src, size_t m) {
     bad |= (uint64_t)((u & 0x7ff0000000000000ull) == 0x7ff0000000000000ull);
   }
   return bad == 0;
+}
+
+// Large host copies (a batch's coordinates in, its gradients out: tens of MB) split over
+// up to eight host threads, one per 2^18 values (2 MB).
+static int copy_threads(size_t m) {
+  const unsigned hw = std::max(1u, std::thread::hardware_concurrency());
+  return (int)std::min<size_t>(std::min<size_t>(8, hw), std::max<size_t>(1, m >> 18));
+}
+bool copy_finite_parallel(double *dst, const double *src, size_t m) {
+  const int T = copy_threads(m);
+  if (T == 1) return copy_finite(dst, src, m);
+  const size_t chunk = (m + T - 1) / T;
+  std::vector<char> ok(T, 1);
+  std::vector<std::thread> th;
+  for (int t = 1; t < T; t++) {
+    const size_t a = std::min(m, t * chunk), b = std::min(m, a + chunk);
+    th.emplace_back([=, &ok]() { ok[t] = copy_finite(dst + a, src + a, b - a); });
+  }
+  ok[0] = copy_finite(dst, src, std::min(m, chunk));
+  for (std::thread &x : th) x.join();
+  for (char c : ok)
+    if (!c) return false;
+  return true;
+}
+void copy_parallel(double *dst, const double *src, size_t m) {
+  const int T = copy_threads(m);
+  const size_t chunk = (m + T - 1) / T;
+  std::vector<std::thread> th;
+  for (int t = 1; t < T; t++) {
+    const size_t a = std::min(m, t * chunk), b = std::min(m, a + chunk);
+    th.emplace_back([=]() { std::memcpy(dst + a, src + a, (b - a) * sizeof(double)); });
+  }
+  std::memcpy(dst, src, std::min(m, chunk) * sizeof(double));
+  for (std::thread &x : th) x.join();
 }
 }  // namespace ffx
 

@@ -272,7 +272,8 @@ int ffxg_set_image_mode(ffxg_handle *h, int mode);
  * takes by its per-axis passes).
  *   systems[n_systems], params[n_systems]: as for ffxg_create, one per system.
  *   xyz, grad: all systems' coordinates / gradients concatenated in system order
- *     ([total atoms][3]; xyz may be NULL to reuse the last coordinates).
+ *     ([total atoms][3]; xyz may be NULL to reuse the last accepted coordinates;
+ *     after a call rejected with FFXG_ERR_NONFINITE there are none: BAD_ARG).
  *   terms[n_systems][FFXG_N_TERMS]; counts[n_systems][FFXG_N_COUNTS] and
  *   status[n_systems] may be NULL.  Returns the first nonzero status, if any. */
 typedef struct ffxg_batch ffxg_batch;

@@ -152,3 +152,36 @@ def test_staged_batch_of_the_reference_crystals(precision, fixtures):
             for j in range(len(systems)):
                 _same(precision, b.terms[j], grads[j], hist[j], CRYSTALS[j])
         assert b.stages() > 50
+
+
+def test_large_batch_host_copies_and_nonfinite_coordinates():
+    """A batch of ~180,000 atoms, whose coordinate and gradient copies are split over
+    several host threads: every system's result is its own handle's (bit for bit, mixed
+    form); a NaN in the last system's coordinates is rejected (NONFINITE) without running,
+    after which there are no coordinates to reuse (a NULL pointer: BAD_ARG); valid
+    coordinates then give the first results again."""
+    import ctypes
+    from forcefieldx_b200.energy import EnergyException
+    w = batch_workload(n_systems=64, seed=53, n_min=2700, n_max=3000, precision=PRECISION_MIXED)
+    systems, params = [s for s, _ in w], [p for _, p in w]
+    assert 3 * sum(s.n_atoms for s in systems) >= 2 * (1 << 18)   # at least two copy threads
+    checked = [0, 31, 63]
+    hist = {j: _single(systems[j], params[j], [systems[j].xyz, systems[j].xyz])[1] for j in checked}
+    with BatchEnergy(systems, params) as b:
+        xs = [s.xyz for s in systems]
+        for _ in range(2):
+            e0, grads = b.energy_and_gradient(xs)
+        for j in checked:
+            _same(PRECISION_MIXED, b.terms[j], grads[j], hist[j], j)
+        bad = [x.copy() for x in xs]
+        bad[-1][-1, 2] = np.nan
+        with pytest.raises(EnergyException) as ei:
+            b.energy_and_gradient(bad)
+        assert ei.value.status == 5                     # FFXG_ERR_NONFINITE
+        D = ctypes.POINTER(ctypes.c_double)
+        st = b.lib.ffxg_batch_energy(b._b, None, 1, b.terms.ctypes.data_as(D), b._grad.ctypes.data_as(D), None, None)
+        assert st == 1                                  # FFXG_ERR_BAD_ARG: nothing to reuse
+        e1, grads = b.energy_and_gradient(xs)
+        assert np.array_equal(e1, e0)
+        for j in checked:
+            _same(PRECISION_MIXED, b.terms[j], grads[j], hist[j], j)
