@@ -11,7 +11,10 @@
 //     k_many per stage for all its systems (csrc/batch.cu): the blocks of system s are
 //     the consecutive range [pre[s], pre[s + 1]) of one grid, each reading system s's
 //     packed arguments and seeing the VGrid of its own launch.
-// The body cannot tell the two forms apart.  (Floating-point arithmetic whose rounding
+// The body cannot tell the two forms apart.  Bodies whose batch instance ran short of
+// registers take their arguments by const reference: that instance then reads each one
+// from the staged pack in shared memory where it is used, instead of holding them all in
+// registers from the start (the single-system instance reads the parameter bank either way).  (Floating-point arithmetic whose rounding
 // must not depend on the instance -- the compiler may fuse a multiply and an add in one
 // instance and not in the other -- is written with explicit roundings, xmul / xadd / xfma.)
 #pragma once

@@ -331,13 +331,15 @@ __device__ __forceinline__ void k_pair_field(VGrid vg, int n, const int *__restr
 // kCombineGroup lanes per atom: the group interpolates the mesh, then its lane q < 6
 // finishes component q (D x, y, z, CR x, y, z).
 template <int MODE, typename T>
-__device__ __forceinline__ void k_pcg_combine(VGrid vg, 
-    int n, const int *__restrict__ igrid, const T *__restrict__ spl, const typename Vec2<T>::type *__restrict__ mesh,
-    int nfx, int nfy, int nfz, const FieldXform &xf, const double *__restrict__ tpair, const double *__restrict__ vD,
-    const double *__restrict__ vP, double aewald3, const double *__restrict__ polar,
-    const double *__restrict__ udirD, const double *__restrict__ udirP, double *p, double *pP, double *tp,
-    int first, const double *__restrict__ r, const double *__restrict__ rP, double *outD, double *outP, T *recP,
-    double *part, unsigned *counter, double *tot) {
+__device__ __forceinline__ void k_pcg_combine(
+    VGrid vg, int const &n, const int *__restrict__ const &igrid, const T *__restrict__ const &spl,
+    const typename Vec2<T>::type *__restrict__ const &mesh, int const &nfx, int const &nfy, int const &nfz,
+    const FieldXform &xf, const double *__restrict__ const &tpair, const double *__restrict__ const &vD,
+    const double *__restrict__ const &vP, double const &aewald3, const double *__restrict__ const &polar,
+    const double *__restrict__ const &udirD, const double *__restrict__ const &udirP, double * const &p,
+    double * const &pP, double * const &tp, int const &first, const double *__restrict__ const &r,
+    const double *__restrict__ const &rP, double * const &outD, double * const &outP, T * const &recP,
+    double * const &part, unsigned * const &counter, double * const &tot) {
   constexpr int G = kCombineGroup;
   const int lane = threadIdx.x & 31, sub = lane & (G - 1), g0 = lane & ~(G - 1);
   const int i = (vg.bid * blockDim.x + threadIdx.x) / G;
@@ -411,11 +413,13 @@ __device__ __forceinline__ void k_pcg_combine(VGrid vg,
 // is finished into d_scalars and the last block forms beta = r.z_new / r.z_old
 // (UpdateConjugateLoop, Fletcher-Reeves; a zero r.z_old counts as 1).
 template <bool INIT, typename T, int G>
-__device__ __forceinline__ void k_pcg_precond(VGrid vg, 
-    int n, const int *__restrict__ prl, const int *__restrict__ prl_cnt, int capP,
-    const PairRec<T> *__restrict__ coefP, const T *__restrict__ coefPB, const T *__restrict__ recP,
-    const double *__restrict__ polar, const double *__restrict__ r, const double *__restrict__ rP, double s,
-    double *zz, double *zP, double *p, double *pP, T *recF, double *part, unsigned *counter, double *tot) {
+__device__ __forceinline__ void k_pcg_precond(
+    VGrid vg, int const &n, const int *__restrict__ const &prl, const int *__restrict__ const &prl_cnt,
+    int const &capP, const PairRec<T> *__restrict__ const &coefP, const T *__restrict__ const &coefPB,
+    const T *__restrict__ const &recP, const double *__restrict__ const &polar,
+    const double *__restrict__ const &r, const double *__restrict__ const &rP, double const &s,
+    double * const &zz, double * const &zP, double * const &p, double * const &pP, T * const &recF,
+    double * const &part, unsigned * const &counter, double * const &tot) {
   constexpr int GPW = 32 / G;
   constexpr int QPL = (6 + G - 1) / G;   // components finished per lane: q = sub, sub + G, ...
   const int lane = threadIdx.x & 31, sub = lane & (G - 1), gi = lane / G, g0 = lane & ~(G - 1);

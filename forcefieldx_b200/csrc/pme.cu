@@ -279,9 +279,10 @@ __device__ __forceinline__ void k_spread_permanent(VGrid vg, int n, const double
 }
 
 template <typename S>
-__device__ __forceinline__ void k_spread_induced(VGrid vg, int n, const double *__restrict__ ud, const double *__restrict__ up,
-                                 const S *__restrict__ spl, const int *__restrict__ igrid, int nfx, int nfy,
-                                 int nfz, double2 *grid, const PmeConst &pc, int *flags) {
+__device__ __forceinline__ void k_spread_induced(
+    VGrid vg, int const &n, const double *__restrict__ const &ud, const double *__restrict__ const &up,
+    const S *__restrict__ const &spl, const int *__restrict__ const &igrid, int const &nfx, int const &nfy,
+    int const &nfz, double2 * const &grid, const PmeConst &pc, int * const &flags) {
   const int warp = (vg.bid * blockDim.x + threadIdx.x) >> 5;
   const int lane = threadIdx.x & 31;
   if (warp >= n || lane >= 25) return;

@@ -53,15 +53,18 @@ struct Excl {
 // so the field of any dipole set is -A u_k + B (u_k . r) r; entries inside the
 // preconditioner cutoff also store the Ewald-free pair (pme/PCGSolver.java:1300-1331).
 template <typename R>
-__device__ __forceinline__ void k_realspace_field(VGrid vg, 
-    int n, const double *__restrict__ x, const double *__restrict__ y, const double *__restrict__ z, const Box &bx,
-    const double *__restrict__ gm, const double *__restrict__ ipdamp, const double *__restrict__ thole,
-    const int *__restrict__ nbr, const int *__restrict__ nbr_cnt, int cap, const int *__restrict__ nbr_sh,
-    double off2, double pcut2, int *ewl, int *ewl_cnt, int capE, int *ewl_sh, int *prl, int *prl_cnt, int capP,
-    PairRec<R> *coefE, R *coefEB,
-    PairRec<R> *coefP, R *coefPB, const Excl &ex, const EwaldCoef &ec, const ScaleTables &c_scales,
-    double *fieldD, double *fieldP, int *flags, const double2 *__restrict__ pos, const R *__restrict__ rec,
-    const int *__restrict__ nbl, const int *__restrict__ nbl_cnt, int capN) {
+__device__ __forceinline__ void k_realspace_field(
+    VGrid vg, int const &n, const double *__restrict__ const &x, const double *__restrict__ const &y,
+    const double *__restrict__ const &z, const Box &bx, const double *__restrict__ const &gm,
+    const double *__restrict__ const &ipdamp, const double *__restrict__ const &thole,
+    const int *__restrict__ const &nbr, const int *__restrict__ const &nbr_cnt, int const &cap,
+    const int *__restrict__ const &nbr_sh, double const &off2, double const &pcut2, int * const &ewl,
+    int * const &ewl_cnt, int const &capE, int * const &ewl_sh, int * const &prl, int * const &prl_cnt,
+    int const &capP, PairRec<R> * const &coefE, R * const &coefEB, PairRec<R> * const &coefP, R * const &coefPB,
+    const Excl &ex, const EwaldCoef &ec, const ScaleTables &c_scales, double * const &fieldD,
+    double * const &fieldP, int * const &flags, const double2 *__restrict__ const &pos,
+    const R *__restrict__ const &rec, const int *__restrict__ const &nbl, const int *__restrict__ const &nbl_cnt,
+    int const &capN) {
   using V2 = typename Vec2<R>::type;
   const int warp = (vg.bid * blockDim.x + threadIdx.x) >> 5;
   const int lane = threadIdx.x & 31;

@@ -34,18 +34,18 @@ __device__ __forceinline__ unsigned vexcl_code(int i, int k, const int *__restri
 
 // ALCH: the softcore variant (launched only while soft atoms are set).
 template <typename R, bool ALCH>
-__device__ __forceinline__ void k_vdw(VGrid vg, int n, const double *__restrict__ rx, const double *__restrict__ ry,
-                                             const double *__restrict__ rz, const Box &bx, const int *__restrict__ vtype,
-                                             int ntypes, const double *__restrict__ vrad,
-                                             const double *__restrict__ veps, const int *__restrict__ nbr,
-                                             const int *__restrict__ nbr_cnt, int cap, const int *__restrict__ nbr_sh,
-                                             const int *__restrict__ eptr,
-                                             const int *__restrict__ ek, const unsigned *__restrict__ ecode,
-                                             const int *__restrict__ elo, const int *__restrict__ ehi, const VdwForm &vf,
-                                             const ScaleTables &c_vscales, int gradient, double *eatom, long long *catom, double *gred,
-                                             const int *__restrict__ soft, const int *__restrict__ mol, const AlchConst &al,
-                                             double *edl, double *ed2l, double *lgred,
-                                             const double2 *__restrict__ rpos) {
+__device__ __forceinline__ void k_vdw(
+    VGrid vg, int const &n, const double *__restrict__ const &rx, const double *__restrict__ const &ry,
+    const double *__restrict__ const &rz, const Box &bx, const int *__restrict__ const &vtype, int const &ntypes,
+    const double *__restrict__ const &vrad, const double *__restrict__ const &veps,
+    const int *__restrict__ const &nbr, const int *__restrict__ const &nbr_cnt, int const &cap,
+    const int *__restrict__ const &nbr_sh, const int *__restrict__ const &eptr,
+    const int *__restrict__ const &ek, const unsigned *__restrict__ const &ecode,
+    const int *__restrict__ const &elo, const int *__restrict__ const &ehi, const VdwForm &vf,
+    const ScaleTables &c_vscales, int const &gradient, double * const &eatom, long long * const &catom,
+    double * const &gred, const int *__restrict__ const &soft, const int *__restrict__ const &mol,
+    const AlchConst &al, double * const &edl, double * const &ed2l, double * const &lgred,
+    const double2 *__restrict__ const &rpos) {
   struct Queue { R x[64], y[64], z[64], r[64], m[64]; int k[64], t[64], f[64]; };
   __shared__ Queue qbuf[8];
   const int warp = (vg.bid * blockDim.x + threadIdx.x) >> 5;
