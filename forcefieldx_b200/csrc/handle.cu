@@ -760,6 +760,19 @@ static void emit_back(Handle &h, double *d_grad_xyz) {
   timer_end(h, tk);
   if (h.capturing && !h.vacuum && !h.batch_branch) cudaStreamWaitEvent(h.stream, h.ev_vdw_join, 0);
   tk = timer_begin(h, FFXG_STAGE_GRADIENT);
+  // In a captured evaluation the energy sums, which read only the per-atom energy and
+  // count rows (complete here), are a branch beside the torque gather and the gradient
+  // assembly.
+  const bool fork_sums = h.capturing && !h.vacuum && !h.batch_branch && !h.step.lam;
+  if (fork_sums) {
+    cudaEventRecord(h.ev_fork, h.stream);
+    cudaStreamWaitEvent(h.aux, h.ev_fork, 0);
+    cudaStream_t main = h.stream;
+    h.stream = h.aux;
+    launch_reduce_results(h);
+    h.stream = main;
+    cudaEventRecord(h.ev_join, h.aux);
+  }
   if (h.want_grad) {
     launch_torque(h);
     launch_assemble(h, d_grad_xyz);
@@ -777,7 +790,8 @@ static void emit_back(Handle &h, double *d_grad_xyz) {
     if (h.vacuum) zero_doubles(h, h.d_lgred + 3 * (size_t)h.n, 3 * (size_t)h.n);
     launch_lambda_grad_add(h, h.d_lgred + 3 * (size_t)h.n);
   }
-  launch_reduce_results(h);
+  if (fork_sums) cudaStreamWaitEvent(h.stream, h.ev_join, 0);
+  else launch_reduce_results(h);
   timer_end(h, tk);
   copy_result(h, h.h_scalars, h.d_result, kEnergyRows * sizeof(double));
   copy_result(h, h.h_flags + 2, h.d_cresult, 2 * sizeof(long long));
